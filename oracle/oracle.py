@@ -1,0 +1,521 @@
+"""Oracle (test infrastructure only -- never imported by the product path).
+
+A CPU restatement of the reference Tractor's forward-model hot path in numpy
+(FP64) over the plain-C kernels in oracle/oracle_c.c.  tests/, the smoke check
+and bench.py's CPU-baseline leg use it as the checker.  Each function cites the
+reference lines it restates; paths are relative to the reference project.
+
+Parity pin: tests/test_oracle_pin.py checks these functions against the
+reference itself (run from its source tree through oracle/refharness.py, in the
+development container) and against the committed fixtures in tests/golden/,
+which were generated from the reference by tests/golden/make_golden.py.
+"""
+import ctypes
+import json
+import math
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, 'liboracle_c.so')
+_TABLES = os.path.join(os.path.dirname(_HERE), 'tractor_b200', 'data', 'profile_tables.json')
+_lib = None
+
+
+def build_lib():
+    """Compile oracle_c.c (plain gcc, no device code)."""
+    src = os.path.join(_HERE, 'oracle_c.c')
+    if (os.path.exists(_LIB_PATH) and
+            os.path.getmtime(_LIB_PATH) >= os.path.getmtime(src)):
+        return _LIB_PATH
+    cmd = 'gcc -O2 -fPIC -shared -std=gnu99 -o %s %s -lm' % (_LIB_PATH, src)
+    if os.system(cmd) != 0:
+        raise RuntimeError('oracle build failed: ' + cmd)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build_lib()
+        L = ctypes.CDLL(_LIB_PATH)
+        I, D = ctypes.c_int, ctypes.c_double
+        P = ctypes.c_void_p
+        L.orc_mog_grid.argtypes = [I, I, I, I, D, D, I, P, P, P, P]
+        L.orc_mog_approx3.argtypes = [I, I, I, I, D, D, D, I, P, P, P, P, P, P, I, I, I, P]
+        L.orc_mog_masked.argtypes = [I, I, I, I, D, D, I, P, P, P, P, P, P, P]
+        L.orc_lanczos3_taps.argtypes = [D, P]
+        L.orc_lanczos_shift3f.argtypes = [P, P, I, I, D, D, P]
+        L.orc_fourier_mog.argtypes = [I, P, P, I, P, I, P, P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+# ---------------------------------------------------------------------------
+# Native kernels
+# ---------------------------------------------------------------------------
+
+def mog_grid(x0, x1, y0, y1, fx, fy, amp, mean, var):
+    """c_gauss_2d_grid (tractor/mix.i:452-524); float64 (y1-y0, x1-x0)."""
+    amp = np.ascontiguousarray(amp, np.float64)
+    mean = np.ascontiguousarray(mean, np.float64).reshape(-1, 2)
+    var = np.ascontiguousarray(var, np.float64).reshape(-1, 2, 2)
+    out = np.zeros((y1 - y0, x1 - x0), np.float64)
+    r = lib().orc_mog_grid(int(x0), int(x1), int(y0), int(y1), float(fx), float(fy),
+                           len(amp), _p(amp), _p(mean), _p(var), _p(out))
+    assert r == 0
+    return out
+
+
+def mog_approx3(x0, x1, y0, y1, fx, fy, minval, amp, mean, var, xc, yc,
+                minradius=3, derivs=False):
+    """c_gauss_2d_approx3 (tractor/approx3.c); returns (out, dx, dy, bbox)."""
+    amp = np.ascontiguousarray(amp, np.float64)
+    mean = np.ascontiguousarray(mean, np.float64).reshape(-1, 2)
+    var = np.ascontiguousarray(var, np.float64).reshape(-1, 2, 2)
+    out = np.zeros((y1 - y0, x1 - x0), np.float64)
+    dxo = np.zeros_like(out) if derivs else None
+    dyo = np.zeros_like(out) if derivs else None
+    bbox = np.zeros(4, np.int32)
+    r = lib().orc_mog_approx3(int(x0), int(x1), int(y0), int(y1), float(fx), float(fy),
+                              float(minval), len(amp), _p(amp), _p(mean), _p(var), _p(out),
+                              _p(dxo) if derivs else None, _p(dyo) if derivs else None,
+                              int(xc), int(yc), int(minradius), _p(bbox))
+    assert r == 0
+    return out, dxo, dyo, tuple(int(b) for b in bbox)
+
+
+def mog_masked(x0, y0, mask, fx, fy, amp, mean, var, derivs=False):
+    """c_gauss_2d_masked (tractor/gauss_masked.c); float32 outputs."""
+    amp = np.ascontiguousarray(amp, np.float32)
+    mean = np.ascontiguousarray(mean, np.float32).reshape(-1, 2)
+    var = np.ascontiguousarray(var, np.float32).reshape(-1, 2, 2)
+    mask = np.ascontiguousarray(mask, np.uint8)
+    h, w = mask.shape
+    out = np.zeros((h, w), np.float32)
+    dxo = np.zeros_like(out) if derivs else None
+    dyo = np.zeros_like(out) if derivs else None
+    lib().orc_mog_masked(int(x0), int(y0), w, h, float(fx), float(fy), len(amp), _p(amp),
+                         _p(mean), _p(var), _p(out), _p(dxo) if derivs else None,
+                         _p(dyo) if derivs else None, _p(mask))
+    return out, dxo, dyo
+
+
+def lanczos3_taps(dx):
+    """lanczos_filter_3 (tractor/mp_fourier.i:355-402)."""
+    t = np.zeros(7, np.float64)
+    lib().orc_lanczos3_taps(float(dx), _p(t))
+    return t
+
+
+def lanczos_shift(img, dx, dy):
+    """lanczos_shift_3f (tractor/mp_fourier.i:405-429) on a float32 image."""
+    img = np.ascontiguousarray(img, np.float32)
+    H, W = img.shape
+    out = np.zeros_like(img)
+    work = np.zeros(H * W, np.float32)
+    lib().orc_lanczos_shift3f(_p(img), _p(out), H, W, float(dx), float(dy), _p(work))
+    return out
+
+
+def fourier_mog(amp, var, v, w):
+    """gaussian_fourier_transform_zero_mean (tractor/mp_fourier.i:431-478)."""
+    amp = np.ascontiguousarray(amp, np.float64)
+    var = np.ascontiguousarray(var, np.float64).reshape(-1, 2, 2)
+    v = np.ascontiguousarray(v, np.float64)
+    w = np.ascontiguousarray(w, np.float64)
+    out = np.zeros((len(w), len(v)), np.float64)
+    lib().orc_fourier_mog(len(amp), _p(amp), _p(var), len(v), _p(v), len(w), _p(w), _p(out))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Profiles
+# ---------------------------------------------------------------------------
+_tables = None
+
+
+def tables():
+    global _tables
+    if _tables is None:
+        with open(_TABLES) as f:
+            _tables = json.load(f)
+    return _tables
+
+
+def exp_profile():
+    """Exp 6-component mixture, tractor/mixture_profiles.py:20-24 (normalised)."""
+    t = tables()['exp']
+    return np.array(t['amp']), np.array(t['var'])
+
+
+def dev_profile():
+    """deV 8 components + delta core, tractor/mixture_profiles.py:26-38."""
+    t = tables()['dev']
+    return np.array(t['amp']), np.array(t['var'])
+
+
+_sersic_splines = None
+
+
+def sersic_profile(n):
+    """SersicMixture._getProfile (tractor/sersic.py:288-342) with scipy's
+    InterpolatedUnivariateSpline built from the raw grid as the reference does
+    (sersic.py:242-282).  Returns (amp[K], var[K]) sorted by variance."""
+    global _sersic_splines
+    from scipy.interpolate import InterpolatedUnivariateSpline as IUS
+    S = tables()['sersic']
+    if _sersic_splines is None:
+        fits = []
+        for r in S['ranges']:
+            grid = r['grid']
+            ns = [g[0] for g in grid]
+            k = 3 if len(grid) > 3 else 1
+            af = [IUS(ns, [g[1][i] for g in grid], k=k) for i in range(r['K'])]
+            vf = [IUS(ns, [np.log(g[2][i]) for g in grid], k=k) for i in range(r['K'])]
+            fits.append((r['lo'], r['hi'], af, vf))
+        core = IUS([c[0] for c in S['cores']], [c[1] for c in S['cores']], k=3)
+        _sersic_splines = (fits, core)
+    fits, core = _sersic_splines
+    lowest, highest = fits[0][0], fits[-1][1]
+    if n <= lowest:
+        m = fits[0]
+        n = lowest
+    elif n >= highest:
+        m = fits[-1]
+        n = highest
+    else:
+        m = [f for f in fits if f[0] <= n < f[1]]
+        assert len(m) == 1
+        m = m[0]
+    lo, hi, af, vf = m
+    amps = np.array([f(n) for f in af])
+    amps /= amps.sum()
+    varr = np.exp(np.array([f(n) for f in vf]))
+    if n > 1.:
+        c = core(n)
+        amps *= (1. - c) / amps.sum()
+        amps = np.append(amps, c)
+        varr = np.append(varr, 0.)
+    I = np.argsort(varr)
+    return amps[I], varr[I]
+
+
+def diag_var(var):
+    """MixtureOfGaussians.set_var for scalar variances (mixture_profiles.py:75-81)."""
+    var = np.asarray(var, np.float64)
+    V = np.zeros((len(var), 2, 2))
+    V[:, 0, 0] = var
+    V[:, 1, 1] = var
+    return V
+
+
+# ---------------------------------------------------------------------------
+# Shapes (pixel-space transforms)
+# ---------------------------------------------------------------------------
+
+def galaxyshape_basis(re, ab, phi):
+    """GalaxyShape.getRaDecBasis, tractor/galaxy.py:73-89."""
+    p = np.deg2rad(90 - phi)
+    re_deg = max(1. / 30, re) / 3600.
+    cp, sp = np.cos(p), np.sin(p)
+    return re_deg * np.array([[cp, sp * ab], [-sp, cp * ab]])
+
+
+def ellipseE_basis(re, e1, e2):
+    """EllipseE.getRaDecBasis, tractor/ellipses.py:126-155."""
+    theta = math.atan2(e2, e1) / 2.
+    ct, st = math.cos(theta), math.sin(theta)
+    e = math.hypot(e1, e2)
+    maxab = 1000.
+    ab = maxab if e >= 1. else min(maxab, (1. + e) / (1. - e))
+    r_deg = re / 3600.
+    return r_deg * np.array([[ct / ab, st], [-st / ab, ct]])
+
+
+def ellipseESoft_to_E(logre, ee1, ee2, maxe=0.999999):
+    """EllipseESoft -> (re, e1, e2), tractor/ellipses.py:55-62, 219-238."""
+    re = math.exp(logre)
+    ee = math.hypot(ee1, ee2)
+    e = min(maxe, 1. - math.exp(-ee))
+    theta = math.atan2(ee2, ee1) / 2.
+    return re, e * math.cos(2. * theta), e * math.sin(2. * theta)
+
+
+def ellipseE_from_rabphi(r, ba, phi):
+    """EllipseE.fromRAbPhi, tractor/ellipses.py:64-71."""
+    ab = 1. / ba
+    e = (ab - 1) / (ab + 1)
+    angle = math.radians(2. * (-phi))
+    return r, e * math.cos(angle), e * math.sin(angle)
+
+
+def nullwcs_cdinv(pixscale=1.):
+    """NullWCS.cd_inverse, tractor/wcs.py:25-28."""
+    return np.eye(2) / (pixscale / 3600.)
+
+
+def sheared(amp, var_scalar, Tinv):
+    """apply_shear (mixture_profiles.py:146-155): var -> T V T^T."""
+    V = diag_var(var_scalar)
+    return np.asarray(amp, np.float64), Tinv @ V @ Tinv.T
+
+
+def convolve(amp, mean, var, pamp, pmean, pvar):
+    """MixtureOfGaussians.convolve, mixture_profiles.py:158-172: for each PSF
+    component (outer loop) a block of all galaxy components."""
+    K, P = len(amp), len(pamp)
+    namp = np.zeros(K * P)
+    nmean = np.zeros((K * P, 2))
+    nvar = np.zeros((K * P, 2, 2))
+    for p in range(P):
+        namp[p * K:(p + 1) * K] = amp * pamp[p]
+        nmean[p * K:(p + 1) * K] = mean + pmean[p]
+        nvar[p * K:(p + 1) * K] = var + pvar[p]
+    return namp, nmean, nvar
+
+
+def circular_psf_mog(sigmas, weights):
+    """getCircularMog (tractor/psf.py:931-944): float32 tables."""
+    K = len(weights)
+    amp = np.array(weights).astype(np.float32)
+    mean = np.zeros((K, 2), np.float32)
+    var = np.zeros((K, 2, 2), np.float32)
+    for k in range(K):
+        var[k, 0, 0] = var[k, 1, 1] = sigmas[k] ** 2
+    return amp, mean, var
+
+
+# ---------------------------------------------------------------------------
+# Geometry helpers
+# ---------------------------------------------------------------------------
+
+def overlapping_region(xlo, xhi, xmin, xmax):
+    """tractor/patch.pyx:20-65 (absolute slices)."""
+    if xlo > xmax or xhi < xmin or xlo > xhi or xmin > xmax:
+        return None
+    lo = max(xlo, xmin)
+    hi = min(xhi, xmax)
+    return slice(lo, hi + 1), slice(lo - xlo, lo - xlo + hi - lo + 1)
+
+
+def fft_size(radius):
+    """PixelizedPSF.getFourierTransformSize, tractor/psf.py:209-212."""
+    return int(2 ** int(np.ceil(np.log2(radius * 2.))))
+
+
+def pad_psf(img, H, W):
+    """PixelizedPSF._padInImage, tractor/psf.py:214-247."""
+    ph, pw = img.shape
+    sub = img
+    if H >= ph:
+        y0 = (H - ph) // 2
+        cy = y0 + ph // 2
+    else:
+        y0 = 0
+        cut = (ph - H) // 2
+        sub = sub[cut:cut + H, :]
+        cy = ph // 2 - cut
+    if W >= pw:
+        x0 = (W - pw) // 2
+        cx = x0 + pw // 2
+    else:
+        x0 = 0
+        cut = (pw - W) // 2
+        sub = sub[:, cut:cut + W]
+        cx = pw // 2 - cut
+    sh, sw = sub.shape
+    pad = np.zeros((H, W), img.dtype)
+    pad[y0:y0 + sh, x0:x0 + sw] = sub
+    return pad, cx, cy
+
+
+def psf_fourier(psf_img, sz, normalized=False):
+    """PixelizedPSF.getFourierTransform (tractor/psf.py:249-280): complex64
+    rfft2 of the padded PSF; NormalizedPsf (psf.py:947-953) divides by |P[0,0]|."""
+    pad, cx, cy = pad_psf(np.asarray(psf_img, np.float32), sz, sz)
+    P = np.fft.rfft2(pad).astype(np.complex64)
+    if normalized:
+        n = np.abs(P[0][0])
+        if n != 0:
+            P /= n
+    v = np.fft.rfftfreq(sz)
+    w = np.fft.fftfreq(sz)
+    return P, (cx, cy), (sz, sz), (v, w)
+
+
+def fft_halfsize_for_mask(px, py, x0, y0, mw, mh, psfh, psfw):
+    """Patch half-size for the FFT path with a ModelMask, galaxy.py:339-351."""
+    x1 = x0 + mw
+    y1 = y0 + mh
+    hs = max(mh / 2., mw / 2.)
+    hs = max(hs, max(max(1 + px - x0, 1 + x1 - px), max(1 + py - y0, 1 + y1 - py)))
+    hs = max(hs, max(psfw / 2., psfh / 2.))
+    return int(np.ceil(hs))
+
+
+# ---------------------------------------------------------------------------
+# Unit-flux galaxy patches
+# ---------------------------------------------------------------------------
+
+def galaxy_fft_masked(amp, var2, px, py, psf_img, mask_x0, mask_y0, mw, mh,
+                      normalized_psf=False, force_halfsize=None):
+    """ProfileGalaxy._realGetUnitFluxModelPatch FFT branch with a ModelMask and
+    a non-hybrid pixelized PSF (tractor/galaxy.py:336-519).  `var2` is the
+    sheared (pixel-space) 2x2 covariance per component.  Returns the float32
+    (mh, mw) unit-flux patch with origin (mask_x0, mask_y0), plus the split
+    (mux, muy, sx, sy, sz) for diagnostics."""
+    psfh, psfw = psf_img.shape
+    hs = fft_halfsize_for_mask(px, py, mask_x0, mask_y0, mw, mh, psfh, psfw)
+    if force_halfsize is not None:
+        hs = int(np.ceil(force_halfsize))
+    sz = fft_size(hs)
+    P, (cx, cy), (pH, pW), (v, w) = psf_fourier(psf_img, sz, normalized_psf)
+    dx = px - cx
+    dy = py - cy
+    mux = dx - mask_x0
+    muy = dy - mask_y0
+    sx = int(np.round(mux))
+    sy = int(np.round(muy))
+    mux -= sx
+    muy -= sy
+    assert abs(mux) <= 0.5 and abs(muy) <= 0.5
+    F = fourier_mog(amp, var2, v, w)
+    G = np.fft.irfftn(F * P)
+    G = G.astype(np.float32)
+    if mux != 0.0 or muy != 0.0:
+        G = lanczos_shift(G, mux, muy)
+    gh, gw = G.shape
+    if sx != 0 or sy != 0:
+        out = np.zeros((mh, mw), np.float32)
+        ry = overlapping_region(-sy, -sy + mh - 1, 0, gh - 1)
+        rx = overlapping_region(-sx, -sx + mw - 1, 0, gw - 1)
+        if ry is not None and rx is not None:
+            out[ry[1], rx[1]] = G[ry[0], rx[0]]
+        G = out
+    if gh > mh or gw > mw:
+        G = G[:mh, :mw]
+    return G, (mux, muy, sx, sy, sz)
+
+
+def galaxy_mog_patch(amp, var_scalar, Tinv, px, py, pamp, pmean, pvar,
+                     x0, x1, y0, y1, minval=0.):
+    """MoG branch without a ModelMask (tractor/galaxy.py:307-326 ->
+    mixture_profiles.py:425-438): affine profile at (px, py), convolved with
+    the PSF, rendered exactly (minval == 0) or by the ring evaluator.
+    Returns (x0, y0, patch float64)."""
+    a = np.asarray(amp, np.float64)
+    V = Tinv @ diag_var(var_scalar) @ Tinv.T
+    mean = np.zeros((len(a), 2)) + np.array([px, py])
+    ca, cm, cv = convolve(a, mean, V, np.asarray(pamp, np.float64),
+                          np.asarray(pmean, np.float64), np.asarray(pvar, np.float64))
+    if minval == 0. or minval is None:
+        return x0, y0, mog_grid(x0, x1, y0, y1, 0., 0., ca, cm, cv)
+    cx = int(cm[0, 0])
+    cy = int(cm[0, 1])
+    if cx < x0 - 100 or cx > x1 + 100 or cy < y0 - 100 or cy > y1 + 100:
+        return None
+    out, _, _, (sx0, sx1, sy0, sy1) = mog_approx3(x0, x1, y0, y1, 0., 0., minval,
+                                                  ca, cm, cv, cx, cy, 3)
+    return x0 + sx0, y0 + sy0, out[sy0:sy1, sx0:sx1].copy()
+
+
+def galaxy_mog_masked_rect(amp, var_scalar, Tinv, px, py, pamp, pmean, pvar,
+                           mx0, my0, mw, mh):
+    """MoG branch with a rectangular ModelMask (galaxy.py:320-326): exact grid
+    over the mask."""
+    return galaxy_mog_patch(amp, var_scalar, Tinv, px, py, pamp, pmean, pvar,
+                            mx0, mx0 + mw, my0, my0 + mh, 0.)[2]
+
+
+def hogg_halfsize(re_pix_radius, px, py, W, H, psf_radius):
+    """HoggGalaxy._getUnitFluxPatchSize, tractor/galaxy.py:678-691 (pixscale 1:
+    `re_pix_radius` = nre * re / pixscale)."""
+    hs = max(1., re_pix_radius)
+    imsize = max(px, W - 1 - px, py, H - 1 - py) + 1
+    hs = min(hs, imsize)
+    hs = max(hs, psf_radius)
+    return int(np.ceil(hs))
+
+
+def image_extent(px, py, halfsize, W, H):
+    """No-mask extent selection, tractor/galaxy.py:274-286."""
+    rx = overlapping_region(int(np.floor(px - halfsize)), int(np.ceil(px + halfsize + 1)), 0, W - 1)
+    ry = overlapping_region(int(np.floor(py - halfsize)), int(np.ceil(py + halfsize + 1)), 0, H - 1)
+    if rx is None or ry is None:
+        return None
+    return rx[0].start, rx[0].stop, ry[0].start, ry[0].stop
+
+
+# ---------------------------------------------------------------------------
+# Point sources
+# ---------------------------------------------------------------------------
+
+def mogpsf_point_patch(pamp, pmean, pvar, px, py, x0, x1, y0, y1):
+    """GaussianMixturePSF.getPointSourcePatch exact branch (psf.py:458-528
+    with minval == 0): grid of the PSF mixture offset by (px, py)."""
+    return mog_grid(x0, x1, y0, y1, px, py, pamp, pmean, pvar)
+
+
+def pixpsf_point_patch_masked(psf_img, px, py, mx0, my0, mw, mh):
+    """PixelizedPSF.getPointSourcePatch with a ModelMask (psf.py:137-207)."""
+    img = np.asarray(psf_img, np.float32)
+    H, W = img.shape
+    ix = int(round(float(px)))
+    iy = int(round(float(py)))
+    dx = px - ix
+    dy = py - iy
+    x0 = ix - W // 2
+    y0 = iy - H // 2
+    if (mx0 >= x0 + W) or (mx0 + mw <= x0) or (my0 >= y0 + H) or (my0 + mh <= y0):
+        return None
+    L = 3
+    mm = np.zeros((mh + 2 * L, mw + 2 * L), np.float32)
+    ry = overlapping_region(my0 - y0 - L, my0 - y0 + mh - 1 + L, 0, H - 1)
+    rx = overlapping_region(mx0 - x0 - L, mx0 - x0 + mw - 1 + L, 0, W - 1)
+    mm[ry[1], rx[1]] = img[ry[0], rx[0]]
+    mm = lanczos_shift(mm, dx, dy)
+    return mm[L:-L, L:-L]
+
+
+# ---------------------------------------------------------------------------
+# Likelihood and least squares
+# ---------------------------------------------------------------------------
+
+def chi_image(data, model, inverr):
+    """Tractor.getChiImage, tractor/engine.py:455-473."""
+    return (data - model) * inverr
+
+
+def log_likelihood(chis):
+    """Tractor.getLogLikelihood, tractor/engine.py:475-479 (FP64 sum)."""
+    return -0.5 * sum(float((c.astype(float) ** 2).sum()) for c in chis)
+
+
+def lsq_update(A_cols, b, priors=None):
+    """The solution LsqrOptimizer.getUpdateDirection converges to
+    (tractor/lsqr_optimizer.py:328-644): columns of A = J * inverr, scaled to
+    unit L2 norm (:423-424, :470-489, dropping |v| <= 1e-8 after scaling),
+    b = chi; x = argmin ||A x - b||; X = x / colscale.  Solved densely in FP64.
+    `A_cols` is (Nrows, P); `priors` an optional (rows, b) pair appended."""
+    A = np.asarray(A_cols, np.float64)
+    b = np.asarray(b, np.float64)
+    if priors is not None:
+        A = np.vstack([A, priors[0]])
+        b = np.concatenate([b, priors[1]])
+    cs = np.sqrt((A ** 2).sum(axis=0))
+    As = np.where(cs > 0, A / np.where(cs > 0, cs, 1.), 0.)
+    As[np.abs(As) <= 1e-8] = 0.
+    x, *_ = np.linalg.lstsq(As, b, rcond=None)
+    X = np.where(cs > 0, x / np.where(cs > 0, cs, 1.), 0.)
+    return X
+
+
+def line_search_alphas():
+    """Default step sizes of Optimizer.tryUpdates, tractor/optimize.py:426-428."""
+    return np.append(2. ** np.arange(-10, 1), [np.sqrt(2.), 2.])
