@@ -1,0 +1,198 @@
+"""Generates the golden fixtures in tests/golden/ by running the reference
+Tractor itself (imported from its source tree through oracle/refharness.py,
+with its own C kernels compiled by oracle/build_ref.sh).
+
+Each fixture stores the scenario's inputs and the reference's outputs, so the
+oracle and the CUDA path can be checked against the reference without the
+reference being present.  All scenarios are seeded.  Run from the repository
+root in the development container:
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def moffat(size=63, fwhm=4.0, beta=3.0):
+    alpha = fwhm / (2 * np.sqrt(2 ** (1 / beta) - 1))
+    y, x = np.mgrid[:size, :size] - size // 2
+    img = (1 + (x ** 2 + y ** 2) / alpha ** 2) ** (-beta)
+    return (img / img.sum()).astype(np.float32)
+
+
+def patches_to_arrays(plist):
+    """[Patch|None] -> (present flags, x0s, y0s, shapes, concatenated pixels)."""
+    present, x0, y0, hh, ww, pix = [], [], [], [], [], []
+    for p in plist:
+        if p is None or p.patch is None:
+            present.append(0)
+            x0.append(0)
+            y0.append(0)
+            hh.append(0)
+            ww.append(0)
+            continue
+        present.append(1)
+        x0.append(p.x0)
+        y0.append(p.y0)
+        hh.append(p.patch.shape[0])
+        ww.append(p.patch.shape[1])
+        pix.append(np.asarray(p.patch, np.float64).ravel())
+    return dict(present=np.array(present), x0=np.array(x0), y0=np.array(y0), h=np.array(hh),
+                w=np.array(ww), pix=np.concatenate(pix) if pix else np.zeros(0))
+
+
+def main():
+    from oracle import refharness
+    t = refharness.load()
+    from tractor import (Image, PixPos, Flux, NanoMaggies, LinearPhotoCal, GaussianMixturePSF,
+                         NCircularGaussianPSF, PixelizedPSF, PointSource, Tractor, EllipseE,
+                         EllipseESoft)
+    from tractor.galaxy import ExpGalaxy, DevGalaxy, GalaxyShape, FixedCompositeGalaxy
+    from tractor.sersic import SersicGalaxy, SersicIndex
+    from tractor.patch import ModelMask
+    from tractor import mp_fourier, mix
+
+    # -- 1. kernel-level vectors -------------------------------------------
+    rng = np.random.default_rng(100)
+    K = 7
+    amp = rng.uniform(0.1, 1, K)
+    mean = rng.normal(size=(K, 2))
+    var = np.zeros((K, 2, 2))
+    for k in range(K):
+        a = rng.normal(size=(2, 2))
+        var[k] = a @ a.T + 0.4 * np.eye(2)
+    grid = np.zeros((24, 31))
+    mix.c_gauss_2d_grid(-5, 26, 3, 27, 7.3, 11.6, amp, mean, var, grid)
+    ap = np.zeros((40, 44))
+    axd = np.zeros_like(ap)
+    ayd = np.zeros_like(ap)
+    rtn, sx0, sx1, sy0, sy1 = mix.c_gauss_2d_approx3(0, 44, 0, 40, 20.4, 18.7, 1e-4, amp, mean,
+                                                     var, ap, axd, ayd, 20, 18, 3)
+    img = rng.normal(size=(33, 41)).astype(np.float32)
+    lz = np.zeros_like(img)
+    work = np.zeros((4096, 4096), np.float32)
+    mp_fourier.lanczos_shift_3f(img, lz, 0.37, -0.21, work)
+    v = np.fft.rfftfreq(32)
+    w = np.fft.fftfreq(32)
+    var2 = var.copy()
+    var2[0] = 0.
+    ft = np.zeros((32, 17))
+    mp_fourier.gaussian_fourier_transform_zero_mean(amp, var2, v, w, ft)
+    np.savez_compressed(os.path.join(OUT, 'kernels.npz'), amp=amp, mean=mean, var=var, var2=var2,
+                        grid=grid, approx=ap, approx_dx=axd, approx_dy=ayd,
+                        approx_bbox=np.array([sx0, sx1, sy0, sy1]), lanczos_in=img,
+                        lanczos_out=lz, fourier=ft)
+
+    # -- 2. MoG galaxies and point sources (exact grid, masks, approx3) ------
+    out = {}
+    psf = GaussianMixturePSF(1., 0., 0., 6., 6., -1.)
+    H, W = 100, 100
+    tim = Image(data=np.zeros((H, W), np.float32), inverr=np.ones((H, W), np.float32), psf=psf,
+                photocal=LinearPhotoCal(1.))
+    srcs = [
+        ExpGalaxy(PixPos(49.5, 50.), Flux(100.), GalaxyShape(2., 0.5, 45.)),
+        DevGalaxy(PixPos(40.2, 61.7), Flux(250.), EllipseE(3.0, 0.2, -0.1)),
+        FixedCompositeGalaxy(PixPos(55.5, 45.3), Flux(500.), 0.3, EllipseE(2.0, -0.1, 0.3),
+                             EllipseE(1.5, 0.05, 0.1)),
+        SersicGalaxy(PixPos(50.3, 49.8), Flux(300.), EllipseE(2.5, 0.3, 0.1), SersicIndex(2.2)),
+        PointSource(PixPos(30.6, 70.1), Flux(80.)),
+    ]
+    names = ['exp', 'dev', 'comp', 'sersic', 'ptsrc']
+    mm = ModelMask(20, 25, 60, 55)
+    for name, s in zip(names, srcs):
+        p = s.getModelPatch(tim)
+        out[name + '_nomask'] = patches_to_arrays([p])
+        p = s.getModelPatch(tim, modelMask=mm)
+        out[name + '_mask'] = patches_to_arrays([p])
+        d = s.getParamDerivatives(tim, modelMask=mm)
+        out[name + '_derivs_mask'] = patches_to_arrays(d)
+        d = s.getParamDerivatives(tim)
+        out[name + '_derivs_nomask'] = patches_to_arrays(d)
+    tim.modelMinval = 0.01
+    for name, s in zip(names, srcs):
+        p = s.getModelPatch(tim)
+        out[name + '_minval'] = patches_to_arrays([p])
+    tim.modelMinval = 0.
+    ncirc = NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2])
+    tim2 = Image(data=np.zeros((64, 64), np.float32), inverr=np.ones((64, 64), np.float32),
+                 psf=ncirc, photocal=LinearPhotoCal(1.))
+    for name, s in zip(names, srcs):
+        s2 = s.copy()
+        s2.pos.x = s.pos.x - 18
+        s2.pos.y = s.pos.y - 18
+        p = s2.getModelPatch(tim2)
+        out[name + '_ncirc'] = patches_to_arrays([p])
+    flat = {}
+    for k, dct in out.items():
+        for kk, vv in dct.items():
+            flat[k + '.' + kk] = vv
+    np.savez_compressed(os.path.join(OUT, 'mog_sources.npz'), **flat)
+
+    # -- 3. Fourier path: Sersic galaxies, 63x63 Moffat PixelizedPSF --------
+    rng = np.random.default_rng(200)
+    mof = moffat()
+    ppsf = PixelizedPSF(mof)
+    rows = []
+    pix = []
+    derivs = []
+    for i in range(6):
+        n = [0.8, 1.7, 3.5, 5.5, 0.45, 1.2][i]
+        re = float(np.exp(rng.uniform(np.log(0.5), np.log(8))))
+        q = float(rng.uniform(0.2, 1))
+        phi = float(rng.uniform(0, 180))
+        dx, dy = rng.uniform(-0.5, 0.5, 2)
+        px, py = 64 + dx, 64 + dy
+        ell = EllipseE.fromRAbPhi(re, q, phi)
+        gal = SersicGalaxy(PixPos(px, py), Flux(1000.), ell, SersicIndex(n))
+        tim3 = Image(data=np.zeros((128, 128), np.float32), inverr=np.ones((128, 128), np.float32),
+                     psf=ppsf, photocal=LinearPhotoCal(1.))
+        mask = ModelMask(0, 0, 128, 128)
+        p = gal.getModelPatch(tim3, modelMask=mask)
+        rows.append([n, re, q, phi, px, py, ell.re, ell.e1, ell.e2])
+        pix.append(p.patch.astype(np.float32))
+        if i < 2:
+            mask64 = ModelMask(32, 32, 64, 64)
+            d = gal.getParamDerivatives(tim3, modelMask=mask64)
+            derivs.append(np.stack([dd.patch.astype(np.float32) for dd in d]))
+    np.savez_compressed(os.path.join(OUT, 'fft_sersic.npz'), params=np.array(rows),
+                        psf=mof, patches=np.stack(pix), derivs=np.stack(derivs))
+
+    # -- 4. Plain small fit (ExpGalaxy on 64x64, 2-component MoG PSF) -------
+    rng = np.random.default_rng(300)
+    truth = ExpGalaxy(PixPos(32., 32.), Flux(1000.), EllipseE.fromRAbPhi(2.0, 0.6, 30.))
+    timc = Image(data=np.zeros((64, 64)), invvar=np.ones((64, 64)),
+                 psf=NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2]), photocal=LinearPhotoCal(1.))
+    trc = Tractor([timc], [truth])
+    trc.modtype = np.float64
+    clean = trc.getModelImage(0)
+    noisy = clean + rng.normal(size=clean.shape)
+    timc.data = noisy
+    e0 = truth.shape
+    start = ExpGalaxy(PixPos(32.5, 32.5), Flux(800.), EllipseE.fromRAbPhi(2.4, 0.6, 30.))
+    tr = Tractor([timc], [start])
+    tr.modtype = np.float64
+    tr.freezeParam('images')
+    lnp0 = tr.getLogProb()
+    mod0 = tr.getModelImage(0)
+    d0 = start.getParamDerivatives(timc)
+    X = tr.optimizer.getLinearUpdateDirection(tr)
+    p_before = np.array(tr.getParams())
+    dlnp, X1, alpha = tr.optimize()
+    p_after1 = np.array(tr.getParams())
+    R = tr.optimize_loop(dchisq=1e-3)
+    p_final = np.array(tr.getParams())
+    np.savez_compressed(os.path.join(OUT, 'fit_plain.npz'), data=noisy, clean=clean, mod0=mod0,
+                        lnp0=lnp0, X=np.array(X), p_before=p_before, dlnp1=dlnp, X1=np.array(X1),
+                        alpha1=alpha, p_after1=p_after1, p_final=p_final, steps=R['steps'],
+                        **dict(('d0.' + k, v) for k, v in patches_to_arrays(d0).items()))
+    print('golden fixtures written to', OUT)
+
+
+if __name__ == '__main__':
+    main()

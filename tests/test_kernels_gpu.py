@@ -1,0 +1,193 @@
+"""Kernel-level parity of the CUDA path (through the C ABI) against the oracle.
+
+Tolerances: model pixels within 1e-5 of the peak (the parity bar for
+rendering); Lanczos bit-exact with the reference's float arithmetic; FFT-based
+spectra within 2e-6 relative to the largest element; least-squares solutions
+within 1e-9 relative of numpy's FP64 lstsq on well-conditioned problems.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PEAK_TOL = 1e-5
+
+
+def _rand_mix(rng, K, spread=3.0, vmin=0.2, vmax=6.0):
+    amp = rng.uniform(0.1, 1.0, K)
+    mean = rng.normal(scale=spread, size=(K, 2))
+    var = np.zeros((K, 2, 2))
+    for k in range(K):
+        a = rng.normal(size=(2, 2))
+        var[k] = a @ a.T * rng.uniform(vmin, vmax) / 2 + vmin * np.eye(2)
+    return amp, mean, var
+
+
+def _moffat(size=63, fwhm=4.0, beta=3.0):
+    alpha = fwhm / (2 * np.sqrt(2 ** (1 / beta) - 1))
+    y, x = np.mgrid[:size, :size] - size // 2
+    img = (1 + (x ** 2 + y ** 2) / alpha ** 2) ** (-beta)
+    return (img / img.sum()).astype(np.float32)
+
+
+def test_mog_grid_matches_oracle(tb, oracle):
+    import torch
+    from tractor_b200 import render
+    rng = np.random.default_rng(1)
+    b = render.MogBatch()
+    cases = []
+    for (w, h, K) in [(33, 33, 12), (64, 64, 6), (45, 17, 3), (100, 130, 27), (1, 1, 2), (255, 255, 45)]:
+        amp, mean, var = _rand_mix(rng, K, spread=w / 6)
+        x0, y0 = int(rng.integers(-50, 50)), int(rng.integers(-50, 50))
+        fx, fy = x0 + w / 2 + rng.normal(), y0 + h / 2 + rng.normal()
+        off = b.add(x0, y0, w, h, amp, mean, var, fx=fx, fy=fy, scale=1.0)
+        cases.append((off, x0, y0, w, h, amp, mean, var, fx, fy))
+    out = b.run().cpu().numpy()
+    for off, x0, y0, w, h, amp, mean, var, fx, fy in cases:
+        ref = oracle.mog_grid(x0, x0 + w, y0, y0 + h, fx, fy, amp, mean, var)
+        got = out[off:off + w * h].reshape(h, w)
+        err = np.abs(got - ref).max() / ref.max()
+        assert err < PEAK_TOL, (w, h, err)
+
+
+def test_mog_masked_matches_oracle(tb, oracle):
+    from tractor_b200 import render
+    rng = np.random.default_rng(2)
+    amp, mean, var = _rand_mix(rng, 9, spread=5)
+    h, w = 40, 50
+    mask = rng.uniform(size=(h, w)) > 0.3
+    b = render.MogBatch()
+    b.add(-3, 4, w, h, amp, mean, var, fx=20.5, fy=22.25, floor=render.FLOOR_MASKED, mask=mask)
+    got = b.run().cpu().numpy().reshape(h, w)
+    ref, _, _ = oracle.mog_masked(-3, 4, mask, 20.5, 22.25, amp, mean, var)
+    assert np.all(got[~mask] == 0)
+    assert np.abs(got - ref).max() / ref.max() < PEAK_TOL
+
+
+def test_mog_atomic_image_matches_sum(tb, oracle):
+    import torch
+    from tractor_b200 import render
+    rng = np.random.default_rng(3)
+    H, W = 96, 80
+    img = torch.zeros(H * W, dtype=torch.float32, device='cuda')
+    ref = np.zeros((H, W))
+    b = render.MogBatch()
+    for i in range(20):
+        amp, mean, var = _rand_mix(rng, 6, spread=1)
+        cx, cy = rng.uniform(0, W), rng.uniform(0, H)
+        hw = int(rng.integers(5, 30))
+        x0, x1 = max(0, int(cx) - hw), min(W, int(cx) + hw + 1)
+        y0, y1 = max(0, int(cy) - hw), min(H, int(cy) + hw + 1)
+        counts = rng.uniform(10, 1000)
+        b.add(x0, y0, x1 - x0, y1 - y0, amp, mean, var, fx=cx, fy=cy, scale=counts,
+              out_off=y0 * W + x0, ldo=W, mode=render.MOG_ATOMIC)
+        ref[y0:y1, x0:x1] += counts * oracle.mog_grid(x0, x1, y0, y1, cx, cy, amp, mean, var)
+    b.run(out=img)
+    got = img.cpu().numpy().reshape(H, W)
+    assert np.abs(got - ref).max() / ref.max() < PEAK_TOL
+
+
+def test_lanczos_bit_exact(tb, oracle):
+    import torch
+    from tractor_b200 import render
+    rng = np.random.default_rng(4)
+    for (h, w) in [(37, 45), (128, 128), (9, 70)]:
+        imgs = rng.normal(size=(3, h, w)).astype(np.float32)
+        shifts = rng.uniform(-0.5, 0.5, size=(3, 2))
+        shifts[1] = [0.0, 0.3]
+        got = render.lanczos_shift(torch.from_numpy(imgs).cuda(), shifts).cpu().numpy()
+        for i in range(3):
+            ref = oracle.lanczos_shift(imgs[i], shifts[i, 0], shifts[i, 1])
+            assert np.array_equal(got[i], ref), (h, w, i, np.abs(got[i] - ref).max())
+
+
+@pytest.mark.parametrize('sz', [32, 64, 128, 256])
+def test_psf_spectrum(tb, sz):
+    from tractor_b200 import render
+    psf = _moffat(min(63, sz - 1) if sz > 32 else 31)
+    spec, cx, cy = render.PsfSpectra().get(('moffat', sz), psf, sz)
+    got = spec.cpu().numpy().view(np.complex64).reshape(sz // 2 + 1, sz).T
+    pad, cx2, cy2 = render.PsfSpectra.pad(psf, sz)
+    ref = np.fft.rfft2(pad)
+    assert (cx, cy) == (cx2, cy2)
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 2e-6
+
+
+@pytest.mark.parametrize('sz,mw,mh', [(256, 128, 128), (128, 64, 64), (64, 40, 33),
+                                      (32, 20, 20), (256, 200, 180)])
+def test_fourier_render_matches_oracle(tb, oracle, sz, mw, mh):
+    from tractor_b200 import render
+    rng = np.random.default_rng(5 + sz + mw)
+    psf = _moffat(63 if sz >= 128 else (31 if sz == 64 else 15))
+    spec, cx, cy = render.psf_spectra().get(('moffat-test', sz), psf, sz)
+    b = render.FftBatch()
+    cases = []
+    for i in range(6):
+        amp, var_s = oracle.exp_profile() if i % 2 else oracle.dev_profile()
+        T = rng.normal(size=(2, 2)) * rng.uniform(0.5, 4)
+        amp2, var2 = oracle.sheared(amp, var_s, T)
+        mx0, my0 = int(rng.integers(-20, 20)), int(rng.integers(-20, 20))
+        px = mx0 + mw / 2 + rng.uniform(-8, 8)
+        py = my0 + mh / 2 + rng.uniform(-8, 8)
+        if i == 5:
+            px = mx0 - 10.3   # source outside the mask: rows / columns clip
+        ref, (mux, muy, sx, sy, rsz) = oracle.galaxy_fft_masked(
+            amp2, var2, px, py, psf, mx0, my0, mw, mh, force_halfsize=sz / 2)
+        assert rsz == sz
+        off = b.add(amp2, var2, sz, ('moffat-test', sz), spec, mw, mh, sx, sy, mux, muy)
+        cases.append((off, ref))
+    out = b.run().cpu().numpy()
+    for off, ref in cases:
+        got = out[off:off + mw * mh].reshape(mh, mw)
+        peak = max(np.abs(ref).max(), 1e-30)
+        assert np.abs(got - ref).max() / peak < PEAK_TOL, np.abs(got - ref).max() / peak
+
+
+def test_normal_equations_and_solve(tb):
+    import torch
+    from tractor_b200 import render
+    rng = np.random.default_rng(6)
+    Ps, Rs = [6, 11, 54], [4096, 900, 3000]
+    A_list, r_list = [], []
+    for P, R in zip(Ps, Rs):
+        A = rng.normal(size=(R, P)).astype(np.float32) * rng.uniform(0.1, 100, P).astype(np.float32)
+        r = rng.normal(size=R).astype(np.float32)
+        A_list.append(A)
+        r_list.append(r)
+    A_flat = np.concatenate([a.T.ravel() for a in A_list])
+    r_flat = np.concatenate(r_list)
+    a_off = np.concatenate([[0], np.cumsum([a.size for a in A_list])[:-1]])
+    r_off = np.concatenate([[0], np.cumsum(Rs)[:-1]])
+    AtA, Atr, ao, ro = render.normal_equations(torch.from_numpy(A_flat).cuda(),
+                                               torch.from_numpy(r_flat).cuda(),
+                                               a_off, r_off, Rs, Ps, Rs)
+    X, info, x_off = render.solve_update(AtA, Atr, ao, ro, Ps)
+    AtA, Atr, X = AtA.cpu().numpy(), Atr.cpu().numpy(), X.cpu().numpy()
+    assert np.all(info.cpu().numpy() == 0)
+    o = 0
+    for i, (P, A, r) in enumerate(zip(Ps, A_list, r_list)):
+        M = AtA[o:o + P * P].reshape(P, P)
+        A64 = A.astype(np.float64)
+        refM = A64.T @ A64
+        assert np.abs(M - refM).max() / np.abs(refM).max() < 1e-6
+        xs, *_ = np.linalg.lstsq(A64, r.astype(np.float64), rcond=None)
+        got = X[x_off[i]:x_off[i] + P]
+        assert np.abs(got - xs).max() / np.abs(xs).max() < 1e-5
+        o += P * P
+
+
+def test_chi2(tb):
+    import torch
+    from tractor_b200 import render
+    rng = np.random.default_rng(7)
+    n = [4096, 100000, 17]
+    d = rng.normal(size=sum(n)).astype(np.float32)
+    m = rng.normal(size=sum(n)).astype(np.float32)
+    ie = rng.uniform(0.5, 2, size=sum(n)).astype(np.float32)
+    off = np.concatenate([[0], np.cumsum(n)[:-1]])
+    got = render.chi2(*(torch.from_numpy(a).cuda() for a in (d, m, ie)), off, n).cpu().numpy()
+    for i in range(3):
+        s = slice(off[i], off[i] + n[i])
+        chi = (d[s] - m[s]) * ie[s]
+        ref = np.sum(chi.astype(np.float64) ** 2)
+        assert abs(got[i] - ref) / ref < 1e-6

@@ -1,0 +1,365 @@
+"""Positions, WCS, brightnesses, photometric calibration, sky and Image, with
+the reference Tractor's semantics (tractor/wcs.py, tractor/brightness.py,
+tractor/sky.py, tractor/image.py, tractor/ducks.py)."""
+import numpy as np
+
+from .params import BaseParams, ScalarParam, ParamList, MultiParams
+from .patch import Patch
+
+
+# ---------------------------------------------------------------------------
+# Positions and WCS
+# ---------------------------------------------------------------------------
+
+class PixPos(ParamList):
+    """Pixel position (tractor/wcs.py:373-390): step 0.1, max step 1."""
+
+    @staticmethod
+    def getNamedParams():
+        return dict(x=0, y=1)
+
+    def __init__(self, *args):
+        super(PixPos, self).__init__(*args)
+        self.stepsizes = [0.1, 0.1]
+        self.maxstep = [1., 1.]
+
+    def __str__(self):
+        return 'pixel (%.2f, %.2f)' % (self.x, self.y)
+
+    def getDimension(self):
+        return 2
+
+
+class NullWCS(BaseParams):
+    """Identity WCS for pixel positions (tractor/wcs.py:8-49).
+
+    cd_inverse is I / (pixscale / 3600), as in the reference; note that the
+    reference's pixelDerivsToPositionDerivs (tractor/ducks.py:413-423) scales
+    PixPos derivatives by it, which this class reproduces exactly."""
+
+    def __init__(self, pixscale=1., dx=0., dy=0.):
+        self.dx = dx
+        self.dy = dy
+        self.setPixscale(pixscale)
+
+    def hashkey(self):
+        return ('NullWCS', self.dx, self.dy)
+
+    def copy(self):
+        return NullWCS(self.pixscale, self.dx, self.dy)
+
+    def setPixscale(self, pixscale):
+        self.pixscale = pixscale
+        self.cd = np.array([[1., 0.], [0., 1.]]) * self.pixscale / 3600.
+        self.cd_inverse = np.array([[1., 0.], [0., 1.]]) / (self.pixscale / 3600.)
+
+    def positionToPixel(self, pos, src=None):
+        return pos.x + self.dx, pos.y + self.dy
+
+    def pixelToPosition(self, x, y, src=None):
+        return PixPos(x - self.dx, y - self.dy)
+
+    def cdAtPixel(self, x, y):
+        return self.cd
+
+    def cdInverseAtPixel(self, x, y):
+        return self.cd_inverse
+
+    def cdInverseAtPosition(self, pos, src=None):
+        return self.cd_inverse
+
+    def pixscale_at(self, x, y):
+        return self.pixscale
+
+    def shifted(self, x, y):
+        return self.copy()
+
+    def pixelDerivsToPositionDerivs(self, pos, src, counts0, patch0, patchdx, patchdy):
+        """tractor/ducks.py:413-423."""
+        cdi = self.cdInverseAtPosition(pos, src=src)
+        derivs = []
+        for i, pname in pos.getThawedParamIndicesAndNames():
+            d = (patchdx * cdi[0, i] + patchdy * cdi[1, i]) * counts0
+            d.setName('d(ptsrc)/d(pos.%s)' % pname)
+            derivs.append(d)
+        return derivs
+
+
+# ---------------------------------------------------------------------------
+# Brightness and photometric calibration
+# ---------------------------------------------------------------------------
+
+class Flux(ScalarParam):
+    """Raw counts (tractor/brightness.py:14-24)."""
+
+    def __mul__(self, factor):
+        new = self.copy()
+        new.val *= factor
+        return new
+
+    __rmul__ = __mul__
+
+
+class Mag(ScalarParam):
+    stepsize = -0.01
+    strformat = '%.3f'
+
+
+class MultiBandBrightness(ParamList):
+    """Per-band values in a fixed band order (tractor/brightness.py:26-71)."""
+
+    def __init__(self, **kwargs):
+        keys = kwargs.pop('order', None)
+        if keys is None:
+            keys = sorted(kwargs.keys())
+        assert set(kwargs.keys()) == set(keys)
+        super(MultiBandBrightness, self).__init__(*[kwargs[k] for k in keys])
+        self.order = list(keys)
+        self.addNamedParams(**dict((k, i) for i, k in enumerate(keys)))
+
+    def copy(self):
+        return self * 1.
+
+    def getBand(self, band):
+        return getattr(self, band)
+
+    def setBand(self, band, value):
+        return setattr(self, band, value)
+
+
+class Fluxes(MultiBandBrightness):
+    """tractor/brightness.py:135-161."""
+
+    def __add__(self, other):
+        return self.__class__(order=self.order,
+                              **dict((b, self.getBand(b) + other.getBand(b)) for b in self.order))
+
+    def __mul__(self, factor):
+        return self.__class__(order=self.order,
+                              **dict((b, self.getFlux(b) * factor) for b in self.order))
+
+    def getFlux(self, band):
+        return self.getBand(band)
+
+    def setFlux(self, band, value):
+        return self.setBand(band, value)
+
+
+class NanoMaggies(Fluxes):
+    """Linear calibrated fluxes (tractor/brightness.py:163-240)."""
+
+    def __repr__(self):
+        return str(self)
+
+    def __str__(self):
+        ss = []
+        for b in self.order:
+            f = self.getFlux(b)
+            if f <= 0:
+                ss.append('%s=(flux %.3g)' % (b, f))
+            else:
+                ss.append('%s=%.3f' % (b, self.getMag(b)))
+        return 'NanoMaggies: ' + ', '.join(ss)
+
+    def getMag(self, band):
+        return NanoMaggies.nanomaggiesToMag(self.getFlux(band))
+
+    @staticmethod
+    def nanomaggiesToMag(nm):
+        return -2.5 * (np.log10(nm) - 9)
+
+    @staticmethod
+    def magToNanomaggies(mag):
+        return 10. ** ((mag - 22.5) / -2.5)
+
+
+class NullPhotoCal(BaseParams):
+    """Brightness is already in counts (tractor/brightness.py:305-314)."""
+
+    def brightnessToCounts(self, brightness):
+        return brightness.getValue()
+
+    def copy(self):
+        return NullPhotoCal()
+
+    def hashkey(self):
+        return ('NullPhotoCal',)
+
+
+class LinearPhotoCal(ScalarParam):
+    """counts = flux * scale (tractor/brightness.py:316-348)."""
+
+    def __init__(self, scale, band=None):
+        super(LinearPhotoCal, self).__init__(scale)
+        self.band = band
+
+    def copy(self):
+        return self.__class__(self.getValue(), band=self.band)
+
+    def getScale(self):
+        return self.val
+
+    def brightnessToCounts(self, brightness):
+        if self.band is None:
+            return brightness.getValue() * self.val
+        return brightness.getFlux(self.band) * self.val
+
+
+# ---------------------------------------------------------------------------
+# Sky
+# ---------------------------------------------------------------------------
+
+class NullSky(BaseParams):
+    """Zero background (tractor/sky.py:6-12)."""
+
+    def addTo(self, img, scale=1.):
+        pass
+
+    def copy(self):
+        return NullSky()
+
+    def hashkey(self):
+        return ('NullSky',)
+
+    def shifted(self, x0, y0):
+        return self.copy()
+
+
+class ConstantSky(ScalarParam):
+    """Constant background level (tractor/sky.py:15-60)."""
+
+    def getParamDerivatives(self, tractor, img, srcs):
+        p = Patch(0, 0, np.ones_like(img.getImage()))
+        p.setName('dsky')
+        return [p]
+
+    def addTo(self, img, scale=1.):
+        if self.val == 0:
+            return
+        img += (self.val * scale)
+
+    def getParamNames(self):
+        return ['sky']
+
+    def getConstant(self):
+        return self.val
+
+    def shifted(self, x0, y0):
+        return self.copy()
+
+
+# ---------------------------------------------------------------------------
+# Image
+# ---------------------------------------------------------------------------
+
+class Image(MultiParams):
+    """An image with inverse error, PSF, WCS, photometric calibration and sky
+    (tractor/image.py:6-272).  The model for an Image can be computed on the
+    GPU; the pixel arrays stay numpy arrays as in the reference."""
+
+    def __init__(self, data=None, invvar=None, inverr=None, psf=None, wcs=None, sky=None,
+                 photocal=None, name=None, time=None, **kwargs):
+        self.data = data
+        if inverr is not None:
+            self.inverr = inverr
+        elif invvar is not None:
+            self.setInvvar(invvar)
+        self.name = name
+        self.zr = kwargs.pop('zr', None)
+        self.time = time
+        if wcs is None:
+            wcs = NullWCS()
+        if sky is None:
+            sky = NullSky()
+        if photocal is None:
+            photocal = NullPhotoCal()
+        self.modelMinval = 0.
+        super(Image, self).__init__(psf, wcs, photocal, sky)
+
+    @staticmethod
+    def getNamedParams():
+        return dict(psf=0, wcs=1, photocal=2, sky=3)
+
+    def __str__(self):
+        return 'Image ' + str(self.name)
+
+    def copy(self):
+        return self.__class__(data=self.data.copy(), inverr=self.inverr.copy(),
+                              wcs=self.wcs.copy(), psf=self.psf.copy(), sky=self.sky.copy(),
+                              photocal=self.photocal.copy(), name=self.name, time=self.time)
+
+    def getParamDerivatives(self, tractor, srcs):
+        derivs = []
+        for s in self._getActiveSubs():
+            if hasattr(s, 'getParamDerivatives'):
+                sd = s.getParamDerivatives(tractor, self, srcs)
+                assert len(sd) == s.numberOfParams()
+                derivs.extend(sd)
+            else:
+                derivs.extend([False] * s.numberOfParams())
+        return derivs
+
+    @property
+    def shape(self):
+        return self.getShape()
+
+    @property
+    def invvar(self):
+        return self.inverr ** 2
+
+    def getShape(self):
+        return self.data.shape
+
+    def getModelShape(self):
+        return self.getShape()
+
+    def getWidth(self):
+        return self.getShape()[1]
+
+    def getHeight(self):
+        return self.getShape()[0]
+
+    def numberOfPixels(self):
+        H, W = self.data.shape
+        return W * H
+
+    def hashkey(self):
+        return ('Image', id(self.data), id(self.inverr), self.psf.hashkey(), self.sky.hashkey(),
+                self.wcs.hashkey(), self.photocal.hashkey())
+
+    def getInvError(self):
+        return self.inverr
+
+    def setInvError(self, inverr):
+        self.inverr = inverr
+
+    def getInvvar(self):
+        return self.inverr ** 2
+
+    def setInvvar(self, iv):
+        with np.errstate(invalid='ignore'):
+            self.inverr = np.sqrt(iv)
+
+    def getImage(self):
+        return self.data
+
+    def setImage(self, img):
+        self.data = img
+
+    def getPsf(self):
+        return self.psf
+
+    def setPsf(self, psf):
+        self.psf = psf
+
+    def getWcs(self):
+        return self.wcs
+
+    def getPhotoCal(self):
+        return self.photocal
+
+    def getSky(self):
+        return self.sky
+
+    def setSky(self, sky):
+        self.sky = sky

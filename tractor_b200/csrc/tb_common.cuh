@@ -1,0 +1,46 @@
+// Shared device helpers for the tractor_b200 kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tractor_b200.h"
+
+#define TB_LOG2E 1.4426950408889634
+#define TB_PI 3.14159265358979323846
+
+namespace tb {
+
+// 2^x on the SFU (MUFU.EX2), flushing denormal results to zero.
+__device__ __forceinline__ float ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Records the first failure of a launch in a device status word.
+__device__ __forceinline__ void report(tb_status* st, int code, int item, int detail) {
+    if (st == nullptr) return;
+    if (atomicCAS(&st->code, 0, code) == 0) {
+        st->item = item;
+        st->detail = detail;
+    }
+    atomicAdd(&st->count, 1);
+}
+
+// Dynamic work distribution for persistent kernels: thread 0 takes the next
+// unit from a global counter and broadcasts it through shared memory.
+__device__ __forceinline__ int64_t next_unit(int32_t* counter, int64_t* slot) {
+    __syncthreads();
+    if (threadIdx.x == 0) *slot = (int64_t)atomicAdd(counter, 1);
+    __syncthreads();
+    return *slot;
+}
+
+inline int num_sms() {
+    int n = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+}  // namespace tb
