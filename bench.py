@@ -1,0 +1,376 @@
+"""Benchmark: the pixelized-PSF Fourier rendering workload.
+
+Workload (per GPU): 256 SersicGalaxy sources (n ~ U[0.7, 6], r_e log-uniform
+in [0.5, 8] px, axis ratio U[0.2, 1], phi U[0, 180)), each on its own 128x128
+ModelMask, PSF a 63x63 normalised Moffat image (beta 3, FWHM 4 px) used as a
+PixelizedPSF, sub-pixel offsets U[-0.5, 0.5] applied by Lanczos-3.  The FFT
+size is 256 (the reference's next power of two of twice the patch
+half-size).  Synthetic, seeded.
+
+One step = render every source's model patch from its parameters already in
+device memory: tb_galaxy_fft_prep (profiles, shapes, item geometry) and
+tb_fourier_render (spectrum, FFTs, Lanczos, crop) -- 2 launches.  The metric
+is Mpix x components per second with Npix = sz^2 per source and the
+source's Gaussian component count (SersicGalaxy mixtures have 5-9), summed
+over sources.  L2 is flushed (a 256 MB write) before every timed step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times the reference's CPU implementation of the same
+workload on the host cores (its own compiled C for the spectrum and the
+Lanczos shift, numpy's irfftn, galaxy.py's geometry), one source per task
+over all cores, each step a bounded sample of the 256 sources.
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SOURCES = 256
+MASK = 128
+SFU_EX2_PER_CLK_PER_SM = 16      # MUFU.EX2 issue rate of an SM (sm_100)
+WORKLOAD = ('256 SersicGalaxy sources, each on a 128x128 ModelMask, 63x63 Moffat '
+            'PixelizedPSF (FFT 256, Lanczos-3)')
+METRIC = 'Mpix*components/s (pixelized-PSF Fourier render)'
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=50)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--cpu-seconds', type=float, default=12.0)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU side (oracle port / reference C), one source per task
+# ---------------------------------------------------------------------------
+
+def _cpu_worker(args):
+    """Renders sources [i0, i1) of the workload on the CPU; returns
+    (pix*components, seconds)."""
+    i0, i1, seed, use_ref, budget = args
+    sys.path.insert(0, ROOT)
+    os.environ.setdefault('OMP_NUM_THREADS', '1')
+    from oracle import oracle as O
+    from tractor_b200 import batch
+    rng = np.random.default_rng(seed)
+    srcs = batch.sersic_sources(N_SOURCES, rng, mask=MASK)
+    psf = batch.moffat_psf()
+    kern = O.reference_kernels() if use_ref else None
+    cdinv = O.nullwcs_cdinv()
+    work = 0.
+    t0 = time.perf_counter()
+    i = i0
+    while i < i1:
+        s = srcs[i]
+        amp, var = O.sersic_profile(float(s['sersic_n']))
+        T = cdinv @ O.ellipseE_basis(s['s0'], s['s1'], s['s2'])
+        a2, v2 = O.sheared(amp, var, T)
+        _, (_, _, _, _, sz) = O.galaxy_fft_masked(a2, v2, s['px'], s['py'], psf, 0, 0, MASK, MASK,
+                                                  kernels=kern)
+        work += sz * sz * len(amp)
+        i += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    return work, time.perf_counter() - t0, i - i0
+
+
+def cpu_rate(seconds, use_ref, seed=1000):
+    """Mpix*components/s of the CPU path on all host cores (spawned worker
+    processes), over a bounded sample of the workload."""
+    ncores = os.cpu_count() or 1
+    ctx = mp.get_context('spawn')
+    per = max(1, N_SOURCES // ncores)
+    tasks = []
+    for c in range(ncores):
+        i0 = (c * per) % N_SOURCES
+        tasks.append((i0, min(N_SOURCES, i0 + per), seed, use_ref, seconds))
+    t0 = time.perf_counter()
+    with ctx.Pool(ncores) as pool:
+        res = pool.map(_cpu_worker, tasks)
+    wall = time.perf_counter() - t0
+    work = sum(r[0] for r in res)
+    nsrc = sum(r[2] for r in res)
+    busy = max(r[1] for r in res)
+    return work / busy / 1e6, ncores, nsrc, wall
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler(object):
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.QUERY,
+                 '--format=csv,noheader,nounits', '-lms', '100'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() in ('active', '1', 'yes'):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': mx, 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+# ---------------------------------------------------------------------------
+
+def init_dist():
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    return world, rank, local
+
+
+def ncu_traffic():
+    """DRAM bytes per tb_fourier_render launch of this workload, from the
+    committed ncu summary (profiles/fourier_render_c2.json), or None."""
+    p = os.path.join(ROOT, 'profiles', 'fourier_render_c2.json')
+    try:
+        with open(p) as f:
+            return json.load(f).get('dram_bytes_per_launch')
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    use_ref = O.reference_kernels() is not None
+    kind = 'reference' if use_ref else 'port'
+    ncores = os.cpu_count() or 1
+    per_step = max(8.0, 60.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_rate(min(per_step, 2.0), use_ref)
+    rates, nsrc = [], 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r, ncores, n, _ = cpu_rate(per_step, use_ref)
+        rates.append(r)
+        nsrc += n
+    wall = time.perf_counter() - t0
+    value = float(np.mean(rates))
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'Mpix*components/s',
+        'n_gpus': 0, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': wall / max(1, args.steps) * 1e3, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64/f32 (reference CPU path)',
+        'data': 'synthetic', 'config': {'workload': WORKLOAD, 'n_sources': N_SOURCES,
+                                        'mask': MASK, 'fft_size': 256},
+        'cpu_baseline': {'value': value, 'unit': 'Mpix*components/s', 'cores': ncores,
+                         'kind': kind,
+                         'sample': '%d source renders over %d steps (%.0f s budget per step), '
+                                   'one process per core' % (nsrc, args.steps, per_step)},
+        'e2e': {'value': value, 'unit': 'Mpix*components/s', 'h2d_bytes_per_step': 0,
+                'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = init_dist()
+    if args.impl == 'reference':
+        if world > 1:
+            import torch.distributed as dist  # noqa: F401
+        run_reference(args, world, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group('nccl', init_method='env://',
+                                timeout=__import__('datetime').timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from tractor_b200 import batch, _lib, build
+    build.build()
+    _lib.load()
+
+    rng = np.random.default_rng(1000 + rank)
+    srcs = batch.sersic_sources(N_SOURCES, rng, mask=MASK)
+    renderer = batch.FourierGalaxyRenderer(batch.moffat_psf())
+    n = len(srcs)
+    nout = n * MASK * MASK
+    dev = torch.device('cuda', local)
+    src_pinned = torch.from_numpy(srcs.view(np.uint8).copy()).pin_memory()
+    d_src = src_pinned.to(dev)
+    out = torch.empty(nout, dtype=torch.float32, device=dev)
+    out_pinned = torch.empty(nout, dtype=torch.float32).pin_memory()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
+    stream = torch.cuda.current_stream()
+
+    def step():
+        renderer.render_device(d_src, n, out)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    flags = renderer._work(n)[3].cpu().numpy()
+    items = renderer._work(n)[0].cpu().numpy().view(_lib.FFT_ITEM)
+    assert np.all(flags == 0), 'prep flagged sources: %s' % np.unique(flags)
+    pixcomp = float(np.sum(items['sz'].astype(np.float64) ** 2 * items['K']))
+    ex2_per_launch = float(np.sum(items['sz'].astype(np.float64) * (items['sz'] // 2 + 1) *
+                                  items['K']))
+
+    # ---- device-timed steps (inputs resident in HBM, L2 flushed) ----
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    props = torch.cuda.get_device_properties(dev)
+    try:
+        gpu_id = '%08X:%02X:%02X.0' % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+    except AttributeError:
+        gpu_id = str(torch.cuda.current_device())
+    clocks = ClockSampler(gpu_id)
+    clocks.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        e0, e1, e2 = ev[k]
+        e0.record(stream)
+        lib = _lib.load()
+        items_t, camp, cvar, flg, misc = renderer._work(n)
+        rc = lib.tb_galaxy_fft_prep(d_src.data_ptr(), n,
+                                    __import__('ctypes').addressof(renderer.image),
+                                    __import__('ctypes').addressof(renderer.tables.struct),
+                                    items_t.data_ptr(), camp.data_ptr(), cvar.data_ptr(),
+                                    batch.COMP_STRIDE, flg.data_ptr(), _lib.stream_ptr())
+        _lib.check(rc, 'tb_galaxy_fft_prep')
+        e1.record(stream)
+        rc = lib.tb_fourier_render(items_t.data_ptr(), n, camp.data_ptr(), cvar.data_ptr(),
+                                   renderer.spec.data_ptr(), out.data_ptr(), misc.data_ptr(),
+                                   misc.data_ptr() + 16, _lib.stream_ptr())
+        _lib.check(rc, 'tb_fourier_render')
+        e2.record(stream)
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(c) for a, b, c in ev]
+    render_ms = [b.elapsed_time(c) for a, b, c in ev]
+    t_total = sum(step_ms) / 1e3
+    if world > 1:
+        t = torch.tensor([t_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+    gpu_launches = 2 * args.steps
+
+    # ---- end to end through the host-buffer API (H2D + render + D2H) ----
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        a, b = ev2[k]
+        a.record(stream)
+        d_src.copy_(src_pinned, non_blocking=True)
+        step()
+        out_pinned.copy_(out, non_blocking=True)
+        b.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    e2e_s = sum(a.elapsed_time(b) for a, b in ev2) / 1e3
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    from tractor_b200 import render as R
+    R.check_status(renderer.status(n).clone(), 'tb_fourier_render')
+
+    value = world * pixcomp * args.steps / t_total / 1e6
+    e2e = world * pixcomp * args.steps / e2e_s / 1e6
+    kern_s = float(np.mean(render_ms)) / 1e3
+    sm_mhz = clk['sm_mhz'] if clk else None
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak_clk = sm_mhz if sm_mhz else 1965.0
+    peak = SFU_EX2_PER_CLK_PER_SM * nsm * peak_clk * 1e6 / 1e9
+    achieved = ex2_per_launch / kern_s / 1e9
+    line = {
+        'metric': METRIC, 'value': value, 'unit': 'Mpix*components/s', 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': t_total / args.steps * 1e3,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+        'data': 'synthetic (seeded)',
+        'config': {'workload': WORKLOAD, 'n_sources_per_gpu': N_SOURCES, 'mask': MASK,
+                   'fft_size': 256, 'pix_components_per_step': pixcomp,
+                   'l2': 'flushed before every timed step (256 MB write)',
+                   'parallelism': 'independent sources per GPU (weak scaling)'},
+        'e2e': {'value': e2e, 'unit': 'Mpix*components/s',
+                'h2d_bytes_per_step': int(src_pinned.numel()),
+                'd2h_bytes_per_step': int(out_pinned.numel() * 4)},
+        'gpu_launches': gpu_launches,
+        'roofline': {'bound': 'sfu', 'kernel': 'tb_fourier_render',
+                     'achieved': achieved, 'peak': peak, 'unit': 'Gex2/s',
+                     'frac': achieved / peak,
+                     'peak_basis': '%d ex2/clk/SM x %d SMs x median SM clock under load '
+                                   '(%s MHz)' % (SFU_EX2_PER_CLK_PER_SM, nsm, peak_clk),
+                     'algorithmic': 'sum over sources of K * sz * (sz/2+1) spectrum '
+                                    'evaluations per launch = %.0f' % ex2_per_launch,
+                     'kernel_ms': kern_s * 1e3,
+                     'traffic': ncu_traffic()},
+        'clocks': clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, nsrc, wall = cpu_rate(args.cpu_seconds, use_ref=False)
+        line['cpu_baseline'] = {'value': rate, 'unit': 'Mpix*components/s', 'cores': cores,
+                                'kind': 'port',
+                                'sample': '%d of the 256 sources rendered by the oracle, one '
+                                          'process per core, %.0f s budget' % (nsrc, args.cpu_seconds)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -6,7 +6,8 @@
  * void*, NULL = legacy default stream), and every call returns an int status
  * (TB_OK = 0) after validating its arguments on the host; it never aborts the
  * process.  Kernels additionally write per-call status words to device memory
- * (tb_status) that the caller reads after synchronising.  The library holds no
+ * (tb_status, may be NULL; zeroed by the call on its stream before the
+ * launch) that the caller reads after synchronising.  The library holds no
  * mutable global state and allocates no memory: callers own every buffer,
  * including workspaces, and may call from one stream per host thread.
  *
@@ -64,13 +65,23 @@ typedef struct {
     int32_t mode;      /* TB_MOG_STORE, TB_MOG_ACCUM or TB_MOG_ATOMIC */
     int32_t ldo;       /* output row stride in elements (0 = w) */
     double fx, fy;     /* evaluation offset added to every mean */
-    double floor;      /* exponent floor, natural-log units */
+    double floor;      /* TB_FLOOR_FIXED: exponent floor (natural-log units);
+                          TB_FLOOR_MINVAL: minval (see below) */
     float scale;       /* output multiplier (counts for a model patch) */
-    int32_t pad1;
+    int32_t floor_mode;
     int64_t out_off;   /* element offset of this item's output */
     int64_t mask_off;  /* element offset of this item's mask, or -1 */
     int64_t tile0;     /* exclusive prefix of tiles (32x32) over items */
+    int64_t deriv_off; /* >= 0: also write d/dmean_x and d/dmean_y (times
+                          scale), two w x h planes at out + deriv_off */
 } tb_mog_item;
+
+/* TB_FLOOR_MINVAL: each component k gets the floor
+ * max(-100, log(minval * 2 pi sqrt(det V_k) / sum(amp))), the per-component
+ * cut of c_gauss_2d_approx3 (tractor/approx3.c:101-125); `floor` holds
+ * minval. */
+#define TB_FLOOR_FIXED 0
+#define TB_FLOOR_MINVAL 1
 
 /* Output modes: STORE writes, ACCUM adds (items must not overlap in the
  * output), ATOMIC adds with atomics (overlapping items allowed, e.g. many
@@ -118,8 +129,8 @@ int tb_lanczos3_shift(const float* in, float* out, const double* shift,
  * galaxy.py:457-465), Lanczos-3 shift by (mux, muy), integer shift by
  * (sx, sy) into the mh x mw mask.  sz is a power of two in [32, 256].
  * psf_spec: sz x (sz/2+1) complex64 (interleaved re, im) per PSF, stored
- * column-major (element (row j, column v) at v*sz + j), PSF p at
- * psf_spec + p * sz*(sz/2+1)*2 floats, as written by tb_psf_spectrum.  Components: amp[c0+k] and the
+ * column-major (element (row j, column v) at v*sz + j), an item's spectrum
+ * at psf_spec + spec_off floats, as written by tb_psf_spectrum.  Components: amp[c0+k] and the
  * sheared 2x2 covariance var[4(c0+k)..] (FP64); a zero covariance is a delta
  * component.  Output: float32 mh x mw at out + out_off (row stride ldo, or
  * mw if ldo = 0), times `scale`.  Items taller than 128 pixels at sz = 256
@@ -128,15 +139,14 @@ int tb_lanczos3_shift(const float* in, float* out, const double* shift,
 typedef struct {
     int32_t c0, K;
     int32_t sz;
-    int32_t psf;       /* PSF spectrum index */
+    int32_t mode;      /* TB_MOG_STORE, TB_MOG_ACCUM or TB_MOG_ATOMIC */
     int32_t mw, mh;
     int32_t sx, sy;
     double mux, muy;
     float scale;
-    int32_t mode;      /* TB_MOG_STORE, TB_MOG_ACCUM or TB_MOG_ATOMIC */
-    int64_t out_off;
     int32_t ldo;       /* output row stride in elements (0 = mw) */
-    int32_t pad0;
+    int64_t out_off;
+    int64_t spec_off;  /* float offset of this item's PSF spectrum in psf_spec */
 } tb_fft_item;
 
 #define TB_FFT_MAX_SZ 256
@@ -145,6 +155,80 @@ int tb_fourier_render(const tb_fft_item* items, int32_t n_items,
                       const double* comp_amp, const double* comp_var,
                       const float* psf_spec, float* out, int32_t* work_counter,
                       tb_status* status, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Galaxy preparation for the Fourier path
+ *
+ * Turns source parameters into tb_fft_item work items and component tables
+ * on the device: the profile mixture (exp, deV, Gaussian, or the Sersic
+ * mixture of tractor/sersic.py:288-342 evaluated from its spline knots and
+ * coefficients), the shape's pixel-space covariance T V T^T with
+ * T = cdInverse * getRaDecBasis() (HoggGalaxy._getShearedProfile,
+ * tractor/galaxy.py:659-669; EllipseE / EllipseESoft / GalaxyShape bases),
+ * the patch half-size and FFT size for a ModelMask (galaxy.py:339-351,
+ * psf.py:209-212), and the integer / sub-pixel split of the offset
+ * (galaxy.py:383-406, np.round's half-to-even rounding).
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    double px, py;       /* pixel position */
+    double counts;       /* brightness in counts: the output scale */
+    double s0, s1, s2;   /* shape parameters, see shape_type */
+    double sersic_n;     /* Sersic index (profile TB_PROFILE_SERSIC) */
+    int64_t out_off;     /* element offset of this source's mh x mw output */
+    int32_t profile;     /* TB_PROFILE_* */
+    int32_t shape_type;  /* TB_SHAPE_* */
+    int32_t mx0, my0, mw, mh;  /* ModelMask */
+} tb_galaxy_src;
+
+#define TB_PROFILE_EXP 0
+#define TB_PROFILE_DEV 1
+#define TB_PROFILE_SERSIC 2
+#define TB_PROFILE_GAUSSIAN 3
+#define TB_SHAPE_ELLIPSE_E 0      /* (re, e1, e2), tractor/ellipses.py:13-155 */
+#define TB_SHAPE_ELLIPSE_ESOFT 1  /* (log re, ee1, ee2), ellipses.py:165-263 */
+#define TB_SHAPE_RABPHI 2         /* GalaxyShape (re, ab, phi), galaxy.py:37-89 */
+
+/* Constants of one image: WCS inverse CD matrix and pixel scale, PSF size,
+ * and for each FFT size 32, 64, 128, 256 the PSF centre in the padded PSF
+ * image and the float offset of its spectrum (-1 if not provided).  Passed by
+ * host pointer, read at call time. */
+typedef struct {
+    double cd_inv[4];
+    double pixscale;
+    int32_t psf_w, psf_h;
+    double psf_cx[4], psf_cy[4];
+    int64_t spec_off[4];
+} tb_fft_image;
+
+/* Profile tables in device memory (pointers), passed by host pointer. */
+typedef struct {
+    int32_t n_ranges;
+    int32_t core_spline;          /* spline index of the core fraction */
+    const double* range_lohi;     /* 2 per Sersic-index range */
+    const int32_t* range_info;    /* 4 per range: K, first amp spline, first log-var spline, 0 */
+    const int32_t* spline_info;   /* 4 per spline: knot offset, knot count, coef offset, degree */
+    const double* knots;
+    const double* coefs;
+    const double* exp_amp;
+    const double* exp_var;
+    const double* dev_amp;
+    const double* dev_var;
+    int32_t exp_K, dev_K;
+    int32_t n_splines, n_knots, n_coefs, pad;
+} tb_profile_tables;
+
+#define TB_PROFILE_SMEM_MAX 49152  /* bytes of tables the prep kernel stages */
+
+/* flags[i]: 0 = item written; 1 = no patch (zero counts, or the source lies
+ * outside its mask farther than its radius: getModelPatch returns None);
+ * 2 = unsupported here (source outside its mask but within its radius -- the
+ * reference raises for a non-hybrid PSF -- or an FFT size above 256).
+ * Items not written get K = 0.  Components: comp_stride (>= 10) slots per
+ * source at comp_amp + i*comp_stride, comp_var + 4*i*comp_stride. */
+int tb_galaxy_fft_prep(const tb_galaxy_src* srcs, int32_t n, const tb_fft_image* image,
+                       const tb_profile_tables* tables, tb_fft_item* items,
+                       double* comp_amp, double* comp_var, int32_t comp_stride,
+                       int32_t* flags, void* stream);
 
 /* Forward real FFT of n zero-padded sz x sz float32 PSF images (prepared by
  * the caller, image i at pad + i*sz*sz) into complex64 spectra
@@ -200,8 +284,9 @@ int tb_chi2(const float* data, const float* model, const float* inverr,
 const char* tb_version(void);
 
 /* ABI guard for bindings: writes sizeof(tb_mog_item), sizeof(tb_fft_item),
- * sizeof(tb_status) into sizes[0..2] (host memory) and returns 3.  No
- * reference counterpart (bindings check their struct layouts with it). */
+ * sizeof(tb_status), sizeof(tb_galaxy_src), sizeof(tb_fft_image) into
+ * sizes[0..4] (host memory) and returns 5.  No reference counterpart
+ * (bindings check their struct layouts with it). */
 int tb_abi_sizes(int32_t* sizes);
 
 #ifdef __cplusplus

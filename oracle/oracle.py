@@ -363,13 +363,37 @@ def fft_halfsize_for_mask(px, py, x0, y0, mw, mh, psfh, psfw):
 # Unit-flux galaxy patches
 # ---------------------------------------------------------------------------
 
+_work_cache = {}
+
+
+def _ref_work(shape):
+    """Scratch for the reference's lanczos_shift_3f (it indexes a compact
+    W x H work array; tractor/psf.py:61 passes a 4096^2 global)."""
+    if shape not in _work_cache:
+        m = max(shape)
+        _work_cache[shape] = np.zeros((m, m), np.float32)
+    return _work_cache[shape]
+
+
+def reference_kernels():
+    """The reference's own Fourier / Lanczos C (tractor/mp_fourier.i), built
+    into oracle/_ref/ by oracle/build_ref.sh, or None if it is not built."""
+    path = os.path.join(_HERE, '_ref', 'libref_mpf.so')
+    if not os.path.exists(path):
+        return None
+    from . import refharness
+    return refharness._mpf_module()
+
+
 def galaxy_fft_masked(amp, var2, px, py, psf_img, mask_x0, mask_y0, mw, mh,
-                      normalized_psf=False, force_halfsize=None):
+                      normalized_psf=False, force_halfsize=None, kernels=None):
     """ProfileGalaxy._realGetUnitFluxModelPatch FFT branch with a ModelMask and
     a non-hybrid pixelized PSF (tractor/galaxy.py:336-519).  `var2` is the
     sheared (pixel-space) 2x2 covariance per component.  Returns the float32
     (mh, mw) unit-flux patch with origin (mask_x0, mask_y0), plus the split
-    (mux, muy, sx, sy, sz) for diagnostics."""
+    (mux, muy, sx, sy, sz) for diagnostics.  `kernels` (from
+    reference_kernels()) swaps in the reference's own compiled C for the
+    spectrum and the Lanczos shift."""
     psfh, psfw = psf_img.shape
     hs = fft_halfsize_for_mask(px, py, mask_x0, mask_y0, mw, mh, psfh, psfw)
     if force_halfsize is not None:
@@ -385,11 +409,20 @@ def galaxy_fft_masked(amp, var2, px, py, psf_img, mask_x0, mask_y0, mw, mh,
     mux -= sx
     muy -= sy
     assert abs(mux) <= 0.5 and abs(muy) <= 0.5
-    F = fourier_mog(amp, var2, v, w)
+    if kernels is None:
+        F = fourier_mog(amp, var2, v, w)
+    else:
+        F = np.zeros((len(w), len(v)), np.float64)
+        kernels.gaussian_fourier_transform_zero_mean(amp, var2, v, w, F)
     G = np.fft.irfftn(F * P)
     G = G.astype(np.float32)
     if mux != 0.0 or muy != 0.0:
-        G = lanczos_shift(G, mux, muy)
+        if kernels is None:
+            G = lanczos_shift(G, mux, muy)
+        else:
+            out = np.empty_like(G)
+            kernels.lanczos_shift_3f(G, out, mux, muy, _ref_work(G.shape))
+            G = out
     gh, gw = G.shape
     if sx != 0 or sy != 0:
         out = np.zeros((mh, mw), np.float32)

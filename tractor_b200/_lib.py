@@ -17,13 +17,43 @@ HEADER = os.path.join(os.path.dirname(_HERE), 'include', 'tractor_b200.h')
 MOG_ITEM = np.dtype([('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'), ('h', '<i4'),
                      ('c0', '<i4'), ('K', '<i4'), ('mode', '<i4'), ('ldo', '<i4'),
                      ('fx', '<f8'), ('fy', '<f8'), ('floor', '<f8'),
-                     ('scale', '<f4'), ('pad1', '<i4'),
-                     ('out_off', '<i8'), ('mask_off', '<i8'), ('tile0', '<i8')])
-FFT_ITEM = np.dtype([('c0', '<i4'), ('K', '<i4'), ('sz', '<i4'), ('psf', '<i4'),
+                     ('scale', '<f4'), ('floor_mode', '<i4'),
+                     ('out_off', '<i8'), ('mask_off', '<i8'), ('tile0', '<i8'),
+                     ('deriv_off', '<i8')])
+FLOOR_FIXED, FLOOR_MINVAL = 0, 1
+FFT_ITEM = np.dtype([('c0', '<i4'), ('K', '<i4'), ('sz', '<i4'), ('mode', '<i4'),
                      ('mw', '<i4'), ('mh', '<i4'), ('sx', '<i4'), ('sy', '<i4'),
-                     ('mux', '<f8'), ('muy', '<f8'), ('scale', '<f4'), ('mode', '<i4'),
-                     ('out_off', '<i8'), ('ldo', '<i4'), ('pad0', '<i4')])
+                     ('mux', '<f8'), ('muy', '<f8'), ('scale', '<f4'), ('ldo', '<i4'),
+                     ('out_off', '<i8'), ('spec_off', '<i8')])
 STATUS = np.dtype([('code', '<i4'), ('item', '<i4'), ('detail', '<i4'), ('count', '<i4')])
+GALAXY_SRC = np.dtype([('px', '<f8'), ('py', '<f8'), ('counts', '<f8'), ('s0', '<f8'),
+                       ('s1', '<f8'), ('s2', '<f8'), ('sersic_n', '<f8'), ('out_off', '<i8'),
+                       ('profile', '<i4'), ('shape_type', '<i4'), ('mx0', '<i4'), ('my0', '<i4'),
+                       ('mw', '<i4'), ('mh', '<i4')])
+
+PROFILE_EXP, PROFILE_DEV, PROFILE_SERSIC, PROFILE_GAUSSIAN = 0, 1, 2, 3
+SHAPE_ELLIPSE_E, SHAPE_ELLIPSE_ESOFT, SHAPE_RABPHI = 0, 1, 2
+
+
+class FftImage(ctypes.Structure):
+    """tb_fft_image."""
+    _fields_ = [('cd_inv', ctypes.c_double * 4), ('pixscale', ctypes.c_double),
+                ('psf_w', ctypes.c_int32), ('psf_h', ctypes.c_int32),
+                ('psf_cx', ctypes.c_double * 4), ('psf_cy', ctypes.c_double * 4),
+                ('spec_off', ctypes.c_int64 * 4)]
+
+
+class ProfileTables(ctypes.Structure):
+    """tb_profile_tables (device pointers)."""
+    _fields_ = [('n_ranges', ctypes.c_int32), ('core_spline', ctypes.c_int32),
+                ('range_lohi', ctypes.c_void_p), ('range_info', ctypes.c_void_p),
+                ('spline_info', ctypes.c_void_p), ('knots', ctypes.c_void_p),
+                ('coefs', ctypes.c_void_p), ('exp_amp', ctypes.c_void_p),
+                ('exp_var', ctypes.c_void_p), ('dev_amp', ctypes.c_void_p),
+                ('dev_var', ctypes.c_void_p), ('exp_K', ctypes.c_int32),
+                ('dev_K', ctypes.c_int32), ('n_splines', ctypes.c_int32),
+                ('n_knots', ctypes.c_int32), ('n_coefs', ctypes.c_int32),
+                ('pad', ctypes.c_int32)]
 
 MOG_STORE, MOG_ACCUM, MOG_ATOMIC = 0, 1, 2
 MOG_TILE = 32
@@ -45,6 +75,7 @@ SIGNATURES = {
     'tb_normal_equations': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _I32, _P]),
     'tb_solve_update': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P, _P]),
     'tb_chi2': (_I32, [_P, _P, _P, _P, _P, _I32, _P, _P]),
+    'tb_galaxy_fft_prep': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _I32, _P, _P]),
     'tb_version': (ctypes.c_char_p, []),
     'tb_abi_sizes': (_I32, [_P]),
 }
@@ -71,9 +102,10 @@ def load():
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
-    sizes = np.zeros(3, np.int32)
+    sizes = np.zeros(5, np.int32)
     lib.tb_abi_sizes(sizes.ctypes.data)
-    want = (MOG_ITEM.itemsize, FFT_ITEM.itemsize, STATUS.itemsize)
+    want = (MOG_ITEM.itemsize, FFT_ITEM.itemsize, STATUS.itemsize, GALAXY_SRC.itemsize,
+            ctypes.sizeof(FftImage))
     if tuple(int(s) for s in sizes) != want:
         raise ImportError('libtractor_b200.so struct layout %s != binding %s' %
                           (tuple(sizes), want))

@@ -281,7 +281,7 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
             if (threadIdx.x == 0) cur_n = N;
         }
         __syncthreads();
-        const float* spec = psf_spec + (int64_t)it.psf * N * (N / 2 + 1) * 2;
+        const float* spec = psf_spec + it.spec_off;
         switch (N) {
             case 256: render_item<256>(it, K, spec, out, sh, kRmax256); break;
             case 128: render_item<128>(it, K, spec, out, sh, 128 + 6); break;
@@ -305,6 +305,8 @@ extern "C" int tb_fourier_render(const tb_fft_item* items, int32_t n_items,
                              kSmemBytes) != cudaSuccess)
         return TB_ERR_LAUNCH;
     if (cudaMemsetAsync(work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return TB_ERR_LAUNCH;
+    if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
     const int grid = n_items < tb::num_sms() ? n_items : tb::num_sms();
     fourier_render_kernel<<<grid, kThreads, kSmemBytes, s>>>(items, n_items, comp_amp, comp_var,
                                                              psf_spec, out, work_counter, status);

@@ -291,5 +291,7 @@ extern "C" int tb_abi_sizes(int32_t* sizes) {
     sizes[0] = (int32_t)sizeof(tb_mog_item);
     sizes[1] = (int32_t)sizeof(tb_fft_item);
     sizes[2] = (int32_t)sizeof(tb_status);
-    return 3;
+    sizes[3] = (int32_t)sizeof(tb_galaxy_src);
+    sizes[4] = (int32_t)sizeof(tb_fft_image);
+    return 5;
 }

@@ -24,6 +24,62 @@ struct GaussC {
 constexpr int kThreads = 256;
 constexpr int kRowsPerThread = TB_MOG_TILE / (kThreads / 32);  // 4
 
+// Evaluates the staged components on one tile: thread column `lane`, rows
+// warp + 8 j.  With kDerivs, also the derivatives with respect to the mean
+// (-G (2 I0 dx + I1 dy), tractor/mix.i:44-82), written to two planes.
+template <bool kDerivs>
+__device__ __forceinline__ void eval_tile(const tb_mog_item& it, const GaussC* comps, int total,
+                                          int tw, int th, int ox, int oy,
+                                          const uint8_t* __restrict__ masks,
+                                          float* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float acc[kRowsPerThread], gx[kRowsPerThread], gy[kRowsPerThread];
+#pragma unroll
+    for (int j = 0; j < kRowsPerThread; j++) acc[j] = gx[j] = gy[j] = 0.f;
+    const float xf = (float)lane;
+    for (int c = 0; c < total; c++) {
+        const GaussC q = comps[c];
+        const float dx = xf - q.mx;
+        const float A = q.qxx * dx * dx;
+        const float B = q.qxy * dx;
+#pragma unroll
+        for (int j = 0; j < kRowsPerThread; j++) {
+            const float dy = (float)(warp + 8 * j) - q.my;
+            const float e = fmaf(dy, fmaf(q.qyy, dy, B), A);
+            const float sv = (e >= q.fl) ? q.s : 0.f;
+            const float ev = tb::ex2(e);
+            acc[j] = fmaf(sv, ev, acc[j]);
+            if (kDerivs) {
+                const float v = sv * ev;
+                // d/dmean in natural-log units: ln2 * (2 qxx dx + qxy dy) etc.
+                gx[j] = fmaf(-v, 0.69314718f * fmaf(2.f * q.qxx, dx, q.qxy * dy), gx[j]);
+                gy[j] = fmaf(-v, 0.69314718f * fmaf(2.f * q.qyy, dy, q.qxy * dx), gy[j]);
+            }
+        }
+    }
+    const float sc = it.scale;
+    const int w = it.w, h = it.h;
+    const int64_t ldo = it.ldo > 0 ? it.ldo : w;
+#pragma unroll
+    for (int j = 0; j < kRowsPerThread; j++) {
+        const int y = warp + 8 * j;
+        if (lane < tw && y < th) {
+            const int64_t o = (int64_t)(oy + y) * w + (ox + lane);
+            const bool on = !(it.mask_off >= 0 && !masks[it.mask_off + o]);
+            const float val = on ? acc[j] * sc : 0.f;
+            float* p = out + it.out_off + (int64_t)(oy + y) * ldo + (ox + lane);
+            if (it.mode == TB_MOG_ACCUM) *p += val;
+            else if (it.mode == TB_MOG_ATOMIC) atomicAdd(p, val);
+            else *p = val;
+            if (kDerivs) {
+                out[it.deriv_off + o] = on ? gx[j] * sc : 0.f;
+                out[it.deriv_off + (int64_t)w * h + o] = on ? gy[j] * sc : 0.f;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads)
 mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_tiles,
                   const double* __restrict__ amp, const double* __restrict__ mean,
@@ -59,7 +115,6 @@ mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_
         const int tw = min(TB_MOG_TILE, w - ox);
         const int th = min(TB_MOG_TILE, h - oy);
         const double tx0 = (double)it.x0 + ox, ty0 = (double)it.y0 + oy;
-        const double fl = it.floor;
         if (K < 0 || K > TB_MOG_MAX_K || w <= 0 || h <= 0) {
             if (threadIdx.x == 0) tb::report(st, TB_STATUS_BAD_ITEM, ii, K);
             continue;
@@ -76,6 +131,13 @@ mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_
             const double det = v0 * v3 - vxy * vxy;
             const double s = a / (2.0 * TB_PI * sqrt(det));
             const double f = -0.5 / det * TB_LOG2E;
+            double fl = it.floor;
+            if (it.floor_mode == TB_FLOOR_MINVAL) {
+                double asum = 0.0;
+                for (int k = 0; k < K; k++) asum += amp[it.c0 + k];
+                fl = -100.0;
+                if (it.floor > 0.0) fl = fmax(-100.0, log(it.floor * 2.0 * TB_PI * sqrt(det) / asum));
+            }
             g.qxx = (float)(v3 * f);
             g.qxy = (float)(-2.0 * vxy * f);
             g.qyy = (float)(v0 * f);
@@ -87,7 +149,7 @@ mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_
             g.my = (float)my;
             g.pad = 0.f;
             const bool finite = det > 0.0 && isfinite(s) && isfinite(f) && isfinite(mx) &&
-                                isfinite(my);
+                                isfinite(my) && isfinite(fl);
             if (!finite) {
                 tb::report(st, TB_STATUS_NONFINITE, ii, threadIdx.x);
             } else if (a != 0.0) {
@@ -111,41 +173,10 @@ mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_
         if (keep) comps[base + __popc(ballot & ((1u << lane) - 1u))] = g;
         __syncthreads();
 
-        // ---- evaluate: column `lane`, rows warp + 8 j ----
-        float acc[kRowsPerThread];
-#pragma unroll
-        for (int j = 0; j < kRowsPerThread; j++) acc[j] = 0.f;
-        const float xf = (float)lane;
-        for (int c = 0; c < total; c++) {
-            const GaussC q = comps[c];
-            const float dx = xf - q.mx;
-            const float A = q.qxx * dx * dx;
-            const float B = q.qxy * dx;
-#pragma unroll
-            for (int j = 0; j < kRowsPerThread; j++) {
-                const float dy = (float)(warp + 8 * j) - q.my;
-                const float e = fmaf(dy, fmaf(q.qyy, dy, B), A);
-                const float v = tb::ex2(e);
-                acc[j] = (e >= q.fl) ? fmaf(q.s, v, acc[j]) : acc[j];
-            }
-        }
-
-        // ---- write ----
-        const float sc = it.scale;
-        const int64_t ldo = it.ldo > 0 ? it.ldo : w;
-#pragma unroll
-        for (int j = 0; j < kRowsPerThread; j++) {
-            const int y = warp + 8 * j;
-            if (lane < tw && y < th) {
-                const int64_t o = (int64_t)(oy + y) * w + (ox + lane);
-                float val = acc[j] * sc;
-                if (it.mask_off >= 0 && !masks[it.mask_off + o]) val = 0.f;
-                float* p = out + it.out_off + (int64_t)(oy + y) * ldo + (ox + lane);
-                if (it.mode == TB_MOG_ACCUM) *p += val;
-                else if (it.mode == TB_MOG_ATOMIC) atomicAdd(p, val);
-                else *p = val;
-            }
-        }
+        if (it.deriv_off >= 0)
+            eval_tile<true>(it, comps, total, tw, th, ox, oy, masks, out);
+        else
+            eval_tile<false>(it, comps, total, tw, th, ox, oy, masks, out);
     }
 }
 
@@ -162,6 +193,8 @@ extern "C" int tb_mog_render(const tb_mog_item* items, int32_t n_items, int64_t 
     if (n_tiles > (int64_t)0x7fffffff) return TB_ERR_SIZE;
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return TB_ERR_LAUNCH;
+    if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
     const int64_t want = (int64_t)tb::num_sms() * 8;
     const int grid = (int)(n_tiles < want ? n_tiles : want);
     mog_render_kernel<<<grid, kThreads, 0, s>>>(items, n_items, n_tiles, comp_amp, comp_mean,

@@ -1,0 +1,120 @@
+"""Deferred GPU rendering.
+
+A RenderPlan collects the renders that one reference-level call needs --
+mixture-of-Gaussians rectangles, Fourier-path galaxies and Lanczos-shifted
+PSF stamps -- runs each kind in one batched launch, copies the results to
+the host once, and then resolves the pending Patch objects.  Source and PSF
+classes add to a plan through their _plan_* methods; the reference-facing
+methods (getModelPatch, getParamDerivatives, ...) create a plan, add their
+renders and resolve it, while Tractor-level calls share one plan across all
+sources.
+"""
+import numpy as np
+import torch
+
+from . import render
+from .patch import Patch
+
+
+class Pending(object):
+    """A value computed after the plan runs: `fn()` builds it."""
+
+    def __init__(self, fn):
+        self.fn = fn
+
+    def result(self):
+        return self.fn()
+
+
+NONE = Pending(lambda: None)
+
+
+def done(value):
+    return Pending(lambda: value)
+
+
+class RenderPlan(object):
+
+    def __init__(self):
+        self.mog = render.MogBatch()
+        self.fft = render.FftBatch()
+        self.lanczos = {}     # (h, w) -> list of (stamp, dx, dy, index)
+        self.nlz = 0
+        self._ran = False
+        self._mog_host = None
+        self._fft_host = None
+        self._lz_host = {}
+
+    # -- adding work -----------------------------------------------------
+    def add_mog(self, x0, y0, w, h, amp, mean, var, fx=0., fy=0., floor=render.FLOOR_GRID,
+                mask=None):
+        """Mixture on [x0, x0+w) x [y0, y0+h); returns a handle to its float32
+        (h, w) result."""
+        if w <= 0 or h <= 0:
+            return ('empty', h, w)
+        off = self.mog.add(x0, y0, w, h, amp, mean, var, fx=fx, fy=fy, floor=floor, mask=mask)
+        return ('mog', off, h, w)
+
+    def add_fft(self, amp, var, sz, spec_key, spec, mw, mh, sx, sy, mux, muy):
+        if mw <= 0 or mh <= 0:
+            return ('empty', mh, mw)
+        off = self.fft.add(amp, var, sz, spec_key, spec, mw, mh, sx, sy, mux, muy)
+        return ('fft', off, mh, mw)
+
+    def add_lanczos(self, stamp, dx, dy):
+        stamp = np.ascontiguousarray(stamp, np.float32)
+        key = stamp.shape
+        lst = self.lanczos.setdefault(key, [])
+        lst.append((stamp, float(dx), float(dy)))
+        return ('lz', key, len(lst) - 1)
+
+    # -- running -----------------------------------------------------------
+    def run(self):
+        if self._ran:
+            return
+        self._ran = True
+        outs = []
+        if len(self.mog):
+            outs.append(('mog', self.mog.run(check=False)))
+        if len(self.fft):
+            outs.append(('fft', self.fft.run(check=False)))
+        lz = {}
+        for key, lst in self.lanczos.items():
+            imgs = torch.from_numpy(np.stack([s for s, _, _ in lst])).to(render.device())
+            shifts = np.array([[dx, dy] for _, dx, dy in lst])
+            lz[key] = render.lanczos_shift(imgs, shifts)
+        for kind, t in outs:
+            host = t.cpu().numpy()
+            if kind == 'mog':
+                render.check_status(self.mog.status, 'tb_mog_render')
+                self._mog_host = host
+            else:
+                render.check_status(self.fft.status, 'tb_fourier_render')
+                self._fft_host = host
+        for key, t in lz.items():
+            self._lz_host[key] = t.cpu().numpy()
+
+    def get(self, handle):
+        """float32 host array of a finished render (a view into the batch
+        buffer; copy before modifying in place)."""
+        self.run()
+        kind = handle[0]
+        if kind == 'empty':
+            return np.zeros((handle[1], handle[2]), np.float32)
+        if kind == 'mog':
+            _, off, h, w = handle
+            return self._mog_host[off:off + h * w].reshape(h, w)
+        if kind == 'fft':
+            _, off, h, w = handle
+            return self._fft_host[off:off + h * w].reshape(h, w)
+        if kind == 'lz':
+            _, key, i = handle
+            return self._lz_host[key][i]
+        raise KeyError(kind)
+
+    def patch(self, x0, y0, handle, dtype=np.float32):
+        return Patch(x0, y0, np.array(self.get(handle), dtype=dtype))
+
+
+def resolve(pending_list):
+    return [p.result() if p is not None else None for p in pending_list]

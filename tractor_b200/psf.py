@@ -1,0 +1,447 @@
+"""PSF models with the reference's rendering rules (tractor/psf.py), rendered
+on the GPU.
+
+GaussianMixturePSF / NCircularGaussianPSF render point sources with the MoG
+evaluator (exact grid, masked, or ring-grown approx3 when minval > 0);
+PixelizedPSF shifts its stamp with the Lanczos-3 kernel and provides the
+spectra for the Fourier galaxy path.
+"""
+import numpy as np
+
+from . import render
+from .params import ParamList, MultiParams
+from .plan import RenderPlan, Pending, NONE
+from .patch import Patch, get_overlapping_region
+from .profiles import MixtureOfGaussians
+
+
+class HybridPSF(object):
+    """Marker class (tractor/psf.py:64-65)."""
+
+
+def _mog_extent(px, py, rr, clipExtent):
+    """get_extent of GaussianMixturePSF.getPointSourcePatch (psf.py:482-494)."""
+    x0 = int(np.floor(px - rr))
+    x1 = int(np.ceil(px + rr)) + 1
+    y0 = int(np.floor(py - rr))
+    y1 = int(np.ceil(py + rr)) + 1
+    if clipExtent is not None:
+        xl, xh, yl, yh = clipExtent
+        x0, x1, y0, y1 = max(x0, xl), min(x1, xh), max(y0, yl), min(y1, yh)
+    return x0, x1, y0, y1
+
+
+def plan_mog_grid(plan, mix, x0, x1, y0, y1, fx, fy):
+    """MixtureOfGaussians.evaluate_grid (mixture_profiles.py:248-263) as a
+    pending float64 Patch."""
+    h = plan.add_mog(x0, y0, x1 - x0, y1 - y0, mix.amp, mix.mean, mix.var, fx=fx, fy=fy)
+    return Pending(lambda: plan.patch(x0, y0, h, np.float64))
+
+
+def plan_mog_masked(plan, mix, x0, y0, mask, fx, fy):
+    """MixtureOfGaussians.evaluate_grid_masked (mixture_profiles.py:299-331),
+    values only: float32, zero outside the mask, exponent floor -30."""
+    mh, mw = mask.shape
+    amp = np.asarray(mix.amp, np.float32).astype(np.float64)
+    mean = np.asarray(mix.mean, np.float32).astype(np.float64)
+    var = np.asarray(mix.var, np.float32).astype(np.float64)
+    h = plan.add_mog(x0, y0, mw, mh, amp, mean, var, fx=fx, fy=fy, floor=render.FLOOR_MASKED,
+                     mask=np.asarray(mask, bool))
+    return Pending(lambda: plan.patch(x0, y0, h, np.float32))
+
+
+def plan_mog_approx3(plan, mix, x0, x1, y0, y1, fx, fy, minval, minradius=3, doslice=True,
+                     maxmargin=100):
+    """MixtureOfGaussians.evaluate_grid_approx3 (mixture_profiles.py:333-399).
+    The ring-grown evaluated region of c_gauss_2d_approx3 (tractor/approx3.c)
+    is computed from the exact grid values on the host side of the plan."""
+    cx = int(mix.mean[0, 0] + fx)
+    cy = int(mix.mean[0, 1] + fy)
+    if cx < x0 - maxmargin or cx > x1 + maxmargin or cy < y0 - maxmargin or cy > y1 + maxmargin:
+        return NONE
+    from . import approx
+    return approx.plan_approx3(plan, mix, x0, x1, y0, y1, fx, fy, minval, cx, cy, minradius,
+                               doslice)
+
+
+def mixture_to_patch(plan, mix, x0, x1, y0, y1, minval=0., exactExtent=False):
+    """tractor/mixture_profiles.py:425-438."""
+    if minval == 0. or minval is None:
+        return plan_mog_grid(plan, mix, x0, x1, y0, y1, 0., 0.)
+    return plan_mog_approx3(plan, mix, x0, x1, y0, y1, 0., 0., minval, doslice=not exactExtent)
+
+
+class MogParams(ParamList):
+    """A MixtureOfGaussians as parameters (tractor/utils.py:1298-1370):
+    amp[K], then means (x, y) per component, then (vxx, vyy, vxy) per
+    component."""
+
+    def __init__(self, *args):
+        if len(args) == 3:
+            amp, mean, var = args
+        else:
+            assert len(args) % 6 == 0
+            K = len(args) // 6
+            amp = np.array(args[:K])
+            mean = np.array(args[K:3 * K]).reshape((K, 2))
+            rest = args[3 * K:]
+            var = np.zeros((K, 2, 2))
+            var[:, 0, 0] = rest[::3]
+            var[:, 1, 1] = rest[1::3]
+            var[:, 0, 1] = var[:, 1, 0] = rest[2::3]
+        self.mog = MixtureOfGaussians(amp, mean, var)
+        K = self.mog.K
+        super(MogParams, self).__init__()
+        names = {}
+        for k in range(K):
+            names['amp%i' % k] = k
+            names['meanx%i' % k] = K + 2 * k
+            names['meany%i' % k] = K + 2 * k + 1
+            names['varxx%i' % k] = 3 * K + 3 * k
+            names['varyy%i' % k] = 3 * K + 3 * k + 1
+            names['varxy%i' % k] = 3 * K + 3 * k + 2
+        self.addNamedParams(**names)
+        self.liquid = [True] * self._numberOfThings()
+        self.lowers = [None] * self._numberOfThings()
+        self.uppers = [None] * self._numberOfThings()
+        self.maxstep = [None] * self._numberOfThings()
+
+    def _numberOfThings(self):
+        return 6 * self.mog.K
+
+    def _getThings(self):
+        m = self.mog
+        v = np.column_stack([m.var[:, 0, 0], m.var[:, 1, 1], m.var[:, 0, 1]]).ravel()
+        return list(m.amp) + list(m.mean.ravel()) + list(v)
+
+    def _getThing(self, i):
+        return self._getThings()[i]
+
+    def _setThings(self, vals):
+        K = self.mog.K
+        self.mog.amp[:] = vals[:K]
+        self.mog.mean[:, :] = np.reshape(vals[K:3 * K], (K, 2))
+        rest = vals[3 * K:]
+        self.mog.var[:, 0, 0] = rest[::3]
+        self.mog.var[:, 1, 1] = rest[1::3]
+        self.mog.var[:, 0, 1] = self.mog.var[:, 1, 0] = rest[2::3]
+
+    def _setThing(self, i, val):
+        v = self._getThings()
+        v[i] = val
+        self._setThings(v)
+
+    def setParams(self, p):
+        v = self._getThings()
+        for i, j in self._indexBoth():
+            v[j] = p[i]
+        self._setThings(v)
+
+    def setAllParams(self, p):
+        self._setThings(list(p))
+
+    def getLogPrior(self):
+        if np.any((self.mog.var[:, 0, 0] < 0.) | (self.mog.var[:, 1, 1] < 0.)):
+            return -np.inf
+        return 0.
+
+    def copy(self):
+        return self.__class__(self.mog.amp.copy(), self.mog.mean.copy(), self.mog.var.copy())
+
+
+class GaussianMixturePSF(MogParams):
+    """General 2-D Gaussian mixture PSF (tractor/psf.py:369-597)."""
+
+    def __init__(self, *args):
+        super(GaussianMixturePSF, self).__init__(*args)
+        self.radius = 25
+        K = self.mog.K
+        self.stepsizes = [0.01] * K + [0.01] * (2 * K) + [0.1] * (3 * K)
+
+    def getShifted(self, x0, y0):
+        return self
+
+    def constantPsfAt(self, x, y):
+        return self
+
+    def mogAt(self, x, y):
+        return self
+
+    def hashkey(self):
+        return ('GaussianMixturePSF',) + tuple(self.getAllParams())
+
+    def __str__(self):
+        return ('GaussianMixturePSF: amps=' + str(tuple(self.mog.amp.ravel())) +
+                ', means=' + str(tuple(self.mog.mean.ravel())) +
+                ', var=' + str(tuple(self.mog.var.ravel())))
+
+    def getMixtureOfGaussians(self, px=None, py=None):
+        return self.mog
+
+    def getRadius(self):
+        return self.radius
+
+    def getNSigma(self):
+        return 5.
+
+    def _plan_point_source(self, plan, px, py, minval=0., radius=None, derivs=False,
+                           minradius=None, modelMask=None, clipExtent=None, **kwargs):
+        """getPointSourcePatch (tractor/psf.py:458-528)."""
+        if modelMask is not None:
+            if modelMask.mask is None:
+                return plan_mog_grid(plan, self.mog, modelMask.x0, modelMask.x1, modelMask.y0,
+                                     modelMask.y1, px, py)
+            return plan_mog_masked(plan, self.mog, modelMask.x0, modelMask.y0, modelMask.mask,
+                                   px, py)
+        if minval is None:
+            minval = 0.
+        if minval > 0. or minradius is not None:
+            if radius is not None:
+                rr = radius
+            elif self.radius is not None:
+                rr = self.radius
+            else:
+                r = 0.
+                for v in self.mog.var:
+                    vv = v[0, 0] + v[1, 1]
+                    norm = 2. * np.pi * np.linalg.det(v)
+                    r2 = vv * -2. * np.log(minval * norm)
+                    if r2 > 0:
+                        r = max(r, np.sqrt(r2))
+                rr = int(np.ceil(r))
+            x0, x1, y0, y1 = _mog_extent(px, py, rr, clipExtent)
+            if x0 >= x1 or y0 >= y1:
+                return NONE
+            kw = {}
+            if minradius is not None:
+                kw['minradius'] = minradius
+            return plan_mog_approx3(plan, self.mog, x0, x1, y0, y1, px, py, minval, **kw)
+        r = self.getRadius() if radius is None else radius
+        x0, x1, y0, y1 = _mog_extent(px, py, r, clipExtent)
+        if x0 >= x1 or y0 >= y1:
+            return NONE
+        return plan_mog_grid(plan, self.mog, x0, x1, y0, y1, px, py)
+
+    def getPointSourcePatch(self, px, py, **kwargs):
+        plan = RenderPlan()
+        p = self._plan_point_source(plan, px, py, **kwargs)
+        return p.result()
+
+
+def getCircularMog(amps, sigmas):
+    """float32 tables as tractor/psf.py:931-944."""
+    K = len(amps)
+    amp = np.array(amps).astype(np.float32)
+    mean = np.zeros((K, 2), np.float32)
+    var = np.zeros((K, 2, 2), np.float32)
+    for k in range(K):
+        var[k, 0, 0] = var[k, 1, 1] = sigmas[k] ** 2
+    return MixtureOfGaussians(amp, mean, var, quick=True)
+
+
+class NCircularGaussianPSF(MultiParams):
+    """N concentric circular Gaussians (tractor/psf.py:792-929)."""
+
+    def __init__(self, sigmas, weights):
+        assert len(sigmas) == len(weights)
+        psig = ParamList(*sigmas)
+        psig.stepsizes = [0.01] * len(sigmas)
+        pw = ParamList(*weights)
+        pw.stepsizes = [0.01] * len(weights)
+        super(NCircularGaussianPSF, self).__init__(psig, pw)
+        self.minradius = 1.
+
+    @staticmethod
+    def getNamedParams():
+        return dict(sigmas=0, weights=1)
+
+    def getShifted(self, x0, y0):
+        return self
+
+    def constantPsfAt(self, x, y):
+        return self
+
+    @property
+    def mysigmas(self):
+        return self.sigmas.vals
+
+    @property
+    def myweights(self):
+        return self.weights.vals
+
+    @property
+    def amp(self):
+        return self.weights
+
+    @property
+    def mog(self):
+        return self.getMixtureOfGaussians()
+
+    def __str__(self):
+        return ('NCircularGaussianPSF: sigmas [ ' + ', '.join('%.3f' % s for s in self.mysigmas) +
+                ' ], weights [ ' + ', '.join('%.3f' % w for w in self.myweights) + ' ]')
+
+    def hashkey(self):
+        return ('NCircularGaussianPSF', tuple(self.mysigmas), tuple(self.myweights))
+
+    def copy(self):
+        return NCircularGaussianPSF(list(self.mysigmas), list(self.myweights))
+
+    def getMixtureOfGaussians(self, px=None, py=None):
+        return getCircularMog(tuple(self.myweights), tuple(self.mysigmas))
+
+    def getNSigma(self):
+        return 5.
+
+    def getRadius(self):
+        if hasattr(self, 'radius'):
+            return self.radius
+        return max(self.minradius, max(self.mysigmas) * self.getNSigma())
+
+    def _plan_point_source(self, plan, px, py, minval=0., radius=None, modelMask=None,
+                           clipExtent=None, **kwargs):
+        """getPointSourcePatch (tractor/psf.py:898-929)."""
+        if modelMask is not None:
+            x0, x1, y0, y1 = modelMask.extent
+        else:
+            ix = int(round(px))
+            iy = int(round(py))
+            rad = int(np.ceil(self.getRadius())) if radius is None else radius
+            x0, x1, y0, y1 = ix - rad, ix + rad + 1, iy - rad, iy + rad + 1
+        if clipExtent is not None:
+            xl, xh, yl, yh = clipExtent
+            x0, x1, y0, y1 = max(x0, xl), min(x1, xh), max(y0, yl), min(y1, yh)
+        mix = self.getMixtureOfGaussians()
+        mix = MixtureOfGaussians(mix.amp, mix.mean + np.array([px, py]), mix.var, quick=True)
+        return mixture_to_patch(plan, mix, x0, x1, y0, y1, minval=minval,
+                                exactExtent=(modelMask is not None))
+
+    def getPointSourcePatch(self, px, py, **kwargs):
+        plan = RenderPlan()
+        return self._plan_point_source(plan, px, py, **kwargs).result()
+
+
+class PixelizedPSF(ParamList):
+    """A PSF image shifted to sub-pixel positions with Lanczos-3; galaxies
+    are rendered through its Fourier transform (tractor/psf.py:68-367).
+    The PSF has no fitted parameters (as in the reference)."""
+
+    def __init__(self, img, sampling=1., Lorder=3):
+        super(PixelizedPSF, self).__init__()
+        img = np.asarray(img).astype(np.float32)
+        H, W = img.shape
+        assert (H % 2) == 1 and (W % 2) == 1
+        if sampling != 1.:
+            raise NotImplementedError('PixelizedPSF sampling != 1 is not supported')
+        self.img = img
+        self.radius = np.hypot(H / 2., W / 2.)
+        self.H, self.W = H, W
+        self.Lorder = Lorder
+        self.sampling = sampling
+        self._key = ('PixelizedPSF', id(self), img.tobytes().__hash__())
+
+    def __str__(self):
+        return 'PixelizedPSF'
+
+    @property
+    def shape(self):
+        return (self.H, self.W)
+
+    def hashkey(self):
+        return ('PixelizedPSF', tuple(self.img.ravel()))
+
+    def copy(self):
+        return self.__class__(self.img.copy())
+
+    def getShifted(self, x0, y0):
+        return self
+
+    def constantPsfAt(self, x, y):
+        return self
+
+    def getRadius(self):
+        return self.radius
+
+    def getImage(self, px, py):
+        return self.img
+
+    _normalized = False
+
+    def getFourierTransformSize(self, radius):
+        return 2 ** int(np.ceil(np.log2(radius * 2.)))
+
+    def spectrum(self, sz):
+        """(device spectrum, cx, cy) at FFT size sz (getFourierTransform,
+        tractor/psf.py:249-280, complex64, NormalizedPsf divides by |P00|)."""
+        return render.psf_spectra().get(self._key, self.getImage(0., 0.), sz,
+                                        normalize=self._normalized)
+
+    def getFourierTransform(self, px, py, radius):
+        """Host copy of the spectrum in the reference's layout:
+        (P (sz, sz/2+1) complex64, (cx, cy), (sz, sz), (v, w))."""
+        sz = self.getFourierTransformSize(radius)
+        spec, cx, cy = self.spectrum(sz)
+        P = spec.cpu().numpy().view(np.complex64).reshape(sz // 2 + 1, sz).T.copy()
+        return P, (cx, cy), (sz, sz), (np.fft.rfftfreq(sz), np.fft.fftfreq(sz))
+
+    def _plan_point_source(self, plan, px, py, minval=0., modelMask=None, radius=None,
+                           derivs=False, **kwargs):
+        """getPointSourcePatch (tractor/psf.py:137-207)."""
+        img = self.getImage(px, py)
+        if radius is not None:
+            R = int(np.ceil(radius))
+            H, W = img.shape
+            cx, cy = W // 2, H // 2
+            img = img[max(cy - R, 0):min(cy + R + 1, H - 1), max(cx - R, 0):min(cx + R + 1, W - 1)]
+        H, W = img.shape
+        ix = round(float(px))
+        iy = round(float(py))
+        dx = px - ix
+        dy = py - iy
+        x0 = ix - W // 2
+        y0 = iy - H // 2
+        if modelMask is None:
+            h = plan.add_lanczos(img, dx, dy)
+            return Pending(lambda: plan.patch(x0, y0, h, np.float32))
+        mh, mw = modelMask.shape
+        mx0, my0 = modelMask.x0, modelMask.y0
+        if (mx0 >= x0 + W) or (mx0 + mw <= x0) or (my0 >= y0 + H) or (my0 + mh <= y0):
+            return NONE
+        L = 3
+        mm = np.zeros((mh + 2 * L, mw + 2 * L), np.float32)
+        yi, yo = get_overlapping_region(my0 - y0 - L, my0 - y0 + mh - 1 + L, 0, H - 1)
+        xi, xo = get_overlapping_region(mx0 - x0 - L, mx0 - x0 + mw - 1 + L, 0, W - 1)
+        mm[yo, xo] = img[yi, xi]
+        h = plan.add_lanczos(mm, dx, dy)
+
+        def finish():
+            a = np.array(plan.get(h)[L:-L, L:-L], np.float32)
+            patch = Patch(mx0, my0, a)
+            if not derivs:
+                return patch
+            ddx = np.zeros_like(a)
+            ddx[1:-1, 1:-1] = -(a[1:-1, 2:] - a[1:-1, :-2]) / 2.
+            ddy = np.zeros_like(a)
+            ddy[1:-1, 1:-1] = -(a[2:, 1:-1] - a[:-2, 1:-1]) / 2.
+            return patch, Patch(mx0, my0, ddx), Patch(mx0, my0, ddy)
+        return Pending(finish)
+
+    def getPointSourcePatch(self, px, py, **kwargs):
+        plan = RenderPlan()
+        return self._plan_point_source(plan, px, py, **kwargs).result()
+
+
+class NormalizedPixelizedPsf(PixelizedPSF):
+    """PixelizedPSF with its image and spectrum normalised to unit sum
+    (tractor/psf.py:947-971)."""
+    _normalized = True
+
+    def getImage(self, px, py):
+        img = self.img.copy()
+        n = np.sum(img)
+        if n != 0:
+            img /= n
+        return img
+
+    def __str__(self):
+        return 'NormalizedPixelizedPSF'

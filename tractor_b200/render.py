@@ -75,25 +75,35 @@ class MogBatch(object):
         return len(self.items)
 
     def add(self, x0, y0, w, h, amp, mean, var, fx=0., fy=0., floor=FLOOR_GRID, scale=1.,
-            mask=None, out_off=None, ldo=0, mode=MOG_STORE):
+            mask=None, out_off=None, ldo=0, mode=MOG_STORE, minval=None, derivs=False):
         """Adds one mixture evaluated on [x0, x0+w) x [y0, y0+h).  Returns the
         element offset of its output (a packed w x h patch unless `out_off`
-        and `ldo` place it inside a larger buffer)."""
+        and `ldo` place it inside a larger buffer).  `minval` selects the
+        per-component floors of c_gauss_2d_approx3; `derivs` also writes the
+        d/dmean_x and d/dmean_y planes right after the patch (packed outputs
+        only)."""
         amp = np.asarray(amp, np.float64).ravel()
         K = len(amp)
         if K > 256:
             raise ValueError('at most 256 components per mixture (got %d)' % K)
         if out_off is None:
             out_off = self.nout
-            self.nout += w * h
+            self.nout += w * h * (3 if derivs else 1)
+        elif derivs:
+            raise ValueError('derivative planes need a packed output')
+        deriv_off = out_off + w * h if derivs else -1
         mask_off = -1
         if mask is not None:
             mask_off = self.nmask
             self.masks.append(np.ascontiguousarray(mask, np.uint8).ravel())
             self.nmask += w * h
+        floor_mode = _lib.FLOOR_FIXED
+        if minval is not None:
+            floor_mode = _lib.FLOOR_MINVAL
+            floor = float(minval)
         self.items.append((int(x0), int(y0), int(w), int(h), self.ncomp, K, int(mode), int(ldo),
-                           float(fx), float(fy), float(floor), float(scale), 0, int(out_off),
-                           int(mask_off), 0))
+                           float(fx), float(fy), float(floor), float(scale), floor_mode,
+                           int(out_off), int(mask_off), 0, int(deriv_off)))
         self.amp.append(amp)
         self.mean.append(np.asarray(mean, np.float64).reshape(K, 2))
         self.var.append(np.asarray(var, np.float64).reshape(K, 2, 2))
@@ -197,15 +207,17 @@ def psf_spectra():
 
 class FftBatch(object):
     """Items for tb_fourier_render (the Fourier branch of
-    ProfileGalaxy._realGetUnitFluxModelPatch, batched)."""
+    ProfileGalaxy._realGetUnitFluxModelPatch, batched).  Items may use
+    different FFT sizes and PSFs; their spectra are gathered into one device
+    buffer and each item points at its own."""
 
     def __init__(self):
         self.items = []
         self.amp = []
         self.var = []
-        self.specs = []      # (sz, key) -> psf index per size
-        self.spec_index = {}
-        self.spec_tensors = {}
+        self.spec_off = {}       # spectrum key -> float offset in the gathered buffer
+        self.spec_list = []
+        self.nspec = 0
         self.ncomp = 0
         self.nout = 0
 
@@ -223,12 +235,14 @@ class FftBatch(object):
         if out_off is None:
             out_off = self.nout
             self.nout += mw * mh
-        idx = self.spec_index.setdefault((sz, spec_key), len([k for k in self.spec_index
-                                                               if k[0] == sz]))
-        self.spec_tensors[(sz, spec_key)] = spec
-        self.items.append((self.ncomp, K, int(sz), idx, int(mw), int(mh), int(sx), int(sy),
-                           float(mux), float(muy), float(scale), int(mode), int(out_off),
-                           int(ldo), 0))
+        key = (sz, spec_key)
+        if key not in self.spec_off:
+            self.spec_off[key] = self.nspec
+            self.spec_list.append(spec)
+            self.nspec += spec.numel()
+        self.items.append((self.ncomp, K, int(sz), int(mode), int(mw), int(mh), int(sx), int(sy),
+                           float(mux), float(muy), float(scale), int(ldo), int(out_off),
+                           self.spec_off[key]))
         self.amp.append(amp)
         self.var.append(np.asarray(var, np.float64).reshape(K, 2, 2))
         self.ncomp += K
@@ -242,33 +256,23 @@ class FftBatch(object):
         if not self.items:
             return out
         items = np.array(self.items, dtype=_lib.FFT_ITEM)
-        amp = np.concatenate(self.amp)
-        var = np.concatenate(self.var)
-        self._keep = []
-        statuses = []
-        for sz in sorted(set(items['sz'].tolist())):
-            sel = items[items['sz'] == sz]
-            keys = sorted([k for k in self.spec_index if k[0] == sz], key=lambda k: self.spec_index[k])
-            specs = torch.cat([self.spec_tensors[k] for k in keys]) if len(keys) > 1 else \
-                self.spec_tensors[keys[0]]
-            pk = _Packer()
-            o_items = pk.add(sel)
-            o_amp = pk.add(amp)
-            o_var = pk.add(var)
-            o_ctr = pk.add(np.zeros(4, np.int32))
-            o_st = pk.add(np.zeros(1, _lib.STATUS))
-            d = pk.to_device(dev)
-            base = d.data_ptr()
-            rc = lib.tb_fourier_render(base + o_items, len(sel), base + o_amp, base + o_var,
-                                       specs.data_ptr(), out.data_ptr(), base + o_ctr,
-                                       base + o_st, _lib.stream_ptr(stream))
-            _lib.check(rc, 'tb_fourier_render')
-            self._keep.append((d, specs))
-            statuses.append(d[o_st:o_st + 16])
-        self.statuses = statuses
+        specs = torch.cat(self.spec_list) if len(self.spec_list) > 1 else self.spec_list[0]
+        pk = _Packer()
+        o_items = pk.add(items)
+        o_amp = pk.add(np.concatenate(self.amp))
+        o_var = pk.add(np.concatenate(self.var))
+        o_ctr = pk.add(np.zeros(4, np.int32))
+        o_st = pk.add(np.zeros(1, _lib.STATUS))
+        d = pk.to_device(dev)
+        base = d.data_ptr()
+        rc = lib.tb_fourier_render(base + o_items, len(items), base + o_amp, base + o_var,
+                                   specs.data_ptr(), out.data_ptr(), base + o_ctr, base + o_st,
+                                   _lib.stream_ptr(stream))
+        _lib.check(rc, 'tb_fourier_render')
+        self._keep = (d, specs)
+        self.status = d[o_st:o_st + 16]
         if check:
-            for s in statuses:
-                check_status(s, 'tb_fourier_render')
+            check_status(self.status, 'tb_fourier_render')
         return out
 
 
