@@ -20,6 +20,15 @@ def oracle():
     return O
 
 
+@pytest.fixture
+def host_only(monkeypatch):
+    """Replaces the device kernels by CPU stand-ins (tests/fake_device.py) to
+    test host-side logic without a GPU."""
+    import fake_device
+    fake_device.install(monkeypatch)
+    yield
+
+
 @pytest.fixture(scope='session')
 def tb():
     """The product package with its CUDA library loaded (GPU tests only)."""

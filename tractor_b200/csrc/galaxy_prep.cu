@@ -18,6 +18,7 @@
 namespace {
 
 constexpr int kMaxComp = 10;
+constexpr int kPrepThreads = 64;
 
 __device__ double bspline(const tb_profile_tables& T, int s, double x) {
     const int to = T.spline_info[4 * s], nt = T.spline_info[4 * s + 1];
@@ -28,17 +29,33 @@ __device__ double bspline(const tb_profile_tables& T, int s, double x) {
     // knot span l: t[l] <= x < t[l+1], clamped to [k, n-1]
     int l = k;
     while (l + 1 < n && t[l + 1] <= x) l++;
-    double d[4];
-    for (int j = 0; j <= k; j++) d[j] = c[j + l - k];
-    for (int r = 1; r <= k; r++) {
-        for (int j = k; j >= r; j--) {
-            const int i = j + l - k;
-            const double den = t[i + k + 1 - r] - t[i];
-            const double a = den == 0.0 ? 0.0 : (x - t[i]) / den;
-            d[j] = (1.0 - a) * d[j - 1] + a * d[j];
-        }
+    // de Boor's recursion, written out per degree with scalars:
+    // d_j <- (1 - a) d_{j-1} + a d_j, a = (x - t_i) / (t_{i+k+1-r} - t_i),
+    // i = j + l - k, for r = 1..k and j = k..r.
+    auto blend = [&](double lo, double hi, int i, int r) {
+        const double den = t[i + k + 1 - r] - t[i];
+        const double a = den == 0.0 ? 0.0 : (x - t[i]) / den;
+        return (1.0 - a) * lo + a * hi;
+    };
+    if (k == 3) {
+        double d0 = c[l - 3], d1 = c[l - 2], d2 = c[l - 1], d3 = c[l];
+        d3 = blend(d2, d3, l, 1);
+        d2 = blend(d1, d2, l - 1, 1);
+        d1 = blend(d0, d1, l - 2, 1);
+        d3 = blend(d2, d3, l, 2);
+        d2 = blend(d1, d2, l - 1, 2);
+        d3 = blend(d2, d3, l, 3);
+        return d3;
     }
-    return d[k];
+    if (k == 2) {
+        double d0 = c[l - 2], d1 = c[l - 1], d2 = c[l];
+        d2 = blend(d1, d2, l, 1);
+        d1 = blend(d0, d1, l - 1, 1);
+        d2 = blend(d1, d2, l, 2);
+        return d2;
+    }
+    if (k == 1) return blend(c[l - 1], c[l], l, 1);
+    return c[l];
 }
 
 // Fills amp/var (scalar variances) and returns K, or -1 on a table error.
@@ -82,15 +99,16 @@ __device__ int profile(const tb_profile_tables& T, int kind, double n, double* a
         var[K] = 0.0;
         Kt = K + 1;
     }
-    // stable insertion sort by variance
-    for (int i = 1; i < Kt; i++) {
-        const double a = amp[i], v = var[i];
-        int j = i - 1;
-        while (j >= 0 && var[j] > v) { amp[j + 1] = amp[j]; var[j + 1] = var[j]; j--; }
-        amp[j + 1] = a;
-        var[j + 1] = v;
-    }
+    // The caller orders the components by variance (sersic.py:338-341).
     return Kt;
+}
+
+// Position of component c when the K components are sorted by increasing
+// variance, ties kept in input order (a stable sort).
+__device__ __forceinline__ int var_rank(const double* var, int K, int c) {
+    int r = 0;
+    for (int j = 0; j < K; j++) r += (var[j] < var[c]) || (var[j] == var[c] && j < c);
+    return r;
 }
 
 __device__ double nre_of(int kind) {
@@ -204,7 +222,10 @@ __global__ void galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, i
     const double T2 = C[2] * G[0] + C[3] * G[2], T3 = C[2] * G[1] + C[3] * G[3];
     const double M00 = T0 * T0 + T1 * T1, M01 = T0 * T2 + T1 * T3, M11 = T2 * T2 + T3 * T3;
 
-    double amp[kMaxComp], var[kMaxComp];
+    // Per-thread profile scratch in shared memory.
+    __shared__ double s_amp[kPrepThreads][kMaxComp], s_var[kPrepThreads][kMaxComp];
+    double* amp = s_amp[threadIdx.x];
+    double* var = s_var[threadIdx.x];
     const int K = profile(T, s.profile, s.sersic_n, amp, var);
 
     // geometry (ModelMask given)
@@ -248,8 +269,9 @@ __global__ void galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, i
         it.muy = muy;
         it.spec_off = img.spec_off[si];
         for (int k = 0; k < K; k++) {
-            camp[it.c0 + k] = amp[k];
-            double* v = cvar + 4 * (it.c0 + k);
+            const int o = it.c0 + var_rank(var, K, k);
+            camp[o] = amp[k];
+            double* v = cvar + 4 * o;
             v[0] = var[k] * M00;
             v[1] = var[k] * M01;
             v[2] = var[k] * M01;
@@ -276,7 +298,7 @@ extern "C" int tb_galaxy_fft_prep(const tb_galaxy_src* srcs, int32_t n, const tb
         cudaFuncSetAttribute(galaxy_fft_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem) != cudaSuccess)
         return TB_ERR_LAUNCH;
-    const int threads = 64;
+    const int threads = kPrepThreads;
     galaxy_fft_prep_kernel<<<(n + threads - 1) / threads, threads, smem, (cudaStream_t)stream>>>(
         srcs, n, *image, *tables, items, comp_amp, comp_var, comp_stride, flags);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;

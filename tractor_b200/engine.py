@@ -1,0 +1,271 @@
+"""The Tractor engine (tractor/engine.py:40-497) with GPU-batched rendering.
+
+Tractor.getModelImage / getChiImage / getLogProb / getDerivs keep the
+reference's signatures and results; all renders of one call (every source in
+every image, every derivative step) go into one RenderPlan, i.e. one launch
+per kernel type.  Patches are accumulated into float32 model images in
+catalog order, as the reference does (engine.py:424-445).
+"""
+import numpy as np
+
+from .params import MultiParams
+from .patch import Patch
+from .plan import RenderPlan
+
+
+def _isint(i):
+    try:
+        return int(i) == i
+    except Exception:
+        return False
+
+
+class Catalog(MultiParams):
+    """A list of sources (engine.py:40-76)."""
+
+    def __str__(self):
+        return 'Catalog: %i sources, %i parameters' % (len(self), self.numberOfParams())
+
+    def getThawedSources(self):
+        return self._getActiveSubs()
+
+    def getFrozenSources(self):
+        return (s for s in self._getFrozenArray(self.subs) if s is not None)
+
+    def printLong(self):
+        print('Catalog with %i sources:' % len(self))
+        for i, x in enumerate(self):
+            print('  %i:' % i, x)
+
+
+class Images(MultiParams):
+    """A list of images (engine.py:78-88)."""
+
+    def getNamedParamName(self, j):
+        return 'image%i' % j
+
+
+class Tractor(MultiParams):
+    """tractor/engine.py:96-497."""
+
+    @staticmethod
+    def getName():
+        return 'Tractor'
+
+    @staticmethod
+    def getNamedParams():
+        return dict(images=0, catalog=1)
+
+    def __init__(self, images=None, catalog=None, optimizer=None, model_kwargs=None):
+        if images is None:
+            images = []
+        if catalog is None:
+            catalog = []
+        if not isinstance(images, Images):
+            images = Images(*images)
+        if not isinstance(catalog, Catalog):
+            catalog = Catalog(*catalog)
+        super(Tractor, self).__init__(images, catalog)
+        self.modtype = np.float32
+        self.modelMasks = None
+        self.expectModelMasks = False
+        if optimizer is None:
+            from .optimizer import B200Optimizer
+            optimizer = B200Optimizer()
+        self.optimizer = optimizer
+        self.model_kwargs = model_kwargs if model_kwargs is not None else {}
+
+    def __str__(self):
+        names = [im.name if im.name is not None else '[unnamed]' for im in self.images]
+        return ('%s with %i sources and %i images' % (self.getName(), len(self.catalog),
+                                                       len(self.images)) +
+                ' (' + ', '.join(names) + ')')
+
+    def __call__(self, X):
+        self.setParams(X)
+        return self.getLogProb()
+
+    def getNImages(self):
+        return len(self.images)
+
+    def getImage(self, i):
+        return self.images[i]
+
+    def getImages(self):
+        return self.images
+
+    def getCatalog(self):
+        return self.catalog
+
+    def setCatalog(self, srcs):
+        self.catalog = srcs
+
+    def setImages(self, ims):
+        self.images = ims
+
+    def addImage(self, img):
+        self.images.append(img)
+
+    def addSource(self, src):
+        self.catalog.append(src)
+
+    def addSources(self, srcs):
+        self.catalog.extend(srcs)
+
+    def removeSource(self, src):
+        self.catalog.remove(src)
+
+    # -- optimisation entry points (engine.py:194-240) --------------------
+    def optimize(self, **kwargs):
+        kw = dict(self.model_kwargs)
+        kw.update(kwargs)
+        return self.optimizer.optimize(self, **kw)
+
+    def optimize_loop(self, **kwargs):
+        kw = dict(self.model_kwargs)
+        kw.update(kwargs)
+        return self.optimizer.optimize_loop(self, **kw)
+
+    def optimize_forced_photometry(self, **kwargs):
+        kw = dict(self.model_kwargs)
+        kw.update(kwargs)
+        return self.optimizer.forced_photometry(self, **kw)
+
+    # -- model masks (engine.py:341-376) ----------------------------------
+    def setModelMasks(self, masks, assumeMasks=True):
+        self.modelMasks = masks
+        assert (masks is None) or (len(masks) == len(self.images))
+        self.expectModelMasks = (masks is not None) and assumeMasks
+
+    def _getModelMaskFor(self, image, src):
+        if self.modelMasks is None:
+            return None
+        i = self.images.index(image)
+        return self.modelMasks[i].get(src, None)
+
+    # -- rendering ----------------------------------------------------------
+    def _plan_model_patch(self, plan, img, src, **kwargs):
+        mask = self._getModelMaskFor(img, src)
+        if self.expectModelMasks and mask is None:
+            return None
+        kw = dict(self.model_kwargs)
+        kw.update(kwargs)
+        return src._plan_model_patch(plan, img, modelMask=mask, **kw)
+
+    def getModelPatch(self, img, src, **kwargs):
+        plan = RenderPlan()
+        p = self._plan_model_patch(plan, img, src, **kwargs)
+        return None if p is None else p.result()
+
+    def _plan_model_image(self, plan, img, srcs=None, sky=True, minsb=None, **kwargs):
+        if _isint(img):
+            img = self.getImage(img)
+        if srcs is None:
+            srcs = self.catalog
+        pend = []
+        for src in srcs:
+            if src is None:
+                continue
+            p = self._plan_model_patch(plan, img, src, minsb=minsb, **kwargs)
+            if p is not None:
+                pend.append(p)
+
+        def finish():
+            mod = np.zeros(img.getModelShape(), self.modtype)
+            if sky:
+                img.getSky().addTo(mod)
+            for p in pend:
+                patch = p.result()
+                if patch is not None:
+                    patch.addTo(mod)
+            return mod
+        return finish
+
+    def getModelImage(self, img, srcs=None, sky=True, minsb=None, **kwargs):
+        """engine.py:424-445: all sources rendered in one batched launch."""
+        plan = RenderPlan()
+        return self._plan_model_image(plan, img, srcs=srcs, sky=sky, minsb=minsb, **kwargs)()
+
+    def getModelImages(self, **kwargs):
+        plan = RenderPlan()
+        fins = [self._plan_model_image(plan, img, **kwargs) for img in self.images]
+        for f in fins:
+            yield f()
+
+    def getChiImage(self, imgi=-1, img=None, srcs=None, minsb=0., **kwargs):
+        if img is None:
+            img = self.getImage(imgi)
+        mod = self.getModelImage(img, srcs=srcs, minsb=minsb, **kwargs)
+        return (img.getImage() - mod) * img.getInvError()
+
+    def getChiImages(self, **kwargs):
+        plan = RenderPlan()
+        fins = [(img, self._plan_model_image(plan, img, minsb=0., **kwargs)) for img in self.images]
+        for img, f in fins:
+            yield (img.getImage() - f()) * img.getInvError()
+
+    def getLogLikelihood(self, **kwargs):
+        chisq = 0.
+        for chi in self.getChiImages(**kwargs):
+            chisq += (chi.astype(float) ** 2).sum()
+        return -0.5 * chisq
+
+    def getLogProb(self, **kwargs):
+        """engine.py:481-497."""
+        lnprior = self.getLogPrior()
+        if lnprior == -np.inf:
+            return lnprior
+        lnl = self.getLogLikelihood(**kwargs)
+        lnp = lnprior + lnl
+        if np.isnan(lnp):
+            return -np.inf
+        return lnp
+
+    # -- derivatives (engine.py:279-339) ----------------------------------
+    def _plan_derivs(self, plan, **kwargs):
+        allderivs = []
+        if self.isParamFrozen('catalog'):
+            srcs = []
+        else:
+            srcs = list(self.catalog.getThawedSources())
+        pend = []
+        if not self.isParamFrozen('images'):
+            for i in self.images.getThawedParamIndices():
+                img = self.images[i]
+                derivs = img.getParamDerivatives(self, self.catalog)
+                for di, deriv in enumerate(derivs):
+                    if deriv is False:
+                        raise NotImplementedError(
+                            'finite-difference image-parameter derivatives (PSF, WCS, photocal) '
+                            'are not provided; freeze the images')
+                    allderivs.append([(deriv, img)])
+        for src in srcs:
+            per_img = []
+            for img in self.images:
+                mask = self._getModelMaskFor(img, src)
+                if self.expectModelMasks and mask is None:
+                    per_img.append((img, [None] * src.numberOfParams()))
+                    continue
+                per_img.append((img, src._plan_derivatives(plan, img, modelMask=mask, **kwargs)))
+            pend.append((src, per_img))
+
+        def finish():
+            out = list(allderivs)
+            for src, per_img in pend:
+                srcderivs = [[] for _ in range(src.numberOfParams())]
+                for img, plist in per_img:
+                    for k, p in enumerate(plist):
+                        d = p.result() if p is not None else None
+                        if d is None:
+                            continue
+                        srcderivs[k].append((d, img))
+                out.extend(srcderivs)
+            assert len(out) == self.numberOfParams()
+            return out
+        return finish
+
+    def getDerivs(self, **kwargs):
+        """Nested list, one entry per thawed parameter, of (Patch, Image)
+        pairs (engine.py:279-339); all renders in one batch."""
+        plan = RenderPlan()
+        return self._plan_derivs(plan, **kwargs)()

@@ -1,0 +1,380 @@
+"""Least-squares optimisers with the reference's Optimizer API
+(tractor/optimize.py, tractor/lsqr_optimizer.py,
+tractor/constrained_optimizer.py), solving on the GPU.
+
+B200Optimizer is a drop-in beside LsqrOptimizer: the update direction is
+the solution of the same column-scaled least-squares problem
+(lsqr_optimizer.py:328-644) -- rows = image pixels weighted by the inverse
+error plus Gaussian-prior rows, b = chi -- formed as normal equations on
+the device (FP32 products, compensated sums, FP64 results) and solved by an
+FP64 Cholesky factorisation with one step of iterative refinement.  The line
+search renders every trial step of tryUpdates (optimize.py:425-470) in one
+batch and applies the reference's sequential acceptance rule to the results.
+
+B200ConstrainedOptimizer adds ConstrainedOptimizer's max-step and bound
+handling (constrained_optimizer.py:12-159).
+"""
+import numpy as np
+import torch
+
+from . import render
+from .plan import RenderPlan
+
+
+def default_alphas():
+    """1/1024 .. 1 in factors of 2, then sqrt(2), 2 (optimize.py:426-428)."""
+    return np.append(2. ** np.arange(-10, 1), [np.sqrt(2.), 2.])
+
+
+class B200Optimizer(object):
+
+    # -- update direction --------------------------------------------------
+    def getLinearUpdateDirection(self, tractor, damp=0, priors=True, scale_columns=True,
+                                 shared_params=True, variance=False, **kwargs):
+        allderivs = tractor.getDerivs()
+        return self.getUpdateDirection(tractor, allderivs, damp=damp, priors=priors,
+                                       scale_columns=scale_columns, shared_params=shared_params,
+                                       variance=variance)
+
+    def getUpdateDirection(self, tractor, allderivs, damp=0., priors=True, scale_columns=True,
+                           scales_only=False, chiImages=None, variance=False,
+                           shared_params=True, get_A_matrix=False):
+        """The least-squares update (lsqr_optimizer.py:328-644).  Rows are
+        restricted, per image, to the union box of the derivative patches
+        (rows outside it are zero in A and do not change the solution)."""
+        Ncols = len(allderivs)
+        if shared_params:
+            p0 = tractor.getParams()
+            tractor.setParams(np.arange(len(p0)))
+            p1 = tractor.getParams()
+            tractor.setParams(p0)
+            U, paramindexmap = np.unique(p1, return_inverse=True)
+        # per-image ROI: union of derivative extents clipped to the image
+        rois = {}
+        order = []
+        for param in allderivs:
+            for deriv, img in param:
+                H, W = img.shape
+                d = deriv.copy()
+                if not d.clipTo(W, H) or d.patch is None:
+                    continue
+                x0, x1, y0, y1 = d.getExtent()
+                if img not in rois:
+                    rois[img] = [x0, x1, y0, y1]
+                    order.append(img)
+                else:
+                    r = rois[img]
+                    rois[img] = [min(r[0], x0), max(r[1], x1), min(r[2], y0), max(r[3], y1)]
+        row0 = {}
+        nrows = 0
+        for img in order:
+            x0, x1, y0, y1 = rois[img]
+            row0[img] = nrows
+            nrows += (x1 - x0) * (y1 - y0)
+        npix_rows = nrows
+        # prior rows
+        prior = None
+        if priors:
+            X = tractor.getLogPriorDerivatives()
+            if X is not None:
+                rA, cA, vA, pb, _ = X
+                nr = max([max(r) for r in rA if len(r)] + [-1]) + 1
+                prior = (rA, cA, vA, pb, nr)
+                nrows += nr
+        if nrows == 0:
+            return []
+        A = np.zeros((Ncols, nrows), np.float32)   # column-major: A[col] is one column
+        b = np.zeros(nrows, np.float32)
+        anyval = False
+        for col, param in enumerate(allderivs):
+            for deriv, img in param:
+                H, W = img.shape
+                d = deriv.copy()
+                if not d.clipTo(W, H) or d.patch is None:
+                    continue
+                x0, x1, y0, y1 = rois[img]
+                rw = x1 - x0
+                vals = d.patch * img.getInvError()[d.getSlice(img)]
+                if not np.any(vals):
+                    continue
+                anyval = True
+                h, w = vals.shape
+                r0 = row0[img] + (d.y0 - y0) * rw + (d.x0 - x0)
+                idx = r0 + np.arange(h)[:, None] * rw + np.arange(w)[None, :]
+                A[col, idx.ravel()] += vals.ravel().astype(np.float32)
+        if prior is not None:
+            rA, cA, vA, pb, nr = prior
+            for ri, ci, vi in zip(rA, cA, vA):
+                A[ci, npix_rows + np.array(ri)] = np.array(vi, np.float32)
+            b[npix_rows:] = np.hstack(pb)
+        if not anyval and prior is None:
+            return []
+        if not np.all(np.isfinite(A)):
+            print('Warning: infinite derivatives; bailing out')
+            return None
+        colscales = np.sqrt((A.astype(np.float64) ** 2).sum(axis=1))
+        if scales_only:
+            return colscales
+        # b = chi over each image's ROI (float32, as the reference)
+        chis = None
+        if chiImages is not None:
+            chis = dict(zip(tractor.getImages(), chiImages))
+        for img in order:
+            x0, x1, y0, y1 = rois[img]
+            chi = chis.get(img) if chis is not None else None
+            if chi is None:
+                chi = tractor.getChiImage(img=img)
+            assert np.all(np.isfinite(chi))
+            b[row0[img]:row0[img] + (x1 - x0) * (y1 - y0)] = chi[y0:y1, x0:x1].ravel()
+        var = colscales ** 2 if variance else None
+        # scale columns (the reference divides each column by its norm and
+        # merges shared parameters afterwards)
+        cs = np.where(colscales > 0, colscales, 1.)
+        As = A / cs[:, None].astype(np.float32) if scale_columns else A
+        if shared_params:
+            ncols = int(paramindexmap.max()) + 1
+            Am = np.zeros((ncols, nrows), np.float32)
+            np.add.at(Am, paramindexmap, As)
+        else:
+            Am = As
+        X = self._solve(Am, b, damp)
+        if X is None:
+            return np.zeros(len(paramindexmap) if shared_params else Ncols)
+        if shared_params:
+            X = X[paramindexmap]
+        if scale_columns:
+            X = np.where(colscales > 0, X / cs, X)
+        if variance:
+            if shared_params:
+                var = var[paramindexmap]
+            return X, 1. / var
+        return X
+
+    def _solve(self, A_colmajor, b, damp):
+        """argmin ||A x - b||^2 + damp^2 ||x||^2 on the device (columns of A
+        are rows of A_colmajor)."""
+        dev = render.device()
+        P, R = A_colmajor.shape
+        A_d = torch.from_numpy(np.ascontiguousarray(A_colmajor).ravel()).to(dev)
+        b_d = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
+        AtA, Atr, ao, ro = render.normal_equations(A_d, b_d, [0], [0], [R], [P], [R])
+        X, info, _ = render.solve_update(AtA, Atr, ao, ro, [P], damp=damp)
+        if int(info.cpu()[0]) != 0:
+            return None
+        return X.cpu().numpy()
+
+    # -- line search ---------------------------------------------------------
+    def _batched_logprobs(self, tractor, p0, X, alphas):
+        """log-prob at p0 + alpha X for every alpha: all model images of all
+        trial steps rendered in one plan."""
+        plan = RenderPlan()
+        fins = []
+        for alpha in alphas:
+            tractor.setParams([p + alpha * d for p, d in zip(p0, X)])
+            lnprior = tractor.getLogPrior()
+            if lnprior == -np.inf:
+                fins.append((lnprior, None))
+                continue
+            fins.append((lnprior, [(img, tractor._plan_model_image(plan, img, minsb=0.))
+                                   for img in tractor.getImages()]))
+        tractor.setParams(p0)
+        out = []
+        for lnprior, imgs in fins:
+            if imgs is None:
+                out.append(lnprior)
+                continue
+            chisq = 0.
+            for img, f in imgs:
+                chi = (img.getImage() - f()) * img.getInvError()
+                chisq += (chi.astype(float) ** 2).sum()
+            lnp = lnprior - 0.5 * chisq
+            out.append(-np.inf if np.isnan(lnp) else lnp)
+        return out
+
+    def tryUpdates(self, tractor, X, alphas=None):
+        """Optimizer.tryUpdates (optimize.py:425-470)."""
+        if alphas is None:
+            alphas = default_alphas()
+        pBefore = tractor.getLogProb()
+        pBest = pBefore
+        alphaBest = None
+        p0 = tractor.getParams()
+        lnps = self._batched_logprobs(tractor, p0, X, alphas)
+        for alpha, pAfter in zip(alphas, lnps):
+            if not np.isfinite(pAfter):
+                break
+            if pAfter < (pBest - 1.):
+                break
+            if pAfter > pBest:
+                alphaBest = alpha
+                pBest = pAfter
+        if alphaBest is None:
+            tractor.setParams(p0)
+            return 0, 0.
+        tractor.setParams([p + alphaBest * d for p, d in zip(p0, X)])
+        return pBest - pBefore, alphaBest
+
+    # -- optimize / loop (lsqr_optimizer.py:280-326) -----------------------
+    def optimize(self, tractor, alphas=None, damp=0, priors=True, scale_columns=True,
+                 shared_params=True, variance=False, just_variance=False, **nil):
+        X = self.getLinearUpdateDirection(tractor, damp=damp, priors=priors,
+                                          scale_columns=scale_columns,
+                                          shared_params=shared_params, variance=variance)
+        if X is None:
+            return (0., None, 0.)
+        if variance:
+            if len(X) == 0:
+                return 0, X, 0, None
+            X, var = X
+            if just_variance:
+                return var
+        if len(X) == 0:
+            return 0, X, 0.
+        dlogprob, alpha = self.tryUpdates(tractor, X, alphas=alphas)
+        if variance:
+            return dlogprob, X, alpha, var
+        return dlogprob, X, alpha
+
+    def optimize_loop(self, tractor, dchisq=0., steps=50, **kwargs):
+        R = {}
+        for step in range(steps):
+            dlnp, X, alpha = self.optimize(tractor, **kwargs)
+            if dlnp <= dchisq:
+                break
+        R.update(steps=step)
+        return R
+
+    def forced_photometry(self, tractor, **kwargs):
+        raise NotImplementedError('forced photometry is not provided by this optimizer')
+
+
+class B200ConstrainedOptimizer(B200Optimizer):
+    """ConstrainedOptimizer semantics (constrained_optimizer.py:12-159):
+    trial steps limited by each parameter's max step and clipped to its
+    bounds; the loop stops on dlnp <= dchisq, or <= dchisq_limited after a
+    limited step."""
+
+    def __init__(self, *args, **kwargs):
+        super(B200ConstrainedOptimizer, self).__init__()
+        self.stepLimited = False
+        self.tiny_alpha = 1e-8
+
+    def optimize_loop(self, tractor, dchisq=0., steps=100, dchisq_limited=1e-6, check_step=None,
+                      **kwargs):
+        R = {}
+        self.hit_limit = False
+        self.last_step_hit_limit = False
+        for step in range(steps):
+            self.stepLimited = False
+            dlnp, X, alpha = self.optimize(tractor, **kwargs)
+            if check_step is not None:
+                if not check_step(optimizer=self, tractor=tractor, dlnp=dlnp, X=X, alpha=alpha):
+                    break
+            if not self.stepLimited and dlnp <= dchisq:
+                break
+            if self.stepLimited and dlnp <= dchisq_limited:
+                break
+        R.update(steps=step)
+        R.update(hit_limit=self.last_step_hit_limit, ever_hit_limit=self.hit_limit)
+        return R
+
+    def tryUpdates(self, tractor, X, alphas=None, check_step=None):
+        p_best = tractor.getParams()
+        logprob_before = tractor.getLogProb()
+        logprob_best = logprob_before
+        alpha_best = None
+        steps = self.getParameterSteps(tractor, X, alphas)
+        if len(steps) == 0:
+            self.stepLimited = True
+            self.last_step_hit_limit = True
+            self.hit_limit = True
+        p0 = tractor.getParams()
+        # evaluate all candidate parameter vectors in one batch
+        plan = RenderPlan()
+        fins = []
+        for alpha, p, step_limit, hit_limit in steps:
+            tractor.setParams(p)
+            lnprior = tractor.getLogPrior()
+            fins.append((lnprior, None if lnprior == -np.inf else
+                         [(img, tractor._plan_model_image(plan, img, minsb=0.))
+                          for img in tractor.getImages()]))
+        tractor.setParams(p0)
+        for (alpha, p, step_limit, hit_limit), (lnprior, imgs) in zip(steps, fins):
+            if hit_limit:
+                self.hit_limit = True
+            if check_step is not None:
+                tractor.setParams(p)
+                ok = check_step(optimizer=self, tractor=tractor, X=X, alpha=alpha)
+                tractor.setParams(p0)
+                if not ok:
+                    break
+            if imgs is None:
+                logprob = lnprior
+            else:
+                chisq = 0.
+                for img, f in imgs:
+                    chi = (img.getImage() - f()) * img.getInvError()
+                    chisq += (chi.astype(float) ** 2).sum()
+                logprob = lnprior - 0.5 * chisq
+                if np.isnan(logprob):
+                    logprob = -np.inf
+            if not np.isfinite(logprob):
+                break
+            if logprob < (logprob_best - 1.):
+                break
+            if logprob > logprob_best:
+                self.last_step_hit_limit = hit_limit
+                alpha_best = alpha
+                logprob_best = logprob
+                p_best = p
+        tractor.setParams(p_best)
+        if alpha_best is None:
+            return 0., 0.
+        return logprob_best - logprob_before, alpha_best
+
+    def getParameterSteps(self, tractor, step_direction, alphas):
+        """constrained_optimizer.py:84-159."""
+        if alphas is None:
+            alphas = default_alphas()
+        p0 = tractor.getParams()
+        max_step_size = tractor.getMaxStep()
+        lowers = tractor.getLowerBounds()
+        uppers = tractor.getUpperBounds()
+        assert np.all(np.diff(alphas) > 0)
+        step_direction = np.array(step_direction)
+        results = []
+        for alpha in alphas:
+            do_break = False
+            step_limit = False
+            for i, mx in enumerate(max_step_size):
+                if mx is None:
+                    continue
+                step = alpha * abs(step_direction[i])
+                if step > mx:
+                    step_limit = True
+                    do_break = True
+                    alpha = mx / abs(step_direction[i])
+                    self.stepLimited = True
+            hit_limit = False
+            for i, (ps, l, u) in enumerate(zip(p0, lowers, uppers)):
+                px = ps + alpha * step_direction[i]
+                if l is not None and px < l:
+                    alpha = (l - ps) / step_direction[i]
+                    hit_limit = True
+                if u is not None and px > u:
+                    alpha = (u - ps) / step_direction[i]
+                    hit_limit = True
+            if alpha < self.tiny_alpha:
+                break
+            p = []
+            for ps, s, l, u in zip(p0, step_direction, lowers, uppers):
+                px = ps + alpha * s
+                if l is not None and px < l:
+                    px = l
+                if u is not None and px > u:
+                    px = u
+                p.append(px)
+            results.append((alpha, p, step_limit, hit_limit))
+            if do_break:
+                break
+        return results
