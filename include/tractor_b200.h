@@ -7,9 +7,10 @@
  * (TB_OK = 0) after validating its arguments on the host; it never aborts the
  * process.  Kernels additionally write per-call status words to device memory
  * (tb_status, may be NULL; zeroed by the call on its stream before the
- * launch) that the caller reads after synchronising.  The library holds no
- * mutable global state and allocates no memory: callers own every buffer,
- * including workspaces, and may call from one stream per host thread.
+ * launch) that the caller reads after synchronising.  The library allocates
+ * no memory: callers own every buffer, including workspaces, and may call
+ * from one stream per host thread.  Its only global state is the scratch
+ * array of tb_solve_update_noalloc and that array's cached device addresses.
  *
  * Each entry point names the reference interface (file:line in the Tractor
  * source tree) whose computation it replaces.
@@ -271,6 +272,29 @@ int tb_solve_update(const double* AtA, const double* Atr,
                     const int32_t* P, const int64_t* x_off, double* X,
                     int32_t* info, double damp, int32_t n_problems,
                     int32_t max_p, double* work, void* stream);
+
+/* Allocation-free variant of tb_solve_update (no counterpart in the
+ * reference).  For callers that cannot allocate device memory when they
+ * call -- code that runs under another allocator that owns the device
+ * memory, or latency-bound loops where an allocation, which can
+ * synchronise the device, is not acceptable -- and so cannot provide the
+ * `work` buffer.  The Cholesky factors go to a file-scope scratch array of
+ * TB_SOLVE_NOALLOC_MAX_DOUBLES doubles (8 MiB) that the library holds on
+ * every GPU that loads it, until the process exits.  Requires
+ * n_problems * max_p * max_p <= TB_SOLVE_NOALLOC_MAX_DOUBLES, else returns
+ * TB_ERR_SIZE.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  All calls share the one array: calls
+ * whose kernels overlap on the GPU (different streams, or different host
+ * threads) race and must be serialised by the caller.  The array keeps the
+ * previous call's contents; the solver writes every factor entry it reads,
+ * so nothing needs clearing.  Allocates nothing (no cudaMalloc / cudaFree). */
+#define TB_SOLVE_NOALLOC_MAX_DOUBLES 1048576
+int tb_solve_update_noalloc(const double* AtA, const double* Atr,
+                            const int64_t* ata_off, const int64_t* atr_off,
+                            const int32_t* P, const int64_t* x_off, double* X,
+                            int32_t* info, double damp, int32_t n_problems,
+                            int32_t max_p, void* stream);
 
 /* Chi-square of n images: sum over pixels of ((data - model) * inverr)^2,
  * FP32 terms with compensated FP32 block sums combined in FP64; out[i] for

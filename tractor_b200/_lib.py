@@ -74,6 +74,7 @@ SIGNATURES = {
     'tb_psf_spectrum': (_I32, [_P, _P, _I32, _I32, _I32, _P]),
     'tb_normal_equations': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _I32, _P]),
     'tb_solve_update': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P, _P]),
+    'tb_solve_update_noalloc': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P]),
     'tb_chi2': (_I32, [_P, _P, _P, _P, _P, _I32, _P, _P]),
     'tb_galaxy_fft_prep': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _I32, _P, _P]),
     'tb_version': (ctypes.c_char_p, []),

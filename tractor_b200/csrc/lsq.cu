@@ -274,6 +274,44 @@ extern "C" int tb_solve_update(const double* AtA, const double* Atr, const int64
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free solve: the factor workspace is a file-scope device array,
+// held by every GPU that loads the library.  Host code cannot use the
+// array's name as a device address; its address is looked up once per device
+// (with that device current) and cached here.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_solve_scratch[TB_SOLVE_NOALLOC_MAX_DOUBLES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+double* g_solve_scratch_addr[kMaxDevices] = {nullptr};
+}  // namespace
+
+extern "C" int tb_solve_update_noalloc(const double* AtA, const double* Atr,
+                                       const int64_t* ata_off, const int64_t* atr_off,
+                                       const int32_t* P, const int64_t* x_off, double* X,
+                                       int32_t* info, double damp, int32_t n_problems,
+                                       int32_t max_p, void* stream) {
+    if (n_problems < 0 || max_p < 0) return TB_ERR_ARG;
+    if (n_problems == 0) return TB_OK;
+    if (max_p > kMaxSmemP) return TB_ERR_SIZE;
+    if ((int64_t)n_problems * max_p * max_p > (int64_t)TB_SOLVE_NOALLOC_MAX_DOUBLES)
+        return TB_ERR_SIZE;
+    if (!AtA || !Atr || !ata_off || !atr_off || !P || !x_off || !X || !info) return TB_ERR_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TB_ERR_LAUNCH;
+    if (g_solve_scratch_addr[dev] == nullptr) {
+        double* addr = nullptr;
+        if (cudaGetSymbolAddress((void**)&addr, g_solve_scratch) != cudaSuccess || !addr)
+            return TB_ERR_LAUNCH;
+        g_solve_scratch_addr[dev] = addr;
+    }
+    solve_kernel<<<n_problems, kSolveThreads, 0, (cudaStream_t)stream>>>(
+        AtA, Atr, ata_off, atr_off, P, x_off, X, info, damp, g_solve_scratch_addr[dev],
+        (int64_t)max_p * max_p);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
 extern "C" int tb_chi2(const float* data, const float* model, const float* inverr,
                        const int64_t* off, const int64_t* npix, int32_t n, double* out,
                        void* stream) {
