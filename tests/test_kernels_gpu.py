@@ -113,6 +113,17 @@ def test_psf_spectrum(tb, sz):
     assert np.abs(got - ref).max() / np.abs(ref).max() < 2e-6
 
 
+def _fourier_path(N, mw, mh, sx, sy, mux, muy):
+    """Which variant tb_fourier_render takes: the Lanczos-3 pass becomes a
+    product in frequency space when no tap of a shifted direction reaches
+    outside the N x N box (the reference's zero edges then never matter)."""
+    gr0, gr1 = max(0, -sy), min(N, mh - sy)
+    gc0, gc1 = max(0, -sx), min(N, mw - sx)
+    xin = mux == 0 or (gc0 >= 3 and gc1 <= N - 3)
+    yin = muy == 0 or (gr0 >= 3 and gr1 <= N - 3)
+    return 'spectral' if xin and yin else 'spatial'
+
+
 @pytest.mark.parametrize('sz,mw,mh', [(256, 128, 128), (128, 64, 64), (64, 40, 33),
                                       (32, 20, 20), (256, 200, 180)])
 def test_fourier_render_matches_oracle(tb, oracle, sz, mw, mh):
@@ -121,7 +132,7 @@ def test_fourier_render_matches_oracle(tb, oracle, sz, mw, mh):
     psf = _moffat(63 if sz >= 128 else (31 if sz == 64 else 15))
     spec, cx, cy = render.psf_spectra().get(('moffat-test', sz), psf, sz)
     b = render.FftBatch()
-    cases = []
+    cases, paths = [], set()
     for i in range(6):
         amp, var_s = oracle.exp_profile() if i % 2 else oracle.dev_profile()
         T = rng.normal(size=(2, 2)) * rng.uniform(0.5, 4)
@@ -136,6 +147,9 @@ def test_fourier_render_matches_oracle(tb, oracle, sz, mw, mh):
         assert rsz == sz
         off = b.add(amp2, var2, sz, ('moffat-test', sz), spec, mw, mh, sx, sy, mux, muy)
         cases.append((off, ref))
+        paths.add(_fourier_path(sz, mw, mh, sx, sy, mux, muy))
+    # both kernel variants (spectral Lanczos, spatial Lanczos at the box edge)
+    assert paths == {'spectral', 'spatial'}, paths
     out = b.run().cpu().numpy()
     for off, ref in cases:
         got = out[off:off + mw * mh].reshape(mh, mw)

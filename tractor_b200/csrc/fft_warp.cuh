@@ -5,9 +5,10 @@
 // for every group j in [0, N/R) with k = j mod L,
 //     y[(j-k) R + k + q L] = sum_m x[j + m N/R] W_{LR}^{s m k} W_R^{s m q},
 // with W_M = exp(2 pi i / M) and s = +1 (inverse, unnormalised) or -1.
-// Intermediate arrays live in a per-group exchange buffer (separate real and
-// imaginary planes, one pad word per 32 to spread banks).  The first pass
-// takes its inputs from registers: thread t holds x[t + m N/8], m = 0..7.
+// Intermediate arrays live in a per-group exchange buffer of float2 (one pad
+// element per 16, which keeps every access conflict-free except one 2-way
+// pattern in the second pass).  The first pass takes its inputs from
+// registers: thread t holds x[t + m N/8], m = 0..7.
 #pragma once
 #include "tb_common.cuh"
 
@@ -19,10 +20,10 @@ template <> struct FftPlan<128> { static constexpr int R2 = 4, R3 = 4, passes = 
 template <> struct FftPlan<64>  { static constexpr int R2 = 8, R3 = 1, passes = 2; };
 template <> struct FftPlan<32>  { static constexpr int R2 = 4, R3 = 1, passes = 2; };
 
-// Floats per group exchange buffer (both planes).
-template <int N> __host__ __device__ constexpr int fft_xbuf_floats() { return 2 * (N + N / 32); }
+// float2 elements of one group's exchange buffer.
+template <int N> __host__ __device__ constexpr int fft_xbuf_elems() { return N + N / 16; }
 
-__device__ __forceinline__ int xpad(int i) { return i + (i >> 5); }
+__device__ __forceinline__ int xpad(int i) { return i + (i >> 4); }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -73,11 +74,11 @@ template <int N, int S> __device__ __forceinline__ float2 twid(const float2* tw,
 
 // Runs the whole transform.  `v` holds the first-pass inputs of thread t
 // (v[m] = x[t + m N/8]).  `store(idx, value)` receives every output in natural
-// order exactly once (8 calls per thread).  `xr`/`xi` is the group's exchange
+// order exactly once (8 calls per thread).  `xb` is the group's exchange
 // buffer.  All threads of the warp must call this together.
 template <int N, int S, class Store>
-__device__ __forceinline__ void fft_run(float2* v, int t, float* xr, float* xi,
-                                        const float2* tw, Store store) {
+__device__ __forceinline__ void fft_run(float2* v, int t, float2* xb, const float2* tw,
+                                        Store store) {
     using P = FftPlan<N>;
     constexpr int R2 = P::R2, R3 = P::R3;
     // pass 1: radix 8, L = 1, group j = t
@@ -88,11 +89,7 @@ __device__ __forceinline__ void fft_run(float2* v, int t, float* xr, float* xi,
         return;
     }
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
-        const int o = xpad(8 * t + q);
-        xr[o] = v[q].x;
-        xi[o] = v[q].y;
-    }
+    for (int q = 0; q < 8; q++) xb[xpad(8 * t + q)] = v[q];
     __syncwarp();
     // pass 2: radix R2, L = 8
     {
@@ -102,10 +99,7 @@ __device__ __forceinline__ void fft_run(float2* v, int t, float* xr, float* xi,
         for (int g = 0; g < G; g++) {
             const int j = t + (N / 8) * g;
 #pragma unroll
-            for (int m = 0; m < R2; m++) {
-                const int o = xpad(j + m * NR);
-                a[g * R2 + m] = make_float2(xr[o], xi[o]);
-            }
+            for (int m = 0; m < R2; m++) a[g * R2 + m] = xb[xpad(j + m * NR)];
         }
         __syncwarp();
 #pragma unroll
@@ -118,13 +112,8 @@ __device__ __forceinline__ void fft_run(float2* v, int t, float* xr, float* xi,
 #pragma unroll
             for (int q = 0; q < R2; q++) {
                 const int oi = (j - k) * R2 + k + q * L;
-                if constexpr (P::passes == 2) {
-                    store(oi, b[q]);
-                } else {
-                    const int o = xpad(oi);
-                    xr[o] = b[q].x;
-                    xi[o] = b[q].y;
-                }
+                if constexpr (P::passes == 2) store(oi, b[q]);
+                else xb[xpad(oi)] = b[q];
             }
         }
         if constexpr (P::passes == 2) return;
@@ -138,10 +127,7 @@ __device__ __forceinline__ void fft_run(float2* v, int t, float* xr, float* xi,
         for (int g = 0; g < G; g++) {
             const int j = t + (N / 8) * g;
 #pragma unroll
-            for (int m = 0; m < R3; m++) {
-                const int o = xpad(j + m * NR);
-                a[g * R3 + m] = make_float2(xr[o], xi[o]);
-            }
+            for (int m = 0; m < R3; m++) a[g * R3 + m] = xb[xpad(j + m * NR)];
         }
         __syncwarp();
 #pragma unroll

@@ -1,24 +1,33 @@
 // K3: fused pixelized-PSF galaxy renderer (sm_100a).
 //
 // One CTA renders one item (galaxy) at a time, persistent over items taken
-// from a global counter, entirely in shared memory:
-//   1. column pass: for each rfft column v (sz/2+1 of them) a thread group
-//      evaluates the zero-mean mixture spectrum sum_k amp_k exp2(e_k(v, w))
-//      for all sz rows w (one SFU ex2 per element and component), multiplies
-//      by the PSF spectrum column (stored column-major, so loads coalesce),
-//      and runs an inverse complex FFT along w; only the rows the output
-//      window needs are kept, in a [row][v] buffer S1.
-//   2. row pass: pairs of kept rows are packed as H1 + i H2 with their
-//      Hermitian extension and one inverse complex FFT along v yields both
-//      real rows (the imaginary parts of the DC and Nyquist bins are dropped,
-//      as numpy's irfft does); only the needed columns are kept, in place.
-//   3. Lanczos-3 along x (in place, per row) and along y, then the integer
-//      shift and crop into the mh x mw output, scaled by scale / sz^2
-//      (irfftn's normalisation).
+// from a global counter, entirely in shared memory.  Two variants, chosen per
+// item:
+//
+// Spectral-Lanczos path (the output window keeps >= 3 pixels from the edges
+// of the sz x sz FFT box in every shifted direction, or there is no shift).
+// The reference's Lanczos-3 correlation with zero edges then equals a
+// circular correlation, i.e. a product of the spectrum with the taps'
+// frequency responses Hx(v) Hy(w), so no spatial pass is needed:
+//   1. column pass: per rfft column v, a thread group evaluates the
+//      zero-mean mixture spectrum sum_k amp_k exp2(e_k(v, w)) for all sz rows
+//      w (one SFU ex2 per element and component), multiplies by the PSF
+//      spectrum column (column-major, coalesced) and by Hy(w), and runs an
+//      inverse complex FFT along w, keeping only the output window's rows.
+//      The DC and Nyquist columns keep only the real part of their
+//      transform, as irfftn does.
+//   2. row pass: pairs of kept rows, times Hx(v), packed as H1 + i H2 with
+//      their Hermitian extension; one inverse complex FFT along v yields both
+//      real rows, written straight to the output (integer shift and crop),
+//      scaled by scale / sz^2 (irfftn's normalisation).
+// Spatial path (windows near the box edge): as above without Hx / Hy, all
+// columns transformed separately, 3 halo rows / columns kept, then Lanczos-3
+// along x in place and along y with the reference's zero edges.
+//
 // This is ProfileGalaxy._realGetUnitFluxModelPatch's FFT branch with a
 // ModelMask (tractor/galaxy.py:336-519) for a non-hybrid PixelizedPSF.
-// Masks taller than 128 rows at sz = 256 are processed in row chunks (the
-// column pass is repeated per chunk).
+// Windows taller than the row buffer are processed in row chunks (the column
+// pass is repeated per chunk).
 #include "fft_warp.cuh"
 
 namespace {
@@ -26,7 +35,7 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxK = 128;
-constexpr int kXbufPerWarp = 528;                  // floats, any N in [32, 256]
+constexpr int kXbufPerWarp = 272;                  // float2, any N in [32, 256]
 constexpr int kRmax256 = 134;                      // kept rows at sz = 256
 
 __host__ __device__ constexpr int s1_bytes(int N, int rmax) { return rmax * (N / 2 + 1) * 8; }
@@ -36,13 +45,16 @@ constexpr int kS1Bytes = s1_bytes(256, kRmax256) > s1_bytes(128, 128) ? s1_bytes
 constexpr int kSmemBytes = 256 * 8               /* twiddles */
                            + kMaxK * 16           /* components */
                            + 16 * 4               /* taps */
-                           + kWarps * kXbufPerWarp * 4 + kS1Bytes;
+                           + (129 + 256) * 8      /* Hx, Hy */
+                           + kWarps * kXbufPerWarp * 8 + kS1Bytes;
 
 struct Shared {
     float2* tw;
     float4* comp;   // (amp, ca, cb, cd): exponent = ca v^2 + cb v w + cd w^2 (log2 units)
     float* taps;    // fx[0..6], fy[0..6]
-    float* xbuf;
+    float2* hx;     // frequency response of the x taps, v = 0..N/2
+    float2* hy;     // frequency response of the y taps, row index j = 0..N-1
+    float2* xbuf;
     float2* s1;
 };
 
@@ -63,36 +75,165 @@ __device__ void taps3(double dx, float* f) {
     for (int i = 0; i < 7; i++) f[i] = (float)t[i];
 }
 
+// Mixture spectrum at (v, w) for the 8 rows of one thread: acc[m] =
+// sum_k amp_k exp2(ca v^2 + cb v w_m + cd w_m^2).
+__device__ __forceinline__ void spectrum8(const float4* comp, int K, float vf, const float* wf,
+                                          float* acc) {
+#pragma unroll
+    for (int m = 0; m < 8; m++) acc[m] = 0.f;
+    for (int k = 0; k < K; k++) {
+        const float4 c = comp[k];
+        const float al = c.y * vf * vf, be = c.z * vf;
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const float e = fmaf(wf[m], fmaf(c.w, wf[m], be), al);
+            acc[m] = fmaf(c.x, tb::ex2(e), acc[m]);
+        }
+    }
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) { return tb::cmul(a, b); }
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+
+// Zero-fills (STORE mode) the output pixels outside the window
+// [gr0, gr1) x [gc0, gc1) of G coordinates.
+__device__ void zero_outside(float* O, int64_t ldo, int mw, int mh, int sx, int sy, int gr0,
+                             int gr1, int gc0, int gc1, bool empty) {
+    for (int i = threadIdx.x; i < mh * mw; i += kThreads) {
+        const int r = i / mw - sy, c = i % mw - sx;
+        if (empty || r < gr0 || r >= gr1 || c < gc0 || c >= gc1)
+            O[(int64_t)(i / mw) * ldo + i % mw] = 0.f;
+    }
+}
+
+__device__ __forceinline__ void put(float* o, float v, int mode) {
+    if (mode == TB_MOG_ATOMIC) atomicAdd(o, v);
+    else if (mode == TB_MOG_ACCUM) *o += v;
+    else *o = v;
+}
+
 template <int N>
-__device__ void render_item(const tb_fft_item& it, int K, const float* __restrict__ spec,
-                            float* __restrict__ out, const Shared& sh, int rmax) {
+__device__ void render_item_spectral(const tb_fft_item& it, int K, const float* __restrict__ spec,
+                                     float* __restrict__ out, const Shared& sh, int rcap) {
     constexpr int NH = N / 2 + 1;
     constexpr int T = N / 8;            // threads per FFT
     constexpr int GPW = 32 / T;         // FFT groups per warp
-    constexpr int XB = tb::fft_xbuf_floats<N>();
+    constexpr int XB = tb::fft_xbuf_elems<N>();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int t = lane % T;
     const int ngroups = kWarps * GPW;
-    float* xr = sh.xbuf + warp * kXbufPerWarp + (lane / T) * XB;
-    float* xi = xr + XB / 2;
+    float2* xb = sh.xbuf + warp * kXbufPerWarp + (lane / T) * XB;
 
     const int mw = it.mw, mh = it.mh, sx = it.sx, sy = it.sy;
     const float osc = it.scale / (float)(N * N);
-    const bool accum = it.mode == TB_MOG_ACCUM || it.mode == TB_MOG_ATOMIC;
     float* O = out + it.out_off;
     const int64_t ldo = it.ldo > 0 ? it.ldo : mw;
-
     const int gr0 = max(0, -sy), gr1 = min(N, mh - sy);
     const int gc0 = max(0, -sx), gc1 = min(N, mw - sx);
-    const bool empty = gr0 >= gr1 || gc0 >= gc1;
-    // Output rows whose source row is outside [gr0, gr1) are zero.
-    if (!accum) {
-        for (int i = threadIdx.x; i < mh * mw; i += kThreads) {
-            const int r = i / mw - sy;
-            if (empty || r < gr0 || r >= gr1) O[(int64_t)(i / mw) * ldo + i % mw] = 0.f;
+
+    // frequency responses of the taps: H(f) = sum_k tap_k exp(2 pi i f (k-3) / N)
+    for (int f = threadIdx.x; f < NH + N; f += kThreads) {
+        const bool isx = f < NH;
+        const int fr = isx ? f : f - NH;
+        const float* tp = isx ? sh.taps : sh.taps + 7;
+        float2 h = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 7; k++) {
+            const float2 w = sh.tw[(fr * (k - 3)) & (N - 1)];
+            h.x = fmaf(tp[k], w.x, h.x);
+            h.y = fmaf(tp[k], w.y, h.y);
         }
+        if (isx) sh.hx[fr] = h; else sh.hy[fr] = h;
     }
-    if (empty) return;
+    __syncthreads();
+
+    for (int a = gr0; a < gr1; a += rcap) {
+        const int rlo = a, rhi = min(gr1, a + rcap);
+        const int nrows = rhi - rlo;
+
+        // ---- 1. column pass: N/2 + 1 column FFTs, times Hy ----
+        for (int v0 = warp * GPW; v0 < NH; v0 += ngroups) {
+            const bool act = v0 + lane / T < NH;
+            const int v = act ? v0 + lane / T : NH - 1;
+            float wf[8], acc[8];
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const int j = t + m * T;
+                wf[m] = (float)(j < N / 2 ? j : j - N) / (float)N;
+            }
+            spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
+            float2 x[8];
+            const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)v * N;
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const int j = t + m * T;
+                const float2 p = __ldg(P + j);
+                x[m] = cmulf(make_float2(acc[m] * p.x, acc[m] * p.y), sh.hy[j]);
+            }
+            // irfftn drops the imaginary parts of the DC and Nyquist columns
+            // after the transform along y.
+            const bool realcol = v == 0 || v == N / 2;
+            float2* S1 = sh.s1;
+            tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int row, float2 z) {
+                if (act && row >= rlo && row < rhi)
+                    S1[(row - rlo) * NH + v] = realcol ? make_float2(z.x, 0.f) : z;
+            });
+            __syncwarp();
+        }
+        __syncthreads();
+
+        // ---- 2. row pass: two real rows per complex FFT, straight to the output ----
+        const int npairs = (nrows + 1) / 2;
+        for (int p0 = warp * GPW; p0 < npairs; p0 += ngroups) {
+            const bool act = p0 + lane / T < npairs;
+            const int p = act ? p0 + lane / T : npairs - 1;
+            const int ia = 2 * p, ib = 2 * p + 1;
+            const bool hasb = ib < nrows;
+            const float2* H1 = sh.s1 + ia * NH;
+            const float2* H2 = sh.s1 + (hasb ? ib : ia) * NH;
+            float2 x[8];
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const int n = t + m * T;
+                const int q = n <= N / 2 ? n : N - n;
+                const float2 hx = sh.hx[q];
+                const float2 h1 = cmulf(H1[q], hx);
+                const float2 h2 = hasb ? cmulf(H2[q], hx) : make_float2(0.f, 0.f);
+                x[m] = n <= N / 2 ? make_float2(h1.x - h2.y, h1.y + h2.x)
+                                  : make_float2(h1.x + h2.y, h2.x - h1.y);
+            }
+            float* oa = O + (int64_t)(rlo + ia + sy) * ldo + sx;
+            float* ob = O + (int64_t)(rlo + ib + sy) * ldo + sx;
+            tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int col, float2 z) {
+                if (act && col >= gc0 && col < gc1) {
+                    put(oa + col, z.x * osc, it.mode);
+                    if (hasb) put(ob + col, z.y * osc, it.mode);
+                }
+            });
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+}
+
+template <int N>
+__device__ void render_item_spatial(const tb_fft_item& it, int K, const float* __restrict__ spec,
+                                    float* __restrict__ out, const Shared& sh, int rmax) {
+    constexpr int NH = N / 2 + 1;
+    constexpr int T = N / 8;
+    constexpr int GPW = 32 / T;
+    constexpr int XB = tb::fft_xbuf_elems<N>();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = lane % T;
+    const int ngroups = kWarps * GPW;
+    float2* xb = sh.xbuf + warp * kXbufPerWarp + (lane / T) * XB;
+
+    const int mw = it.mw, mh = it.mh, sx = it.sx, sy = it.sy;
+    const float osc = it.scale / (float)(N * N);
+    float* O = out + it.out_off;
+    const int64_t ldo = it.ldo > 0 ? it.ldo : mw;
+    const int gr0 = max(0, -sy), gr1 = min(N, mh - sy);
+    const int gc0 = max(0, -sx), gc1 = min(N, mw - sx);
     const int c0 = max(0, gc0 - 3), c1 = min(N, gc1 + 3);
     const int chunk = rmax - 6;
     const float* fx = sh.taps;
@@ -103,31 +244,17 @@ __device__ void render_item(const tb_fft_item& it, int K, const float* __restric
         const int rlo = max(0, a - 3), rhi = min(N, b + 3);
         const int nrows = rhi - rlo;
 
-        // ---- 1. column pass ----
-        // Every lane of a warp runs the same number of iterations (groups past
-        // the end compute on a clamped column and store nothing), so the
-        // warp-wide syncs inside the FFT see all 32 lanes.
+        // ---- 1. column pass (all N/2 + 1 columns) ----
         for (int v0 = warp * GPW; v0 < NH; v0 += ngroups) {
             const bool act = v0 + lane / T < NH;
             const int v = act ? v0 + lane / T : NH - 1;
-            const float vf = (float)v / (float)N;
-            float acc[8];
-            float wf[8];
+            float wf[8], acc[8];
 #pragma unroll
             for (int m = 0; m < 8; m++) {
                 const int j = t + m * T;
                 wf[m] = (float)(j < N / 2 ? j : j - N) / (float)N;
-                acc[m] = 0.f;
             }
-            for (int k = 0; k < K; k++) {
-                const float4 c = sh.comp[k];
-                const float al = c.y * vf * vf, be = c.z * vf;
-#pragma unroll
-                for (int m = 0; m < 8; m++) {
-                    const float e = fmaf(wf[m], fmaf(c.w, wf[m], be), al);
-                    acc[m] = fmaf(c.x, tb::ex2(e), acc[m]);
-                }
-            }
+            spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
             float2 x[8];
             const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)v * N;
 #pragma unroll
@@ -136,7 +263,7 @@ __device__ void render_item(const tb_fft_item& it, int K, const float* __restric
                 x[m] = make_float2(acc[m] * p.x, acc[m] * p.y);
             }
             float2* S1 = sh.s1;
-            tb::fft_run<N, +1>(x, t, xr, xi, sh.tw, [&](int row, float2 z) {
+            tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int row, float2 z) {
                 if (act && row >= rlo && row < rhi) S1[(row - rlo) * NH + v] = z;
             });
             __syncwarp();
@@ -165,7 +292,7 @@ __device__ void render_item(const tb_fft_item& it, int K, const float* __restric
             }
             float* rowA = reinterpret_cast<float*>(sh.s1 + ia * NH);
             float* rowB = reinterpret_cast<float*>(sh.s1 + ib * NH);
-            tb::fft_run<N, +1>(x, t, xr, xi, sh.tw, [&](int col, float2 z) {
+            tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int col, float2 z) {
                 if (act && col >= c0 && col < c1) {
                     rowA[col - c0] = z.x;
                     if (hasb) rowB[col - c0] = z.y;
@@ -206,29 +333,42 @@ __device__ void render_item(const tb_fft_item& it, int K, const float* __restric
 
         // ---- 3b. Lanczos along y, shift, crop, write ----
         const int orows = b - a;
-        for (int idx = threadIdx.x; idx < orows * mw; idx += kThreads) {
-            const int r = a + idx / mw;
-            const int j = idx % mw;
-            const int c = j - sx;
+        for (int idx = threadIdx.x; idx < orows * ncol; idx += kThreads) {
+            const int r = a + idx / ncol;
+            const int c = gc0 + idx % ncol;
             float val = 0.f;
-            if (c >= gc0 && c < gc1) {
 #pragma unroll
-                for (int k = 0; k < 7; k++) {
-                    const int rr = r - 3 + k;
-                    if (rr >= rlo && rr < rhi) {
-                        const float* row = reinterpret_cast<const float*>(sh.s1 + (rr - rlo) * NH);
-                        val = fmaf(fy[k], row[c - gc0], val);
-                    }
+            for (int k = 0; k < 7; k++) {
+                const int rr = r - 3 + k;
+                if (rr >= rlo && rr < rhi) {
+                    const float* row = reinterpret_cast<const float*>(sh.s1 + (rr - rlo) * NH);
+                    val = fmaf(fy[k], row[c - gc0], val);
                 }
             }
-            float* o = O + (int64_t)(r + sy) * ldo + j;
-            const float res = val * osc;
-            if (it.mode == TB_MOG_ATOMIC) atomicAdd(o, res);
-            else if (accum) *o += res;
-            else *o = res;
+            put(O + (int64_t)(r + sy) * ldo + (c + sx), val * osc, it.mode);
         }
         __syncthreads();
     }
+}
+
+template <int N>
+__device__ void render_item(const tb_fft_item& it, int K, const float* __restrict__ spec,
+                            float* __restrict__ out, const Shared& sh) {
+    const int mw = it.mw, mh = it.mh, sx = it.sx, sy = it.sy;
+    const int gr0 = max(0, -sy), gr1 = min(N, mh - sy);
+    const int gc0 = max(0, -sx), gc1 = min(N, mw - sx);
+    const bool empty = gr0 >= gr1 || gc0 >= gc1;
+    const bool accum = it.mode == TB_MOG_ACCUM || it.mode == TB_MOG_ATOMIC;
+    if (!accum)
+        zero_outside(out + it.out_off, it.ldo > 0 ? it.ldo : mw, mw, mh, sx, sy, gr0, gr1, gc0,
+                     gc1, empty);
+    if (empty) return;
+    // Zero-edged Lanczos = circular correlation when no tap leaves the box.
+    const bool xin = it.mux == 0.0 || (gc0 >= 3 && gc1 <= N - 3);
+    const bool yin = it.muy == 0.0 || (gr0 >= 3 && gr1 <= N - 3);
+    const int rcap = N == 256 ? kRmax256 : N;
+    if (xin && yin) render_item_spectral<N>(it, K, spec, out, sh, rcap);
+    else render_item_spatial<N>(it, K, spec, out, sh, N == 256 ? kRmax256 : N + 6);
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
@@ -238,11 +378,20 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
                       int32_t* counter, tb_status* st) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Shared sh;
-    sh.tw = reinterpret_cast<float2*>(smem_raw);
-    sh.comp = reinterpret_cast<float4*>(smem_raw + 256 * 8);
-    sh.taps = reinterpret_cast<float*>(smem_raw + 256 * 8 + kMaxK * 16);
-    sh.xbuf = sh.taps + 16;
-    sh.s1 = reinterpret_cast<float2*>(sh.xbuf + kWarps * kXbufPerWarp);
+    unsigned char* p = smem_raw;
+    sh.tw = reinterpret_cast<float2*>(p);
+    p += 256 * 8;
+    sh.comp = reinterpret_cast<float4*>(p);
+    p += kMaxK * 16;
+    sh.taps = reinterpret_cast<float*>(p);
+    p += 16 * 4;
+    sh.hx = reinterpret_cast<float2*>(p);
+    p += 129 * 8;
+    sh.hy = reinterpret_cast<float2*>(p);
+    p += 256 * 8;
+    sh.xbuf = reinterpret_cast<float2*>(p);
+    p += kWarps * kXbufPerWarp * 8;
+    sh.s1 = reinterpret_cast<float2*>(p);
     __shared__ int64_t slot;
     __shared__ int cur_n;
     if (threadIdx.x == 0) cur_n = 0;
@@ -283,10 +432,10 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
         __syncthreads();
         const float* spec = psf_spec + it.spec_off;
         switch (N) {
-            case 256: render_item<256>(it, K, spec, out, sh, kRmax256); break;
-            case 128: render_item<128>(it, K, spec, out, sh, 128 + 6); break;
-            case 64: render_item<64>(it, K, spec, out, sh, 64 + 6); break;
-            default: render_item<32>(it, K, spec, out, sh, 32 + 6); break;
+            case 256: render_item<256>(it, K, spec, out, sh); break;
+            case 128: render_item<128>(it, K, spec, out, sh); break;
+            case 64: render_item<64>(it, K, spec, out, sh); break;
+            default: render_item<32>(it, K, spec, out, sh); break;
         }
     }
 }
@@ -324,12 +473,11 @@ constexpr int kSpecThreads = 256;
 
 template <int N>
 __device__ void spec_rows(const float* __restrict__ pad, float* __restrict__ spec, int img,
-                          float* xbuf, const float2* tw) {
-    constexpr int T = N / 8, GPW = 32 / T, XB = tb::fft_xbuf_floats<N>();
+                          float2* xbuf, const float2* tw) {
+    constexpr int T = N / 8, GPW = 32 / T, XB = tb::fft_xbuf_elems<N>();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int t = lane % T;
-    float* xr = xbuf + warp * kXbufPerWarp + (lane / T) * XB;
-    float* xi = xr + XB / 2;
+    float2* xb = xbuf + warp * kXbufPerWarp + (lane / T) * XB;
     const int nwarps = kSpecThreads / 32;
     const float* I = pad + (int64_t)img * N * N;
     float2* S = reinterpret_cast<float2*>(spec) + (int64_t)img * N * (N / 2 + 1);
@@ -338,7 +486,7 @@ __device__ void spec_rows(const float* __restrict__ pad, float* __restrict__ spe
         float2 x[8];
 #pragma unroll
         for (int m = 0; m < 8; m++) x[m] = make_float2(I[(int64_t)y * N + t + m * T], 0.f);
-        tb::fft_run<N, -1>(x, t, xr, xi, tw, [&](int k, float2 z) {
+        tb::fft_run<N, -1>(x, t, xb, tw, [&](int k, float2 z) {
             if (k <= N / 2) S[(int64_t)k * N + y] = z;
         });
         __syncwarp();
@@ -346,12 +494,11 @@ __device__ void spec_rows(const float* __restrict__ pad, float* __restrict__ spe
 }
 
 template <int N>
-__device__ void spec_cols(float* __restrict__ spec, int img, float* xbuf, const float2* tw) {
-    constexpr int T = N / 8, GPW = 32 / T, XB = tb::fft_xbuf_floats<N>(), NH = N / 2 + 1;
+__device__ void spec_cols(float* __restrict__ spec, int img, float2* xbuf, const float2* tw) {
+    constexpr int T = N / 8, GPW = 32 / T, XB = tb::fft_xbuf_elems<N>(), NH = N / 2 + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int t = lane % T;
-    float* xr = xbuf + warp * kXbufPerWarp + (lane / T) * XB;
-    float* xi = xr + XB / 2;
+    float2* xb = xbuf + warp * kXbufPerWarp + (lane / T) * XB;
     const int nwarps = kSpecThreads / 32;
     float2* S = reinterpret_cast<float2*>(spec) + (int64_t)img * N * NH;
     for (int v0 = blockIdx.x * nwarps * GPW + warp * GPW; v0 < NH; v0 += gridDim.x * nwarps * GPW) {
@@ -361,7 +508,7 @@ __device__ void spec_cols(float* __restrict__ spec, int img, float* xbuf, const 
 #pragma unroll
         for (int m = 0; m < 8; m++) x[m] = S[(int64_t)v * N + t + m * T];
         __syncwarp();
-        tb::fft_run<N, -1>(x, t, xr, xi, tw, [&](int j, float2 z) {
+        tb::fft_run<N, -1>(x, t, xb, tw, [&](int j, float2 z) {
             if (act) S[(int64_t)v * N + j] = z;
         });
         __syncwarp();
@@ -371,7 +518,7 @@ __device__ void spec_cols(float* __restrict__ spec, int img, float* xbuf, const 
 template <int N>
 __global__ void __launch_bounds__(kSpecThreads) spec_kernel(const float* pad, float* spec, int pass) {
     __shared__ float2 tw[N];
-    __shared__ float xbuf[(kSpecThreads / 32) * kXbufPerWarp];
+    __shared__ float2 xbuf[(kSpecThreads / 32) * kXbufPerWarp];
     tb::build_twiddles<N>(tw);
     __syncthreads();
     if (pass == 0) spec_rows<N>(pad, spec, blockIdx.y, xbuf, tw);

@@ -18,7 +18,7 @@
 namespace {
 
 constexpr int kMaxComp = 10;
-constexpr int kPrepThreads = 64;
+constexpr int kPrepThreads = 128;   // 4 sources (warps) per block
 
 __device__ double bspline(const tb_profile_tables& T, int s, double x) {
     const int to = T.spline_info[4 * s], nt = T.spline_info[4 * s + 1];
@@ -56,59 +56,6 @@ __device__ double bspline(const tb_profile_tables& T, int s, double x) {
     }
     if (k == 1) return blend(c[l - 1], c[l], l, 1);
     return c[l];
-}
-
-// Fills amp/var (scalar variances) and returns K, or -1 on a table error.
-__device__ int profile(const tb_profile_tables& T, int kind, double n, double* amp, double* var) {
-    if (kind == TB_PROFILE_EXP || kind == TB_PROFILE_DEV) {
-        const int K = kind == TB_PROFILE_EXP ? T.exp_K : T.dev_K;
-        const double* a = kind == TB_PROFILE_EXP ? T.exp_amp : T.dev_amp;
-        const double* v = kind == TB_PROFILE_EXP ? T.exp_var : T.dev_var;
-        if (K > kMaxComp) return -1;
-        for (int k = 0; k < K; k++) { amp[k] = a[k]; var[k] = v[k]; }
-        return K;
-    }
-    if (kind == TB_PROFILE_GAUSSIAN) {
-        amp[0] = 1.0;
-        var[0] = 1.0;
-        return 1;
-    }
-    const double lowest = T.range_lohi[0], highest = T.range_lohi[2 * T.n_ranges - 1];
-    int r = -1;
-    if (n <= lowest) { r = 0; n = lowest; }
-    else if (n >= highest) { r = T.n_ranges - 1; n = highest; }
-    else {
-        for (int i = 0; i < T.n_ranges; i++)
-            if (T.range_lohi[2 * i] <= n && n < T.range_lohi[2 * i + 1]) { r = i; break; }
-    }
-    if (r < 0) return -1;
-    const int K = T.range_info[4 * r], sa = T.range_info[4 * r + 1], sv = T.range_info[4 * r + 2];
-    if (K + 1 > kMaxComp) return -1;
-    double s = 0.0;
-    for (int k = 0; k < K; k++) { amp[k] = bspline(T, sa + k, n); s += amp[k]; }
-    for (int k = 0; k < K; k++) amp[k] /= s;
-    for (int k = 0; k < K; k++) var[k] = exp(bspline(T, sv + k, n));
-    int Kt = K;
-    if (n > 1.0) {
-        const double core = bspline(T, T.core_spline, n);
-        double s2 = 0.0;
-        for (int k = 0; k < K; k++) s2 += amp[k];
-        const double f = (1.0 - core) / s2;
-        for (int k = 0; k < K; k++) amp[k] *= f;
-        amp[K] = core;
-        var[K] = 0.0;
-        Kt = K + 1;
-    }
-    // The caller orders the components by variance (sersic.py:338-341).
-    return Kt;
-}
-
-// Position of component c when the K components are sorted by increasing
-// variance, ties kept in input order (a stable sort).
-__device__ __forceinline__ int var_rank(const double* var, int K, int c) {
-    int r = 0;
-    for (int j = 0; j < K; j++) r += (var[j] < var[c]) || (var[j] == var[c] && j < c);
-    return r;
 }
 
 __device__ double nre_of(int kind) {
@@ -158,34 +105,80 @@ __host__ __device__ inline int tables_smem_bytes(const tb_profile_tables& G) {
            4 * (4 * G.n_ranges + 4 * G.n_splines);
 }
 
-__global__ void galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, int n,
-                                       tb_fft_image img, tb_profile_tables Tg,
-                                       tb_fft_item* __restrict__ items, double* __restrict__ camp,
-                                       double* __restrict__ cvar, int stride,
-                                       int32_t* __restrict__ flags) {
+// Sum over lanes 0..K-1 of v, accumulated in lane order (the reference's
+// sequential numpy sum for these short vectors).
+__device__ __forceinline__ double lane_sum(double v, int K) {
+    double s = 0.0;
+    for (int k = 0; k < K; k++) s += __shfl_sync(0xffffffffu, v, k);
+    return s;
+}
+
+// One warp per source.  Lane l < K evaluates component l's amplitude and
+// log-variance splines; sums and the stable variance ranking use shuffles;
+// the shape and geometry are computed redundantly by every lane.
+__global__ void __launch_bounds__(kPrepThreads)
+galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, int n, tb_fft_image img,
+                       tb_profile_tables Tg, tb_fft_item* __restrict__ items,
+                       double* __restrict__ camp, double* __restrict__ cvar, int stride,
+                       int32_t* __restrict__ flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const tb_profile_tables T = stage_tables(Tg, smem_raw);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (kPrepThreads / 32) + (threadIdx.x >> 5);
+    if (i >= n) return;   // whole warps leave together
     const tb_galaxy_src s = srcs[i];
-    tb_fft_item it;
-    it.c0 = i * stride;
-    it.K = 0;
-    it.sz = 32;
-    it.mode = TB_MOG_STORE;
-    it.mw = s.mw;
-    it.mh = s.mh;
-    it.sx = 0;
-    it.sy = 0;
-    it.mux = 0.0;
-    it.muy = 0.0;
-    it.scale = (float)s.counts;
-    it.ldo = 0;
-    it.out_off = s.out_off;
-    it.spec_off = img.spec_off[0] >= 0 ? img.spec_off[0] : 0;
-    int flag = 0;
 
-    // shape -> (re [arcsec], theta, ab) -> basis G
+    // ---- profile: lane l holds component l ----
+    double a = 0.0, v = 0.0;
+    int K = -1;
+    if (s.profile == TB_PROFILE_EXP || s.profile == TB_PROFILE_DEV) {
+        const bool ex = s.profile == TB_PROFILE_EXP;
+        K = ex ? T.exp_K : T.dev_K;
+        if (K > kMaxComp) K = -1;
+        else if (lane < K) {
+            a = ex ? T.exp_amp[lane] : T.dev_amp[lane];
+            v = ex ? T.exp_var[lane] : T.dev_var[lane];
+        }
+    } else if (s.profile == TB_PROFILE_GAUSSIAN) {
+        K = 1;
+        if (lane == 0) { a = 1.0; v = 1.0; }
+    } else {
+        double nn = s.sersic_n;
+        const double lowest = T.range_lohi[0], highest = T.range_lohi[2 * T.n_ranges - 1];
+        int r = -1;
+        if (nn <= lowest) { r = 0; nn = lowest; }
+        else if (nn >= highest) { r = T.n_ranges - 1; nn = highest; }
+        else {
+            for (int q = 0; q < T.n_ranges; q++)
+                if (T.range_lohi[2 * q] <= nn && nn < T.range_lohi[2 * q + 1]) { r = q; break; }
+        }
+        if (r >= 0) {
+            const int Kr = T.range_info[4 * r], sa = T.range_info[4 * r + 1];
+            const int sv = T.range_info[4 * r + 2];
+            if (Kr + 1 <= kMaxComp) {
+                if (lane < Kr) {
+                    a = bspline(T, sa + lane, nn);
+                    v = exp(bspline(T, sv + lane, nn));
+                }
+                a /= lane_sum(a, Kr);
+                K = Kr;
+                if (nn > 1.0) {
+                    const double core = bspline(T, T.core_spline, nn);
+                    a *= (1.0 - core) / lane_sum(a, Kr);
+                    if (lane == Kr) { a = core; v = 0.0; }
+                    K = Kr + 1;
+                }
+            }
+        }
+    }
+    // stable rank by increasing variance (sersic.py:338-341)
+    int rank = 0;
+    for (int j = 0; j < (K > 0 ? K : 0); j++) {
+        const double vj = __shfl_sync(0xffffffffu, v, j);
+        rank += (vj < v) || (vj == v && j < lane);
+    }
+
+    // ---- shape -> basis G -> pixel covariance factor M = T T^T ----
     double re, G[4];
     if (s.shape_type == TB_SHAPE_RABPHI) {
         const double phi = (90.0 - s.s2) * (TB_PI / 180.0);
@@ -222,13 +215,7 @@ __global__ void galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, i
     const double T2 = C[2] * G[0] + C[3] * G[2], T3 = C[2] * G[1] + C[3] * G[3];
     const double M00 = T0 * T0 + T1 * T1, M01 = T0 * T2 + T1 * T3, M11 = T2 * T2 + T3 * T3;
 
-    // Per-thread profile scratch in shared memory.
-    __shared__ double s_amp[kPrepThreads][kMaxComp], s_var[kPrepThreads][kMaxComp];
-    double* amp = s_amp[threadIdx.x];
-    double* var = s_var[threadIdx.x];
-    const int K = profile(T, s.profile, s.sersic_n, amp, var);
-
-    // geometry (ModelMask given)
+    // ---- geometry (ModelMask given) ----
     const double px = s.px, py = s.py;
     const int x0 = s.mx0, y0 = s.my0, x1 = s.mx0 + s.mw, y1 = s.my0 + s.mh;
     double hs = fmax(s.mh / 2.0, s.mw / 2.0);
@@ -238,8 +225,8 @@ __global__ void galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, i
     int sz = 1;
     while (sz < 2.0 * hsi && sz < (1 << 20)) sz *= 2;
     const bool out = px < x0 || px > x1 - 1 || py < y0 || py > y1 - 1;
-    int si = sz == 32 ? 0 : sz == 64 ? 1 : sz == 128 ? 2 : sz == 256 ? 3 : -1;
-
+    const int si = sz == 32 ? 0 : sz == 64 ? 1 : sz == 128 ? 2 : sz == 256 ? 3 : -1;
+    int flag = 0;
     if (K < 0 || s.mw <= 0 || s.mh <= 0) {
         flag = 2;
     } else if (s.counts == 0.0) {
@@ -255,31 +242,46 @@ __global__ void galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, i
     } else if (si < 0 || img.spec_off[si] < 0) {
         flag = 2;
     }
-    if (flag == 0) {
-        const double dx = px - img.psf_cx[si], dy = py - img.psf_cy[si];
-        double mux = dx - x0, muy = dy - y0;
-        const double sxd = rint(mux), syd = rint(muy);
-        mux -= sxd;
-        muy -= syd;
-        it.K = K;
-        it.sz = sz;
-        it.sx = (int)sxd;
-        it.sy = (int)syd;
-        it.mux = mux;
-        it.muy = muy;
-        it.spec_off = img.spec_off[si];
-        for (int k = 0; k < K; k++) {
-            const int o = it.c0 + var_rank(var, K, k);
-            camp[o] = amp[k];
-            double* v = cvar + 4 * o;
-            v[0] = var[k] * M00;
-            v[1] = var[k] * M01;
-            v[2] = var[k] * M01;
-            v[3] = var[k] * M11;
-        }
+    const int c0 = i * stride;
+    if (flag == 0 && lane < K) {
+        camp[c0 + rank] = a;
+        double* w = cvar + 4 * (c0 + rank);
+        w[0] = v * M00;
+        w[1] = v * M01;
+        w[2] = v * M01;
+        w[3] = v * M11;
     }
-    items[i] = it;
-    flags[i] = flag;
+    if (lane == 0) {
+        tb_fft_item it;
+        it.c0 = c0;
+        it.K = 0;
+        it.sz = 32;
+        it.mode = TB_MOG_STORE;
+        it.mw = s.mw;
+        it.mh = s.mh;
+        it.sx = 0;
+        it.sy = 0;
+        it.mux = 0.0;
+        it.muy = 0.0;
+        it.scale = (float)s.counts;
+        it.ldo = 0;
+        it.out_off = s.out_off;
+        it.spec_off = img.spec_off[0] >= 0 ? img.spec_off[0] : 0;
+        if (flag == 0) {
+            const double dx = px - img.psf_cx[si], dy = py - img.psf_cy[si];
+            double mux = dx - x0, muy = dy - y0;
+            const double sxd = rint(mux), syd = rint(muy);
+            it.K = K;
+            it.sz = sz;
+            it.sx = (int)sxd;
+            it.sy = (int)syd;
+            it.mux = mux - sxd;
+            it.muy = muy - syd;
+            it.spec_off = img.spec_off[si];
+        }
+        items[i] = it;
+        flags[i] = flag;
+    }
 }
 
 }  // namespace
@@ -298,8 +300,9 @@ extern "C" int tb_galaxy_fft_prep(const tb_galaxy_src* srcs, int32_t n, const tb
         cudaFuncSetAttribute(galaxy_fft_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem) != cudaSuccess)
         return TB_ERR_LAUNCH;
-    const int threads = kPrepThreads;
-    galaxy_fft_prep_kernel<<<(n + threads - 1) / threads, threads, smem, (cudaStream_t)stream>>>(
+    const int per_block = kPrepThreads / 32;
+    galaxy_fft_prep_kernel<<<(n + per_block - 1) / per_block, kPrepThreads, smem,
+                             (cudaStream_t)stream>>>(
         srcs, n, *image, *tables, items, comp_amp, comp_var, comp_stride, flags);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
