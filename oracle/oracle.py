@@ -520,6 +520,74 @@ def pixpsf_point_patch_masked(psf_img, px, py, mx0, my0, mw, mh):
 # Likelihood and least squares
 # ---------------------------------------------------------------------------
 
+# ---------------------------------------------------------------------------
+# Batched scenes (Tractor.getModelImage with rectangular model masks)
+# ---------------------------------------------------------------------------
+
+SCENE_POINT, SCENE_EXP, SCENE_DEV, SCENE_COMP = 0, 1, 2, 3
+
+
+def scene_source_mixture(kind, px, py, fdev, shape_a, shape_b, pamp, pmean, pvar,
+                         cdinv=None):
+    """Pixel-space mixture of one source with the PSF applied, in the order
+    the reference evaluates it.  Point source: the PSF mixture itself, offset
+    by (px, py) at evaluation (psf.py:458-528), returned with fx, fy = px, py.
+    Exp / deV: _getAffineProfile (galaxy.py:648-669) convolved with the PSF
+    (galaxy.py:307-326, mixture_profiles.py:158-172).  FixedComposite:
+    _getAffineProfile of galaxy.py:847-876 -- deV block (amp x fracDev) then
+    exp block (amp x (1 - fracDev)), each present only when its fraction is
+    non-zero.  `shape_a` is the exp (or single) EllipseE (re, e1, e2),
+    `shape_b` the deV one of a composite.  Returns (amp, mean, var, fx, fy)."""
+    pamp = np.asarray(pamp, np.float64)
+    pmean = np.asarray(pmean, np.float64)
+    pvar = np.asarray(pvar, np.float64)
+    if kind == SCENE_POINT:
+        return pamp, pmean, pvar, px, py
+    cdinv = nullwcs_cdinv() if cdinv is None else cdinv
+    blocks = []
+    if kind == SCENE_COMP:
+        f = min(1., max(0., fdev))
+        if f > 0.:
+            blocks.append((f, dev_profile(), shape_b))
+        if f < 1.:
+            blocks.append((1. - f, exp_profile(), shape_a))
+    else:
+        blocks.append((1., exp_profile() if kind == SCENE_EXP else dev_profile(), shape_a))
+    amps, vars_ = [], []
+    for frac, (a, v), shp in blocks:
+        T = cdinv @ ellipseE_basis(*shp)
+        amps.append(np.asarray(a, np.float64) * frac)
+        vars_.append(T @ diag_var(v) @ T.T)
+    amp = np.concatenate(amps)
+    var = np.concatenate(vars_)
+    mean = np.zeros((len(amp), 2)) + np.array([px, py])
+    ca, cm, cv = convolve(amp, mean, var, pamp, pmean, pvar)
+    return ca, cm, cv, 0., 0.
+
+
+def scene_model(sources, pamp, psig, H, W):
+    """Tractor.getModelImage (engine.py:424-445) of a scene whose every source
+    has a rectangular ModelMask inside the image: each patch is the exact grid
+    over its mask (float64), times counts (LinearPhotoCal(1): counts = flux,
+    pointsource.py:36-60), added in catalog order into a float32 image
+    (Patch.addTo, patch.py:341-354).  `sources` rows: kind, px, py, flux, mx0,
+    my0, mw, mh, fracDev, exp-or-single (re, e1, e2), deV (re, e1, e2)."""
+    K = len(pamp)
+    pmean = np.zeros((K, 2))
+    pvar = np.zeros((K, 2, 2))
+    pvar[:, 0, 0] = pvar[:, 1, 1] = np.asarray(psig, np.float64) ** 2
+    mod = np.zeros((H, W), np.float32)
+    for row in np.asarray(sources, np.float64):
+        kind = int(row[0])
+        px, py, flux = row[1], row[2], row[3]
+        mx0, my0, mw, mh = (int(v) for v in row[4:8])
+        ca, cm, cv, fx, fy = scene_source_mixture(kind, px, py, row[8], row[9:12], row[12:15],
+                                                  pamp, pmean, pvar)
+        p = mog_grid(mx0, mx0 + mw, my0, my0 + mh, fx, fy, ca, cm, cv) * flux
+        mod[my0:my0 + mh, mx0:mx0 + mw] += p
+    return mod
+
+
 def chi_image(data, model, inverr):
     """Tractor.getChiImage, tractor/engine.py:455-473."""
     return (data - model) * inverr

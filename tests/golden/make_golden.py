@@ -191,6 +191,55 @@ def main():
                         lnp0=lnp0, X=np.array(X), p_before=p_before, dlnp1=dlnp, X1=np.array(X1),
                         alpha1=alpha, p_after1=p_after1, p_final=p_final, steps=R['steps'],
                         **dict(('d0.' + k, v) for k, v in patches_to_arrays(d0).items()))
+    # -- 5. Batched-render scene: mixed sources with square model masks on one
+    #       float32 image, 3-component MoG PSF, through Tractor.getModelImage --
+    rng = np.random.default_rng(500)
+    H, W = 256, 320
+    s1 = rng.uniform(1., 2.)
+    pamp = np.array([0.7, 0.2, 0.1])
+    psig = np.array([s1, 2. * s1, 4. * s1])
+    psf5 = GaussianMixturePSF(pamp, np.zeros((3, 2)),
+                              np.array([np.eye(2) * s ** 2 for s in psig]))
+    tim5 = Image(data=np.zeros((H, W), np.float32), inverr=np.ones((H, W), np.float32),
+                 psf=psf5, photocal=LinearPhotoCal(1.))
+    rows, srcs5, masks5 = [], [], {}
+    for i in range(80):
+        kind = rng.choice(4, p=[0.4, 0.3, 0.2, 0.1])
+        px, py = rng.uniform(-5, W + 5), rng.uniform(-5, H + 5)
+        flux = float(np.exp(rng.uniform(np.log(10.), np.log(1e5))))
+        hw = int(np.round(np.exp(rng.uniform(np.log(7), np.log(60)))))
+        shp = []
+        for _ in range(2):
+            re = float(np.exp(rng.uniform(np.log(0.5), np.log(8))))
+            shp += [re, float(rng.uniform(0.2, 1)), float(rng.uniform(0, 180))]
+        fdev = float(rng.uniform(0, 1))
+        ea = EllipseE.fromRAbPhi(*shp[:3])
+        eb = EllipseE.fromRAbPhi(*shp[3:])
+        pos, br = PixPos(px, py), Flux(flux)
+        if kind == 0:
+            s = PointSource(pos, br)
+        elif kind == 1:
+            s = ExpGalaxy(pos, br, ea)
+        elif kind == 2:
+            s = DevGalaxy(pos, br, ea)
+        else:
+            s = FixedCompositeGalaxy(pos, br, fdev, ea, eb)
+        # square mask centred on the nearest pixel, clipped to the image
+        cx, cy = int(np.round(px)), int(np.round(py))
+        mx0, mx1 = max(0, cx - hw), min(W, cx + hw + 1)
+        my0, my1 = max(0, cy - hw), min(H, cy + hw + 1)
+        if mx0 >= mx1 or my0 >= my1:
+            continue
+        masks5[s] = ModelMask(mx0, my0, mx1 - mx0, my1 - my0)
+        srcs5.append(s)
+        rows.append([kind, px, py, flux, mx0, my0, mx1 - mx0, my1 - my0, fdev,
+                     ea.re, ea.e1, ea.e2, eb.re, eb.e1, eb.e2])
+    tr5 = Tractor([tim5], srcs5)
+    tr5.setModelMasks([masks5])
+    mod5 = tr5.getModelImage(0)
+    assert mod5.dtype == np.float32
+    np.savez_compressed(os.path.join(OUT, 'scene_mog.npz'), sources=np.array(rows),
+                        psf_amp=pamp, psf_sigma=psig, shape=np.array([H, W]), model=mod5)
     print('golden fixtures written to', OUT)
 
 

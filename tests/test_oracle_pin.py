@@ -83,6 +83,17 @@ def test_mog_paths_match_golden(oracle):
     assert np.abs(p2 * 100. - ref2[2]).max() < 1e-12 * ref2[2].max()
 
 
+def test_scene_model_matches_golden(oracle):
+    """80 mixed sources (point / exp / deV / composite) with square model
+    masks and a 3-component MoG PSF, through the reference's
+    Tractor.getModelImage: the oracle's scene model is bit-identical."""
+    g = _golden('scene_mog.npz')
+    H, W = (int(v) for v in g['shape'])
+    mod = oracle.scene_model(g['sources'], g['psf_amp'], g['psf_sigma'], H, W)
+    assert mod.dtype == np.float32
+    assert np.array_equal(mod, g['model'])
+
+
 def test_reference_known_answers(oracle):
     """test_galaxy.py:93-96: patch origin (24, 25), shape (52, 53), sum 100;
     test_tractor.py:74-88: peak flux / (2 pi sigma^2), lnp = -143.681."""
