@@ -241,6 +241,93 @@ int tb_psf_spectrum(const float* pad, float* spec, int32_t n, int32_t sz,
                     int32_t normalize, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Scene rendering: many sources into whole images (mixture-of-Gaussians PSFs)
+ *
+ * The batched form of Tractor.getModelImage (tractor/engine.py:424-445) for
+ * images whose PSF is a Gaussian mixture: every source's getModelPatch with
+ * a rectangular ModelMask (galaxy.py:266-326 run_mog with evaluate_grid,
+ * PointSource via GaussianMixturePSF.getPointSourcePatch, psf.py:458-528),
+ * times its counts, added into a float32 image (Patch.addTo clips to the
+ * image, patch.py:341-354).  One record per (source, image): a source seen
+ * in several images (bands) has one record per image, each with its counts.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    double px, py;          /* pixel position in this image */
+    double counts;          /* brightness in this image's counts */
+    double fdev;            /* TB_PROFILE_COMPOSITE: deV fraction, clamped to [0, 1] */
+    double sa0, sa1, sa2;   /* shape (see shape_type): the galaxy's, or the exp
+                               part of a composite */
+    double sb0, sb1, sb2;   /* deV shape of a composite */
+    double sersic_n;        /* TB_PROFILE_SERSIC */
+    int32_t profile;        /* TB_PROFILE_* (incl. POINT and COMPOSITE) */
+    int32_t shape_type;     /* TB_SHAPE_* (both shapes of a composite) */
+    int32_t image;          /* index into the image table */
+    int32_t mx0, my0, mw, mh;  /* ModelMask rectangle (image pixels) */
+    int32_t pad;
+} tb_scene_src;
+
+#define TB_PROFILE_POINT 4       /* PointSource (tractor/pointsource.py) */
+#define TB_PROFILE_COMPOSITE 5   /* FixedCompositeGalaxy (galaxy.py:779-1029) */
+
+/* One image: size, output placement, PSF mixture and WCS.  tile0 = the
+ * exclusive prefix over images of ceil(W/32) * ceil(H/tile_h) for the tile
+ * height passed to tb_scene_render; n_tiles = the total. */
+typedef struct {
+    int32_t W, H;
+    int32_t ldo;            /* row stride in elements (0 = W) */
+    int32_t psf_c0, psf_K;  /* PSF components psf_amp[psf_c0 + k] (k < psf_K <= 32) */
+    int32_t pad;
+    int64_t out_off;        /* element offset of pixel (0, 0) in `out` */
+    int64_t tile0;
+    double cd_inv[4];       /* WCS cdInverse (row-major), NullWCS: I * 3600 / pixscale */
+    double pixscale;
+} tb_scene_image;
+
+/* A prepared (source, image) record.  flag: 0 = rendered; 1 = no patch
+ * (zero counts, or the mask misses the image); 2 = unsupported (bad image
+ * index, unknown profile, too many components). */
+typedef struct {
+    int32_t x0, y0, w, h;   /* rectangle: the mask clipped to the image */
+    int32_t c0, K;          /* components comp_*[c0 .. c0+K) */
+    int32_t image;
+    int32_t flag;
+    double fx, fy;          /* evaluation offset (point sources: the position) */
+    float scale;            /* counts */
+    float floor;            /* exponent floor, natural-log units (-50: the grid cut) */
+} tb_scene_item;
+
+/* Prepares n records: profile mixture (exp / deV / Sersic / Gaussian /
+ * composite / point), shape to pixel covariance, convolution with the
+ * image's PSF mixture (mixture_profiles.py:158-172: PSF component outer,
+ * galaxy component inner), rectangle.  Components of record i go to
+ * comp_*[i * comp_stride ...] (FP64; mean 2, var 4 values per component),
+ * K = (galaxy components) x psf_K <= comp_stride <= 256. */
+int tb_scene_prep(const tb_scene_src* srcs, int32_t n, const tb_scene_image* images,
+                  int32_t n_images, const double* psf_amp, const double* psf_mean,
+                  const double* psf_var, const tb_profile_tables* tables,
+                  tb_scene_item* items, double* comp_amp, double* comp_mean,
+                  double* comp_var, int32_t comp_stride, void* stream);
+
+/* Workspace bytes tb_scene_render needs for n_tiles tiles and at most
+ * max_pairs (item, tile) overlaps (host call, writes *bytes). */
+int tb_scene_workspace(int64_t n_tiles, int64_t max_pairs, int64_t* bytes);
+
+/* Renders every image: bins the items by image tile (32 x tile_h pixels,
+ * tile_h 16, 32 or 64), then one persistent launch evaluates each tile's
+ * sources in item order (each source's components summed first, as a
+ * patch, then added inside its rectangle) and writes the tile once.
+ * mode TB_MOG_STORE writes every pixel of every image (0 where no source
+ * reaches), TB_MOG_ACCUM adds to `out`.  Summation order is the item order
+ * for tiles reached by at most 1024 items.  max_pairs bounds the (item,
+ * tile) overlaps; more are reported as TB_STATUS_BAD_ITEM (detail -3). */
+int tb_scene_render(const tb_scene_item* items, int32_t n_items,
+                    const tb_scene_image* images, int32_t n_images, int64_t n_tiles,
+                    int32_t tile_h, const double* comp_amp, const double* comp_mean,
+                    const double* comp_var, float* out, int32_t mode, void* workspace,
+                    int64_t workspace_bytes, int64_t max_pairs, tb_status* status,
+                    void* stream);
+
+/* ------------------------------------------------------------------------
  * Least-squares step
  * ------------------------------------------------------------------------ */
 
@@ -308,8 +395,9 @@ int tb_chi2(const float* data, const float* model, const float* inverr,
 const char* tb_version(void);
 
 /* ABI guard for bindings: writes sizeof(tb_mog_item), sizeof(tb_fft_item),
- * sizeof(tb_status), sizeof(tb_galaxy_src), sizeof(tb_fft_image) into
- * sizes[0..4] (host memory) and returns 5.  No reference counterpart
+ * sizeof(tb_status), sizeof(tb_galaxy_src), sizeof(tb_fft_image),
+ * sizeof(tb_scene_src), sizeof(tb_scene_image), sizeof(tb_scene_item) into
+ * sizes[0..7] (host memory) and returns 8.  No reference counterpart
  * (bindings check their struct layouts with it). */
 int tb_abi_sizes(int32_t* sizes);
 

@@ -31,7 +31,21 @@ GALAXY_SRC = np.dtype([('px', '<f8'), ('py', '<f8'), ('counts', '<f8'), ('s0', '
                        ('profile', '<i4'), ('shape_type', '<i4'), ('mx0', '<i4'), ('my0', '<i4'),
                        ('mw', '<i4'), ('mh', '<i4')])
 
+SCENE_SRC = np.dtype([('px', '<f8'), ('py', '<f8'), ('counts', '<f8'), ('fdev', '<f8'),
+                      ('sa0', '<f8'), ('sa1', '<f8'), ('sa2', '<f8'),
+                      ('sb0', '<f8'), ('sb1', '<f8'), ('sb2', '<f8'), ('sersic_n', '<f8'),
+                      ('profile', '<i4'), ('shape_type', '<i4'), ('image', '<i4'),
+                      ('mx0', '<i4'), ('my0', '<i4'), ('mw', '<i4'), ('mh', '<i4'),
+                      ('pad', '<i4')])
+SCENE_IMAGE = np.dtype([('W', '<i4'), ('H', '<i4'), ('ldo', '<i4'), ('psf_c0', '<i4'),
+                        ('psf_K', '<i4'), ('pad', '<i4'), ('out_off', '<i8'), ('tile0', '<i8'),
+                        ('cd_inv', '<f8', (4,)), ('pixscale', '<f8')])
+SCENE_ITEM = np.dtype([('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'), ('h', '<i4'),
+                       ('c0', '<i4'), ('K', '<i4'), ('image', '<i4'), ('flag', '<i4'),
+                       ('fx', '<f8'), ('fy', '<f8'), ('scale', '<f4'), ('floor', '<f4')])
+
 PROFILE_EXP, PROFILE_DEV, PROFILE_SERSIC, PROFILE_GAUSSIAN = 0, 1, 2, 3
+PROFILE_POINT, PROFILE_COMPOSITE = 4, 5
 SHAPE_ELLIPSE_E, SHAPE_ELLIPSE_ESOFT, SHAPE_RABPHI = 0, 1, 2
 
 
@@ -77,6 +91,10 @@ SIGNATURES = {
     'tb_solve_update_noalloc': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P]),
     'tb_chi2': (_I32, [_P, _P, _P, _P, _P, _I32, _P, _P]),
     'tb_galaxy_fft_prep': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _I32, _P, _P]),
+    'tb_scene_prep': (_I32, [_P, _I32, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P]),
+    'tb_scene_workspace': (_I32, [_I64, _I64, _P]),
+    'tb_scene_render': (_I32, [_P, _I32, _P, _I32, _I64, _I32, _P, _P, _P, _P, _I32, _P, _I64,
+                               _I64, _P, _P]),
     'tb_version': (ctypes.c_char_p, []),
     'tb_abi_sizes': (_I32, [_P]),
 }
@@ -103,10 +121,11 @@ def load():
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
-    sizes = np.zeros(5, np.int32)
+    sizes = np.zeros(8, np.int32)
     lib.tb_abi_sizes(sizes.ctypes.data)
     want = (MOG_ITEM.itemsize, FFT_ITEM.itemsize, STATUS.itemsize, GALAXY_SRC.itemsize,
-            ctypes.sizeof(FftImage))
+            ctypes.sizeof(FftImage), SCENE_SRC.itemsize, SCENE_IMAGE.itemsize,
+            SCENE_ITEM.itemsize)
     if tuple(int(s) for s in sizes) != want:
         raise ImportError('libtractor_b200.so struct layout %s != binding %s' %
                           (tuple(sizes), want))

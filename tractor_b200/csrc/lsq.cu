@@ -331,5 +331,8 @@ extern "C" int tb_abi_sizes(int32_t* sizes) {
     sizes[2] = (int32_t)sizeof(tb_status);
     sizes[3] = (int32_t)sizeof(tb_galaxy_src);
     sizes[4] = (int32_t)sizeof(tb_fft_image);
-    return 5;
+    sizes[5] = (int32_t)sizeof(tb_scene_src);
+    sizes[6] = (int32_t)sizeof(tb_scene_image);
+    sizes[7] = (int32_t)sizeof(tb_scene_item);
+    return 8;
 }
