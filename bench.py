@@ -16,6 +16,12 @@ over sources.  L2 is flushed (a 256 MB write) before every timed step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+The JSON line also carries, under "secondary", the batched-scene workload
+(20,000 point / exp / deV / composite sources on one 4096x4096 image through
+a 3-component MoG PSF; prep + binning + one persistent tile render, the
+tile height autotuned) with its own end-to-end number, roofline and CPU
+baseline (--no-secondary skips it).
+
 --impl reference times the reference's CPU implementation of the same
 workload on the host cores (its own compiled C for the spectrum and the
 Lanczos shift, numpy's irfftn, galaxy.py's geometry), one source per task
@@ -51,6 +57,8 @@ def parse():
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--cpu-seconds', type=float, default=12.0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-secondary', action='store_true',
+                    help='skip the batched-scene measurement added to the JSON line')
     return ap.parse_args()
 
 
@@ -166,6 +174,160 @@ class ClockSampler(object):
 
 
 # ---------------------------------------------------------------------------
+# secondary workload: the batched scene (20,000 sources on one 4096^2 image)
+# ---------------------------------------------------------------------------
+
+SCENE_N = 20000
+SCENE_WH = 4096
+SCENE_WORKLOAD = ('20,000 sources (40% point, 30% exp, 20% deV, 10% exp+deV composite) on one '
+                  '4096x4096 float32 image, square ModelMasks of half-width log-U[7, 127], '
+                  'fluxes log-U[10, 1e5], 3-component MoG PSF')
+
+
+def _scene_inputs(seed):
+    from tractor_b200 import batch
+    rng = np.random.default_rng(seed)
+    s1 = rng.uniform(1., 2.)
+    sig, wts = [s1, 2 * s1, 4 * s1], [0.7, 0.2, 0.1]
+    recs = batch.scene_sources(SCENE_N, rng, W=SCENE_WH, H=SCENE_WH)
+    return recs, sig, wts
+
+
+def _scene_cpu_worker(args):
+    """Oracle scene render of records [i0, i1) (each source's grid over its
+    mask clipped to the image); returns (pix*components, seconds, count)."""
+    i0, i1, seed, budget = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    recs, sig, wts = _scene_inputs(seed)
+    pa = np.asarray(wts, np.float64)
+    pm = np.zeros((3, 2))
+    pv = np.zeros((3, 2, 2))
+    pv[:, 0, 0] = pv[:, 1, 1] = np.asarray(sig) ** 2
+    kind = {4: 0, 0: 1, 1: 2, 5: 3}
+    work, t0, i = 0., time.perf_counter(), i0
+    while i < i1 and time.perf_counter() - t0 < budget:
+        q = recs[i]
+        x0, y0 = max(q['mx0'], 0), max(q['my0'], 0)
+        x1, y1 = min(q['mx0'] + q['mw'], SCENE_WH), min(q['my0'] + q['mh'], SCENE_WH)
+        if x1 > x0 and y1 > y0:
+            ca, cm, cv, fx, fy = O.scene_source_mixture(
+                kind[int(q['profile'])], q['px'], q['py'], q['fdev'],
+                [q['sa0'], q['sa1'], q['sa2']], [q['sb0'], q['sb1'], q['sb2']], pa, pm, pv)
+            O.mog_grid(x0, x1, y0, y1, fx, fy, ca, cm, cv)
+            work += (x1 - x0) * (y1 - y0) * len(ca)
+        i += 1
+    return work, time.perf_counter() - t0, i - i0
+
+
+def scene_cpu_rate(seconds, seed):
+    ncores = os.cpu_count() or 1
+    per = SCENE_N // ncores
+    tasks = [(c * per, (c + 1) * per, seed, seconds) for c in range(ncores)]
+    with mp.get_context('spawn').Pool(ncores) as pool:
+        res = pool.map(_scene_cpu_worker, tasks)
+    work = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    return work / busy / 1e6, ncores, sum(r[2] for r in res)
+
+
+def bench_scene(args, dev, flush, clk, cpu_seconds):
+    """The batched-scene workload: autotuned tile height, device-timed steps
+    (prep + bin + render from records resident in HBM, L2 flushed), the
+    host-buffer call end to end, roofline against the SFU ex2 rate."""
+    import ctypes
+    import torch
+    from tractor_b200 import batch, _lib, render as R
+    recs, sig, wts = _scene_inputs(2000)
+    img = batch.SceneImage.circular(SCENE_WH, SCENE_WH, sig, wts)
+    r = batch.SceneRenderer([img])
+    n = len(recs)
+    pinned = torch.from_numpy(recs.view(np.uint8).copy()).pin_memory()
+    d_src = pinned.to(dev)
+    mp_by_h = dict((th, r.max_pairs(recs, th)) for th in batch.SCENE_TILE_HEIGHTS)
+    tune = r.autotune(d_src, n, mp_by_h)
+    th = r.tile_h
+    out = torch.empty(r.npix, dtype=torch.float32, device=dev)
+    out_pinned = torch.empty(r.npix, dtype=torch.float32).pin_memory()
+    for _ in range(max(3, args.warmup)):
+        r.render_device(d_src, n, out, mp_by_h[th], th)
+    torch.cuda.synchronize()
+    items = r.items(n)
+    assert np.all(items['flag'] == 0)
+    pixcomp = float(np.sum(items['w'].astype(np.float64) * items['h'] * items['K']))
+    lib = _lib.load()
+    d_img, n_tiles = r.image_table(th)
+    _, ws, it_t, comps, status = r.workspace(n, mp_by_h[th], th)
+    stride = r.comp_stride
+    base = comps.data_ptr()
+    camp, cmean, cvar = base, base + 8 * n * stride, base + 24 * n * stride
+    pb = r._psf.data_ptr()
+    steps = max(3, min(args.steps, 20))
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    stream = _lib.stream_ptr()
+    for k in range(steps):
+        flush.zero_()
+        ev[k][0].record()
+        _lib.check(lib.tb_scene_prep(d_src.data_ptr(), n, d_img.data_ptr(), 1, pb + r._o_pamp,
+                                     pb + r._o_pmean, pb + r._o_pvar,
+                                     ctypes.addressof(r.tables.struct), it_t.data_ptr(), camp,
+                                     cmean, cvar, stride, stream), 'tb_scene_prep')
+        ev[k][1].record()
+        _lib.check(lib.tb_scene_render(it_t.data_ptr(), n, d_img.data_ptr(), 1, n_tiles, th,
+                                       camp, cmean, cvar, out.data_ptr(), _lib.MOG_STORE,
+                                       ws.data_ptr(), ws.numel(), mp_by_h[th],
+                                       status.data_ptr(), stream), 'tb_scene_render')
+        ev[k][2].record()
+    torch.cuda.synchronize()
+    step_s = sum(e[0].elapsed_time(e[2]) for e in ev) / 1e3 / steps
+    render_s = sum(e[1].elapsed_time(e[2]) for e in ev) / 1e3 / steps
+    R.check_status(status.clone(), 'tb_scene_render')
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        ev2[k][0].record()
+        d_src.copy_(pinned, non_blocking=True)
+        r.render_device(d_src, n, out, mp_by_h[th], th)
+        out_pinned.copy_(out, non_blocking=True)
+        ev2[k][1].record()
+    torch.cuda.synchronize()
+    e2e_s = sum(a.elapsed_time(b) for a, b in ev2) / 1e3 / steps
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak_clk = clk['sm_mhz'] if clk else 1965.0
+    peak = SFU_EX2_PER_CLK_PER_SM * nsm * peak_clk * 1e6 / 1e9
+    achieved = pixcomp / render_s / 1e9
+    line = {
+        'workload': SCENE_WORKLOAD,
+        'metric': 'Mpix*components/s (batched scene render)',
+        'value': pixcomp / step_s / 1e6, 'unit': 'Mpix*components/s',
+        'ms_per_step': step_s * 1e3, 'steps': steps,
+        'pix_components_per_step': pixcomp,
+        'autotuned_tile': {'tile_w': 32, 'tile_h': th,
+                           'ms_by_tile_h': dict((str(k), v) for k, v in tune.items())},
+        'e2e': {'value': pixcomp / e2e_s / 1e6, 'unit': 'Mpix*components/s',
+                'h2d_bytes_per_step': int(pinned.numel()),
+                'd2h_bytes_per_step': int(out_pinned.numel() * 4)},
+        'gpu_launches_per_step': 7,
+        'roofline': {'bound': 'sfu', 'kernel': 'tb_scene_render (bin + render)',
+                     'achieved': achieved, 'peak': peak, 'unit': 'Gex2/s',
+                     'frac': achieved / peak,
+                     'algorithmic': 'sum over sources of rectangle pixels x components = '
+                                    '%.0f ex2 per launch' % pixcomp,
+                     'kernel_ms': render_s * 1e3,
+                     'traffic': ncu_traffic('scene_render_c3.json')},
+    }
+    if cpu_seconds:
+        rate, cores, nsrc = scene_cpu_rate(cpu_seconds, 2000)
+        line['cpu_baseline'] = {'value': rate, 'unit': 'Mpix*components/s', 'cores': cores,
+                                'kind': 'port',
+                                'sample': '%d of the 20,000 sources rendered by the oracle '
+                                          '(c_gauss_2d_grid restatement), one process per core'
+                                          % nsrc}
+    return line
+
+
+# ---------------------------------------------------------------------------
 
 def init_dist():
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -174,10 +336,10 @@ def init_dist():
     return world, rank, local
 
 
-def ncu_traffic():
-    """DRAM bytes per tb_fourier_render launch of this workload, from the
-    committed ncu summary (profiles/fourier_render_c2.json), or None."""
-    p = os.path.join(ROOT, 'profiles', 'fourier_render_c2.json')
+def ncu_traffic(name='fourier_render_c2.json'):
+    """DRAM bytes per launch of a workload's top kernel, from its committed
+    ncu summary under profiles/, or None."""
+    p = os.path.join(ROOT, 'profiles', name)
     try:
         with open(p) as f:
             return json.load(f).get('dram_bytes_per_launch')
@@ -359,6 +521,10 @@ def main():
                      'traffic': ncu_traffic()},
         'clocks': clk,
     }
+    if not args.no_secondary:
+        line['secondary'] = [bench_scene(args, dev, flush, clk,
+                                         None if (args.no_cpu_baseline or world > 1 or rank)
+                                         else min(args.cpu_seconds, 8.0))]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, nsrc, wall = cpu_rate(args.cpu_seconds, use_ref=False)
         line['cpu_baseline'] = {'value': rate, 'unit': 'Mpix*components/s', 'cores': cores,
