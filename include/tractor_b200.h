@@ -383,6 +383,127 @@ int tb_solve_update_noalloc(const double* AtA, const double* Atr,
                             int32_t* info, double damp, int32_t n_problems,
                             int32_t max_p, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched blob fitting (Levenberg-Marquardt over many independent blobs)
+ *
+ * The batched form of Tractor.optimize_loop with LsqrOptimizer
+ * (tractor/lsqr_optimizer.py:280-326; engine.py:279-339 getDerivs,
+ * engine.py:455-473 getChiImage) and ConstrainedOptimizer's step limits
+ * (tractor/constrained_optimizer.py:12-159) for galaxies and point sources
+ * seen in up to 3 bands through mixture-of-Gaussians PSFs.  A blob is a set
+ * of sources and one image per band (all of one size, aligned); every
+ * (blob, band) image is a "unit".
+ *
+ * Parameters: TB_FIT_NPAR slots per source, in the reference's order for a
+ * SersicGalaxy with NanoMaggies brightness and an EllipseESoft shape:
+ * x, y (pixels), flux[3] (counts; LinearPhotoCal(1)), log r_e, ee1, ee2,
+ * Sersic n.  Unused slots (missing bands, the index of exp / deV galaxies,
+ * the shape of point sources) have zero derivative and never move.
+ * Source k of blob b is sources[b.src0 + k]; its parameters start at
+ * params[TB_FIT_NPAR * (b.src0 + k)].
+ * ------------------------------------------------------------------------ */
+#define TB_FIT_NPAR 9
+#define TB_FIT_MAX_BANDS 3
+#define TB_FIT_MAX_SRC 32
+#define TB_FIT_MAX_PSF 4
+#define TB_FIT_SERSIC_MIN 0.29   /* SersicIndex bounds, tractor/sersic.py:349-351 */
+#define TB_FIT_SERSIC_MAX 6.3
+
+typedef struct {
+    int32_t profile;          /* TB_PROFILE_SERSIC, _EXP, _DEV or _POINT */
+    int32_t x0, y0, w, h;     /* ModelMask in blob pixels (fixed during a fit) */
+    int32_t blob;             /* the blob it belongs to */
+} tb_fit_source;
+
+/* Buffers of blob b: hbuf + h_off holds (n_bands + 2) P x P FP64 blocks
+ * (per-band partial A^T A, accepted A^T A, Cholesky factor); gbuf + g_off
+ * holds (n_bands + 1) P-vectors (per-band A^T r, accepted). */
+typedef struct {
+    int32_t n_src;            /* sources (<= TB_FIT_MAX_SRC) */
+    int32_t src0;             /* first source */
+    int32_t P;                /* n_src * TB_FIT_NPAR */
+    int32_t unit0;            /* chi2_part[unit0 + band] holds band `band`'s chi^2 */
+    int64_t h_off, g_off;
+    int64_t tile_off;         /* the blob's 32 x 8 tiles in `tiles`: first the n_active */
+    int32_t n_active;         /* tiles some source mask reaches, then the others */
+    int32_t n_tiles;          /* (each entry tx | ty << 16) */
+} tb_fit_blob;
+
+/* One (blob, band) image: W x H float32 pixels of data and inverr at
+ * pix_off (row stride W), and the band's PSF mixture (psf_K <= 4).  The
+ * unit table is in blob-major, band-minor order: unit blob * n_bands + band. */
+typedef struct {
+    int32_t blob, band;
+    int32_t W, H;
+    int64_t pix_off;
+    int32_t psf_K;
+    int32_t pad;
+    double psf_amp[4];
+    double psf_mean[8];
+    double psf_var[16];
+} tb_fit_unit;
+
+/* Per-blob optimiser state.  status: 0 running, 1 converged (the predicted
+ * log-likelihood gain of the next step is below tol), 2 stopped (damping
+ * exhausted, or non-finite chi^2 at the start), 3 iteration limit. */
+typedef struct {
+    double chi2;              /* chi^2 of the accepted parameters */
+    double dlnp;              /* log-likelihood gain of the last accepted step */
+    double lambda;            /* Marquardt damping (relative to the scaled diagonal) */
+    double pred;              /* predicted log-likelihood gain of the next step */
+    int32_t iters, accepted, rejected, status;
+} tb_fit_state;
+
+/* Bytes of the workspace tb_fit_prep writes and tb_fit_pass reads: per
+ * source a summary and its PSF-convolved components in every band (host
+ * call). */
+int tb_fit_workspace(int32_t n_src, int32_t n_bands, int64_t* bytes);
+
+/* Initialises n_blobs states (status 0, chi^2 = inf, lambda = lambda0). */
+int tb_fit_reset(tb_fit_state* state, int32_t n_blobs, double lambda0, void* stream);
+
+/* Per-source tables at `params` (the trial parameters): profile mixture and
+ * its derivative in n (tractor/sersic.py:288-342), shape factor T T^T and
+ * its derivatives in (log r_e, ee1, ee2) (ellipses.py:165-263,
+ * galaxy.py:659-669) by FP64 central differences, and from them every
+ * band's PSF-convolved components (mixture_profiles.py:158-172) with their
+ * derivative coefficients.  cd_inv: the WCS cdInverse, 4 doubles in HOST
+ * memory (one WCS for every blob). */
+int tb_fit_prep(const tb_fit_source* srcs, int32_t n_src, const double* params,
+                int32_t n_bands, const tb_fit_unit* units, int32_t n_units,
+                const double* cd_inv, const tb_profile_tables* tables, void* workspace,
+                void* stream);
+
+/* mode 0: for every unit of a running blob, over the tiles its sources'
+ * masks reach: the model (each source's PSF-convolved mixture on its mask,
+ * summed), r = (data - model) * inverr, the analytic derivative columns
+ * A = dmodel/dparams * inverr, and the unit's A^T A (upper triangle), A^T r
+ * and r^T r + chi2_const (chi2_part[blob.unit0 + band]).  mode 1 (once per
+ * data set): chi2_const[blob.unit0 + band] = r^T r over the other tiles,
+ * where the model is zero.  Replaces getDerivs / getChiImage / the A and b
+ * assembly of lsqr_optimizer.py:328-520.  A persistent grid takes units
+ * in the order `order` lists them (e.g. largest first) from work_counter
+ * (one int32 of device scratch). */
+int tb_fit_pass(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
+                const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
+                const void* workspace, const float* data, const float* inverr,
+                const int32_t* tiles, double* hbuf, double* gbuf, double* chi2_part,
+                double* chi2_const, const tb_fit_state* state, int32_t n_bands,
+                int32_t mode, int32_t* work_counter, tb_status* status, void* stream);
+
+/* One Levenberg-Marquardt step per running blob: accept the trial
+ * parameters if chi^2 fell (the first pass is always accepted), else raise
+ * the damping; solve (D^-1 H D^-1 + lambda I) x = D^-1 g, D = sqrt(diag H),
+ * by FP64 Cholesky with one refinement step; scale the step to respect the
+ * maximum steps (PixPos 1, log r_e 1, ee 0.1, n 0.1) and the Sersic-index
+ * bounds; write params + step into `trial`.  Stops a blob when the step's
+ * predicted log-likelihood gain is below `tol` with lambda <= 1
+ * (optimize_loop's dchisq, tested on the prediction). */
+int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
+                const tb_fit_source* srcs, double* params, double* trial, double* hbuf,
+                double* gbuf, const double* chi2_part, tb_fit_state* state, double tol,
+                int32_t max_iter, void* stream);
+
 /* Chi-square of n images: sum over pixels of ((data - model) * inverr)^2,
  * FP32 terms with compensated FP32 block sums combined in FP64; out[i] for
  * image i of npix[i] pixels starting at offset off[i].  Replaces
@@ -396,8 +517,9 @@ const char* tb_version(void);
 
 /* ABI guard for bindings: writes sizeof(tb_mog_item), sizeof(tb_fft_item),
  * sizeof(tb_status), sizeof(tb_galaxy_src), sizeof(tb_fft_image),
- * sizeof(tb_scene_src), sizeof(tb_scene_image), sizeof(tb_scene_item) into
- * sizes[0..7] (host memory) and returns 8.  No reference counterpart
+ * sizeof(tb_scene_src), sizeof(tb_scene_image), sizeof(tb_scene_item),
+ * sizeof(tb_fit_source), sizeof(tb_fit_blob), sizeof(tb_fit_unit),
+ * sizeof(tb_fit_state) into sizes[0..11] (host memory) and returns 12.  No reference counterpart
  * (bindings check their struct layouts with it). */
 int tb_abi_sizes(int32_t* sizes);
 

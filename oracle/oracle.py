@@ -620,3 +620,117 @@ def lsq_update(A_cols, b, priors=None):
 def line_search_alphas():
     """Default step sizes of Optimizer.tryUpdates, tractor/optimize.py:426-428."""
     return np.append(2. ** np.arange(-10, 1), [np.sqrt(2.), 2.])
+
+
+# ---------------------------------------------------------------------------
+# Blob fitting (the batched form of Tractor.optimize_loop over several bands)
+# ---------------------------------------------------------------------------
+
+BLOB_NPAR = 9   # x, y, flux[3], log r_e, ee1, ee2, Sersic n
+
+
+def blob_source_mixture(theta, band, pamp, pmean, pvar, cdinv=None):
+    """PSF-convolved mixture of a SersicGalaxy (EllipseESoft shape,
+    NanoMaggies counts = flux with LinearPhotoCal(1)) in one band: the
+    profile (sersic.py:288-342), the shape (ellipses.py:165-263,
+    galaxy.py:659-669), the convolution (mixture_profiles.py:158-172).
+    Returns (amp x counts, mean, var)."""
+    cdinv = nullwcs_cdinv() if cdinv is None else cdinv
+    amp, var = sersic_profile(float(theta[8]))
+    T = cdinv @ ellipseE_basis(*ellipseESoft_to_E(theta[5], theta[6], theta[7]))
+    a2, v2 = sheared(amp, var, T)
+    mean = np.zeros((len(a2), 2)) + np.array([theta[0], theta[1]])
+    ca, cm, cv = convolve(a2, mean, v2, np.asarray(pamp, np.float64),
+                          np.asarray(pmean, np.float64), np.asarray(pvar, np.float64))
+    return ca * theta[2 + band], cm, cv
+
+
+def blob_model(params, rects, W, H, psf, n_bands):
+    """(n_bands, H, W) FP64 model of one blob: every source's grid over its
+    mask rectangle clipped to the image (c_gauss_2d_grid, mix.i:452-524),
+    summed (Tractor.getModelImage, engine.py:424-445)."""
+    mod = np.zeros((n_bands, H, W))
+    for k in range(n_bands):
+        pamp, pmean, pvar = psf[k]
+        for th, (x0, y0, w, h) in zip(params, rects):
+            a, m, v = blob_source_mixture(th, k, pamp, pmean, pvar)
+            X0, Y0 = max(x0, 0), max(y0, 0)
+            X1, Y1 = min(x0 + w, W), min(y0 + h, H)
+            if X1 <= X0 or Y1 <= Y0:
+                continue
+            mod[k, Y0:Y1, X0:X1] += mog_grid(X0, X1, Y0, Y1, 0., 0., a, m, v)
+    return mod
+
+
+def blob_normal_equations(params, rects, W, H, psf, n_bands, data, inverr, steps=None):
+    """A^T A, A^T r, chi^2 of one blob in FP64 with A = d model / d params *
+    inverr by central differences (fluxes exactly: the model is linear in
+    them) and r = (data - model) * inverr (lsqr_optimizer.py:328-520 builds
+    the same A and b)."""
+    params = np.asarray(params, np.float64)
+    n = len(params)
+    P = n * BLOB_NPAR
+    base = blob_model(params, rects, W, H, psf, n_bands)
+    r = ((data - base) * inverr).ravel()
+    cols = np.zeros((r.size, P))
+    h = np.array([1e-5, 1e-5, 0., 0., 0., 1e-6, 1e-6, 1e-6, 1e-6]) if steps is None else steps
+    for s in range(n):
+        for j in range(BLOB_NPAR):
+            if 2 <= j < 5:
+                if j - 2 >= n_bands:
+                    continue
+                one = params[s:s + 1].copy()
+                one[0, 2:5] = 0.
+                one[0, j] = 1.
+                d = blob_model(one, rects[s:s + 1], W, H, psf, n_bands)
+            else:
+                pp, pm = params.copy(), params.copy()
+                pp[s, j] += h[j]
+                pm[s, j] -= h[j]
+                d = (blob_model(pp[s:s + 1], rects[s:s + 1], W, H, psf, n_bands) -
+                     blob_model(pm[s:s + 1], rects[s:s + 1], W, H, psf, n_bands)) / (2 * h[j])
+            cols[:, s * BLOB_NPAR + j] = (d * inverr).ravel()
+    return cols.T @ cols, cols.T @ r, float(r @ r)
+
+
+def blob_fit(params0, rects, W, Himg, psf, n_bands, data, inverr, tol=1e-12, max_iter=60,
+             lower_n=0.29, upper_n=6.3):
+    """FP64 damped Gauss-Newton fit of one blob to a tight optimum (for
+    parity: the optimum is a property of the objective, not of the path),
+    stopping when the predicted log-likelihood gain of the next step is below
+    tol.  Returns (params, H at the optimum, held), `held` marking the
+    parameters held at a bound."""
+    p = np.array(params0, np.float64)
+    H, g, c2 = blob_normal_equations(p, rects, W, Himg, psf, n_bands, data, inverr)
+    lam = 1e-3
+    for _ in range(max_iter):
+        d = np.sqrt(np.maximum(np.diag(H), 0.))
+        live = d > 0
+        # a Sersic index at a bound that the gradient pushes against is held
+        # (projected step: the bound-constrained optimum)
+        nidx = np.arange(len(p)) * BLOB_NPAR + 8
+        held = ((p[:, 8] >= upper_n) & (g[nidx] > 0)) | ((p[:, 8] <= lower_n) & (g[nidx] < 0))
+        live[nidx[held]] = False
+        Hs = H[np.ix_(live, live)] / np.outer(d[live], d[live]) + lam * np.eye(live.sum())
+        x = np.zeros(len(d))
+        xs = np.linalg.solve(Hs, g[live] / d[live])
+        x[live] = xs / d[live]
+        # predicted log-likelihood gain of the damped step
+        pred = 0.5 * (xs @ (g[live] / d[live]) + lam * xs @ xs)
+        if pred < tol and lam <= 1.:
+            break
+        trial = p + x.reshape(p.shape)
+        trial[:, 8] = np.clip(trial[:, 8], lower_n, upper_n)
+        H2, g2, c22 = blob_normal_equations(trial, rects, W, Himg, psf, n_bands, data,
+                                            inverr)
+        if c22 <= c2:
+            p, H, g, c2 = trial, H2, g2, c22
+            lam = max(lam * 0.3, 1e-12)
+        else:
+            lam *= 10.
+            if lam > 1e12:
+                break
+    nidx = np.arange(len(p)) * BLOB_NPAR + 8
+    held = np.zeros(p.size, bool)
+    held[nidx] = ((p[:, 8] >= upper_n) & (g[nidx] > 0)) | ((p[:, 8] <= lower_n) & (g[nidx] < 0))
+    return p, H, held

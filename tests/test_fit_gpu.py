@@ -1,0 +1,134 @@
+"""Batched blob fitting (tb_fit_prep / tb_fit_pass / tb_fit_step) against the
+oracle's FP64 blob model, its central-difference normal equations and its
+tightly converged FP64 fit.
+
+Tolerances: A^T A and A^T r within 1e-4 of their natural scales
+(sqrt(H_ii H_jj), sqrt(H_ii chi^2)); chi^2 within 1e-5 relative; fitted
+parameters within 1e-3 sigma of the FP64 optimum (sigma from the FP64
+inverse Fisher matrix)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_blobs(oracle, seed, n_blobs=3, flux=(300., 4000.)):
+    from tractor_b200 import fit, _lib
+    rng = np.random.default_rng(seed)
+    w = fit.blob_workload(n_blobs, rng, side_range=(40, 64), mean_src=2, max_src=3,
+                          flux_range=flux)
+    # Sersic indices in the middle of the spline ranges (central differences
+    # in the oracle must not straddle a range edge)
+    ns = np.array([0.8, 1.2, 2.2, 4.5, 5.5])
+    w['truth'][:, 8] = ns[rng.integers(0, len(ns), len(w['truth']))]
+    w['start'][:, 8] = w['truth'][:, 8] + rng.uniform(-0.05, 0.05, len(w['truth']))
+    datas, inverrs = [], []
+    for b in range(n_blobs):
+        s0, s1 = w['blob_src'][b], w['blob_src'][b + 1]
+        W, H = w['sides'][b]
+        rects = [tuple(int(v) for v in (r['x0'], r['y0'], r['w'], r['h']))
+                 for r in w['sources'][s0:s1]]
+        mod = oracle.blob_model(w['truth'][s0:s1], rects, W, H, w['psf'][b], 3)
+        sig = w['noise'][b][:, None, None]
+        datas.append((mod + sig * rng.normal(size=mod.shape)).astype(np.float32))
+        inverrs.append(np.broadcast_to(1. / sig, mod.shape).astype(np.float32))
+    return w, datas, inverrs
+
+
+def _fitter(w, datas, inverrs):
+    import torch
+    from tractor_b200 import fit
+    data = torch.from_numpy(np.concatenate([d.ravel() for d in datas])).cuda()
+    inv = torch.from_numpy(np.concatenate([d.ravel() for d in inverrs])).cuda()
+    return fit.BlobFitter(w['blob_src'], w['sides'], w['psf'], w['sources'], w['start'], data,
+                          inv)
+
+
+def _blob_args(w, b):
+    s0, s1 = w['blob_src'][b], w['blob_src'][b + 1]
+    W, H = (int(v) for v in w['sides'][b])
+    rects = [tuple(int(v) for v in (r['x0'], r['y0'], r['w'], r['h']))
+             for r in w['sources'][s0:s1]]
+    return s0, s1, W, H, rects
+
+
+def test_normal_equations_match_oracle(tb, oracle):
+    """One pass at the starting parameters: the analytic FP32 derivative
+    columns reproduce the FP64 central-difference A^T A, A^T r, chi^2."""
+    w, datas, inverrs = _small_blobs(oracle, 1)
+    f = _fitter(w, datas, inverrs)
+    f.fit(max_iter=1, check_every=1, graph=False)
+    st = f.states()
+    for b in range(len(datas)):
+        s0, s1, W, H, rects = _blob_args(w, b)
+        Ho, go, c2o = oracle.blob_normal_equations(w['start'][s0:s1], rects, W, H, w['psf'][b], 3,
+                                                   datas[b].astype(np.float64),
+                                                   inverrs[b].astype(np.float64))
+        Hg, gg = f.normal_equations(b)
+        d = np.sqrt(np.diag(Ho))
+        scale = np.outer(d, d)
+        live = scale > 0
+        assert np.all(np.abs(Hg - Ho)[live] <= 1e-4 * scale[live]), b
+        assert np.all(Hg[~live] == 0)
+        assert np.all(np.abs(gg - go) <= 1e-4 * d * np.sqrt(c2o) + 1e-9), b
+        assert abs(st['chi2'][b] - c2o) <= 1e-5 * c2o, b
+
+
+def test_fit_converges_to_fp64_optimum(tb, oracle):
+    """From the same perturbed start, the batched FP32 fitter and the FP64
+    oracle fitter reach the same optimum within 1e-3 sigma."""
+    w, datas, inverrs = _small_blobs(oracle, 2)
+    f = _fitter(w, datas, inverrs)
+    f.fit(tol=1e-7, max_iter=80, check_every=4)
+    st = f.states()
+    assert np.all(st['status'] != 0), st['status']
+    got = f.result()
+    for b in range(len(datas)):
+        s0, s1, W, H, rects = _blob_args(w, b)
+        p, Hf, held = oracle.blob_fit(w['start'][s0:s1], rects, W, H, w['psf'][b], 3,
+                                      datas[b].astype(np.float64),
+                                      inverrs[b].astype(np.float64))
+        # sigma from the Fisher matrix of the free parameters; a parameter
+        # held at a bound must sit at the same bound
+        free = ~held & (np.diag(Hf) > 0)
+        sig = np.full(p.size, np.inf)
+        sig[free] = np.sqrt(np.diag(np.linalg.inv(Hf[np.ix_(free, free)])))
+        sig = sig.reshape(p.shape)
+        assert np.array_equal(got[s0:s1].ravel()[held], p.ravel()[held]), b
+        err = np.abs(got[s0:s1] - p) / sig
+        assert err.max() < 1e-3, (b, err.max(), np.unravel_index(err.argmax(), err.shape))
+
+
+def test_graph_and_eager_iterations_agree(tb, oracle):
+    """CUDA-graph replays of the iteration give the same result as eager
+    launches (same kernels, same order)."""
+    w, datas, inverrs = _small_blobs(oracle, 3)
+    f = _fitter(w, datas, inverrs)
+    f.fit(tol=1e-3, max_iter=24, check_every=4, graph=True, params0=w['start'])
+    a, sa = f.result().copy(), f.states().copy()
+    f.fit(tol=1e-3, max_iter=24, check_every=4, graph=False, params0=w['start'])
+    b, sb = f.result(), f.states()
+    assert np.array_equal(a, b)
+    assert np.array_equal(sa['iters'], sb['iters'])
+
+
+def test_many_blobs_fit_at_least_as_well_as_truth(tb):
+    """200 blobs of the full-size distribution (sides 192-512, Poisson(6)
+    sources, 3 bands): every blob stops, and the fitted chi^2 is no worse
+    than the chi^2 of the true parameters for nearly all of them."""
+    from tractor_b200 import fit
+    rng = np.random.default_rng(7)
+    w = fit.blob_workload(200, rng)
+    data, inv = fit.render_blobs(w, w['truth'], seed=11)
+    f = fit.BlobFitter(w['blob_src'], w['sides'], w['psf'], w['sources'], w['start'], data, inv)
+    f.fit(tol=1e-3, max_iter=60, check_every=4)
+    st = f.states()
+    assert np.all(st['status'] != 0)
+    assert np.mean(st['status'] == 1) > 0.95, np.bincount(st['status'])
+    fitted = st['chi2'].copy()
+    f.fit(max_iter=1, check_every=1, graph=False, params0=w['truth'])
+    truth = f.states()['chi2']
+    npix = np.diff(fit.pix_offsets(w['sides'], 3)).reshape(-1, 3).sum(axis=1)
+    assert np.all(np.abs(truth / npix - 1) < 0.05)          # noise model sanity
+    ok = fitted <= truth + 1.0
+    assert np.mean(ok) > 0.95, np.sort(fitted - truth)[-10:]

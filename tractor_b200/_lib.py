@@ -44,6 +44,20 @@ SCENE_ITEM = np.dtype([('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'), ('h', '<i4'),
                        ('c0', '<i4'), ('K', '<i4'), ('image', '<i4'), ('flag', '<i4'),
                        ('fx', '<f8'), ('fy', '<f8'), ('scale', '<f4'), ('floor', '<f4')])
 
+FIT_NPAR, FIT_MAX_BANDS, FIT_MAX_SRC, FIT_MAX_PSF = 9, 3, 32, 4
+FIT_SOURCE = np.dtype([('profile', '<i4'), ('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'),
+                       ('h', '<i4'), ('blob', '<i4')])
+FIT_BLOB = np.dtype([('n_src', '<i4'), ('src0', '<i4'), ('P', '<i4'), ('unit0', '<i4'),
+                     ('h_off', '<i8'), ('g_off', '<i8'), ('tile_off', '<i8'),
+                     ('n_active', '<i4'), ('n_tiles', '<i4')])
+FIT_UNIT = np.dtype([('blob', '<i4'), ('band', '<i4'), ('W', '<i4'), ('H', '<i4'),
+                     ('pix_off', '<i8'), ('psf_K', '<i4'), ('pad', '<i4'),
+                     ('psf_amp', '<f8', (4,)), ('psf_mean', '<f8', (8,)),
+                     ('psf_var', '<f8', (16,))])
+FIT_STATE = np.dtype([('chi2', '<f8'), ('dlnp', '<f8'), ('lambda', '<f8'), ('pred', '<f8'),
+                      ('iters', '<i4'),
+                      ('accepted', '<i4'), ('rejected', '<i4'), ('status', '<i4')])
+
 PROFILE_EXP, PROFILE_DEV, PROFILE_SERSIC, PROFILE_GAUSSIAN = 0, 1, 2, 3
 PROFILE_POINT, PROFILE_COMPOSITE = 4, 5
 SHAPE_ELLIPSE_E, SHAPE_ELLIPSE_ESOFT, SHAPE_RABPHI = 0, 1, 2
@@ -93,6 +107,12 @@ SIGNATURES = {
     'tb_galaxy_fft_prep': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _I32, _P, _P]),
     'tb_scene_prep': (_I32, [_P, _I32, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P]),
     'tb_scene_workspace': (_I32, [_I64, _I64, _P]),
+    'tb_fit_workspace': (_I32, [_I32, _I32, _P]),
+    'tb_fit_reset': (_I32, [_P, _I32, _D, _P]),
+    'tb_fit_prep': (_I32, [_P, _I32, _P, _I32, _P, _I32, _P, _P, _P, _P]),
+    'tb_fit_pass': (_I32, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32,
+                           _I32, _P, _P, _P]),
+    'tb_fit_step': (_I32, [_P, _I32, _I32, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _P]),
     'tb_scene_render': (_I32, [_P, _I32, _P, _I32, _I64, _I32, _P, _P, _P, _P, _I32, _P, _I64,
                                _I64, _P, _P]),
     'tb_version': (ctypes.c_char_p, []),
@@ -121,11 +141,12 @@ def load():
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
-    sizes = np.zeros(8, np.int32)
+    sizes = np.zeros(12, np.int32)
     lib.tb_abi_sizes(sizes.ctypes.data)
     want = (MOG_ITEM.itemsize, FFT_ITEM.itemsize, STATUS.itemsize, GALAXY_SRC.itemsize,
             ctypes.sizeof(FftImage), SCENE_SRC.itemsize, SCENE_IMAGE.itemsize,
-            SCENE_ITEM.itemsize)
+            SCENE_ITEM.itemsize, FIT_SOURCE.itemsize, FIT_BLOB.itemsize, FIT_UNIT.itemsize,
+            FIT_STATE.itemsize)
     if tuple(int(s) for s in sizes) != want:
         raise ImportError('libtractor_b200.so struct layout %s != binding %s' %
                           (tuple(sizes), want))

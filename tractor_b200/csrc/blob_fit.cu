@@ -1,0 +1,922 @@
+// Batched blob fitting (sm_100a): Levenberg-Marquardt on many independent
+// blobs at once, each blob a few galaxies seen in several bands.  It is the
+// batched form of Tractor.optimize / optimize_loop with LsqrOptimizer
+// (tractor/lsqr_optimizer.py:280-326) over getDerivs + getChiImage
+// (tractor/engine.py:279-339, 455-473), with ConstrainedOptimizer's bounds and
+// maximum steps (tractor/constrained_optimizer.py:12-159).
+//
+// One iteration = three launches:
+//   tb_fit_prep  one warp per source: the profile mixture (exp / deV /
+//                Sersic) and its derivative with respect to the Sersic index,
+//                the pixel-space shape factor M = T T^T and its derivatives
+//                with respect to (log r_e, ee1, ee2) -- FP64 central
+//                differences of the exact FP64 maps (sersic.py:288-342,
+//                ellipses.py:165-263);
+//   tb_fit_pass  one CTA per (blob, band) image, 32 x 8 pixel tiles: the
+//                model (every source's PSF-convolved mixture, as
+//                galaxy.py:307-326) and the analytic derivative columns
+//                (position, flux, shape, index), weighted by inverr, staged
+//                in shared memory; per tile A^T A, A^T r and r^T r added into
+//                buffers the CTA owns (no atomics);
+//   tb_fit_step  one CTA per blob: sums the band partials, accepts or
+//                rejects the trial parameters, solves the Marquardt-damped
+//                normal equations by FP64 Cholesky with one refinement step,
+//                limits the step (bounds, maximum steps) and writes the next
+//                trial parameters.
+#include "profile_eval.cuh"
+
+namespace {
+
+constexpr int kPrepThreads = 128;      // 4 sources per block
+constexpr int kMaxGalK = 10;           // galaxy components of one source
+constexpr int kThreads = 256;          // pass CTA = one 32 x 8 tile, one pixel per thread
+constexpr int kTileW = 32;
+constexpr int kTileH = 8;
+constexpr int kCols = 7;               // columns per (source, band): x y flux logre ee1 ee2 n
+constexpr int kG = 5;                  // sources per shared-memory column group
+constexpr int kLd = kThreads + 1;      // padded column stride (floats)
+constexpr int kStageMax = kG * kMaxGalK * TB_FIT_MAX_PSF;
+constexpr double kHn = 1e-5;           // central-difference step in n
+constexpr double kHs = 1e-6;           // central-difference step in shape parameters
+
+constexpr int kCompStride = kMaxGalK * TB_FIT_MAX_PSF;   // component slots per (source, band)
+
+// Per-source summary written by tb_fit_prep.
+struct SrcTab {
+    double flux[TB_FIT_MAX_BANDS];
+    int32_t K[TB_FIT_MAX_BANDS];   // components in each band (galaxy x PSF)
+    int32_t ok;
+};
+
+// One PSF-convolved component of a (source, band), written by tb_fit_prep:
+// value, position and shape-derivative coefficients, the 1/2 of dN/dC
+// folded in.  The mean stays FP64 (absolute pixels); the pass makes it
+// tile-relative.
+struct FitC {
+    double mx, my;
+    float qxx, qxy, qyy;      // exponent, log2 units
+    float ixx, ixy, iyy;      // C^-1
+    float s;                  // unit-flux amplitude a / (2 pi sqrt det)
+    float sn;                 // d a / d n / (2 pi sqrt det)
+    float fl;                 // exponent floor, log2 units
+    float dxx[4], dxy2[4], dyy[4], t[4];  // 1/2 dC (xy doubled), 1/2 tr(C^-1 dC)
+    int32_t pad[3];
+};
+
+// The same, staged in shared memory for one tile (FP32 tile-relative mean).
+struct FitS {
+    float mx, my;
+    float qxx, qxy, qyy, ixx, ixy, iyy, s, sn, fl;
+    float dxx[4], dxy2[4], dyy[4], t[4];
+    int32_t rec;              // source position in the tile's list
+};
+
+// ---------------------------------------------------------------------------
+// prep
+// ---------------------------------------------------------------------------
+
+// Sersic mixture of range r at index nn with the core present or not, lane l
+// holding component l (the spline evaluation of warp_profile without the
+// range lookup, so that both sides of a central difference use the same
+// components).
+__device__ int sersic_fixed(const tb_profile_tables& T, int r, double nn, bool core_on, int lane,
+                            double& a, double& v) {
+    const int Kr = T.range_info[4 * r], sa = T.range_info[4 * r + 1];
+    const int sv = T.range_info[4 * r + 2];
+    a = 0.0;
+    v = 0.0;
+    if (lane < Kr) {
+        a = tb::bspline(T, sa + lane, nn);
+        v = exp(tb::bspline(T, sv + lane, nn));
+    }
+    a /= tb::lane_sum(a, Kr);
+    if (!core_on) return Kr;
+    const double core = tb::bspline(T, T.core_spline, nn);
+    a *= (1.0 - core) / tb::lane_sum(a, Kr);
+    if (lane == Kr) { a = core; v = 0.0; }
+    return Kr + 1;
+}
+
+__device__ void shape_M(const double* cd, double s0, double s1, double s2, double M[3]) {
+    double G[4], re;
+    tb::shape_basis(TB_SHAPE_ELLIPSE_ESOFT, s0, s1, s2, G, re);
+    tb::pixel_factor(cd, G, M[0], M[1], M[2]);
+}
+
+__global__ void __launch_bounds__(kPrepThreads)
+fit_prep_kernel(const tb_fit_source* __restrict__ srcs, int n, const double* __restrict__ params,
+                int n_bands, const tb_fit_unit* __restrict__ units, int n_units,
+                tb_profile_tables Tg, double cd0, double cd1, double cd2, double cd3,
+                SrcTab* __restrict__ tab, FitC* __restrict__ comps) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const tb_profile_tables T = tb::stage_tables(Tg, smem_raw);
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (kPrepThreads / 32) + (threadIdx.x >> 5);
+    if (i >= n) return;
+    const tb_fit_source s = srcs[i];
+    const double* p = params + (int64_t)i * TB_FIT_NPAR;
+    const double cd[4] = {cd0, cd1, cd2, cd3};
+    int ok = s.blob >= 0 && (int64_t)(s.blob + 1) * n_bands <= n_units;
+    double a = 0.0, v = 0.0, da = 0.0, dv = 0.0;
+    int K = 0;
+    if (s.profile == TB_PROFILE_SERSIC) {
+        double nn = p[8];
+        const double lowest = T.range_lohi[0], highest = T.range_lohi[2 * T.n_ranges - 1];
+        int r = -1;
+        bool clamped = false;
+        if (nn <= lowest) { r = 0; nn = lowest; clamped = true; }
+        else if (nn >= highest) { r = T.n_ranges - 1; nn = highest; clamped = true; }
+        else {
+            for (int q = 0; q < T.n_ranges; q++)
+                if (T.range_lohi[2 * q] <= nn && nn < T.range_lohi[2 * q + 1]) { r = q; break; }
+        }
+        if (r < 0 || T.range_info[4 * r] + 1 > kMaxGalK) {
+            ok = 0;
+        } else {
+            const bool core = nn > 1.0;
+            K = sersic_fixed(T, r, nn, core, lane, a, v);
+            if (!clamped) {
+                double ap, vp, am, vm;
+                sersic_fixed(T, r, nn + kHn, core, lane, ap, vp);
+                sersic_fixed(T, r, nn - kHn, core, lane, am, vm);
+                da = (ap - am) / (2.0 * kHn);
+                dv = (vp - vm) / (2.0 * kHn);
+            }
+            // components sorted by variance (sersic.py:338-341); the sort is
+            // a permutation of lanes, kept fixed for the derivative
+            const int rank = tb::variance_rank(v, K, lane);
+            double a2 = 0.0, v2 = 0.0, da2 = 0.0, dv2 = 0.0;
+            for (int j = 0; j < K; j++) {
+                const int rj = __shfl_sync(0xffffffffu, rank, j);
+                const double aj = __shfl_sync(0xffffffffu, a, j);
+                const double vj = __shfl_sync(0xffffffffu, v, j);
+                const double daj = __shfl_sync(0xffffffffu, da, j);
+                const double dvj = __shfl_sync(0xffffffffu, dv, j);
+                if (rj == lane) { a2 = aj; v2 = vj; da2 = daj; dv2 = dvj; }
+            }
+            a = a2; v = v2; da = da2; dv = dv2;
+        }
+    } else if (s.profile == TB_PROFILE_EXP || s.profile == TB_PROFILE_DEV) {
+        K = tb::warp_profile(T, s.profile, 0.0, lane, kMaxGalK, a, v);
+        if (K < 0) { ok = 0; K = 0; }
+    } else if (s.profile == TB_PROFILE_POINT) {
+        K = 1;
+        a = lane == 0 ? 1.0 : 0.0;
+    } else {
+        ok = 0;
+    }
+    // shape factor and its derivatives (every lane, redundantly)
+    double M[3] = {0.0, 0.0, 0.0};
+    double dM[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    if (s.profile != TB_PROFILE_POINT) {
+        const double* sh = p + 5;
+        shape_M(cd, sh[0], sh[1], sh[2], M);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            double hp[3] = {sh[0], sh[1], sh[2]}, hm[3] = {sh[0], sh[1], sh[2]};
+            hp[j] += kHs;
+            hm[j] -= kHs;
+            double Mp[3], Mm[3];
+            shape_M(cd, hp[0], hp[1], hp[2], Mp);
+            shape_M(cd, hm[0], hm[1], hm[2], Mm);
+#pragma unroll
+            for (int q = 0; q < 3; q++) dM[j][q] = (Mp[q] - Mm[q]) / (2.0 * kHs);
+        }
+    }
+    bool fin = isfinite(p[0]) && isfinite(p[1]);
+    for (int q = 0; q < 3; q++) fin = fin && isfinite(M[q]);
+    ok = ok && fin;
+    // components per band: PSF component p (outer) x galaxy component gi
+    // (inner), mixture_profiles.py:158-172
+    int Kb[TB_FIT_MAX_BANDS] = {0, 0, 0};
+    for (int bd = 0; bd < n_bands; bd++) {
+        const tb_fit_unit* u = ok ? units + (int64_t)s.blob * n_bands + bd : units;
+        const int Kp = u->psf_K;
+        if (Kp < 1 || Kp > TB_FIT_MAX_PSF) ok = 0;
+        const int Kt = ok ? K * Kp : 0;
+        Kb[bd] = Kt;
+        for (int k0 = 0; k0 < kCompStride; k0 += 32) {
+            const int k = k0 + lane;
+            const int gi = (Kt > 0 && k < Kt) ? k % K : 0;
+            const int pp = (Kt > 0 && k < Kt) ? k / K : 0;
+            const double ag = __shfl_sync(0xffffffffu, a, gi);
+            const double vg = __shfl_sync(0xffffffffu, v, gi);
+            const double dag = __shfl_sync(0xffffffffu, da, gi);
+            const double dvg = __shfl_sync(0xffffffffu, dv, gi);
+            if (k >= Kt) continue;
+            const double C00 = vg * M[0] + u->psf_var[4 * pp];
+            const double C01 = vg * M[1] + 0.5 * (u->psf_var[4 * pp + 1] + u->psf_var[4 * pp + 2]);
+            const double C11 = vg * M[2] + u->psf_var[4 * pp + 3];
+            const double det = C00 * C11 - C01 * C01;
+            const double i00 = C11 / det, i01 = -C01 / det, i11 = C00 / det;
+            const double norm = 1.0 / (2.0 * TB_PI * sqrt(det));
+            FitC c;
+            c.mx = p[0] + u->psf_mean[2 * pp];
+            c.my = p[1] + u->psf_mean[2 * pp + 1];
+            c.qxx = (float)(-0.5 * TB_LOG2E * i00);
+            c.qxy = (float)(-TB_LOG2E * i01);
+            c.qyy = (float)(-0.5 * TB_LOG2E * i11);
+            c.ixx = (float)i00;
+            c.ixy = (float)i01;
+            c.iyy = (float)i11;
+            c.s = (float)(ag * u->psf_amp[pp] * norm);
+            c.sn = (float)(dag * u->psf_amp[pp] * norm);
+            c.fl = (float)(-50.0 * TB_LOG2E);
+            // dC / d(logre, ee1, ee2) = v dM; dC / dn = dv M
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                double d0, d1, d2;
+                if (j < 3) { d0 = vg * dM[j][0]; d1 = vg * dM[j][1]; d2 = vg * dM[j][2]; }
+                else { d0 = dvg * M[0]; d1 = dvg * M[1]; d2 = dvg * M[2]; }
+                c.dxx[j] = (float)(0.5 * d0);
+                c.dxy2[j] = (float)d1;
+                c.dyy[j] = (float)(0.5 * d2);
+                c.t[j] = (float)(0.5 * (i00 * d0 + 2.0 * i01 * d1 + i11 * d2));
+            }
+            c.pad[0] = c.pad[1] = c.pad[2] = 0;
+            const bool good = det > 0.0 && isfinite(norm);
+            if (!good) ok = 0;
+            comps[((int64_t)i * n_bands + bd) * kCompStride + k] = c;
+        }
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    if (lane == 0) {
+        SrcTab t;
+        for (int bd = 0; bd < TB_FIT_MAX_BANDS; bd++) {
+            t.flux[bd] = bd < n_bands ? p[2 + bd] : 0.0;
+            t.K[bd] = bd < n_bands ? Kb[bd] : 0;
+        }
+        t.ok = ok;
+        tab[i] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pass
+// ---------------------------------------------------------------------------
+
+struct TileRec {
+    int32_t x0, x1, y0, y1;   // rectangle, tile-relative, clipped to the tile
+    float counts;
+    int32_t src;              // source index within the blob
+    int32_t K;                // components (galaxy x PSF)
+    int32_t pad;
+};
+
+struct PassSmem {
+    float A[2][kG * kCols][kLd];   // two column groups
+    FitS comps[kStageMax];
+    TileRec recs[TB_FIT_MAX_SRC];
+    float r[kThreads];
+    double red[kThreads / 32];
+    int64_t slot;
+    int nrec;
+    int skip;
+};
+
+// Evaluates sources [q0, q0 + nq) of the tile list at this thread's pixel.
+// kDeriv: writes the 7 weighted columns of each source into `A` (column
+// 7 (q - q0) + c) and returns the model; otherwise returns the model only.
+template <bool kDeriv>
+__device__ float eval_group(PassSmem& sm, const FitC* __restrict__ gcomps, int src0, int band,
+                            int n_bands, int q0, int nq, int ox, int oy, float w,
+                            float (*A)[kLd]) {
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    // zero this group's columns (each thread its own pixel)
+    if (kDeriv) {
+        for (int c = 0; c < nq * kCols; c++) A[c][tid] = 0.f;
+    }
+    // stage components: record-major, PSF component outer, galaxy inner
+    int total = 0;
+    for (int q = q0; q < q0 + nq; q++) total += sm.recs[q].K;
+    __syncthreads();   // previous users of comps / A are done
+    for (int g = tid; g < total; g += kThreads) {
+        int q = q0, k = g;
+        while (k >= sm.recs[q].K) { k -= sm.recs[q].K; q++; }
+        const FitC& c = gcomps[((int64_t)(src0 + sm.recs[q].src) * n_bands + band) * kCompStride + k];
+        FitS f;
+        f.mx = (float)(c.mx - (double)ox);
+        f.my = (float)(c.my - (double)oy);
+        f.qxx = c.qxx; f.qxy = c.qxy; f.qyy = c.qyy;
+        f.ixx = c.ixx; f.ixy = c.ixy; f.iyy = c.iyy;
+        f.s = c.s; f.sn = c.sn; f.fl = c.fl;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            f.dxx[j] = c.dxx[j]; f.dxy2[j] = c.dxy2[j]; f.dyy[j] = c.dyy[j]; f.t[j] = c.t[j];
+        }
+        f.rec = q;
+        sm.comps[g] = f;
+    }
+    __syncthreads();
+    const float xf = (float)lane, yf = (float)warp;
+    float model = 0.f;
+    float m = 0.f, jx = 0.f, jy = 0.f, j0 = 0.f, j1 = 0.f, j2 = 0.f, jn = 0.f;
+    int cur = -1;
+    for (int g = 0; g <= total; g++) {
+        const int rec = g < total ? sm.comps[g].rec : -2;
+        if (rec != cur) {
+            if (cur >= 0) {
+                // source `cur` done: add its patch inside its rectangle and
+                // write its weighted columns
+                const TileRec& R = sm.recs[cur];
+                const bool in = lane >= R.x0 && lane < R.x1 && warp >= R.y0 && warp < R.y1;
+                const float cnt = R.counts;
+                model += in ? cnt * m : 0.f;
+                if (kDeriv) {
+                    const float cw = in ? cnt * w : 0.f;
+                    float* col = &A[(cur - q0) * kCols][tid];
+                    col[0 * kLd] = cw * jx;
+                    col[1 * kLd] = cw * jy;
+                    col[2 * kLd] = in ? w * m : 0.f;
+                    col[3 * kLd] = cw * j0;
+                    col[4 * kLd] = cw * j1;
+                    col[5 * kLd] = cw * j2;
+                    col[6 * kLd] = cw * jn;
+                }
+            }
+            if (g == total) break;
+            cur = rec;
+            m = jx = jy = j0 = j1 = j2 = jn = 0.f;
+        }
+        const FitS& c = sm.comps[g];
+        const float dx = xf - c.mx, dy = yf - c.my;
+        const float e = fmaf(dx, fmaf(c.qxx, dx, c.qxy * dy), c.qyy * dy * dy);
+        const float E = (e >= c.fl) ? tb::ex2(e) : 0.f;
+        const float val = c.s * E;
+        m += val;
+        if (kDeriv) {
+            const float ux = fmaf(c.ixx, dx, c.ixy * dy);
+            const float uy = fmaf(c.ixy, dx, c.iyy * dy);
+            jx = fmaf(val, ux, jx);
+            jy = fmaf(val, uy, jy);
+            const float pxx = ux * ux, pxy = ux * uy, pyy = uy * uy;
+            j0 = fmaf(val, fmaf(c.dxx[0], pxx, fmaf(c.dxy2[0], pxy, fmaf(c.dyy[0], pyy, -c.t[0]))), j0);
+            j1 = fmaf(val, fmaf(c.dxx[1], pxx, fmaf(c.dxy2[1], pxy, fmaf(c.dyy[1], pyy, -c.t[1]))), j1);
+            j2 = fmaf(val, fmaf(c.dxx[2], pxx, fmaf(c.dxy2[2], pxy, fmaf(c.dyy[2], pyy, -c.t[2]))), j2);
+            jn = fmaf(val, fmaf(c.dxx[3], pxx, fmaf(c.dxy2[3], pxy, fmaf(c.dyy[3], pyy, -c.t[3]))), jn);
+            jn = fmaf(c.sn, E, jn);
+        }
+    }
+    __syncthreads();   // columns complete
+    return model;
+}
+
+__device__ __forceinline__ int col_of(int src, int c, int band, int n_bands) {
+    // parameter slots per source: x, y, flux[3], logre, ee1, ee2, n
+    (void)n_bands;
+    const int off = c < 2 ? c : (c == 2 ? 2 + band : c + 2);
+    return src * TB_FIT_NPAR + off;
+}
+
+// Adds A_a^T A_b (columns of groups a and b) into the owned H block: each
+// warp takes 2 x 2 blocks of column pairs and splits the tile's pixels over
+// its lanes (conflict-free consecutive shared-memory reads), then reduces.
+__device__ void add_block(PassSmem& sm, float (*Aa)[kLd], int qa0, int na, float (*Ab)[kLd],
+                          int qb0, int nb, bool diag, double* H, int P, int band, int n_bands) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ca = na * kCols, cb = nb * kCols;
+    const int ba = (ca + 1) / 2, bb = (cb + 1) / 2;
+    for (int e = warp; e < ba * bb; e += kThreads / 32) {
+        const int i = (e / bb) * 2, j = (e % bb) * 2;
+        if (diag && j + 1 < i) continue;   // upper triangle of 2 x 2 blocks (warp-uniform)
+        const int i1 = min(i + 1, ca - 1), j1 = min(j + 1, cb - 1);
+        float s00 = 0.f, s01 = 0.f, s10 = 0.f, s11 = 0.f;
+#pragma unroll
+        for (int p = lane; p < kThreads; p += 32) {
+            const float x0 = Aa[i][p], x1 = Aa[i1][p], y0 = Ab[j][p], y1 = Ab[j1][p];
+            s00 = fmaf(x0, y0, s00);
+            s01 = fmaf(x0, y1, s01);
+            s10 = fmaf(x1, y0, s10);
+            s11 = fmaf(x1, y1, s11);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s00 += __shfl_xor_sync(0xffffffffu, s00, o);
+            s01 += __shfl_xor_sync(0xffffffffu, s01, o);
+            s10 += __shfl_xor_sync(0xffffffffu, s10, o);
+            s11 += __shfl_xor_sync(0xffffffffu, s11, o);
+        }
+        if (lane < 4) {
+            const int di = lane >> 1, dj = lane & 1;
+            const int ii = i + di, jj = j + dj;
+            if (ii < ca && jj < cb && !(diag && jj < ii)) {
+                const float v = di == 0 ? (dj == 0 ? s00 : s01) : (dj == 0 ? s10 : s11);
+                const int ga = col_of(sm.recs[qa0 + ii / kCols].src, ii % kCols, band, n_bands);
+                const int gb = col_of(sm.recs[qb0 + jj / kCols].src, jj % kCols, band, n_bands);
+                // upper triangle in global parameter order
+                const int r = min(ga, gb), c = max(ga, gb);
+                H[(int64_t)r * P + c] += (double)v;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// A^T r of one group into the owned g vector (one warp per column).
+__device__ void add_grad(PassSmem& sm, float (*A)[kLd], int q0, int nq, double* g, int band,
+                         int n_bands) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = warp; c < nq * kCols; c += kThreads / 32) {
+        float s = 0.f;
+        for (int p = lane; p < kThreads; p += 32) s = fmaf(A[c][p], sm.r[p], s);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) g[col_of(sm.recs[q0 + c / kCols].src, c % kCols, band, n_bands)] += (double)s;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kThreads)
+fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict__ order,
+                int n_units, const tb_fit_blob* __restrict__ blobs,
+                const tb_fit_source* __restrict__ srcs, const SrcTab* __restrict__ tab,
+                const FitC* __restrict__ gcomps, const float* __restrict__ data,
+                const float* __restrict__ inverr, double* __restrict__ hbuf,
+                double* __restrict__ gbuf, double* __restrict__ chi2_part,
+                const tb_fit_state* __restrict__ state, int n_bands,
+                const int32_t* __restrict__ tiles, double* __restrict__ chi2_const, int mode,
+                int32_t* counter, tb_status* st) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PassSmem& sm = *reinterpret_cast<PassSmem*>(smem_raw);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    for (;;) {
+        const int64_t oi = tb::next_unit(counter, &sm.slot);
+        if (oi >= n_units) break;
+        const int ui = order[oi];
+        if (ui < 0 || ui >= n_units) {
+            if (tid == 0) tb::report(st, TB_STATUS_BAD_ITEM, (int)oi, ui);
+            continue;
+        }
+        const tb_fit_unit& u = units[ui];
+        const tb_fit_blob b = blobs[u.blob];
+        if (mode == 0 && state[u.blob].status != 0) continue;   // converged or stopped
+        const int P = b.P;
+        const int nsrc = b.n_src;
+        double* H = hbuf + b.h_off + (int64_t)u.band * P * P;
+        double* g = gbuf + b.g_off + (int64_t)u.band * P;
+        if (mode == 0) {
+            for (int e = tid; e < P * P; e += kThreads) H[e] = 0.0;
+            for (int e = tid; e < P; e += kThreads) g[e] = 0.0;
+        }
+        if (tid == 0) {
+            int bad = nsrc > TB_FIT_MAX_SRC || P != nsrc * TB_FIT_NPAR || u.psf_K < 1 ||
+                      u.psf_K > TB_FIT_MAX_PSF || u.band >= n_bands;
+            for (int s2 = 0; s2 < nsrc && !bad; s2++) bad = !tab[b.src0 + s2].ok;
+            sm.skip = bad;
+            if (bad) tb::report(st, TB_STATUS_BAD_ITEM, ui, nsrc);
+        }
+        __syncthreads();
+        if (sm.skip) {
+            if (tid == 0) {
+                if (mode == 0) chi2_part[b.unit0 + u.band] = INFINITY;
+                else chi2_const[b.unit0 + u.band] = INFINITY;
+            }
+            continue;
+        }
+        double chi2 = 0.0;
+        // mode 0: the tiles some source's mask reaches; mode 1: the others
+        // (their chi^2 does not depend on the parameters)
+        const int n_t = mode == 0 ? b.n_active : b.n_tiles - b.n_active;
+        const int32_t* tl = tiles + b.tile_off + (mode == 0 ? 0 : b.n_active);
+        // this thread's pixel of tile t (0 outside the image)
+        auto load_px = [&](int t, float& d, float& w) {
+            d = 0.f;
+            w = 0.f;
+            if (t >= n_t) return;
+            const int px = (tl[t] & 0xffff) * kTileW + lane, py = (tl[t] >> 16) * kTileH + warp;
+            if (px < u.W && py < u.H) {
+                const int64_t pix = u.pix_off + (int64_t)py * u.W + px;
+                d = data[pix];
+                w = inverr[pix];
+            }
+        };
+        float d_next, w_next;
+        load_px(0, d_next, w_next);
+        for (int t = 0; t < n_t; t++) {
+            const int ox = (tl[t] & 0xffff) * kTileW, oy = (tl[t] >> 16) * kTileH;
+            const float d = d_next, w = w_next;
+            load_px(t + 1, d_next, w_next);   // prefetch the next tile's pixel
+            // sources whose rectangle meets this tile (source order)
+            if (warp == 0) {
+                bool hit = false;
+                tb_fit_source fs;
+                if (lane < nsrc) {
+                    fs = srcs[b.src0 + lane];
+                    hit = fs.x0 < ox + kTileW && fs.x0 + fs.w > ox && fs.y0 < oy + kTileH &&
+                          fs.y0 + fs.h > oy && fs.w > 0 && fs.h > 0;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, hit);
+                if (hit) {
+                    const int q = __popc(bal & ((1u << lane) - 1u));
+                    TileRec R;
+                    R.x0 = max(fs.x0 - ox, 0);
+                    R.x1 = min(fs.x0 + fs.w - ox, kTileW);
+                    R.y0 = max(fs.y0 - oy, 0);
+                    R.y1 = min(fs.y0 + fs.h - oy, kTileH);
+                    const SrcTab& S = tab[b.src0 + lane];
+                    R.counts = (float)S.flux[u.band];
+                    R.src = lane;
+                    R.K = S.K[u.band];
+                    R.pad = 0;
+                    sm.recs[q] = R;
+                }
+                if (lane == 0) sm.nrec = __popc(bal);
+            }
+            __syncthreads();
+            const int R = sm.nrec;
+            if (R == 0) {
+                const float rr = d * w;
+                chi2 += (double)(rr * rr);
+                __syncthreads();
+                continue;
+            }
+            const int ngroups = (R + kG - 1) / kG;
+            float model;
+            if (ngroups == 1) {
+                model = eval_group<true>(sm, gcomps, b.src0, u.band, n_bands, 0, R, ox, oy, w,
+                                         sm.A[0]);
+            } else {
+                model = 0.f;
+                for (int q0 = 0; q0 < R; q0 += kG)
+                    model += eval_group<false>(sm, gcomps, b.src0, u.band, n_bands, q0,
+                                               min(kG, R - q0), ox, oy, w, sm.A[0]);
+            }
+            const float rr = (d - model) * w;
+            chi2 += (double)(rr * rr);
+            sm.r[tid] = rr;
+            __syncthreads();
+            for (int ga = 0; ga < ngroups; ga++) {
+                const int qa = ga * kG, na = min(kG, R - qa);
+                if (ngroups > 1)
+                    eval_group<true>(sm, gcomps, b.src0, u.band, n_bands, qa, na, ox, oy, w,
+                                     sm.A[0]);
+                add_grad(sm, sm.A[0], qa, na, g, u.band, n_bands);
+                add_block(sm, sm.A[0], qa, na, sm.A[0], qa, na, true, H, P, u.band, n_bands);
+                for (int gb = ga + 1; gb < ngroups; gb++) {
+                    const int qb = gb * kG, nb = min(kG, R - qb);
+                    eval_group<true>(sm, gcomps, b.src0, u.band, n_bands, qb, nb, ox, oy, w,
+                                     sm.A[1]);
+                    add_block(sm, sm.A[0], qa, na, sm.A[1], qb, nb, false, H, P, u.band, n_bands);
+                }
+            }
+        }
+        // chi^2 of the unit: fixed-order block reduction
+        for (int o = 16; o > 0; o >>= 1) chi2 += __shfl_xor_sync(0xffffffffu, chi2, o);
+        if (lane == 0) sm.red[warp] = chi2;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w2 = 0; w2 < kThreads / 32; w2++) s += sm.red[w2];
+            if (mode == 0) chi2_part[b.unit0 + u.band] = s + chi2_const[b.unit0 + u.band];
+            else chi2_const[b.unit0 + u.band] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// step
+// ---------------------------------------------------------------------------
+
+constexpr int kStepThreads = 256;
+
+__device__ double max_step(int off) {
+    // PixPos [1, 1] (wcs.py:384), fluxes unlimited, EllipseESoft inherits
+    // EllipseE's [1, 0.1, 0.1] (ellipses.py:48), SersicIndex 0.1 (sersic.py:352)
+    switch (off) {
+        case 0: case 1: case 5: return 1.0;
+        case 6: case 7: case 8: return 0.1;
+        default: return 0.0;   // none
+    }
+}
+
+__global__ void __launch_bounds__(kStepThreads)
+fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
+                const tb_fit_source* __restrict__ srcs, double* __restrict__ params,
+                double* __restrict__ trial, double* __restrict__ hbuf, double* __restrict__ gbuf,
+                const double* __restrict__ chi2_part, tb_fit_state* __restrict__ state,
+                double tol, int max_iter) {
+    __shared__ double dsc[TB_FIT_MAX_SRC * TB_FIT_NPAR];
+    __shared__ double y[TB_FIT_MAX_SRC * TB_FIT_NPAR];
+    __shared__ double xs[TB_FIT_MAX_SRC * TB_FIT_NPAR];
+    __shared__ double red[kStepThreads / 32];
+    __shared__ int s_accept, s_active, s_bad;
+    __shared__ double s_lambda, s_scale;
+    const int bi = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (bi >= n_blobs) return;
+    const tb_fit_blob b = blobs[bi];
+    tb_fit_state& S = state[bi];
+    const int status0 = S.status;
+    __syncthreads();   // every thread has read the status before thread 0 updates it
+    if (status0 != 0) return;
+    const int P = b.P;
+    double* Hp = hbuf + b.h_off;                        // band partials
+    double* Ha = Hp + (int64_t)n_bands * P * P;         // accepted H
+    double* L = Ha + (int64_t)P * P;                    // Cholesky factor
+    double* gp = gbuf + b.g_off;
+    double* ga = gp + (int64_t)n_bands * P;
+    double* pa = params + (int64_t)b.src0 * TB_FIT_NPAR;
+    double* pt = trial + (int64_t)b.src0 * TB_FIT_NPAR;
+
+    if (tid == 0) {
+        double c2 = 0.0;
+        for (int k = 0; k < n_bands; k++) c2 += chi2_part[b.unit0 + k];
+        const bool first = S.accepted == 0;
+        const bool acc = isfinite(c2) && (first || c2 < S.chi2);
+        int status = 0;
+        if (acc) {
+            S.dlnp = first ? INFINITY : 0.5 * (S.chi2 - c2);
+            S.chi2 = c2;
+            S.accepted += 1;
+            S.lambda = fmax(S.lambda * 0.3, 1e-9);
+        } else {
+            S.lambda *= 10.0;
+            S.rejected += 1;
+            if (!(S.lambda < 1e12) || !isfinite(c2) && first) status = 2;
+        }
+        S.iters += 1;
+        if (status == 0 && S.iters >= max_iter) status = 3;
+        s_accept = acc;
+        s_lambda = S.lambda;
+        s_active = status == 0;
+        S.status = status;
+        s_bad = 0;
+    }
+    __syncthreads();
+    if (s_accept) {
+        for (int e = tid; e < P; e += kStepThreads) pa[e] = pt[e];
+        // accepted H (symmetric, from the band partials' upper triangles) and g
+        for (int e = tid; e < P * P; e += kStepThreads) {
+            const int i = e / P, j = e % P;
+            const int r = min(i, j), c = max(i, j);
+            double s = 0.0;
+            for (int k = 0; k < n_bands; k++) s += Hp[(int64_t)k * P * P + (int64_t)r * P + c];
+            Ha[e] = s;
+        }
+        for (int e = tid; e < P; e += kStepThreads) {
+            double s = 0.0;
+            for (int k = 0; k < n_bands; k++) s += gp[(int64_t)k * P + e];
+            ga[e] = s;
+        }
+    }
+    __syncthreads();
+    if (!s_active) {
+        // stopped: the trial parameters are the accepted ones
+        for (int e = tid; e < P; e += kStepThreads) pt[e] = pa[e];
+        return;
+    }
+    const double lam = s_lambda;
+    // Marquardt scaling: D = sqrt(diag H); (D^-1 H D^-1 + lambda I) x = D^-1 g
+    for (int i = tid; i < P; i += kStepThreads) {
+        const double a = Ha[(int64_t)i * P + i];
+        double d = (a > 0.0 && isfinite(a)) ? sqrt(a) : 0.0;
+        // a Sersic index held at a bound that the gradient pushes against is
+        // left out of the step (projected step; the bound-constrained optimum)
+        if (i % TB_FIT_NPAR == TB_FIT_NPAR - 1 &&
+            srcs[b.src0 + i / TB_FIT_NPAR].profile == TB_PROFILE_SERSIC &&
+            ((pa[i] >= TB_FIT_SERSIC_MAX && ga[i] > 0.0) ||
+             (pa[i] <= TB_FIT_SERSIC_MIN && ga[i] < 0.0)))
+            d = 0.0;
+        dsc[i] = d;
+    }
+    __syncthreads();
+    auto scaled = [&](int i, int j) -> double {
+        if (dsc[i] == 0.0 || dsc[j] == 0.0) return i == j ? 1.0 : 0.0;
+        return Ha[(int64_t)i * P + j] / (dsc[i] * dsc[j]) + (i == j ? lam : 0.0);
+    };
+    for (int e = tid; e < P * P; e += kStepThreads) {
+        const int i = e / P, j = e % P;
+        if (j <= i) L[e] = scaled(i, j);
+    }
+    __syncthreads();
+    for (int k = 0; k < P; k++) {
+        if (tid == 0) {
+            const double a = L[(int64_t)k * P + k];
+            if (!(a > 0.0) || !isfinite(a)) s_bad = k + 1;
+            else L[(int64_t)k * P + k] = sqrt(a);
+        }
+        __syncthreads();
+        if (s_bad) break;
+        const double lkk = L[(int64_t)k * P + k];
+        for (int i = k + 1 + tid; i < P; i += kStepThreads) L[(int64_t)i * P + k] /= lkk;
+        __syncthreads();
+        const int m = P - k - 1;
+        for (int e = tid; e < m * m; e += kStepThreads) {
+            const int ii = k + 1 + e / m, jj = k + 1 + e % m;
+            if (jj > ii) continue;
+            L[(int64_t)ii * P + jj] -= L[(int64_t)ii * P + k] * L[(int64_t)jj * P + k];
+        }
+        __syncthreads();
+    }
+    if (s_bad) {
+        // not positive definite: treat as a rejected step with more damping
+        if (tid == 0) {
+            S.lambda *= 10.0;
+            if (!(S.lambda < 1e12)) S.status = 2;
+        }
+        for (int e = tid; e < P; e += kStepThreads) pt[e] = pa[e];
+        return;
+    }
+    for (int i = tid; i < P; i += kStepThreads) {
+        xs[i] = 0.0;
+        y[i] = dsc[i] == 0.0 ? 0.0 : ga[i] / dsc[i];
+    }
+    __syncthreads();
+    // solution and one refinement step; triangular solves by warp 0
+    for (int pass = 0; pass < 2; pass++) {
+        if (pass == 1) {
+            for (int i = tid; i < P; i += kStepThreads) {
+                double acc = dsc[i] == 0.0 ? 0.0 : ga[i] / dsc[i];
+                for (int j = 0; j < P; j++) acc -= scaled(i, j) * xs[j];
+                y[i] = acc;
+            }
+            __syncthreads();
+        }
+        if (warp == 0) {
+            for (int i = 0; i < P; i++) {
+                double part = 0.0;
+                for (int j = lane; j < i; j += 32) part += L[(int64_t)i * P + j] * y[j];
+                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                if (lane == 0) y[i] = (y[i] - part) / L[(int64_t)i * P + i];
+                __syncwarp();
+            }
+            for (int i = P - 1; i >= 0; i--) {
+                double part = 0.0;
+                for (int j = i + 1 + lane; j < P; j += 32) part += L[(int64_t)j * P + i] * y[j];
+                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                if (lane == 0) y[i] = (y[i] - part) / L[(int64_t)i * P + i];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < P; i += kStepThreads) xs[i] += y[i];
+        __syncthreads();
+    }
+    // Predicted log-likelihood gain of this damped step,
+    // 1/2 (x . D^-1 g + lambda x . x); the blob has converged when it is below
+    // tol while the damping is moderate (optimize_loop stops on the gain of
+    // the last step, dchisq; the prediction is immune to FP32 noise in chi^2).
+    {
+        double pr = 0.0;
+        for (int i = tid; i < P; i += kStepThreads) {
+            const double y0 = dsc[i] == 0.0 ? 0.0 : ga[i] / dsc[i];
+            pr += xs[i] * y0 + lam * xs[i] * xs[i];
+        }
+        for (int o = 16; o > 0; o >>= 1) pr += __shfl_xor_sync(0xffffffffu, pr, o);
+        if (lane == 0) red[warp] = pr;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w2 = 0; w2 < kStepThreads / 32; w2++) t += red[w2];
+            S.pred = 0.5 * t;
+            s_active = !(0.5 * t < tol && lam <= 1.0);
+            if (!s_active) S.status = 1;
+        }
+        __syncthreads();
+        if (!s_active) {
+            for (int e = tid; e < P; e += kStepThreads) pt[e] = pa[e];
+            return;
+        }
+    }
+    // step = x / D, limited by maximum steps and the Sersic-index bounds
+    // (ConstrainedOptimizer scales the whole step, constrained_optimizer.py)
+    double lim = 1.0;
+    for (int i = tid; i < P; i += kStepThreads) {
+        const double dlt = dsc[i] == 0.0 ? 0.0 : xs[i] / dsc[i];
+        y[i] = dlt;
+        const int off = i % TB_FIT_NPAR;
+        const double ms = max_step(off);
+        if (ms > 0.0 && fabs(dlt) > ms) lim = fmin(lim, ms / fabs(dlt));
+        if (off == TB_FIT_NPAR - 1 && srcs[b.src0 + i / TB_FIT_NPAR].profile == TB_PROFILE_SERSIC) {
+            const double nv = pa[i] + dlt;
+            if (nv > TB_FIT_SERSIC_MAX && dlt > 0.0) lim = fmin(lim, (TB_FIT_SERSIC_MAX - pa[i]) / dlt);
+            if (nv < TB_FIT_SERSIC_MIN && dlt < 0.0) lim = fmin(lim, (TB_FIT_SERSIC_MIN - pa[i]) / dlt);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) lim = fmin(lim, __shfl_xor_sync(0xffffffffu, lim, o));
+    if (lane == 0) red[warp] = lim;
+    __syncthreads();
+    if (tid == 0) {
+        double l = 1.0;
+        for (int w2 = 0; w2 < kStepThreads / 32; w2++) l = fmin(l, red[w2]);
+        s_scale = fmax(l, 0.0);
+    }
+    __syncthreads();
+    for (int i = tid; i < P; i += kStepThreads) {
+        double v = pa[i] + s_scale * y[i];
+        if (i % TB_FIT_NPAR == TB_FIT_NPAR - 1 &&
+            srcs[b.src0 + i / TB_FIT_NPAR].profile == TB_PROFILE_SERSIC)
+            v = fmin(fmax(v, TB_FIT_SERSIC_MIN), TB_FIT_SERSIC_MAX);
+        pt[i] = v;
+    }
+}
+
+__global__ void fit_reset_kernel(tb_fit_state* state, int n, double lambda0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    tb_fit_state s;
+    s.chi2 = INFINITY;
+    s.dlnp = INFINITY;
+    s.lambda = lambda0;
+    s.pred = INFINITY;
+    s.iters = 0;
+    s.accepted = 0;
+    s.rejected = 0;
+    s.status = 0;
+    state[i] = s;
+}
+
+}  // namespace
+
+extern "C" int tb_fit_workspace(int32_t n_src, int32_t n_bands, int64_t* bytes) {
+    if (n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS || !bytes) return TB_ERR_ARG;
+    const int64_t tab = ((int64_t)n_src * (int64_t)sizeof(SrcTab) + 255) / 256 * 256;
+    *bytes = tab + (int64_t)n_src * n_bands * kCompStride * (int64_t)sizeof(FitC);
+    return TB_OK;
+}
+
+namespace {
+inline SrcTab* ws_tab(void* ws) { return static_cast<SrcTab*>(ws); }
+inline FitC* ws_comps(void* ws, int32_t n_src) {
+    const int64_t tab = ((int64_t)n_src * (int64_t)sizeof(SrcTab) + 255) / 256 * 256;
+    return reinterpret_cast<FitC*>(static_cast<char*>(ws) + tab);
+}
+}  // namespace
+
+extern "C" int tb_fit_reset(tb_fit_state* state, int32_t n_blobs, double lambda0, void* stream) {
+    if (n_blobs < 0 || (n_blobs > 0 && !state)) return TB_ERR_ARG;
+    if (n_blobs == 0) return TB_OK;
+    fit_reset_kernel<<<(n_blobs + 255) / 256, 256, 0, (cudaStream_t)stream>>>(state, n_blobs,
+                                                                             lambda0);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+extern "C" int tb_fit_prep(const tb_fit_source* srcs, int32_t n_src, const double* params,
+                           int32_t n_bands, const tb_fit_unit* units, int32_t n_units,
+                           const double* cd_inv, const tb_profile_tables* tables, void* workspace,
+                           void* stream) {
+    if (n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS || n_units < 0) return TB_ERR_ARG;
+    if (n_src == 0) return TB_OK;
+    if (!srcs || !params || !units || !cd_inv || !tables || !workspace) return TB_ERR_ARG;
+    const int smem = tb::tables_smem_bytes(*tables);
+    if (smem > TB_PROFILE_SMEM_MAX) return TB_ERR_SIZE;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(fit_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess)
+        return TB_ERR_LAUNCH;
+    const int per_block = kPrepThreads / 32;
+    fit_prep_kernel<<<(n_src + per_block - 1) / per_block, kPrepThreads, smem,
+                      (cudaStream_t)stream>>>(srcs, n_src, params, n_bands, units, n_units,
+                                              *tables, cd_inv[0], cd_inv[1], cd_inv[2], cd_inv[3],
+                                              ws_tab(workspace), ws_comps(workspace, n_src));
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+extern "C" int tb_fit_pass(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
+                           const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
+                           const void* workspace, const float* data, const float* inverr,
+                           const int32_t* tiles, double* hbuf, double* gbuf, double* chi2_part,
+                           double* chi2_const, const tb_fit_state* state, int32_t n_bands,
+                           int32_t mode, int32_t* work_counter, tb_status* status,
+                           void* stream) {
+    if (n_units < 0 || n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS) return TB_ERR_ARG;
+    if (mode != 0 && mode != 1) return TB_ERR_ARG;
+    if (n_units == 0) return TB_OK;
+    if (!units || !order || !blobs || !srcs || !workspace || !data || !inverr || !tiles ||
+        !hbuf || !gbuf || !chi2_part || !chi2_const || !state || !work_counter)
+        return TB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int smem = (int)sizeof(PassSmem);
+    if (cudaFuncSetAttribute(fit_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+        return TB_ERR_LAUNCH;
+    if (cudaMemsetAsync(work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return TB_ERR_LAUNCH;
+    if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fit_pass_kernel, kThreads, smem) !=
+            cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int64_t want = (int64_t)tb::num_sms() * per_sm;
+    const int grid = (int)(n_units < want ? n_units : want);
+    void* ws = const_cast<void*>(workspace);
+    fit_pass_kernel<<<grid, kThreads, smem, s>>>(
+        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps(ws, n_src), data, inverr, hbuf,
+        gbuf, chi2_part, state, n_bands, tiles, chi2_const, mode, work_counter, status);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+extern "C" int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
+                           const tb_fit_source* srcs, double* params, double* trial,
+                           double* hbuf, double* gbuf, const double* chi2_part,
+                           tb_fit_state* state, double tol, int32_t max_iter, void* stream) {
+    if (n_blobs < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS) return TB_ERR_ARG;
+    if (n_blobs == 0) return TB_OK;
+    if (!blobs || !srcs || !params || !trial || !hbuf || !gbuf || !chi2_part || !state)
+        return TB_ERR_ARG;
+    fit_step_kernel<<<n_blobs, kStepThreads, 0, (cudaStream_t)stream>>>(
+        blobs, n_blobs, n_bands, srcs, params, trial, hbuf, gbuf, chi2_part, state, tol, max_iter);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}

@@ -334,5 +334,9 @@ extern "C" int tb_abi_sizes(int32_t* sizes) {
     sizes[5] = (int32_t)sizeof(tb_scene_src);
     sizes[6] = (int32_t)sizeof(tb_scene_image);
     sizes[7] = (int32_t)sizeof(tb_scene_item);
-    return 8;
+    sizes[8] = (int32_t)sizeof(tb_fit_source);
+    sizes[9] = (int32_t)sizeof(tb_fit_blob);
+    sizes[10] = (int32_t)sizeof(tb_fit_unit);
+    sizes[11] = (int32_t)sizeof(tb_fit_state);
+    return 12;
 }

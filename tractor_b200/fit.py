@@ -1,0 +1,373 @@
+"""Batched blob fitting on the device: Levenberg-Marquardt over many
+independent blobs at once (tb_fit_prep / tb_fit_pass / tb_fit_step).
+
+A blob is a few sources (SersicGalaxy, ExpGalaxy, DevGalaxy or PointSource)
+seen in up to three aligned band images with mixture-of-Gaussians PSFs.  The
+fitter is the batched form of Tractor.optimize_loop with LsqrOptimizer
+(tractor/lsqr_optimizer.py:280-326): every iteration renders every blob's
+model and analytic derivatives, forms the normal equations per blob, and
+takes one damped Gauss-Newton step with ConstrainedOptimizer's step limits;
+a blob stops when the predicted log-likelihood gain of its next step is below
+`tol` (optimize_loop's dchisq, tested on the prediction, which FP32 noise in
+chi^2 does not disturb).  Only the 32 x 8 tiles that some source's mask
+reaches are visited per iteration; the chi^2 of the others is computed once.
+Iterations run as CUDA graphs of `check_every` steps; the host only counts
+the running blobs between graphs.
+
+Parameters per source (TB_FIT_NPAR = 9 slots): x, y, flux[3] (counts),
+log r_e, ee1, ee2 (EllipseESoft), Sersic n.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib, batch, render
+
+NPAR = _lib.FIT_NPAR
+SERSIC_MIN, SERSIC_MAX = 0.29, 6.3
+
+
+class BlobFitter(object):
+    """Device state for fitting a set of blobs.
+
+    blob_src:   (n_blobs + 1,) source offsets (sources of blob b are
+                blob_src[b] .. blob_src[b+1]);
+    sides:      (n_blobs, 2) image (W, H) of every blob (all bands alike);
+    psf:        (n_blobs, n_bands) tuples (amp (K,), mean (K, 2), var (K, 2, 2));
+    sources:    FIT_SOURCE records (profile, mask rectangle in blob pixels);
+    params0:    (n_src, 9) starting parameters;
+    data, inverr: float32 device tensors, unit (blob, band) images packed in
+                blob-major, band-minor order (see `pix_offsets`)."""
+
+    def __init__(self, blob_src, sides, psf, sources, params0, data, inverr, n_bands=3,
+                 cd_inv=None):
+        lib = _lib.load()
+        self.dev = render.device()
+        self.n_bands = int(n_bands)
+        if not 1 <= self.n_bands <= _lib.FIT_MAX_BANDS:
+            raise ValueError('1 to 3 bands')
+        blob_src = np.asarray(blob_src, np.int64)
+        self.n_blobs = len(blob_src) - 1
+        nsrc = np.diff(blob_src)
+        if nsrc.min() < 1 or nsrc.max() > _lib.FIT_MAX_SRC:
+            raise ValueError('every blob needs 1 to %d sources' % _lib.FIT_MAX_SRC)
+        self.n_src = int(blob_src[-1])
+        sides = np.asarray(sides, np.int64).reshape(self.n_blobs, 2)
+        P = nsrc * NPAR
+        blobs = np.zeros(self.n_blobs, _lib.FIT_BLOB)
+        blobs['n_src'] = nsrc
+        blobs['src0'] = blob_src[:-1]
+        blobs['P'] = P
+        blobs['unit0'] = np.arange(self.n_blobs) * self.n_bands
+        hsz = (self.n_bands + 2) * P * P
+        gsz = (self.n_bands + 1) * P
+        blobs['h_off'] = np.concatenate([[0], np.cumsum(hsz)[:-1]])
+        blobs['g_off'] = np.concatenate([[0], np.cumsum(gsz)[:-1]])
+        tiles, n_active, n_tiles = blob_tiles(sides, sources, blob_src)
+        blobs['n_active'] = n_active
+        blobs['n_tiles'] = n_tiles
+        blobs['tile_off'] = np.concatenate([[0], np.cumsum(n_tiles)[:-1]])
+        self.pix_offsets = pix_offsets(sides, self.n_bands)
+        units = np.zeros(self.n_blobs * self.n_bands, _lib.FIT_UNIT)
+        for b in range(self.n_blobs):
+            for k in range(self.n_bands):
+                u = units[b * self.n_bands + k]
+                u['blob'], u['band'] = b, k
+                u['W'], u['H'] = sides[b]
+                u['pix_off'] = self.pix_offsets[b * self.n_bands + k]
+                amp, mean, var = psf[b][k]
+                K = len(amp)
+                if K > _lib.FIT_MAX_PSF:
+                    raise ValueError('at most %d PSF components' % _lib.FIT_MAX_PSF)
+                u['psf_K'] = K
+                u['psf_amp'][:K] = amp
+                u['psf_mean'][:2 * K] = np.asarray(mean, np.float64).ravel()
+                u['psf_var'][:4 * K] = np.asarray(var, np.float64).ravel()
+        # the pass takes units largest first
+        cost = n_active[units['blob']].astype(np.float64) * (1 + nsrc[units['blob']])
+        order = np.argsort(-cost, kind='stable').astype(np.int32)
+        npix = int(self.pix_offsets[-1])
+        if data.numel() < npix or inverr.numel() < npix:
+            raise ValueError('data / inverr hold %d pixels, the blobs need %d' %
+                             (min(data.numel(), inverr.numel()), npix))
+        self.data, self.inverr = data, inverr
+        to = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(self.dev)
+        self.blobs_np, self.units_np = blobs, units
+        self.d_blobs, self.d_units = to(blobs), to(units)
+        self.d_order = torch.from_numpy(order).to(self.dev)
+        self.sources_np = np.ascontiguousarray(sources, _lib.FIT_SOURCE).copy()
+        self.sources_np['blob'] = np.repeat(np.arange(self.n_blobs), nsrc)
+        self.d_sources = to(self.sources_np)
+        self.params = torch.from_numpy(np.ascontiguousarray(params0, np.float64).reshape(-1)).to(
+            self.dev)
+        self.trial = self.params.clone()
+        self.hbuf = torch.zeros(int(hsz.sum()), dtype=torch.float64, device=self.dev)
+        self.gbuf = torch.zeros(int(gsz.sum()), dtype=torch.float64, device=self.dev)
+        self.d_tiles = torch.from_numpy(tiles).to(self.dev)
+        self.chi2_part = torch.zeros(self.n_blobs * self.n_bands, dtype=torch.float64,
+                                     device=self.dev)
+        self.chi2_const = torch.zeros_like(self.chi2_part)
+        self._const_done = False
+        self.state = torch.zeros(self.n_blobs * _lib.FIT_STATE.itemsize, dtype=torch.uint8,
+                                 device=self.dev)
+        nb = ctypes.c_int64()
+        _lib.check(lib.tb_fit_workspace(self.n_src, self.n_bands, ctypes.byref(nb)),
+                   'tb_fit_workspace')
+        self.workspace = torch.empty(max(nb.value, 256), dtype=torch.uint8, device=self.dev)
+        self.misc = torch.zeros(8, dtype=torch.int32, device=self.dev)   # counter + status
+        cd = np.eye(2) * 3600. if cd_inv is None else np.asarray(cd_inv, np.float64)
+        self.cd_inv = np.ascontiguousarray(cd, np.float64).ravel()
+        self.tables = batch.device_profile_tables()
+        self.iterations = 0
+        self._graph = None
+
+    # -- one iteration -----------------------------------------------------
+    def _prep(self):
+        lib = _lib.load()
+        _lib.check(lib.tb_fit_prep(self.d_sources.data_ptr(), self.n_src, self.trial.data_ptr(),
+                                   self.n_bands, self.d_units.data_ptr(), len(self.units_np),
+                                   self.cd_inv.ctypes.data, ctypes.addressof(self.tables.struct),
+                                   self.workspace.data_ptr(), _lib.stream_ptr()), 'tb_fit_prep')
+
+    def _pass(self, mode):
+        lib = _lib.load()
+        _lib.check(lib.tb_fit_pass(self.d_units.data_ptr(), self.d_order.data_ptr(),
+                                   len(self.units_np), self.d_blobs.data_ptr(),
+                                   self.d_sources.data_ptr(), self.n_src,
+                                   self.workspace.data_ptr(), self.data.data_ptr(),
+                                   self.inverr.data_ptr(), self.d_tiles.data_ptr(),
+                                   self.hbuf.data_ptr(), self.gbuf.data_ptr(),
+                                   self.chi2_part.data_ptr(), self.chi2_const.data_ptr(),
+                                   self.state.data_ptr(), self.n_bands, mode,
+                                   self.misc.data_ptr(), self.misc.data_ptr() + 16,
+                                   _lib.stream_ptr()), 'tb_fit_pass')
+
+    def _iteration(self, tol, max_iter):
+        lib = _lib.load()
+        s = _lib.stream_ptr()
+        self._prep()
+        self._pass(0)
+        _lib.check(lib.tb_fit_step(self.d_blobs.data_ptr(), self.n_blobs, self.n_bands,
+                                   self.d_sources.data_ptr(), self.params.data_ptr(),
+                                   self.trial.data_ptr(), self.hbuf.data_ptr(),
+                                   self.gbuf.data_ptr(), self.chi2_part.data_ptr(),
+                                   self.state.data_ptr(), float(tol), int(max_iter), s),
+                   'tb_fit_step')
+
+    def reset(self, params0=None, lambda0=1e-3):
+        lib = _lib.load()
+        if params0 is not None:
+            self.params.copy_(torch.as_tensor(np.asarray(params0, np.float64).reshape(-1)))
+        self.trial.copy_(self.params)
+        _lib.check(lib.tb_fit_reset(self.state.data_ptr(), self.n_blobs, float(lambda0),
+                                    _lib.stream_ptr()), 'tb_fit_reset')
+        self.iterations = 0
+        if not self._const_done:
+            # chi^2 of the tiles no source reaches: fixed for the data set
+            self._prep()
+            self._pass(1)
+            self._const_done = True
+
+    def running(self):
+        st = self.state.view(torch.int32).view(self.n_blobs, _lib.FIT_STATE.itemsize // 4)
+        return int((st[:, -1] == 0).sum().item())
+
+    def fit(self, tol=1e-3, max_iter=50, check_every=4, graph=True, params0=None,
+            lambda0=1e-3):
+        """Runs iterations until every blob stops (or max_iter).  Returns the
+        number of iterations launched."""
+        self.reset(params0, lambda0)
+        g = None
+        if graph:
+            g = self._capture(check_every, tol, max_iter)
+        while self.iterations < max_iter:
+            if g is not None:
+                g.replay()
+            else:
+                for _ in range(check_every):
+                    self._iteration(tol, max_iter)
+            self.iterations += check_every
+            if self.running() == 0:
+                break
+        return self.iterations
+
+    def _capture(self, k, tol, max_iter):
+        key = (k, float(tol), int(max_iter))
+        if self._graph is not None and self._graph[0] == key:
+            return self._graph[1]
+        # warm-up launch outside capture (function attributes, lazy loading),
+        # then restore the starting state
+        p0 = self.params.clone()
+        s0 = self.state.clone()
+        self._iteration(tol, max_iter)
+        torch.cuda.synchronize()
+        self.params.copy_(p0)
+        self.trial.copy_(p0)
+        self.state.copy_(s0)
+        g = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(g, stream=side):
+                for _ in range(k):
+                    self._iteration(tol, max_iter)
+        torch.cuda.current_stream().wait_stream(side)
+        self._graph = (key, g)
+        return g
+
+    # -- results -------------------------------------------------------------
+    def states(self):
+        return self.state.cpu().numpy().view(_lib.FIT_STATE)
+
+    def result(self):
+        return self.params.cpu().numpy().reshape(self.n_src, NPAR)
+
+    def normal_equations(self, b):
+        """(H, g) of blob b at the last accepted parameters (FP64, host)."""
+        bl = self.blobs_np[b]
+        P = int(bl['P'])
+        h0 = int(bl['h_off']) + self.n_bands * P * P
+        g0 = int(bl['g_off']) + self.n_bands * P
+        H = self.hbuf[h0:h0 + P * P].cpu().numpy().reshape(P, P)
+        g = self.gbuf[g0:g0 + P].cpu().numpy()
+        return H, g
+
+    def status(self):
+        return self.misc[4:8]
+
+
+def blob_tiles(sides, sources, blob_src):
+    """Per blob, its 32 x 8 tiles (tx | ty << 16): first those some source
+    mask reaches, then the others.  Returns (tiles, n_active, n_tiles)."""
+    sides = np.asarray(sides, np.int64).reshape(-1, 2)
+    out, n_act, n_all = [], [], []
+    for b in range(len(sides)):
+        W, H = sides[b]
+        tx_n, ty_n = (W + 31) // 32, (H + 7) // 8
+        grid = np.zeros((ty_n, tx_n), bool)
+        for r in sources[blob_src[b]:blob_src[b + 1]]:
+            x0, x1 = max(r['x0'], 0), min(r['x0'] + r['w'], W)
+            y0, y1 = max(r['y0'], 0), min(r['y0'] + r['h'], H)
+            if x1 > x0 and y1 > y0:
+                grid[y0 // 8:(y1 - 1) // 8 + 1, x0 // 32:(x1 - 1) // 32 + 1] = True
+        ty, tx = np.nonzero(grid)
+        pty, ptx = np.nonzero(~grid)
+        out.append(np.concatenate([tx | (ty << 16), ptx | (pty << 16)]).astype(np.int32))
+        n_act.append(len(ty))
+        n_all.append(tx_n * ty_n)
+    return np.concatenate(out), np.array(n_act, np.int32), np.array(n_all, np.int32)
+
+
+def pix_offsets(sides, n_bands):
+    """Element offsets of the (blob, band) images packed blob-major (and the
+    total at the end)."""
+    sides = np.asarray(sides, np.int64).reshape(-1, 2)
+    sz = np.repeat(sides[:, 0] * sides[:, 1], n_bands)
+    return np.concatenate([[0], np.cumsum(sz)]).astype(np.int64)
+
+
+def esoft_from_rabphi(re, q, phi):
+    """EllipseESoft (log r_e, ee1, ee2) of radius, axis ratio, angle (deg)."""
+    ab = 1. / np.asarray(q, np.float64)
+    e = np.minimum((ab - 1) / (ab + 1), 0.999999)
+    ee = -np.log(1. - e)
+    ang = np.radians(-2. * np.asarray(phi, np.float64))
+    return np.log(re), ee * np.cos(ang), ee * np.sin(ang)
+
+
+def blob_workload(n_blobs, rng, side_range=(192, 512), n_bands=3, mean_src=6, max_src=30,
+                  flux_range=(500., 5e4), noise_range=(1., 3.)):
+    """Seeded synthetic blobs: sides U[side_range], Poisson(mean_src) Sersic
+    sources clipped to [1, max_src] placed uniformly, n U[0.7, 6], r_e
+    log-U[0.5, 8] px, axis ratio U[0.2, 1], phi U[0, 180), per-band fluxes
+    log-uniform in flux_range, per (blob, band) 3-component MoG PSF
+    (sigma1 U[1, 2], x2, x4; weights 0.7 / 0.2 / 0.1) and Gaussian noise
+    sigma U[noise_range].  Square masks of half-width
+    clip(round(6 r_e + 12 sigma1), 8, 64).  Returns a dict of host arrays
+    (truth, a perturbed start, geometry)."""
+    side = rng.integers(side_range[0], side_range[1] + 1, n_blobs)
+    nsrc = np.clip(rng.poisson(mean_src, n_blobs), 1, max_src)
+    blob_src = np.concatenate([[0], np.cumsum(nsrc)]).astype(np.int64)
+    n = int(blob_src[-1])
+    blob_of = np.repeat(np.arange(n_blobs), nsrc)
+    s1 = rng.uniform(1., 2., (n_blobs, n_bands))
+    noise = rng.uniform(noise_range[0], noise_range[1], (n_blobs, n_bands))
+    truth = np.zeros((n, NPAR))
+    S = side[blob_of]
+    truth[:, 0] = rng.uniform(8, S - 8)
+    truth[:, 1] = rng.uniform(8, S - 8)
+    for k in range(n_bands):
+        truth[:, 2 + k] = np.exp(rng.uniform(np.log(flux_range[0]), np.log(flux_range[1]), n))
+    re = np.exp(rng.uniform(np.log(0.5), np.log(8.), n))
+    q = rng.uniform(0.2, 1., n)
+    phi = rng.uniform(0., 180., n)
+    truth[:, 5], truth[:, 6], truth[:, 7] = esoft_from_rabphi(re, q, phi)
+    truth[:, 8] = rng.uniform(0.7, 6., n)
+    start = truth.copy()
+    start[:, 0:2] += rng.uniform(-0.5, 0.5, (n, 2))
+    start[:, 2:2 + n_bands] *= rng.uniform(0.8, 1.25, (n, n_bands))
+    start[:, 5] += rng.uniform(-0.2, 0.2, n)
+    start[:, 6:8] += rng.uniform(-0.05, 0.05, (n, 2))
+    start[:, 8] = np.clip(start[:, 8] + rng.uniform(-0.5, 0.5, n), 0.5, 6.)
+    hw = np.clip(np.round(6 * re + 12 * s1.max(axis=1)[blob_of]), 8, 64).astype(np.int64)
+    cx = np.round(truth[:, 0]).astype(np.int64)
+    cy = np.round(truth[:, 1]).astype(np.int64)
+    sources = np.zeros(n, _lib.FIT_SOURCE)
+    sources['profile'] = _lib.PROFILE_SERSIC
+    sources['x0'], sources['y0'] = cx - hw, cy - hw
+    sources['w'] = sources['h'] = 2 * hw + 1
+    psf = []
+    for b in range(n_blobs):
+        row = []
+        for k in range(n_bands):
+            sig = np.array([1., 2., 4.]) * s1[b, k]
+            var = np.zeros((3, 2, 2))
+            var[:, 0, 0] = var[:, 1, 1] = sig ** 2
+            row.append((np.array([0.7, 0.2, 0.1]), np.zeros((3, 2)), var))
+        psf.append(row)
+    return dict(blob_src=blob_src, sides=np.stack([side, side], 1), psf=psf, sources=sources,
+                truth=truth, start=start, noise=noise, n_bands=n_bands)
+
+
+def render_blobs(w, params, seed=None):
+    """Device images of the blobs' model at `params` through the scene
+    renderer (an independent path), plus Gaussian noise of each unit's sigma
+    when `seed` is given.  Returns (data, inverr) float32 device tensors."""
+    n_bands = w['n_bands']
+    sides = w['sides']
+    nb = len(sides)
+    imgs = []
+    for b in range(nb):
+        for k in range(n_bands):
+            amp, mean, var = w['psf'][b][k]
+            imgs.append(batch.SceneImage(sides[b, 0], sides[b, 1], amp, mean, var))
+    r = batch.SceneRenderer(imgs, comp_stride=64)
+    src = w['sources']
+    blob_of = np.repeat(np.arange(nb), np.diff(w['blob_src']))
+    n = len(src)
+    recs = np.zeros(n * n_bands, _lib.SCENE_SRC)
+    for k in range(n_bands):
+        rk = recs[k::n_bands]
+        rk['px'], rk['py'] = params[:, 0], params[:, 1]
+        rk['counts'] = params[:, 2 + k]
+        rk['sa0'], rk['sa1'], rk['sa2'] = params[:, 5], params[:, 6], params[:, 7]
+        rk['sersic_n'] = params[:, 8]
+        rk['profile'] = src['profile']
+        rk['shape_type'] = _lib.SHAPE_ELLIPSE_ESOFT
+        rk['image'] = blob_of * n_bands + k
+        rk['mx0'], rk['my0'], rk['mw'], rk['mh'] = src['x0'], src['y0'], src['w'], src['h']
+        recs[k::n_bands] = rk
+    dev = render.device()
+    out = torch.zeros(r.npix, dtype=torch.float32, device=dev)
+    d = torch.from_numpy(recs.view(np.uint8).copy()).to(dev)
+    st = r.render_device(d, len(recs), out, r.max_pairs(recs, 32), 32)
+    render.check_status(st.clone(), 'tb_scene_render')
+    sig = np.repeat(np.asarray(w['noise'], np.float64).reshape(-1), 1)
+    npx = np.diff(pix_offsets(sides, n_bands))
+    sig_px = torch.from_numpy(np.repeat(sig, npx).astype(np.float32)).to(dev)
+    if seed is not None:
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(int(seed))
+        out += sig_px * torch.randn(out.shape, generator=gen, device=dev, dtype=torch.float32)
+    return out, 1. / sig_px
