@@ -58,7 +58,9 @@ def parse():
     ap.add_argument('--cpu-seconds', type=float, default=12.0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-secondary', action='store_true',
-                    help='skip the batched-scene measurement added to the JSON line')
+                    help='skip the batched-scene and blob-fitting measurements')
+    ap.add_argument('--fit-blobs', type=int, default=2000,
+                    help='blobs in the blob-fitting measurement (2000 = the full workload)')
     return ap.parse_args()
 
 
@@ -328,6 +330,168 @@ def bench_scene(args, dev, flush, clk, cpu_seconds):
 
 
 # ---------------------------------------------------------------------------
+# secondary workload: batched blob fitting (2,000 blobs x 3 bands)
+# ---------------------------------------------------------------------------
+
+FIT_FLOPS_PER_PIXCOMP = 58    # FP32 flops of one pixel x component in tb_fit_pass's inner loop
+
+
+def fit_workload_text(n):
+    return ('%d blobs, sides U[192, 512] px, Poisson(6) SersicGalaxy sources clipped to [1, 30] '
+            '(n U[0.7, 6], r_e log-U[0.5, 8] px, q U[0.2, 1]), 3 bands (g, r, z) with per-band '
+            '3-component MoG PSFs and Gaussian noise sigma U[1, 3]; 9 parameters per source; '
+            'fit from a perturbed start until the predicted dlnp < 1e-3' % n)
+
+
+def _fit_cpu_worker(args):
+    """The oracle's FP64 blob fitter (central-difference Jacobian) on blobs
+    [b0, b1) of the workload until the time budget; returns (sources fitted,
+    seconds)."""
+    b0, b1, n_blobs, seed, budget = args
+    sys.path.insert(0, ROOT)
+    os.environ.setdefault('OMP_NUM_THREADS', '1')
+    from oracle import oracle as O
+    from tractor_b200 import fit
+    w = fit.blob_workload(n_blobs, np.random.default_rng(seed))
+    rng = np.random.default_rng(seed + 1)
+    done, t0 = 0, time.perf_counter()
+    for b in range(b0, b1):
+        if time.perf_counter() - t0 > budget:
+            break
+        s0, s1 = w['blob_src'][b], w['blob_src'][b + 1]
+        W, H = (int(v) for v in w['sides'][b])
+        rects = [tuple(int(v) for v in (r['x0'], r['y0'], r['w'], r['h']))
+                 for r in w['sources'][s0:s1]]
+        mod = O.blob_model(w['truth'][s0:s1], rects, W, H, w['psf'][b], 3)
+        sig = w['noise'][b][:, None, None]
+        data = mod + sig * rng.normal(size=mod.shape)
+        inv = np.broadcast_to(1. / sig, mod.shape)
+        O.blob_fit(w['start'][s0:s1], rects, W, H, w['psf'][b], 3, data, inv, tol=1e-3,
+                   max_iter=60)
+        done += s1 - s0
+    return done, time.perf_counter() - t0
+
+
+def fit_cpu_rate(seconds, n_blobs, seed):
+    ncores = os.cpu_count() or 1
+    per = max(1, n_blobs // ncores)
+    tasks = [((c * per) % n_blobs, min(n_blobs, (c * per) % n_blobs + per), n_blobs, seed,
+              seconds) for c in range(ncores)]
+    with mp.get_context('spawn').Pool(ncores) as pool:
+        res = pool.map(_fit_cpu_worker, tasks)
+    done = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    return done / busy, ncores, done
+
+
+def bench_fit(args, dev, flush, clk, cpu_seconds):
+    """Batched blob fitting: fitted sources per second, device-timed from
+    data resident in HBM (warm graph), and end to end with the pixels copied
+    in from pinned host memory and the parameters copied out."""
+    import torch
+    from tractor_b200 import fit
+    n_blobs = args.fit_blobs
+    w = fit.blob_workload(n_blobs, np.random.default_rng(3000))
+    data, inv = fit.render_blobs(w, w['truth'], seed=3001)
+    f = fit.BlobFitter(w['blob_src'], w['sides'], w['psf'], w['sources'], w['start'], data, inv)
+    n_src = int(w['blob_src'][-1])
+    for _ in range(max(1, min(args.warmup, 2))):
+        f.fit(params0=w['start'])
+    torch.cuda.synchronize()
+    steps = max(2, min(args.steps, 5))
+    times, iters = [], []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        iters.append(f.fit(params0=w['start']))
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    st = f.states()
+    fit_s = float(np.mean(times))
+    # the dominant kernel at full activity: one pass over every blob
+    f.reset(w['start'])
+    f._prep()
+    pe = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    pe[0].record()
+    f._pass(0)
+    pe[1].record()
+    pe[1].synchronize()
+    pass_s = pe[0].elapsed_time(pe[1]) / 1e3
+    # pixel x component evaluations of one pass: every source's mask pixels
+    # inside its blob, Sersic mixtures of up to 9 components x 3 PSF components
+    x0 = np.maximum(w['sources']['x0'], 0)
+    y0 = np.maximum(w['sources']['y0'], 0)
+    side = np.repeat(w['sides'][:, 0], np.diff(w['blob_src']))
+    x1 = np.minimum(w['sources']['x0'] + w['sources']['w'], side)
+    y1 = np.minimum(w['sources']['y0'] + w['sources']['h'], side)
+    area = np.maximum(x1 - x0, 0).astype(np.float64) * np.maximum(y1 - y0, 0)
+    kgal = np.array([fit_ncomp(n) for n in w['start'][:, 8]])
+    pixcomp = float(np.sum(area * kgal * 3 * 3))   # 3 PSF components, 3 bands
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak_clk = clk['sm_mhz'] if clk else 1965.0
+    peak = 128 * 2 * nsm * peak_clk * 1e6 / 1e12
+    achieved = pixcomp * FIT_FLOPS_PER_PIXCOMP / pass_s / 1e12
+    # end to end: pixels in from pinned host memory, fit, parameters out
+    h_data = data.cpu().pin_memory()
+    h_inv = inv.cpu().pin_memory()
+    h_out = torch.empty(n_src * fit.NPAR, dtype=torch.float64).pin_memory()
+    e2e = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        data.copy_(h_data, non_blocking=True)
+        inv.copy_(h_inv, non_blocking=True)
+        f.fit(params0=w['start'])
+        h_out.copy_(f.params, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        e2e.append(e0.elapsed_time(e1) / 1e3)
+    line = {
+        'workload': fit_workload_text(n_blobs),
+        'metric': 'fitted sources/s (batched LM blob fitting)',
+        'value': n_src / fit_s, 'unit': 'sources/s', 'ms_per_step': fit_s * 1e3,
+        'steps': steps, 'n_sources': n_src, 'n_blobs': n_blobs,
+        'iterations_per_fit': float(np.mean(iters)),
+        'status': {'converged': int(np.sum(st['status'] == 1)),
+                   'stopped': int(np.sum(st['status'] == 2)),
+                   'iteration_limit': int(np.sum(st['status'] == 3))},
+        'mean_blob_iterations': float(st['iters'].mean()),
+        'e2e': {'value': n_src / float(np.mean(e2e)), 'unit': 'sources/s',
+                'h2d_bytes_per_step': int(h_data.numel() * 4 + h_inv.numel() * 4),
+                'd2h_bytes_per_step': int(h_out.numel() * 8)},
+        'roofline': {'bound': 'fp32', 'kernel': 'tb_fit_pass (all blobs running)',
+                     'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                     'frac': achieved / peak,
+                     'peak_basis': '128 FP32 FMA/clk/SM x 2 x %d SMs x %s MHz' % (nsm, peak_clk),
+                     'algorithmic': '%.4g pixel x component evaluations x %d FP32 flops per '
+                                    'pass' % (pixcomp, FIT_FLOPS_PER_PIXCOMP),
+                     'kernel_ms': pass_s * 1e3,
+                     'traffic': ncu_traffic('fit_pass_c5.json')},
+    }
+    if cpu_seconds:
+        rate, cores, done = fit_cpu_rate(cpu_seconds, n_blobs, 3000)
+        line['cpu_baseline'] = {'value': rate, 'unit': 'sources/s', 'cores': cores,
+                                'kind': 'port',
+                                'sample': '%d sources in whole blobs fitted by the oracle\'s '
+                                          'FP64 fitter (central-difference Jacobian), one '
+                                          'process per core' % done}
+    return line
+
+
+def fit_ncomp(n):
+    """Galaxy components of a Sersic mixture at index n (the spline range's
+    count, plus the core for n > 1)."""
+    from tractor_b200 import profiles
+    S = profiles.tables()['sersic']
+    for r in S['ranges']:
+        if r['lo'] <= n < r['hi']:
+            return r['K'] + (1 if n > 1 else 0)
+    return S['ranges'][-1]['K'] + 1
+
+
+# ---------------------------------------------------------------------------
 
 def init_dist():
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -522,9 +686,9 @@ def main():
         'clocks': clk,
     }
     if not args.no_secondary:
-        line['secondary'] = [bench_scene(args, dev, flush, clk,
-                                         None if (args.no_cpu_baseline or world > 1 or rank)
-                                         else min(args.cpu_seconds, 8.0))]
+        cpu_s = None if (args.no_cpu_baseline or world > 1 or rank) else min(args.cpu_seconds, 8.0)
+        line['secondary'] = [bench_scene(args, dev, flush, clk, cpu_s),
+                             bench_fit(args, dev, flush, clk, cpu_s)]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, nsrc, wall = cpu_rate(args.cpu_seconds, use_ref=False)
         line['cpu_baseline'] = {'value': rate, 'unit': 'Mpix*components/s', 'cores': cores,

@@ -671,7 +671,15 @@ def blob_normal_equations(params, rects, W, H, psf, n_bands, data, inverr, steps
     n = len(params)
     P = n * BLOB_NPAR
     base = blob_model(params, rects, W, H, psf, n_bands)
-    r = ((data - base) * inverr).ravel()
+    r_all = ((data - base) * inverr).ravel()
+    # rows: the pixels some source mask reaches (the others have zero
+    # derivatives; their chi^2 is added as is)
+    cover = np.zeros((n_bands, H, W), bool)
+    for (x0, y0, w, h) in rects:
+        cover[:, max(y0, 0):max(min(y0 + h, H), 0), max(x0, 0):max(min(x0 + w, W), 0)] = True
+    cover = cover.ravel()
+    r = r_all[cover]
+    c2_out = float(r_all[~cover] @ r_all[~cover])
     cols = np.zeros((r.size, P))
     h = np.array([1e-5, 1e-5, 0., 0., 0., 1e-6, 1e-6, 1e-6, 1e-6]) if steps is None else steps
     for s in range(n):
@@ -689,8 +697,8 @@ def blob_normal_equations(params, rects, W, H, psf, n_bands, data, inverr, steps
                 pm[s, j] -= h[j]
                 d = (blob_model(pp[s:s + 1], rects[s:s + 1], W, H, psf, n_bands) -
                      blob_model(pm[s:s + 1], rects[s:s + 1], W, H, psf, n_bands)) / (2 * h[j])
-            cols[:, s * BLOB_NPAR + j] = (d * inverr).ravel()
-    return cols.T @ cols, cols.T @ r, float(r @ r)
+            cols[:, s * BLOB_NPAR + j] = (d * inverr).ravel()[cover]
+    return cols.T @ cols, cols.T @ r, float(r @ r) + c2_out
 
 
 def blob_fit(params0, rects, W, Himg, psf, n_bands, data, inverr, tol=1e-12, max_iter=60,
