@@ -148,14 +148,41 @@ typedef struct {
     int32_t ldo;       /* output row stride in elements (0 = mw) */
     int64_t out_off;
     int64_t spec_off;  /* float offset of this item's PSF spectrum in psf_spec */
+    int32_t dmode;     /* TB_FFT_VALUE, or a derivative (see below) */
+    int32_t dc0;       /* TB_FFT_DSPEC: coefficients at comp_dcoef[4 (dc0 + k) ..] */
+    int64_t dot_off;   /* mode TB_FFT_DOT: result slot in dots */
 } tb_fft_item;
 
 #define TB_FFT_MAX_SZ 256
+/* Derivative items (tb_fourier_render_deriv): DSPEC renders
+ * d/dtheta sum_k a_k exp(-2 pi^2 f^T C_k f) from per-component (da_k,
+ * dC_k00, dC_k01, dC_k11); DX / DY render the derivative with respect to the
+ * sub-pixel shift mux / muy (the Lanczos-3 taps' derivative). */
+#define TB_FFT_VALUE 0
+#define TB_FFT_DSPEC 1
+#define TB_FFT_DX 2
+#define TB_FFT_DY 3
+/* Output mode of a Fourier item: instead of writing its pixels, accumulate
+ * sum over its pixels of out[pixel] * value into dots[dot_off] (out then
+ * holds the upstream gradient, read only): the vector-Jacobian product. */
+#define TB_FFT_DOT 3
 
 int tb_fourier_render(const tb_fft_item* items, int32_t n_items,
                       const double* comp_amp, const double* comp_var,
                       const float* psf_spec, float* out, int32_t* work_counter,
                       tb_status* status, void* stream);
+
+/* tb_fourier_render with derivative items and the TB_FFT_DOT output mode:
+ * the analytic parameter derivatives of the Fourier path that
+ * Galaxy.getParamDerivatives / SersicGalaxy.getParamDerivatives
+ * (tractor/galaxy.py:137-223, tractor/sersic.py:402-445) approximate by
+ * finite differences, and their contraction with an upstream gradient.
+ * comp_dcoef may be NULL when no item is DSPEC, dots when none is DOT. */
+int tb_fourier_render_deriv(const tb_fft_item* items, int32_t n_items,
+                            const double* comp_amp, const double* comp_var,
+                            const double* comp_dcoef, const float* psf_spec, float* out,
+                            double* dots, int32_t* work_counter, tb_status* status,
+                            void* stream);
 
 /* ------------------------------------------------------------------------
  * Galaxy preparation for the Fourier path
@@ -230,6 +257,21 @@ int tb_galaxy_fft_prep(const tb_galaxy_src* srcs, int32_t n, const tb_fft_image*
                        const tb_profile_tables* tables, tb_fft_item* items,
                        double* comp_amp, double* comp_var, int32_t comp_stride,
                        int32_t* flags, void* stream);
+
+/* Jacobian items of n galaxies: items[7 i + j] for the parameters j = x, y,
+ * counts, s0, s1, s2 (shape, per shape_type), Sersic n of source i, on the
+ * geometry tb_galaxy_fft_prep gives its value item, with out_off =
+ * srcs[i].out_off + j * col_stride and dot_off = 7 i + j.  comp_dcoef:
+ * 4 * n * comp_stride * 4 doubles (per source and shape / index parameter,
+ * per component: da, dC00, dC01, dC11), by FP64 central differences of the
+ * profile (Sersic range held fixed) and of the shape's T T^T.  mode:
+ * TB_MOG_STORE / TB_MOG_ACCUM (Jacobian patches) or TB_FFT_DOT (with
+ * col_stride 0: the upstream gradient patch at srcs[i].out_off). */
+int tb_galaxy_fft_jac_prep(const tb_galaxy_src* srcs, int32_t n, const tb_fft_image* image,
+                           const tb_profile_tables* tables, tb_fft_item* items,
+                           double* comp_amp, double* comp_var, double* comp_dcoef,
+                           int32_t comp_stride, int32_t mode, int64_t col_stride,
+                           int32_t* flags, void* stream);
 
 /* Forward real FFT of n zero-padded sz x sz float32 PSF images (prepared by
  * the caller, image i at pad + i*sz*sz) into complex64 spectra

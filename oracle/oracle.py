@@ -742,3 +742,63 @@ def blob_fit(params0, rects, W, Himg, psf, n_bands, data, inverr, tol=1e-12, max
     held = np.zeros(p.size, bool)
     held[nidx] = ((p[:, 8] >= upper_n) & (g[nidx] > 0)) | ((p[:, 8] <= lower_n) & (g[nidx] < 0))
     return p, H, held
+
+
+# ---------------------------------------------------------------------------
+# Fourier path in FP64 throughout (for finite-difference derivative checks)
+# ---------------------------------------------------------------------------
+
+def lanczos_shift_f64(img, dx, dy):
+    """lanczos_shift_3f's separable Lanczos-3 correlation with zero edges
+    (tractor/mp_fourier.i:267-429) in FP64: rows first, then columns;
+    out[c] = sum_k taps(dx)[k] in[c - 3 + k]."""
+    img = np.asarray(img, np.float64)
+    H, W = img.shape
+    fx, fy = lanczos3_taps(dx), lanczos3_taps(dy)
+    pad = np.zeros((H, W + 6))
+    pad[:, 3:W + 3] = img
+    tmp = sum(fx[k] * pad[:, k:k + W] for k in range(7))
+    pad = np.zeros((H + 6, W))
+    pad[3:H + 3, :] = tmp
+    return sum(fy[k] * pad[k:k + H, :] for k in range(7))
+
+
+def galaxy_fft_masked_f64(amp, var2, px, py, psf_img, mask_x0, mask_y0, mw, mh):
+    """galaxy_fft_masked without the reference's FP32 roundings (PSF spectrum
+    complex128, irfftn output and Lanczos shift in FP64): a smooth function of
+    the parameters for central-difference derivative checks."""
+    psfh, psfw = psf_img.shape
+    hs = fft_halfsize_for_mask(px, py, mask_x0, mask_y0, mw, mh, psfh, psfw)
+    sz = fft_size(hs)
+    pad, cx, cy = pad_psf(np.asarray(psf_img, np.float64), sz, sz)
+    P = np.fft.rfft2(pad)
+    v = np.fft.rfftfreq(sz)
+    w = np.fft.fftfreq(sz)
+    mux = px - cx - mask_x0
+    muy = py - cy - mask_y0
+    sx = int(np.round(mux))
+    sy = int(np.round(muy))
+    mux -= sx
+    muy -= sy
+    G = np.fft.irfftn(fourier_mog(amp, var2, v, w) * P)
+    if mux != 0.0 or muy != 0.0:
+        G = lanczos_shift_f64(G, mux, muy)
+    gh, gw = G.shape
+    out = np.zeros((mh, mw))
+    ry = overlapping_region(-sy, -sy + mh - 1, 0, gh - 1)
+    rx = overlapping_region(-sx, -sx + mw - 1, 0, gw - 1)
+    if ry is not None and rx is not None:
+        out[ry[1], rx[1]] = G[ry[0], rx[0]]
+    return out
+
+
+def sersic_fft_model_f64(theta, psf_img, mask_x0, mask_y0, mw, mh, shape='E'):
+    """FP64 Fourier-path model of a SersicGalaxy, theta = (x, y, counts, s0,
+    s1, s2, n) with an EllipseE ('E': re, e1, e2) or EllipseESoft ('ESoft':
+    log re, ee1, ee2) shape and NullWCS."""
+    x, y, c, s0, s1, s2, n = (float(t) for t in theta)
+    amp, var = sersic_profile(n)
+    e = (s0, s1, s2) if shape == 'E' else ellipseESoft_to_E(s0, s1, s2)
+    T = nullwcs_cdinv() @ ellipseE_basis(*e)
+    a2, v2 = sheared(amp, var, T)
+    return c * galaxy_fft_masked_f64(a2, v2, x, y, psf_img, mask_x0, mask_y0, mw, mh)

@@ -24,7 +24,10 @@ FLOOR_FIXED, FLOOR_MINVAL = 0, 1
 FFT_ITEM = np.dtype([('c0', '<i4'), ('K', '<i4'), ('sz', '<i4'), ('mode', '<i4'),
                      ('mw', '<i4'), ('mh', '<i4'), ('sx', '<i4'), ('sy', '<i4'),
                      ('mux', '<f8'), ('muy', '<f8'), ('scale', '<f4'), ('ldo', '<i4'),
-                     ('out_off', '<i8'), ('spec_off', '<i8')])
+                     ('out_off', '<i8'), ('spec_off', '<i8'), ('dmode', '<i4'), ('dc0', '<i4'),
+                     ('dot_off', '<i8')])
+FFT_VALUE, FFT_DSPEC, FFT_DX, FFT_DY = 0, 1, 2, 3
+FFT_DOT = 3
 STATUS = np.dtype([('code', '<i4'), ('item', '<i4'), ('detail', '<i4'), ('count', '<i4')])
 GALAXY_SRC = np.dtype([('px', '<f8'), ('py', '<f8'), ('counts', '<f8'), ('s0', '<f8'),
                        ('s1', '<f8'), ('s2', '<f8'), ('sersic_n', '<f8'), ('out_off', '<i8'),
@@ -105,6 +108,9 @@ SIGNATURES = {
     'tb_solve_update_noalloc': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P]),
     'tb_chi2': (_I32, [_P, _P, _P, _P, _P, _I32, _P, _P]),
     'tb_galaxy_fft_prep': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _I32, _P, _P]),
+    'tb_galaxy_fft_jac_prep': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _I32, _I32, _I64, _P,
+                                      _P]),
+    'tb_fourier_render_deriv': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     'tb_scene_prep': (_I32, [_P, _I32, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P]),
     'tb_scene_workspace': (_I32, [_I64, _I64, _P]),
     'tb_fit_workspace': (_I32, [_I32, _I32, _P]),

@@ -75,28 +75,6 @@ struct FitS {
 // prep
 // ---------------------------------------------------------------------------
 
-// Sersic mixture of range r at index nn with the core present or not, lane l
-// holding component l (the spline evaluation of warp_profile without the
-// range lookup, so that both sides of a central difference use the same
-// components).
-__device__ int sersic_fixed(const tb_profile_tables& T, int r, double nn, bool core_on, int lane,
-                            double& a, double& v) {
-    const int Kr = T.range_info[4 * r], sa = T.range_info[4 * r + 1];
-    const int sv = T.range_info[4 * r + 2];
-    a = 0.0;
-    v = 0.0;
-    if (lane < Kr) {
-        a = tb::bspline(T, sa + lane, nn);
-        v = exp(tb::bspline(T, sv + lane, nn));
-    }
-    a /= tb::lane_sum(a, Kr);
-    if (!core_on) return Kr;
-    const double core = tb::bspline(T, T.core_spline, nn);
-    a *= (1.0 - core) / tb::lane_sum(a, Kr);
-    if (lane == Kr) { a = core; v = 0.0; }
-    return Kr + 1;
-}
-
 __device__ void shape_M(const double* cd, double s0, double s1, double s2, double M[3]) {
     double G[4], re;
     tb::shape_basis(TB_SHAPE_ELLIPSE_ESOFT, s0, s1, s2, G, re);
@@ -134,11 +112,11 @@ fit_prep_kernel(const tb_fit_source* __restrict__ srcs, int n, const double* __r
             ok = 0;
         } else {
             const bool core = nn > 1.0;
-            K = sersic_fixed(T, r, nn, core, lane, a, v);
+            K = tb::sersic_fixed(T, r, nn, core, lane, a, v);
             if (!clamped) {
                 double ap, vp, am, vm;
-                sersic_fixed(T, r, nn + kHn, core, lane, ap, vp);
-                sersic_fixed(T, r, nn - kHn, core, lane, am, vm);
+                tb::sersic_fixed(T, r, nn + kHn, core, lane, ap, vp);
+                tb::sersic_fixed(T, r, nn - kHn, core, lane, am, vm);
                 da = (ap - am) / (2.0 * kHn);
                 dv = (vp - vm) / (2.0 * kHn);
             }

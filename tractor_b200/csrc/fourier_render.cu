@@ -43,7 +43,7 @@ __host__ __device__ constexpr int s1_bytes(int N, int rmax) { return rmax * (N /
 constexpr int kS1Bytes = s1_bytes(256, kRmax256) > s1_bytes(128, 128) ? s1_bytes(256, kRmax256)
                                                                        : s1_bytes(128, 128);
 constexpr int kSmemBytes = 256 * 8               /* twiddles */
-                           + kMaxK * 16           /* components */
+                           + 2 * kMaxK * 16       /* components, derivative prefactors */
                            + 16 * 4               /* taps */
                            + (129 + 256) * 8      /* Hx, Hy */
                            + kWarps * kXbufPerWarp * 8 + kS1Bytes;
@@ -51,6 +51,7 @@ constexpr int kSmemBytes = 256 * 8               /* twiddles */
 struct Shared {
     float2* tw;
     float4* comp;   // (amp, ca, cb, cd): exponent = ca v^2 + cb v w + cd w^2 (log2 units)
+    float4* dcomp;  // derivative items: prefactor (da, ba, bb, bc) = da + ba v^2 + bb v w + bc w^2
     float* taps;    // fx[0..6], fy[0..6]
     float2* hx;     // frequency response of the x taps, v = 0..N/2
     float2* hy;     // frequency response of the y taps, row index j = 0..N-1
@@ -75,6 +76,30 @@ __device__ void taps3(double dx, float* f) {
     for (int i = 0; i < 7; i++) f[i] = (float)t[i];
 }
 
+// d taps / d dx of the normalised Lanczos-3 taps above (quotient rule on
+// L(p) = 3 sin(p) sin(p/3) / p^2, p = pi (i - 3 + dx)); at dx = 0 the limit
+// from dx > 0 (the taps' support 0..5; the |i - 3| = 3 terms vanish).
+__device__ void taps3_deriv(double dx, float* f) {
+    double L[7] = {0, 0, 0, 0, 0, 0, 0}, D[7] = {0, 0, 0, 0, 0, 0, 0};
+    const int lo = dx >= 0.0 ? 0 : 1, hi = dx >= 0.0 ? 6 : 7;
+    double S = 0.0, Sd = 0.0;
+    for (int i = lo; i < hi; i++) {
+        const double p = TB_PI * (i - 3.0 + dx);
+        if (p == 0.0) {
+            L[i] = 1.0;
+            D[i] = 0.0;
+        } else {
+            const double sp = sin(p), s3 = sin(p / 3.0), cp = cos(p), c3 = cos(p / 3.0);
+            L[i] = 3.0 * sp * s3 / (p * p);
+            D[i] = TB_PI * 3.0 * (cp * s3 / (p * p) + sp * c3 / (3.0 * p * p) -
+                                  2.0 * sp * s3 / (p * p * p));
+        }
+        S += L[i];
+        Sd += D[i];
+    }
+    for (int i = 0; i < 7; i++) f[i] = (i >= lo && i < hi) ? (float)((D[i] - L[i] / S * Sd) / S) : 0.f;
+}
+
 // Mixture spectrum at (v, w) for the 8 rows of one thread: acc[m] =
 // sum_k amp_k exp2(ca v^2 + cb v w_m + cd w_m^2).
 __device__ __forceinline__ void spectrum8(const float4* comp, int K, float vf, const float* wf,
@@ -88,6 +113,27 @@ __device__ __forceinline__ void spectrum8(const float4* comp, int K, float vf, c
         for (int m = 0; m < 8; m++) {
             const float e = fmaf(wf[m], fmaf(c.w, wf[m], be), al);
             acc[m] = fmaf(c.x, tb::ex2(e), acc[m]);
+        }
+    }
+}
+
+// Derivative spectrum: acc[m] = sum_k (da_k + ba_k v^2 + bb_k v w_m + bc_k w_m^2)
+// * amp-less exp2(...) -- d/dtheta [a exp(-2 pi^2 f^T C f)] for a parameter
+// theta that moves a and C.
+__device__ __forceinline__ void dspectrum8(const float4* comp, const float4* dcomp, int K,
+                                           float vf, const float* wf, float* acc) {
+#pragma unroll
+    for (int m = 0; m < 8; m++) acc[m] = 0.f;
+    for (int k = 0; k < K; k++) {
+        const float4 c = comp[k];
+        const float4 d = dcomp[k];
+        const float al = c.y * vf * vf, be = c.z * vf;
+        const float d0 = fmaf(d.y * vf, vf, d.x), d1 = d.z * vf;
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const float e = fmaf(wf[m], fmaf(c.w, wf[m], be), al);
+            const float pre = fmaf(wf[m], fmaf(d.w, wf[m], d1), d0);
+            acc[m] = fmaf(pre, tb::ex2(e), acc[m]);
         }
     }
 }
@@ -106,15 +152,21 @@ __device__ void zero_outside(float* O, int64_t ldo, int mw, int mh, int sx, int 
     }
 }
 
-__device__ __forceinline__ void put(float* o, float v, int mode) {
-    if (mode == TB_MOG_ATOMIC) atomicAdd(o, v);
+// Writes one output pixel; in TB_FFT_DOT mode `o` points into the upstream
+// gradient and the pixel's contribution to the item's dot product is
+// accumulated instead.
+template <bool kDeriv>
+__device__ __forceinline__ void put(float* o, float v, int mode, float& dot) {
+    if (kDeriv && mode == TB_FFT_DOT) dot = fmaf(*o, v, dot);
+    else if (mode == TB_MOG_ATOMIC) atomicAdd(o, v);
     else if (mode == TB_MOG_ACCUM) *o += v;
     else *o = v;
 }
 
-template <int N>
+template <int N, bool kDeriv>
 __device__ void render_item_spectral(const tb_fft_item& it, int K, const float* __restrict__ spec,
-                                     float* __restrict__ out, const Shared& sh, int rcap) {
+                                     float* __restrict__ out, const Shared& sh, int rcap,
+                                     float& dot) {
     constexpr int NH = N / 2 + 1;
     constexpr int T = N / 8;            // threads per FFT
     constexpr int GPW = 32 / T;         // FFT groups per warp
@@ -161,7 +213,10 @@ __device__ void render_item_spectral(const tb_fft_item& it, int K, const float* 
                 const int j = t + m * T;
                 wf[m] = (float)(j < N / 2 ? j : j - N) / (float)N;
             }
-            spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
+            if (kDeriv && it.dmode == TB_FFT_DSPEC)
+                dspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
+            else
+                spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
             float2 x[8];
             const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)v * N;
 #pragma unroll
@@ -206,8 +261,8 @@ __device__ void render_item_spectral(const tb_fft_item& it, int K, const float* 
             float* ob = O + (int64_t)(rlo + ib + sy) * ldo + sx;
             tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int col, float2 z) {
                 if (act && col >= gc0 && col < gc1) {
-                    put(oa + col, z.x * osc, it.mode);
-                    if (hasb) put(ob + col, z.y * osc, it.mode);
+                    put<kDeriv>(oa + col, z.x * osc, it.mode, dot);
+                    if (hasb) put<kDeriv>(ob + col, z.y * osc, it.mode, dot);
                 }
             });
             __syncwarp();
@@ -216,9 +271,10 @@ __device__ void render_item_spectral(const tb_fft_item& it, int K, const float* 
     }
 }
 
-template <int N>
+template <int N, bool kDeriv>
 __device__ void render_item_spatial(const tb_fft_item& it, int K, const float* __restrict__ spec,
-                                    float* __restrict__ out, const Shared& sh, int rmax) {
+                                    float* __restrict__ out, const Shared& sh, int rmax,
+                                    float& dot) {
     constexpr int NH = N / 2 + 1;
     constexpr int T = N / 8;
     constexpr int GPW = 32 / T;
@@ -254,7 +310,10 @@ __device__ void render_item_spatial(const tb_fft_item& it, int K, const float* _
                 const int j = t + m * T;
                 wf[m] = (float)(j < N / 2 ? j : j - N) / (float)N;
             }
-            spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
+            if (kDeriv && it.dmode == TB_FFT_DSPEC)
+                dspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
+            else
+                spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
             float2 x[8];
             const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)v * N;
 #pragma unroll
@@ -345,43 +404,48 @@ __device__ void render_item_spatial(const tb_fft_item& it, int K, const float* _
                     val = fmaf(fy[k], row[c - gc0], val);
                 }
             }
-            put(O + (int64_t)(r + sy) * ldo + (c + sx), val * osc, it.mode);
+            put<kDeriv>(O + (int64_t)(r + sy) * ldo + (c + sx), val * osc, it.mode, dot);
         }
         __syncthreads();
     }
 }
 
-template <int N>
+template <int N, bool kDeriv>
 __device__ void render_item(const tb_fft_item& it, int K, const float* __restrict__ spec,
-                            float* __restrict__ out, const Shared& sh) {
+                            float* __restrict__ out, const Shared& sh, float& dot) {
     const int mw = it.mw, mh = it.mh, sx = it.sx, sy = it.sy;
     const int gr0 = max(0, -sy), gr1 = min(N, mh - sy);
     const int gc0 = max(0, -sx), gc1 = min(N, mw - sx);
     const bool empty = gr0 >= gr1 || gc0 >= gc1;
-    const bool accum = it.mode == TB_MOG_ACCUM || it.mode == TB_MOG_ATOMIC;
+    const bool accum = it.mode == TB_MOG_ACCUM || it.mode == TB_MOG_ATOMIC || it.mode == TB_FFT_DOT;
     if (!accum)
         zero_outside(out + it.out_off, it.ldo > 0 ? it.ldo : mw, mw, mh, sx, sy, gr0, gr1, gc0,
                      gc1, empty);
     if (empty) return;
-    // Zero-edged Lanczos = circular correlation when no tap leaves the box.
-    const bool xin = it.mux == 0.0 || (gc0 >= 3 && gc1 <= N - 3);
-    const bool yin = it.muy == 0.0 || (gr0 >= 3 && gr1 <= N - 3);
+    // Zero-edged Lanczos = circular correlation when no tap leaves the box
+    // (no shift: the identity taps; a tap derivative is never the identity).
+    const bool xin = (it.mux == 0.0 && it.dmode != TB_FFT_DX) || (gc0 >= 3 && gc1 <= N - 3);
+    const bool yin = (it.muy == 0.0 && it.dmode != TB_FFT_DY) || (gr0 >= 3 && gr1 <= N - 3);
     const int rcap = N == 256 ? kRmax256 : N;
-    if (xin && yin) render_item_spectral<N>(it, K, spec, out, sh, rcap);
-    else render_item_spatial<N>(it, K, spec, out, sh, N == 256 ? kRmax256 : N + 6);
+    if (xin && yin) render_item_spectral<N, kDeriv>(it, K, spec, out, sh, rcap, dot);
+    else render_item_spatial<N, kDeriv>(it, K, spec, out, sh, N == 256 ? kRmax256 : N + 6, dot);
 }
 
+template <bool kDeriv>
 __global__ void __launch_bounds__(kThreads, 1)
 fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
                       const double* __restrict__ amp, const double* __restrict__ var,
-                      const float* __restrict__ psf_spec, float* __restrict__ out,
-                      int32_t* counter, tb_status* st) {
+                      const double* __restrict__ dcoef, const float* __restrict__ psf_spec,
+                      float* __restrict__ out, double* __restrict__ dots, int32_t* counter,
+                      tb_status* st) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Shared sh;
     unsigned char* p = smem_raw;
     sh.tw = reinterpret_cast<float2*>(p);
     p += 256 * 8;
     sh.comp = reinterpret_cast<float4*>(p);
+    p += kMaxK * 16;
+    sh.dcomp = reinterpret_cast<float4*>(p);
     p += kMaxK * 16;
     sh.taps = reinterpret_cast<float*>(p);
     p += 16 * 4;
@@ -402,7 +466,11 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
         const tb_fft_item& it = items[u];
         const int N = it.sz, K = it.K;
         const bool okN = N == 32 || N == 64 || N == 128 || N == 256;
-        if (!okN || K < 0 || K > kMaxK || it.mw <= 0 || it.mh <= 0 ||
+        const bool okD = kDeriv ? (it.dmode >= TB_FFT_VALUE && it.dmode <= TB_FFT_DY &&
+                                   (it.dmode != TB_FFT_DSPEC || dcoef != nullptr) &&
+                                   (it.mode != TB_FFT_DOT || dots != nullptr))
+                                : (it.dmode == TB_FFT_VALUE && it.mode != TB_FFT_DOT);
+        if (!okN || !okD || K < 0 || K > kMaxK || it.mw <= 0 || it.mh <= 0 ||
             !(fabs(it.mux) <= 0.5) || !(fabs(it.muy) <= 0.5)) {
             if (threadIdx.x == 0) tb::report(st, TB_STATUS_BAD_ITEM, (int)u, N);
             continue;
@@ -414,9 +482,22 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
             const double a = var[4 * c], bb = var[4 * c + 1], d = var[4 * c + 3];
             sh.comp[k] = make_float4((float)amp[c], (float)(c2 * a), (float)(c2 * 2.0 * bb),
                                      (float)(c2 * d));
+            if (kDeriv && it.dmode == TB_FFT_DSPEC) {
+                // d/dtheta [a exp(-2 pi^2 f^T C f)] = (da - 2 pi^2 a f^T dC f) exp(...)
+                const double* dc = dcoef + 4 * ((int64_t)it.dc0 + k);
+                const double m2 = -2.0 * TB_PI * TB_PI * amp[c];
+                sh.dcomp[k] = make_float4((float)dc[0], (float)(m2 * dc[1]),
+                                          (float)(m2 * 2.0 * dc[2]), (float)(m2 * dc[3]));
+            }
         }
-        if (threadIdx.x == 32) taps3(it.mux, sh.taps);
-        if (threadIdx.x == 64) taps3(it.muy, sh.taps + 7);
+        if (threadIdx.x == 32) {
+            if (kDeriv && it.dmode == TB_FFT_DX) taps3_deriv(it.mux, sh.taps);
+            else taps3(it.mux, sh.taps);
+        }
+        if (threadIdx.x == 64) {
+            if (kDeriv && it.dmode == TB_FFT_DY) taps3_deriv(it.muy, sh.taps + 7);
+            else taps3(it.muy, sh.taps + 7);
+        }
         __syncthreads();
         if (cur_n != N) {
             __syncthreads();
@@ -431,35 +512,74 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
         }
         __syncthreads();
         const float* spec = psf_spec + it.spec_off;
+        float dot = 0.f;
         switch (N) {
-            case 256: render_item<256>(it, K, spec, out, sh); break;
-            case 128: render_item<128>(it, K, spec, out, sh); break;
-            case 64: render_item<64>(it, K, spec, out, sh); break;
-            default: render_item<32>(it, K, spec, out, sh); break;
+            case 256: render_item<256, kDeriv>(it, K, spec, out, sh, dot); break;
+            case 128: render_item<128, kDeriv>(it, K, spec, out, sh, dot); break;
+            case 64: render_item<64, kDeriv>(it, K, spec, out, sh, dot); break;
+            default: render_item<32, kDeriv>(it, K, spec, out, sh, dot); break;
+        }
+        if (kDeriv && it.mode == TB_FFT_DOT) {
+            // fixed-order block reduction of the item's dot product
+            __shared__ double red[kWarps];
+            double dd = (double)dot;
+            for (int o = 16; o > 0; o >>= 1) dd += __shfl_xor_sync(0xffffffffu, dd, o);
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dd;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double s2 = 0.0;
+                for (int w = 0; w < kWarps; w++) s2 += red[w];
+                dots[it.dot_off] = s2;
+            }
+            __syncthreads();
         }
     }
 }
 
 }  // namespace
 
-extern "C" int tb_fourier_render(const tb_fft_item* items, int32_t n_items,
-                                 const double* comp_amp, const double* comp_var,
-                                 const float* psf_spec, float* out, int32_t* work_counter,
-                                 tb_status* status, void* stream) {
+static int launch_fourier(const tb_fft_item* items, int32_t n_items, const double* comp_amp,
+                          const double* comp_var, const double* comp_dcoef, const float* psf_spec,
+                          float* out, double* dots, int32_t* work_counter, tb_status* status,
+                          void* stream) {
     if (n_items < 0) return TB_ERR_ARG;
     if (n_items == 0) return TB_OK;
     if (!items || !comp_amp || !comp_var || !psf_spec || !out || !work_counter) return TB_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    if (cudaFuncSetAttribute(fourier_render_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kSmemBytes) != cudaSuccess)
+    const bool deriv = comp_dcoef != nullptr || dots != nullptr;
+    if (cudaFuncSetAttribute(deriv ? fourier_render_kernel<true> : fourier_render_kernel<false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
         return TB_ERR_LAUNCH;
     if (cudaMemsetAsync(work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return TB_ERR_LAUNCH;
     if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
         return TB_ERR_LAUNCH;
     const int grid = n_items < tb::num_sms() ? n_items : tb::num_sms();
-    fourier_render_kernel<<<grid, kThreads, kSmemBytes, s>>>(items, n_items, comp_amp, comp_var,
-                                                             psf_spec, out, work_counter, status);
+    if (deriv)
+        fourier_render_kernel<true><<<grid, kThreads, kSmemBytes, s>>>(
+            items, n_items, comp_amp, comp_var, comp_dcoef, psf_spec, out, dots, work_counter,
+            status);
+    else
+        fourier_render_kernel<false><<<grid, kThreads, kSmemBytes, s>>>(
+            items, n_items, comp_amp, comp_var, nullptr, psf_spec, out, nullptr, work_counter,
+            status);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+extern "C" int tb_fourier_render(const tb_fft_item* items, int32_t n_items,
+                                 const double* comp_amp, const double* comp_var,
+                                 const float* psf_spec, float* out, int32_t* work_counter,
+                                 tb_status* status, void* stream) {
+    return launch_fourier(items, n_items, comp_amp, comp_var, nullptr, psf_spec, out, nullptr,
+                          work_counter, status, stream);
+}
+
+extern "C" int tb_fourier_render_deriv(const tb_fft_item* items, int32_t n_items,
+                                       const double* comp_amp, const double* comp_var,
+                                       const double* comp_dcoef, const float* psf_spec,
+                                       float* out, double* dots, int32_t* work_counter,
+                                       tb_status* status, void* stream) {
+    return launch_fourier(items, n_items, comp_amp, comp_var, comp_dcoef, psf_spec, out, dots,
+                          work_counter, status, stream);
 }
 
 // ---------------------------------------------------------------------------

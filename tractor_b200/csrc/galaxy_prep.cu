@@ -20,6 +20,54 @@ namespace {
 constexpr int kMaxComp = 10;
 constexpr int kPrepThreads = 128;   // 4 sources (warps) per block
 
+// Patch geometry for a ModelMask: half-size (galaxy.py:339-351), FFT size
+// (psf.py:209-212), the source-outside-mask rule (galaxy.py:353-374).
+// flag: 0 render, 1 no patch, 2 unsupported; si: index of sz in 32..256.
+__device__ void prep_geometry(const tb_galaxy_src& s, const tb_fft_image& img, int K, double re,
+                              int& flag, int& sz, int& si) {
+    const double px = s.px, py = s.py;
+    const int x0 = s.mx0, y0 = s.my0, x1 = s.mx0 + s.mw, y1 = s.my0 + s.mh;
+    double hs = fmax(s.mh / 2.0, s.mw / 2.0);
+    hs = fmax(hs, fmax(fmax(1 + px - x0, 1 + x1 - px), fmax(1 + py - y0, 1 + y1 - py)));
+    hs = fmax(hs, fmax(img.psf_w / 2.0, img.psf_h / 2.0));
+    const double hsi = ceil(hs);
+    sz = 1;
+    while (sz < 2.0 * hsi && sz < (1 << 20)) sz *= 2;
+    const bool out = px < x0 || px > x1 - 1 || py < y0 || py > y1 - 1;
+    si = sz == 32 ? 0 : sz == 64 ? 1 : sz == 128 ? 2 : sz == 256 ? 3 : -1;
+    flag = 0;
+    if (K < 0 || s.mw <= 0 || s.mh <= 0) {
+        flag = 2;
+    } else if (s.counts == 0.0) {
+        flag = 1;
+    } else if (out) {
+        double ndx = 0.0, ndy = 0.0;
+        if (px < x0) ndx = x0 - px;
+        if (px > x1) ndx = px - x1;
+        if (py < y0) ndy = y0 - py;
+        if (py > y1) ndy = py - y1;
+        const double nearest = hypot(ndx, ndy);
+        flag = (nearest > tb::nre_of(s.profile) * re / img.pixscale) ? 1 : 2;
+    } else if (si < 0 || img.spec_off[si] < 0) {
+        flag = 2;
+    }
+}
+
+// Fills a rendered item's geometry: integer / sub-pixel split of the offset
+// with half-to-even rounding (galaxy.py:383-406).
+__device__ void item_geometry(const tb_galaxy_src& s, const tb_fft_image& img, int sz, int si,
+                              tb_fft_item& it) {
+    const double dx = s.px - img.psf_cx[si], dy = s.py - img.psf_cy[si];
+    const double mux = dx - s.mx0, muy = dy - s.my0;
+    const double sxd = rint(mux), syd = rint(muy);
+    it.sz = sz;
+    it.sx = (int)sxd;
+    it.sy = (int)syd;
+    it.mux = mux - sxd;
+    it.muy = muy - syd;
+    it.spec_off = img.spec_off[si];
+}
+
 // One warp per source.  Lane l < K evaluates component l's amplitude and
 // log-variance splines; sums and the stable variance ranking use shuffles;
 // the shape and geometry are computed redundantly by every lane.
@@ -48,32 +96,8 @@ galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, int n, tb_fft_ima
     tb::pixel_factor(img.cd_inv, G, M00, M01, M11);
 
     // ---- geometry (ModelMask given) ----
-    const double px = s.px, py = s.py;
-    const int x0 = s.mx0, y0 = s.my0, x1 = s.mx0 + s.mw, y1 = s.my0 + s.mh;
-    double hs = fmax(s.mh / 2.0, s.mw / 2.0);
-    hs = fmax(hs, fmax(fmax(1 + px - x0, 1 + x1 - px), fmax(1 + py - y0, 1 + y1 - py)));
-    hs = fmax(hs, fmax(img.psf_w / 2.0, img.psf_h / 2.0));
-    const double hsi = ceil(hs);
-    int sz = 1;
-    while (sz < 2.0 * hsi && sz < (1 << 20)) sz *= 2;
-    const bool out = px < x0 || px > x1 - 1 || py < y0 || py > y1 - 1;
-    const int si = sz == 32 ? 0 : sz == 64 ? 1 : sz == 128 ? 2 : sz == 256 ? 3 : -1;
-    int flag = 0;
-    if (K < 0 || s.mw <= 0 || s.mh <= 0) {
-        flag = 2;
-    } else if (s.counts == 0.0) {
-        flag = 1;
-    } else if (out) {
-        double ndx = 0.0, ndy = 0.0;
-        if (px < x0) ndx = x0 - px;
-        if (px > x1) ndx = px - x1;
-        if (py < y0) ndy = y0 - py;
-        if (py > y1) ndy = py - y1;
-        const double nearest = hypot(ndx, ndy);
-        flag = (nearest > tb::nre_of(s.profile) * re / img.pixscale) ? 1 : 2;
-    } else if (si < 0 || img.spec_off[si] < 0) {
-        flag = 2;
-    }
+    int flag, sz, si;
+    prep_geometry(s, img, K, re, flag, sz, si);
     const int c0 = i * stride;
     if (flag == 0 && lane < K) {
         camp[c0 + rank] = a;
@@ -99,21 +123,150 @@ galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, int n, tb_fft_ima
         it.ldo = 0;
         it.out_off = s.out_off;
         it.spec_off = img.spec_off[0] >= 0 ? img.spec_off[0] : 0;
+        it.dmode = TB_FFT_VALUE;
+        it.dc0 = 0;
+        it.dot_off = 0;
         if (flag == 0) {
-            const double dx = px - img.psf_cx[si], dy = py - img.psf_cy[si];
-            double mux = dx - x0, muy = dy - y0;
-            const double sxd = rint(mux), syd = rint(muy);
             it.K = K;
-            it.sz = sz;
-            it.sx = (int)sxd;
-            it.sy = (int)syd;
-            it.mux = mux - sxd;
-            it.muy = muy - syd;
-            it.spec_off = img.spec_off[si];
+            item_geometry(s, img, sz, si, it);
         }
         items[i] = it;
         flags[i] = flag;
     }
+}
+
+
+constexpr double kHn = 1e-5;   // central-difference step in the Sersic index
+constexpr double kHs = 1e-6;   // central-difference step in shape parameters
+
+__device__ void shape_factor(const tb_fft_image& img, int shape_type, double s0, double s1,
+                             double s2, double M[3], double& re) {
+    double G[4];
+    tb::shape_basis(shape_type, s0, s1, s2, G, re);
+    tb::pixel_factor(img.cd_inv, G, M[0], M[1], M[2]);
+}
+
+// Jacobian items: per source 7 items (x, y, counts, s0, s1, s2, n) on the
+// value item's geometry.  Position: the derivative Lanczos taps; counts: the
+// unit-flux render; shape and index: the spectrum's derivative with
+// coefficients (da_k, dC_k) in dcoef -- dC = v_k dM/ds_j for the shape, and
+// (da_k, dv_k M) for the Sersic index -- by FP64 central differences of the
+// exact maps (the range held fixed for n).
+__global__ void __launch_bounds__(kPrepThreads)
+galaxy_fft_jac_prep_kernel(const tb_galaxy_src* __restrict__ srcs, int n, tb_fft_image img,
+                           tb_profile_tables Tg, tb_fft_item* __restrict__ items,
+                           double* __restrict__ camp, double* __restrict__ cvar,
+                           double* __restrict__ dcoef, int stride, int mode, int64_t col_stride,
+                           int32_t* __restrict__ flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const tb_profile_tables T = tb::stage_tables(Tg, smem_raw);
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (kPrepThreads / 32) + (threadIdx.x >> 5);
+    if (i >= n) return;
+    const tb_galaxy_src s = srcs[i];
+
+    double a = 0.0, v = 0.0, da = 0.0, dv = 0.0;
+    int K;
+    if (s.profile == TB_PROFILE_SERSIC) {
+        double nn = s.sersic_n;
+        const double lowest = T.range_lohi[0], highest = T.range_lohi[2 * T.n_ranges - 1];
+        int r = -1;
+        bool clamped = false;
+        if (nn <= lowest) { r = 0; nn = lowest; clamped = true; }
+        else if (nn >= highest) { r = T.n_ranges - 1; nn = highest; clamped = true; }
+        else {
+            for (int q = 0; q < T.n_ranges; q++)
+                if (T.range_lohi[2 * q] <= nn && nn < T.range_lohi[2 * q + 1]) { r = q; break; }
+        }
+        if (r < 0 || T.range_info[4 * r] + 1 > kMaxComp) {
+            K = -1;
+        } else {
+            const bool core = nn > 1.0;
+            K = tb::sersic_fixed(T, r, nn, core, lane, a, v);
+            if (!clamped) {
+                double ap, vp, am, vm;
+                tb::sersic_fixed(T, r, nn + kHn, core, lane, ap, vp);
+                tb::sersic_fixed(T, r, nn - kHn, core, lane, am, vm);
+                da = (ap - am) / (2.0 * kHn);
+                dv = (vp - vm) / (2.0 * kHn);
+            }
+        }
+    } else {
+        K = tb::warp_profile(T, s.profile, s.sersic_n, lane, kMaxComp, a, v);
+    }
+    // sorted by variance (sersic.py:338-341), the permutation kept for the
+    // derivative
+    const int rank = tb::variance_rank(v, K, lane);
+
+    double M[3], re;
+    shape_factor(img, s.shape_type, s.s0, s.s1, s.s2, M, re);
+    double dM[3][3];
+    const double sp[3] = {s.s0, s.s1, s.s2};
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        double hp[3] = {sp[0], sp[1], sp[2]}, hm[3] = {sp[0], sp[1], sp[2]};
+        hp[j] += kHs;
+        hm[j] -= kHs;
+        double Mp[3], Mm[3], rr;
+        shape_factor(img, s.shape_type, hp[0], hp[1], hp[2], Mp, rr);
+        shape_factor(img, s.shape_type, hm[0], hm[1], hm[2], Mm, rr);
+#pragma unroll
+        for (int q = 0; q < 3; q++) dM[j][q] = (Mp[q] - Mm[q]) / (2.0 * kHs);
+    }
+
+    int flag, sz, si;
+    prep_geometry(s, img, K, re, flag, sz, si);
+    const int c0 = i * stride;
+    if (flag == 0 && lane < K) {
+        const int c = c0 + rank;
+        camp[c] = a;
+        double* w = cvar + 4 * c;
+        w[0] = v * M[0];
+        w[1] = v * M[1];
+        w[2] = v * M[1];
+        w[3] = v * M[2];
+        for (int j = 0; j < 4; j++) {
+            double* d = dcoef + 4 * ((int64_t)(4 * i + j) * stride + rank);
+            if (j < 3) {
+                d[0] = 0.0;
+                d[1] = v * dM[j][0];
+                d[2] = v * dM[j][1];
+                d[3] = v * dM[j][2];
+            } else {
+                d[0] = da;
+                d[1] = dv * M[0];
+                d[2] = dv * M[1];
+                d[3] = dv * M[2];
+            }
+        }
+    }
+    if (lane < 7) {
+        const int j = lane;
+        tb_fft_item it;
+        it.c0 = c0;
+        it.K = 0;
+        it.sz = 32;
+        it.mode = mode;
+        it.mw = s.mw;
+        it.mh = s.mh;
+        it.sx = 0;
+        it.sy = 0;
+        it.mux = 0.0;
+        it.muy = 0.0;
+        it.scale = j == 2 ? 1.0f : (float)s.counts;
+        it.ldo = 0;
+        it.out_off = s.out_off + j * col_stride;
+        it.spec_off = img.spec_off[0] >= 0 ? img.spec_off[0] : 0;
+        it.dmode = j == 0 ? TB_FFT_DX : j == 1 ? TB_FFT_DY : j == 2 ? TB_FFT_VALUE : TB_FFT_DSPEC;
+        it.dc0 = j >= 3 ? (4 * i + (j - 3)) * stride : 0;
+        it.dot_off = 7 * (int64_t)i + j;
+        if (flag == 0) {
+            it.K = K;
+            item_geometry(s, img, sz, si, it);
+        }
+        items[7 * (int64_t)i + j] = it;
+    }
+    if (lane == 0) flags[i] = flag;
 }
 
 }  // namespace
@@ -136,5 +289,30 @@ extern "C" int tb_galaxy_fft_prep(const tb_galaxy_src* srcs, int32_t n, const tb
     galaxy_fft_prep_kernel<<<(n + per_block - 1) / per_block, kPrepThreads, smem,
                              (cudaStream_t)stream>>>(
         srcs, n, *image, *tables, items, comp_amp, comp_var, comp_stride, flags);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+extern "C" int tb_galaxy_fft_jac_prep(const tb_galaxy_src* srcs, int32_t n, const tb_fft_image* image,
+                                      const tb_profile_tables* tables, tb_fft_item* items,
+                                      double* comp_amp, double* comp_var, double* comp_dcoef,
+                                      int32_t comp_stride, int32_t mode, int64_t col_stride,
+                                      int32_t* flags, void* stream) {
+    if (n < 0) return TB_ERR_ARG;
+    if (n == 0) return TB_OK;
+    if (!srcs || !image || !tables || !items || !comp_amp || !comp_var || !comp_dcoef || !flags)
+        return TB_ERR_ARG;
+    if (mode != TB_MOG_STORE && mode != TB_MOG_ACCUM && mode != TB_FFT_DOT) return TB_ERR_ARG;
+    if (comp_stride < kMaxComp) return TB_ERR_SIZE;
+    const int smem = tb::tables_smem_bytes(*tables);
+    if (smem > TB_PROFILE_SMEM_MAX) return TB_ERR_SIZE;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(galaxy_fft_jac_prep_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    const int per_block = kPrepThreads / 32;
+    galaxy_fft_jac_prep_kernel<<<(n + per_block - 1) / per_block, kPrepThreads, smem,
+                                 (cudaStream_t)stream>>>(srcs, n, *image, *tables, items,
+                                                         comp_amp, comp_var, comp_dcoef,
+                                                         comp_stride, mode, col_stride, flags);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }

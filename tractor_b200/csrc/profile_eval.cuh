@@ -163,6 +163,28 @@ __device__ inline int warp_profile(const tb_profile_tables& T, int profile, doub
     return K;
 }
 
+// Sersic mixture of range r at index nn with the core present or not, lane l
+// holding component l (the spline evaluation of warp_profile without the
+// range lookup, so that both sides of a central difference use the same
+// components).
+__device__ inline int sersic_fixed(const tb_profile_tables& T, int r, double nn, bool core_on,
+                                   int lane, double& a, double& v) {
+    const int Kr = T.range_info[4 * r], sa = T.range_info[4 * r + 1];
+    const int sv = T.range_info[4 * r + 2];
+    a = 0.0;
+    v = 0.0;
+    if (lane < Kr) {
+        a = bspline(T, sa + lane, nn);
+        v = exp(bspline(T, sv + lane, nn));
+    }
+    a /= lane_sum(a, Kr);
+    if (!core_on) return Kr;
+    const double core = bspline(T, T.core_spline, nn);
+    a *= (1.0 - core) / lane_sum(a, Kr);
+    if (lane == Kr) { a = core; v = 0.0; }
+    return Kr + 1;
+}
+
 // Stable rank of this lane's variance among lanes 0..K-1 (the argsort of
 // sersic.py:338-341).
 __device__ __forceinline__ int variance_rank(double v, int K, int lane) {

@@ -242,7 +242,7 @@ class FftBatch(object):
             self.nspec += spec.numel()
         self.items.append((self.ncomp, K, int(sz), int(mode), int(mw), int(mh), int(sx), int(sy),
                            float(mux), float(muy), float(scale), int(ldo), int(out_off),
-                           self.spec_off[key]))
+                           self.spec_off[key], _lib.FFT_VALUE, 0, 0))
         self.amp.append(amp)
         self.var.append(np.asarray(var, np.float64).reshape(K, 2, 2))
         self.ncomp += K
