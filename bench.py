@@ -98,6 +98,57 @@ def _cpu_worker(args):
     return work, time.perf_counter() - t0, i - i0
 
 
+def fourier_plain_fp64(srcs, out, dev, budget):
+    """The plain FP64 GPU renderer (tractor_b200.plain.fourier_render_fp64:
+    one galaxy at a time, FP64 torch ops and cuFFT) over the workload's
+    sources for about `budget` seconds: Mpix x components / s, and the
+    batched FP32 patches' largest deviation from it (of each patch's peak)."""
+    import torch
+    from tractor_b200 import plain, profiles
+    psf = batch_moffat()
+    cdinv = np.eye(2) * 3600.
+    specs = {}
+    got = out.view(len(srcs), MASK, MASK)
+    err, work, n = 0., 0., 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i, s in enumerate(srcs):
+        amp, var = profiles.sersic_mixture().profile(float(s['sersic_n']))
+        from tractor_b200 import ellipses
+        G = ellipses.EllipseE(s['s0'], s['s1'], s['s2']).getRaDecBasis()
+        T = cdinv @ G
+        v2 = np.array([v * (T @ T.T) for v in var])
+        hs = max(MASK / 2., 1 + s['px'], 1 + MASK - s['px'], 1 + s['py'], 1 + MASK - s['py'], 31.5)
+        sz = 1
+        while sz < 2 * np.ceil(hs):
+            sz *= 2
+        if sz not in specs:
+            specs[sz] = plain.psf_spectrum_fp64(psf.astype(np.float64), sz, dev)
+        spec, cx, cy = specs[sz]
+        p = plain.fourier_render_fp64(amp, v2, spec, cx, cy, sz, float(s['px']), float(s['py']),
+                                      0, 0, MASK, MASK, counts=float(s['counts']))
+        g = got[i].double()
+        err = max(err, float((g - p).abs().max() / p.abs().max()))
+        work += sz * sz * len(amp)
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    e1.record()
+    e1.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    return {'value': work / secs / 1e6, 'unit': 'Mpix*components/s', 'sources': n,
+            'seconds': secs, 'batched_fp32_max_err_of_peak': err,
+            'how': 'tractor_b200.plain.fourier_render_fp64, one galaxy at a time, FP64 torch '
+                   'ops and cuFFT on the same GPU'}
+
+
+def batch_moffat():
+    from tractor_b200 import batch
+    return batch.moffat_psf()
+
+
 def cpu_rate(seconds, use_ref, seed=1000):
     """Mpix*components/s of the CPU path on all host cores (spawned worker
     processes), over a bounded sample of the workload."""
@@ -448,6 +499,7 @@ def bench_fit(args, dev, flush, clk, cpu_seconds):
         e1.record()
         e1.synchronize()
         e2e.append(e0.elapsed_time(e1) / 1e3)
+    plain = fit_plain_fp64(w, data, inv, f.result(), dev, budget=8.0)
     line = {
         'workload': fit_workload_text(n_blobs),
         'metric': 'fitted sources/s (batched LM blob fitting)',
@@ -461,6 +513,8 @@ def bench_fit(args, dev, flush, clk, cpu_seconds):
         'e2e': {'value': n_src / float(np.mean(e2e)), 'unit': 'sources/s',
                 'h2d_bytes_per_step': int(h_data.numel() * 4 + h_inv.numel() * 4),
                 'd2h_bytes_per_step': int(h_out.numel() * 8)},
+        'plain_fp64': plain,
+        'speedup_vs_plain_fp64': (n_src / fit_s) / plain['value'] if plain['value'] else None,
         'roofline': {'bound': 'fp32', 'kernel': 'tb_fit_pass (all blobs running)',
                      'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
                      'frac': achieved / peak,
@@ -478,6 +532,56 @@ def bench_fit(args, dev, flush, clk, cpu_seconds):
                                           'FP64 fitter (central-difference Jacobian), one '
                                           'process per core' % done}
     return line
+
+
+def fit_plain_fp64(w, data, inv, batched, dev, budget):
+    """The plain FP64 GPU fitter (tractor_b200.plain.BlobFitFP64: one blob at
+    a time, FP64 torch / cuSOLVER) on the workload's first blobs for about
+    `budget` seconds: fitted sources / s, and the batched FP32 fitter's
+    parameters against it in units of the FP64 sigma (both stopped at
+    predicted dlnp < 1e-3)."""
+    import torch
+    from tractor_b200 import fit, plain
+    po = fit.pix_offsets(w['sides'], 3)
+    hd, hi = data.cpu().numpy(), inv.cpu().numpy()
+    done, errs, blobs = 0, [], 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    fits = []
+    for b in range(len(w['sides'])):
+        s0, s1 = w['blob_src'][b], w['blob_src'][b + 1]
+        W, H = (int(v) for v in w['sides'][b])
+        d3 = np.stack([hd[po[3 * b + k]:po[3 * b + k + 1]].reshape(H, W) for k in range(3)])
+        i3 = np.stack([hi[po[3 * b + k]:po[3 * b + k + 1]].reshape(H, W) for k in range(3)])
+        rects = [tuple(int(v) for v in (r['x0'], r['y0'], r['w'], r['h']))
+                 for r in w['sources'][s0:s1]]
+        pf = plain.BlobFitFP64(d3, i3, w['psf'][b], rects, dev)
+        th, _ = pf.fit(w['start'][s0:s1], tol=1e-3)
+        fits.append((pf, th, s0, s1))
+        done += s1 - s0
+        blobs += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    e1.record()
+    e1.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    for pf, th, s0, s1 in fits:
+        Hf = pf.fisher(th)
+        d = np.diag(Hf)
+        free = d > 0
+        sig = np.full(Hf.shape[0], np.inf)
+        sig[free] = np.sqrt(np.diag(np.linalg.inv(Hf[np.ix_(free, free)])))
+        errs.append(np.max(np.abs(batched[s0:s1] - th).ravel() / sig))
+    return {'value': done / secs, 'unit': 'sources/s', 'blobs': blobs, 'sources': int(done),
+            'seconds': secs,
+            'batched_vs_plain_max_sigma': float(np.max(errs)) if errs else None,
+            'batched_vs_plain_median_sigma': float(np.median(errs)) if errs else None,
+            'how': 'tractor_b200.plain.BlobFitFP64, one blob at a time, FP64 torch ops + '
+                   'cuSOLVER Cholesky on the same GPU, same stopping rule (predicted '
+                   'dlnp < 1e-3); error = max over parameters of |batched - plain| / sigma '
+                   '(FP64 Fisher matrix)'}
 
 
 def fit_ncomp(n):
@@ -689,6 +793,9 @@ def main():
         cpu_s = None if (args.no_cpu_baseline or world > 1 or rank) else min(args.cpu_seconds, 8.0)
         line['secondary'] = [bench_scene(args, dev, flush, clk, cpu_s),
                              bench_fit(args, dev, flush, clk, cpu_s)]
+    line['plain_fp64'] = fourier_plain_fp64(srcs, out, dev, budget=3.0)
+    if line['plain_fp64']['value']:
+        line['speedup_vs_plain_fp64'] = value / line['plain_fp64']['value']
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, nsrc, wall = cpu_rate(args.cpu_seconds, use_ref=False)
         line['cpu_baseline'] = {'value': rate, 'unit': 'Mpix*components/s', 'cores': cores,
