@@ -33,7 +33,7 @@ constexpr int kThreads = 256;          // pass CTA = one 32 x 8 tile, one pixel 
 constexpr int kTileW = 32;
 constexpr int kTileH = 8;
 constexpr int kCols = 7;               // columns per (source, band): x y flux logre ee1 ee2 n
-constexpr int kG = 5;                  // sources per shared-memory column group
+constexpr int kG = 4;                  // sources per shared-memory column group
 constexpr int kLd = kThreads + 1;      // padded column stride (floats)
 constexpr int kStageMax = kG * kMaxGalK * TB_FIT_MAX_PSF;
 constexpr double kHn = 1e-5;           // central-difference step in n
@@ -44,6 +44,8 @@ constexpr int kCompStride = kMaxGalK * TB_FIT_MAX_PSF;   // component slots per 
 // Per-source summary written by tb_fit_prep.
 struct SrcTab {
     double flux[TB_FIT_MAX_BANDS];
+    float M[3];                    // T T^T (xx, xy, yy)
+    float dM[3][3];                // d(T T^T) / d(logre, ee1, ee2)
     int32_t K[TB_FIT_MAX_BANDS];   // components in each band (galaxy x PSF)
     int32_t ok;
 };
@@ -52,6 +54,10 @@ struct SrcTab {
 // value, position and shape-derivative coefficients, the 1/2 of dN/dC
 // folded in.  The mean stays FP64 (absolute pixels); the pass makes it
 // tile-relative.
+// The shape derivative of component k is dC_k = v_k dM (dM per source), the
+// index derivative dC_k = dv_k M: the pass accumulates per source the
+// moments sum_k val_k v_k u u^T and sum_k val_k dv_k u u^T over components
+// and applies dM / M once per source and pixel.
 struct FitC {
     double mx, my;
     float qxx, qxy, qyy;      // exponent, log2 units
@@ -59,16 +65,17 @@ struct FitC {
     float s;                  // unit-flux amplitude a / (2 pi sqrt det)
     float sn;                 // d a / d n / (2 pi sqrt det)
     float fl;                 // exponent floor, log2 units
-    float dxx[4], dxy2[4], dyy[4], t[4];  // 1/2 dC (xy doubled), 1/2 tr(C^-1 dC)
-    int32_t pad[3];
+    float v, dv;              // the galaxy component's variance and d/dn
+    float t[4];               // tr(C^-1 dM_j) (j < 3), tr(C^-1 M)
+    int32_t pad[7];
 };
 
 // The same, staged in shared memory for one tile (FP32 tile-relative mean).
 struct FitS {
     float mx, my;
-    float qxx, qxy, qyy, ixx, ixy, iyy, s, sn, fl;
-    float dxx[4], dxy2[4], dyy[4], t[4];
-    int32_t rec;              // source position in the tile's list
+    float qxx, qxy, qyy, ixx, ixy, iyy, s, sn, fl, v, dv;
+    float t[4];
+    int32_t pad[3];
 };
 
 // ---------------------------------------------------------------------------
@@ -200,18 +207,16 @@ fit_prep_kernel(const tb_fit_source* __restrict__ srcs, int n, const double* __r
             c.s = (float)(ag * u->psf_amp[pp] * norm);
             c.sn = (float)(dag * u->psf_amp[pp] * norm);
             c.fl = (float)(-50.0 * TB_LOG2E);
-            // dC / d(logre, ee1, ee2) = v dM; dC / dn = dv M
+            c.v = (float)vg;
+            c.dv = (float)dvg;
+            // dC / d(logre, ee1, ee2) = v dM_j; dC / dn = dv M
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                double d0, d1, d2;
-                if (j < 3) { d0 = vg * dM[j][0]; d1 = vg * dM[j][1]; d2 = vg * dM[j][2]; }
-                else { d0 = dvg * M[0]; d1 = dvg * M[1]; d2 = dvg * M[2]; }
-                c.dxx[j] = (float)(0.5 * d0);
-                c.dxy2[j] = (float)d1;
-                c.dyy[j] = (float)(0.5 * d2);
-                c.t[j] = (float)(0.5 * (i00 * d0 + 2.0 * i01 * d1 + i11 * d2));
+                const double* d = j < 3 ? dM[j] : M;
+                c.t[j] = (float)(i00 * d[0] + 2.0 * i01 * d[1] + i11 * d[2]);
             }
-            c.pad[0] = c.pad[1] = c.pad[2] = 0;
+#pragma unroll
+            for (int q = 0; q < 7; q++) c.pad[q] = 0;
             const bool good = det > 0.0 && isfinite(norm);
             if (!good) ok = 0;
             comps[((int64_t)i * n_bands + bd) * kCompStride + k] = c;
@@ -225,6 +230,10 @@ fit_prep_kernel(const tb_fit_source* __restrict__ srcs, int n, const double* __r
             t.K[bd] = bd < n_bands ? Kb[bd] : 0;
         }
         t.ok = ok;
+        for (int q = 0; q < 3; q++) {
+            t.M[q] = (float)M[q];
+            for (int j = 0; j < 3; j++) t.dM[j][q] = (float)dM[j][q];
+        }
         tab[i] = t;
     }
 }
@@ -239,6 +248,8 @@ struct TileRec {
     int32_t src;              // source index within the blob
     int32_t K;                // components (galaxy x PSF)
     int32_t pad;
+    float M[3];               // T T^T (xx, xy, yy)
+    float dM[3][3];           // its shape derivatives
 };
 
 struct PassSmem {
@@ -278,62 +289,69 @@ __device__ float eval_group(PassSmem& sm, const FitC* __restrict__ gcomps, int s
         f.my = (float)(c.my - (double)oy);
         f.qxx = c.qxx; f.qxy = c.qxy; f.qyy = c.qyy;
         f.ixx = c.ixx; f.ixy = c.ixy; f.iyy = c.iyy;
-        f.s = c.s; f.sn = c.sn; f.fl = c.fl;
+        f.s = c.s; f.sn = c.sn; f.fl = c.fl; f.v = c.v; f.dv = c.dv;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            f.dxx[j] = c.dxx[j]; f.dxy2[j] = c.dxy2[j]; f.dyy[j] = c.dyy[j]; f.t[j] = c.t[j];
-        }
-        f.rec = q;
+        for (int j = 0; j < 4; j++) f.t[j] = c.t[j];
+        f.pad[0] = f.pad[1] = f.pad[2] = 0;
         sm.comps[g] = f;
     }
     __syncthreads();
     const float xf = (float)lane, yf = (float)warp;
     float model = 0.f;
-    float m = 0.f, jx = 0.f, jy = 0.f, j0 = 0.f, j1 = 0.f, j2 = 0.f, jn = 0.f;
-    int cur = -1;
-    for (int g = 0; g <= total; g++) {
-        const int rec = g < total ? sm.comps[g].rec : -2;
-        if (rec != cur) {
-            if (cur >= 0) {
-                // source `cur` done: add its patch inside its rectangle and
-                // write its weighted columns
-                const TileRec& R = sm.recs[cur];
-                const bool in = lane >= R.x0 && lane < R.x1 && warp >= R.y0 && warp < R.y1;
-                const float cnt = R.counts;
-                model += in ? cnt * m : 0.f;
-                if (kDeriv) {
-                    const float cw = in ? cnt * w : 0.f;
-                    float* col = &A[(cur - q0) * kCols][tid];
-                    col[0 * kLd] = cw * jx;
-                    col[1 * kLd] = cw * jy;
-                    col[2 * kLd] = in ? w * m : 0.f;
-                    col[3 * kLd] = cw * j0;
-                    col[4 * kLd] = cw * j1;
-                    col[5 * kLd] = cw * j2;
-                    col[6 * kLd] = cw * jn;
-                }
+    int kb = 0;
+    for (int q = q0; q < q0 + nq; q++) {
+        const TileRec& R = sm.recs[q];
+        const int K = R.K;
+        // per-source moments over its components (see FitC)
+        float m = 0.f, jx = 0.f, jy = 0.f, jn = 0.f;
+        float axx = 0.f, axy = 0.f, ayy = 0.f, t0 = 0.f, t1 = 0.f, t2 = 0.f;
+        float bxx = 0.f, bxy = 0.f, byy = 0.f, tn = 0.f;
+#pragma unroll 2
+        for (int g = kb; g < kb + K; g++) {
+            const FitS& c = sm.comps[g];
+            const float dx = xf - c.mx, dy = yf - c.my;
+            const float e = fmaf(dx, fmaf(c.qxx, dx, c.qxy * dy), c.qyy * dy * dy);
+            const float E = (e >= c.fl) ? tb::ex2(e) : 0.f;
+            const float val = c.s * E;
+            m += val;
+            if (kDeriv) {
+                const float ux = fmaf(c.ixx, dx, c.ixy * dy);
+                const float uy = fmaf(c.ixy, dx, c.iyy * dy);
+                jx = fmaf(val, ux, jx);
+                jy = fmaf(val, uy, jy);
+                const float pxx = ux * ux, pxy = ux * uy, pyy = uy * uy;
+                const float sv = val * c.v, wv = val * c.dv;
+                axx = fmaf(sv, pxx, axx);
+                axy = fmaf(sv, pxy, axy);
+                ayy = fmaf(sv, pyy, ayy);
+                t0 = fmaf(sv, c.t[0], t0);
+                t1 = fmaf(sv, c.t[1], t1);
+                t2 = fmaf(sv, c.t[2], t2);
+                bxx = fmaf(wv, pxx, bxx);
+                bxy = fmaf(wv, pxy, bxy);
+                byy = fmaf(wv, pyy, byy);
+                tn = fmaf(wv, c.t[3], tn);
+                jn = fmaf(c.sn, E, jn);
             }
-            if (g == total) break;
-            cur = rec;
-            m = jx = jy = j0 = j1 = j2 = jn = 0.f;
         }
-        const FitS& c = sm.comps[g];
-        const float dx = xf - c.mx, dy = yf - c.my;
-        const float e = fmaf(dx, fmaf(c.qxx, dx, c.qxy * dy), c.qyy * dy * dy);
-        const float E = (e >= c.fl) ? tb::ex2(e) : 0.f;
-        const float val = c.s * E;
-        m += val;
+        kb += K;
+        // source done: add its patch inside its rectangle and write its
+        // weighted columns, d/dtheta = 1/2 (dM : sum v val u u^T - sum v val tr(C^-1 dM))
+        const bool in = lane >= R.x0 && lane < R.x1 && warp >= R.y0 && warp < R.y1;
+        const float cnt = R.counts;
+        model += in ? cnt * m : 0.f;
         if (kDeriv) {
-            const float ux = fmaf(c.ixx, dx, c.ixy * dy);
-            const float uy = fmaf(c.ixy, dx, c.iyy * dy);
-            jx = fmaf(val, ux, jx);
-            jy = fmaf(val, uy, jy);
-            const float pxx = ux * ux, pxy = ux * uy, pyy = uy * uy;
-            j0 = fmaf(val, fmaf(c.dxx[0], pxx, fmaf(c.dxy2[0], pxy, fmaf(c.dyy[0], pyy, -c.t[0]))), j0);
-            j1 = fmaf(val, fmaf(c.dxx[1], pxx, fmaf(c.dxy2[1], pxy, fmaf(c.dyy[1], pyy, -c.t[1]))), j1);
-            j2 = fmaf(val, fmaf(c.dxx[2], pxx, fmaf(c.dxy2[2], pxy, fmaf(c.dyy[2], pyy, -c.t[2]))), j2);
-            jn = fmaf(val, fmaf(c.dxx[3], pxx, fmaf(c.dxy2[3], pxy, fmaf(c.dyy[3], pyy, -c.t[3]))), jn);
-            jn = fmaf(c.sn, E, jn);
+            const float cw = in ? cnt * w : 0.f;
+            float* col = &A[(q - q0) * kCols][tid];
+            col[0 * kLd] = cw * jx;
+            col[1 * kLd] = cw * jy;
+            col[2 * kLd] = in ? w * m : 0.f;
+            const float h = 0.5f * cw;
+            col[3 * kLd] = h * (fmaf(R.dM[0][0], axx, fmaf(2.f * R.dM[0][1], axy, R.dM[0][2] * ayy)) - t0);
+            col[4 * kLd] = h * (fmaf(R.dM[1][0], axx, fmaf(2.f * R.dM[1][1], axy, R.dM[1][2] * ayy)) - t1);
+            col[5 * kLd] = h * (fmaf(R.dM[2][0], axx, fmaf(2.f * R.dM[2][1], axy, R.dM[2][2] * ayy)) - t2);
+            col[6 * kLd] = h * (fmaf(R.M[0], bxx, fmaf(2.f * R.M[1], bxy, R.M[2] * byy)) - tn) +
+                           cw * jn;
         }
     }
     __syncthreads();   // columns complete
@@ -497,6 +515,12 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
                     R.src = lane;
                     R.K = S.K[u.band];
                     R.pad = 0;
+#pragma unroll
+                    for (int q = 0; q < 3; q++) {
+                        R.M[q] = S.M[q];
+#pragma unroll
+                        for (int j = 0; j < 3; j++) R.dM[j][q] = S.dM[j][q];
+                    }
                     sm.recs[q] = R;
                 }
                 if (lane == 0) sm.nrec = __popc(bal);
