@@ -257,6 +257,7 @@ struct PassSmem {
     FitS comps[kStageMax];
     TileRec recs[TB_FIT_MAX_SRC];
     float r[kThreads];
+    float runred[kThreads / 32][36];
     double red[kThreads / 32];
     int64_t slot;
     int nrec;
@@ -266,20 +267,20 @@ struct PassSmem {
 // Evaluates sources [q0, q0 + nq) of the tile list at this thread's pixel.
 // kDeriv: writes the 7 weighted columns of each source into `A` (column
 // 7 (q - q0) + c) and returns the model; otherwise returns the model only.
+// Every source of the group has components (a unit with a source that has
+// none is skipped), so each of the group's 7 nq columns is written.
+// need_sync: other threads may still read comps / A (a second group of the
+// same tile); the first group of a tile follows a barrier already.
 template <bool kDeriv>
 __device__ float eval_group(PassSmem& sm, const FitC* __restrict__ gcomps, int src0, int band,
                             int n_bands, int q0, int nq, int ox, int oy, float w,
-                            float (*A)[kLd]) {
+                            float (*A)[kLd], bool need_sync) {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    // zero this group's columns (each thread its own pixel)
-    if (kDeriv) {
-        for (int c = 0; c < nq * kCols; c++) A[c][tid] = 0.f;
-    }
     // stage components: record-major, PSF component outer, galaxy inner
     int total = 0;
     for (int q = q0; q < q0 + nq; q++) total += sm.recs[q].K;
-    __syncthreads();   // previous users of comps / A are done
+    if (need_sync) __syncthreads();
     for (int g = tid; g < total; g += kThreads) {
         int q = q0, k = g;
         while (k >= sm.recs[q].K) { k -= sm.recs[q].K; q++; }
@@ -365,6 +366,108 @@ __device__ __forceinline__ int col_of(int src, int c, int band, int n_bands) {
     return src * TB_FIT_NPAR + off;
 }
 
+// One source on this tile (the common case): model and the 7 weighted
+// derivative columns at this thread's pixel, returned in registers (J),
+// with the source's record built by every thread from the tables.  Two
+// barriers: after staging and at the end (the next tile restages).
+__device__ float eval_single(PassSmem& sm, const FitC* __restrict__ gcomps,
+                             const tb_fit_source& fs, const SrcTab& S, int src_global, int band,
+                             int n_bands, int ox, int oy, float w, float* J) {
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int K = S.K[band];
+    for (int g = tid; g < K; g += kThreads) {
+        const FitC& c = gcomps[((int64_t)src_global * n_bands + band) * kCompStride + g];
+        FitS f;
+        f.mx = (float)(c.mx - (double)ox);
+        f.my = (float)(c.my - (double)oy);
+        f.qxx = c.qxx; f.qxy = c.qxy; f.qyy = c.qyy;
+        f.ixx = c.ixx; f.ixy = c.ixy; f.iyy = c.iyy;
+        f.s = c.s; f.sn = c.sn; f.fl = c.fl; f.v = c.v; f.dv = c.dv;
+#pragma unroll
+        for (int j = 0; j < 4; j++) f.t[j] = c.t[j];
+        f.pad[0] = f.pad[1] = f.pad[2] = 0;
+        sm.comps[g] = f;
+    }
+    __syncthreads();
+    const float xf = (float)lane, yf = (float)warp;
+    float m = 0.f, jx = 0.f, jy = 0.f, jn = 0.f;
+    float axx = 0.f, axy = 0.f, ayy = 0.f, t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    float bxx = 0.f, bxy = 0.f, byy = 0.f, tn = 0.f;
+#pragma unroll 2
+    for (int g = 0; g < K; g++) {
+        const FitS& c = sm.comps[g];
+        const float dx = xf - c.mx, dy = yf - c.my;
+        const float e = fmaf(dx, fmaf(c.qxx, dx, c.qxy * dy), c.qyy * dy * dy);
+        const float E = (e >= c.fl) ? tb::ex2(e) : 0.f;
+        const float val = c.s * E;
+        m += val;
+        const float ux = fmaf(c.ixx, dx, c.ixy * dy);
+        const float uy = fmaf(c.ixy, dx, c.iyy * dy);
+        jx = fmaf(val, ux, jx);
+        jy = fmaf(val, uy, jy);
+        const float pxx = ux * ux, pxy = ux * uy, pyy = uy * uy;
+        const float sv = val * c.v, wv = val * c.dv;
+        axx = fmaf(sv, pxx, axx);
+        axy = fmaf(sv, pxy, axy);
+        ayy = fmaf(sv, pyy, ayy);
+        t0 = fmaf(sv, c.t[0], t0);
+        t1 = fmaf(sv, c.t[1], t1);
+        t2 = fmaf(sv, c.t[2], t2);
+        bxx = fmaf(wv, pxx, bxx);
+        bxy = fmaf(wv, pxy, bxy);
+        byy = fmaf(wv, pyy, byy);
+        tn = fmaf(wv, c.t[3], tn);
+        jn = fmaf(c.sn, E, jn);
+    }
+    __syncthreads();   // comps are restaged by the next tile
+    const int px = ox + lane, py = oy + warp;
+    const bool in = px >= fs.x0 && px < fs.x0 + fs.w && py >= fs.y0 && py < fs.y0 + fs.h;
+    const float cnt = (float)S.flux[band];
+    const float cw = in ? cnt * w : 0.f;
+    const float h = 0.5f * cw;
+    J[0] = cw * jx;
+    J[1] = cw * jy;
+    J[2] = in ? w * m : 0.f;
+    J[3] = h * (fmaf(S.dM[0][0], axx, fmaf(2.f * S.dM[0][1], axy, S.dM[0][2] * ayy)) - t0);
+    J[4] = h * (fmaf(S.dM[1][0], axx, fmaf(2.f * S.dM[1][1], axy, S.dM[1][2] * ayy)) - t1);
+    J[5] = h * (fmaf(S.dM[2][0], axx, fmaf(2.f * S.dM[2][1], axy, S.dM[2][2] * ayy)) - t2);
+    J[6] = h * (fmaf(S.M[0], bxx, fmaf(2.f * S.M[1], bxy, S.M[2] * byy)) - tn) + cw * jn;
+    return in ? cnt * m : 0.f;
+}
+
+// Adds a single-source run's register accumulators (this thread's share of
+// the 7 x 7 block's upper triangle and of A^T r) into the owned H / g:
+// warp reductions, then a fixed-order sum over warps.
+__device__ void flush_run(PassSmem& sm, float* hacc, float* gacc, int src, double* H, double* g,
+                          int P, int band, int n_bands) {
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int v = 0; v < 35; v++) {
+        float x = v < 28 ? hacc[v] : gacc[v - 28];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sm.runred[warp][v] = x;
+    }
+    __syncthreads();
+    if (tid < 35) {
+        double sum = 0.0;
+        for (int w2 = 0; w2 < kThreads / 32; w2++) sum += (double)sm.runred[w2][tid];
+        if (tid < 28) {
+            // upper-triangle index tid -> (c, c'), row-major over c <= c'
+            int c = 0, base = 0;
+            while (base + (kCols - c) <= tid) { base += kCols - c; c++; }
+            const int c2 = c + (tid - base);
+            const int r = col_of(src, c, band, n_bands), cc = col_of(src, c2, band, n_bands);
+            H[(int64_t)r * P + cc] += sum;
+        } else {
+            g[col_of(src, tid - 28, band, n_bands)] += sum;
+        }
+    }
+    __syncthreads();
+}
+
 // Adds A_a^T A_b (columns of groups a and b) into the owned H block: each
 // warp takes 2 x 2 blocks of column pairs and splits the tile's pixels over
 // its lanes (conflict-free consecutive shared-memory reads), then reduces.
@@ -419,7 +522,7 @@ __device__ void add_grad(PassSmem& sm, float (*A)[kLd], int q0, int nq, double* 
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) g[col_of(sm.recs[q0 + c / kCols].src, c % kCols, band, n_bands)] += (double)s;
     }
-    __syncthreads();
+    // no barrier: add_block only reads what this function reads
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -480,7 +583,7 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
             d = 0.f;
             w = 0.f;
             if (t >= n_t) return;
-            const int px = (tl[t] & 0xffff) * kTileW + lane, py = (tl[t] >> 16) * kTileH + warp;
+            const int px = (tl[t] & 0x3ff) * kTileW + lane, py = ((tl[t] >> 10) & 0x3ff) * kTileH + warp;
             if (px < u.W && py < u.H) {
                 const int64_t pix = u.pix_off + (int64_t)py * u.W + px;
                 d = data[pix];
@@ -489,10 +592,39 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
         };
         float d_next, w_next;
         load_px(0, d_next, w_next);
+        // single-source runs: this thread's pixel contributions to the run's
+        // 7 x 7 block (upper triangle) and gradient
+        int run_src = -1;
+        float hacc[28], gacc[7];
         for (int t = 0; t < n_t; t++) {
-            const int ox = (tl[t] & 0xffff) * kTileW, oy = (tl[t] >> 16) * kTileH;
+            const int ox = (tl[t] & 0x3ff) * kTileW, oy = ((tl[t] >> 10) & 0x3ff) * kTileH;
+            const int single = mode == 0 ? ((tl[t] >> 20) & 0xff) - 1 : -1;
             const float d = d_next, w = w_next;
             load_px(t + 1, d_next, w_next);   // prefetch the next tile's pixel
+            if (single != run_src) {
+                if (run_src >= 0) flush_run(sm, hacc, gacc, run_src, H, g, P, u.band, n_bands);
+                run_src = single;
+#pragma unroll
+                for (int v = 0; v < 28; v++) hacc[v] = 0.f;
+#pragma unroll
+                for (int v = 0; v < 7; v++) gacc[v] = 0.f;
+            }
+            if (single >= 0 && single < nsrc) {
+                float J[7];
+                const float model = eval_single(sm, gcomps, srcs[b.src0 + single],
+                                                tab[b.src0 + single], b.src0 + single, u.band,
+                                                n_bands, ox, oy, w, J);
+                const float rr = (d - model) * w;
+                chi2 += (double)(rr * rr);
+                int v = 0;
+#pragma unroll
+                for (int c = 0; c < kCols; c++) {
+                    gacc[c] = fmaf(J[c], rr, gacc[c]);
+#pragma unroll
+                    for (int c2 = c; c2 < kCols; c2++, v++) hacc[v] = fmaf(J[c], J[c2], hacc[v]);
+                }
+                continue;
+            }
             // sources whose rectangle meets this tile (source order)
             if (warp == 0) {
                 bool hit = false;
@@ -537,12 +669,12 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
             float model;
             if (ngroups == 1) {
                 model = eval_group<true>(sm, gcomps, b.src0, u.band, n_bands, 0, R, ox, oy, w,
-                                         sm.A[0]);
+                                         sm.A[0], false);
             } else {
                 model = 0.f;
                 for (int q0 = 0; q0 < R; q0 += kG)
                     model += eval_group<false>(sm, gcomps, b.src0, u.band, n_bands, q0,
-                                               min(kG, R - q0), ox, oy, w, sm.A[0]);
+                                               min(kG, R - q0), ox, oy, w, sm.A[0], q0 > 0);
             }
             const float rr = (d - model) * w;
             chi2 += (double)(rr * rr);
@@ -552,17 +684,18 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
                 const int qa = ga * kG, na = min(kG, R - qa);
                 if (ngroups > 1)
                     eval_group<true>(sm, gcomps, b.src0, u.band, n_bands, qa, na, ox, oy, w,
-                                     sm.A[0]);
+                                     sm.A[0], true);
                 add_grad(sm, sm.A[0], qa, na, g, u.band, n_bands);
                 add_block(sm, sm.A[0], qa, na, sm.A[0], qa, na, true, H, P, u.band, n_bands);
                 for (int gb = ga + 1; gb < ngroups; gb++) {
                     const int qb = gb * kG, nb = min(kG, R - qb);
                     eval_group<true>(sm, gcomps, b.src0, u.band, n_bands, qb, nb, ox, oy, w,
-                                     sm.A[1]);
+                                     sm.A[1], true);
                     add_block(sm, sm.A[0], qa, na, sm.A[1], qb, nb, false, H, P, u.band, n_bands);
                 }
             }
         }
+        if (run_src >= 0) flush_run(sm, hacc, gacc, run_src, H, g, P, u.band, n_bands);
         // chi^2 of the unit: fixed-order block reduction
         for (int o = 16; o > 0; o >>= 1) chi2 += __shfl_xor_sync(0xffffffffu, chi2, o);
         if (lane == 0) sm.red[warp] = chi2;

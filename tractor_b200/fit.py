@@ -238,23 +238,35 @@ class BlobFitter(object):
 
 
 def blob_tiles(sides, sources, blob_src):
-    """Per blob, its 32 x 8 tiles (tx | ty << 16): first those some source
-    mask reaches, then the others.  Returns (tiles, n_active, n_tiles)."""
+    """Per blob, its 32 x 8 tiles, encoded tx | ty << 10 | (s + 1) << 20:
+    first the tiles exactly one source mask reaches (s, grouped by source:
+    the fitting pass accumulates such runs in registers), then the tiles
+    several masks reach (s + 1 = 0), then the others.  Returns (tiles,
+    n_active, n_tiles)."""
     sides = np.asarray(sides, np.int64).reshape(-1, 2)
     out, n_act, n_all = [], [], []
     for b in range(len(sides)):
         W, H = sides[b]
         tx_n, ty_n = (W + 31) // 32, (H + 7) // 8
-        grid = np.zeros((ty_n, tx_n), bool)
-        for r in sources[blob_src[b]:blob_src[b + 1]]:
+        count = np.zeros((ty_n, tx_n), np.int32)
+        last = np.full((ty_n, tx_n), -1, np.int32)
+        for k, r in enumerate(sources[blob_src[b]:blob_src[b + 1]]):
             x0, x1 = max(r['x0'], 0), min(r['x0'] + r['w'], W)
             y0, y1 = max(r['y0'], 0), min(r['y0'] + r['h'], H)
             if x1 > x0 and y1 > y0:
-                grid[y0 // 8:(y1 - 1) // 8 + 1, x0 // 32:(x1 - 1) // 32 + 1] = True
-        ty, tx = np.nonzero(grid)
-        pty, ptx = np.nonzero(~grid)
-        out.append(np.concatenate([tx | (ty << 16), ptx | (pty << 16)]).astype(np.int32))
-        n_act.append(len(ty))
+                sl = (slice(y0 // 8, (y1 - 1) // 8 + 1), slice(x0 // 32, (x1 - 1) // 32 + 1))
+                count[sl] += 1
+                last[sl] = k
+        ty, tx = np.nonzero(count == 1)
+        src = last[ty, tx]
+        order = np.lexsort((tx, ty, src))
+        single = tx[order] | (ty[order] << 10) | ((src[order] + 1) << 20)
+        my, mx = np.nonzero(count > 1)
+        multi = mx | (my << 10)
+        py_, px_ = np.nonzero(count == 0)
+        passive = px_ | (py_ << 10)
+        out.append(np.concatenate([single, multi, passive]).astype(np.int32))
+        n_act.append(len(single) + len(multi))
         n_all.append(tx_n * ty_n)
     return np.concatenate(out), np.array(n_act, np.int32), np.array(n_all, np.int32)
 
