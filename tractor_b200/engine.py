@@ -181,10 +181,115 @@ class Tractor(MultiParams):
             return mod
         return finish
 
+    # Catalogs at least this large on an eligible image go through the scene
+    # renderer (tb_scene_render) instead of per-source patches.
+    SCENE_MIN_SOURCES = 64
+
     def getModelImage(self, img, srcs=None, sky=True, minsb=None, **kwargs):
-        """engine.py:424-445: all sources rendered in one batched launch."""
+        """engine.py:424-445: all sources rendered in one batched launch --
+        for large catalogs with rectangular model masks on a MoG-PSF image,
+        one scene render of the whole image (tb_scene_render); otherwise
+        per-source patches batched into one launch per kernel type."""
+        if _isint(img):
+            img = self.getImage(img)
+        if not kwargs:
+            mod = self._scene_model(img, self.catalog if srcs is None else srcs, sky, minsb)
+            if mod is not None:
+                return mod
         plan = RenderPlan()
         return self._plan_model_image(plan, img, srcs=srcs, sky=sky, minsb=minsb, **kwargs)()
+
+    def _scene_records(self, img, srcs, minsb):
+        """SCENE_SRC records of `srcs` on `img`, or None when the scene
+        renderer does not reproduce getModelImage's per-source path here."""
+        from . import _lib, psf as psfmod, sources as S, ellipses as E
+        from .basics import NullWCS
+        from .patch import ModelMask
+        psf = img.getPsf()
+        if not hasattr(psf, 'getMixtureOfGaussians') or isinstance(psf, psfmod.HybridPSF):
+            return None
+        if not isinstance(img.getWcs(), NullWCS) or self.modelMasks is None:
+            return None
+        if (img.modelMinval if minsb is None else minsb) != 0.:
+            return None
+        rows = []
+        for src in srcs:
+            if src is None:
+                continue
+            mask = self._getModelMaskFor(img, src)
+            if mask is None:
+                if self.expectModelMasks:
+                    continue
+                return None
+            if not isinstance(mask, ModelMask) or mask.mask is not None:
+                return None
+            counts = S._counts(img, src.getBrightness()) if hasattr(src, 'getBrightness') else None
+            if counts is None or not np.isfinite(np.float32(counts)):
+                return None
+            if counts == 0:
+                continue
+            r = np.zeros(1, _lib.SCENE_SRC)[0]
+            px, py = img.getWcs().positionToPixel(src.getPosition(), src)
+            r['px'], r['py'], r['counts'] = px, py, counts
+            r['mx0'], r['my0'], r['mw'], r['mh'] = mask.x0, mask.y0, mask.w, mask.h
+            shapes = []
+            if isinstance(src, S.PointSource):
+                r['profile'] = _lib.PROFILE_POINT
+            elif isinstance(src, S.FixedCompositeGalaxy):
+                r['profile'] = _lib.PROFILE_COMPOSITE
+                r['fdev'] = src.fracDev.clipped()
+                shapes = [src.shapeExp, src.shapeDev]
+            elif isinstance(src, S.SersicGalaxy):
+                r['profile'] = _lib.PROFILE_SERSIC
+                r['sersic_n'] = src.sersicindex.val
+                shapes = [src.shape]
+            elif isinstance(src, (S.ExpGalaxy, S.DevGalaxy, S.GaussianGalaxy)):
+                r['profile'] = {S.ExpGalaxy: _lib.PROFILE_EXP, S.DevGalaxy: _lib.PROFILE_DEV,
+                                S.GaussianGalaxy: _lib.PROFILE_GAUSSIAN}[type(src)]
+                shapes = [src.shape]
+            else:
+                return None
+            kinds = set()
+            for k, sh in enumerate(shapes):
+                if isinstance(sh, E.EllipseESoft):
+                    kinds.add(_lib.SHAPE_ELLIPSE_ESOFT)
+                elif isinstance(sh, E.EllipseE):
+                    kinds.add(_lib.SHAPE_ELLIPSE_E)
+                elif isinstance(sh, E.GalaxyShape):
+                    kinds.add(_lib.SHAPE_RABPHI)
+                else:
+                    return None
+                vals = [float(v) for v in sh.getAllParams()]
+                pre = 'sa' if k == 0 else 'sb'
+                r[pre + '0'], r[pre + '1'], r[pre + '2'] = vals
+            if len(kinds) > 1:
+                return None
+            r['shape_type'] = kinds.pop() if kinds else _lib.SHAPE_ELLIPSE_E
+            rows.append(r)
+        return np.array(rows, _lib.SCENE_SRC) if rows else np.zeros(0, _lib.SCENE_SRC)
+
+    def _scene_model(self, img, srcs, sky, minsb):
+        srcs = [s for s in srcs if s is not None]
+        if len(srcs) < self.SCENE_MIN_SOURCES or self.modtype != np.float32:
+            return None
+        recs = self._scene_records(img, srcs, minsb)
+        if recs is None:
+            return None
+        from . import batch
+        psf = img.getPsf()
+        mog = psf.getMixtureOfGaussians()
+        H, W = img.getModelShape()
+        cd = img.getWcs().cdInverseAtPixel(0, 0)
+        scene = batch.SceneImage(W, H, np.asarray(mog.amp, np.float64),
+                                 np.asarray(mog.mean, np.float64), np.asarray(mog.var, np.float64),
+                                 pixscale=img.getWcs().pixscale_at(0, 0), cd_inv=cd)
+        mod = np.zeros((H, W), np.float32)
+        if sky:
+            img.getSky().addTo(mod)
+        if len(recs):
+            r = batch.SceneRenderer([scene], comp_stride=16 * max(len(mog.amp), 1))
+            mod += r.image(r.render(recs).numpy(), 0)
+        return mod
 
     def getModelImages(self, **kwargs):
         plan = RenderPlan()
