@@ -240,6 +240,53 @@ def main():
     assert mod5.dtype == np.float32
     np.savez_compressed(os.path.join(OUT, 'scene_mog.npz'), sources=np.array(rows),
                         psf_amp=pamp, psf_sigma=psig, shape=np.array([H, W]), model=mod5)
+    # -- 6. Forced photometry: 6 sources of fixed shape / position seen in
+    #       two 64 x 72 images of one band (different PSFs and photometric
+    #       scales), fluxes fitted, with variance -------------------------
+    rng = np.random.default_rng(600)
+    H6, W6 = 64, 72
+    psf6 = [NCircularGaussianPSF([1.2, 2.6], [0.75, 0.25]),
+            GaussianMixturePSF(np.array([0.6, 0.3, 0.1]), np.zeros((3, 2)),
+                               np.array([np.eye(2) * s ** 2 for s in (1.5, 3.0, 6.0)]))]
+    scales6 = [1.0, 2.5]
+    rows6, srcs6 = [], []
+    for i in range(6):
+        kind = i % 3
+        px, py = rng.uniform(8, W6 - 8), rng.uniform(8, H6 - 8)
+        fl = rng.uniform(50., 500., 1)
+        re = float(rng.uniform(1., 3.))
+        e1, e2 = rng.uniform(-0.3, 0.3, 2)
+        br = Flux(fl[0])
+        if kind == 0:
+            s = PointSource(PixPos(px, py), br)
+        elif kind == 1:
+            s = ExpGalaxy(PixPos(px, py), br, EllipseE(re, e1, e2))
+        else:
+            s = DevGalaxy(PixPos(px, py), br, EllipseE(re, e1, e2))
+        rows6.append([kind, px, py, fl[0], re, e1, e2])
+        srcs6.append(s)
+    tims6 = []
+    for b in range(2):
+        tim = Image(data=np.zeros((H6, W6), np.float32), inverr=np.ones((H6, W6), np.float32),
+                    psf=psf6[b], photocal=LinearPhotoCal(scales6[b]))
+        tims6.append(tim)
+    trt = Tractor(tims6, srcs6)
+    trt.freezeParam('images')
+    datas6 = []
+    for b, tim in enumerate(tims6):
+        clean = trt.getModelImage(b)
+        tim.data = (clean + rng.normal(size=clean.shape) * 0.5).astype(np.float32)
+        tim.inverr = np.full((H6, W6), 2., np.float32)
+        datas6.append(tim.data.copy())
+    # start from wrong fluxes, shapes and positions frozen
+    for s in srcs6:
+        s.freezeAllBut('brightness')
+        s.brightness.setParams([v * 0.7 + 5. for v in s.brightness.getParams()])
+    start6 = np.array(trt.getParams())
+    R = trt.optimize_forced_photometry(variance=True, shared_params=False)
+    np.savez_compressed(os.path.join(OUT, 'forced_phot.npz'), sources=np.array(rows6),
+                        data=np.stack(datas6), scales=np.array(scales6), start=start6,
+                        fluxes=np.array(trt.getParams()), IV=np.array(R.IV))
     print('golden fixtures written to', OUT)
 
 

@@ -1,0 +1,143 @@
+"""Forced photometry (Tractor.optimize_forced_photometry through
+B200Optimizer.forced_photometry): the reference's own known answers
+(test/test_forced_phot.py:69-147) and a multi-source, two-image fit against
+the reference itself (tests/golden/forced_phot.npz, made by
+tests/golden/make_golden.py).  Runs on the host stand-ins and on the GPU."""
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), 'golden')
+
+
+@pytest.fixture(params=['host', pytest.param('gpu', marks=pytest.mark.gpu)])
+def backend(request, monkeypatch):
+    if request.param == 'host':
+        import fake_device
+        fake_device.install(monkeypatch)
+    else:
+        request.getfixturevalue('tb')
+    from tractor_b200 import render
+    render._spectra.cache.clear()
+    return request.param
+
+
+def _constant_source_classes():
+    import tractor_b200 as T
+    from tractor_b200.patch import Patch
+
+    class ConstantSource(T.MultiParams, T.BasicSource):
+        """A source whose unit-flux model is 1 on every pixel (the
+        reference test's ConstantSource)."""
+
+        def __init__(self, br):
+            super(ConstantSource, self).__init__(br)
+
+        @staticmethod
+        def getNamedParams():
+            return dict(brightness=0)
+
+        def getBrightness(self):
+            return self.brightness
+
+        def getBrightnesses(self):
+            return [self.brightness]
+
+        def getUnitFluxModelPatches(self, img, modelMask=None, **kwargs):
+            shape = img.shape if modelMask is None else modelMask.shape
+            return [Patch(0, 0, np.ones(shape, np.float32))]
+
+        def getModelPatch(self, img, modelMask=None, **kwargs):
+            counts = img.getPhotoCal().brightnessToCounts(self.brightness)
+            if counts == 0:
+                return None
+            return self.getUnitFluxModelPatches(img, modelMask=modelMask)[0] * counts
+
+        def _plan_model_patch(self, plan, img, modelMask=None, **kwargs):
+            from tractor_b200.plan import done
+            return done(self.getModelPatch(img, modelMask=modelMask))
+
+    class ConstantSourceWithPrior(T.GaussianPriorsMixin, ConstantSource):
+        priorStd = 1.
+
+        def __init__(self, *args, **kwargs):
+            super(ConstantSourceWithPrior, self).__init__(*args, **kwargs)
+            self.gpriors.add('brightness', 0., self.priorStd, param=self)
+
+    return ConstantSource, ConstantSourceWithPrior
+
+
+def _pixel_tim(val):
+    import tractor_b200 as T
+    return T.Image(data=np.zeros((1, 1), np.float32) + val, inverr=np.ones((1, 1), np.float32),
+                   photocal=T.LinearPhotoCal(1.))
+
+
+def test_pixel(backend):
+    """test_forced_phot.py:69-88."""
+    import tractor_b200 as T
+    ConstantSource, _ = _constant_source_classes()
+    tim = _pixel_tim(42.)
+    src = ConstantSource(T.Flux(10.))
+    tr = T.Tractor([tim], [src])
+    tr.freezeParam('images')
+    tr.optimize_forced_photometry()
+    assert abs(src.getParams()[0] - 42.) < 1e-6
+
+
+def test_pixel_with_prior(backend):
+    """test_forced_phot.py:90-147: a Gaussian prior of sigma 1 at 0 halves
+    the fitted value; with inverr 2 the fit is the inverse-variance mean."""
+    import tractor_b200 as T
+    ConstantSource, ConstantSourceWithPrior = _constant_source_classes()
+    val = 4.
+    tim = _pixel_tim(val)
+    src = ConstantSource(T.Flux(0.))
+    tr = T.Tractor([tim], [src])
+    tr.freezeParam('images')
+    tr.optimize_forced_photometry()
+    assert abs(src.getParams()[0] - val) < 1e-6
+    src = ConstantSourceWithPrior(T.Flux(0.))
+    tr = T.Tractor([tim], [src])
+    tr.freezeParam('images')
+    tr.optimize_forced_photometry(priors=True)
+    assert abs(src.getParams()[0] - val / 2.) < 1e-6
+    src.setParams([1.])
+    tr.optimize_forced_photometry(priors=True)
+    assert abs(src.getParams()[0] - val / 2.) < 1e-6
+    tim.inverr[:, :] = 2.
+    src.setParams([0.])
+    tr.optimize_forced_photometry(priors=True)
+    pval = (4. * val) / (4. + 1.)
+    assert abs(src.getParams()[0] - pval) < 1e-6
+
+
+def test_fluxes_and_variance_match_reference(backend):
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'forced_phot.npz'))
+    H, W = g['data'].shape[1:]
+    psfs = [T.NCircularGaussianPSF([1.2, 2.6], [0.75, 0.25]),
+            T.GaussianMixturePSF(np.array([0.6, 0.3, 0.1]), np.zeros((3, 2)),
+                                 np.array([np.eye(2) * s ** 2 for s in (1.5, 3.0, 6.0)]))]
+    tims = [T.Image(data=g['data'][b], inverr=np.full((H, W), 2., np.float32), psf=psfs[b],
+                    photocal=T.LinearPhotoCal(float(g['scales'][b]))) for b in range(2)]
+    srcs = []
+    for kind, px, py, fl, re, e1, e2 in g['sources']:
+        pos, br = T.PixPos(px, py), T.Flux(fl)
+        if int(kind) == 0:
+            s = T.PointSource(pos, br)
+        elif int(kind) == 1:
+            s = T.ExpGalaxy(pos, br, T.EllipseE(re, e1, e2))
+        else:
+            s = T.DevGalaxy(pos, br, T.EllipseE(re, e1, e2))
+        srcs.append(s)
+    tr = T.Tractor(tims, srcs)
+    tr.freezeParam('images')
+    for s in srcs:
+        s.freezeAllBut('brightness')
+    tr.setParams(g['start'])
+    R = tr.optimize_forced_photometry(variance=True, shared_params=False)
+    got = np.array(tr.getParams())
+    assert np.allclose(got, g['fluxes'], rtol=1e-5, atol=0), (got, g['fluxes'])
+    assert np.allclose(R.IV, g['IV'], rtol=1e-4), (R.IV, g['IV'])

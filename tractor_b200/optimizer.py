@@ -21,6 +21,10 @@ from . import render
 from .plan import RenderPlan
 
 
+class OptResult(object):
+    """Results of a forced-photometry fit (optimize.py: OptResult)."""
+
+
 def default_alphas():
     """1/1024 .. 1 in factors of 2, then sqrt(2), 2 (optimize.py:426-428)."""
     return np.append(2. ** np.arange(-10, 1), [np.sqrt(2.), 2.])
@@ -244,8 +248,183 @@ class B200Optimizer(object):
         R.update(steps=step)
         return R
 
-    def forced_photometry(self, tractor, **kwargs):
-        raise NotImplementedError('forced photometry is not provided by this optimizer')
+    # -- forced photometry (optimize.py:16-146, lsqr_optimizer.py:11-251) ---
+    def forced_photometry(self, tractor, alphas=None, damp=0, priors=False, minsb=0.,
+                          mindlnp=1., rois=None, sky=False, minFlux=None, fitstats=False,
+                          fitstat_extras=None, justims0=False, variance=False,
+                          skyvariance=False, shared_params=True, nonneg=False,
+                          nilcounts=-1e30, wantims=True, negfluxval=None, **kwargs):
+        """Linear fit of the thawed sources' brightnesses with every other
+        parameter fixed: unit-flux models of all (image, source) pairs
+        rendered in one batch, the frozen sources' model as the base, then the
+        reference's loop -- an unscaled least-squares update on the device
+        (getUpdateDirection with chi images of the current fluxes), alpha = 1
+        when the fluxes stay above minFlux, otherwise the line search with
+        growing damping -- until the gain is below mindlnp.  Returns an
+        OptResult with ims0 / ims1 (img, model, inverr, chi, roi) and, with
+        variance=True, IV: the inverse variance of each flux."""
+        if sky or fitstats or rois is not None or nonneg or justims0:
+            raise NotImplementedError('forced photometry with sky fitting, fit statistics, ROIs, '
+                                      'non-negativity or justims0 is not provided')
+        from .basics import LinearPhotoCal
+        result = OptResult()
+        imgs = list(tractor.getImages())
+        scales = []
+        for img in imgs:
+            assert isinstance(img.getPhotoCal(), LinearPhotoCal)
+            scales.append(img.getPhotoCal().getScale())
+        srcs = list(tractor.catalog.getThawedSources())
+        nparams = tractor.catalog.numberOfParams()
+        umodels = self._unit_models(tractor, srcs, imgs, minsb, **kwargs)
+        for um in umodels:
+            assert len(um) == nparams
+        fsrcs = list(tractor.catalog.getFrozenSources())
+        mod0 = [tractor.getModelImage(img, fsrcs, minsb=minsb, sky=True) for img in imgs]
+        derivs = [[] for _ in range(nparams)]
+        for img, umods, scale in zip(imgs, umodels, scales):
+            for um, dd in zip(umods, derivs):
+                if um is not None:
+                    dd.append((um * scale, img))
+        lnp0, chis0, ims0 = None, None, None
+        imsBest = None
+        damp0 = 1e-3
+        damping = damp
+        while True:
+            tryAgain = False
+            quitNow = False
+            p0 = tractor.getParams()
+            if lnp0 is None:
+                lnp0, chis0, ims0 = self._lnp_for_update(tractor, mod0, imgs, umodels, None, None,
+                                                         p0, scales, priors, minFlux)
+                assert np.isfinite(lnp0)
+            X = self.getUpdateDirection(tractor, derivs, damp=damping, priors=priors,
+                                        scale_columns=False, chiImages=chis0,
+                                        shared_params=shared_params)
+            if X is None or len(X) == 0:
+                break
+            trial = alphas
+            if trial is None:
+                trial = default_alphas()
+            if minFlux is None or np.all((np.array(p0) + X) >= minFlux):
+                trial = [1.]
+                quitNow = True
+            elif damp == 0.:
+                damping = damp0
+                damp0 *= 10.
+                if damp0 < 1e3:
+                    tryAgain = True
+            lnpBest, alphaBest, chiBest = lnp0, None, None
+            for alpha in trial:
+                lnp, chis, ims = self._lnp_for_update(tractor, mod0, imgs, umodels, X, alpha, p0,
+                                                      scales, priors, minFlux)
+                if lnp < lnpBest - 1. or not np.isfinite(lnp):
+                    break
+                if lnp > lnpBest:
+                    alphaBest, lnpBest, chiBest, imsBest = alpha, lnp, chis, ims
+            if alphaBest is not None:
+                pa = [p + alphaBest * d for p, d in zip(p0, X)]
+                if minFlux is not None:
+                    pa = [max(minFlux, v) for v in pa]
+                tractor.catalog.setParams(pa)
+                dlogprob = lnpBest - lnp0
+                lnp0, chis0 = lnpBest, chiBest
+            else:
+                dlogprob = 0.
+            if dlogprob < mindlnp and not tryAgain:
+                break
+            if quitNow:
+                break
+        if wantims:
+            result.ims0 = ims0
+            result.ims1 = imsBest
+        if variance:
+            result.IV = self._flux_iv(imgs, umodels, scales, nparams)
+        return result
+
+    def _unit_models(self, tractor, srcs, imgs, minsb, **kwargs):
+        """(n_images, n_params) unit-flux patches (Optimizer._get_umodels,
+        optimize.py:147-219), rendered in one batch where the source can
+        plan its renders."""
+        plan = RenderPlan()
+        pend = []
+        for img in imgs:
+            pcal = img.getPhotoCal()
+            row = []
+            for src in srcs:
+                counts = sum([pcal.brightnessToCounts(b) for b in src.getBrightnesses()])
+                mv = 1e-3 if counts <= 0 else minsb / counts
+                mask = tractor._getModelMaskFor(img, src)
+                if hasattr(src, '_plan_unit_patch'):
+                    row.append(('plan', src._plan_unit_patch(plan, img, minval=mv, modelMask=mask,
+                                                             **kwargs)))
+                else:
+                    row.append(('list', src.getUnitFluxModelPatches(img, minval=mv,
+                                                                   modelMask=mask, **kwargs)))
+            pend.append(row)
+        umodels = []
+        for row in pend:
+            umods = []
+            for kind, v in row:
+                ums = [v.result()] if kind == 'plan' else list(v)
+                for um in ums:
+                    if um is not None and um.patch is not None:
+                        assert np.all(np.isfinite(um.patch))
+                umods.extend(ums)
+            umodels.append(umods)
+        return umodels
+
+    @staticmethod
+    def _getims(fluxes, imgs, umodels, mod0, scales, minFlux):
+        """Model, inverr and chi images at the given fluxes (optimize.py:472-530)."""
+        ims = []
+        for img, umods, m0, scale in zip(imgs, umodels, mod0, scales):
+            mod = m0.copy()
+            for f, um in zip(fluxes, umods):
+                if um is None or um.patch is None:
+                    continue
+                if minFlux is not None:
+                    f = max(f, minFlux)
+                counts = f * scale
+                if counts == 0.:
+                    continue
+                (um * counts).addTo(mod)
+            ie = img.getInvError()
+            chi = (img.getImage() - mod) * ie
+            ims.append((img, mod, ie, chi, None))
+        return ims
+
+    def _lnp_for_update(self, tractor, mod0, imgs, umodels, X, alpha, p0, scales, priors,
+                        minFlux):
+        pa = p0 if X is None else [p + alpha * d for p, d in zip(p0, X)]
+        lnp = 0.
+        if priors:
+            saved = tractor.getParams()
+            tractor.setParams(pa)
+            lnp += tractor.getLogPrior()
+            tractor.setParams(saved)
+            if not np.isfinite(lnp):
+                return lnp, None, None
+        ims = self._getims(pa, imgs, umodels, mod0, scales, minFlux)
+        chis = [chi for _, _, _, chi, _ in ims]
+        lnp += -0.5 * sum((chi.astype(np.float64) ** 2).sum() for chi in chis)
+        return lnp, chis, ims
+
+    @staticmethod
+    def _flux_iv(imgs, umodels, scales, nparams):
+        """Inverse variance of each flux (Optimizer._get_iv, optimize.py:378-423):
+        sum over images of (unit model x scale x inverr)^2."""
+        IV = np.zeros(nparams)
+        for img, umods, scale in zip(imgs, umodels, scales):
+            ie = img.getInvError()
+            H, W = img.shape
+            for ui, um in enumerate(umods):
+                if um is None or um.patch is None:
+                    continue
+                d = um.copy()
+                if not d.clipTo(W, H) or d.patch is None:
+                    continue
+                IV[ui] += np.sum((d.patch * scale * ie[d.getSlice(img)]) ** 2)
+        return IV
 
 
 class B200ConstrainedOptimizer(B200Optimizer):
