@@ -132,3 +132,49 @@ def test_many_blobs_fit_at_least_as_well_as_truth(tb):
     assert np.all(np.abs(truth / npix - 1) < 0.05)          # noise model sanity
     ok = fitted <= truth + 1.0
     assert np.mean(ok) > 0.95, np.sort(fitted - truth)[-10:]
+
+
+def test_fit_tractors_through_the_object_api(tb, oracle):
+    """fit.fit_tractors: the same blobs given as reference-style Tractor
+    objects (SersicGalaxy, NanoMaggies in g, r, z, EllipseESoft,
+    SersicIndex, model masks) reach the FP64 optimum within 1e-3 sigma, and
+    the parameters are written back into the objects."""
+    import tractor_b200 as T
+    from tractor_b200 import fit
+    w, datas, inverrs = _small_blobs(oracle, 2)
+    bands = ['g', 'r', 'z']
+    tractors = []
+    for b in range(len(datas)):
+        s0, s1, W, H, rects = _blob_args(w, b)
+        tims = []
+        for k in range(3):
+            amp, mean, var = w['psf'][b][k]
+            tims.append(T.Image(data=datas[b][k], inverr=inverrs[b][k],
+                                psf=T.GaussianMixturePSF(amp, mean, var),
+                                photocal=T.LinearPhotoCal(1., band=bands[k])))
+        srcs, masks = [], {}
+        for i in range(s0, s1):
+            th = w['start'][i]
+            src = T.SersicGalaxy(T.PixPos(th[0], th[1]),
+                                 T.NanoMaggies(g=th[2], r=th[3], z=th[4]),
+                                 T.EllipseESoft(th[5], th[6], th[7]), T.SersicIndex(th[8]))
+            srcs.append(src)
+            masks[src] = T.ModelMask(*rects[i - s0])
+        tr = T.Tractor(tims, srcs)
+        tr.setModelMasks([masks] * 3)
+        tractors.append(tr)
+    st = fit.fit_tractors(tractors, tol=1e-7, max_iter=80)
+    assert np.all(st['status'] != 0)
+    for b, tr in enumerate(tractors):
+        s0, s1, W, H, rects = _blob_args(w, b)
+        got = np.array([[s.pos.x, s.pos.y, s.brightness.getFlux('g'), s.brightness.getFlux('r'),
+                         s.brightness.getFlux('z'), s.shape.logre, s.shape.ee1, s.shape.ee2,
+                         s.sersicindex.val] for s in tr.catalog])
+        p, Hf, held = oracle.blob_fit(w['start'][s0:s1], rects, W, H, w['psf'][b], 3,
+                                      datas[b].astype(np.float64),
+                                      inverrs[b].astype(np.float64))
+        free = ~held & (np.diag(Hf) > 0)
+        sig = np.full(p.size, np.inf)
+        sig[free] = np.sqrt(np.diag(np.linalg.inv(Hf[np.ix_(free, free)])))
+        err = np.abs(got - p).ravel() / sig
+        assert err.max() < 1e-3, (b, err.max())

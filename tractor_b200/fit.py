@@ -383,3 +383,123 @@ def render_blobs(w, params, seed=None):
         gen.manual_seed(int(seed))
         out += sig_px * torch.randn(out.shape, generator=gen, device=dev, dtype=torch.float32)
     return out, 1. / sig_px
+
+
+def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
+    """Fits many independent blobs, each given as a reference-style Tractor,
+    in one batched device fit, and writes the fitted parameters back.
+
+    Each Tractor holds 1 to 3 images of one size with NullWCS, a
+    LinearPhotoCal with a band (or no band for a single image) and a
+    mixture-of-Gaussians PSF of at most 4 components, and at most 32
+    sources: SersicGalaxy, ExpGalaxy or DevGalaxy with an EllipseESoft
+    shape, or PointSource, at a PixPos, with a brightness holding one value
+    per image band (Flux for a single image, NanoMaggies / Fluxes
+    otherwise).  Model masks set with Tractor.setModelMasks are used (the
+    same rectangle in every image); without them a source's mask is the
+    whole image.  Every source parameter is fitted (frozen parameters are
+    not honoured).  Returns the per-blob FIT_STATE records."""
+    from . import sources as S, ellipses as E
+    from .basics import NullWCS, LinearPhotoCal
+    from .patch import ModelMask
+    if not tractors:
+        raise ValueError('no blobs')
+    n_bands = max(len(tr.getImages()) for tr in tractors)
+    blob_src, sides, psf, recs, params, datas, inverrs, layout = [0], [], [], [], [], [], [], []
+    cd_inv = None
+    for tr in tractors:
+        imgs = list(tr.getImages())
+        if not 1 <= len(imgs) <= _lib.FIT_MAX_BANDS:
+            raise ValueError('a blob needs 1 to %d images' % _lib.FIT_MAX_BANDS)
+        H, W = imgs[0].shape
+        for img in imgs:
+            if img.shape != (H, W) or not isinstance(img.getWcs(), NullWCS):
+                raise ValueError('blob images must share one shape and a NullWCS')
+            if not isinstance(img.getPhotoCal(), LinearPhotoCal):
+                raise ValueError('blob images need a LinearPhotoCal')
+            if len(imgs) > 1 and img.getPhotoCal().band is None:
+                raise ValueError('several images of a blob need LinearPhotoCal bands')
+            if not hasattr(img.getPsf(), 'getMixtureOfGaussians'):
+                raise ValueError('blob images need a mixture-of-Gaussians PSF')
+            cdi = np.asarray(img.getWcs().cdInverseAtPixel(0, 0), np.float64)
+            if cd_inv is None:
+                cd_inv = cdi
+            elif not np.array_equal(cdi, cd_inv):
+                raise ValueError('all blobs need the same pixel scale')
+        row = []
+        for b in range(n_bands):
+            img = imgs[min(b, len(imgs) - 1)]
+            mog = img.getPsf().getMixtureOfGaussians()
+            row.append((np.asarray(mog.amp, np.float64), np.asarray(mog.mean, np.float64),
+                        np.asarray(mog.var, np.float64)))
+        psf.append(row)
+        sides.append((W, H))
+        for b in range(n_bands):
+            img = imgs[min(b, len(imgs) - 1)]
+            datas.append(np.asarray(img.getImage(), np.float32).ravel())
+            # a missing band: zero weight
+            ie = img.getInvError() if b < len(imgs) else np.zeros((H, W))
+            inverrs.append(np.asarray(ie, np.float32).ravel())
+        srcs = list(tr.catalog)
+        if not 1 <= len(srcs) <= _lib.FIT_MAX_SRC:
+            raise ValueError('a blob needs 1 to %d sources' % _lib.FIT_MAX_SRC)
+        for src in srcs:
+            r = np.zeros(1, _lib.FIT_SOURCE)[0]
+            th = np.zeros(NPAR)
+            if isinstance(src, S.PointSource):
+                r['profile'] = _lib.PROFILE_POINT
+            elif isinstance(src, (S.SersicGalaxy, S.ExpGalaxy, S.DevGalaxy)):
+                if not isinstance(src.shape, E.EllipseESoft):
+                    raise ValueError('galaxies need an EllipseESoft shape')
+                th[5:8] = src.shape.getAllParams()
+                if isinstance(src, S.SersicGalaxy):
+                    r['profile'] = _lib.PROFILE_SERSIC
+                    th[8] = src.sersicindex.val
+                else:
+                    r['profile'] = (_lib.PROFILE_EXP if isinstance(src, S.ExpGalaxy)
+                                    else _lib.PROFILE_DEV)
+            else:
+                raise ValueError('unsupported source %s' % type(src).__name__)
+            px, py = imgs[0].getWcs().positionToPixel(src.getPosition(), src)
+            th[0], th[1] = px, py
+            for b, img in enumerate(imgs):
+                th[2 + b] = img.getPhotoCal().brightnessToCounts(src.getBrightness())
+            mask = tr._getModelMaskFor(imgs[0], src)
+            if mask is None:
+                r['x0'], r['y0'], r['w'], r['h'] = 0, 0, W, H
+            else:
+                if not isinstance(mask, ModelMask) or mask.mask is not None:
+                    raise ValueError('model masks must be rectangles')
+                r['x0'], r['y0'], r['w'], r['h'] = mask.x0, mask.y0, mask.w, mask.h
+            recs.append(r)
+            params.append(th)
+        blob_src.append(blob_src[-1] + len(srcs))
+        layout.append((tr, imgs, srcs))
+    import torch
+    dev = render.device()
+    data = torch.from_numpy(np.concatenate(datas)).to(dev)
+    inv = torch.from_numpy(np.concatenate(inverrs)).to(dev)
+    f = BlobFitter(blob_src, sides, psf, np.array(recs, _lib.FIT_SOURCE), np.array(params),
+                   data, inv, n_bands=n_bands, cd_inv=cd_inv)
+    f.fit(tol=tol, max_iter=max_iter, check_every=check_every)
+    out = f.result()
+    k = 0
+    for tr, imgs, srcs in layout:
+        for src in srcs:
+            th = out[k]
+            k += 1
+            wcs = imgs[0].getWcs()
+            src.getPosition().setAllParams([th[0] - wcs.dx, th[1] - wcs.dy])
+            br = src.getBrightness()
+            for b, img in enumerate(imgs):
+                pc = img.getPhotoCal()
+                val = th[2 + b] / pc.getScale()
+                if pc.band is None:
+                    br.setAllParams([val])
+                else:
+                    br.setFlux(pc.band, val)
+            if not isinstance(src, S.PointSource):
+                src.shape.setAllParams(list(th[5:8]))
+                if isinstance(src, S.SersicGalaxy):
+                    src.sersicindex.setAllParams([th[8]])
+    return f.states()
