@@ -377,8 +377,15 @@ int tb_scene_render(const tb_scene_item* items, int32_t n_items,
  * Problem b has P[b] parameters and R[b] rows; its design matrix is stored
  * column-major at A + a_off[b] with leading dimension lda[b] (rows), its
  * right-hand side at rhs + r_off[b].  Writes (FP64) AtA[b] (P x P, at
- * ata_off[b]) and Atr[b] (P, at atr_off[b]) with FP32 products accumulated
- * by compensated (two-sum) FP32 partial sums combined in FP64.
+ * ata_off[b], exactly symmetric) and Atr[b] (P, at atr_off[b]).  For
+ * max_p <= 255 the products run on the tensor cores (tcgen05 kind::tf32):
+ * each value is split into TF32 hi + lo parts and hi*hi + hi*lo + lo*hi is
+ * accumulated in FP32 over at most 128 rows, then summed in FP64 (about 22
+ * significant bits per product).  For 255 < max_p <= 320 FP32 CUDA-core
+ * products are accumulated by compensated (two-sum) FP32 partial sums
+ * combined in FP64.  max_p must bound every P[b]; a problem above it is
+ * skipped.  A tensor-core wait that times out (1 s) writes NaN into that
+ * problem's outputs and counts in tb_tensor_core_timeouts.
  * Replaces the sparse A / b assembly and LSQR solve of
  * LsqrOptimizer.getUpdateDirection (tractor/lsqr_optimizer.py:328-644). */
 int tb_normal_equations(const float* A, const float* rhs, const int64_t* a_off,
@@ -387,6 +394,10 @@ int tb_normal_equations(const float* A, const float* rhs, const int64_t* a_off,
                         const int64_t* ata_off, const int64_t* atr_off,
                         double* AtA, double* Atr, int32_t n_problems,
                         int32_t max_p, void* stream);
+
+/* Number of tensor-core waits that timed out since the library was loaded
+ * on the current device (0 in a healthy run).  Synchronous. */
+int tb_tensor_core_timeouts(uint32_t* count);
 
 /* Solves each problem's column-scaled normal equations in FP64 on the device
  * (column scaling as lsqr_optimizer.py:470-489 with scale = sqrt(diag),

@@ -104,6 +104,7 @@ SIGNATURES = {
     'tb_fourier_render': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _P]),
     'tb_psf_spectrum': (_I32, [_P, _P, _I32, _I32, _I32, _P]),
     'tb_normal_equations': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _I32, _P]),
+    'tb_tensor_core_timeouts': (_I32, [_P]),
     'tb_solve_update': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P, _P]),
     'tb_solve_update_noalloc': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P]),
     'tb_chi2': (_I32, [_P, _P, _P, _P, _P, _I32, _P, _P]),

@@ -1,8 +1,9 @@
 // K5: least-squares step kernels (sm_100a).
 //
-//  * normal equations A^T A, A^T r of many independent problems: FP32
-//    products, compensated (Kahan) FP32 running sums per output, final values
-//    in FP64;
+//  * normal equations A^T A, A^T r of many independent problems: on the
+//    tensor cores (tcgen05 kind::tf32, three-term TF32 split, FP32 partial
+//    sums over at most 128 rows, FP64 totals) for P <= 255; above that
+//    FP32 CUDA-core products with compensated (Kahan) FP32 running sums;
 //  * FP64 column-scaled Cholesky solve with a damping ridge and one step of
 //    iterative refinement, one CTA per problem;
 //  * per-image chi^2 with compensated FP32 sums reduced in FP64 in a fixed
@@ -11,6 +12,7 @@
 // LsqrOptimizer.getUpdateDirection (tractor/lsqr_optimizer.py:328-644) and
 // the chi-square sum of Tractor.getLogLikelihood (tractor/engine.py:475-479).
 #include "tb_common.cuh"
+#include "tc_sm100.cuh"
 
 namespace {
 
@@ -92,6 +94,327 @@ normal_eq_kernel(const float* __restrict__ A, const float* __restrict__ rhs,
                 AtA[ata_off[b] + (int64_t)j * P + i] = v;
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Normal equations on the tensor cores (tcgen05, kind::tf32).
+//
+// Problem b's operand is the Q x R matrix [A^T; r^T] (Q = P + 1 rows: the P
+// design-matrix columns, then the right-hand side), K-major: the R pixel rows
+// are the contraction dimension.  A pass covers the 128 operand rows
+// [r0, r0 + 128) against the columns [r0, Q): one pass for Q <= 128, two
+// (r0 = 0, 128) for Q <= 256, which together give the upper triangle.  Within
+// a pass (Qp = Q - r0 operand rows, Q8 = Qp rounded up to 8) a stage covers
+// KC pixel rows (KC = 32 .. 128, the largest power of two with Q8 KC <=
+// 32 QM, so a stage moves up to 16 KB (QM = 128) or 32 KB (QM = 256)):
+//  * every thread copies its quads (4 consecutive pixel rows of one operand
+//    row) of a stage with cp.async into its own slots of a ring of raw
+//    stages (kRaw stages in flight, no registers held): one 16-byte copy when
+//    the problem's columns are 16-byte aligned, else four 4-byte copies;
+//  * when its copies of stage s have landed, the thread splits each value into
+//    TF32 hi and lo parts and stores each quad as one 16-byte core-matrix row
+//    of the canonical no-swizzle K-major layout (two operand stages; the K
+//    chunks Q8 * 16 + 16 bytes apart keep the stores bank-conflict-free);
+//  * one thread issues S += Hi_t Hi^T, E += Hi_t Lo^T + Lo_t Hi^T (three TF32
+//    MMAs of M = 128 per K = 8 step) into two TMEM accumulators and commits
+//    to the stage's mbarrier.
+// The tensor core's FP32 accumulation truncates, so its error grows with the
+// number of accumulations: every 128 rows (16 accumulations into S) the
+// accumulators are drained, and S and E are kept apart so that the small
+// cross terms add no roundings to S.  QM = 128 drains S + E into a
+// compensated (Kahan) FP32 total T, C held in TMEM next to S and E (512
+// columns) and writes the FP64 results once at the end; QM = 256 (S and E
+// already take 512 columns) adds the drains in FP64 at AtA[j P + i]
+// (coalesced over i) and Atr[i] and mirrors the lower triangle at the end.
+// Either way AtA is exactly symmetric.  Operand rows Qp .. 127 and columns
+// Qp .. N of the MMAs hold stale values; they only reach rows and columns of
+// D that are never read.
+namespace tcne {
+constexpr int kThreads = 256;
+constexpr int kChunkRows = 128;     // rows per FP32 accumulation chunk
+constexpr uint64_t kWaitNs = 1000000000ull;   // 1 s: far above any real MMA batch
+__host__ __device__ constexpr int elems(int qm) { return 32 * qm; }        // per raw stage
+__host__ __device__ constexpr int qpt(int qm) { return elems(qm) / 4 / kThreads; }   // quads
+__host__ __device__ constexpr int raw_stages(int qm) { return qm == 128 ? 4 : 2; }
+__host__ __device__ constexpr int kc_of(int qm, int q8) {
+    int kc = 128;
+    while (kc > 32 && kc * q8 > elems(qm)) kc >>= 1;
+    return kc;
+}
+// bytes one operand buffer spans, the MMA's reads of all 128 A rows and N B
+// rows past the last K chunk included
+__host__ __device__ constexpr int cbuf_need(int qm, int q8) {
+    const int kc = kc_of(qm, q8), lbo = q8 * 16 + 16, n = (q8 + 15) / 16 * 16;
+    return (kc / 4 - 1) * lbo + (n * 16 > 2048 ? n * 16 : 2048);
+}
+__host__ __device__ constexpr int cbuf_bytes(int qm) {
+    int m = 0;
+    for (int q8 = 8; q8 <= qm; q8 += 8) m = cbuf_need(qm, q8) > m ? cbuf_need(qm, q8) : m;
+    return (m + 127) / 128 * 128;
+}
+__host__ __device__ constexpr int raw_bytes(int qm) { return raw_stages(qm) * elems(qm) * 4; }
+__host__ __device__ constexpr int smem_bytes(int qm) {
+    return raw_bytes(qm) + 4 * cbuf_bytes(qm) + 64;
+}
+// QM = 128: S, E, T, C at columns 0, 128, 256, 384; QM = 256: S, E at 0, 256
+constexpr uint32_t kTmemCols = 512;
+}  // namespace tcne
+
+__device__ unsigned int g_ne_timeouts = 0;
+
+__device__ __forceinline__ void cp_async4(uint32_t dst, const float* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src),
+                 "r"(valid ? 4 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const float* src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int QM>
+__global__ void __launch_bounds__(tcne::kThreads, 1)
+normal_eq_tc_kernel(const float* __restrict__ A, const float* __restrict__ rhs,
+                    const int64_t* a_off, const int64_t* r_off, const int32_t* lda,
+                    const int32_t* Pv, const int32_t* Rv, const int64_t* ata_off,
+                    const int64_t* atr_off, double* AtA, double* Atr) {
+    using namespace tb::tc;
+    constexpr int QPT = tcne::qpt(QM);
+    constexpr int NRAW = tcne::raw_stages(QM);
+    constexpr int CBUF = tcne::cbuf_bytes(QM);
+    constexpr int RAW = tcne::raw_bytes(QM);
+    constexpr uint32_t NCOLS = tcne::kTmemCols;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4* raw = reinterpret_cast<float4*>(smem);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + RAW + 4 * CBUF);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + RAW + 4 * CBUF + 16);
+
+    const int b = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int P = Pv[b], R = Rv[b], ld = lda[b];
+    const int Q = P + 1;
+    if (P <= 0 || Q > QM) return;
+    double* M = AtA + ata_off[b];
+    double* g = Atr + atr_off[b];
+    if (R <= 0) {
+        for (int e = tid; e < P * P; e += tcne::kThreads) M[e] = 0.0;
+        for (int e = tid; e < P; e += tcne::kThreads) g[e] = 0.0;
+        return;
+    }
+    const float* Ab = A + a_off[b];
+    const float* rb = rhs + r_off[b];
+    // 16-byte copies when every column starts on a 16-byte boundary
+    const bool vec = ((reinterpret_cast<uintptr_t>(Ab) | reinterpret_cast<uintptr_t>(rb)) & 15) == 0 &&
+                     (ld & 3) == 0;
+
+    if (warp == 0) tmem_alloc(tslot, NCOLS);
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tS = *tslot, tE = tS + QM;
+    const uint32_t tT = tS + 256, tC = tS + 384;   // QM = 128 only
+    const uint32_t lane_sel = (uint32_t)((warp & 3) * 32) << 16;
+    const uint32_t raw_base = smem_u32(raw);
+
+    bool fail = false;
+    int gs = 0;              // stage counter over both passes (operand buffer, phase)
+    int last_commit = -1;
+    int nchunk = 0;          // drains so far (QM = 128: T and C hold data after the first)
+    for (int r0 = 0; r0 < Q && !fail; r0 += 128) {
+        const int Qp = Q - r0;                        // operand rows of this pass
+        const int Q8 = (Qp + 7) & ~7;
+        const int N = (Qp + 15) & ~15;                // columns r0 .. r0 + N
+        const int KC = tcne::kc_of(QM, Q8);
+        const int KQ = KC / 4;                        // quads per operand row and stage
+        const int LBO = Q8 * 16 + 16;
+        const int nst = (R + KC - 1) / KC;
+        const int chunk_st = tcne::kChunkRows / KC;   // stages per accumulation chunk
+        const uint32_t idesc = idesc_tf32(128, N);
+        // this thread's quads: pixel rows k .. k + 3 of operand rows c0 + m * cs
+        const int k = 4 * (tid % KQ), c0 = tid / KQ, cs = tcne::kThreads / KQ;
+        const float* src[QPT];
+        int soff[QPT];
+#pragma unroll
+        for (int m = 0; m < QPT; m++) {
+            const int c = c0 + m * cs, col = r0 + c;
+            src[m] = c < Qp ? (col < P ? Ab + (int64_t)col * ld : rb) + k : nullptr;
+            soff[m] = (k >> 2) * LBO + (c >> 3) * 128 + (c & 7) * 16;
+        }
+        auto issue = [&](int s) {
+            const int slot = s % NRAW;
+            const int row = s * KC + k;
+            const int nv = s < nst ? min(max(R - row, 0), 4) : 0;   // valid rows of the quad
+#pragma unroll
+            for (int m = 0; m < QPT; m++) {
+                if (src[m] == nullptr || s >= nst) continue;
+                const uint32_t dst = raw_base + 16 * ((slot * QPT + m) * tcne::kThreads + tid);
+                const float* p = src[m] + (int64_t)s * KC;
+                if (vec) {
+                    cp_async16(dst, nv > 0 ? p : Ab, 4 * nv);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) cp_async4(dst + 4 * q, q < nv ? p + q : Ab, q < nv);
+                }
+            }
+            cp_async_commit();
+        };
+        for (int s = 0; s < NRAW - 1; s++) issue(s);
+        for (int s = 0; s < nst; s++, gs++) {
+            issue(s + NRAW - 1);
+            cp_async_wait<NRAW - 1>();    // this thread's copies of stage s have landed
+            const int bi = gs & 1;
+            unsigned char* hi = smem + RAW + (2 * bi) * CBUF;
+            unsigned char* lo = smem + RAW + (2 * bi + 1) * CBUF;
+            // operand buffer bi is free once the MMAs of stage gs - 2 have completed
+            bool ok = true;
+            if (s >= 2) ok = mbar_wait(&bar[bi], ((gs >> 1) - 1) & 1, tcne::kWaitNs);
+            const int slot = s % NRAW;
+#pragma unroll
+            for (int m = 0; m < QPT; m++) {
+                if (src[m] == nullptr) continue;
+                const float4 v = raw[(slot * QPT + m) * tcne::kThreads + tid];
+                float4 h, l;
+                split_tf32(v.x, h.x, l.x);
+                split_tf32(v.y, h.y, l.y);
+                split_tf32(v.z, h.z, l.z);
+                split_tf32(v.w, h.w, l.w);
+                *reinterpret_cast<float4*>(hi + soff[m]) = h;
+                *reinterpret_cast<float4*>(lo + soff[m]) = l;
+            }
+            fence_async_smem();
+            if (__syncthreads_or(!ok)) { fail = true; break; }
+            if (tid == 0) {
+                fence_after_sync();
+                const bool fresh = (s % chunk_st) == 0;
+                const uint32_t ha = smem_u32(hi), la = smem_u32(lo);
+                for (int kk = 0; kk < KC / 8; kk++) {
+                    const uint32_t o = kk * 2 * LBO;
+                    const uint64_t dh = smem_desc(ha + o, LBO, 128);
+                    const uint64_t dl = smem_desc(la + o, LBO, 128);
+                    const uint32_t acc = (fresh && kk == 0) ? 0u : 1u;
+                    mma_tf32(tS, dh, dh, idesc, acc);
+                    mma_tf32(tE, dh, dl, idesc, acc);
+                    mma_tf32(tE, dl, dh, idesc, 1u);
+                }
+                commit(&bar[bi]);
+            }
+            last_commit = gs;
+            const bool drain = (s % chunk_st) == chunk_st - 1 || s == nst - 1;
+            if (!drain) continue;
+            ok = mbar_wait(&bar[bi], (gs >> 1) & 1, tcne::kWaitNs);
+            if (__syncthreads_or(!ok)) { fail = true; break; }
+            fence_after_sync();
+            const int row0 = r0 + (warp & 3) * 32;     // first D row of this warp
+            const int i = row0 + lane;
+            for (int cb = warp >> 2; cb < (N + 31) / 32; cb += 2) {
+                // blocks wholly below the diagonal or past row P - 1 hold nothing needed
+                if (r0 + cb * 32 + 31 < row0 || row0 >= P) continue;
+                float vs[32], ve[32];
+                tmem_ld32(tS + cb * 32 + lane_sel, vs);
+                tmem_ld32(tE + cb * 32 + lane_sel, ve);
+                if constexpr (QM == 128) {
+                    // T, C += S + E (Kahan)
+                    if (nchunk == 0) {
+#pragma unroll
+                        for (int jj = 0; jj < 32; jj++) { vs[jj] += ve[jj]; ve[jj] = 0.f; }
+                    } else {
+                        float vt[32], vc[32];
+                        tmem_ld32(tT + cb * 32 + lane_sel, vt);
+                        tmem_ld32(tC + cb * 32 + lane_sel, vc);
+#pragma unroll
+                        for (int jj = 0; jj < 32; jj++) {
+                            const float y = (vs[jj] + ve[jj]) - vc[jj];
+                            const float t = vt[jj] + y;
+                            ve[jj] = (t - vt[jj]) - y;
+                            vs[jj] = t;
+                        }
+                    }
+                    tmem_st32(tT + cb * 32 + lane_sel, vs);
+                    tmem_st32(tC + cb * 32 + lane_sel, ve);
+                } else {
+                    if (i >= P) continue;
+                    const bool first = s < chunk_st;
+                    // all loads of the block first, then the stores
+                    double old[32];
+#pragma unroll
+                    for (int jj = 0; jj < 32; jj++) {
+                        const int j = r0 + cb * 32 + jj;
+                        old[jj] = 0.0;
+                        if (first || j < i || j > P) continue;
+                        old[jj] = j == P ? g[i] : M[(int64_t)j * P + i];
+                    }
+#pragma unroll
+                    for (int jj = 0; jj < 32; jj++) {
+                        const int j = r0 + cb * 32 + jj;
+                        if (j < i || j > P) continue;
+                        const double x = old[jj] + ((double)vs[jj] + (double)ve[jj]);
+                        if (j == P) g[i] = x;
+                        else M[(int64_t)j * P + i] = x;
+                    }
+                }
+            }
+            nchunk++;
+            fence_before_sync();
+            __syncthreads();   // the next chunk's first MMAs overwrite the accumulators
+        }
+        cp_async_wait<0>();
+    }
+    if (fail) {
+        if (tid == 0) atomicAdd(&g_ne_timeouts, 1u);
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        for (int e = tid; e < P * P; e += tcne::kThreads) M[e] = nan;
+        for (int e = tid; e < P; e += tcne::kThreads) g[e] = nan;
+        // let the MMAs in flight finish (bounded) before the TMEM is freed
+        if (last_commit >= 0)
+            mbar_wait(&bar[last_commit & 1], (last_commit >> 1) & 1, tcne::kWaitNs);
+    } else if constexpr (QM == 128) {
+        // FP64 results from the compensated totals: D[i][j], i <= j
+        fence_after_sync();
+        const int row0 = (warp & 3) * 32, i = row0 + lane;
+        for (int cb = warp >> 2; cb < (((Q + 15) & ~15) + 31) / 32; cb += 2) {
+            if (cb * 32 + 31 < row0 || row0 >= P) continue;
+            float vt[32], vc[32];
+            tmem_ld32(tT + cb * 32 + lane_sel, vt);
+            tmem_ld32(tC + cb * 32 + lane_sel, vc);
+            if (i >= P) continue;
+#pragma unroll
+            for (int jj = 0; jj < 32; jj++) {
+                const int j = cb * 32 + jj;
+                if (j < i || j > P) continue;
+                const double x = (double)vt[jj] - (double)vc[jj];
+                if (j == P) {
+                    g[i] = x;
+                } else {
+                    M[(int64_t)j * P + i] = x;
+                    M[(int64_t)i * P + j] = x;
+                }
+            }
+        }
+    } else {
+        // lower triangle from the accumulated upper one (M[j P + i], i <= j)
+        __syncthreads();
+        for (int e = tid; e < P * P; e += tcne::kThreads) {
+            const int i = e / P, j = e % P;
+            if (i < j) M[e] = M[(int64_t)j * P + i];
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after_sync();
+        tmem_dealloc(tS, NCOLS);
     }
 }
 
@@ -243,6 +566,24 @@ chi2_kernel(const float* __restrict__ data, const float* __restrict__ model,
     if (threadIdx.x == 0) out[b] = red[0];
 }
 
+// One CTA per problem and, by its shared memory, per SM: the 512 TMEM
+// columns it takes are always free.
+template <int QM>
+int launch_normal_eq_tc(const float* A, const float* rhs, const int64_t* a_off,
+                        const int64_t* r_off, const int32_t* lda, const int32_t* P,
+                        const int32_t* R, const int64_t* ata_off, const int64_t* atr_off,
+                        double* AtA, double* Atr, int32_t n_problems, cudaStream_t s) {
+    constexpr int smem = tcne::smem_bytes(QM);
+    static_assert(smem > 114 * 1024, "one CTA per SM");
+    static_assert(smem <= 227 * 1024, "shared memory per CTA");
+    if (cudaFuncSetAttribute(normal_eq_tc_kernel<QM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    normal_eq_tc_kernel<QM><<<n_problems, tcne::kThreads, smem, s>>>(
+        A, rhs, a_off, r_off, lda, P, R, ata_off, atr_off, AtA, Atr);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
 }  // namespace
 
 extern "C" int tb_normal_equations(const float* A, const float* rhs, const int64_t* a_off,
@@ -255,9 +596,24 @@ extern "C" int tb_normal_equations(const float* A, const float* rhs, const int64
     if (max_p > kMaxSmemP) return TB_ERR_SIZE;
     if (!A || !rhs || !a_off || !r_off || !lda || !P || !R || !ata_off || !atr_off || !AtA || !Atr)
         return TB_ERR_ARG;
-    normal_eq_kernel<<<n_problems, kNeThreads, 0, (cudaStream_t)stream>>>(
-        A, rhs, a_off, r_off, lda, P, R, ata_off, atr_off, AtA, Atr);
+    const cudaStream_t s = (cudaStream_t)stream;
+    if (max_p + 1 <= 128)
+        return launch_normal_eq_tc<128>(A, rhs, a_off, r_off, lda, P, R, ata_off, atr_off, AtA,
+                                        Atr, n_problems, s);
+    if (max_p + 1 <= 256)
+        return launch_normal_eq_tc<256>(A, rhs, a_off, r_off, lda, P, R, ata_off, atr_off, AtA,
+                                        Atr, n_problems, s);
+    normal_eq_kernel<<<n_problems, kNeThreads, 0, s>>>(A, rhs, a_off, r_off, lda, P, R, ata_off,
+                                                        atr_off, AtA, Atr);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+extern "C" int tb_tensor_core_timeouts(uint32_t* count) {
+    if (!count) return TB_ERR_ARG;
+    unsigned int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_ne_timeouts, sizeof(v)) != cudaSuccess) return TB_ERR_LAUNCH;
+    *count = v;
+    return TB_OK;
 }
 
 extern "C" int tb_solve_update(const double* AtA, const double* Atr, const int64_t* ata_off,
