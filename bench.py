@@ -19,8 +19,10 @@ over sources.  L2 is flushed (a 256 MB write) before every timed step.
 The JSON line also carries, under "secondary", the batched-scene workload
 (20,000 point / exp / deV / composite sources on one 4096x4096 image through
 a 3-component MoG PSF; prep + binning + one persistent tile render, the
-tile height autotuned) with its own end-to-end number, roofline and CPU
-baseline (--no-secondary skips it).
+tile height autotuned), batched blob fitting (2,000 blobs x 3 bands) and the
+dense normal equations on the tensor cores (512 problems x 63 parameters x
+16,384 rows), each with its own end-to-end number, roofline and CPU baseline
+(--no-secondary skips them).
 
 --impl reference times the reference's CPU implementation of the same
 workload on the host cores (its own compiled C for the spectrum and the
@@ -58,7 +60,8 @@ def parse():
     ap.add_argument('--cpu-seconds', type=float, default=12.0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-secondary', action='store_true',
-                    help='skip the batched-scene and blob-fitting measurements')
+                    help='skip the batched-scene, blob-fitting and normal-equation '
+                         'measurements')
     ap.add_argument('--fit-blobs', type=int, default=2000,
                     help='blobs in the blob-fitting measurement (2000 = the full workload)')
     return ap.parse_args()
@@ -534,6 +537,136 @@ def bench_fit(args, dev, flush, clk, cpu_seconds):
     return line
 
 
+# ---------------------------------------------------------------------------
+# secondary workload: dense normal equations on the tensor cores
+# ---------------------------------------------------------------------------
+
+NE_PROBLEMS, NE_P, NE_R = 512, 63, 16384
+
+
+def _ne_call(lib, A, r, meta, AtA, Atr, n, max_p, stream):
+    from tractor_b200 import _lib
+    return lib.tb_normal_equations(A.data_ptr(), r.data_ptr(), *[m.data_ptr() for m in meta],
+                                   AtA.data_ptr(), Atr.data_ptr(), n, max_p,
+                                   _lib.stream_ptr(stream))
+
+
+def bench_normal_equations(args, dev, flush, clk, cpu_seconds):
+    """tb_normal_equations (A^T A and A^T r of many independent least-squares
+    problems, the LsqrOptimizer step) on NE_PROBLEMS problems of NE_P
+    parameters x NE_R pixel rows, FP32 column-major in HBM (2.1 GB, above L2):
+    problems per second, device-timed and end to end from pinned host memory,
+    HBM roofline of the tensor-core kernel, the CUDA-core kernel the library
+    keeps for P > 255 timed on the same problems, and numpy FP64 on the host."""
+    import torch
+    from tractor_b200 import _lib
+    lib = _lib.load()
+    n, P, R = NE_PROBLEMS, NE_P, NE_R
+    g = torch.Generator(device=dev).manual_seed(4000)
+    A = torch.randn(n * P * R, device=dev, generator=g)
+    r = torch.randn(n * R, device=dev, generator=g)
+    t = lambda a, dt: torch.as_tensor(np.asarray(a, dt), device=dev)  # noqa: E731
+    meta = [t(np.arange(n) * P * R, np.int64), t(np.arange(n) * R, np.int64), t([R] * n, np.int32),
+            t([P] * n, np.int32), t([R] * n, np.int32), t(np.arange(n) * P * P, np.int64),
+            t(np.arange(n) * P, np.int64)]
+    AtA = torch.empty(n * P * P, dtype=torch.float64, device=dev)
+    Atr = torch.empty(n * P, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def timed(max_p, steps):
+        for _ in range(3):
+            _lib.check(_ne_call(lib, A, r, meta, AtA, Atr, n, max_p, stream), 'tb_normal_equations')
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _ne_call(lib, A, r, meta, AtA, Atr, n, max_p, stream)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return float(np.mean(ts))
+
+    steps = max(3, min(args.steps, 20))
+    tc_s = timed(P, steps)
+    # accuracy of the timed results against FP64 on a few problems
+    err = 0.
+    for q in (0, n // 2, n - 1):
+        Aq = A[q * P * R:(q + 1) * P * R].view(P, R).double()
+        ref = (Aq @ Aq.T).cpu().numpy()
+        d = np.sqrt(np.diag(ref))
+        got = AtA[q * P * P:(q + 1) * P * P].view(P, P).cpu().numpy()
+        err = max(err, float((np.abs(got - ref) / np.outer(d, d)).max()))
+    simt_s = timed(300, 3)   # max_p above 255 selects the CUDA-core kernel
+    in_bytes = float(n * (P + 1) * R * 4)
+    out_bytes = float(n * (P * P + P) * 8)
+    achieved = (in_bytes + out_bytes) / tc_s / 1e9
+    peak, peak_kind = measured_hbm_peak()
+    # end to end: the problems copied in from pinned host memory, results out
+    h_A = A.cpu().pin_memory()
+    h_r = r.cpu().pin_memory()
+    h_AtA = torch.empty(AtA.shape, dtype=AtA.dtype).pin_memory()
+    h_Atr = torch.empty(Atr.shape, dtype=Atr.dtype).pin_memory()
+    e2e = []
+    for _ in range(max(2, min(steps, 3))):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        A.copy_(h_A, non_blocking=True)
+        r.copy_(h_r, non_blocking=True)
+        _ne_call(lib, A, r, meta, AtA, Atr, n, P, stream)
+        h_AtA.copy_(AtA, non_blocking=True)
+        h_Atr.copy_(Atr, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        e2e.append(e0.elapsed_time(e1) / 1e3)
+    line = {
+        'workload': '%d least-squares problems x %d parameters x %d pixel rows, FP32 '
+                    'column-major (A^T A, A^T r in FP64)' % (n, P, R),
+        'metric': 'normal-equation problems/s (tb_normal_equations)',
+        'value': n / tc_s, 'unit': 'problems/s', 'ms_per_step': tc_s * 1e3, 'steps': steps,
+        'max_scaled_error_vs_fp64': err,
+        'cuda_core_kernel': {'ms_per_step': simt_s * 1e3, 'value': n / simt_s,
+                             'speedup_tensor_cores': simt_s / tc_s},
+        'e2e': {'value': n / float(np.mean(e2e)), 'unit': 'problems/s',
+                'h2d_bytes_per_step': int(in_bytes), 'd2h_bytes_per_step': int(out_bytes)},
+        'roofline': {'bound': 'hbm', 'kernel': 'normal_eq_tc_kernel (tcgen05 kind::tf32)',
+                     'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                     'frac': achieved / peak, 'peak_basis': peak_kind,
+                     'algorithmic': '%d x (%d + 1) x %d x 4 bytes read + %d x (%d^2 + %d) x 8 '
+                                    'bytes written per launch' % (n, P, R, n, P, P),
+                     'kernel_ms': tc_s * 1e3,
+                     'traffic': ncu_traffic('normal_eq_tc.json')},
+    }
+    if cpu_seconds:
+        An = A[:P * R].view(P, R).cpu().numpy().astype(np.float64)
+        rn = r[:R].cpu().numpy().astype(np.float64)
+        t0 = time.time()
+        done = 0
+        while time.time() - t0 < cpu_seconds and done < n:
+            _ = An @ An.T, An @ rn
+            done += 1
+        rate = done / (time.time() - t0)
+        line['cpu_baseline'] = {'value': rate, 'unit': 'problems/s',
+                                'cores': os.cpu_count() or 1, 'kind': 'port',
+                                'sample': '%d problems, numpy FP64 A^T A and A^T r (BLAS, all '
+                                          'host threads)' % done}
+    return line
+
+
+def measured_hbm_peak():
+    """The pool's measured copy bandwidth (GB/s) and where it came from."""
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        if 'hbm_gbs' in d:
+            return float(d['hbm_gbs']), 'measured copy bandwidth (MEASURED_PEAKS.json hbm_gbs)'
+    except (OSError, ValueError):
+        pass
+    return 6650.0, 'fallback 6.65 TB/s'
+
+
 def fit_plain_fp64(w, data, inv, batched, dev, budget):
     """The plain FP64 GPU fitter (tractor_b200.plain.BlobFitFP64: one blob at
     a time, FP64 torch / cuSOLVER) on the workload's first blobs for about
@@ -792,7 +925,9 @@ def main():
     if not args.no_secondary:
         cpu_s = None if (args.no_cpu_baseline or world > 1 or rank) else min(args.cpu_seconds, 8.0)
         line['secondary'] = [bench_scene(args, dev, flush, clk, cpu_s),
-                             bench_fit(args, dev, flush, clk, cpu_s)]
+                             bench_fit(args, dev, flush, clk, cpu_s),
+                             bench_normal_equations(args, dev, flush, clk,
+                                                    cpu_s and min(cpu_s, 4.0))]
     line['plain_fp64'] = fourier_plain_fp64(srcs, out, dev, budget=3.0)
     if line['plain_fp64']['value']:
         line['speedup_vs_plain_fp64'] = value / line['plain_fp64']['value']

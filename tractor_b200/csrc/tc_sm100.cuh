@@ -159,11 +159,13 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) 
         : "memory");
 }
 
-// Round-to-nearest TF32 value of x (low 13 mantissa bits zero).
+// TF32 value of x rounded to nearest, ties away from zero (low 13 mantissa
+// bits zero), by integer arithmetic on the ALU pipe: adding half a TF32 ulp
+// to the bit pattern carries into the kept bits (and the exponent) exactly
+// when the dropped bits are at least half an ulp.  Finite x only (values
+// within a TF32 ulp of FLT_MAX round to infinity).
 __device__ __forceinline__ float tf32_round(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 // x = hi + lo with hi and lo TF32: the products hi*hi + hi*lo + lo*hi of two
