@@ -1,6 +1,8 @@
 """tb_normal_equations on the tensor cores (tcgen05 kind::tf32, three-term
 TF32 split, FP32 partial sums over at most 128 rows, FP64 totals) against
-FP64 numpy, plus the CUDA-core kernel it keeps for P > 255.
+FP64 numpy: the stacked one-MMA kernel for P <= 63 (launches whose max_p is
+at most 63), the general kernel for P <= 255, and the CUDA-core kernel kept
+for P > 255.
 
 Tolerance: every A^T A entry within 2e-6 of sqrt(H_ii H_jj) (the
 Cauchy-Schwarz bound of the entry's sum of |products|), every A^T r entry
@@ -66,6 +68,17 @@ def _run_and_check(Ps, Rs, seed, pad=0, align=False):
     assert lib.tb_tensor_core_timeouts(ctypes.byref(n)) == 0
     assert n.value == 0
     return worst
+
+
+def test_stacked_kernel_mixed_sizes(tb):
+    """P <= 63 (one MMA per K step on the stacked [Hi; Lo] operand): sizes on
+    and off the 8 / 16 / 32 boundaries and the 32-row block edge, rows not a
+    multiple of the 64-row stage or of the 128-row chunk, a single stage,
+    R = 0."""
+    w = _run_and_check([1, 6, 7, 15, 31, 32, 33, 47, 54, 63, 20],
+                       [4096, 33, 1, 3000, 2049, 128, 64, 1025, 2500, 700, 0], seed=7)
+    w2 = _run_and_check([63, 32, 5], [5003, 130, 9], seed=8, align=True)
+    print('worst scaled error (stacked):', w, w2)
 
 
 def test_one_m_tile_mixed_sizes(tb):

@@ -566,6 +566,323 @@ chi2_kernel(const float* __restrict__ data, const float* __restrict__ model,
     if (threadIdx.x == 0) out[b] = red[0];
 }
 
+// ---------------------------------------------------------------------------
+// Normal equations on the tensor cores for Q = P + 1 <= 64 (warp-specialised,
+// one MMA per K step).
+//
+// The A operand of the MMA is the stacked 128-row tile [Hi; Lo] of the
+// problem's Q operand rows (hi parts in rows 0-63, lo parts in rows 64-127)
+// and the B operand its hi rows, so ONE kind::tf32 MMA of M = 128 per K = 8
+// step gives S = Hi Hi^T (D rows 0-63) and E = Lo Hi^T (D rows 64-127);
+// D = S + E + E^T, the cross terms symmetrised when the accumulators are
+// drained.  Warps 0-7 (converters) stage KC = 64 pixel rows per stage (4-
+// or 16-byte cp.async into their own slots of a raw ring, split into TF32 hi
+// and lo, one 16-byte core-matrix row each in the canonical no-swizzle
+// K-major layout) and arrive on `full`; warp 8 issues the stage's 8 MMAs and
+// commits to `empty`.  Chunks of 128 rows alternate between two
+// accumulator sets (TMEM columns 0 and 128); the converters drain chunk c
+// after staging the first stage of chunk c + 1, whose MMAs wait until that
+// drain is done: TMEM loads that ran while MMAs into the other set were in
+// flight returned wrong values on B200 (two column layouts tried), so a drain
+// never overlaps an MMA.  A set holds two tiles (columns +0 and +64) that
+// take alternate K steps, so each FP32 accumulator takes 8 accumulations per
+// chunk: the tensor core's accumulation truncates, and its error grows with
+// that count.  A drain: the warps
+// holding E rows copy their 32 x 32 blocks to shared memory, a converter
+// barrier, then the warps holding S rows add S + E + E^T of their blocks on
+// or above the diagonal into compensated (Kahan) FP32 totals in shared
+// memory, and arrive on `accfree` (the set may be overwritten).  The FP64
+// results are written once at the end, AtA exactly symmetric.
+// ---------------------------------------------------------------------------
+namespace tc64 {
+constexpr int kConv = 256;                 // converter threads
+constexpr int kThreads = kConv + 32;       // + the MMA warp
+constexpr int kKc = 64;                    // pixel rows per stage
+constexpr int kChunkSt = 2;                // stages per 128-row accumulation chunk
+constexpr int kRaw = 4;                    // raw stages in flight
+constexpr int kQpt = 4;                    // quads per thread and stage (64 x 64 / 4 / 256)
+constexpr int kLbo = 128 / 8 * 128 + 16;   // bytes between K chunks (128 stacked rows)
+constexpr int kCbuf = 33280;               // kKc / 4 chunks of kLbo bytes, MMA over-read included
+constexpr int kRawBytes = kRaw * kQpt * kConv * 16;
+constexpr int kEsLd = 65;                  // E staging row stride (floats)
+constexpr int kEsBytes = 64 * kEsLd * 4;
+constexpr int kTotBytes = 3 * 2 * 32 * 32 * 4;   // T, C of blocks (0,0), (0,1), (1,1)
+constexpr int kBarOff = kRawBytes + 2 * kCbuf + kEsBytes + kTotBytes;
+constexpr int kSmem = kBarOff + 128;
+constexpr uint32_t kTmemCols = 256;
+constexpr uint64_t kWaitNs = 1000000000ull;
+static_assert((kKc / 4 - 1) * kLbo + 2048 <= kCbuf, "MMA reads stay inside the operand buffer");
+static_assert(kSmem > 114 * 1024 && kSmem <= 227 * 1024, "one CTA per SM");
+}  // namespace tc64
+
+__device__ __forceinline__ void conv_barrier() {
+    asm volatile("bar.sync 1, 256;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tb::tc::smem_u32(bar))
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(tc64::kThreads, 1)
+normal_eq_tc64_kernel(const float* __restrict__ A, const float* __restrict__ rhs,
+                      const int64_t* a_off, const int64_t* r_off, const int32_t* lda,
+                      const int32_t* Pv, const int32_t* Rv, const int64_t* ata_off,
+                      const int64_t* atr_off, double* AtA, double* Atr) {
+    using namespace tb::tc;
+    using namespace tc64;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4* raw = reinterpret_cast<float4*>(smem);
+    unsigned char* cbuf = smem + kRawBytes;
+    float* Es = reinterpret_cast<float*>(smem + kRawBytes + 2 * kCbuf);
+    float* tot = reinterpret_cast<float*>(smem + kRawBytes + 2 * kCbuf + kEsBytes);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kBarOff);
+    uint64_t* full = bar;          // [2] converters -> MMA warp: operand buffer written
+    uint64_t* empty = bar + 2;     // [2] MMA warp -> converters: the stage's MMAs completed
+    uint64_t* accfree = bar + 4;   // [2] converters -> MMA warp: accumulator set drained
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 6);
+    int* flag = reinterpret_cast<int*>(bar + 7);   // a wait timed out
+
+    const int b = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int P = Pv[b], R = Rv[b], ld = lda[b];
+    const int Q = P + 1;
+    if (P <= 0 || Q > 64) return;
+    double* M = AtA + ata_off[b];
+    double* g = Atr + atr_off[b];
+    if (R <= 0) {
+        for (int e = tid; e < P * P; e += kThreads) M[e] = 0.0;
+        for (int e = tid; e < P; e += kThreads) g[e] = 0.0;
+        return;
+    }
+    const float* Ab = A + a_off[b];
+    const float* rb = rhs + r_off[b];
+    const bool vec = ((reinterpret_cast<uintptr_t>(Ab) | reinterpret_cast<uintptr_t>(rb)) & 15) == 0 &&
+                     (ld & 3) == 0;
+    const int N = (Q + 15) & ~15;
+    const int nst = (R + kKc - 1) / kKc;
+
+    if (warp == 0) tmem_alloc(tslot, kTmemCols);
+    if (tid == 0) {
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&full[i], kConv);
+            mbar_init(&empty[i], 1);
+            mbar_init(&accfree[i], kConv);
+        }
+        *flag = 0;
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tbase = *tslot;
+
+    if (warp == 8) {
+        // ---------------- MMA warp ----------------
+        const uint32_t idesc = idesc_tf32(128, N);
+        int last = -1;
+        bool ok = true;
+        for (int s = 0; s < nst && ok; s++) {
+            const int bi = s & 1, c = s / kChunkSt;
+            if (lane == 0) {
+                ok = mbar_wait(&full[bi], (s >> 1) & 1, kWaitNs);
+                // the previous chunk has been drained: no TMEM load of a drain
+                // runs while MMAs are in flight
+                if (ok && s % kChunkSt == 0 && c >= 1)
+                    ok = mbar_wait(&accfree[(c - 1) & 1], ((c - 1) >> 1) & 1, kWaitNs);
+                if (ok) {
+                    fence_after_sync();
+                    const uint32_t base = smem_u32(cbuf + bi * kCbuf);
+                    const uint32_t d = tbase + (uint32_t)(128 * (c & 1));
+                    // K steps alternate between the set's two tiles (columns
+                    // +0, +64): 8 accumulations per tile and chunk
+                    for (int kk = 0; kk < kKc / 8; kk++) {
+                        const uint64_t desc = smem_desc(base + kk * 2 * kLbo, kLbo, 128);
+                        mma_tf32(d + 64 * (kk & 1), desc, desc, idesc,
+                                 (s % kChunkSt == 0 && kk < 2) ? 0u : 1u);
+                    }
+                } else {
+                    atomicExch(flag, 1);
+                }
+                commit(&empty[bi]);   // in every case: no converter waits on a stage never committed
+                last = s;
+            }
+            ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+            if (*reinterpret_cast<volatile int*>(flag)) ok = false;
+        }
+        // every MMA this warp issued has completed before the TMEM is freed
+        if (lane == 0 && last >= 0 && !mbar_wait(&empty[last & 1], (last >> 1) & 1, kWaitNs))
+            atomicExch(flag, 1);
+        __syncwarp();
+    } else {
+        // ---------------- converter warps ----------------
+        const int q = warp & 3;                       // TMEM lane quarter
+        const uint32_t lane_sel = (uint32_t)(q * 32) << 16;
+        const uint32_t raw_base = smem_u32(raw);
+        // this thread's quads: pixel rows k .. k + 3 of operand rows c0 + 16 m
+        const int k = 4 * (tid & 15), c0 = tid >> 4;
+        const float* src[kQpt];
+        int soff[kQpt];
+#pragma unroll
+        for (int m = 0; m < kQpt; m++) {
+            const int c = c0 + 16 * m;
+            src[m] = c < Q ? (c < P ? Ab + (int64_t)c * ld : rb) + k : nullptr;
+            soff[m] = (k >> 2) * kLbo + (c >> 3) * 128 + (c & 7) * 16;
+        }
+        auto issue = [&](int s) {
+            const int slot = s % kRaw;
+            const int row = s * kKc + k;
+            const int nv = s < nst ? min(max(R - row, 0), 4) : 0;
+#pragma unroll
+            for (int m = 0; m < kQpt; m++) {
+                if (src[m] == nullptr || s >= nst) continue;
+                const uint32_t dst = raw_base + 16 * ((slot * kQpt + m) * kConv + tid);
+                const float* p = src[m] + (int64_t)s * kKc;
+                if (vec) {
+                    cp_async16(dst, nv > 0 ? p : Ab, 4 * nv);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; j++) cp_async4(dst + 4 * j, j < nv ? p + j : Ab, j < nv);
+                }
+            }
+            cp_async_commit();
+        };
+        int drains = 0;
+        // Drain of chunk `drains` (accumulator set drains & 1), last stage
+        // s_last.  Every converter thread runs every drain and its barrier in
+        // the same order, also after a wait has timed out (`skip`: the waits
+        // are left out, the values then are garbage and the outputs NaN).
+        auto drain = [&](int s_last, bool skip) -> bool {
+            const bool ok = __all_sync(
+                0xffffffffu, !skip && mbar_wait(&empty[s_last & 1], (s_last >> 1) & 1, kWaitNs));
+            const uint32_t d = tbase + (uint32_t)(128 * (drains & 1));
+            const int cb = warp >> 2;                  // 32-column block
+            if (ok) {
+                fence_after_sync();
+                // E rows (q - 2) * 32 .. + 31 of this column block -> shared memory
+                const int e0 = (q - 2) * 32;
+                if (q >= 2 && e0 < Q && cb * 32 < N) {
+                    float v[32], v2[32];
+                    tmem_ld32(d + cb * 32 + lane_sel, v);
+                    tmem_ld32(d + 64 + cb * 32 + lane_sel, v2);
+#pragma unroll
+                    for (int jj = 0; jj < 32; jj++)
+                        Es[(e0 + lane) * kEsLd + cb * 32 + jj] = v[jj] + v2[jj];
+                }
+            }
+            conv_barrier();
+            if (ok && q < 2 && cb >= q && q * 32 < P && cb * 32 <= P) {
+                // S block (I = q, J = cb) on or above the diagonal: T, C += S + E + E^T
+                float v[32], v2[32];
+                tmem_ld32(d + cb * 32 + lane_sel, v);
+                tmem_ld32(d + 64 + cb * 32 + lane_sel, v2);
+#pragma unroll
+                for (int jj = 0; jj < 32; jj++) v[jj] += v2[jj];
+                const int i = q * 32 + lane;
+                float* Tt = tot + (q + cb) * 2 * 1024;    // blocks (0,0) 0, (0,1) 1, (1,1) 2
+                float* Cc = Tt + 1024;
+#pragma unroll 8
+                for (int jj = 0; jj < 32; jj++) {
+                    const int j = cb * 32 + jj;
+                    const float x = v[jj] + (Es[i * kEsLd + j] + Es[j * kEsLd + i]);
+                    if (drains == 0) {
+                        Tt[jj * 32 + lane] = x;
+                        Cc[jj * 32 + lane] = 0.f;
+                    } else {
+                        const float t0 = Tt[jj * 32 + lane], c0v = Cc[jj * 32 + lane];
+                        const float y = x - c0v;
+                        const float t = t0 + y;
+                        Cc[jj * 32 + lane] = (t - t0) - y;
+                        Tt[jj * 32 + lane] = t;
+                    }
+                }
+            }
+            // the E block copies are read by other warps: no warp refills Es
+            // before every S warp has read it (the next drain needs the next
+            // chunk, whose stages need every converter's arrival)
+            fence_before_sync();
+            mbar_arrive(&accfree[drains & 1]);
+            drains++;
+            return ok;
+        };
+        bool fail = false;
+        for (int s = 0; s < kRaw - 1; s++) issue(s);
+        for (int s = 0; s < nst; s++) {
+            issue(s + kRaw - 1);
+            cp_async_wait<kRaw - 1>();    // this thread's copies of stage s have landed
+            const int bi = s & 1;
+            unsigned char* buf = cbuf + bi * kCbuf;
+            // operand buffer bi is free once the MMAs of stage s - 2 have completed
+            if (s >= 2 && !fail && !mbar_wait(&empty[bi], ((s >> 1) - 1) & 1, kWaitNs)) fail = true;
+            const int slot = s % kRaw;
+#pragma unroll
+            for (int m = 0; m < kQpt; m++) {
+                if (src[m] == nullptr) continue;
+                const float4 v = raw[(slot * kQpt + m) * kConv + tid];
+                float4 h, l;
+                split_tf32(v.x, h.x, l.x);
+                split_tf32(v.y, h.y, l.y);
+                split_tf32(v.z, h.z, l.z);
+                split_tf32(v.w, h.w, l.w);
+                *reinterpret_cast<float4*>(buf + soff[m]) = h;          // row c
+                *reinterpret_cast<float4*>(buf + soff[m] + 1024) = l;   // row 64 + c
+            }
+            fence_async_smem();
+            mbar_arrive(&full[bi]);
+            // the previous chunk's accumulators, while this chunk is multiplied
+            if (s % kChunkSt == 0 && s > 0 && !drain(s - 1, fail)) fail = true;
+        }
+        cp_async_wait<0>();
+        if (!drain(nst - 1, fail)) fail = true;
+        if (fail) atomicExch(flag, 1);
+        conv_barrier();
+        // FP64 results from the compensated totals: D[i][j], i <= j <= P
+        const int cb = warp >> 2;
+        if (!fail && !*reinterpret_cast<volatile int*>(flag) && q < 2 && cb >= q && q * 32 < P &&
+            cb * 32 <= P) {
+            const int i = q * 32 + lane;
+            const float* Tt = tot + (q + cb) * 2 * 1024;
+            const float* Cc = Tt + 1024;
+            if (i < P) {
+                for (int jj = 0; jj < 32; jj++) {
+                    const int j = cb * 32 + jj;
+                    if (j < i || j > P) continue;
+                    const double x = (double)Tt[jj * 32 + lane] - (double)Cc[jj * 32 + lane];
+                    if (j == P) {
+                        g[i] = x;
+                    } else {
+                        M[(int64_t)j * P + i] = x;
+                        M[(int64_t)i * P + j] = x;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (*reinterpret_cast<volatile int*>(flag)) {
+        if (tid == 0) atomicAdd(&g_ne_timeouts, 1u);
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        for (int e = tid; e < P * P; e += kThreads) M[e] = nan;
+        for (int e = tid; e < P; e += kThreads) g[e] = nan;
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after_sync();
+        tmem_dealloc(tbase, kTmemCols);
+    }
+}
+
+int launch_normal_eq_tc64(const float* A, const float* rhs, const int64_t* a_off,
+                          const int64_t* r_off, const int32_t* lda, const int32_t* P,
+                          const int32_t* R, const int64_t* ata_off, const int64_t* atr_off,
+                          double* AtA, double* Atr, int32_t n_problems, cudaStream_t s) {
+    if (cudaFuncSetAttribute(normal_eq_tc64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tc64::kSmem) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    normal_eq_tc64_kernel<<<n_problems, tc64::kThreads, tc64::kSmem, s>>>(
+        A, rhs, a_off, r_off, lda, P, R, ata_off, atr_off, AtA, Atr);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
 // One CTA per problem and, by its shared memory, per SM: the 512 TMEM
 // columns it takes are always free.
 template <int QM>
@@ -597,6 +914,9 @@ extern "C" int tb_normal_equations(const float* A, const float* rhs, const int64
     if (!A || !rhs || !a_off || !r_off || !lda || !P || !R || !ata_off || !atr_off || !AtA || !Atr)
         return TB_ERR_ARG;
     const cudaStream_t s = (cudaStream_t)stream;
+    if (max_p + 1 <= 64)
+        return launch_normal_eq_tc64(A, rhs, a_off, r_off, lda, P, R, ata_off, atr_off, AtA, Atr,
+                                     n_problems, s);
     if (max_p + 1 <= 128)
         return launch_normal_eq_tc<128>(A, rhs, a_off, r_off, lda, P, R, ata_off, atr_off, AtA,
                                         Atr, n_problems, s);
