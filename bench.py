@@ -630,7 +630,7 @@ def bench_normal_equations(args, dev, flush, clk, cpu_seconds):
                              'speedup_tensor_cores': simt_s / tc_s},
         'e2e': {'value': n / float(np.mean(e2e)), 'unit': 'problems/s',
                 'h2d_bytes_per_step': int(in_bytes), 'd2h_bytes_per_step': int(out_bytes)},
-        'roofline': {'bound': 'hbm', 'kernel': 'normal_eq_tc_kernel (tcgen05 kind::tf32)',
+        'roofline': {'bound': 'hbm', 'kernel': 'normal_eq_tc64_kernel (tcgen05 kind::tf32, P <= 63)',
                      'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                      'frac': achieved / peak, 'peak_basis': peak_kind,
                      'algorithmic': '%d x (%d + 1) x %d x 4 bytes read + %d x (%d^2 + %d) x 8 '
