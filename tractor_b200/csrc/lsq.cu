@@ -575,10 +575,10 @@ chi2_kernel(const float* __restrict__ data, const float* __restrict__ model,
 // and the B operand its hi rows, so ONE kind::tf32 MMA of M = 128 per K = 8
 // step gives S = Hi Hi^T (D rows 0-63) and E = Lo Hi^T (D rows 64-127);
 // D = S + E + E^T, the cross terms symmetrised when the accumulators are
-// drained.  Warps 0-7 (converters) stage KC = 64 pixel rows per stage (4-
+// drained.  Warps 0-7 (converters) stage KC = 32 pixel rows per stage (4-
 // or 16-byte cp.async into their own slots of a raw ring, split into TF32 hi
 // and lo, one 16-byte core-matrix row each in the canonical no-swizzle
-// K-major layout) and arrive on `full`; warp 8 issues the stage's 8 MMAs and
+// K-major layout) and arrive on `full`; warp 8 issues the stage's 4 MMAs and
 // commits to `empty`.  Chunks of 128 rows alternate between two
 // accumulator sets (TMEM columns 0 and 128); the converters drain chunk c
 // after staging the first stage of chunk c + 1, whose MMAs wait until that
@@ -597,12 +597,14 @@ chi2_kernel(const float* __restrict__ data, const float* __restrict__ model,
 namespace tc64 {
 constexpr int kConv = 256;                 // converter threads
 constexpr int kThreads = kConv + 32;       // + the MMA warp
-constexpr int kKc = 64;                    // pixel rows per stage
-constexpr int kChunkSt = 2;                // stages per 128-row accumulation chunk
-constexpr int kRaw = 4;                    // raw stages in flight
-constexpr int kQpt = 4;                    // quads per thread and stage (64 x 64 / 4 / 256)
+constexpr int kKc = 32;                    // pixel rows per stage
+constexpr int kChunkSt = 4;                // stages per 128-row accumulation chunk
+constexpr int kRaw = 3;                    // raw stages in flight
+constexpr int kKq = kKc / 4;               // quads per operand row and stage
+constexpr int kRowStep = kConv / kKq;      // operand rows between a thread's quads
+constexpr int kQpt = 64 / kRowStep;        // quads per thread and stage (64 x 32 / 4 / 256)
 constexpr int kLbo = 128 / 8 * 128 + 16;   // bytes between K chunks (128 stacked rows)
-constexpr int kCbuf = 33280;               // kKc / 4 chunks of kLbo bytes, MMA over-read included
+constexpr int kCbuf = 16512;               // kKc / 4 chunks of kLbo bytes, MMA over-read included
 constexpr int kRawBytes = kRaw * kQpt * kConv * 16;
 constexpr int kEsLd = 65;                  // E staging row stride (floats)
 constexpr int kEsBytes = 64 * kEsLd * 4;
@@ -612,7 +614,8 @@ constexpr int kSmem = kBarOff + 128;
 constexpr uint32_t kTmemCols = 256;
 constexpr uint64_t kWaitNs = 1000000000ull;
 static_assert((kKc / 4 - 1) * kLbo + 2048 <= kCbuf, "MMA reads stay inside the operand buffer");
-static_assert(kSmem > 114 * 1024 && kSmem <= 227 * 1024, "one CTA per SM");
+// two CTAs per SM (shared memory), whose 2 x 256 TMEM columns always fit
+static_assert(kSmem + 1024 > 232448 / 3 && 2 * (kSmem + 1024) <= 232448, "two CTAs per SM");
 }  // namespace tc64
 
 __device__ __forceinline__ void conv_barrier() {
@@ -623,7 +626,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
                  : "memory");
 }
 
-__global__ void __launch_bounds__(tc64::kThreads, 1)
+__global__ void __launch_bounds__(tc64::kThreads, 2)
 normal_eq_tc64_kernel(const float* __restrict__ A, const float* __restrict__ rhs,
                       const int64_t* a_off, const int64_t* r_off, const int32_t* lda,
                       const int32_t* Pv, const int32_t* Rv, const int64_t* ata_off,
@@ -717,13 +720,14 @@ normal_eq_tc64_kernel(const float* __restrict__ A, const float* __restrict__ rhs
         const int q = warp & 3;                       // TMEM lane quarter
         const uint32_t lane_sel = (uint32_t)(q * 32) << 16;
         const uint32_t raw_base = smem_u32(raw);
-        // this thread's quads: pixel rows k .. k + 3 of operand rows c0 + 16 m
-        const int k = 4 * (tid & 15), c0 = tid >> 4;
+        // this thread's quads: pixel rows k .. k + 3 of operand rows
+        // c0 + kRowStep m
+        const int k = 4 * (tid % kKq), c0 = tid / kKq;
         const float* src[kQpt];
         int soff[kQpt];
 #pragma unroll
         for (int m = 0; m < kQpt; m++) {
-            const int c = c0 + 16 * m;
+            const int c = c0 + kRowStep * m;
             src[m] = c < Q ? (c < P ? Ab + (int64_t)c * ld : rb) + k : nullptr;
             soff[m] = (k >> 2) * kLbo + (c >> 3) * 128 + (c & 7) * 16;
         }
