@@ -7,7 +7,8 @@ oracle and the CUDA path can be checked against the reference without the
 reference being present.  All scenarios are seeded.  Run from the repository
 root in the development container:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture but hybrid_psf
+    python tests/golden/make_golden.py hybrid   # hybrid_psf.npz
 """
 import os
 import sys
@@ -290,5 +291,58 @@ def main():
     print('golden fixtures written to', OUT)
 
 
+def hybrid():
+    """HybridPixelizedPSF (psf.py:600-655): galaxies rendered by the hybrid
+    split of ProfileGalaxy._realGetUnitFluxModelPatch (galaxy.py:412-455,
+    510-518) -- all-Fourier, ramped, all-MoG, a source outside its mask
+    (MoG), no mask -- and a point source (the pixelized model)."""
+    from oracle import refharness
+    refharness.load()
+    from tractor import (Image, PixPos, Flux, LinearPhotoCal, GaussianMixturePSF, PixelizedPSF,
+                         PointSource, EllipseE)
+    from tractor.psf import HybridPixelizedPSF
+    from tractor.galaxy import ExpGalaxy, DevGalaxy
+    from tractor.sersic import SersicGalaxy, SersicIndex
+    from tractor.patch import ModelMask
+    mof = moffat()
+    gauss = dict(amp=np.array([0.8, 0.2]), mean=np.zeros((2, 2)),
+                 var=np.array([[[2.0, 0.1], [0.1, 2.2]], [[9.0, 0.], [0., 9.0]]]))
+    psf = HybridPixelizedPSF(PixelizedPSF(mof),
+                             GaussianMixturePSF(gauss['amp'], gauss['mean'], gauss['var']))
+    # kind 0 exp, 1 deV, 2 Sersic, 3 point source; px, py, r_e, b/a, phi, n;
+    # mask (x0, y0, w, h), w = 0: none
+    cases = [(0, 64.3, 63.8, 2.0, 0.7, 30., 1.0, (0, 0, 128, 128)),
+             (0, 64.3, 63.8, 12.0, 0.7, 30., 1.0, (0, 0, 64 + 64, 128)),
+             (0, 32.2, 31.6, 9.0, 0.8, 60., 1.0, (0, 0, 64, 64)),
+             (1, 32.4, 32.3, 14.0, 0.6, 10., 1.0, (0, 0, 64, 64)),
+             (2, 40.1, 36.9, 7.0, 0.5, 120., 3.0, (8, 4, 64, 64)),
+             (0, -20.0, 40.0, 10.0, 0.9, 0., 1.0, (0, 0, 64, 64)),
+             (0, 50.3, 49.6, 3.0, 0.6, 45., 1.0, (0, 0, 0, 0)),
+             (0, 31.7, 32.5, 30.0, 0.8, 75., 1.0, (0, 0, 64, 64)),
+             (2, 48.2, 47.7, 20.0, 0.7, 15., 1.5, (0, 0, 96, 96)),
+             (3, 33.7, 30.2, 0.0, 1.0, 0., 1.0, (0, 0, 64, 64))]
+    out = []
+    for kind, px, py, re, ab, phi, n, mk in cases:
+        pos, flux = PixPos(px, py), Flux(1000.)
+        if kind == 3:
+            src = PointSource(pos, flux)
+        else:
+            ell = EllipseE.fromRAbPhi(re, ab, phi)
+            src = (ExpGalaxy(pos, flux, ell) if kind == 0 else DevGalaxy(pos, flux, ell)
+                   if kind == 1 else SersicGalaxy(pos, flux, ell, SersicIndex(n)))
+        tim = Image(data=np.zeros((100, 100), np.float32), inverr=np.ones((100, 100), np.float32),
+                    psf=psf, photocal=LinearPhotoCal(1.))
+        mm = ModelMask(*mk) if mk[2] > 0 else None
+        out.append(src.getModelPatch(tim, modelMask=mm))
+    table = np.array([list(c[:7]) + list(c[7]) for c in cases], np.float64)
+    np.savez_compressed(os.path.join(OUT, 'hybrid_psf.npz'), cases=table,
+                        psf=mof, gauss_amp=gauss['amp'], gauss_mean=gauss['mean'],
+                        gauss_var=gauss['var'], **patches_to_arrays(out))
+    print('hybrid fixture written to', OUT)
+
+
 if __name__ == '__main__':
-    main()
+    if sys.argv[1:] == ['hybrid']:
+        hybrid()
+    else:
+        main()

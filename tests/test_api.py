@@ -1,6 +1,6 @@
 """The drop-in object API against the reference's own outputs
-(tests/golden/mog_sources.npz, fit_plain.npz, fft_sersic.npz, produced by
-tests/golden/make_golden.py) and the reference's test assertions.
+(tests/golden/mog_sources.npz, fit_plain.npz, fft_sersic.npz, hybrid_psf.npz,
+produced by tests/golden/make_golden.py) and the reference's test assertions.
 
 Each test runs twice: on CPU with the device kernels replaced by the test
 stand-ins (host logic: geometry rules, plans, finite differences, least
@@ -126,6 +126,36 @@ def test_sources_match_reference(backend):
         s2.pos.y = s.pos.y - 18
         _check_patch(s2.getModelPatch(tim2), _unpack(g, name + '_ncirc')[0], PEAK_TOL,
                      name + ' ncirc')
+
+
+def test_hybrid_pixelized_psf_matches_reference(backend):
+    """HybridPixelizedPSF (tractor/psf.py:600-655) in getModelPatch: galaxies
+    through the hybrid split of the Fourier path (all-Fourier, ramped and
+    mostly pixel-space mixtures, a source outside its mask rendered with the
+    mixture, no mask) and a point source (the pixelized model), against the
+    reference's own patches."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'hybrid_psf.npz'))
+    psf = T.HybridPixelizedPSF(T.PixelizedPSF(g['psf']),
+                               T.GaussianMixturePSF(g['gauss_amp'], g['gauss_mean'], g['gauss_var']))
+    o = 0
+    for i, c in enumerate(g['cases']):
+        kind, px, py, re, ab, phi, n, x0, y0, w, h = c
+        pos, flux = T.PixPos(px, py), T.Flux(1000.)
+        if kind == 3:
+            src = T.PointSource(pos, flux)
+        else:
+            ell = T.EllipseE.fromRAbPhi(re, ab, phi)
+            src = (T.ExpGalaxy(pos, flux, ell) if kind == 0 else T.DevGalaxy(pos, flux, ell)
+                   if kind == 1 else T.SersicGalaxy(pos, flux, ell, T.SersicIndex(n)))
+        tim = T.Image(data=np.zeros((100, 100), np.float32), inverr=np.ones((100, 100), np.float32),
+                      psf=psf, photocal=T.LinearPhotoCal(1.))
+        mm = T.ModelMask(int(x0), int(y0), int(w), int(h)) if w > 0 else None
+        p = src.getModelPatch(tim, modelMask=mm)
+        ph, pw = int(g['h'][i]), int(g['w'][i])
+        ref = (int(g['x0'][i]), int(g['y0'][i]), g['pix'][o:o + ph * pw].reshape(ph, pw))
+        o += ph * pw
+        _check_patch(p, ref, PEAK_TOL, 'hybrid case %d' % i)
 
 
 def test_fft_sersic_matches_reference(backend):

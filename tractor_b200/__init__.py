@@ -16,8 +16,8 @@ from .basics import (PixPos, NullWCS, Flux, Mag, Fluxes, NanoMaggies, MultiBandB
                      NullPhotoCal, LinearPhotoCal, NullSky, ConstantSky, Image)
 from .ellipses import GalaxyShape, EllipseE, EllipseESoft
 from .profiles import MixtureOfGaussians, SersicMixture
-from .psf import (HybridPSF, GaussianMixturePSF, NCircularGaussianPSF, PixelizedPSF,
-                  NormalizedPixelizedPsf, MogParams)
+from .psf import (HybridPSF, HybridPixelizedPSF, GaussianMixturePSF, NCircularGaussianPSF,
+                  PixelizedPSF, NormalizedPixelizedPsf, MogParams)
 from .sources import (BasicSource, SingleProfileSource, PointSource, Galaxy, ProfileGalaxy,
                       HoggGalaxy, GaussianGalaxy, ExpGalaxy, DevGalaxy, SersicGalaxy, SersicIndex,
                       FracDev, SoftenedFracDev, FixedCompositeGalaxy)
@@ -31,7 +31,7 @@ __all__ = [
     'NullSky', 'ConstantSky', 'Image',
     'GalaxyShape', 'EllipseE', 'EllipseESoft',
     'MixtureOfGaussians', 'SersicMixture',
-    'HybridPSF', 'GaussianMixturePSF', 'NCircularGaussianPSF', 'PixelizedPSF',
+    'HybridPSF', 'HybridPixelizedPSF', 'GaussianMixturePSF', 'NCircularGaussianPSF', 'PixelizedPSF',
     'NormalizedPixelizedPsf',
     'PointSource', 'Galaxy', 'ProfileGalaxy', 'HoggGalaxy', 'GaussianGalaxy', 'ExpGalaxy',
     'DevGalaxy', 'SersicGalaxy', 'SersicIndex', 'FracDev', 'SoftenedFracDev',

@@ -431,6 +431,59 @@ class PixelizedPSF(ParamList):
         return self._plan_point_source(plan, px, py, **kwargs).result()
 
 
+class HybridPixelizedPSF(HybridPSF):
+    """A PixelizedPSF with a Gaussian-mixture approximation
+    (tractor/psf.py:600-655).  Point sources use the pixelized model;
+    galaxies take the Fourier path with the pixelized spectrum, except their
+    components that are wide for the FFT box, which are rendered in pixel
+    space through the mixture `gauss` (with a linear ramp between the two,
+    ProfileGalaxy's hybrid split).  Every other attribute is the pixelized
+    model's.  `gauss` must be given: fitting it to the PSF stamp
+    (GaussianMixturePSF.fromStamp, an EM fit) is not provided."""
+
+    def __init__(self, pix, gauss=None, N=2, cx=0., cy=0.):
+        object.__setattr__(self, 'pix', pix)
+        if gauss is None:
+            raise NotImplementedError('HybridPixelizedPSF needs its Gaussian approximation '
+                                      '`gauss` (fitting it to the stamp is not provided)')
+        object.__setattr__(self, 'gauss', gauss)
+
+    def __str__(self):
+        return ('HybridPixelizedPSF: Gaussian sigma %.2f, Pix %s' %
+                (np.sqrt(self.gauss.mog.var[0, 0, 0]), str(self.pix)))
+
+    def copy(self):
+        return self.__class__(self.pix.copy(), self.gauss.copy())
+
+    def getMixtureOfGaussians(self, **kwargs):
+        return self.gauss.getMixtureOfGaussians(**kwargs)
+
+    def getShifted(self, dx, dy):
+        return HybridPixelizedPSF(self.pix.getShifted(dx, dy), self.gauss)
+
+    def constantPsfAt(self, x, y):
+        return HybridPixelizedPSF(self.pix.constantPsfAt(x, y), self.gauss)
+
+    def __getattr__(self, name):
+        # only called for attributes this object does not have: the
+        # pixelized model's (never 'pix' itself, which __init__ sets first)
+        if name in ('pix', 'gauss'):
+            raise AttributeError(name)
+        return getattr(self.__dict__['pix'], name)
+
+    def __setattr__(self, name, val):
+        if name in ('gauss', 'pix'):
+            return object.__setattr__(self, name, val)
+        setattr(self.__dict__['pix'], name, val)
+
+    def __getstate__(self):
+        return (self.gauss, self.pix)
+
+    def __setstate__(self, state):
+        object.__setattr__(self, 'gauss', state[0])
+        object.__setattr__(self, 'pix', state[1])
+
+
 class NormalizedPixelizedPsf(PixelizedPSF):
     """PixelizedPSF with its image and spectrum normalised to unit sum
     (tractor/psf.py:947-971)."""
