@@ -122,17 +122,20 @@ def install(monkeypatch):
         self.status = torch.zeros(16, dtype=torch.uint8)
         return out
 
+    def spectra_compute(self, img, sz, normalize=False):
+        pad, cx, cy = render.PsfSpectra.pad(img, sz)
+        P = np.fft.rfft2(pad).astype(np.complex64)
+        if normalize:
+            n = np.abs(P[0][0])
+            if n != 0:
+                P /= n
+        flat = np.ascontiguousarray(P.T).view(np.float32).ravel()
+        return (torch.from_numpy(flat.copy()), cx, cy)
+
     def spectra_get(self, key, img, sz, normalize=False):
         k = (key, sz, bool(normalize))
         if k not in self.cache:
-            pad, cx, cy = render.PsfSpectra.pad(img, sz)
-            P = np.fft.rfft2(pad).astype(np.complex64)
-            if normalize:
-                n = np.abs(P[0][0])
-                if n != 0:
-                    P /= n
-            flat = np.ascontiguousarray(P.T).view(np.float32).ravel()
-            self.cache[k] = (torch.from_numpy(flat.copy()), cx, cy)
+            self.cache[k] = spectra_compute(self, img, sz, normalize)
         return self.cache[k]
 
     def lanczos(imgs, shifts, stream=None):
@@ -188,6 +191,7 @@ def install(monkeypatch):
     monkeypatch.setattr(render.MogBatch, 'run', mog_run)
     monkeypatch.setattr(render.FftBatch, 'run', fft_run)
     monkeypatch.setattr(render.PsfSpectra, 'get', spectra_get)
+    monkeypatch.setattr(render.PsfSpectra, 'compute', spectra_compute)
     monkeypatch.setattr(render, 'lanczos_shift', lanczos)
     monkeypatch.setattr(render, 'normal_equations', normal_equations)
     monkeypatch.setattr(render, 'solve_update', solve_update)

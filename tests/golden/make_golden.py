@@ -9,6 +9,7 @@ root in the development container:
 
     python tests/golden/make_golden.py          # every fixture but hybrid_psf
     python tests/golden/make_golden.py hybrid   # hybrid_psf.npz
+    python tests/golden/make_golden.py psfex    # psfex.npz
 """
 import os
 import sys
@@ -341,8 +342,67 @@ def hybrid():
     print('hybrid fixture written to', OUT)
 
 
+def psfex():
+    """PixelizedPsfEx (psfex.py:428-521) built from a degree-2 model's arrays
+    (no FITS file: attributes set as PsfExModel.shifted does): galaxies on the
+    Fourier path with the position-dependent spectrum, point sources with the
+    position-dependent image, at several positions, and one galaxy with a
+    HybridPixelizedPSF around the PsfEx model."""
+    from oracle import refharness
+    refharness.load()
+    from tractor import (Image, PixPos, Flux, LinearPhotoCal, GaussianMixturePSF, PointSource,
+                         EllipseE)
+    from tractor.psf import HybridPixelizedPSF
+    from tractor.psfex import PsfExModel, PixelizedPsfEx
+    from tractor.galaxy import ExpGalaxy
+    from tractor.sersic import SersicGalaxy, SersicIndex
+    from tractor.patch import ModelMask
+    base = moffat(33, 4.0, 3.0)
+    wide = moffat(33, 5.5, 2.5)
+    y, x = np.mgrid[:33, :33] - 16
+    bases = np.stack([base, 0.3 * (wide - base), 0.02 * x * base, 0.15 * (wide - base),
+                      0.01 * x * y * base, 0.02 * y * base]).astype(np.float32)
+    m = PsfExModel()
+    m.sampling, m.psfbases, m.degree = 1., bases, 2
+    m.x0, m.y0, m.xscale, m.yscale = 50., 40., 100., 80.
+    m.radius, m.fwhm = (33 + 1) / 2., 4.0
+    psf = PixelizedPsfEx(None, psfex=m)
+    mc = m.copy()
+    mc.fwhm = m.fwhm     # as PixelizedPsfEx.copy does (shifted() leaves it out)
+    hyb = HybridPixelizedPSF(PixelizedPsfEx(None, psfex=mc),
+                             GaussianMixturePSF(np.array([1.]), np.zeros((1, 2)),
+                                                np.array([[[2.5, 0.], [0., 2.5]]])))
+    # kind 0 exp, 1 Sersic, 3 point source, 4 exp with the hybrid PSF; px, py,
+    # r_e, b/a, phi, n; mask (x0, y0, w, h)
+    cases = [(0, 10.3, 12.7, 3.0, 0.6, 20., 1.0, (0, 0, 32, 32)),
+             (1, 88.6, 20.1, 4.0, 0.5, 110., 2.5, (70, 0, 30, 48)),
+             (1, 51.2, 85.4, 6.0, 0.8, 60., 0.9, (20, 50, 64, 50)),
+             (3, 15.4, 80.2, 0., 1., 0., 1., (0, 60, 40, 40)),
+             (3, 90.1, 10.6, 0., 1., 0., 1., (70, 0, 30, 30)),
+             (4, 70.2, 70.8, 12.0, 0.7, 45., 1.0, (40, 40, 60, 60))]
+    out = []
+    for kind, px, py, re, ab, phi, n, mk in cases:
+        pos, flux = PixPos(px, py), Flux(1000.)
+        if kind == 3:
+            src = PointSource(pos, flux)
+        else:
+            ell = EllipseE.fromRAbPhi(re, ab, phi)
+            src = (SersicGalaxy(pos, flux, ell, SersicIndex(n)) if kind == 1
+                   else ExpGalaxy(pos, flux, ell))
+        tim = Image(data=np.zeros((100, 100), np.float32), inverr=np.ones((100, 100), np.float32),
+                    psf=hyb if kind == 4 else psf, photocal=LinearPhotoCal(1.))
+        out.append(src.getModelPatch(tim, modelMask=ModelMask(*mk)))
+    table = np.array([list(c[:7]) + list(c[7]) for c in cases], np.float64)
+    np.savez_compressed(os.path.join(OUT, 'psfex.npz'), cases=table, bases=bases,
+                        poly=np.array([m.degree, m.x0, m.y0, m.xscale, m.yscale]),
+                        **patches_to_arrays(out))
+    print('psfex fixture written to', OUT)
+
+
 if __name__ == '__main__':
     if sys.argv[1:] == ['hybrid']:
         hybrid()
+    elif sys.argv[1:] == ['psfex']:
+        psfex()
     else:
         main()

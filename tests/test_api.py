@@ -1,6 +1,6 @@
 """The drop-in object API against the reference's own outputs
 (tests/golden/mog_sources.npz, fit_plain.npz, fft_sersic.npz, hybrid_psf.npz,
-produced by tests/golden/make_golden.py) and the reference's test assertions.
+psfex.npz, produced by tests/golden/make_golden.py) and the reference's test assertions.
 
 Each test runs twice: on CPU with the device kernels replaced by the test
 stand-ins (host logic: geometry rules, plans, finite differences, least
@@ -156,6 +156,41 @@ def test_hybrid_pixelized_psf_matches_reference(backend):
         ref = (int(g['x0'][i]), int(g['y0'][i]), g['pix'][o:o + ph * pw].reshape(ph, pw))
         o += ph * pw
         _check_patch(p, ref, PEAK_TOL, 'hybrid case %d' % i)
+
+
+def test_pixelized_psfex_matches_reference(backend):
+    """PixelizedPsfEx (tractor/psfex.py:428-521), a degree-2 model built
+    from its arrays: galaxies on the Fourier path with the spectrum of the
+    position's PSF, point sources with the position's image, and a galaxy
+    with a HybridPixelizedPSF around the model, against the reference's own
+    patches (tests/golden/psfex.npz)."""
+    import tractor_b200 as T
+    from tractor_b200.psfex import PsfExModel, PixelizedPsfEx
+    g = np.load(os.path.join(GOLDEN, 'psfex.npz'))
+    deg, x0m, y0m, xs, ys = g['poly']
+    model = PsfExModel(g['bases'], degree=int(deg), x0=x0m, y0=y0m, xscale=xs, yscale=ys,
+                       fwhm=4.0)
+    psf = PixelizedPsfEx(psfex=model)
+    hyb = T.HybridPixelizedPSF(PixelizedPsfEx(psfex=model.copy()),
+                               T.GaussianMixturePSF(np.array([1.]), np.zeros((1, 2)),
+                                                    np.array([[[2.5, 0.], [0., 2.5]]])))
+    o = 0
+    for i, c in enumerate(g['cases']):
+        kind, px, py, re, ab, phi, n, mx0, my0, mw, mh = c
+        pos, flux = T.PixPos(px, py), T.Flux(1000.)
+        if kind == 3:
+            src = T.PointSource(pos, flux)
+        else:
+            ell = T.EllipseE.fromRAbPhi(re, ab, phi)
+            src = (T.SersicGalaxy(pos, flux, ell, T.SersicIndex(n)) if kind == 1
+                   else T.ExpGalaxy(pos, flux, ell))
+        tim = T.Image(data=np.zeros((100, 100), np.float32), inverr=np.ones((100, 100), np.float32),
+                      psf=hyb if kind == 4 else psf, photocal=T.LinearPhotoCal(1.))
+        p = src.getModelPatch(tim, modelMask=T.ModelMask(int(mx0), int(my0), int(mw), int(mh)))
+        ph, pw = int(g['h'][i]), int(g['w'][i])
+        ref = (int(g['x0'][i]), int(g['y0'][i]), g['pix'][o:o + ph * pw].reshape(ph, pw))
+        o += ph * pw
+        _check_patch(p, ref, PEAK_TOL, 'psfex case %d' % i)
 
 
 def test_fft_sersic_matches_reference(backend):

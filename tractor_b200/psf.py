@@ -376,11 +376,17 @@ class PixelizedPSF(ParamList):
         return render.psf_spectra().get(self._key, self.getImage(0., 0.), sz,
                                         normalize=self._normalized)
 
+    def fourier_spectrum(self, px, py, sz):
+        """(spectrum key, device spectrum, cx, cy) at FFT size sz for a source
+        at (px, py); the same for every position of a constant PSF."""
+        spec, cx, cy = self.spectrum(sz)
+        return self._key, spec, cx, cy
+
     def getFourierTransform(self, px, py, radius):
         """Host copy of the spectrum in the reference's layout:
         (P (sz, sz/2+1) complex64, (cx, cy), (sz, sz), (v, w))."""
         sz = self.getFourierTransformSize(radius)
-        spec, cx, cy = self.spectrum(sz)
+        _, spec, cx, cy = self.fourier_spectrum(px, py, sz)
         P = spec.cpu().numpy().view(np.complex64).reshape(sz // 2 + 1, sz).T.copy()
         return P, (cx, cy), (sz, sz), (np.fft.rfftfreq(sz), np.fft.fftfreq(sz))
 

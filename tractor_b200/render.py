@@ -184,8 +184,13 @@ class PsfSpectra(object):
         """Returns (device spectrum tensor, cx, cy) for PSF image `img` at FFT
         size sz; `key` identifies the PSF for caching."""
         k = (key, sz, bool(normalize))
-        if k in self.cache:
-            return self.cache[k]
+        if k not in self.cache:
+            self.cache[k] = self.compute(img, sz, normalize)
+        return self.cache[k]
+
+    def compute(self, img, sz, normalize=False):
+        """(device spectrum tensor, cx, cy) of `img` at FFT size sz, not cached
+        (position-dependent PSFs)."""
         lib = _lib.load()
         dev = device()
         pad, cx, cy = self.pad(img, sz)
@@ -194,8 +199,7 @@ class PsfSpectra(object):
         rc = lib.tb_psf_spectrum(dpad.data_ptr(), spec.data_ptr(), 1, sz, int(bool(normalize)),
                                  _lib.stream_ptr())
         _lib.check(rc, 'tb_psf_spectrum')
-        self.cache[k] = (spec, cx, cy)
-        return self.cache[k]
+        return (spec, cx, cy)
 
 
 _spectra = PsfSpectra()

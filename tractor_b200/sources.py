@@ -506,7 +506,7 @@ class ProfileGalaxy(object):
         sz = psf.getFourierTransformSize(halfsize)
         if sz > 256:
             raise NotImplementedError('Fourier-path patch size %d above the supported 256' % sz)
-        spec, cx, cy = psf.spectrum(sz)
+        spec_key, spec, cx, cy = psf.fourier_spectrum(px, py, sz)
         pH = pW = sz
         dx = px - cx
         dy = py - cy
@@ -560,7 +560,7 @@ class ProfileGalaxy(object):
             rx0, ry0, rw, rh = gx0, gy0, max(0, gx1 - gx0), max(0, gy1 - gy0)
             ssx, ssy = ix0 - rx0, iy0 - ry0
         if fftmix is not None and rw > 0 and rh > 0:
-            h = plan.add_fft(fftmix.amp, fftmix.var, sz, psf._key, spec, rw, rh, ssx, ssy,
+            h = plan.add_fft(fftmix.amp, fftmix.var, sz, spec_key, spec, rw, rh, ssx, ssy,
                              mux, muy)
         else:
             h = ('empty', rh, rw)
