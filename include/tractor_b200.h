@@ -466,6 +466,9 @@ typedef struct {
     int32_t profile;          /* TB_PROFILE_SERSIC, _EXP, _DEV or _POINT */
     int32_t x0, y0, w, h;     /* ModelMask in blob pixels (fixed during a fit) */
     int32_t blob;             /* the blob it belongs to */
+    int32_t frozen;           /* bit k set: parameter slot k held at its start value
+                                 (frozen parameters, utils.py:195-320) */
+    int32_t pad;
 } tb_fit_source;
 
 /* Buffers of blob b: hbuf + h_off holds (n_bands + 2) P x P FP64 blocks

@@ -702,13 +702,16 @@ def blob_normal_equations(params, rects, W, H, psf, n_bands, data, inverr, steps
 
 
 def blob_fit(params0, rects, W, Himg, psf, n_bands, data, inverr, tol=1e-12, max_iter=60,
-             lower_n=0.29, upper_n=6.3):
+             lower_n=0.29, upper_n=6.3, frozen=None):
     """FP64 damped Gauss-Newton fit of one blob to a tight optimum (for
     parity: the optimum is a property of the objective, not of the path),
     stopping when the predicted log-likelihood gain of the next step is below
-    tol.  Returns (params, H at the optimum, held), `held` marking the
-    parameters held at a bound."""
+    tol.  `frozen` (bool, the shape of params0) marks parameters held at
+    their start values (frozen parameters, tractor/utils.py:195-320).
+    Returns (params, H at the optimum, held), `held` marking the parameters
+    held at a bound."""
     p = np.array(params0, np.float64)
+    fz = np.zeros(p.size, bool) if frozen is None else np.asarray(frozen, bool).ravel()
     H, g, c2 = blob_normal_equations(p, rects, W, Himg, psf, n_bands, data, inverr)
     lam = 1e-3
     for _ in range(max_iter):
@@ -719,6 +722,7 @@ def blob_fit(params0, rects, W, Himg, psf, n_bands, data, inverr, tol=1e-12, max
         nidx = np.arange(len(p)) * BLOB_NPAR + 8
         held = ((p[:, 8] >= upper_n) & (g[nidx] > 0)) | ((p[:, 8] <= lower_n) & (g[nidx] < 0))
         live[nidx[held]] = False
+        live[fz] = False
         Hs = H[np.ix_(live, live)] / np.outer(d[live], d[live]) + lam * np.eye(live.sum())
         x = np.zeros(len(d))
         xs = np.linalg.solve(Hs, g[live] / d[live])

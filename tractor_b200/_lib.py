@@ -49,7 +49,7 @@ SCENE_ITEM = np.dtype([('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'), ('h', '<i4'),
 
 FIT_NPAR, FIT_MAX_BANDS, FIT_MAX_SRC, FIT_MAX_PSF = 9, 3, 32, 4
 FIT_SOURCE = np.dtype([('profile', '<i4'), ('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'),
-                       ('h', '<i4'), ('blob', '<i4')])
+                       ('h', '<i4'), ('blob', '<i4'), ('frozen', '<i4'), ('pad', '<i4')])
 FIT_BLOB = np.dtype([('n_src', '<i4'), ('src0', '<i4'), ('P', '<i4'), ('unit0', '<i4'),
                      ('h_off', '<i8'), ('g_off', '<i8'), ('tile_off', '<i8'),
                      ('n_active', '<i4'), ('n_tiles', '<i4')])

@@ -814,6 +814,8 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
             ((pa[i] >= TB_FIT_SERSIC_MAX && ga[i] > 0.0) ||
              (pa[i] <= TB_FIT_SERSIC_MIN && ga[i] < 0.0)))
             d = 0.0;
+        // frozen parameters are left out of the step
+        if ((srcs[b.src0 + i / TB_FIT_NPAR].frozen >> (i % TB_FIT_NPAR)) & 1) d = 0.0;
         dsc[i] = d;
     }
     __syncthreads();

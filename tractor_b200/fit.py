@@ -397,8 +397,9 @@ def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
     per image band (Flux for a single image, NanoMaggies / Fluxes
     otherwise).  Model masks set with Tractor.setModelMasks are used (the
     same rectangle in every image); without them a source's mask is the
-    whole image.  Every source parameter is fitted (frozen parameters are
-    not honoured).  Returns the per-blob FIT_STATE records."""
+    whole image.  Frozen parameters (freezeParam / freezeAllBut) keep their
+    values; every thawed one is fitted.  Returns the per-blob FIT_STATE
+    records."""
     from . import sources as S, ellipses as E
     from .basics import NullWCS, LinearPhotoCal
     from .patch import ModelMask
@@ -464,6 +465,19 @@ def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
             th[0], th[1] = px, py
             for b, img in enumerate(imgs):
                 th[2 + b] = img.getPhotoCal().brightnessToCounts(src.getBrightness())
+            # parameter slots held fixed: those whose name is not thawed
+            thawed = set(src.getParamNames())
+            ball = src.getBrightness().copy()
+            if hasattr(ball, 'thawAllParams'):
+                ball.thawAllParams()
+            bnames = ball.getParamNames()      # every brightness value's name
+            bslots = [('brightness.' + (img.getPhotoCal().band
+                                        if img.getPhotoCal().band in bnames else bnames[0]))
+                      for img in imgs]
+            names = ['pos.x', 'pos.y'] + bslots + [None] * (3 - len(imgs)) + \
+                ['shape.logre', 'shape.ee1', 'shape.ee2', 'sersicindex.SersicIndex']
+            r['frozen'] = sum(1 << k for k, nm in enumerate(names)
+                              if nm is not None and nm not in thawed)
             mask = tr._getModelMaskFor(imgs[0], src)
             if mask is None:
                 r['x0'], r['y0'], r['w'], r['h'] = 0, 0, W, H
@@ -487,11 +501,18 @@ def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
     for tr, imgs, srcs in layout:
         for src in srcs:
             th = out[k]
+            fz = int(recs[k]['frozen'])
             k += 1
+            thawed = lambda slot: not (fz >> slot) & 1   # noqa: E731
             wcs = imgs[0].getWcs()
-            src.getPosition().setAllParams([th[0] - wcs.dx, th[1] - wcs.dy])
+            pos = src.getPosition()
+            xy = pos.getAllParams()
+            pos.setAllParams([th[0] - wcs.dx if thawed(0) else xy[0],
+                              th[1] - wcs.dy if thawed(1) else xy[1]])
             br = src.getBrightness()
             for b, img in enumerate(imgs):
+                if not thawed(2 + b):
+                    continue
                 pc = img.getPhotoCal()
                 val = th[2 + b] / pc.getScale()
                 if pc.band is None:
@@ -499,7 +520,8 @@ def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
                 else:
                     br.setFlux(pc.band, val)
             if not isinstance(src, S.PointSource):
-                src.shape.setAllParams(list(th[5:8]))
-                if isinstance(src, S.SersicGalaxy):
+                sh = src.shape.getAllParams()
+                src.shape.setAllParams([th[5 + j] if thawed(5 + j) else sh[j] for j in range(3)])
+                if isinstance(src, S.SersicGalaxy) and thawed(8):
                     src.sersicindex.setAllParams([th[8]])
     return f.states()
