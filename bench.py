@@ -21,8 +21,9 @@ The JSON line also carries, under "secondary", the batched-scene workload
 a 3-component MoG PSF; prep + binning + one persistent tile render, the
 tile height autotuned), batched blob fitting (2,000 blobs x 3 bands) and the
 dense normal equations on the tensor cores (512 problems x 63 parameters x
-16,384 rows), each with its own end-to-end number, roofline and CPU baseline
-(--no-secondary skips them).
+16,384 rows), each with its own end-to-end number, roofline and CPU baseline,
+and the small plain fit through the object API (latency-bound: us per render,
+ms per fit) (--no-secondary skips them).
 
 --impl reference times the reference's CPU implementation of the same
 workload on the host cores (its own compiled C for the spectrum and the
@@ -654,6 +655,55 @@ def bench_normal_equations(args, dev, flush, clk, cpu_seconds):
     return line
 
 
+def bench_plain_small(args, dev):
+    """The small plain fit through the object API (an ExpGalaxy, r_e 2 px, b/a
+    0.6, phi 30, flux 1000, at the centre of a 64 x 64 FP64 image, two-
+    Gaussian PSF with sigma 1.5 / 3.0 and weights 0.8 / 0.2, noise sigma 1
+    drawn from seed 300; start off by 0.5 px and 20 % in flux and r_e):
+    microseconds per Tractor.getModelImage and milliseconds per
+    optimize_loop(dchisq=1e-3) with B200Optimizer, host timed (each call
+    returns host arrays: copies and launches included).  The case is
+    latency-bound (49k pixel x components per render): no roofline."""
+    import tractor_b200 as T
+    psf = T.NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2])
+    truth = T.ExpGalaxy(T.PixPos(32., 32.), T.Flux(1000.), T.EllipseE.fromRAbPhi(2.0, 0.6, 30.))
+    tim = T.Image(data=np.zeros((64, 64)), invvar=np.ones((64, 64)), psf=psf,
+                  photocal=T.LinearPhotoCal(1.))
+    trc = T.Tractor([tim], [truth])
+    trc.modtype = np.float64
+    clean = trc.getModelImage(0)
+    tim.data = clean + np.random.default_rng(300).normal(size=clean.shape)
+    start = [32.5, 32.5, 800.] + list(T.EllipseE.fromRAbPhi(2.4, 0.6, 30.).getAllParams())
+    src = T.ExpGalaxy(T.PixPos(32.5, 32.5), T.Flux(800.), T.EllipseE.fromRAbPhi(2.4, 0.6, 30.))
+    tr = T.Tractor([tim], [src])
+    tr.modtype = np.float64
+    tr.freezeParam('images')
+    for _ in range(5):
+        tr.getModelImage(0)
+    reps = 50
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        tr.getModelImage(0)
+    render_us = (time.perf_counter() - t0) / reps * 1e6
+    fits, steps = [], 0
+    for _ in range(max(2, min(args.steps, 3)) + 1):
+        tr.setParams(start)
+        t0 = time.perf_counter()
+        R = tr.optimize_loop(dchisq=1e-3)
+        fits.append(time.perf_counter() - t0)
+        steps = R['steps']
+    fit_s = float(np.median(fits[1:]))
+    return {'workload': 'ExpGalaxy on a 64x64 image, 2-Gaussian PSF, LSQ fit of position, flux '
+                        'and shape from an offset start (optimize_loop, dchisq 1e-3)',
+            'metric': 'fitted sources/s (plain small fit, object API)',
+            'value': 1.0 / fit_s, 'unit': 'sources/s', 'ms_per_fit': fit_s * 1e3,
+            'steps_per_fit': steps, 'us_per_render': render_us,
+            'timing': 'host wall clock per call (launches, copies and host logic included)',
+            'roofline': None, 'cpu_baseline': None,
+            'note': 'latency-bound (49k pixel x components per render); the reference CPU '
+                    'fitter is not on the GPU host'}
+
+
 def measured_hbm_peak():
     """The pool's measured copy bandwidth (GB/s) and where it came from."""
     p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
@@ -927,7 +977,8 @@ def main():
         line['secondary'] = [bench_scene(args, dev, flush, clk, cpu_s),
                              bench_fit(args, dev, flush, clk, cpu_s),
                              bench_normal_equations(args, dev, flush, clk,
-                                                    cpu_s and min(cpu_s, 4.0))]
+                                                    cpu_s and min(cpu_s, 4.0)),
+                             bench_plain_small(args, dev)]
     line['plain_fp64'] = fourier_plain_fp64(srcs, out, dev, budget=3.0)
     if line['plain_fp64']['value']:
         line['speedup_vs_plain_fp64'] = value / line['plain_fp64']['value']

@@ -193,6 +193,34 @@ def test_pixelized_psfex_matches_reference(backend):
         _check_patch(p, ref, PEAK_TOL, 'psfex case %d' % i)
 
 
+def test_plain_fit_matches_reference_optimize_loop(backend):
+    """The small plain fit (an ExpGalaxy on 64 x 64, two-Gaussian PSF, from a
+    start off by 0.5 px and 20 % in flux and r_e): one Tractor.optimize()
+    step and the whole optimize_loop(dchisq=1e-3) through B200Optimizer end
+    where the reference's LsqrOptimizer ends (fit_plain.npz: its parameters
+    after the first step and at the end, its step count).  Fluxes within
+    5e-5 relative, positions and shape within 2e-4 (about 0.02 sigma here);
+    the same line-search step and a step count within 3."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'fit_plain.npz'))
+    tim = T.Image(data=g['data'], invvar=np.ones((64, 64)),
+                  psf=T.NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2]), photocal=T.LinearPhotoCal(1.))
+    src = T.ExpGalaxy(T.PixPos(32.5, 32.5), T.Flux(800.), T.EllipseE.fromRAbPhi(2.4, 0.6, 30.))
+    tr = T.Tractor([tim], [src])
+    tr.modtype = np.float64
+    tr.freezeParam('images')
+    dlnp, X1, alpha = tr.optimize()
+    assert alpha == g['alpha1']
+    p1 = np.array(tr.getParams())
+    assert abs(p1[2] - g['p_after1'][2]) <= 5e-5 * abs(g['p_after1'][2]), (p1, g['p_after1'])
+    assert np.all(np.abs(np.delete(p1 - g['p_after1'], 2)) <= 2e-4), (p1, g['p_after1'])
+    R = tr.optimize_loop(dchisq=1e-3)
+    pf = np.array(tr.getParams())
+    assert abs(pf[2] - g['p_final'][2]) <= 5e-5 * abs(g['p_final'][2]), (pf, g['p_final'])
+    assert np.all(np.abs(np.delete(pf - g['p_final'], 2)) <= 2e-4), (pf, g['p_final'])
+    assert abs(R['steps'] - int(g['steps'])) <= 3, (R['steps'], g['steps'])
+
+
 def test_fft_sersic_matches_reference(backend):
     import tractor_b200 as T
     g = np.load(os.path.join(GOLDEN, 'fft_sersic.npz'))
