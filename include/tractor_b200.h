@@ -471,29 +471,38 @@ typedef struct {
     int32_t pad;
 } tb_fit_source;
 
-/* Buffers of blob b: hbuf + h_off holds (n_bands + 2) P x P FP64 blocks
- * (per-band partial A^T A, accepted A^T A, Cholesky factor); gbuf + g_off
- * holds (n_bands + 1) P-vectors (per-band A^T r, accepted). */
+/* Buffers of blob b: hbuf + h_off holds (n_slices + 2) P x P FP64 blocks
+ * (per-slice partial A^T A, accepted A^T A, Cholesky factor); gbuf + g_off
+ * holds (n_slices + 1) P-vectors (per-slice A^T r, accepted).  A slice is
+ * one pass unit's share: a band's image, or a range of its active tiles. */
 typedef struct {
     int32_t n_src;            /* sources (<= TB_FIT_MAX_SRC) */
     int32_t src0;             /* first source */
     int32_t P;                /* n_src * TB_FIT_NPAR */
-    int32_t unit0;            /* chi2_part[unit0 + band] holds band `band`'s chi^2 */
+    int32_t unit0;            /* chi2_part[unit0 + slice] holds a slice's chi^2 */
     int64_t h_off, g_off;
     int64_t tile_off;         /* the blob's 32 x 8 tiles in `tiles`: first the n_active */
     int32_t n_active;         /* tiles some source mask reaches, then the others */
     int32_t n_tiles;          /* (each entry tx | ty << 16) */
+    int32_t n_slices;         /* partial blocks summed by tb_fit_step (>= 1) */
+    int32_t pad;
 } tb_fit_blob;
 
 /* One (blob, band) image: W x H float32 pixels of data and inverr at
- * pix_off (row stride W), and the band's PSF mixture (psf_K <= 4).  The
- * unit table is in blob-major, band-minor order: unit blob * n_bands + band. */
+ * pix_off (row stride W), and the band's PSF mixture (psf_K <= 4).
+ * tb_fit_prep takes the table of (blob, band) images in blob-major,
+ * band-minor order (unit blob * n_bands + band).  tb_fit_pass takes units
+ * that may split an image's active tiles into ranges [t0, t1) (t0 = t1 = 0
+ * and t1 = n_active describe the whole list); each unit owns the blob's
+ * partial blocks and chi^2 of its `slice`, and the unit with t0 = 0 also
+ * covers the image's inactive tiles in mode 1. */
 typedef struct {
     int32_t blob, band;
     int32_t W, H;
     int64_t pix_off;
     int32_t psf_K;
-    int32_t pad;
+    int32_t slice;            /* partial block of the blob this unit owns */
+    int32_t t0, t1;           /* range of the blob's active tiles */
     double psf_amp[4];
     double psf_mean[8];
     double psf_var[16];
@@ -530,13 +539,14 @@ int tb_fit_prep(const tb_fit_source* srcs, int32_t n_src, const double* params,
                 const double* cd_inv, const tb_profile_tables* tables, void* workspace,
                 void* stream);
 
-/* mode 0: for every unit of a running blob, over the tiles its sources'
- * masks reach: the model (each source's PSF-convolved mixture on its mask,
- * summed), r = (data - model) * inverr, the analytic derivative columns
- * A = dmodel/dparams * inverr, and the unit's A^T A (upper triangle), A^T r
- * and r^T r + chi2_const (chi2_part[blob.unit0 + band]).  mode 1 (once per
- * data set): chi2_const[blob.unit0 + band] = r^T r over the other tiles,
- * where the model is zero.  Replaces getDerivs / getChiImage / the A and b
+/* mode 0: for every unit of a running blob, over its range of the tiles its
+ * sources' masks reach: the model (each source's PSF-convolved mixture on
+ * its mask, summed), r = (data - model) * inverr, the analytic derivative
+ * columns A = dmodel/dparams * inverr, and the unit's A^T A (upper
+ * triangle), A^T r and r^T r + chi2_const into its slice
+ * (chi2_part[blob.unit0 + slice]).  mode 1 (once per data set):
+ * chi2_const[blob.unit0 + slice] = r^T r over the image's other tiles
+ * (where the model is zero) for units with t0 = 0, else 0.  Replaces getDerivs / getChiImage / the A and b
  * assembly of lsqr_optimizer.py:328-520.  A persistent grid takes units
  * in the order `order` lists them (e.g. largest first) from work_counter
  * (one int32 of device scratch). */

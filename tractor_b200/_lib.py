@@ -52,9 +52,11 @@ FIT_SOURCE = np.dtype([('profile', '<i4'), ('x0', '<i4'), ('y0', '<i4'), ('w', '
                        ('h', '<i4'), ('blob', '<i4'), ('frozen', '<i4'), ('pad', '<i4')])
 FIT_BLOB = np.dtype([('n_src', '<i4'), ('src0', '<i4'), ('P', '<i4'), ('unit0', '<i4'),
                      ('h_off', '<i8'), ('g_off', '<i8'), ('tile_off', '<i8'),
-                     ('n_active', '<i4'), ('n_tiles', '<i4')])
+                     ('n_active', '<i4'), ('n_tiles', '<i4'), ('n_slices', '<i4'),
+                     ('pad', '<i4')])
 FIT_UNIT = np.dtype([('blob', '<i4'), ('band', '<i4'), ('W', '<i4'), ('H', '<i4'),
-                     ('pix_off', '<i8'), ('psf_K', '<i4'), ('pad', '<i4'),
+                     ('pix_off', '<i8'), ('psf_K', '<i4'), ('slice', '<i4'),
+                     ('t0', '<i4'), ('t1', '<i4'),
                      ('psf_amp', '<f8', (4,)), ('psf_mean', '<f8', (8,)),
                      ('psf_var', '<f8', (16,))])
 FIT_STATE = np.dtype([('chi2', '<f8'), ('dlnp', '<f8'), ('lambda', '<f8'), ('pred', '<f8'),

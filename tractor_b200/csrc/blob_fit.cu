@@ -552,15 +552,16 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
         if (mode == 0 && state[u.blob].status != 0) continue;   // converged or stopped
         const int P = b.P;
         const int nsrc = b.n_src;
-        double* H = hbuf + b.h_off + (int64_t)u.band * P * P;
-        double* g = gbuf + b.g_off + (int64_t)u.band * P;
+        double* H = hbuf + b.h_off + (int64_t)u.slice * P * P;
+        double* g = gbuf + b.g_off + (int64_t)u.slice * P;
         if (mode == 0) {
             for (int e = tid; e < P * P; e += kThreads) H[e] = 0.0;
             for (int e = tid; e < P; e += kThreads) g[e] = 0.0;
         }
         if (tid == 0) {
             int bad = nsrc > TB_FIT_MAX_SRC || P != nsrc * TB_FIT_NPAR || u.psf_K < 1 ||
-                      u.psf_K > TB_FIT_MAX_PSF || u.band >= n_bands;
+                      u.psf_K > TB_FIT_MAX_PSF || u.band >= n_bands || u.slice < 0 ||
+                      u.slice >= b.n_slices || u.t0 < 0 || u.t1 < u.t0 || u.t1 > b.n_active;
             for (int s2 = 0; s2 < nsrc && !bad; s2++) bad = !tab[b.src0 + s2].ok;
             sm.skip = bad;
             if (bad) tb::report(st, TB_STATUS_BAD_ITEM, ui, nsrc);
@@ -568,16 +569,17 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
         __syncthreads();
         if (sm.skip) {
             if (tid == 0) {
-                if (mode == 0) chi2_part[b.unit0 + u.band] = INFINITY;
-                else chi2_const[b.unit0 + u.band] = INFINITY;
+                if (mode == 0) chi2_part[b.unit0 + u.slice] = INFINITY;
+                else chi2_const[b.unit0 + u.slice] = INFINITY;
             }
             continue;
         }
         double chi2 = 0.0;
-        // mode 0: the tiles some source's mask reaches; mode 1: the others
-        // (their chi^2 does not depend on the parameters)
-        const int n_t = mode == 0 ? b.n_active : b.n_tiles - b.n_active;
-        const int32_t* tl = tiles + b.tile_off + (mode == 0 ? 0 : b.n_active);
+        // mode 0: the unit's range of the tiles some source's mask reaches;
+        // mode 1: the others (their chi^2 does not depend on the parameters),
+        // covered by the unit that starts the range
+        const int n_t = mode == 0 ? u.t1 - u.t0 : (u.t0 == 0 ? b.n_tiles - b.n_active : 0);
+        const int32_t* tl = tiles + b.tile_off + (mode == 0 ? u.t0 : b.n_active);
         // this thread's pixel of tile t (0 outside the image)
         auto load_px = [&](int t, float& d, float& w) {
             d = 0.f;
@@ -703,8 +705,8 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
         if (tid == 0) {
             double s = 0.0;
             for (int w2 = 0; w2 < kThreads / 32; w2++) s += sm.red[w2];
-            if (mode == 0) chi2_part[b.unit0 + u.band] = s + chi2_const[b.unit0 + u.band];
-            else chi2_const[b.unit0 + u.band] = s;
+            if (mode == 0) chi2_part[b.unit0 + u.slice] = s + chi2_const[b.unit0 + u.slice];
+            else chi2_const[b.unit0 + u.slice] = s;
         }
         __syncthreads();
     }
@@ -747,17 +749,18 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     __syncthreads();   // every thread has read the status before thread 0 updates it
     if (status0 != 0) return;
     const int P = b.P;
-    double* Hp = hbuf + b.h_off;                        // band partials
-    double* Ha = Hp + (int64_t)n_bands * P * P;         // accepted H
+    const int ns = b.n_slices;
+    double* Hp = hbuf + b.h_off;                        // slice partials
+    double* Ha = Hp + (int64_t)ns * P * P;              // accepted H
     double* L = Ha + (int64_t)P * P;                    // Cholesky factor
     double* gp = gbuf + b.g_off;
-    double* ga = gp + (int64_t)n_bands * P;
+    double* ga = gp + (int64_t)ns * P;
     double* pa = params + (int64_t)b.src0 * TB_FIT_NPAR;
     double* pt = trial + (int64_t)b.src0 * TB_FIT_NPAR;
 
     if (tid == 0) {
         double c2 = 0.0;
-        for (int k = 0; k < n_bands; k++) c2 += chi2_part[b.unit0 + k];
+        for (int k = 0; k < ns; k++) c2 += chi2_part[b.unit0 + k];
         const bool first = S.accepted == 0;
         const bool acc = isfinite(c2) && (first || c2 < S.chi2);
         int status = 0;
@@ -787,12 +790,12 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
             const int i = e / P, j = e % P;
             const int r = min(i, j), c = max(i, j);
             double s = 0.0;
-            for (int k = 0; k < n_bands; k++) s += Hp[(int64_t)k * P * P + (int64_t)r * P + c];
+            for (int k = 0; k < ns; k++) s += Hp[(int64_t)k * P * P + (int64_t)r * P + c];
             Ha[e] = s;
         }
         for (int e = tid; e < P; e += kStepThreads) {
             double s = 0.0;
-            for (int k = 0; k < n_bands; k++) s += gp[(int64_t)k * P + e];
+            for (int k = 0; k < ns; k++) s += gp[(int64_t)k * P + e];
             ga[e] = s;
         }
     }

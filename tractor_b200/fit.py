@@ -25,6 +25,7 @@ import torch
 from . import _lib, batch, render
 
 NPAR = _lib.FIT_NPAR
+UNIT_TILES = 64      # active 32 x 8 tiles per pass unit (larger images are split)
 SERSIC_MIN, SERSIC_MAX = 0.29, 6.3
 
 
@@ -59,15 +60,21 @@ class BlobFitter(object):
         blobs['n_src'] = nsrc
         blobs['src0'] = blob_src[:-1]
         blobs['P'] = P
-        blobs['unit0'] = np.arange(self.n_blobs) * self.n_bands
-        hsz = (self.n_bands + 2) * P * P
-        gsz = (self.n_bands + 1) * P
-        blobs['h_off'] = np.concatenate([[0], np.cumsum(hsz)[:-1]])
-        blobs['g_off'] = np.concatenate([[0], np.cumsum(gsz)[:-1]])
         tiles, n_active, n_tiles = blob_tiles(sides, sources, blob_src)
         blobs['n_active'] = n_active
         blobs['n_tiles'] = n_tiles
         blobs['tile_off'] = np.concatenate([[0], np.cumsum(n_tiles)[:-1]])
+        # a band's active tiles go to ceil(n_active / UNIT_TILES) pass units,
+        # each with its own partial blocks (slices), so that no unit holds
+        # one CTA for long while few blobs are still running
+        parts = np.maximum(1, -(-n_active // UNIT_TILES)).astype(np.int64)
+        n_slices = self.n_bands * parts
+        blobs['n_slices'] = n_slices
+        blobs['unit0'] = np.concatenate([[0], np.cumsum(n_slices)[:-1]])
+        hsz = (n_slices + 2) * P * P
+        gsz = (n_slices + 1) * P
+        blobs['h_off'] = np.concatenate([[0], np.cumsum(hsz)[:-1]])
+        blobs['g_off'] = np.concatenate([[0], np.cumsum(gsz)[:-1]])
         self.pix_offsets = pix_offsets(sides, self.n_bands)
         units = np.zeros(self.n_blobs * self.n_bands, _lib.FIT_UNIT)
         for b in range(self.n_blobs):
@@ -84,8 +91,23 @@ class BlobFitter(object):
                 u['psf_amp'][:K] = amp
                 u['psf_mean'][:2 * K] = np.asarray(mean, np.float64).ravel()
                 u['psf_var'][:4 * K] = np.asarray(var, np.float64).ravel()
+        units['t1'] = n_active[units['blob']]
+        units['slice'] = units['band']
+        # pass units: the (blob, band) images split into tile ranges
+        pu = []
+        for b in range(self.n_blobs):
+            q = int(parts[b])
+            cut = (np.arange(q + 1) * int(n_active[b])) // q
+            for k in range(self.n_bands):
+                for j in range(q):
+                    u = units[b * self.n_bands + k].copy()
+                    u['slice'] = k * q + j
+                    u['t0'], u['t1'] = cut[j], cut[j + 1]
+                    pu.append(u)
+        pass_units = np.array(pu, _lib.FIT_UNIT)
         # the pass takes units largest first
-        cost = n_active[units['blob']].astype(np.float64) * (1 + nsrc[units['blob']])
+        cost = (pass_units['t1'] - pass_units['t0']).astype(np.float64) * \
+            (1 + nsrc[pass_units['blob']])
         order = np.argsort(-cost, kind='stable').astype(np.int32)
         npix = int(self.pix_offsets[-1])
         if data.numel() < npix or inverr.numel() < npix:
@@ -93,8 +115,9 @@ class BlobFitter(object):
                              (min(data.numel(), inverr.numel()), npix))
         self.data, self.inverr = data, inverr
         to = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(self.dev)
-        self.blobs_np, self.units_np = blobs, units
+        self.blobs_np, self.units_np, self.pass_units_np = blobs, units, pass_units
         self.d_blobs, self.d_units = to(blobs), to(units)
+        self.d_pass_units = to(pass_units)
         self.d_order = torch.from_numpy(order).to(self.dev)
         self.sources_np = np.ascontiguousarray(sources, _lib.FIT_SOURCE).copy()
         self.sources_np['blob'] = np.repeat(np.arange(self.n_blobs), nsrc)
@@ -105,7 +128,7 @@ class BlobFitter(object):
         self.hbuf = torch.zeros(int(hsz.sum()), dtype=torch.float64, device=self.dev)
         self.gbuf = torch.zeros(int(gsz.sum()), dtype=torch.float64, device=self.dev)
         self.d_tiles = torch.from_numpy(tiles).to(self.dev)
-        self.chi2_part = torch.zeros(self.n_blobs * self.n_bands, dtype=torch.float64,
+        self.chi2_part = torch.zeros(int(n_slices.sum()), dtype=torch.float64,
                                      device=self.dev)
         self.chi2_const = torch.zeros_like(self.chi2_part)
         self._const_done = False
@@ -132,8 +155,8 @@ class BlobFitter(object):
 
     def _pass(self, mode):
         lib = _lib.load()
-        _lib.check(lib.tb_fit_pass(self.d_units.data_ptr(), self.d_order.data_ptr(),
-                                   len(self.units_np), self.d_blobs.data_ptr(),
+        _lib.check(lib.tb_fit_pass(self.d_pass_units.data_ptr(), self.d_order.data_ptr(),
+                                   len(self.pass_units_np), self.d_blobs.data_ptr(),
                                    self.d_sources.data_ptr(), self.n_src,
                                    self.workspace.data_ptr(), self.data.data_ptr(),
                                    self.inverr.data_ptr(), self.d_tiles.data_ptr(),
@@ -227,8 +250,8 @@ class BlobFitter(object):
         """(H, g) of blob b at the last accepted parameters (FP64, host)."""
         bl = self.blobs_np[b]
         P = int(bl['P'])
-        h0 = int(bl['h_off']) + self.n_bands * P * P
-        g0 = int(bl['g_off']) + self.n_bands * P
+        h0 = int(bl['h_off']) + int(bl['n_slices']) * P * P
+        g0 = int(bl['g_off']) + int(bl['n_slices']) * P
         H = self.hbuf[h0:h0 + P * P].cpu().numpy().reshape(P, P)
         g = self.gbuf[g0:g0 + P].cpu().numpy()
         return H, g
