@@ -254,6 +254,8 @@ struct TileRec {
 
 struct PassSmem {
     float A[2][kG * kCols][kLd];   // two column groups
+    float hstage[kG * kCols][kG * kCols];   // a block of A^T A before its global update
+    float gstage[kG * kCols];               // a group's A^T r before its global update
     FitS comps[kStageMax];
     TileRec recs[TB_FIT_MAX_SRC];
     float r[kThreads];
@@ -499,15 +501,21 @@ __device__ void add_block(PassSmem& sm, float (*Aa)[kLd], int qa0, int na, float
         if (lane < 4) {
             const int di = lane >> 1, dj = lane & 1;
             const int ii = i + di, jj = j + dj;
-            if (ii < ca && jj < cb && !(diag && jj < ii)) {
-                const float v = di == 0 ? (dj == 0 ? s00 : s01) : (dj == 0 ? s10 : s11);
-                const int ga = col_of(sm.recs[qa0 + ii / kCols].src, ii % kCols, band, n_bands);
-                const int gb = col_of(sm.recs[qb0 + jj / kCols].src, jj % kCols, band, n_bands);
-                // upper triangle in global parameter order
-                const int r = min(ga, gb), c = max(ga, gb);
-                H[(int64_t)r * P + c] += (double)v;
-            }
+            if (ii < ca && jj < cb && !(diag && jj < ii))
+                sm.hstage[ii][jj] = di == 0 ? (dj == 0 ? s00 : s01) : (dj == 0 ? s10 : s11);
         }
+    }
+    __syncthreads();
+    // the block's global updates by all threads at once (each element once:
+    // independent read-modify-writes instead of a chain per warp)
+    for (int e = threadIdx.x; e < ca * cb; e += kThreads) {
+        const int ii = e / cb, jj = e % cb;
+        if (diag && jj < ii) continue;
+        const int ga = col_of(sm.recs[qa0 + ii / kCols].src, ii % kCols, band, n_bands);
+        const int gb = col_of(sm.recs[qb0 + jj / kCols].src, jj % kCols, band, n_bands);
+        // upper triangle in global parameter order
+        const int r = min(ga, gb), c = max(ga, gb);
+        H[(int64_t)r * P + c] += (double)sm.hstage[ii][jj];
     }
     __syncthreads();
 }
@@ -520,8 +528,11 @@ __device__ void add_grad(PassSmem& sm, float (*A)[kLd], int q0, int nq, double* 
         float s = 0.f;
         for (int p = lane; p < kThreads; p += 32) s = fmaf(A[c][p], sm.r[p], s);
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) g[col_of(sm.recs[q0 + c / kCols].src, c % kCols, band, n_bands)] += (double)s;
+        if (lane == 0) sm.gstage[c] = s;
     }
+    __syncthreads();
+    for (int c = threadIdx.x; c < nq * kCols; c += kThreads)
+        g[col_of(sm.recs[q0 + c / kCols].src, c % kCols, band, n_bands)] += (double)sm.gstage[c];
     // no barrier: add_block only reads what this function reads
 }
 
