@@ -264,7 +264,76 @@ struct PassSmem {
     int64_t slot;
     int nrec;
     int skip;
+    int kc[kG];                    // staged (not culled) components per source of a group
 };
+
+// Largest exponent (log2 units) of a staged component over the pixel
+// rectangle [x0, x1] x [y0, y1] (tile-relative, inclusive).  The exponent
+// e = qxx dx^2 + qxy dx dy + qyy dy^2 is negative definite: its maximum is
+// 0 when the centre lies inside the rectangle, else it is on an edge, where
+// e is a 1-D quadratic with its maximiser clamped to the edge.
+__device__ __forceinline__ float max_exponent(float mx, float my, float qxx, float qxy, float qyy,
+                                              float x0, float x1, float y0, float y1) {
+    if (mx >= x0 && mx <= x1 && my >= y0 && my <= y1) return 0.f;
+    auto ev = [&](float x, float y) {
+        const float dx = x - mx, dy = y - my;
+        return fmaf(dx, fmaf(qxx, dx, qxy * dy), qyy * dy * dy);
+    };
+    float best = -INFINITY;
+    for (int side = 0; side < 2; side++) {
+        const float x = side ? x1 : x0;
+        const float y = fminf(fmaxf(my - qxy * (x - mx) / (2.f * qyy), y0), y1);
+        best = fmaxf(best, ev(x, y));
+        const float yy = side ? y1 : y0;
+        const float xx = fminf(fmaxf(mx - qxy * (yy - my) / (2.f * qxx), x0), x1);
+        best = fmaxf(best, ev(xx, yy));
+    }
+    return best;
+}
+
+// Builds the staged record of component k of a source, tile origin (ox, oy).
+__device__ __forceinline__ FitS stage_comp(const FitC& c, int ox, int oy) {
+    FitS f;
+    f.mx = (float)(c.mx - (double)ox);
+    f.my = (float)(c.my - (double)oy);
+    f.qxx = c.qxx; f.qxy = c.qxy; f.qyy = c.qyy;
+    f.ixx = c.ixx; f.ixy = c.ixy; f.iyy = c.iyy;
+    f.s = c.s; f.sn = c.sn; f.fl = c.fl; f.v = c.v; f.dv = c.dv;
+#pragma unroll
+    for (int j = 0; j < 4; j++) f.t[j] = c.t[j];
+    f.pad[0] = f.pad[1] = f.pad[2] = 0;
+    return f;
+}
+
+// Stages, by one warp, the components of one source that reach the pixel
+// rectangle [x0, x1] x [y0, y1] of this tile into comps[0 ..), in their
+// order; returns how many.  A component whose exponent stays below its
+// floor (minus a margin of 1, far above FP32 rounding) over the whole
+// rectangle contributes exactly zero to every pixel (E = 0, val = 0) and
+// is left out, so the sums over the staged components are the same.
+// Components with non-finite coefficients are always staged.
+__device__ __forceinline__ int stage_source(FitS* comps, const FitC* __restrict__ src_comps, int K,
+                                            int ox, int oy, float x0, float x1, float y0,
+                                            float y1) {
+    const int lane = threadIdx.x & 31;
+    int n = 0;
+    for (int k0 = 0; k0 < K; k0 += 32) {
+        const int k = k0 + lane;
+        bool keep = false;
+        if (k < K) {
+            const FitC& c = src_comps[k];
+            const float mx = (float)(c.mx - (double)ox), my = (float)(c.my - (double)oy);
+            const bool finite = isfinite(c.qxx) && isfinite(c.qxy) && isfinite(c.qyy) &&
+                                isfinite(mx) && isfinite(my);
+            keep = !finite ||
+                   !(max_exponent(mx, my, c.qxx, c.qxy, c.qyy, x0, x1, y0, y1) < c.fl - 1.f);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) comps[n + __popc(bal & ((1u << lane) - 1u))] = stage_comp(src_comps[k], ox, oy);
+        n += __popc(bal);
+    }
+    return n;
+}
 
 // Evaluates sources [q0, q0 + nq) of the tile list at this thread's pixel.
 // kDeriv: writes the 7 weighted columns of each source into `A` (column
@@ -279,32 +348,24 @@ __device__ float eval_group(PassSmem& sm, const FitC* __restrict__ gcomps, int s
                             float (*A)[kLd], bool need_sync) {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    // stage components: record-major, PSF component outer, galaxy inner
-    int total = 0;
-    for (int q = q0; q < q0 + nq; q++) total += sm.recs[q].K;
+    // stage components, source q at comps[(q - q0) kCompStride ..] (PSF
+    // component outer, galaxy inner), culled to the source's rectangle in
+    // this tile; warp w stages source q0 + w
     if (need_sync) __syncthreads();
-    for (int g = tid; g < total; g += kThreads) {
-        int q = q0, k = g;
-        while (k >= sm.recs[q].K) { k -= sm.recs[q].K; q++; }
-        const FitC& c = gcomps[((int64_t)(src0 + sm.recs[q].src) * n_bands + band) * kCompStride + k];
-        FitS f;
-        f.mx = (float)(c.mx - (double)ox);
-        f.my = (float)(c.my - (double)oy);
-        f.qxx = c.qxx; f.qxy = c.qxy; f.qyy = c.qyy;
-        f.ixx = c.ixx; f.ixy = c.ixy; f.iyy = c.iyy;
-        f.s = c.s; f.sn = c.sn; f.fl = c.fl; f.v = c.v; f.dv = c.dv;
-#pragma unroll
-        for (int j = 0; j < 4; j++) f.t[j] = c.t[j];
-        f.pad[0] = f.pad[1] = f.pad[2] = 0;
-        sm.comps[g] = f;
+    if (warp < nq) {
+        const TileRec& R = sm.recs[q0 + warp];
+        const int n = stage_source(
+            sm.comps + warp * kCompStride,
+            gcomps + ((int64_t)(src0 + R.src) * n_bands + band) * kCompStride, R.K, ox, oy,
+            (float)R.x0, (float)(R.x1 - 1), (float)R.y0, (float)(R.y1 - 1));
+        if (lane == 0) sm.kc[warp] = n;
     }
     __syncthreads();
     const float xf = (float)lane, yf = (float)warp;
     float model = 0.f;
-    int kb = 0;
     for (int q = q0; q < q0 + nq; q++) {
         const TileRec& R = sm.recs[q];
-        const int K = R.K;
+        const int K = sm.kc[q - q0], kb = (q - q0) * kCompStride;
         // per-source moments over its components (see FitC)
         float m = 0.f, jx = 0.f, jy = 0.f, jn = 0.f;
         float axx = 0.f, axy = 0.f, ayy = 0.f, t0 = 0.f, t1 = 0.f, t2 = 0.f;
@@ -337,7 +398,6 @@ __device__ float eval_group(PassSmem& sm, const FitC* __restrict__ gcomps, int s
                 jn = fmaf(c.sn, E, jn);
             }
         }
-        kb += K;
         // source done: add its patch inside its rectangle and write its
         // weighted columns, d/dtheta = 1/2 (dM : sum v val u u^T - sum v val tr(C^-1 dM))
         const bool in = lane >= R.x0 && lane < R.x1 && warp >= R.y0 && warp < R.y1;
@@ -377,21 +437,16 @@ __device__ float eval_single(PassSmem& sm, const FitC* __restrict__ gcomps,
                              int n_bands, int ox, int oy, float w, float* J) {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int K = S.K[band];
-    for (int g = tid; g < K; g += kThreads) {
-        const FitC& c = gcomps[((int64_t)src_global * n_bands + band) * kCompStride + g];
-        FitS f;
-        f.mx = (float)(c.mx - (double)ox);
-        f.my = (float)(c.my - (double)oy);
-        f.qxx = c.qxx; f.qxy = c.qxy; f.qyy = c.qyy;
-        f.ixx = c.ixx; f.ixy = c.ixy; f.iyy = c.iyy;
-        f.s = c.s; f.sn = c.sn; f.fl = c.fl; f.v = c.v; f.dv = c.dv;
-#pragma unroll
-        for (int j = 0; j < 4; j++) f.t[j] = c.t[j];
-        f.pad[0] = f.pad[1] = f.pad[2] = 0;
-        sm.comps[g] = f;
+    // the source's components that reach its rectangle in this tile
+    if (warp == 0) {
+        const int n = stage_source(
+            sm.comps, gcomps + ((int64_t)src_global * n_bands + band) * kCompStride, S.K[band],
+            ox, oy, (float)max(fs.x0 - ox, 0), (float)(min(fs.x0 + fs.w - ox, kTileW) - 1),
+            (float)max(fs.y0 - oy, 0), (float)(min(fs.y0 + fs.h - oy, kTileH) - 1));
+        if (lane == 0) sm.kc[0] = n;
     }
     __syncthreads();
+    const int K = sm.kc[0];
     const float xf = (float)lane, yf = (float)warp;
     float m = 0.f, jx = 0.f, jy = 0.f, jn = 0.f;
     float axx = 0.f, axy = 0.f, ayy = 0.f, t0 = 0.f, t1 = 0.f, t2 = 0.f;
@@ -536,7 +591,7 @@ __device__ void add_grad(PassSmem& sm, float (*A)[kLd], int q0, int nq, double* 
     // no barrier: add_block only reads what this function reads
 }
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict__ order,
                 int n_units, const tb_fit_blob* __restrict__ blobs,
                 const tb_fit_source* __restrict__ srcs, const SrcTab* __restrict__ tab,
