@@ -35,7 +35,6 @@ constexpr int kTileH = 8;
 constexpr int kCols = 7;               // columns per (source, band): x y flux logre ee1 ee2 n
 constexpr int kG = 4;                  // sources per shared-memory column group
 constexpr int kLd = kThreads + 1;      // padded column stride (floats)
-constexpr int kStageMax = kG * kMaxGalK * TB_FIT_MAX_PSF;
 constexpr double kHn = 1e-5;           // central-difference step in n
 constexpr double kHs = 1e-6;           // central-difference step in shape parameters
 
@@ -70,12 +69,17 @@ struct FitC {
     int32_t pad[7];
 };
 
-// The same, staged in shared memory for one tile (FP32 tile-relative mean).
-struct FitS {
-    float mx, my;
-    float qxx, qxy, qyy, ixx, ixy, iyy, s, sn, fl, v, dv;
-    float t[4];
-    int32_t pad[3];
+// One component staged for one pixel row y of a tile (origin (ox, oy)) by
+// the warp that owns the row: its FP32 tile-relative mean x, the exponent
+// along the row e(dx) = qxx dx^2 + bx dx + c0 (bx = qxy dy, c0 = qyy dy^2,
+// dy = y - my), C^-1 u = (ixx dx + uxy, ixy dx + uyy) (uxy = ixy dy,
+// uyy = iyy dy), and the per-component factors of FitC.
+struct __align__(16) FitR {
+    float mx, qxx, bx, c0;
+    float s, fl, ixx, ixy;
+    float uxy, uyy, sn, v;
+    float dv, t0, t1, t2;
+    float t3, pad[3];
 };
 
 // ---------------------------------------------------------------------------
@@ -242,145 +246,112 @@ fit_prep_kernel(const tb_fit_source* __restrict__ srcs, int n, const double* __r
 // pass
 // ---------------------------------------------------------------------------
 
-struct TileRec {
-    int32_t x0, x1, y0, y1;   // rectangle, tile-relative, clipped to the tile
-    float counts;
-    int32_t src;              // source index within the blob
-    int32_t K;                // components (galaxy x PSF)
-    int32_t pad;
+// One source of the unit (its mask rectangle and shape factors in the
+// unit's band), copied to shared memory once per unit.
+struct UnitSrc {
+    int32_t x0, y0, x1, y1;   // mask [x0, x1) x [y0, y1), image pixels; an empty mask is all 0
+    float counts;             // flux in the unit's band
+    int32_t K;                // components (galaxy x PSF) in the unit's band
     float M[3];               // T T^T (xx, xy, yy)
     float dM[3][3];           // its shape derivatives
 };
 
 struct PassSmem {
-    float A[2][kG * kCols][kLd];   // two column groups
+    float A[2][kG * kCols][kLd];            // two column groups (multi-source tiles)
     float hstage[kG * kCols][kG * kCols];   // a block of A^T A before its global update
     float gstage[kG * kCols];               // a group's A^T r before its global update
-    FitS comps[kStageMax];
-    TileRec recs[TB_FIT_MAX_SRC];
+    FitR wc[kThreads / 32][kCompStride];    // each warp's components staged for its pixel row
+    UnitSrc us[TB_FIT_MAX_SRC];
     float r[kThreads];
     float runred[kThreads / 32][36];
     double red[kThreads / 32];
     int64_t slot;
-    int nrec;
     int skip;
-    int kc[kG];                    // staged (not culled) components per source of a group
 };
 
-// Largest exponent (log2 units) of a staged component over the pixel
-// rectangle [x0, x1] x [y0, y1] (tile-relative, inclusive).  The exponent
-// e = qxx dx^2 + qxy dx dy + qyy dy^2 is negative definite: its maximum is
-// 0 when the centre lies inside the rectangle, else it is on an edge, where
-// e is a 1-D quadratic with its maximiser clamped to the edge.
-__device__ __forceinline__ float max_exponent(float mx, float my, float qxx, float qxy, float qyy,
-                                              float x0, float x1, float y0, float y1) {
-    if (mx >= x0 && mx <= x1 && my >= y0 && my <= y1) return 0.f;
-    auto ev = [&](float x, float y) {
-        const float dx = x - mx, dy = y - my;
-        return fmaf(dx, fmaf(qxx, dx, qxy * dy), qyy * dy * dy);
-    };
-    float best = -INFINITY;
-    for (int side = 0; side < 2; side++) {
-        const float x = side ? x1 : x0;
-        const float y = fminf(fmaxf(my - qxy * (x - mx) / (2.f * qyy), y0), y1);
-        best = fmaxf(best, ev(x, y));
-        const float yy = side ? y1 : y0;
-        const float xx = fminf(fmaxf(mx - qxy * (yy - my) / (2.f * qxx), x0), x1);
-        best = fmaxf(best, ev(xx, yy));
-    }
-    return best;
-}
-
-// Builds the staged record of component k of a source, tile origin (ox, oy).
-__device__ __forceinline__ FitS stage_comp(const FitC& c, int ox, int oy) {
-    FitS f;
-    f.mx = (float)(c.mx - (double)ox);
-    f.my = (float)(c.my - (double)oy);
-    f.qxx = c.qxx; f.qxy = c.qxy; f.qyy = c.qyy;
-    f.ixx = c.ixx; f.ixy = c.ixy; f.iyy = c.iyy;
-    f.s = c.s; f.sn = c.sn; f.fl = c.fl; f.v = c.v; f.dv = c.dv;
-#pragma unroll
-    for (int j = 0; j < 4; j++) f.t[j] = c.t[j];
-    f.pad[0] = f.pad[1] = f.pad[2] = 0;
-    return f;
-}
-
-// Stages, by one warp, the components of one source that reach the pixel
-// rectangle [x0, x1] x [y0, y1] of this tile into comps[0 ..), in their
-// order; returns how many.  A component whose exponent stays below its
-// floor (minus a margin of 1, far above FP32 rounding) over the whole
-// rectangle contributes exactly zero to every pixel (E = 0, val = 0) and
-// is left out, so the sums over the staged components are the same.
-// Components with non-finite coefficients are always staged.
-__device__ __forceinline__ int stage_source(FitS* comps, const FitC* __restrict__ src_comps, int K,
-                                            int ox, int oy, float x0, float x1, float y0,
-                                            float y1) {
+// Stages, by one warp, the components of one source (src_comps[0, K)) that
+// reach pixels [x0, x1] (tile-relative, inclusive) of row y of the tile at
+// (ox, oy) into wc[0 ..), in their order; returns how many.  Along a row
+// the exponent is a concave quadratic in dx whose maximum over the segment
+// is at its vertex clamped to the segment.  A component whose maximum
+// stays below its floor (minus a margin of 1, far above FP32 rounding)
+// contributes exactly zero to every pixel of the segment (E = 0, val = 0)
+// and is left out, so the sums over the staged components are the same.
+// Components with non-finite or non-concave coefficients are always staged.
+// The row terms are computed as the per-pixel expressions would compute
+// them, so every pixel's exponent and C^-1 u is bit-identical.
+__device__ __forceinline__ int stage_row(FitR* wc, const FitC* __restrict__ src_comps, int K,
+                                         int ox, int oy, int y, float x0, float x1) {
     const int lane = threadIdx.x & 31;
     int n = 0;
+    __syncwarp();   // the warp's previous components are no longer read
     for (int k0 = 0; k0 < K; k0 += 32) {
         const int k = k0 + lane;
         bool keep = false;
+        float mx = 0.f, dy = 0.f, bx = 0.f, c0 = 0.f;
         if (k < K) {
             const FitC& c = src_comps[k];
-            const float mx = (float)(c.mx - (double)ox), my = (float)(c.my - (double)oy);
-            const bool finite = isfinite(c.qxx) && isfinite(c.qxy) && isfinite(c.qyy) &&
-                                isfinite(mx) && isfinite(my);
-            keep = !finite ||
-                   !(max_exponent(mx, my, c.qxx, c.qxy, c.qyy, x0, x1, y0, y1) < c.fl - 1.f);
+            mx = (float)(c.mx - (double)ox);
+            dy = (float)y - (float)(c.my - (double)oy);
+            bx = c.qxy * dy;
+            c0 = c.qyy * dy * dy;
+            const float qxx = c.qxx;
+            const bool ok = isfinite(mx) && isfinite(bx) && isfinite(c0) && qxx < 0.f;
+            float emax = 0.f;
+            if (ok) {
+                const float xs = fminf(fmaxf(mx - bx / (2.f * qxx), x0), x1);
+                const float dx = xs - mx;
+                emax = fmaf(dx, fmaf(qxx, dx, bx), c0);
+            }
+            keep = !ok || !(emax < c.fl - 1.f);
         }
         const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (keep) comps[n + __popc(bal & ((1u << lane) - 1u))] = stage_comp(src_comps[k], ox, oy);
+        if (keep) {
+            const FitC& c = src_comps[k];
+            float4* f = reinterpret_cast<float4*>(wc + n + __popc(bal & ((1u << lane) - 1u)));
+            f[0] = make_float4(mx, c.qxx, bx, c0);
+            f[1] = make_float4(c.s, c.fl, c.ixx, c.ixy);
+            f[2] = make_float4(c.ixy * dy, c.iyy * dy, c.sn, c.v);
+            f[3] = make_float4(c.dv, c.t[0], c.t[1], c.t[2]);
+            f[4] = make_float4(c.t[3], 0.f, 0.f, 0.f);
+        }
         n += __popc(bal);
     }
+    __syncwarp();   // staged components visible to the whole warp
     return n;
 }
 
-// Evaluates sources [q0, q0 + nq) of the tile list at this thread's pixel.
-// kDeriv: writes the 7 weighted columns of each source into `A` (column
-// 7 (q - q0) + c) and returns the model; otherwise returns the model only.
-// Every source of the group has components (a unit with a source that has
-// none is skipped), so each of the group's 7 nq columns is written.
-// need_sync: other threads may still read comps / A (a second group of the
-// same tile); the first group of a tile follows a barrier already.
+// One source at this thread's pixel (lane, warp) of the tile at (ox, oy):
+// returns its model (counts x its PSF-convolved mixture, 0 outside its
+// mask) and, with kDeriv, its 7 weighted derivative columns in J (0 outside
+// the mask), d/dtheta = 1/2 (dM : sum v val u u^T - sum v val tr(C^-1 dM))
+// for the shape and likewise (M, dv) for the index.  The warp stages the
+// components that reach its row of the mask; a row outside the mask
+// evaluates nothing.  No block barrier: each warp works on its own.
 template <bool kDeriv>
-__device__ float eval_group(PassSmem& sm, const FitC* __restrict__ gcomps, int src0, int band,
-                            int n_bands, int q0, int nq, int ox, int oy, float w,
-                            float (*A)[kLd], bool need_sync) {
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    // stage components, source q at comps[(q - q0) kCompStride ..] (PSF
-    // component outer, galaxy inner), culled to the source's rectangle in
-    // this tile; warp w stages source q0 + w
-    if (need_sync) __syncthreads();
-    if (warp < nq) {
-        const TileRec& R = sm.recs[q0 + warp];
-        const int n = stage_source(
-            sm.comps + warp * kCompStride,
-            gcomps + ((int64_t)(src0 + R.src) * n_bands + band) * kCompStride, R.K, ox, oy,
-            (float)R.x0, (float)(R.x1 - 1), (float)R.y0, (float)(R.y1 - 1));
-        if (lane == 0) sm.kc[warp] = n;
-    }
-    __syncthreads();
-    const float xf = (float)lane, yf = (float)warp;
-    float model = 0.f;
-    for (int q = q0; q < q0 + nq; q++) {
-        const TileRec& R = sm.recs[q];
-        const int K = sm.kc[q - q0], kb = (q - q0) * kCompStride;
-        // per-source moments over its components (see FitC)
-        float m = 0.f, jx = 0.f, jy = 0.f, jn = 0.f;
-        float axx = 0.f, axy = 0.f, ayy = 0.f, t0 = 0.f, t1 = 0.f, t2 = 0.f;
-        float bxx = 0.f, bxy = 0.f, byy = 0.f, tn = 0.f;
+__device__ __forceinline__ float eval_source(FitR* wc, const FitC* __restrict__ src_comps,
+                                             const UnitSrc& U, int ox, int oy, float w,
+                                             float* J) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int xa = max(U.x0 - ox, 0), xb = min(U.x1 - ox, kTileW);
+    const bool row = warp >= U.y0 - oy && warp < U.y1 - oy && xa < xb;   // warp-uniform
+    float m = 0.f, jx = 0.f, jy = 0.f, jn = 0.f;
+    float axx = 0.f, axy = 0.f, ayy = 0.f, t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    float bxx = 0.f, bxy = 0.f, byy = 0.f, tn = 0.f;
+    if (row) {
+        const int K = stage_row(wc, src_comps, U.K, ox, oy, warp, (float)xa, (float)(xb - 1));
+        const float xf = (float)lane;
 #pragma unroll 2
-        for (int g = kb; g < kb + K; g++) {
-            const FitS& c = sm.comps[g];
-            const float dx = xf - c.mx, dy = yf - c.my;
-            const float e = fmaf(dx, fmaf(c.qxx, dx, c.qxy * dy), c.qyy * dy * dy);
+        for (int g = 0; g < K; g++) {
+            const FitR& c = wc[g];
+            const float dx = xf - c.mx;
+            const float e = fmaf(dx, fmaf(c.qxx, dx, c.bx), c.c0);
             const float E = (e >= c.fl) ? tb::ex2(e) : 0.f;
             const float val = c.s * E;
             m += val;
             if (kDeriv) {
-                const float ux = fmaf(c.ixx, dx, c.ixy * dy);
-                const float uy = fmaf(c.ixy, dx, c.iyy * dy);
+                const float ux = fmaf(c.ixx, dx, c.uxy);
+                const float uy = fmaf(c.ixy, dx, c.uyy);
                 jx = fmaf(val, ux, jx);
                 jy = fmaf(val, uy, jy);
                 const float pxx = ux * ux, pxy = ux * uy, pyy = uy * uy;
@@ -388,116 +359,77 @@ __device__ float eval_group(PassSmem& sm, const FitC* __restrict__ gcomps, int s
                 axx = fmaf(sv, pxx, axx);
                 axy = fmaf(sv, pxy, axy);
                 ayy = fmaf(sv, pyy, ayy);
-                t0 = fmaf(sv, c.t[0], t0);
-                t1 = fmaf(sv, c.t[1], t1);
-                t2 = fmaf(sv, c.t[2], t2);
+                t0 = fmaf(sv, c.t0, t0);
+                t1 = fmaf(sv, c.t1, t1);
+                t2 = fmaf(sv, c.t2, t2);
                 bxx = fmaf(wv, pxx, bxx);
                 bxy = fmaf(wv, pxy, bxy);
                 byy = fmaf(wv, pyy, byy);
-                tn = fmaf(wv, c.t[3], tn);
+                tn = fmaf(wv, c.t3, tn);
                 jn = fmaf(c.sn, E, jn);
             }
         }
-        // source done: add its patch inside its rectangle and write its
-        // weighted columns, d/dtheta = 1/2 (dM : sum v val u u^T - sum v val tr(C^-1 dM))
-        const bool in = lane >= R.x0 && lane < R.x1 && warp >= R.y0 && warp < R.y1;
-        const float cnt = R.counts;
-        model += in ? cnt * m : 0.f;
+    }
+    const bool in = row && lane >= xa && lane < xb;
+    const float cnt = U.counts;
+    if (kDeriv) {
+        const float cw = in ? cnt * w : 0.f;
+        const float h = 0.5f * cw;
+        J[0] = cw * jx;
+        J[1] = cw * jy;
+        J[2] = in ? w * m : 0.f;
+        J[3] = h * (fmaf(U.dM[0][0], axx, fmaf(2.f * U.dM[0][1], axy, U.dM[0][2] * ayy)) - t0);
+        J[4] = h * (fmaf(U.dM[1][0], axx, fmaf(2.f * U.dM[1][1], axy, U.dM[1][2] * ayy)) - t1);
+        J[5] = h * (fmaf(U.dM[2][0], axx, fmaf(2.f * U.dM[2][1], axy, U.dM[2][2] * ayy)) - t2);
+        J[6] = h * (fmaf(U.M[0], bxx, fmaf(2.f * U.M[1], bxy, U.M[2] * byy)) - tn) + cw * jn;
+    }
+    return in ? cnt * m : 0.f;
+}
+
+// Position of the (q+1)-th set bit of m (q < popc(m)).
+__device__ __forceinline__ int nth_bit(unsigned m, int q) {
+    for (int i = 0; i < q; i++) m &= m - 1u;
+    return __ffs(m) - 1;
+}
+
+// Sources q0 .. q0 + nq - 1 of the tile's hit list (the set bits of `hit`,
+// in source order) at this thread's pixel: returns their model; with
+// kDeriv writes the 7 columns of source q at A[7 (q - q0) + c][thread].
+// No block barrier inside.
+template <bool kDeriv>
+__device__ float eval_group(PassSmem& sm, const FitC* __restrict__ band_comps, int n_bands,
+                            unsigned hit, int q0, int nq, int ox, int oy, float w,
+                            float (*A)[kLd]) {
+    const int tid = threadIdx.x, warp = tid >> 5;
+    unsigned mm = hit;
+    for (int i = 0; i < q0; i++) mm &= mm - 1u;
+    float model = 0.f;
+    for (int q = q0; q < q0 + nq; q++) {
+        const int s = __ffs(mm) - 1;
+        mm &= mm - 1u;
+        float J[kCols];
+        model += eval_source<kDeriv>(sm.wc[warp], band_comps + (int64_t)s * n_bands * kCompStride,
+                                     sm.us[s], ox, oy, w, J);
         if (kDeriv) {
-            const float cw = in ? cnt * w : 0.f;
             float* col = &A[(q - q0) * kCols][tid];
-            col[0 * kLd] = cw * jx;
-            col[1 * kLd] = cw * jy;
-            col[2 * kLd] = in ? w * m : 0.f;
-            const float h = 0.5f * cw;
-            col[3 * kLd] = h * (fmaf(R.dM[0][0], axx, fmaf(2.f * R.dM[0][1], axy, R.dM[0][2] * ayy)) - t0);
-            col[4 * kLd] = h * (fmaf(R.dM[1][0], axx, fmaf(2.f * R.dM[1][1], axy, R.dM[1][2] * ayy)) - t1);
-            col[5 * kLd] = h * (fmaf(R.dM[2][0], axx, fmaf(2.f * R.dM[2][1], axy, R.dM[2][2] * ayy)) - t2);
-            col[6 * kLd] = h * (fmaf(R.M[0], bxx, fmaf(2.f * R.M[1], bxy, R.M[2] * byy)) - tn) +
-                           cw * jn;
+#pragma unroll
+            for (int c = 0; c < kCols; c++) col[c * kLd] = J[c];
         }
     }
-    __syncthreads();   // columns complete
     return model;
 }
 
-__device__ __forceinline__ int col_of(int src, int c, int band, int n_bands) {
+__device__ __forceinline__ int col_of(int src, int c, int band) {
     // parameter slots per source: x, y, flux[3], logre, ee1, ee2, n
-    (void)n_bands;
     const int off = c < 2 ? c : (c == 2 ? 2 + band : c + 2);
     return src * TB_FIT_NPAR + off;
-}
-
-// One source on this tile (the common case): model and the 7 weighted
-// derivative columns at this thread's pixel, returned in registers (J),
-// with the source's record built by every thread from the tables.  Two
-// barriers: after staging and at the end (the next tile restages).
-__device__ float eval_single(PassSmem& sm, const FitC* __restrict__ gcomps,
-                             const tb_fit_source& fs, const SrcTab& S, int src_global, int band,
-                             int n_bands, int ox, int oy, float w, float* J) {
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    // the source's components that reach its rectangle in this tile
-    if (warp == 0) {
-        const int n = stage_source(
-            sm.comps, gcomps + ((int64_t)src_global * n_bands + band) * kCompStride, S.K[band],
-            ox, oy, (float)max(fs.x0 - ox, 0), (float)(min(fs.x0 + fs.w - ox, kTileW) - 1),
-            (float)max(fs.y0 - oy, 0), (float)(min(fs.y0 + fs.h - oy, kTileH) - 1));
-        if (lane == 0) sm.kc[0] = n;
-    }
-    __syncthreads();
-    const int K = sm.kc[0];
-    const float xf = (float)lane, yf = (float)warp;
-    float m = 0.f, jx = 0.f, jy = 0.f, jn = 0.f;
-    float axx = 0.f, axy = 0.f, ayy = 0.f, t0 = 0.f, t1 = 0.f, t2 = 0.f;
-    float bxx = 0.f, bxy = 0.f, byy = 0.f, tn = 0.f;
-#pragma unroll 2
-    for (int g = 0; g < K; g++) {
-        const FitS& c = sm.comps[g];
-        const float dx = xf - c.mx, dy = yf - c.my;
-        const float e = fmaf(dx, fmaf(c.qxx, dx, c.qxy * dy), c.qyy * dy * dy);
-        const float E = (e >= c.fl) ? tb::ex2(e) : 0.f;
-        const float val = c.s * E;
-        m += val;
-        const float ux = fmaf(c.ixx, dx, c.ixy * dy);
-        const float uy = fmaf(c.ixy, dx, c.iyy * dy);
-        jx = fmaf(val, ux, jx);
-        jy = fmaf(val, uy, jy);
-        const float pxx = ux * ux, pxy = ux * uy, pyy = uy * uy;
-        const float sv = val * c.v, wv = val * c.dv;
-        axx = fmaf(sv, pxx, axx);
-        axy = fmaf(sv, pxy, axy);
-        ayy = fmaf(sv, pyy, ayy);
-        t0 = fmaf(sv, c.t[0], t0);
-        t1 = fmaf(sv, c.t[1], t1);
-        t2 = fmaf(sv, c.t[2], t2);
-        bxx = fmaf(wv, pxx, bxx);
-        bxy = fmaf(wv, pxy, bxy);
-        byy = fmaf(wv, pyy, byy);
-        tn = fmaf(wv, c.t[3], tn);
-        jn = fmaf(c.sn, E, jn);
-    }
-    __syncthreads();   // comps are restaged by the next tile
-    const int px = ox + lane, py = oy + warp;
-    const bool in = px >= fs.x0 && px < fs.x0 + fs.w && py >= fs.y0 && py < fs.y0 + fs.h;
-    const float cnt = (float)S.flux[band];
-    const float cw = in ? cnt * w : 0.f;
-    const float h = 0.5f * cw;
-    J[0] = cw * jx;
-    J[1] = cw * jy;
-    J[2] = in ? w * m : 0.f;
-    J[3] = h * (fmaf(S.dM[0][0], axx, fmaf(2.f * S.dM[0][1], axy, S.dM[0][2] * ayy)) - t0);
-    J[4] = h * (fmaf(S.dM[1][0], axx, fmaf(2.f * S.dM[1][1], axy, S.dM[1][2] * ayy)) - t1);
-    J[5] = h * (fmaf(S.dM[2][0], axx, fmaf(2.f * S.dM[2][1], axy, S.dM[2][2] * ayy)) - t2);
-    J[6] = h * (fmaf(S.M[0], bxx, fmaf(2.f * S.M[1], bxy, S.M[2] * byy)) - tn) + cw * jn;
-    return in ? cnt * m : 0.f;
 }
 
 // Adds a single-source run's register accumulators (this thread's share of
 // the 7 x 7 block's upper triangle and of A^T r) into the owned H / g:
 // warp reductions, then a fixed-order sum over warps.
 __device__ void flush_run(PassSmem& sm, float* hacc, float* gacc, int src, double* H, double* g,
-                          int P, int band, int n_bands) {
+                          int P, int band) {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll
@@ -516,79 +448,101 @@ __device__ void flush_run(PassSmem& sm, float* hacc, float* gacc, int src, doubl
             int c = 0, base = 0;
             while (base + (kCols - c) <= tid) { base += kCols - c; c++; }
             const int c2 = c + (tid - base);
-            const int r = col_of(src, c, band, n_bands), cc = col_of(src, c2, band, n_bands);
+            const int r = col_of(src, c, band), cc = col_of(src, c2, band);
             H[(int64_t)r * P + cc] += sum;
         } else {
-            g[col_of(src, tid - 28, band, n_bands)] += sum;
+            g[col_of(src, tid - 28, band)] += sum;
         }
     }
     __syncthreads();
 }
 
-// Adds A_a^T A_b (columns of groups a and b) into the owned H block: each
-// warp takes 2 x 2 blocks of column pairs and splits the tile's pixels over
-// its lanes (conflict-free consecutive shared-memory reads), then reduces.
-__device__ void add_block(PassSmem& sm, float (*Aa)[kLd], int qa0, int na, float (*Ab)[kLd],
-                          int qb0, int nb, bool diag, double* H, int P, int band, int n_bands) {
+// A_a^T A_b of the column groups in Aa (na sources) and Ab (nb sources)
+// into hstage (upper triangle when diag) and, with grad, A_a^T r into
+// gstage.  Tasks of 2 x 2 column pairs (or 2 gradient columns) go to the
+// warps in turn; each task splits the tile's pixels over the lanes
+// (conflict-free consecutive shared-memory reads), then reduces.
+__device__ void stage_products(PassSmem& sm, float (*Aa)[kLd], int na, float (*Ab)[kLd], int nb,
+                               bool diag, bool grad) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ca = na * kCols, cb = nb * kCols;
     const int ba = (ca + 1) / 2, bb = (cb + 1) / 2;
-    for (int e = warp; e < ba * bb; e += kThreads / 32) {
-        const int i = (e / bb) * 2, j = (e % bb) * 2;
-        if (diag && j + 1 < i) continue;   // upper triangle of 2 x 2 blocks (warp-uniform)
-        const int i1 = min(i + 1, ca - 1), j1 = min(j + 1, cb - 1);
-        float s00 = 0.f, s01 = 0.f, s10 = 0.f, s11 = 0.f;
+    const int nblk = diag ? ba * (ba + 1) / 2 : ba * bb;
+    const int ntask = nblk + (grad ? ba : 0);
+    for (int e = warp; e < ntask; e += kThreads / 32) {
+        if (e < nblk) {
+            int bi, bj;
+            if (diag) {   // row-major over the upper triangle of 2 x 2 blocks
+                int t = e;
+                bi = 0;
+                while (t >= ba - bi) { t -= ba - bi; bi++; }
+                bj = bi + t;
+            } else {
+                bi = e / bb;
+                bj = e % bb;
+            }
+            const int i = 2 * bi, j = 2 * bj;
+            const int i1 = min(i + 1, ca - 1), j1 = min(j + 1, cb - 1);
+            float s00 = 0.f, s01 = 0.f, s10 = 0.f, s11 = 0.f;
 #pragma unroll
-        for (int p = lane; p < kThreads; p += 32) {
-            const float x0 = Aa[i][p], x1 = Aa[i1][p], y0 = Ab[j][p], y1 = Ab[j1][p];
-            s00 = fmaf(x0, y0, s00);
-            s01 = fmaf(x0, y1, s01);
-            s10 = fmaf(x1, y0, s10);
-            s11 = fmaf(x1, y1, s11);
-        }
+            for (int p = lane; p < kThreads; p += 32) {
+                const float x0 = Aa[i][p], x1 = Aa[i1][p], y0 = Ab[j][p], y1 = Ab[j1][p];
+                s00 = fmaf(x0, y0, s00);
+                s01 = fmaf(x0, y1, s01);
+                s10 = fmaf(x1, y0, s10);
+                s11 = fmaf(x1, y1, s11);
+            }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            s00 += __shfl_xor_sync(0xffffffffu, s00, o);
-            s01 += __shfl_xor_sync(0xffffffffu, s01, o);
-            s10 += __shfl_xor_sync(0xffffffffu, s10, o);
-            s11 += __shfl_xor_sync(0xffffffffu, s11, o);
-        }
-        if (lane < 4) {
-            const int di = lane >> 1, dj = lane & 1;
-            const int ii = i + di, jj = j + dj;
-            if (ii < ca && jj < cb && !(diag && jj < ii))
-                sm.hstage[ii][jj] = di == 0 ? (dj == 0 ? s00 : s01) : (dj == 0 ? s10 : s11);
+            for (int o = 16; o > 0; o >>= 1) {
+                s00 += __shfl_xor_sync(0xffffffffu, s00, o);
+                s01 += __shfl_xor_sync(0xffffffffu, s01, o);
+                s10 += __shfl_xor_sync(0xffffffffu, s10, o);
+                s11 += __shfl_xor_sync(0xffffffffu, s11, o);
+            }
+            if (lane < 4) {
+                const int di = lane >> 1, dj = lane & 1;
+                const int ii = i + di, jj = j + dj;
+                if (ii < ca && jj < cb && !(diag && jj < ii))
+                    sm.hstage[ii][jj] = di == 0 ? (dj == 0 ? s00 : s01) : (dj == 0 ? s10 : s11);
+            }
+        } else {
+            const int i = 2 * (e - nblk), i1 = min(i + 1, ca - 1);
+            float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+            for (int p = lane; p < kThreads; p += 32) {
+                const float rp = sm.r[p];
+                s0 = fmaf(Aa[i][p], rp, s0);
+                s1 = fmaf(Aa[i1][p], rp, s1);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+                s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            }
+            if (lane == 0) sm.gstage[i] = s0;
+            if (lane == 1 && i + 1 < ca) sm.gstage[i + 1] = s1;
         }
     }
-    __syncthreads();
-    // the block's global updates by all threads at once (each element once:
-    // independent read-modify-writes instead of a chain per warp)
+}
+
+// The staged products' global updates by all threads at once (each element
+// of the owned H / g once: independent read-modify-writes).  Column c of
+// group a belongs to hit source qa0 + c / 7 (likewise for b).
+__device__ void apply_products(PassSmem& sm, unsigned hit, int qa0, int na, int qb0, int nb,
+                               bool diag, bool grad, double* H, double* g, int P, int band) {
+    const int ca = na * kCols, cb = nb * kCols;
     for (int e = threadIdx.x; e < ca * cb; e += kThreads) {
         const int ii = e / cb, jj = e % cb;
         if (diag && jj < ii) continue;
-        const int ga = col_of(sm.recs[qa0 + ii / kCols].src, ii % kCols, band, n_bands);
-        const int gb = col_of(sm.recs[qb0 + jj / kCols].src, jj % kCols, band, n_bands);
+        const int ga = col_of(nth_bit(hit, qa0 + ii / kCols), ii % kCols, band);
+        const int gb = col_of(nth_bit(hit, qb0 + jj / kCols), jj % kCols, band);
         // upper triangle in global parameter order
         const int r = min(ga, gb), c = max(ga, gb);
         H[(int64_t)r * P + c] += (double)sm.hstage[ii][jj];
     }
-    __syncthreads();
-}
-
-// A^T r of one group into the owned g vector (one warp per column).
-__device__ void add_grad(PassSmem& sm, float (*A)[kLd], int q0, int nq, double* g, int band,
-                         int n_bands) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int c = warp; c < nq * kCols; c += kThreads / 32) {
-        float s = 0.f;
-        for (int p = lane; p < kThreads; p += 32) s = fmaf(A[c][p], sm.r[p], s);
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) sm.gstage[c] = s;
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < nq * kCols; c += kThreads)
-        g[col_of(sm.recs[q0 + c / kCols].src, c % kCols, band, n_bands)] += (double)sm.gstage[c];
-    // no barrier: add_block only reads what this function reads
+    if (grad)
+        for (int c = threadIdx.x; c < ca; c += kThreads)
+            g[col_of(nth_bit(hit, qa0 + c / kCols), c % kCols, band)] += (double)sm.gstage[c];
 }
 
 __global__ void __launch_bounds__(kThreads, 2)
@@ -606,7 +560,7 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     for (;;) {
-        const int64_t oi = tb::next_unit(counter, &sm.slot);
+        const int64_t oi = tb::next_unit(counter, &sm.slot);   // barriers on both sides
         if (oi >= n_units) break;
         const int ui = order[oi];
         if (ui < 0 || ui >= n_units) {
@@ -624,13 +578,39 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
             for (int e = tid; e < P * P; e += kThreads) H[e] = 0.0;
             for (int e = tid; e < P; e += kThreads) g[e] = 0.0;
         }
-        if (tid == 0) {
-            int bad = nsrc > TB_FIT_MAX_SRC || P != nsrc * TB_FIT_NPAR || u.psf_K < 1 ||
-                      u.psf_K > TB_FIT_MAX_PSF || u.band >= n_bands || u.slice < 0 ||
-                      u.slice >= b.n_slices || u.t0 < 0 || u.t1 < u.t0 || u.t1 > b.n_active;
-            for (int s2 = 0; s2 < nsrc && !bad; s2++) bad = !tab[b.src0 + s2].ok;
-            sm.skip = bad;
-            if (bad) tb::report(st, TB_STATUS_BAD_ITEM, ui, nsrc);
+        // checks, and the unit's sources into shared memory (lane = source)
+        if (warp == 0) {
+            const bool unit_bad = nsrc < 0 || nsrc > TB_FIT_MAX_SRC || P != nsrc * TB_FIT_NPAR ||
+                                  u.psf_K < 1 || u.psf_K > TB_FIT_MAX_PSF || u.band < 0 ||
+                                  u.band >= n_bands || u.slice < 0 || u.slice >= b.n_slices ||
+                                  u.t0 < 0 || u.t1 < u.t0 || u.t1 > b.n_active;
+            bool src_bad = false;
+            if (!unit_bad && lane < nsrc) {
+                const SrcTab& S = tab[b.src0 + lane];
+                const int K = S.K[u.band];
+                src_bad = !S.ok || K < 0 || K > kCompStride;
+                const tb_fit_source fs = srcs[b.src0 + lane];
+                const bool live = fs.w > 0 && fs.h > 0;
+                UnitSrc U;
+                U.x0 = live ? fs.x0 : 0;
+                U.y0 = live ? fs.y0 : 0;
+                U.x1 = live ? fs.x0 + fs.w : 0;
+                U.y1 = live ? fs.y0 + fs.h : 0;
+                U.counts = (float)S.flux[u.band];
+                U.K = K;
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    U.M[q] = S.M[q];
+#pragma unroll
+                    for (int j = 0; j < 3; j++) U.dM[j][q] = S.dM[j][q];
+                }
+                sm.us[lane] = U;
+            }
+            const bool bad = unit_bad || __any_sync(0xffffffffu, src_bad);
+            if (lane == 0) {
+                sm.skip = bad;
+                if (bad) tb::report(st, TB_STATUS_BAD_ITEM, ui, nsrc);
+            }
         }
         __syncthreads();
         if (sm.skip) {
@@ -640,6 +620,8 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
             }
             continue;
         }
+        // the unit's band of source s: band_comps + s * n_bands * kCompStride
+        const FitC* band_comps = gcomps + ((int64_t)b.src0 * n_bands + u.band) * kCompStride;
         double chi2 = 0.0;
         // mode 0: the unit's range of the tiles some source's mask reaches;
         // mode 1: the others (their chi^2 does not depend on the parameters),
@@ -670,7 +652,7 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
             const float d = d_next, w = w_next;
             load_px(t + 1, d_next, w_next);   // prefetch the next tile's pixel
             if (single != run_src) {
-                if (run_src >= 0) flush_run(sm, hacc, gacc, run_src, H, g, P, u.band, n_bands);
+                if (run_src >= 0) flush_run(sm, hacc, gacc, run_src, H, g, P, u.band);
                 run_src = single;
 #pragma unroll
                 for (int v = 0; v < 28; v++) hacc[v] = 0.f;
@@ -678,10 +660,11 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
                 for (int v = 0; v < 7; v++) gacc[v] = 0.f;
             }
             if (single >= 0 && single < nsrc) {
-                float J[7];
-                const float model = eval_single(sm, gcomps, srcs[b.src0 + single],
-                                                tab[b.src0 + single], b.src0 + single, u.band,
-                                                n_bands, ox, oy, w, J);
+                // one source: every warp on its own row, no block barrier
+                float J[kCols];
+                const float model = eval_source<true>(
+                    sm.wc[warp], band_comps + (int64_t)single * n_bands * kCompStride,
+                    sm.us[single], ox, oy, w, J);
                 const float rr = (d - model) * w;
                 chi2 += (double)(rr * rr);
                 int v = 0;
@@ -693,77 +676,56 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
                 }
                 continue;
             }
-            // sources whose rectangle meets this tile (source order)
-            if (warp == 0) {
-                bool hit = false;
-                tb_fit_source fs;
-                if (lane < nsrc) {
-                    fs = srcs[b.src0 + lane];
-                    hit = fs.x0 < ox + kTileW && fs.x0 + fs.w > ox && fs.y0 < oy + kTileH &&
-                          fs.y0 + fs.h > oy && fs.w > 0 && fs.h > 0;
-                }
-                const unsigned bal = __ballot_sync(0xffffffffu, hit);
-                if (hit) {
-                    const int q = __popc(bal & ((1u << lane) - 1u));
-                    TileRec R;
-                    R.x0 = max(fs.x0 - ox, 0);
-                    R.x1 = min(fs.x0 + fs.w - ox, kTileW);
-                    R.y0 = max(fs.y0 - oy, 0);
-                    R.y1 = min(fs.y0 + fs.h - oy, kTileH);
-                    const SrcTab& S = tab[b.src0 + lane];
-                    R.counts = (float)S.flux[u.band];
-                    R.src = lane;
-                    R.K = S.K[u.band];
-                    R.pad = 0;
-#pragma unroll
-                    for (int q = 0; q < 3; q++) {
-                        R.M[q] = S.M[q];
-#pragma unroll
-                        for (int j = 0; j < 3; j++) R.dM[j][q] = S.dM[j][q];
-                    }
-                    sm.recs[q] = R;
-                }
-                if (lane == 0) sm.nrec = __popc(bal);
+            // sources whose mask meets this tile, in source order (every warp
+            // finds the same set); mode 1 tiles meet none by construction
+            bool meets = false;
+            if (mode == 0 && lane < nsrc) {
+                const UnitSrc& U = sm.us[lane];
+                meets = U.x0 < ox + kTileW && U.x1 > ox && U.y0 < oy + kTileH && U.y1 > oy;
             }
-            __syncthreads();
-            const int R = sm.nrec;
+            const unsigned hit = __ballot_sync(0xffffffffu, meets);
+            const int R = __popc(hit);
             if (R == 0) {
                 const float rr = d * w;
                 chi2 += (double)(rr * rr);
-                __syncthreads();
                 continue;
             }
+            // Shared A, r, hstage and gstage are written only after the
+            // previous multi-source tile's reads of them have passed a
+            // barrier: A and r are read before its second barrier, hstage
+            // and gstage after it and are written here only after this
+            // tile's first barrier.
             const int ngroups = (R + kG - 1) / kG;
-            float model;
+            float model = 0.f;
             if (ngroups == 1) {
-                model = eval_group<true>(sm, gcomps, b.src0, u.band, n_bands, 0, R, ox, oy, w,
-                                         sm.A[0], false);
+                model = eval_group<true>(sm, band_comps, n_bands, hit, 0, R, ox, oy, w, sm.A[0]);
             } else {
-                model = 0.f;
                 for (int q0 = 0; q0 < R; q0 += kG)
-                    model += eval_group<false>(sm, gcomps, b.src0, u.band, n_bands, q0,
-                                               min(kG, R - q0), ox, oy, w, sm.A[0], q0 > 0);
+                    model += eval_group<false>(sm, band_comps, n_bands, hit, q0, min(kG, R - q0),
+                                               ox, oy, w, sm.A[0]);
             }
             const float rr = (d - model) * w;
             chi2 += (double)(rr * rr);
             sm.r[tid] = rr;
-            __syncthreads();
             for (int ga = 0; ga < ngroups; ga++) {
                 const int qa = ga * kG, na = min(kG, R - qa);
                 if (ngroups > 1)
-                    eval_group<true>(sm, gcomps, b.src0, u.band, n_bands, qa, na, ox, oy, w,
-                                     sm.A[0], true);
-                add_grad(sm, sm.A[0], qa, na, g, u.band, n_bands);
-                add_block(sm, sm.A[0], qa, na, sm.A[0], qa, na, true, H, P, u.band, n_bands);
+                    eval_group<true>(sm, band_comps, n_bands, hit, qa, na, ox, oy, w, sm.A[0]);
+                __syncthreads();   // columns (and r) complete; earlier updates applied
+                stage_products(sm, sm.A[0], na, sm.A[0], na, true, true);
+                __syncthreads();
+                apply_products(sm, hit, qa, na, qa, na, true, true, H, g, P, u.band);
                 for (int gb = ga + 1; gb < ngroups; gb++) {
                     const int qb = gb * kG, nb = min(kG, R - qb);
-                    eval_group<true>(sm, gcomps, b.src0, u.band, n_bands, qb, nb, ox, oy, w,
-                                     sm.A[1], true);
-                    add_block(sm, sm.A[0], qa, na, sm.A[1], qb, nb, false, H, P, u.band, n_bands);
+                    eval_group<true>(sm, band_comps, n_bands, hit, qb, nb, ox, oy, w, sm.A[1]);
+                    __syncthreads();
+                    stage_products(sm, sm.A[0], na, sm.A[1], nb, false, false);
+                    __syncthreads();
+                    apply_products(sm, hit, qa, na, qb, nb, false, false, H, g, P, u.band);
                 }
             }
         }
-        if (run_src >= 0) flush_run(sm, hacc, gacc, run_src, H, g, P, u.band, n_bands);
+        if (run_src >= 0) flush_run(sm, hacc, gacc, run_src, H, g, P, u.band);
         // chi^2 of the unit: fixed-order block reduction
         for (int o = 16; o > 0; o >>= 1) chi2 += __shfl_xor_sync(0xffffffffu, chi2, o);
         if (lane == 0) sm.red[warp] = chi2;
@@ -774,7 +736,6 @@ fit_pass_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict
             if (mode == 0) chi2_part[b.unit0 + u.slice] = s + chi2_const[b.unit0 + u.slice];
             else chi2_const[b.unit0 + u.slice] = s;
         }
-        __syncthreads();
     }
 }
 
