@@ -755,20 +755,26 @@ __device__ double max_step(int off) {
     }
 }
 
-__global__ void __launch_bounds__(kStepThreads)
+// One CTA per blob.  The factor lives in the blob's global area (L2
+// resident); shared memory and registers stay small so that five blobs
+// share an SM.
+__global__ void __launch_bounds__(kStepThreads, 5)
 fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
                 const tb_fit_source* __restrict__ srcs, double* __restrict__ params,
                 double* __restrict__ trial, double* __restrict__ hbuf, double* __restrict__ gbuf,
                 const double* __restrict__ chi2_part, tb_fit_state* __restrict__ state,
                 double tol, int max_iter) {
     __shared__ double dsc[TB_FIT_MAX_SRC * TB_FIT_NPAR];
+    __shared__ double dinv[TB_FIT_MAX_SRC * TB_FIT_NPAR];
     __shared__ double y[TB_FIT_MAX_SRC * TB_FIT_NPAR];
     __shared__ double xs[TB_FIT_MAX_SRC * TB_FIT_NPAR];
+    __shared__ double rdg[TB_FIT_MAX_SRC * TB_FIT_NPAR];
     __shared__ double red[kStepThreads / 32];
-    __shared__ int s_accept, s_active, s_bad;
+    __shared__ int s_accept, s_active;
     __shared__ double s_lambda, s_scale;
     const int bi = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    (void)n_bands;
     if (bi >= n_blobs) return;
     const tb_fit_blob b = blobs[bi];
     tb_fit_state& S = state[bi];
@@ -779,7 +785,7 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     const int ns = b.n_slices;
     double* Hp = hbuf + b.h_off;                        // slice partials
     double* Ha = Hp + (int64_t)ns * P * P;              // accepted H
-    double* L = Ha + (int64_t)P * P;                    // Cholesky factor
+    double* L = Ha + (int64_t)P * P;                    // factor
     double* gp = gbuf + b.g_off;
     double* ga = gp + (int64_t)ns * P;
     double* pa = params + (int64_t)b.src0 * TB_FIT_NPAR;
@@ -807,19 +813,18 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
         s_lambda = S.lambda;
         s_active = status == 0;
         S.status = status;
-        s_bad = 0;
     }
     __syncthreads();
     if (s_accept) {
         for (int e = tid; e < P; e += kStepThreads) pa[e] = pt[e];
-        // accepted H (symmetric, from the band partials' upper triangles) and g
-        for (int e = tid; e < P * P; e += kStepThreads) {
-            const int i = e / P, j = e % P;
-            const int r = min(i, j), c = max(i, j);
-            double s = 0.0;
-            for (int k = 0; k < ns; k++) s += Hp[(int64_t)k * P * P + (int64_t)r * P + c];
-            Ha[e] = s;
-        }
+        // accepted H (symmetric, from the slice partials' upper triangles) and g
+        for (int r = warp; r < P; r += kStepThreads / 32)
+            for (int c = r + lane; c < P; c += 32) {
+                double s = 0.0;
+                for (int k = 0; k < ns; k++) s += Hp[(int64_t)k * P * P + (int64_t)r * P + c];
+                Ha[(int64_t)r * P + c] = s;
+                Ha[(int64_t)c * P + r] = s;
+            }
         for (int e = tid; e < P; e += kStepThreads) {
             double s = 0.0;
             for (int k = 0; k < ns; k++) s += gp[(int64_t)k * P + e];
@@ -847,37 +852,36 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
         // frozen parameters are left out of the step
         if ((srcs[b.src0 + i / TB_FIT_NPAR].frozen >> (i % TB_FIT_NPAR)) & 1) d = 0.0;
         dsc[i] = d;
+        dinv[i] = d == 0.0 ? 0.0 : 1.0 / d;
     }
     __syncthreads();
+    // element (i, j) of the scaled matrix (H symmetric: read along i)
     auto scaled = [&](int i, int j) -> double {
-        if (dsc[i] == 0.0 || dsc[j] == 0.0) return i == j ? 1.0 : 0.0;
-        return Ha[(int64_t)i * P + j] / (dsc[i] * dsc[j]) + (i == j ? lam : 0.0);
+        if (dinv[i] == 0.0 || dinv[j] == 0.0) return i == j ? 1.0 : 0.0;
+        return Ha[(int64_t)j * P + i] * dinv[i] * dinv[j] + (i == j ? lam : 0.0);
     };
-    for (int e = tid; e < P * P; e += kStepThreads) {
-        const int i = e / P, j = e % P;
-        if (j <= i) L[e] = scaled(i, j);
-    }
+    // LDL^T of the scaled matrix, lower triangle column-major (element
+    // (i, j), i >= j, at L[j P + i]), right-looking: step k subtracts
+    // L[k P + i] L[k P + j] / d_k from the trailing columns and leaves column
+    // k as d_k (diagonal) and d_k l_ik below it, so no column is rescaled
+    // and each step takes one barrier.
+    for (int j = warp; j < P; j += kStepThreads / 32)
+        for (int i = j + lane; i < P; i += 32) L[(int64_t)j * P + i] = scaled(i, j);
     __syncthreads();
+    bool bad = false;
     for (int k = 0; k < P; k++) {
-        if (tid == 0) {
-            const double a = L[(int64_t)k * P + k];
-            if (!(a > 0.0) || !isfinite(a)) s_bad = k + 1;
-            else L[(int64_t)k * P + k] = sqrt(a);
-        }
-        __syncthreads();
-        if (s_bad) break;
-        const double lkk = L[(int64_t)k * P + k];
-        for (int i = k + 1 + tid; i < P; i += kStepThreads) L[(int64_t)i * P + k] /= lkk;
-        __syncthreads();
-        const int m = P - k - 1;
-        for (int e = tid; e < m * m; e += kStepThreads) {
-            const int ii = k + 1 + e / m, jj = k + 1 + e % m;
-            if (jj > ii) continue;
-            L[(int64_t)ii * P + jj] -= L[(int64_t)ii * P + k] * L[(int64_t)jj * P + k];
+        const double* ck = L + (int64_t)k * P;
+        const double dk = ck[k];   // final since step k - 1; the same in every thread
+        if (!(dk > 0.0) || !isfinite(dk)) { bad = true; break; }
+        const double rk = 1.0 / dk;
+        for (int j = k + 1 + warp; j < P; j += kStepThreads / 32) {
+            const double cj = ck[j] * rk;
+            double* colj = L + (int64_t)j * P;
+            for (int i = j + lane; i < P; i += 32) colj[i] = fma(-ck[i], cj, colj[i]);
         }
         __syncthreads();
     }
-    if (s_bad) {
+    if (bad) {
         // not positive definite: treat as a rejected step with more damping
         if (tid == 0) {
             S.lambda *= 10.0;
@@ -887,34 +891,65 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
         return;
     }
     for (int i = tid; i < P; i += kStepThreads) {
+        rdg[i] = 1.0 / L[(int64_t)i * P + i];
         xs[i] = 0.0;
-        y[i] = dsc[i] == 0.0 ? 0.0 : ga[i] / dsc[i];
+        y[i] = ga[i] * dinv[i];
     }
     __syncthreads();
-    // solution and one refinement step; triangular solves by warp 0
+    // solution and one refinement step
     for (int pass = 0; pass < 2; pass++) {
         if (pass == 1) {
             for (int i = tid; i < P; i += kStepThreads) {
-                double acc = dsc[i] == 0.0 ? 0.0 : ga[i] / dsc[i];
+                double acc = ga[i] * dinv[i];
                 for (int j = 0; j < P; j++) acc -= scaled(i, j) * xs[j];
                 y[i] = acc;
             }
             __syncthreads();
         }
         if (warp == 0) {
-            for (int i = 0; i < P; i++) {
-                double part = 0.0;
-                for (int j = lane; j < i; j += 32) part += L[(int64_t)i * P + j] * y[j];
-                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-                if (lane == 0) y[i] = (y[i] - part) / L[(int64_t)i * P + i];
-                __syncwarp();
+            // L z = y, w = D^-1 z, L^T x = w by columns, lane l holding rows
+            // l + 32 m in registers: l_ik = L[k P + i] / d_k
+            constexpr int kSlots = (TB_FIT_MAX_SRC * TB_FIT_NPAR + 31) / 32;
+            double v[kSlots];
+#pragma unroll
+            for (int m = 0; m < kSlots; m++) {
+                const int i = lane + 32 * m;
+                v[m] = i < P ? y[i] : 0.0;
             }
-            for (int i = P - 1; i >= 0; i--) {
-                double part = 0.0;
-                for (int j = i + 1 + lane; j < P; j += 32) part += L[(int64_t)j * P + i] * y[j];
-                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-                if (lane == 0) y[i] = (y[i] - part) / L[(int64_t)i * P + i];
-                __syncwarp();
+            for (int k = 0; k < P; k++) {
+                double zk = 0.0;
+#pragma unroll
+                for (int m = 0; m < kSlots; m++)
+                    if (m == (k >> 5)) zk = v[m];
+                zk = __shfl_sync(0xffffffffu, zk, k & 31) * rdg[k];
+                const double* ck = L + (int64_t)k * P;
+#pragma unroll
+                for (int m = 0; m < kSlots; m++) {
+                    const int i = lane + 32 * m;
+                    if (i > k && i < P) v[m] = fma(-ck[i], zk, v[m]);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < kSlots; m++) {
+                const int i = lane + 32 * m;
+                if (i < P) v[m] *= rdg[i];
+            }
+            for (int k = P - 1; k > 0; k--) {
+                double xk = 0.0;
+#pragma unroll
+                for (int m = 0; m < kSlots; m++)
+                    if (m == (k >> 5)) xk = v[m];
+                xk = __shfl_sync(0xffffffffu, xk, k & 31);
+#pragma unroll
+                for (int m = 0; m < kSlots; m++) {
+                    const int j = lane + 32 * m;
+                    if (j < k) v[m] = fma(-L[(int64_t)j * P + k] * rdg[j], xk, v[m]);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < kSlots; m++) {
+                const int i = lane + 32 * m;
+                if (i < P) y[i] = v[m];
             }
         }
         __syncthreads();
