@@ -578,6 +578,25 @@ int tb_chi2(const float* data, const float* model, const float* inverr,
             const int64_t* off, const int64_t* npix, int32_t n, double* out,
             void* stream);
 
+/* EM fit of K-component 2-D Gaussian mixtures to n images, the batched
+ * em_fit_2d_reg (tractor/emfit.i:274-557) that GaussianMixturePSF.fromStamp
+ * (tractor/psf.py:536-597) runs on a PSF stamp.  Image s is ny x nx FP64
+ * values, row-major, at img + s*ny*nx; pixel (ix, iy) sits at
+ * (x0 + ix, y0 + iy) with (x0, y0) = xy0[2s], xy0[2s + 1], or
+ * (-(nx/2), -(ny/2)) when xy0 is NULL.  amp (n x K), mean (n x K x 2) and
+ * var (n x K x 2 x 2, row-major) hold the initial mixtures and receive the
+ * fitted ones after `steps` iterations; alpha is the reference's
+ * inverse-Wishart prior strength (alpha I added to the scatter matrix,
+ * alpha to its weight).  status[s] (optional) is 0, or 1 when a component's
+ * covariance determinant became non-positive: that image's fit stops there
+ * with the previous iteration's mixture, as the reference returns -1.
+ * FP64 throughout; every pointer is device memory.  1 <= K <= TB_EM_MAX_K,
+ * ny * nx <= 2^24. */
+#define TB_EM_MAX_K 8
+int tb_em_fit_2d(const double* img, int32_t n, int32_t ny, int32_t nx, const int32_t* xy0,
+                 double* amp, double* mean, double* var, int32_t K, double alpha,
+                 int32_t steps, int32_t* status, void* stream);
+
 /* Library version string (host memory, static). */
 const char* tb_version(void);
 

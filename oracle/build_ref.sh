@@ -2,13 +2,14 @@
 # Test infrastructure: builds the reference Tractor's own C kernels into
 # oracle/_ref/ so that the oracle can be checked against them.
 #
-# The reference compiles these with SWIG (tractor/mix.i, tractor/mp_fourier.i);
+# The reference compiles these with SWIG (tractor/mix.i, tractor/mp_fourier.i,
+# tractor/emfit.i);
 # SWIG is not installed here, so this recipe copies the C text of the
 # `%{ ... %}` and `%inline %{ ... %}` blocks out of the .i files (by block
 # markers, verbatim) into oracle/_ref/, and compiles it together with a small
-# shim (oracle/ref_shim_mix.c, oracle/ref_shim_mpf.c) that only adds exported
-# entry points.  approx3.c and gauss_masked.c are #included from where they
-# lie in the reference tree.  Nothing here is used by the product path.
+# shim (oracle/ref_shim_mix.c, oracle/ref_shim_mpf.c, oracle/ref_shim_emfit.c)
+# that only adds exported entry points.  approx3.c, gauss_masked.c and
+# emfit2.c are #included from where they lie in the reference tree.  Nothing here is used by the product path.
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail
@@ -32,6 +33,7 @@ extract() {
 }
 extract "$REF/tractor/mix.i"        > "$OUT/ref_mix_blocks.c"
 extract "$REF/tractor/mp_fourier.i" > "$OUT/ref_mpf_blocks.c"
+extract "$REF/tractor/emfit.i"      > "$OUT/ref_emfit_blocks.c"
 
 PYINC="$(python3 -c 'import sysconfig; print(sysconfig.get_paths()["include"])')"
 NPINC="$(python3 -c 'import numpy; print(numpy.get_include())')"
@@ -41,4 +43,6 @@ gcc $CFLAGS -I"$OUT" -I"$REF/tractor" -I"$PYINC" -I"$NPINC" \
     "$HERE/ref_shim_mix.c" -o "$OUT/libref_mix.so" -lm
 gcc $CFLAGS -I"$OUT" -I"$REF/tractor" -I"$PYINC" -I"$NPINC" \
     "$HERE/ref_shim_mpf.c" -o "$OUT/libref_mpf.so" -lm
-echo "built $OUT/libref_mix.so $OUT/libref_mpf.so"
+gcc $CFLAGS -I"$OUT" -I"$REF/tractor" -I"$PYINC" -I"$NPINC" \
+    "$HERE/ref_shim_emfit.c" -o "$OUT/libref_emfit.so" -lm
+echo "built $OUT/libref_mix.so $OUT/libref_mpf.so $OUT/libref_emfit.so"

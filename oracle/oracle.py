@@ -806,3 +806,61 @@ def sersic_fft_model_f64(theta, psf_img, mask_x0, mask_y0, mw, mh, shape='E'):
     T = nullwcs_cdinv() @ ellipseE_basis(*e)
     a2, v2 = sheared(amp, var, T)
     return c * galaxy_fft_masked_f64(a2, v2, x, y, psf_img, mask_x0, mask_y0, mw, mh)
+
+
+# ---------------------------------------------------------------------------
+# EM fit of a Gaussian mixture to an image (tractor/emfit.i)
+# ---------------------------------------------------------------------------
+
+def em_fit_2d_reg(img, x0, y0, amp, mean, var, alpha, steps):
+    """em_fit_2d_reg (tractor/emfit.i:274-557), vectorised over pixels: each
+    step computes C^-1 and amp / sqrt((2 pi)^2 det) (a non-positive
+    determinant returns -1, emfit.i:403-409), the responsibilities
+    z_k / sum_j z_j with z = 0 where dsq >= 100 (a pixel whose sum is 0
+    keeps its unnormalised z, emfit.i:424-454), then the mean, the
+    covariance about the new mean with the alpha prior and the amplitude
+    (emfit.i:460-509).  amp / mean / var (float64) are updated in place;
+    returns 0 or -1."""
+    img = np.asarray(img, np.float64)
+    NY, NX = img.shape
+    K = len(amp)
+    iy, ix = np.mgrid[:NY, :NX]
+    x = (x0 + ix).ravel().astype(np.float64)
+    y = (y0 + iy).ravel().astype(np.float64)
+    I = img.ravel()
+    tpd = (2. * np.pi) ** 2
+    for step in range(steps):
+        V = var.reshape(K, 4)
+        det = V[:, 0] * V[:, 3] - V[:, 1] * V[:, 2]
+        if np.any(det <= 0.):
+            return -1
+        iv = np.stack([V[:, 3] / det, -V[:, 1] / det, -V[:, 2] / det, V[:, 0] / det], 1)
+        scale = amp / np.sqrt(tpd * det)
+        dx = x[None, :] - mean[:, 0:1]
+        dy = y[None, :] - mean[:, 1:2]
+        dsq = (iv[:, 0:1] * dx * dx + iv[:, 1:2] * dx * dy + iv[:, 2:3] * dx * dy +
+               iv[:, 3:4] * dy * dy)
+        Z = np.where(dsq >= 100, 0., scale[:, None] * np.exp(-0.5 * np.minimum(dsq, 100.)))
+        zsum = np.zeros_like(I)
+        for k in range(K):
+            zsum = zsum + Z[k]
+        nz = zsum != 0
+        Z[:, nz] = Z[:, nz] / zsum[nz]
+        W = I[None, :] * Z
+        wsum = W.sum(axis=1)
+        mx = (W * x[None, :]).sum(axis=1) / wsum
+        my = (W * y[None, :]).sum(axis=1) / wsum
+        mean[:, 0] = mx
+        mean[:, 1] = my
+        ddx = x[None, :] - mx[:, None]
+        ddy = y[None, :] - my[:, None]
+        vxx = alpha + (W * ddx * ddx).sum(axis=1)
+        vxy = (W * ddx * ddy).sum(axis=1)
+        vyy = alpha + (W * ddy * ddy).sum(axis=1)
+        den = wsum + alpha
+        var[:, 0, 0] = vxx / den
+        var[:, 0, 1] = vxy / den
+        var[:, 1, 0] = vxy / den
+        var[:, 1, 1] = vyy / den
+        amp[:] = wsum
+    return 0

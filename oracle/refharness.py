@@ -7,7 +7,7 @@ tests that need it skip elsewhere.  It is used to generate the golden fixtures
 under tests/golden/ and to pin the oracle restatement against the reference.
 
 What is shimmed, and why:
-  * tractor.mix / tractor.mp_fourier -- the SWIG modules.  Each shim function
+  * tractor.mix / tractor.mp_fourier / tractor.emfit -- the SWIG modules.  Each shim function
     calls the reference's C entry point with the same arguments SWIG would
     pass (tractor/mix.i:311 makes c_gauss_2d_approx3 return
     (rtn, sx0, sx1, sy0, sy1)).
@@ -143,6 +143,26 @@ def _mpf_module():
     return m
 
 
+def _emfit_module():
+    lib = ctypes.PyDLL(os.path.join(_REFLIB, 'libref_emfit.so'))
+    if lib.ref_emfit_init() != 0:
+        raise RuntimeError('numpy C-API init failed in libref_emfit.so')
+    P = ctypes.py_object
+    I = ctypes.c_int
+    D = ctypes.c_double
+    lib.ref_em_fit_2d_reg.argtypes = [P, I, I, P, P, P, D, I]
+    lib.ref_em_fit_2d_reg.restype = I
+    m = types.ModuleType('tractor.emfit')
+
+    def em_fit_2d_reg(img, x0, y0, amp, mean, var, alpha, steps):
+        return lib.ref_em_fit_2d_reg(img, int(x0), int(y0), amp, mean, var, float(alpha),
+                                     int(steps))
+
+    m.em_fit_2d_reg = em_fit_2d_reg
+    m._lib = lib
+    return m
+
+
 def _get_overlapping_region(xlo, xhi, xmin, xmax):
     # Same contract as tractor/patch.pyx:20-65.
     if xlo > xmax or xhi < xmin or xlo > xhi or xmin > xmax:
@@ -184,6 +204,8 @@ def _install_shims():
     mods['tractor.mix'] = tmix
     mods['tractor.mp_fourier'] = tmpf
     mods['tractor.version'] = ver
+    if os.path.isfile(os.path.join(_REFLIB, 'libref_emfit.so')):
+        mods['tractor.emfit'] = _emfit_module()
 
     astro = types.ModuleType('astrometry')
     astro.__path__ = []
@@ -203,7 +225,7 @@ def _install_shims():
                  'astrometry.sdss', 'astrometry.libkd',
                  'astrometry.libkd.spherematch', 'astrometry.util.plotutils',
                  'astrometry.util.multiproc']:
-        if name not in sys.modules:
+        if name not in sys.modules and name not in mods:
             mods[name] = _Stub(name)
     try:
         import matplotlib  # noqa: F401

@@ -188,6 +188,18 @@ def install(monkeypatch):
         return torch.from_numpy(np.concatenate(X)), torch.tensor(info, dtype=torch.int32), \
             np.array(xo)
 
+    def em_run(imgs, amp, mean, var, alpha, steps, xy):
+        n, ny, nx = imgs.shape
+        amp, mean, var = amp.copy(), mean.copy(), var.copy()
+        st = np.zeros(n, np.int32)
+        for i in range(n):
+            x0, y0 = (int(xy[i, 0]), int(xy[i, 1])) if xy is not None else (-(nx // 2),
+                                                                           -(ny // 2))
+            st[i] = O.em_fit_2d_reg(imgs[i], x0, y0, amp[i], mean[i], var[i], alpha, steps) != 0
+        return amp, mean, var, st
+
+    from tractor_b200 import emfit
+    monkeypatch.setattr(emfit, '_run', em_run)
     monkeypatch.setattr(render.MogBatch, 'run', mog_run)
     monkeypatch.setattr(render.FftBatch, 'run', fft_run)
     monkeypatch.setattr(render.PsfSpectra, 'get', spectra_get)

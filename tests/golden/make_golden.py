@@ -10,6 +10,8 @@ root in the development container:
     python tests/golden/make_golden.py          # every fixture but hybrid_psf
     python tests/golden/make_golden.py hybrid   # hybrid_psf.npz
     python tests/golden/make_golden.py psfex    # psfex.npz
+    python tests/golden/make_golden.py emfit    # emfit.npz
+    python tests/golden/make_golden.py psfderiv # psf_derivs.npz
 """
 import os
 import sys
@@ -399,10 +401,133 @@ def psfex():
     print('psfex fixture written to', OUT)
 
 
+def emfit():
+    """GaussianMixturePSF.fromStamp (psf.py:536-597) -- the EM fit of
+    em_fit_2d_reg (emfit.i:274-557) after fromStamp's normalisation -- on
+    seeded stamps: Moffat and Gaussian-sum profiles with noise, square and
+    not, 1 to 4 components, with and without the alpha prior, default and
+    explicit origins, and an initial guess P0."""
+    from oracle import refharness
+    refharness.load()
+    from tractor.psf import GaussianMixturePSF
+    rng = np.random.default_rng(777)
+
+    def gsum(h, w, parts, noise):
+        y, x = np.mgrid[:h, :w]
+        x = x - w // 2
+        y = y - h // 2
+        img = np.zeros((h, w))
+        for a, mx, my, sx, sy, rho in parts:
+            dx, dy = x - mx, y - my
+            q = (dx / sx) ** 2 - 2 * rho * dx * dy / (sx * sy) + (dy / sy) ** 2
+            img += a * np.exp(-0.5 * q / (1 - rho ** 2))
+        img /= img.sum()
+        return img + rng.normal(0., noise, img.shape)
+
+    cases = [
+        # stamp, N, alpha, steps, xy0, P0
+        (moffat(25, 4.0, 3.0), 3, 0., 1000, None, None),
+        (moffat(33, 5.0, 2.5), 2, 0., 500, None, None),
+        (moffat(21, 3.0, 4.0), 1, 0.5, 300, None, None),
+        (gsum(25, 25, [(0.6, 0., 0., 1.5, 1.5, 0.), (0.3, 0.5, 0., 3., 2.5, 0.2),
+                       (0.1, 0., -0.3, 6., 6., 0.)], 1e-4).astype(np.float32),
+         3, 0., 1000, None, None),
+        (gsum(21, 31, [(0.7, 0.2, 0.1, 1.2, 2.0, -0.3), (0.3, 0., 0., 3.5, 3.0, 0.1)], 3e-4),
+         2, 0.1, 800, (-15, -10), None),
+        (gsum(29, 29, [(0.5, 0., 0., 1.0, 1.0, 0.), (0.3, 0., 0., 2.0, 2.0, 0.),
+                       (0.15, 0., 0., 4.0, 4.0, 0.), (0.05, 0., 0., 8.0, 8.0, 0.)], 2e-5),
+         4, 0., 1000, None, None),
+        (moffat(25, 4.0, 3.0), 3, 0., 400, None,
+         (np.array([0.5, 0.3, 0.2]), np.zeros((3, 2)),
+          np.array([np.eye(2) * 1.5, np.eye(2) * 4., np.eye(2) * 12.]))),
+    ]
+    arrays = {}
+    for i, (stamp, N, alpha, steps, xy0, P0) in enumerate(cases):
+        P0c = None if P0 is None else tuple(np.array(a, copy=True) for a in P0)
+        psf = GaussianMixturePSF.fromStamp(stamp, N=N, P0=P0c, xy0=xy0, alpha=alpha,
+                                           emsteps=steps)
+        arrays['stamp%d' % i] = stamp
+        arrays['cfg%d' % i] = np.array([N, alpha, steps, xy0 is not None,
+                                        0 if xy0 is None else xy0[0],
+                                        0 if xy0 is None else xy0[1], P0 is not None])
+        if P0 is not None:
+            arrays['p0amp%d' % i], arrays['p0mean%d' % i], arrays['p0var%d' % i] = P0
+        arrays['amp%d' % i] = psf.mog.amp
+        arrays['mean%d' % i] = psf.mog.mean
+        arrays['var%d' % i] = psf.mog.var
+    np.savez_compressed(os.path.join(OUT, 'emfit.npz'), n=len(cases), **arrays)
+    print('emfit fixture written to', OUT)
+
+
+def psf_scene(tractor_mod, ellipse):
+    """A 40 x 36 image with two point sources and an exp galaxy under a
+    2-component MoG PSF (GaussianMixturePSF, or GaussianMixtureEllipsePSF
+    when `ellipse`) and a constant sky, the PSF and sky thawed, the catalog
+    frozen."""
+    T = tractor_mod
+    from tractor.psf import GaussianMixtureEllipsePSF
+    from tractor.sky import ConstantSky
+    from tractor.galaxy import ExpGalaxy
+    if ellipse:
+        psf = GaussianMixtureEllipsePSF(np.array([0.7, 0.3]), np.array([[0.1, -0.05], [0., 0.2]]),
+                                        [T.EllipseESoft(0.4, 0.05, -0.1),
+                                         T.EllipseESoft(1.1, -0.02, 0.03)])
+    else:
+        psf = T.GaussianMixturePSF(np.array([0.7, 0.3]), np.array([[0.1, -0.05], [0., 0.2]]),
+                                   np.array([[[1.6, 0.2], [0.2, 1.9]], [[7.5, -0.4], [-0.4, 8.2]]]))
+    tim = T.Image(data=np.zeros((36, 40), np.float32), inverr=np.ones((36, 40), np.float32),
+                  psf=psf, sky=ConstantSky(2.5), photocal=T.LinearPhotoCal(1.))
+    srcs = [T.PointSource(T.PixPos(12.3, 10.6), T.Flux(800.)),
+            T.PointSource(T.PixPos(27.8, 25.1), T.Flux(450.)),
+            ExpGalaxy(T.PixPos(20.4, 17.2), T.Flux(1200.), T.EllipseE(2.5, 0.2, -0.1))]
+    tr = T.Tractor([tim], srcs)
+    tr.freezeParam('catalog')
+    tim.freezeAllBut('psf', 'sky')
+    return tr, tim
+
+
+def psfderiv():
+    """Image-parameter derivatives (engine.py:306-324: forward differences of
+    the model image for the PSF, the sky's own derivative) for both MoG PSF
+    parameterisations, and the optimiser-based PSF fits
+    GaussianMixtureEllipsePSF.fromStamp (psf.py:757-789) and
+    GaussianMixturePSF.fromStamp(v3=True) (psf.py:563-575)."""
+    from oracle import refharness
+    T = refharness.load()
+    import tractor
+    from tractor.psf import GaussianMixturePSF, GaussianMixtureEllipsePSF
+    arrays = {}
+    for tag, ellipse in (('mog', False), ('ell', True)):
+        tr, tim = psf_scene(tractor, ellipse)
+        derivs = tr.getDerivs()
+        arrays[tag + '_names'] = np.array(tr.getParamNames())
+        arrays[tag + '_params'] = np.array(tr.getParams())
+        cols = []
+        for d in derivs:
+            (patch, img), = d
+            full = np.zeros(img.shape, np.float64)
+            patch.addTo(full)
+            cols.append(full)
+        arrays[tag + '_derivs'] = np.array(cols)
+        arrays[tag + '_model'] = tr.getModelImage(0)
+    stamp = moffat(25, 4.0, 3.0)
+    p1 = GaussianMixtureEllipsePSF.fromStamp(stamp, N=2)
+    arrays['ell_fit'] = np.array(p1.getAllParams())
+    p2 = GaussianMixturePSF.fromStamp(stamp, N=2, v3=True)
+    arrays['v3_fit'] = np.array(p2.getAllParams())
+    arrays['stamp'] = stamp
+    np.savez_compressed(os.path.join(OUT, 'psf_derivs.npz'), **arrays)
+    print('psf_derivs fixture written to', OUT)
+
+
 if __name__ == '__main__':
     if sys.argv[1:] == ['hybrid']:
         hybrid()
     elif sys.argv[1:] == ['psfex']:
         psfex()
+    elif sys.argv[1:] == ['emfit']:
+        emfit()
+    elif sys.argv[1:] == ['psfderiv']:
+        psfderiv()
     else:
         main()

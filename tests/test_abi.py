@@ -33,3 +33,5 @@ def test_invalid_arguments_are_rejected_without_a_device():
     assert lib.tb_psf_spectrum(1, 1, 1, 48, 0, None) == -3
     assert lib.tb_normal_equations(None, None, None, None, None, None, None, None, None, None,
                                    None, 1, 400, None) == -3
+    assert lib.tb_em_fit_2d(None, 1, 9, 9, None, None, None, None, 3, 0., 10, None, None) == -1
+    assert lib.tb_em_fit_2d(None, 1, 9, 9, None, None, None, None, 9, 0., 10, None, None) == -1

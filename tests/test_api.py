@@ -262,3 +262,107 @@ def test_plain_fit_matches_reference(backend):
     X = tr.optimizer.getLinearUpdateDirection(tr)
     Xr = g['X']
     assert np.all(np.abs(X - Xr) <= 1e-3 * np.abs(Xr) + 1e-9), (X, Xr)
+
+
+def _psf_scene(T, ellipse):
+    """The scene of tests/golden/make_golden.py:psf_scene with this package:
+    two point sources and an exp galaxy under a 2-component MoG PSF, a
+    constant sky, the PSF and sky thawed, the catalog frozen."""
+    if ellipse:
+        psf = T.GaussianMixtureEllipsePSF(np.array([0.7, 0.3]), np.array([[0.1, -0.05], [0., 0.2]]),
+                                          [T.EllipseESoft(0.4, 0.05, -0.1),
+                                           T.EllipseESoft(1.1, -0.02, 0.03)])
+    else:
+        psf = T.GaussianMixturePSF(np.array([0.7, 0.3]), np.array([[0.1, -0.05], [0., 0.2]]),
+                                   np.array([[[1.6, 0.2], [0.2, 1.9]], [[7.5, -0.4], [-0.4, 8.2]]]))
+    tim = T.Image(data=np.zeros((36, 40), np.float32), inverr=np.ones((36, 40), np.float32),
+                  psf=psf, sky=T.ConstantSky(2.5), photocal=T.LinearPhotoCal(1.))
+    srcs = [T.PointSource(T.PixPos(12.3, 10.6), T.Flux(800.)),
+            T.PointSource(T.PixPos(27.8, 25.1), T.Flux(450.)),
+            T.ExpGalaxy(T.PixPos(20.4, 17.2), T.Flux(1200.), T.EllipseE(2.5, 0.2, -0.1))]
+    tr = T.Tractor([tim], srcs)
+    tr.freezeParam('catalog')
+    tim.freezeAllBut('psf', 'sky')
+    return tr, tim
+
+
+# Forward differences (steps 0.01 / 0.1 for GaussianMixturePSF, 0.001 for
+# GaussianMixtureEllipsePSF) of two float32 model images: each image within
+# ~1e-7 of the reference's relative to its peak, so a column agrees within
+# ~1e-7 * peak(model) / step; stated against the model's peak.
+FD_TOL = 2e-6
+
+
+def test_image_param_derivatives_match_reference(backend):
+    """getDerivs with the PSF and sky thawed (engine.py:306-324): forward
+    differences of the model image for every PSF parameter of a
+    GaussianMixturePSF and a GaussianMixtureEllipsePSF, the sky's own
+    derivative, against the reference's columns (psf_derivs.npz)."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'psf_derivs.npz'))
+    for tag, ellipse in (('mog', False), ('ell', True)):
+        tr, tim = _psf_scene(T, ellipse)
+        assert tr.getParamNames() == list(g[tag + '_names'])
+        np.testing.assert_allclose(tr.getParams(), g[tag + '_params'], rtol=0, atol=1e-12)
+        mod = tr.getModelImage(0)
+        ref = g[tag + '_model']
+        peak = np.abs(ref).max()
+        assert np.abs(mod - ref).max() <= PEAK_TOL * peak, tag
+        derivs = tr.getDerivs()
+        assert len(derivs) == len(g[tag + '_names'])
+        steps = tim.getStepSizes()
+        for k, d in enumerate(derivs):
+            (patch, img), = d
+            full = np.zeros(img.shape, np.float64)
+            patch.addTo(full)
+            err = np.abs(full - g[tag + '_derivs'][k]).max()
+            assert err <= FD_TOL * peak / steps[k], (tag, k, err, peak / steps[k])
+
+
+def test_psf_optimizer_fits_match_reference(backend):
+    """GaussianMixtureEllipsePSF.fromStamp (psf.py:757-789) and
+    GaussianMixturePSF.fromStamp(v3=True) (psf.py:563-575): the optimiser,
+    the PSF thawed, on a Moffat stamp, against the reference's fitted
+    parameters."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'psf_derivs.npz'))
+    p1 = T.GaussianMixtureEllipsePSF.fromStamp(g['stamp'], N=2)
+    np.testing.assert_allclose(p1.getAllParams(), g['ell_fit'], rtol=2e-3, atol=2e-4)
+    p2 = T.GaussianMixturePSF.fromStamp(g['stamp'], N=2, v3=True)
+    np.testing.assert_allclose(p2.getAllParams(), g['v3_fit'], rtol=2e-3, atol=2e-4)
+
+
+def test_em_from_stamp_matches_reference(backend):
+    """GaussianMixturePSF.fromStamp's EM fit (em_fit_2d_reg, emfit.i:274-557,
+    on the device in FP64) against the reference's fits (emfit.npz): 7
+    stamps, 1-4 components, the alpha prior, explicit origins, P0; the
+    batched fromStamps equal to one fit per stamp."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'emfit.npz'))
+    for i in range(int(g['n'])):
+        N, alpha, steps, hasxy, x0, y0, hasp0 = g['cfg%d' % i]
+        P0 = ((g['p0amp%d' % i].copy(), g['p0mean%d' % i].copy(), g['p0var%d' % i].copy())
+              if hasp0 else None)
+        psf = T.GaussianMixturePSF.fromStamp(g['stamp%d' % i], N=int(N), P0=P0,
+                                             xy0=(int(x0), int(y0)) if hasxy else None,
+                                             alpha=float(alpha), emsteps=int(steps))
+        np.testing.assert_allclose(psf.mog.amp, g['amp%d' % i], rtol=1e-9, atol=1e-13)
+        np.testing.assert_allclose(psf.mog.mean, g['mean%d' % i], rtol=0, atol=1e-9)
+        np.testing.assert_allclose(psf.mog.var, g['var%d' % i], rtol=1e-9, atol=1e-12)
+    stamps = [g['stamp%d' % i] for i in (0, 6)]   # two 25 x 25 stamps
+    batch = T.GaussianMixturePSF.fromStamps(stamps, N=3, alpha=0.2, emsteps=300)
+    for st, b in zip(stamps, batch):
+        one = T.GaussianMixturePSF.fromStamp(st, N=3, alpha=0.2, emsteps=300)
+        assert np.array_equal(b.mog.amp, one.mog.amp)
+        assert np.array_equal(b.mog.var, one.mog.var)
+
+
+def test_em_fit_reports_degenerate_covariance(backend):
+    """A non-positive covariance determinant stops the fit with the
+    parameters as they were and returns -1 (emfit.i:403-409)."""
+    from tractor_b200 import emfit
+    st = np.ones((9, 9)) / 81.
+    w, mu = np.array([1.]), np.zeros((1, 2))
+    var = np.array([[[1., 2.], [2., 1.]]])
+    assert emfit.em_fit_2d_reg(st, -4, -4, w, mu, var, 0., 10) == -1
+    assert w[0] == 1. and not mu.any() and var[0, 0, 1] == 2.

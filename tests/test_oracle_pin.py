@@ -155,3 +155,71 @@ def test_oracle_matches_live_reference(oracle):
         m = SersicMixture.getProfile(n)
         a, v = oracle.sersic_profile(n)
         assert np.array_equal(m.amp, a) and np.array_equal(m.var[:, 0, 0], v)
+
+
+def _em_case(g, i):
+    """Inputs of golden EM case i after fromStamp's preprocessing
+    (tractor/psf.py:549-591)."""
+    N, alpha, steps, hasxy, x0, y0, hasp0 = g['cfg%d' % i]
+    N, steps = int(N), int(steps)
+    st = g['stamp%d' % i].copy()
+    st /= st.sum()
+    st = np.maximum(st, 0)
+    if hasp0:
+        w, mu, var = g['p0amp%d' % i].copy(), g['p0mean%d' % i].copy(), g['p0var%d' % i].copy()
+    else:
+        w = np.ones(N) / N
+        mu = np.zeros((N, 2))
+        var = np.array([np.eye(2) * (k + 1) for k in range(N)])
+    ny, nx = st.shape
+    xy = (int(x0), int(y0)) if hasxy else (-(nx // 2), -(ny // 2))
+    return st, N, float(alpha), steps, xy, (w, mu, var), bool(hasxy), bool(hasp0)
+
+
+def test_em_fit_matches_golden(oracle):
+    """The oracle's em_fit_2d_reg against GaussianMixturePSF.fromStamp run by
+    the reference (emfit.npz): 7 stamps, 1-4 components, prior, origins, P0."""
+    g = _golden('emfit.npz')
+    for i in range(int(g['n'])):
+        st, N, alpha, steps, (xm, ym), (w, mu, var), _, _ = _em_case(g, i)
+        assert oracle.em_fit_2d_reg(st, xm, ym, w, mu, var, alpha, steps) == 0
+        np.testing.assert_allclose(w, g['amp%d' % i], rtol=1e-11, atol=1e-14)
+        np.testing.assert_allclose(mu, g['mean%d' % i], rtol=0, atol=1e-11)
+        np.testing.assert_allclose(var, g['var%d' % i], rtol=1e-11, atol=1e-13)
+
+
+def test_em_fit_failure_leaves_parameters(oracle):
+    """A non-positive covariance determinant returns -1 before any update
+    (tractor/emfit.i:403-409)."""
+    st = np.ones((9, 9)) / 81.
+    w, mu = np.array([1.]), np.zeros((1, 2))
+    var = np.array([[[1., 2.], [2., 1.]]])
+    assert oracle.em_fit_2d_reg(st, -4, -4, w, mu, var, 0., 10) == -1
+    assert w[0] == 1. and not mu.any() and var[0, 0, 1] == 2.
+
+
+@pytest.mark.reference
+def test_em_oracle_matches_live_reference(oracle):
+    from oracle import refharness
+    if not refharness.available():
+        pytest.skip('reference source tree not present')
+    refharness.load()
+    from tractor import emfit
+    rng = np.random.default_rng(11)
+    for trial in range(6):
+        K = int(rng.integers(1, 5))
+        h, w_ = int(rng.integers(9, 30)), int(rng.integers(9, 30))
+        y, x = np.mgrid[:h, :w_]
+        img = np.exp(-0.5 * ((x - w_ / 2.) ** 2 + (y - h / 2.) ** 2) / rng.uniform(1, 9))
+        img = np.maximum(img / img.sum() + rng.normal(0, 1e-4, img.shape), 0)
+        amp = np.ones(K) / K
+        mean = rng.normal(0, 0.5, (K, 2))
+        var = np.array([np.eye(2) * (k + 1) for k in range(K)])
+        alpha = float(rng.choice([0., 0.3]))
+        a2, m2, v2 = amp.copy(), mean.copy(), var.copy()
+        r1 = emfit.em_fit_2d_reg(img, -(w_ // 2), -(h // 2), amp, mean, var, alpha, 200)
+        r2 = oracle.em_fit_2d_reg(img, -(w_ // 2), -(h // 2), a2, m2, v2, alpha, 200)
+        assert r1 == r2 == 0
+        np.testing.assert_allclose(a2, amp, rtol=1e-11, atol=1e-14)
+        np.testing.assert_allclose(m2, mean, rtol=0, atol=1e-10)
+        np.testing.assert_allclose(v2, var, rtol=1e-11, atol=1e-13)

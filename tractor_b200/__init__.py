@@ -16,7 +16,8 @@ from .basics import (PixPos, NullWCS, Flux, Mag, Fluxes, NanoMaggies, MultiBandB
                      NullPhotoCal, LinearPhotoCal, NullSky, ConstantSky, Image)
 from .ellipses import GalaxyShape, EllipseE, EllipseESoft
 from .profiles import MixtureOfGaussians, SersicMixture
-from .psf import (HybridPSF, HybridPixelizedPSF, GaussianMixturePSF, NCircularGaussianPSF,
+from .psf import (HybridPSF, HybridPixelizedPSF, GaussianMixturePSF, GaussianMixtureEllipsePSF,
+                  NCircularGaussianPSF,
                   PixelizedPSF, NormalizedPixelizedPsf, MogParams)
 from .sources import (BasicSource, SingleProfileSource, PointSource, Galaxy, ProfileGalaxy,
                       HoggGalaxy, GaussianGalaxy, ExpGalaxy, DevGalaxy, SersicGalaxy, SersicIndex,
@@ -31,7 +32,8 @@ __all__ = [
     'NullSky', 'ConstantSky', 'Image',
     'GalaxyShape', 'EllipseE', 'EllipseESoft',
     'MixtureOfGaussians', 'SersicMixture',
-    'HybridPSF', 'HybridPixelizedPSF', 'GaussianMixturePSF', 'NCircularGaussianPSF', 'PixelizedPSF',
+    'HybridPSF', 'HybridPixelizedPSF', 'GaussianMixturePSF', 'GaussianMixtureEllipsePSF',
+    'NCircularGaussianPSF', 'PixelizedPSF',
     'NormalizedPixelizedPsf',
     'PointSource', 'Galaxy', 'ProfileGalaxy', 'HoggGalaxy', 'GaussianGalaxy', 'ExpGalaxy',
     'DevGalaxy', 'SersicGalaxy', 'SersicIndex', 'FracDev', 'SoftenedFracDev',

@@ -48,6 +48,7 @@ SCENE_ITEM = np.dtype([('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'), ('h', '<i4'),
                        ('fx', '<f8'), ('fy', '<f8'), ('scale', '<f4'), ('floor', '<f4')])
 
 FIT_NPAR, FIT_MAX_BANDS, FIT_MAX_SRC, FIT_MAX_PSF = 9, 3, 32, 4
+EM_MAX_K = 8   # TB_EM_MAX_K
 FIT_SOURCE = np.dtype([('profile', '<i4'), ('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'),
                        ('h', '<i4'), ('blob', '<i4'), ('frozen', '<i4'), ('pad', '<i4')])
 FIT_BLOB = np.dtype([('n_src', '<i4'), ('src0', '<i4'), ('P', '<i4'), ('unit0', '<i4'),
@@ -107,6 +108,7 @@ SIGNATURES = {
     'tb_psf_spectrum': (_I32, [_P, _P, _I32, _I32, _I32, _P]),
     'tb_normal_equations': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _I32, _P]),
     'tb_tensor_core_timeouts': (_I32, [_P]),
+    'tb_em_fit_2d': (_I32, [_P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _D, _I32, _P, _P]),
     'tb_solve_update': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P, _P]),
     'tb_solve_update_noalloc': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P]),
     'tb_chi2': (_I32, [_P, _P, _P, _P, _P, _I32, _P, _P]),

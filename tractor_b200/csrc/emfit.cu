@@ -1,0 +1,173 @@
+// Batched EM fit of 2-D Gaussian mixtures to images (sm_100a): the batched
+// form of em_fit_2d_reg (tractor/emfit.i:274-557), which
+// GaussianMixturePSF.fromStamp (tractor/psf.py:536-597) runs on a PSF stamp.
+//
+// One CTA per image, all iterations inside the kernel, FP64 throughout (as
+// the reference).  Each iteration:
+//   * per component: C^-1 and amp / (2 pi sqrt det C) (a non-positive
+//     determinant stops the fit, as the reference returns -1 there);
+//   * E step: the responsibility of component k at pixel (x, y) is
+//     z_k / sum_j z_j with z_k = scale_k exp(-dsq_k / 2), 0 for dsq >= 100
+//     (z itself where the sum is 0, as the reference leaves it);
+//   * M step from the weighted moments w = img z_k / sum z (sum w, sum w x,
+//     sum w y, sum w x^2, sum w x y, sum w y^2), summed per thread over a
+//     fixed pixel stride and then over the block in a fixed order (every
+//     launch gives the same result): mean = (sum w x, sum w y) / sum w,
+//     covariance = (alpha I + sum w (x - mean)(x - mean)^T) / (sum w + alpha)
+//     with sum w (x - m)^2 = sum w x^2 - m sum w x, amplitude = sum w.
+// The reference sums the second moments about the new mean in a second pass
+// over the pixels; the expansion above is the same sum in one pass (the
+// difference is FP64 rounding).
+#include "tb_common.cuh"
+
+namespace {
+
+constexpr int kEmThreads = 128;
+constexpr int kWarps = kEmThreads / 32;
+
+template <int K>
+__global__ void __launch_bounds__(kEmThreads, 4)
+em_fit_kernel(const double* __restrict__ img, int n, int ny, int nx,
+              const int32_t* __restrict__ xy0, double* __restrict__ amp,
+              double* __restrict__ mean, double* __restrict__ var, double alpha, int steps,
+              int32_t* __restrict__ status) {
+    constexpr int kM = 6 * K;   // moments per image
+    __shared__ double w_s[K], mu_s[K][2], v_s[K][4];
+    __shared__ double iv_s[K][4], sc_s[K];
+    __shared__ double red[kWarps][kM];
+    __shared__ int bad;
+    const int s = blockIdx.x;
+    if (s >= n) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double* im = img + (int64_t)s * ny * nx;
+    double* A = amp + (int64_t)s * K;
+    double* Mu = mean + (int64_t)s * K * 2;
+    double* V = var + (int64_t)s * K * 4;
+    const int x0 = xy0 ? xy0[2 * s] : -(nx / 2);
+    const int y0 = xy0 ? xy0[2 * s + 1] : -(ny / 2);
+    const int npix = nx * ny;
+    const double tpd = 4.0 * TB_PI * TB_PI;   // (2 pi)^D, D = 2
+    if (tid < K) {
+        w_s[tid] = A[tid];
+        mu_s[tid][0] = Mu[2 * tid];
+        mu_s[tid][1] = Mu[2 * tid + 1];
+#pragma unroll
+        for (int d = 0; d < 4; d++) v_s[tid][d] = V[4 * tid + d];
+    }
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    for (int step = 0; step < steps; step++) {
+        if (tid < K) {
+            const double* Vk = v_s[tid];
+            const double det = Vk[0] * Vk[3] - Vk[1] * Vk[2];
+            if (det <= 0.0) bad = 1;
+            iv_s[tid][0] = Vk[3] / det;
+            iv_s[tid][1] = -Vk[1] / det;
+            iv_s[tid][2] = -Vk[2] / det;
+            iv_s[tid][3] = Vk[0] / det;
+            sc_s[tid] = w_s[tid] / sqrt(tpd * det);
+        }
+        __syncthreads();
+        if (bad) break;   // the same value in every thread
+        double acc[kM];
+#pragma unroll
+        for (int v = 0; v < kM; v++) acc[v] = 0.0;
+        for (int i = tid; i < npix; i += kEmThreads) {
+            const int iy = i / nx, ix = i - iy * nx;
+            const double x = (double)(x0 + ix), y = (double)(y0 + iy);
+            double z[K];
+            double zsum = 0.0;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const double dx = x - mu_s[k][0], dy = y - mu_s[k][1];
+                const double dsq = iv_s[k][0] * dx * dx + iv_s[k][1] * dx * dy +
+                                   iv_s[k][2] * dx * dy + iv_s[k][3] * dy * dy;
+                z[k] = dsq >= 100.0 ? 0.0 : sc_s[k] * exp(-0.5 * dsq);
+                zsum += z[k];
+            }
+            // a pixel whose z sum to 0 keeps them unnormalised (all 0 unless
+            // some amplitude is negative), as the reference does
+            const bool norm = zsum != 0.0;
+            const double d = im[i];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const double wi = d * (norm ? z[k] / zsum : z[k]);
+                acc[6 * k + 0] += wi;
+                acc[6 * k + 1] += wi * x;
+                acc[6 * k + 2] += wi * y;
+                acc[6 * k + 3] += wi * x * x;
+                acc[6 * k + 4] += wi * x * y;
+                acc[6 * k + 5] += wi * y * y;
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < kM; v++) {
+            double a = acc[v];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+            if (lane == 0) red[warp][v] = a;
+        }
+        __syncthreads();
+        if (tid < K) {
+            double m[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                double t = 0.0;
+                for (int w2 = 0; w2 < kWarps; w2++) t += red[w2][6 * tid + q];
+                m[q] = t;
+            }
+            const double ws = m[0];
+            const double mx = m[1] / ws, my = m[2] / ws;
+            mu_s[tid][0] = mx;
+            mu_s[tid][1] = my;
+            const double den = ws + alpha;
+            v_s[tid][0] = (alpha + (m[3] - mx * m[1])) / den;
+            v_s[tid][1] = (m[4] - mx * m[2]) / den;
+            v_s[tid][2] = v_s[tid][1];
+            v_s[tid][3] = (alpha + (m[5] - my * m[2])) / den;
+            w_s[tid] = ws;
+        }
+        __syncthreads();
+    }
+    if (tid < K) {
+        A[tid] = w_s[tid];
+        Mu[2 * tid] = mu_s[tid][0];
+        Mu[2 * tid + 1] = mu_s[tid][1];
+#pragma unroll
+        for (int d = 0; d < 4; d++) V[4 * tid + d] = v_s[tid][d];
+    }
+    if (tid == 0 && status) status[s] = bad;
+}
+
+template <int K>
+int launch(const double* img, int n, int ny, int nx, const int32_t* xy0, double* amp,
+           double* mean, double* var, double alpha, int steps, int32_t* status,
+           cudaStream_t s) {
+    em_fit_kernel<K><<<n, kEmThreads, 0, s>>>(img, n, ny, nx, xy0, amp, mean, var, alpha, steps,
+                                              status);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+}  // namespace
+
+extern "C" int tb_em_fit_2d(const double* img, int32_t n, int32_t ny, int32_t nx,
+                            const int32_t* xy0, double* amp, double* mean, double* var,
+                            int32_t K, double alpha, int32_t steps, int32_t* status,
+                            void* stream) {
+    if (n < 0 || ny < 1 || nx < 1 || (int64_t)ny * nx > (1 << 24) || K < 1 ||
+        K > TB_EM_MAX_K || steps < 0)
+        return TB_ERR_ARG;
+    if (n == 0) return TB_OK;
+    if (!img || !amp || !mean || !var) return TB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (K) {
+        case 1: return launch<1>(img, n, ny, nx, xy0, amp, mean, var, alpha, steps, status, s);
+        case 2: return launch<2>(img, n, ny, nx, xy0, amp, mean, var, alpha, steps, status, s);
+        case 3: return launch<3>(img, n, ny, nx, xy0, amp, mean, var, alpha, steps, status, s);
+        case 4: return launch<4>(img, n, ny, nx, xy0, amp, mean, var, alpha, steps, status, s);
+        case 5: return launch<5>(img, n, ny, nx, xy0, amp, mean, var, alpha, steps, status, s);
+        case 6: return launch<6>(img, n, ny, nx, xy0, amp, mean, var, alpha, steps, status, s);
+        case 7: return launch<7>(img, n, ny, nx, xy0, amp, mean, var, alpha, steps, status, s);
+        default: return launch<8>(img, n, ny, nx, xy0, amp, mean, var, alpha, steps, status, s);
+    }
+}

@@ -45,6 +45,30 @@ class Images(MultiParams):
         return 'image%i' % j
 
 
+def _once(fn):
+    """fn() evaluated at most once."""
+    box = []
+
+    def get():
+        if not box:
+            box.append(fn())
+        return box[0]
+    return get
+
+
+class _FiniteDifference(object):
+    """A pending forward-difference column of an image parameter:
+    Patch(0, 0, (mod - mod0) / step) (engine.py:318-320)."""
+
+    def __init__(self, fin, fin0, step, name):
+        self.fin, self.fin0, self.step, self.name = fin, fin0, step, name
+
+    def result(self):
+        deriv = Patch(0, 0, (self.fin() - self.fin0()) / self.step)
+        deriv.name = self.name
+        return deriv
+
+
 class Tractor(MultiParams):
     """tractor/engine.py:96-497."""
 
@@ -169,11 +193,13 @@ class Tractor(MultiParams):
             p = self._plan_model_patch(plan, img, src, minsb=minsb, **kwargs)
             if p is not None:
                 pend.append(p)
+        # the sky as it is now (the plan may run after parameters change)
+        mod0 = np.zeros(img.getModelShape(), self.modtype)
+        if sky:
+            img.getSky().addTo(mod0)
 
         def finish():
-            mod = np.zeros(img.getModelShape(), self.modtype)
-            if sky:
-                img.getSky().addTo(mod)
+            mod = mod0.copy()
             for p in pend:
                 patch = p.result()
                 if patch is not None:
@@ -335,14 +361,26 @@ class Tractor(MultiParams):
             srcs = list(self.catalog.getThawedSources())
         pend = []
         if not self.isParamFrozen('images'):
+            # image parameters (PSF, sky, ...) without analytic derivatives:
+            # forward differences of the whole model image (engine.py:306-324),
+            # the unperturbed and every perturbed model planned into the same
+            # batch (a plan renders the state at the time of the call)
             for i in self.images.getThawedParamIndices():
                 img = self.images[i]
                 derivs = img.getParamDerivatives(self, self.catalog)
+                fin0 = None
                 for di, deriv in enumerate(derivs):
                     if deriv is False:
-                        raise NotImplementedError(
-                            'finite-difference image-parameter derivatives (PSF, WCS, photocal) '
-                            'are not provided; freeze the images')
+                        if fin0 is None:
+                            fin0 = _once(self._plan_model_image(plan, img, **kwargs))
+                            p0 = img.getParams()
+                            stepsizes = img.getStepSizes()
+                            paramnames = img.getParamNames()
+                        oldval = img.setParam(di, p0[di] + stepsizes[di])
+                        fin = self._plan_model_image(plan, img, **kwargs)
+                        img.setParam(di, oldval)
+                        deriv = _FiniteDifference(fin, fin0, stepsizes[di],
+                                                  'd(im%i)/d(%s)' % (i, paramnames[di]))
                     allderivs.append([(deriv, img)])
         for src in srcs:
             per_img = []
@@ -355,7 +393,8 @@ class Tractor(MultiParams):
             pend.append((src, per_img))
 
         def finish():
-            out = list(allderivs)
+            out = [[(d.result() if isinstance(d, _FiniteDifference) else d, img)
+                    for d, img in col] for col in allderivs]
             for src, per_img in pend:
                 srcderivs = [[] for _ in range(src.numberOfParams())]
                 for img, plist in per_img:

@@ -92,6 +92,13 @@ class MogParams(ParamList):
         self.mog = MixtureOfGaussians(amp, mean, var)
         K = self.mog.K
         super(MogParams, self).__init__()
+        self._set_param_names(K)
+        self.liquid = [True] * self._numberOfThings()
+        self.lowers = [None] * self._numberOfThings()
+        self.uppers = [None] * self._numberOfThings()
+        self.maxstep = [None] * self._numberOfThings()
+
+    def _set_param_names(self, K):
         names = {}
         for k in range(K):
             names['amp%i' % k] = k
@@ -101,10 +108,6 @@ class MogParams(ParamList):
             names['varyy%i' % k] = 3 * K + 3 * k + 1
             names['varxy%i' % k] = 3 * K + 3 * k + 2
         self.addNamedParams(**names)
-        self.liquid = [True] * self._numberOfThings()
-        self.lowers = [None] * self._numberOfThings()
-        self.uppers = [None] * self._numberOfThings()
-        self.maxstep = [None] * self._numberOfThings()
 
     def _numberOfThings(self):
         return 6 * self.mog.K
@@ -226,6 +229,201 @@ class GaussianMixturePSF(MogParams):
         plan = RenderPlan()
         p = self._plan_point_source(plan, px, py, **kwargs)
         return p.result()
+
+    @staticmethod
+    def _stamp_for_em(stamp):
+        # fromStamp's preprocessing, in the stamp's own dtype (psf.py:590-591)
+        stamp = np.array(stamp, copy=True)
+        stamp /= stamp.sum()
+        return np.maximum(stamp, 0)
+
+    @staticmethod
+    def fromStamp(stamp, N=3, P0=None, xy0=None, alpha=0., emsteps=1000, v2=False,
+                  approx=1e-30, v3=False):
+        """GaussianMixturePSF.fromStamp (tractor/psf.py:536-597): an N-component
+        mixture fit to a PSF stamp by EM on the GPU (em_fit_2d_reg), or with
+        v3 by the Tractor optimiser with the PSF's parameters thawed."""
+        from .emfit import em_init_params, em_fit_2d_reg
+        if P0 is not None:
+            w, mu, var = P0
+        else:
+            w, mu, var = em_init_params(N, None, None, None)
+        stamp = stamp.copy()
+        if xy0 is None:
+            xm, ym = -(stamp.shape[1] // 2), -(stamp.shape[0] // 2)
+        else:
+            xm, ym = xy0
+        if v3:
+            from .basics import Image, PixPos, Flux
+            from .engine import Tractor
+            from .sources import PointSource
+            tpsf = GaussianMixturePSF(w, mu, var)
+            tim = Image(data=stamp, invvar=1e6 * np.ones_like(stamp), psf=tpsf)
+            h, ww = tim.shape
+            src = PointSource(PixPos(ww // 2, h // 2), Flux(1.))
+            tr = Tractor([tim], [src])
+            tr.freezeParam('catalog')
+            tim.freezeAllBut('psf')
+            tim.modelMinval = approx
+            for step in range(20):
+                dlnp, X, alpha = tr.optimize(shared_params=False)
+                if dlnp < 1e-6:
+                    break
+            return tpsf
+        if v2:
+            raise NotImplementedError('fromStamp(v2=True) (em_fit_2d_reg2, a mixture plus a '
+                                      'sky term) is not provided')
+        stamp = GaussianMixturePSF._stamp_for_em(stamp)
+        w = np.array(w, np.float64)
+        mu = np.array(mu, np.float64)
+        var = np.array(var, np.float64)
+        em_fit_2d_reg(stamp, xm, ym, w, mu, var, alpha, emsteps)
+        return GaussianMixturePSF(w, mu, var)
+
+    @staticmethod
+    def fromStamps(stamps, N=3, P0=None, xy0=None, alpha=0., emsteps=1000):
+        """fromStamp's EM fit for many stamps of one size at once (one launch;
+        P0 and xy0 apply to every stamp).  Returns a list of
+        GaussianMixturePSF, None where the fit failed (a non-positive
+        covariance determinant: fromStamp's em_fit_2d_reg returns -1 there)."""
+        from .emfit import em_init_params, em_fit_2d_batch
+        if P0 is not None:
+            w, mu, var = P0
+        else:
+            w, mu, var = em_init_params(N, None, None, None)
+        stamps = [GaussianMixturePSF._stamp_for_em(s) for s in stamps]
+        if not stamps:
+            return []
+        ny, nx = stamps[0].shape
+        n = len(stamps)
+        if xy0 is None:
+            xy0 = (-(nx // 2), -(ny // 2))
+        a, m, v, st = em_fit_2d_batch(np.stack(stamps),
+                                      np.broadcast_to(np.asarray(w, np.float64), (n, len(w))),
+                                      np.broadcast_to(np.asarray(mu, np.float64), (n,) + np.shape(mu)),
+                                      np.broadcast_to(np.asarray(var, np.float64), (n,) + np.shape(var)),
+                                      alpha, emsteps, xy0=xy0)
+        return [None if st[i] else GaussianMixturePSF(a[i], m[i], v[i]) for i in range(n)]
+
+
+class GaussianMixtureEllipsePSF(GaussianMixturePSF):
+    """A GaussianMixturePSF whose covariances are EllipseESoft shapes
+    (tractor/psf.py:658-789): parameters amp[K], the means (x, y) per
+    component, then (logr, ee1, ee2) per component; rendered as the mixture
+    of their covariances."""
+
+    def __init__(self, *args):
+        from .ellipses import EllipseESoft
+        if len(args) == 3:
+            amp, mean, ell = args
+        else:
+            assert len(args) % 6 == 0
+            K = len(args) // 6
+            amp = np.array(args[:K])
+            mean = np.array(args[K:3 * K]).reshape((K, 2))
+            rest = args[3 * K:]
+            ell = [EllipseESoft(*rest[3 * k: 3 * (k + 1)]) for k in range(K)]
+        K = len(amp)
+        var = np.zeros((K, 2, 2))
+        for k in range(K):
+            var[k] = self.ellipseToVariance(ell[k])
+        self.ellipses = [e.copy() for e in ell]
+        super(GaussianMixtureEllipsePSF, self).__init__(amp, mean, var)
+        self.stepsizes = [0.001] * K + [0.001] * (K * 2) + [0.001] * (K * 3)
+
+    def ellipseToVariance(self, ell):
+        return ell.getCovariance()
+
+    def getShifted(self, x0, y0):
+        return self
+
+    def _set_param_names(self, K):
+        names = {}
+        for k in range(K):
+            names['amp%i' % k] = k
+            names['meanx%i' % k] = K + (k * 2)
+            names['meany%i' % k] = K + (k * 2) + 1
+            names['logr%i' % k] = K * 3 + (k * 3)
+            names['ee1-%i' % k] = K * 3 + (k * 3) + 1
+            names['ee2-%i' % k] = K * 3 + (k * 3) + 2
+        self.addNamedParams(**names)
+
+    def toMog(self):
+        return GaussianMixturePSF(self.mog.amp, self.mog.mean, self.mog.var)
+
+    def mogAt(self, x, y):
+        return self.toMog()
+
+    def constantPsfAt(self, x, y):
+        return self.mogAt(x, y)
+
+    def hashkey(self):
+        return ('GaussianMixtureEllipsePSF',) + tuple(self.getAllParams())
+
+    def copy(self):
+        return GaussianMixtureEllipsePSF(self.mog.amp.copy(), self.mog.mean.copy(),
+                                         [e.copy() for e in self.ellipses])
+
+    def __str__(self):
+        return ('GaussianMixtureEllipsePSF: amps=' +
+                '[' + ', '.join(['%.3f' % a for a in self.mog.amp.ravel()]) + ']' +
+                ', means=[' + ', '.join(['(%.3f, %.3f)' % (x, y) for x, y in self.mog.mean]) +
+                ']' + ', ellipses=' + ', '.join(str(e) for e in self.ellipses) +
+                ', var=' + str(tuple(self.mog.var.ravel())))
+
+    def _getThings(self):
+        p = list(self.mog.amp) + list(self.mog.mean.ravel())
+        for e in self.ellipses:
+            p += e.getAllParams()
+        return p
+
+    def _setThings(self, p):
+        K = self.mog.K
+        self.mog.amp = np.atleast_1d(np.asarray(p[:K], np.float64))
+        pp = p[K:]
+        self.mog.mean = np.atleast_2d(np.asarray(pp[:K * 2], np.float64)).reshape(K, 2)
+        pp = pp[K * 2:]
+        for i, e in enumerate(self.ellipses):
+            e.setAllParams(pp[:3])
+            pp = pp[3:]
+            self.mog.var[i, :, :] = self.ellipseToVariance(e)
+
+    def _setThing(self, i, p):
+        things = self._getThings()
+        old = things[i]
+        things[i] = p
+        self._setThings(things)
+        return old
+
+    @staticmethod
+    def fromStamp(stamp, N=3, P0=None, approx=1e-6, damp=0.):
+        """GaussianMixtureEllipsePSF.fromStamp (tractor/psf.py:757-789): the
+        Tractor optimiser, the PSF's parameters thawed, fitting a point
+        source at the stamp centre (model images and their forward
+        differences rendered on the GPU)."""
+        from .basics import Image, PixPos, Flux
+        from .ellipses import EllipseESoft
+        from .engine import Tractor
+        from .sources import PointSource
+        w = np.ones(N) / float(N)
+        mu = np.zeros((N, 2))
+        ell = [EllipseESoft(np.log(2 * r), 0., 0.) for r in range(1, N + 1)]
+        psf = GaussianMixtureEllipsePSF(w, mu, ell)
+        if P0 is not None:
+            psf.setAllParams(P0)
+        tim = Image(data=stamp, invvar=1e6 * np.ones_like(stamp), psf=psf)
+        H, W = stamp.shape
+        src = PointSource(PixPos(W // 2, H // 2), Flux(1.))
+        tr = Tractor([tim], [src])
+        tr.freezeParam('catalog')
+        tim.freezeAllBut('psf')
+        tim.modelMinval = approx
+        alphas = [0.1, 0.3, 1.0]
+        for step in range(50):
+            dlnp, X, alpha = tr.optimize(shared_params=False, alphas=alphas, damp=damp)
+            if dlnp < 1e-6:
+                break
+        return psf
 
 
 def getCircularMog(amps, sigmas):

@@ -82,7 +82,10 @@ class MogBatch(object):
         per-component floors of c_gauss_2d_approx3; `derivs` also writes the
         d/dmean_x and d/dmean_y planes right after the patch (packed outputs
         only)."""
-        amp = np.asarray(amp, np.float64).ravel()
+        # copies: a plan renders the state at the time of the call even if
+        # the caller's arrays change before it runs (line searches, finite
+        # differences of image parameters)
+        amp = np.array(amp, np.float64).ravel()
         K = len(amp)
         if K > 256:
             raise ValueError('at most 256 components per mixture (got %d)' % K)
@@ -105,8 +108,8 @@ class MogBatch(object):
                            float(fx), float(fy), float(floor), float(scale), floor_mode,
                            int(out_off), int(mask_off), 0, int(deriv_off)))
         self.amp.append(amp)
-        self.mean.append(np.asarray(mean, np.float64).reshape(K, 2))
-        self.var.append(np.asarray(var, np.float64).reshape(K, 2, 2))
+        self.mean.append(np.array(mean, np.float64).reshape(K, 2))
+        self.var.append(np.array(var, np.float64).reshape(K, 2, 2))
         self.ncomp += K
         return out_off
 
@@ -230,7 +233,7 @@ class FftBatch(object):
 
     def add(self, amp, var, sz, spec_key, spec, mw, mh, sx, sy, mux, muy, scale=1.,
             out_off=None, ldo=0, mode=MOG_STORE):
-        amp = np.asarray(amp, np.float64).ravel()
+        amp = np.array(amp, np.float64).ravel()   # copies, as MogBatch.add
         K = len(amp)
         if K > 128:
             raise ValueError('at most 128 components per galaxy (got %d)' % K)
@@ -248,7 +251,7 @@ class FftBatch(object):
                            float(mux), float(muy), float(scale), int(ldo), int(out_off),
                            self.spec_off[key], _lib.FFT_VALUE, 0, 0))
         self.amp.append(amp)
-        self.var.append(np.asarray(var, np.float64).reshape(K, 2, 2))
+        self.var.append(np.array(var, np.float64).reshape(K, 2, 2))
         self.ncomp += K
         return out_off
 
