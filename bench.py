@@ -22,8 +22,9 @@ a 3-component MoG PSF; prep + binning + one persistent tile render, the
 tile height autotuned), batched blob fitting (2,000 blobs x 3 bands) and the
 dense normal equations on the tensor cores (512 problems x 63 parameters x
 16,384 rows), each with its own end-to-end number, roofline and CPU baseline,
-and the small plain fit through the object API (latency-bound: us per render,
-ms per fit) (--no-secondary skips them).
+the small plain fit through the object API (latency-bound: us per render,
+ms per fit) and EM fits of 4,096 PSF stamps (GaussianMixturePSF.fromStamp's
+em_fit_2d_reg, FP64) (--no-secondary skips them).
 
 --impl reference times the reference's CPU implementation of the same
 workload on the host cores (its own compiled C for the spectrum and the
@@ -704,6 +705,124 @@ def bench_plain_small(args, dev):
                     'fitter is not on the GPU host'}
 
 
+# secondary workload: EM fits of PSF stamps (GaussianMixturePSF.fromStamp)
+EM_STAMPS, EM_SIDE, EM_K, EM_STEPS = 4096, 25, 3, 1000
+FP64_NOMINAL_TFLOPS = 40.0     # B200 FP64 (non-tensor), nominal: no measured figure
+
+
+def em_stamps(n, seed=900):
+    """Seeded 25 x 25 PSF stamps: two concentric Gaussians (sigma s and 2.5 s,
+    s U[1, 2], weights 0.7 / 0.3, centre offset U[-0.5, 0.5] px) plus noise
+    of 1e-5 of the total, normalised and clipped at 0 as fromStamp does."""
+    rng = np.random.default_rng(seed)
+    h = EM_SIDE // 2
+    y, x = np.mgrid[:EM_SIDE, :EM_SIDE] - float(h)
+    out = np.empty((n, EM_SIDE, EM_SIDE))
+    for i in range(n):
+        s = rng.uniform(1., 2.)
+        cx, cy = rng.uniform(-0.5, 0.5, 2)
+        r2 = (x - cx) ** 2 + (y - cy) ** 2
+        im = 0.7 * np.exp(-r2 / (2 * s * s)) + 0.3 * np.exp(-r2 / (2 * (2.5 * s) ** 2))
+        im = im / im.sum() + rng.normal(0., 1e-5, im.shape)
+        out[i] = np.maximum(im / im.sum(), 0.)
+    return out
+
+
+def bench_emfit(args, dev, flush, clk, cpu_seconds):
+    """EM fits of 3-Gaussian mixtures to 4,096 PSF stamps of 25 x 25 pixels,
+    1,000 iterations each (GaussianMixturePSF.fromStamp's em_fit_2d_reg,
+    FP64): device-resident launches of tb_em_fit_2d timed with CUDA events,
+    and end to end through tractor_b200.emfit.em_fit_2d_batch from host
+    arrays.  CPU baseline: the reference's own em_fit_2d_reg (compiled from
+    tractor/emfit.i into oracle/_ref) on a bounded sample, one core."""
+    import torch
+    from tractor_b200 import _lib, emfit
+    lib = _lib.load()
+    n, K = EM_STAMPS, EM_K
+    imgs = em_stamps(n)
+    w, mu, var = emfit.em_init_params(K, None, None, None)
+    A0 = np.ascontiguousarray(np.broadcast_to(w, (n, K)))
+    M0 = np.ascontiguousarray(np.broadcast_to(mu, (n, K, 2)))
+    V0 = np.ascontiguousarray(np.broadcast_to(var, (n, K, 2, 2)))
+    d_img = torch.from_numpy(imgs).to(dev)
+    init = [torch.from_numpy(a).to(dev) for a in (A0, M0, V0)]
+    work = [t.clone() for t in init]
+    d_st = torch.zeros(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def launch():
+        for t, t0 in zip(work, init):
+            t.copy_(t0)
+        rc = lib.tb_em_fit_2d(d_img.data_ptr(), n, EM_SIDE, EM_SIDE, None, work[0].data_ptr(),
+                              work[1].data_ptr(), work[2].data_ptr(), K, 0., EM_STEPS,
+                              d_st.data_ptr(), stream.cuda_stream)
+        assert rc == 0
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(args.steps):
+        flush.fill_(1.)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        launch()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+    kern_s = float(np.median(ts))
+    fails = int(d_st.sum().item())
+    value = n / kern_s
+    # end to end: host stamps and initial mixtures in, fitted mixtures out
+    emfit.em_fit_2d_batch(imgs[:64], A0[:64], M0[:64], V0[:64], 0., EM_STEPS)
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        emfit.em_fit_2d_batch(imgs, A0, M0, V0, 0., EM_STEPS)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e_t))
+    units = float(n) * EM_SIDE * EM_SIDE * K * EM_STEPS
+    flops_per_unit = 30   # dx, dy, dsq (10), scale x exp, sum, z / zsum, w, 6 moments (11)
+    achieved = units * flops_per_unit / kern_s / 1e12
+    cpu = None
+    if cpu_seconds:
+        try:
+            from oracle import refharness
+            ref = refharness._emfit_module()
+            kind, fit = 'reference', ref.em_fit_2d_reg
+        except Exception:
+            from oracle import oracle as O
+            kind, fit = 'port', O.em_fit_2d_reg
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < cpu_seconds and done < n:
+            a, m_, v = A0[done].copy(), M0[done].copy(), V0[done].copy()
+            fit(imgs[done], -(EM_SIDE // 2), -(EM_SIDE // 2), a, m_, v, 0., EM_STEPS)
+            done += 1
+        cpu = {'value': done / (time.perf_counter() - t0), 'unit': 'stamps/s', 'cores': 1,
+               'kind': kind,
+               'sample': '%d of the %d stamps, em_fit_2d_reg one after another, %.0f s budget'
+                         % (done, n, cpu_seconds)}
+    return {'workload': '%d PSF stamps of %dx%d px, %d-Gaussian EM fit, %d iterations '
+                        '(GaussianMixturePSF.fromStamp / em_fit_2d_reg), FP64'
+                        % (n, EM_SIDE, EM_SIDE, K, EM_STEPS),
+            'metric': 'PSF stamps fitted/s', 'value': value, 'unit': 'stamps/s',
+            'ms_per_step': kern_s * 1e3, 'failed_fits': fails,
+            'e2e': {'value': n / e2e_s, 'unit': 'stamps/s',
+                    'h2d_bytes_per_step': int(imgs.nbytes + A0.nbytes + M0.nbytes + V0.nbytes),
+                    'd2h_bytes_per_step': int(A0.nbytes + M0.nbytes + V0.nbytes + 4 * n)},
+            'gpu_launches_per_step': 1,
+            'roofline': {'bound': 'fp64', 'kernel': 'tb_em_fit_2d',
+                         'achieved': achieved, 'peak': FP64_NOMINAL_TFLOPS, 'unit': 'TFLOP/s',
+                         'frac': achieved / FP64_NOMINAL_TFLOPS,
+                         'peak_basis': 'nominal B200 FP64 (no measured FP64 peak on this pool)',
+                         'algorithmic': '%.3g pixel x component x iterations x %d FP64 flops '
+                                        '(exp not counted)' % (units, flops_per_unit),
+                         'traffic': None,
+                         'note': 'latency-bound: three block barriers per iteration over 625 '
+                                 'pixels per stamp'},
+            'cpu_baseline': cpu}
+
+
 def measured_hbm_peak():
     """The pool's measured copy bandwidth (GB/s) and where it came from."""
     p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
@@ -978,7 +1097,8 @@ def main():
                              bench_fit(args, dev, flush, clk, cpu_s),
                              bench_normal_equations(args, dev, flush, clk,
                                                     cpu_s and min(cpu_s, 4.0)),
-                             bench_plain_small(args, dev)]
+                             bench_plain_small(args, dev),
+                             bench_emfit(args, dev, flush, clk, cpu_s and min(cpu_s, 4.0))]
     line['plain_fp64'] = fourier_plain_fp64(srcs, out, dev, budget=3.0)
     if line['plain_fp64']['value']:
         line['speedup_vs_plain_fp64'] = value / line['plain_fp64']['value']
