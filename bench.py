@@ -817,9 +817,9 @@ def bench_emfit(args, dev, flush, clk, cpu_seconds):
                          'peak_basis': 'nominal B200 FP64 (no measured FP64 peak on this pool)',
                          'algorithmic': '%.3g pixel x component x iterations x %d FP64 flops '
                                         '(exp not counted)' % (units, flops_per_unit),
-                         'traffic': None,
-                         'note': 'latency-bound: three block barriers per iteration over 625 '
-                                 'pixels per stamp'},
+                         'traffic': ncu_traffic('emfit_psf_stamps.json'),
+                         'note': 'FP64-pipe and dependency-latency bound (FP64 exp per pixel x '
+                                 'component); the stamps stay on chip'},
             'cpu_baseline': cpu}
 
 

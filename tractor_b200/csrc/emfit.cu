@@ -7,8 +7,9 @@
 //   * per component: C^-1 and amp / (2 pi sqrt det C) (a non-positive
 //     determinant stops the fit, as the reference returns -1 there);
 //   * E step: the responsibility of component k at pixel (x, y) is
-//     z_k / sum_j z_j with z_k = scale_k exp(-dsq_k / 2), 0 for dsq >= 100
-//     (z itself where the sum is 0, as the reference leaves it);
+//     z_k / sum_j z_j (as z_k times the sum's reciprocal) with
+//     z_k = scale_k exp(-dsq_k / 2), 0 for dsq >= 100 (z itself where the
+//     sum is 0, as the reference leaves it);
 //   * M step from the weighted moments w = img z_k / sum z (sum w, sum w x,
 //     sum w y, sum w x^2, sum w x y, sum w y^2), summed per thread over a
 //     fixed pixel stride and then over the block in a fixed order (every
@@ -46,6 +47,8 @@ em_fit_kernel(const double* __restrict__ img, int n, int ny, int nx,
     const int x0 = xy0 ? xy0[2 * s] : -(nx / 2);
     const int y0 = xy0 ? xy0[2 * s + 1] : -(ny / 2);
     const int npix = nx * ny;
+    const int ix0 = tid % nx, iy0 = tid / nx;                       // this thread's first pixel
+    const int step_x = kEmThreads % nx, step_y = kEmThreads / nx;   // and its stride
     const double tpd = 4.0 * TB_PI * TB_PI;   // (2 pi)^D, D = 2
     if (tid < K) {
         w_s[tid] = A[tid];
@@ -72,9 +75,16 @@ em_fit_kernel(const double* __restrict__ img, int n, int ny, int nx,
         double acc[kM];
 #pragma unroll
         for (int v = 0; v < kM; v++) acc[v] = 0.0;
+        // pixel i = tid + kEmThreads j at (ix, iy), advanced without a division
+        int ix = ix0, iy = iy0;
         for (int i = tid; i < npix; i += kEmThreads) {
-            const int iy = i / nx, ix = i - iy * nx;
             const double x = (double)(x0 + ix), y = (double)(y0 + iy);
+            ix += step_x;
+            iy += step_y;
+            if (ix >= nx) {
+                ix -= nx;
+                iy++;
+            }
             double z[K];
             double zsum = 0.0;
 #pragma unroll
@@ -86,12 +96,13 @@ em_fit_kernel(const double* __restrict__ img, int n, int ny, int nx,
                 zsum += z[k];
             }
             // a pixel whose z sum to 0 keeps them unnormalised (all 0 unless
-            // some amplitude is negative), as the reference does
-            const bool norm = zsum != 0.0;
+            // some amplitude is negative), as the reference does; one
+            // reciprocal per pixel instead of a division per component
+            const double rz = zsum != 0.0 ? 1.0 / zsum : 1.0;
             const double d = im[i];
 #pragma unroll
             for (int k = 0; k < K; k++) {
-                const double wi = d * (norm ? z[k] / zsum : z[k]);
+                const double wi = d * (z[k] * rz);
                 acc[6 * k + 0] += wi;
                 acc[6 * k + 1] += wi * x;
                 acc[6 * k + 2] += wi * y;
