@@ -597,6 +597,29 @@ int tb_em_fit_2d(const double* img, int32_t n, int32_t ny, int32_t nx, const int
                  double* amp, double* mean, double* var, int32_t K, double alpha,
                  int32_t steps, int32_t* status, void* stream);
 
+/* Blob segmentation for callers that cut images into blobs before
+ * Tractor.setModelMasks / the batched fitter (the callers of
+ * tractor/engine.py:341-361).  tb_label_components labels the connected
+ * components of mask (H x W bytes, nonzero = foreground, row-major) with
+ * 4-connectivity (conn8 = 0, scipy.ndimage.label's default structure) or
+ * 8-connectivity (conn8 = 1): labels (H x W int32) receives 0 for
+ * background and 1..n for the components, numbered in the raster order of
+ * each component's first pixel (scipy.ndimage.label's numbering); *n_labels
+ * (device int32) receives n.  workspace: tb_label_workspace_bytes(H, W)
+ * bytes of device memory, 16-byte aligned.  *error (device int32) is set to
+ * 1 if a merge ran out of its retry bound (never expected).  H * W <= 2^30.
+ * Every pointer is device memory. */
+int64_t tb_label_workspace_bytes(int32_t H, int32_t W);
+int tb_label_components(const uint8_t* mask, int32_t H, int32_t W, int32_t conn8,
+                        int32_t* labels, int32_t* n_labels, void* workspace, int32_t* error,
+                        void* stream);
+
+/* Bounding boxes of labels 1..n_labels (scipy.ndimage.find_objects):
+ * boxes[4(l-1) ..] = y0, x0, y1, x1 (y1, x1 exclusive); a label with no
+ * pixel keeps (H, W, 0, 0). */
+int tb_component_boxes(const int32_t* labels, int32_t H, int32_t W, int32_t n_labels,
+                       int32_t* boxes, void* stream);
+
 /* Library version string (host memory, static). */
 const char* tb_version(void);
 

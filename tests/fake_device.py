@@ -198,8 +198,24 @@ def install(monkeypatch):
             st[i] = O.em_fit_2d_reg(imgs[i], x0, y0, amp[i], mean[i], var[i], alpha, steps) != 0
         return amp, mean, var, st
 
-    from tractor_b200 import emfit
+    def label_run(mask, conn8):
+        import scipy.ndimage as ndi
+        st = np.ones((3, 3), bool) if conn8 else None
+        lab, n = ndi.label(np.asarray(mask) != 0, structure=st)
+        return lab.astype(np.int32), int(n)
+
+    def boxes_run(labels, n):
+        import scipy.ndimage as ndi
+        out = np.tile(np.array([labels.shape[0], labels.shape[1], 0, 0], np.int32), (n, 1))
+        for l, sl in enumerate(ndi.find_objects(labels, n)):
+            if sl is not None:
+                out[l] = (sl[0].start, sl[1].start, sl[0].stop, sl[1].stop)
+        return out
+
+    from tractor_b200 import emfit, blobs
     monkeypatch.setattr(emfit, '_run', em_run)
+    monkeypatch.setattr(blobs, '_run_label', label_run)
+    monkeypatch.setattr(blobs, '_run_boxes', boxes_run)
     monkeypatch.setattr(render.MogBatch, 'run', mog_run)
     monkeypatch.setattr(render.FftBatch, 'run', fft_run)
     monkeypatch.setattr(render.PsfSpectra, 'get', spectra_get)

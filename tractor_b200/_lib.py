@@ -109,6 +109,9 @@ SIGNATURES = {
     'tb_normal_equations': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _I32, _P]),
     'tb_tensor_core_timeouts': (_I32, [_P]),
     'tb_em_fit_2d': (_I32, [_P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _D, _I32, _P, _P]),
+    'tb_label_workspace_bytes': (ctypes.c_int64, [_I32, _I32]),
+    'tb_label_components': (_I32, [_P, _I32, _I32, _I32, _P, _P, _P, _P, _P]),
+    'tb_component_boxes': (_I32, [_P, _I32, _I32, _I32, _P, _P]),
     'tb_solve_update': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P, _P]),
     'tb_solve_update_noalloc': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _I32, _P]),
     'tb_chi2': (_I32, [_P, _P, _P, _P, _P, _I32, _P, _P]),
@@ -136,7 +139,8 @@ _lib = None
 def header_symbols():
     """Entry points declared in include/tractor_b200.h."""
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r'^\s*(?:int|const char\*)\s+(tb_\w+)\s*\(', txt, re.M)))
+    return sorted(set(re.findall(r'^\s*(?:int64_t|int|const char\*)\s+(tb_\w+)\s*\(', txt,
+                                 re.M)))
 
 
 def load():
