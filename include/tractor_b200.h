@@ -533,11 +533,13 @@ int tb_fit_reset(tb_fit_state* state, int32_t n_blobs, double lambda0, void* str
  * galaxy.py:659-669) by FP64 central differences, and from them every
  * band's PSF-convolved components (mixture_profiles.py:158-172) with their
  * derivative coefficients.  cd_inv: the WCS cdInverse, 4 doubles in HOST
- * memory (one WCS for every blob). */
+ * memory (one WCS for every blob).  state (optional, n_blobs entries):
+ * sources of blobs whose status is not 0 (converged or stopped) are left
+ * as they are -- the pass and the step skip those blobs. */
 int tb_fit_prep(const tb_fit_source* srcs, int32_t n_src, const double* params,
                 int32_t n_bands, const tb_fit_unit* units, int32_t n_units,
                 const double* cd_inv, const tb_profile_tables* tables, void* workspace,
-                void* stream);
+                const tb_fit_state* state, void* stream);
 
 /* mode 0: for every unit of a running blob, over its range of the tiles its
  * sources' masks reach: the model (each source's PSF-convolved mixture on

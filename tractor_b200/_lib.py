@@ -123,7 +123,7 @@ SIGNATURES = {
     'tb_scene_workspace': (_I32, [_I64, _I64, _P]),
     'tb_fit_workspace': (_I32, [_I32, _I32, _P]),
     'tb_fit_reset': (_I32, [_P, _I32, _D, _P]),
-    'tb_fit_prep': (_I32, [_P, _I32, _P, _I32, _P, _I32, _P, _P, _P, _P]),
+    'tb_fit_prep': (_I32, [_P, _I32, _P, _I32, _P, _I32, _P, _P, _P, _P, _P]),
     'tb_fit_pass': (_I32, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32,
                            _I32, _P, _P, _P]),
     'tb_fit_step': (_I32, [_P, _I32, _I32, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _P]),

@@ -96,13 +96,18 @@ __global__ void __launch_bounds__(kPrepThreads)
 fit_prep_kernel(const tb_fit_source* __restrict__ srcs, int n, const double* __restrict__ params,
                 int n_bands, const tb_fit_unit* __restrict__ units, int n_units,
                 tb_profile_tables Tg, double cd0, double cd1, double cd2, double cd3,
-                SrcTab* __restrict__ tab, FitC* __restrict__ comps) {
+                SrcTab* __restrict__ tab, FitC* __restrict__ comps,
+                const tb_fit_state* __restrict__ state) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const tb_profile_tables T = tb::stage_tables(Tg, smem_raw);
     const int lane = threadIdx.x & 31;
     const int i = blockIdx.x * (kPrepThreads / 32) + (threadIdx.x >> 5);
     if (i >= n) return;
     const tb_fit_source s = srcs[i];
+    // a converged or stopped blob's tables stay as they are (nothing reads them)
+    if (state && s.blob >= 0 && (int64_t)(s.blob + 1) * n_bands <= n_units &&
+        state[s.blob].status != 0)
+        return;
     const double* p = params + (int64_t)i * TB_FIT_NPAR;
     const double cd[4] = {cd0, cd1, cd2, cd3};
     int ok = s.blob >= 0 && (int64_t)(s.blob + 1) * n_bands <= n_units;
@@ -1058,7 +1063,7 @@ extern "C" int tb_fit_reset(tb_fit_state* state, int32_t n_blobs, double lambda0
 extern "C" int tb_fit_prep(const tb_fit_source* srcs, int32_t n_src, const double* params,
                            int32_t n_bands, const tb_fit_unit* units, int32_t n_units,
                            const double* cd_inv, const tb_profile_tables* tables, void* workspace,
-                           void* stream) {
+                           const tb_fit_state* state, void* stream) {
     if (n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS || n_units < 0) return TB_ERR_ARG;
     if (n_src == 0) return TB_OK;
     if (!srcs || !params || !units || !cd_inv || !tables || !workspace) return TB_ERR_ARG;
@@ -1072,7 +1077,8 @@ extern "C" int tb_fit_prep(const tb_fit_source* srcs, int32_t n_src, const doubl
     fit_prep_kernel<<<(n_src + per_block - 1) / per_block, kPrepThreads, smem,
                       (cudaStream_t)stream>>>(srcs, n_src, params, n_bands, units, n_units,
                                               *tables, cd_inv[0], cd_inv[1], cd_inv[2], cd_inv[3],
-                                              ws_tab(workspace), ws_comps(workspace, n_src));
+                                              ws_tab(workspace), ws_comps(workspace, n_src),
+                                              state);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 

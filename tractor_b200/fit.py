@@ -151,7 +151,8 @@ class BlobFitter(object):
         _lib.check(lib.tb_fit_prep(self.d_sources.data_ptr(), self.n_src, self.trial.data_ptr(),
                                    self.n_bands, self.d_units.data_ptr(), len(self.units_np),
                                    self.cd_inv.ctypes.data, ctypes.addressof(self.tables.struct),
-                                   self.workspace.data_ptr(), _lib.stream_ptr()), 'tb_fit_prep')
+                                   self.workspace.data_ptr(), self.state.data_ptr(),
+                                   _lib.stream_ptr()), 'tb_fit_prep')
 
     def _pass(self, mode):
         lib = _lib.load()
