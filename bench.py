@@ -23,8 +23,9 @@ tile height autotuned), batched blob fitting (2,000 blobs x 3 bands) and the
 dense normal equations on the tensor cores (512 problems x 63 parameters x
 16,384 rows), each with its own end-to-end number, roofline and CPU baseline,
 the small plain fit through the object API (latency-bound: us per render,
-ms per fit) and EM fits of 4,096 PSF stamps (GaussianMixturePSF.fromStamp's
-em_fit_2d_reg, FP64) (--no-secondary skips them).
+ms per fit), EM fits of 4,096 PSF stamps (GaussianMixturePSF.fromStamp's
+em_fit_2d_reg, FP64) and blob segmentation of a 4096x4096 detection map
+(--no-secondary skips them).
 
 --impl reference times the reference's CPU implementation of the same
 workload on the host cores (its own compiled C for the spectrum and the
@@ -823,6 +824,105 @@ def bench_emfit(args, dev, flush, clk, cpu_seconds):
             'cpu_baseline': cpu}
 
 
+# secondary workload: blob segmentation of a detection map
+SEG_SIDE = 4096
+
+
+def seg_map(seed=950):
+    """A seeded 4096 x 4096 detection map: white noise smoothed by a
+    Gaussian of sigma 4 px, thresholded at 0.02 (about 11k blobs, 40 % of
+    the pixels set), and 20,000 source positions drawn on it."""
+    import scipy.ndimage as ndi
+    rng = np.random.default_rng(seed)
+    f = ndi.gaussian_filter(rng.normal(size=(SEG_SIDE, SEG_SIDE)).astype(np.float32), 4)
+    pos = rng.uniform(0, SEG_SIDE - 1, (20000, 2))
+    return f > 0.02, pos
+
+
+def bench_segment(args, dev, flush, clk, cpu_seconds):
+    """Blob segmentation (tractor_b200.blobs): connected components of a
+    4096 x 4096 detection map with scipy.ndimage.label's numbering and their
+    boxes, device-resident launches timed with CUDA events; end to end
+    through blobs.segment from the host map (plus 20,000 source positions
+    assigned to blobs).  CPU baseline: scipy.ndimage.label + find_objects
+    (the tool the reference's callers use) on the same map, one core."""
+    import torch
+    import scipy.ndimage as ndi
+    from tractor_b200 import _lib, blobs
+    lib = _lib.load()
+    det, pos = seg_map()
+    H = W = SEG_SIDE
+    d_mask = torch.from_numpy(det.astype(np.uint8)).to(dev)
+    labels, n = blobs._label_device(d_mask, H, W, 0)
+    nbytes = int(lib.tb_label_workspace_bytes(H, W))
+    ws = torch.empty((nbytes + 15) // 16 * 4, dtype=torch.int32, device=dev)
+    scal = torch.zeros(2, dtype=torch.int32, device=dev)
+    boxes = torch.empty((n, 4), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def launch():
+        assert lib.tb_label_components(d_mask.data_ptr(), H, W, 0, labels.data_ptr(),
+                                       scal.data_ptr(), ws.data_ptr(), scal.data_ptr() + 4,
+                                       stream.cuda_stream) == 0
+        assert lib.tb_component_boxes(labels.data_ptr(), H, W, n, boxes.data_ptr(),
+                                      stream.cuda_stream) == 0
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(args.steps):
+        flush.fill_(1.)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        launch()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+    kern_s = float(np.median(ts))
+    assert int(scal[0].item()) == n and int(scal[1].item()) == 0
+    blobs.segment(det[:256, :256])
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        seg = blobs.segment(det, pos)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e_t))
+    assert seg.n == n
+    cpu = None
+    if cpu_seconds:
+        t0 = time.perf_counter()
+        reps = 0
+        while reps == 0 or time.perf_counter() - t0 < min(cpu_seconds, 2.0):
+            ref, nr = ndi.label(det)
+            ndi.find_objects(ref)
+            reps += 1
+        cpu_s = (time.perf_counter() - t0) / reps
+        assert nr == n
+        cpu = {'value': H * W / cpu_s / 1e6, 'unit': 'Mpix/s', 'cores': 1, 'kind': 'port',
+               'sample': 'the whole map, scipy.ndimage.label + find_objects (the checker of the '
+                         'tests), %d runs' % reps}
+    peak, basis = measured_hbm_peak()
+    alg_bytes = H * W * (1 + 4)
+    achieved = alg_bytes / kern_s / 1e9
+    return {'workload': '4096x4096 detection map (smoothed noise > 0.02, %d blobs), 4-connected '
+                        'components with scipy.ndimage.label numbering + bounding boxes' % n,
+            'metric': 'Mpix/s segmented (blob labelling + boxes)',
+            'value': H * W / kern_s / 1e6, 'unit': 'Mpix/s', 'ms_per_step': kern_s * 1e3,
+            'n_blobs': n,
+            'e2e': {'value': H * W / e2e_s / 1e6, 'unit': 'Mpix/s',
+                    'h2d_bytes_per_step': int(H * W), 'd2h_bytes_per_step': int(H * W * 4 + n * 16)},
+            'gpu_launches_per_step': 9,
+            'roofline': {'bound': 'hbm', 'kernel': 'tb_label_components + tb_component_boxes',
+                         'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'peak_basis': basis,
+                         'algorithmic': '1 byte read + 4 bytes written per pixel',
+                         'traffic': None,
+                         'note': 'latency / atomics bound: union-find merges chase parent '
+                                 'chains; 9 launches per step'},
+            'cpu_baseline': cpu}
+
+
 def measured_hbm_peak():
     """The pool's measured copy bandwidth (GB/s) and where it came from."""
     p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
@@ -1098,7 +1198,8 @@ def main():
                              bench_normal_equations(args, dev, flush, clk,
                                                     cpu_s and min(cpu_s, 4.0)),
                              bench_plain_small(args, dev),
-                             bench_emfit(args, dev, flush, clk, cpu_s and min(cpu_s, 4.0))]
+                             bench_emfit(args, dev, flush, clk, cpu_s and min(cpu_s, 4.0)),
+                             bench_segment(args, dev, flush, clk, cpu_s)]
     line['plain_fp64'] = fourier_plain_fp64(srcs, out, dev, budget=3.0)
     if line['plain_fp64']['value']:
         line['speedup_vs_plain_fp64'] = value / line['plain_fp64']['value']

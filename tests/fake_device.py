@@ -216,6 +216,11 @@ def install(monkeypatch):
     monkeypatch.setattr(emfit, '_run', em_run)
     monkeypatch.setattr(blobs, '_run_label', label_run)
     monkeypatch.setattr(blobs, '_run_boxes', boxes_run)
+
+    def segment_run(mask, conn8):
+        lab, n = label_run(mask, conn8)
+        return lab, n, boxes_run(lab, n)
+    monkeypatch.setattr(blobs, '_run_segment', segment_run)
     monkeypatch.setattr(render.MogBatch, 'run', mog_run)
     monkeypatch.setattr(render.FftBatch, 'run', fft_run)
     monkeypatch.setattr(render.PsfSpectra, 'get', spectra_get)

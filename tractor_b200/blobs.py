@@ -59,10 +59,11 @@ def _boxes_device(labels, n):
 
 
 def _mask_tensor(mask):
-    m = np.ascontiguousarray(np.asarray(mask) != 0, np.uint8)
+    m = np.asarray(mask)
     if m.ndim != 2:
         raise ValueError('2-D mask expected')
-    return torch.from_numpy(m).to(render.device()), m.shape
+    m8 = m.view(np.uint8) if m.dtype == np.bool_ else (m != 0).view(np.uint8)
+    return torch.from_numpy(np.ascontiguousarray(m8)).to(render.device()), m.shape
 
 
 def _run_label(mask, conn8):
@@ -70,6 +71,15 @@ def _run_label(mask, conn8):
     d, (H, W) = _mask_tensor(mask)
     labels, n = _label_device(d, H, W, conn8)
     return labels.cpu().numpy(), n
+
+
+def _run_segment(mask, conn8):
+    """Host mask -> (labels numpy int32, n, boxes numpy (n, 4)): labels and
+    boxes computed on the device, one copy of each back."""
+    d, (H, W) = _mask_tensor(mask)
+    labels, n = _label_device(d, H, W, conn8)
+    boxes = _boxes_device(labels, n)
+    return labels.cpu().numpy(), n, boxes.cpu().numpy()
 
 
 def _run_boxes(labels, n):
@@ -109,7 +119,11 @@ class Segmentation(object):
 
     def __init__(self, labels, n, slices, blob_of):
         self.labels, self.n, self.slices, self.blob_of = labels, n, slices, blob_of
-        self.sources = [np.flatnonzero(blob_of == b) for b in range(n)]
+        # group by blob with one stable sort (source order kept within a blob)
+        order = np.argsort(blob_of, kind='stable')
+        counts = np.bincount(blob_of[blob_of >= 0], minlength=n) if n else np.zeros(0, int)
+        start = int(np.count_nonzero(blob_of < 0))
+        self.sources = np.split(order[start:], np.cumsum(counts)[:-1]) if n else []
 
 
 def segment(detmap, positions=None, structure=None):
@@ -117,8 +131,9 @@ def segment(detmap, positions=None, structure=None):
     (`find_objects`) and assigns each source position (x, y), rounded to
     its pixel, to the blob under it (-1 outside the map or on background).
     Returns a Segmentation."""
-    labels, n = label(detmap, structure)
-    slices = find_objects(labels, n)
+    labels, n, boxes = _run_segment(detmap, _conn8(structure))
+    slices = [None if y1 == 0 else (slice(int(y0), int(y1)), slice(int(x0), int(x1)))
+              for y0, x0, y1, x1 in boxes]
     H, W = labels.shape
     if positions is None:
         blob_of = np.zeros(0, np.int64)
