@@ -5,12 +5,17 @@
 // (callers of tractor/engine.py:341-361).
 //
 // Labelling is union-find over the pixel grid:
-//   1. every foreground pixel is its own set (parent = its raster index);
-//   2. every foreground pixel merges with its foreground neighbours above and
-//      to the left (and the two upper diagonals with 8-connectivity); a merge
-//      links the larger root under the smaller with atomicMin, retrying when
-//      another thread moved the root first, so every set's root is its
-//      smallest raster index;
+//   1. per 32 x 32 tile, in shared memory: every foreground pixel merges with
+//      its foreground neighbours above and to the left (and the two upper
+//      diagonals with 8-connectivity) inside the tile; a merge links the
+//      larger root under the smaller with atomicMin, retrying when another
+//      thread moved the root first, so every set's root is its smallest
+//      index -- in row-major tile order, the same order as the raster order
+//      -- and each pixel's global parent becomes its tile-local root;
+//   2. pixels on a tile's top / left edge (and right edge, for the
+//      8-connected upper-right diagonal) merge with their neighbours across
+//      the edge in global memory by the same rule, so every set's root is
+//      its smallest raster index;
 //   3. every pixel's parent is replaced by its root;
 //   4. roots are counted per block, the block counts scanned by one CTA, and
 //      each root numbered 1 + (roots before it in raster order) -- the order
@@ -53,28 +58,107 @@ __device__ __forceinline__ bool unite(int32_t* parent, int a, int b, int bound) 
     return false;
 }
 
-__global__ void ccl_init(const uint8_t* __restrict__ mask, int64_t n, int32_t* __restrict__ parent) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x)
-        parent[i] = mask[i] ? (int32_t)i : -1;
+constexpr int kTile = 32;   // tile side of the shared-memory pass
+
+__device__ __forceinline__ int find_local(volatile int* lp, int x) {
+    int p = lp[x];
+    while (p != x) {
+        x = p;
+        p = lp[x];
+    }
+    return x;
 }
 
-__global__ void ccl_merge(const uint8_t* __restrict__ mask, int H, int W, int conn8,
+__device__ __forceinline__ bool unite_local(int* lp, int a, int b, int bound) {
+    for (int it = 0; it < bound; it++) {
+        a = find_local(lp, a);
+        b = find_local(lp, b);
+        if (a == b) return true;
+        if (a > b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        const int old = atomicMin(lp + b, a);
+        if (old == b) return true;
+        b = old;
+    }
+    return false;
+}
+
+// One CTA per 32 x 32 tile (kThreads threads, 4 rows each): the tile's
+// components in shared memory, then every pixel's global parent = the global
+// index of its tile-local root (-1 for background).
+__global__ void __launch_bounds__(kThreads)
+ccl_local(const uint8_t* __restrict__ mask, int H, int W, int conn8, int tiles_x,
+          int32_t* __restrict__ parent, int* err) {
+    __shared__ int lp[kTile * kTile];
+    const int tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
+    const int lx = threadIdx.x % kTile, ly0 = threadIdx.x / kTile;
+    constexpr int kRows = kTile * kTile / kThreads;
+    const int gx = tx * kTile + lx;
+#pragma unroll
+    for (int k = 0; k < kRows; k++) {
+        const int ly = ly0 + k * (kThreads / kTile), gy = ty * kTile + ly;
+        const int l = ly * kTile + lx;
+        lp[l] = (gx < W && gy < H && mask[(int64_t)gy * W + gx]) ? l : -1;
+    }
+    __syncthreads();
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < kRows; k++) {
+        const int ly = ly0 + k * (kThreads / kTile);
+        const int l = ly * kTile + lx;
+        if (lp[l] < 0) continue;
+        if (lx > 0 && lp[l - 1] >= 0) ok &= unite_local(lp, l, l - 1, 1 << 20);
+        if (ly > 0) {
+            const int u = l - kTile;
+            if (lp[u] >= 0) ok &= unite_local(lp, l, u, 1 << 20);
+            if (conn8) {
+                if (lx > 0 && lp[u - 1] >= 0) ok &= unite_local(lp, l, u - 1, 1 << 20);
+                if (lx + 1 < kTile && lp[u + 1] >= 0) ok &= unite_local(lp, l, u + 1, 1 << 20);
+            }
+        }
+    }
+    if (!ok) atomicExch(err, 1);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kRows; k++) {
+        const int ly = ly0 + k * (kThreads / kTile), gy = ty * kTile + ly;
+        if (gx >= W || gy >= H) continue;
+        const int l = ly * kTile + lx;
+        int32_t g = -1;
+        if (lp[l] >= 0) {
+            const int r = find_local(lp, l);
+            g = (ty * kTile + r / kTile) * W + tx * kTile + r % kTile;
+        }
+        parent[(int64_t)gy * W + gx] = g;
+    }
+}
+
+// Merges across tile edges in global memory (pairs inside a tile were
+// merged by ccl_local).
+__global__ void ccl_edges(const uint8_t* __restrict__ mask, int H, int W, int conn8,
                           int32_t* parent, int* err) {
     const int64_t n = (int64_t)H * W;
     const int bound = 1 << 26;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        if (!mask[i]) continue;
         const int y = (int)(i / W), x = (int)(i - (int64_t)y * W);
+        const int lx = x % kTile, ly = y % kTile;
+        const bool left = lx == 0, top = ly == 0, right = lx == kTile - 1;
+        if (!(left || top || (conn8 && right))) continue;
+        if (!mask[i]) continue;
         bool ok = true;
-        if (x > 0 && mask[i - 1]) ok &= unite(parent, (int)i, (int)(i - 1), bound);
+        if (left && x > 0 && mask[i - 1]) ok &= unite(parent, (int)i, (int)(i - 1), bound);
         if (y > 0) {
             const int64_t u = i - W;
-            if (mask[u]) ok &= unite(parent, (int)i, (int)u, bound);
+            if (top && mask[u]) ok &= unite(parent, (int)i, (int)u, bound);
             if (conn8) {
-                if (x > 0 && mask[u - 1]) ok &= unite(parent, (int)i, (int)(u - 1), bound);
-                if (x + 1 < W && mask[u + 1]) ok &= unite(parent, (int)i, (int)(u + 1), bound);
+                if ((left || top) && x > 0 && mask[u - 1])
+                    ok &= unite(parent, (int)i, (int)(u - 1), bound);
+                if ((right || top) && x + 1 < W && mask[u + 1])
+                    ok &= unite(parent, (int)i, (int)(u + 1), bound);
             }
         }
         if (!ok) atomicExch(err, 1);
@@ -201,8 +285,11 @@ extern "C" int tb_label_components(const uint8_t* mask, int32_t H, int32_t W, in
     int32_t* block_roots = parent + n;
     if (cudaMemsetAsync(error, 0, sizeof(int32_t), s) != cudaSuccess) return TB_ERR_LAUNCH;
     const int g = grid_for(n);
-    ccl_init<<<g, kThreads, 0, s>>>(mask, n, parent);
-    ccl_merge<<<g, kThreads, 0, s>>>(mask, H, W, conn8, parent, error);
+    const int tiles_x = (W + kTile - 1) / kTile, tiles_y = (H + kTile - 1) / kTile;
+    const int64_t ntiles = (int64_t)tiles_x * tiles_y;
+    if (ntiles > INT32_MAX) return TB_ERR_ARG;
+    ccl_local<<<(int)ntiles, kThreads, 0, s>>>(mask, H, W, conn8, tiles_x, parent, error);
+    ccl_edges<<<g, kThreads, 0, s>>>(mask, H, W, conn8, parent, error);
     ccl_flatten<<<g, kThreads, 0, s>>>(n, parent);
     ccl_count<<<nb, kThreads, 0, s>>>(n, parent, block_roots);
     ccl_scan<<<1, kScanThreads, 0, s>>>(nb, block_roots, n_labels);
