@@ -23,11 +23,11 @@
 
 namespace {
 
-constexpr int kEmThreads = 128;
+constexpr int kEmThreads = 64;
 constexpr int kWarps = kEmThreads / 32;
 
 template <int K>
-__global__ void __launch_bounds__(kEmThreads, 4)
+__global__ void __launch_bounds__(kEmThreads, 8)
 em_fit_kernel(const double* __restrict__ img, int n, int ny, int nx,
               const int32_t* __restrict__ xy0, double* __restrict__ amp,
               double* __restrict__ mean, double* __restrict__ var, double alpha, int steps,
