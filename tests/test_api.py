@@ -366,3 +366,26 @@ def test_em_fit_reports_degenerate_covariance(backend):
     var = np.array([[[1., 2.], [2., 1.]]])
     assert emfit.em_fit_2d_reg(st, -4, -4, w, mu, var, 0., 10) == -1
     assert w[0] == 1. and not mu.any() and var[0, 0, 1] == 2.
+
+
+def test_plan_renders_the_state_at_planning_time(backend):
+    """A RenderPlan renders the parameters as they were when a model was
+    planned, even if the PSF's arrays are changed in place and the sky is
+    changed before the plan runs (the batched line search and the image-
+    parameter forward differences plan several states into one batch)."""
+    import tractor_b200 as T
+    from tractor_b200.plan import RenderPlan
+    psf = T.GaussianMixturePSF(np.array([0.8, 0.2]), np.zeros((2, 2)),
+                               np.array([[[1.5, 0.], [0., 1.5]], [[6., 0.], [0., 6.]]]))
+    tim = T.Image(data=np.zeros((30, 30), np.float32), inverr=np.ones((30, 30), np.float32),
+                  psf=psf, sky=T.ConstantSky(1.5), photocal=T.LinearPhotoCal(1.))
+    tr = T.Tractor([tim], [T.PointSource(T.PixPos(14.2, 15.7), T.Flux(100.))])
+    want = tr.getModelImage(0)
+    plan = RenderPlan()
+    fin = tr._plan_model_image(plan, tim)
+    psf.mog.var[:] *= 2.        # in place, before the plan runs
+    psf.mog.amp[:] = [0.5, 0.5]
+    tim.sky.setParams([7.])
+    got = fin()
+    assert np.array_equal(got, want)
+    assert not np.array_equal(tr.getModelImage(0), want)
