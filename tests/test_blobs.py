@@ -113,3 +113,19 @@ def test_label_large_image_matches_scipy(tb):
     lab8, n8 = blobs.label(m, structure=FULL)
     ref8, nr8 = ndi.label(m, structure=FULL)
     assert n8 == nr8 and np.array_equal(lab8, ref8)
+
+
+def test_segment_connectivity_and_empty(backend):
+    """8-connectivity joins diagonal neighbours; an empty map has no blobs
+    and every source is off-blob."""
+    from tractor_b200 import blobs
+    det = np.zeros((9, 9), bool)
+    det[2, 2] = det[3, 3] = det[6, 6] = True
+    s4 = blobs.segment(det, [[2, 2], [3, 3]])
+    s8 = blobs.segment(det, [[2, 2], [3, 3]], structure=FULL)
+    assert s4.n == 3 and list(s4.blob_of) == [0, 1]
+    assert s8.n == 2 and list(s8.blob_of) == [0, 0]
+    assert [list(x) for x in s8.sources] == [[0, 1], []]
+    assert s8.slices[0] == (slice(2, 4), slice(2, 4))
+    e = blobs.segment(np.zeros((5, 7), bool), [[1., 1.], [-3., 2.]])
+    assert e.n == 0 and list(e.blob_of) == [-1, -1] and e.sources == [] and e.slices == []

@@ -113,17 +113,38 @@ def find_objects(input, max_label=0):
 
 class Segmentation(object):
     """Blobs of a detection map: `labels` (int32, 0 = background), `n`
-    blobs, `slices[b]` the bounding box of blob b + 1, `blob_of[i]` the blob
-    (0-based) under source i's pixel or -1, `sources[b]` the sources in blob
-    b (in source order)."""
+    blobs, `boxes` (n, 4: y0, x0, y1, x1 exclusive), `slices[b]` the
+    bounding box of blob b + 1 as (row slice, column slice), `blob_of[i]`
+    the blob (0-based) under source i's pixel or -1, `sources[b]` the
+    sources in blob b (in source order).  `slices` and `sources` are built
+    on first use."""
 
-    def __init__(self, labels, n, slices, blob_of):
-        self.labels, self.n, self.slices, self.blob_of = labels, n, slices, blob_of
-        # group by blob with one stable sort (source order kept within a blob)
-        order = np.argsort(blob_of, kind='stable')
-        counts = np.bincount(blob_of[blob_of >= 0], minlength=n) if n else np.zeros(0, int)
-        start = int(np.count_nonzero(blob_of < 0))
-        self.sources = np.split(order[start:], np.cumsum(counts)[:-1]) if n else []
+    def __init__(self, labels, n, boxes, blob_of):
+        self.labels, self.n, self.boxes, self.blob_of = labels, n, boxes, blob_of
+        self._slices = None
+        self._sources = None
+
+    @property
+    def slices(self):
+        if self._slices is None:
+            self._slices = [None if y1 == 0 else (slice(int(y0), int(y1)),
+                                                  slice(int(x0), int(x1)))
+                            for y0, x0, y1, x1 in self.boxes]
+        return self._slices
+
+    @property
+    def sources(self):
+        if self._sources is None:
+            # group by blob with one stable sort (source order kept in a blob)
+            bo, n = self.blob_of, self.n
+            if n == 0:
+                self._sources = []
+            else:
+                order = np.argsort(bo, kind='stable')
+                counts = np.bincount(bo[bo >= 0], minlength=n)
+                start = int(np.count_nonzero(bo < 0))
+                self._sources = np.split(order[start:], np.cumsum(counts)[:-1])
+        return self._sources
 
 
 def segment(detmap, positions=None, structure=None):
@@ -132,8 +153,6 @@ def segment(detmap, positions=None, structure=None):
     its pixel, to the blob under it (-1 outside the map or on background).
     Returns a Segmentation."""
     labels, n, boxes = _run_segment(detmap, _conn8(structure))
-    slices = [None if y1 == 0 else (slice(int(y0), int(y1)), slice(int(x0), int(x1)))
-              for y0, x0, y1, x1 in boxes]
     H, W = labels.shape
     if positions is None:
         blob_of = np.zeros(0, np.int64)
@@ -144,7 +163,7 @@ def segment(detmap, positions=None, structure=None):
         inside = (ix >= 0) & (ix < W) & (iy >= 0) & (iy < H)
         blob_of = np.full(len(xy), -1, np.int64)
         blob_of[inside] = labels[iy[inside], ix[inside]].astype(np.int64) - 1
-    return Segmentation(labels, n, slices, blob_of)
+    return Segmentation(labels, n, boxes, blob_of)
 
 
 def blob_model_masks(tractor, seg, sources=None):
@@ -160,6 +179,6 @@ def blob_model_masks(tractor, seg, sources=None):
     for src, b in zip(srcs, seg.blob_of):
         if b < 0:
             continue
-        sy, sx = seg.slices[b]
-        d[src] = ModelMask(sx.start, sy.start, sx.stop - sx.start, sy.stop - sy.start)
+        y0, x0, y1, x1 = (int(v) for v in seg.boxes[b])
+        d[src] = ModelMask(x0, y0, x1 - x0, y1 - y0)
     return [dict(d) for _ in tractor.getImages()]
