@@ -455,6 +455,15 @@ def emfit():
         arrays['amp%d' % i] = psf.mog.amp
         arrays['mean%d' % i] = psf.mog.mean
         arrays['var%d' % i] = psf.mog.var
+    # HybridPixelizedPSF without its Gaussian approximation fits one to the
+    # pixelized model's image (psf.py:606-618)
+    from tractor.psf import HybridPixelizedPSF, PixelizedPSF
+    hstamp = moffat(33, 4.5, 2.8)
+    hyb = HybridPixelizedPSF(PixelizedPSF(hstamp), N=2)
+    arrays['hyb_stamp'] = hstamp
+    arrays['hyb_amp'] = hyb.gauss.mog.amp
+    arrays['hyb_mean'] = hyb.gauss.mog.mean
+    arrays['hyb_var'] = hyb.gauss.mog.var
     np.savez_compressed(os.path.join(OUT, 'emfit.npz'), n=len(cases), **arrays)
     print('emfit fixture written to', OUT)
 

@@ -389,3 +389,15 @@ def test_plan_renders_the_state_at_planning_time(backend):
     got = fin()
     assert np.array_equal(got, want)
     assert not np.array_equal(tr.getModelImage(0), want)
+
+
+def test_hybrid_psf_fits_its_gaussian_approximation(backend):
+    """HybridPixelizedPSF(pix) without `gauss` fits an N-component mixture to
+    the pixelized model's image by EM (psf.py:606-618), as the reference's
+    (emfit.npz)."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'emfit.npz'))
+    hyb = T.HybridPixelizedPSF(T.PixelizedPSF(g['hyb_stamp']), N=2)
+    np.testing.assert_allclose(hyb.gauss.mog.amp, g['hyb_amp'], rtol=1e-9, atol=1e-13)
+    np.testing.assert_allclose(hyb.gauss.mog.mean, g['hyb_mean'], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(hyb.gauss.mog.var, g['hyb_var'], rtol=1e-9, atol=1e-12)

@@ -642,14 +642,14 @@ class HybridPixelizedPSF(HybridPSF):
     components that are wide for the FFT box, which are rendered in pixel
     space through the mixture `gauss` (with a linear ramp between the two,
     ProfileGalaxy's hybrid split).  Every other attribute is the pixelized
-    model's.  `gauss` must be given: fitting it to the PSF stamp
-    (GaussianMixturePSF.fromStamp, an EM fit) is not provided."""
+    model's.  Without `gauss`, an N-component GaussianMixturePSF is fit to
+    the pixelized model's image at (cx, cy) by GaussianMixturePSF.fromStamp
+    (the EM fit, on the GPU), as the reference does."""
 
     def __init__(self, pix, gauss=None, N=2, cx=0., cy=0.):
         object.__setattr__(self, 'pix', pix)
         if gauss is None:
-            raise NotImplementedError('HybridPixelizedPSF needs its Gaussian approximation '
-                                      '`gauss` (fitting it to the stamp is not provided)')
+            gauss = GaussianMixturePSF.fromStamp(pix.getImage(cx, cy), N=N)
         object.__setattr__(self, 'gauss', gauss)
 
     def __str__(self):
