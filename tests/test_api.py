@@ -168,7 +168,7 @@ def test_pixelized_psfex_matches_reference(backend):
     from tractor_b200.psfex import PsfExModel, PixelizedPsfEx
     g = np.load(os.path.join(GOLDEN, 'psfex.npz'))
     deg, x0m, y0m, xs, ys = g['poly']
-    model = PsfExModel(g['bases'], degree=int(deg), x0=x0m, y0=y0m, xscale=xs, yscale=ys,
+    model = PsfExModel(bases=g['bases'], degree=int(deg), x0=x0m, y0=y0m, xscale=xs, yscale=ys,
                        fwhm=4.0)
     psf = PixelizedPsfEx(psfex=model)
     hyb = T.HybridPixelizedPSF(PixelizedPsfEx(psfex=model.copy()),
