@@ -12,6 +12,7 @@ root in the development container:
     python tests/golden/make_golden.py psfex    # psfex.npz
     python tests/golden/make_golden.py emfit    # emfit.npz
     python tests/golden/make_golden.py psfderiv # psf_derivs.npz
+    python tests/golden/make_golden.py forcedsky # forced_sky.npz
 """
 import os
 import sys
@@ -529,6 +530,85 @@ def psfderiv():
     print('psf_derivs fixture written to', OUT)
 
 
+def forced_scene(T, rng, sky_true=None):
+    """Six sources of fixed shape / position (point, exp, deV) seen in two
+    64 x 72 images of one band with different PSFs and photometric scales;
+    noisy data drawn from the true model (plus a constant sky per image when
+    `sky_true` is given).  Returns (tractor, images, sources, rows, datas)."""
+    from tractor.galaxy import ExpGalaxy, DevGalaxy
+    H, W = 64, 72
+    psfs = [T.NCircularGaussianPSF([1.2, 2.6], [0.75, 0.25]),
+            T.GaussianMixturePSF(np.array([0.6, 0.3, 0.1]), np.zeros((3, 2)),
+                                 np.array([np.eye(2) * s ** 2 for s in (1.5, 3.0, 6.0)]))]
+    scales = [1.0, 2.5]
+    rows, srcs = [], []
+    for i in range(6):
+        kind = i % 3
+        px, py = rng.uniform(8, W - 8), rng.uniform(8, H - 8)
+        fl = rng.uniform(50., 500.)
+        re = float(rng.uniform(1., 3.))
+        e1, e2 = rng.uniform(-0.3, 0.3, 2)
+        br = T.Flux(fl)
+        if kind == 0:
+            s = T.PointSource(T.PixPos(px, py), br)
+        elif kind == 1:
+            s = ExpGalaxy(T.PixPos(px, py), br, T.EllipseE(re, e1, e2))
+        else:
+            s = DevGalaxy(T.PixPos(px, py), br, T.EllipseE(re, e1, e2))
+        rows.append([kind, px, py, fl, re, e1, e2])
+        srcs.append(s)
+    from tractor.sky import ConstantSky
+    tims = []
+    for b in range(2):
+        sky = ConstantSky(0. if sky_true is None else sky_true[b])
+        tims.append(T.Image(data=np.zeros((H, W), np.float32),
+                            inverr=np.ones((H, W), np.float32), psf=psfs[b],
+                            photocal=T.LinearPhotoCal(scales[b]), sky=sky))
+    tr = T.Tractor(tims, srcs)
+    datas = []
+    for b, tim in enumerate(tims):
+        clean = tr.getModelImage(b)
+        tim.data = (clean + rng.normal(size=clean.shape) * 0.5).astype(np.float32)
+        tim.inverr = np.full((H, W), 2., np.float32)
+        datas.append(tim.data.copy())
+    return tr, tims, srcs, rows, datas
+
+
+def forcedsky():
+    """Forced photometry (optimize.py:16-145, lsqr_optimizer.py:11-235) with
+    the images' constant skies fitted along with the fluxes (sky=True, the
+    fluxes' variance), the fit statistics (optimize.py:233-375),
+    and justims0's first evaluation, on the forced-photometry scene with a
+    sky added to the data."""
+    from oracle import refharness
+    refharness.load()
+    import tractor
+    rng = np.random.default_rng(610)
+    tr, tims, srcs, rows, datas = forced_scene(tractor, rng, sky_true=[3.0, -1.5])
+    for s in srcs:
+        s.freezeAllBut('brightness')
+        s.brightness.setParams([v * 0.7 + 5. for v in s.brightness.getParams()])
+    for tim in tims:
+        tim.freezeAllBut('sky')
+        tim.getSky().setParams([0.5])
+    start = np.array(tr.getParams())
+    R0 = tr.optimize_forced_photometry(sky=True, justims0=True, shared_params=False)
+    lnp0 = R0.lnp0
+    chis0 = np.stack(R0.chis0)
+    # (skyvariance=True fails in the reference: _get_iv unpacks its
+    # [(dsky, img)] lists as pairs, optimize.py:381)
+    R = tr.optimize_forced_photometry(sky=True, variance=True, fitstats=True,
+                                      shared_params=False)
+    fs = R.fitstats
+    keys = ['prochi2', 'pronpix', 'promasked', 'profracflux', 'proflux', 'npix', 'fracin',
+            'imchisq', 'imnpix', 'sky']
+    np.savez_compressed(os.path.join(OUT, 'forced_sky.npz'), sources=np.array(rows),
+                        data=np.stack(datas), start=start, params=np.array(tr.getParams()),
+                        names=np.array(tr.getParamNames()), IV=np.array(R.IV), lnp0=lnp0,
+                        chis0=chis0, **{'fs_' + k: np.asarray(getattr(fs, k)) for k in keys})
+    print('forced_sky fixture written to', OUT)
+
+
 if __name__ == '__main__':
     if sys.argv[1:] == ['hybrid']:
         hybrid()
@@ -538,5 +618,7 @@ if __name__ == '__main__':
         emfit()
     elif sys.argv[1:] == ['psfderiv']:
         psfderiv()
+    elif sys.argv[1:] == ['forcedsky']:
+        forcedsky()
     else:
         main()

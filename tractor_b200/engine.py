@@ -32,6 +32,9 @@ class Catalog(MultiParams):
     def getFrozenSources(self):
         return (s for s in self._getFrozenArray(self.subs) if s is not None)
 
+    def getNamedParamName(self, j):
+        return 'source%i' % j
+
     def printLong(self):
         print('Catalog with %i sources:' % len(self))
         for i, x in enumerate(self):

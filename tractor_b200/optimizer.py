@@ -254,18 +254,23 @@ class B200Optimizer(object):
                           fitstat_extras=None, justims0=False, variance=False,
                           skyvariance=False, shared_params=True, nonneg=False,
                           nilcounts=-1e30, wantims=True, negfluxval=None, **kwargs):
-        """Linear fit of the thawed sources' brightnesses with every other
-        parameter fixed: unit-flux models of all (image, source) pairs
-        rendered in one batch, the frozen sources' model as the base, then the
-        reference's loop -- an unscaled least-squares update on the device
-        (getUpdateDirection with chi images of the current fluxes), alpha = 1
-        when the fluxes stay above minFlux, otherwise the line search with
-        growing damping -- until the gain is below mindlnp.  Returns an
-        OptResult with ims0 / ims1 (img, model, inverr, chi, roi) and, with
-        variance=True, IV: the inverse variance of each flux."""
-        if sky or fitstats or rois is not None or nonneg or justims0:
-            raise NotImplementedError('forced photometry with sky fitting, fit statistics, ROIs, '
-                                      'non-negativity or justims0 is not provided')
+        """Linear fit of the thawed sources' brightnesses (and, with sky=True,
+        of every image's one-parameter sky) with every other parameter fixed
+        (Optimizer.forced_photometry, optimize.py:16-145, with
+        LsqrOptimizer's loop, lsqr_optimizer.py:11-235): unit-flux models of
+        all (image, source) pairs rendered in one batch, the frozen sources'
+        model as the base (without the sky when it is fitted), then an
+        unscaled least-squares update on the device (getUpdateDirection with
+        chi images of the current state; sky columns first), alpha = 1 when
+        the fluxes stay above minFlux, otherwise the line search with growing
+        damping, until the gain is below mindlnp.  Returns an OptResult with
+        ims0 / ims1 (image, model, inverr, chi, roi), with justims0 only the
+        first evaluation (lnp0, chis0, ims0), with variance=True IV (the
+        sky parameters first with skyvariance), with fitstats=True the
+        reference's fit statistics."""
+        if rois is not None or nonneg:
+            raise NotImplementedError('forced photometry with ROIs or non-negativity is not '
+                                      'provided')
         from .basics import LinearPhotoCal
         result = OptResult()
         imgs = list(tractor.getImages())
@@ -273,18 +278,33 @@ class B200Optimizer(object):
         for img in imgs:
             assert isinstance(img.getPhotoCal(), LinearPhotoCal)
             scales.append(img.getPhotoCal().getScale())
+        if sky:
+            for img in imgs:
+                assert img.getSky().numberOfParams() == 1
         srcs = list(tractor.catalog.getThawedSources())
         nparams = tractor.catalog.numberOfParams()
-        umodels = self._unit_models(tractor, srcs, imgs, minsb, **kwargs)
+        umodels, umodsforsource = self._unit_models(tractor, srcs, imgs, minsb, **kwargs)
         for um in umodels:
             assert len(um) == nparams
         fsrcs = list(tractor.catalog.getFrozenSources())
-        mod0 = [tractor.getModelImage(img, fsrcs, minsb=minsb, sky=True) for img in imgs]
+        # with the sky fitted, each trial renders it from its parameters
+        mod0 = [tractor.getModelImage(img, fsrcs, minsb=minsb, sky=not sky) for img in imgs]
+        skyderivs, nsky = None, 0
+        if sky:
+            skyderivs = []
+            for img in imgs:
+                for dsky in img.getSky().getParamDerivatives(tractor, img, None):
+                    skyderivs.append([(dsky, img)])
+            nsky = len(skyderivs)
+            assert nsky == tractor.images.numberOfParams()
+            assert nsky + nparams == tractor.numberOfParams()
         derivs = [[] for _ in range(nparams)]
         for img, umods, scale in zip(imgs, umodels, scales):
             for um, dd in zip(umods, derivs):
                 if um is not None:
                     dd.append((um * scale, img))
+        if sky:
+            derivs = skyderivs + derivs
         lnp0, chis0, ims0 = None, None, None
         imsBest = None
         damp0 = 1e-3
@@ -293,15 +313,25 @@ class B200Optimizer(object):
             tryAgain = False
             quitNow = False
             p0 = tractor.getParams()
+            p0sky = None
+            if sky:
+                p0sky, p0 = p0[:nsky], p0[nsky:]
             if lnp0 is None:
                 lnp0, chis0, ims0 = self._lnp_for_update(tractor, mod0, imgs, umodels, None, None,
-                                                         p0, scales, priors, minFlux)
+                                                         p0, scales, None, None, priors, sky,
+                                                         minFlux)
                 assert np.isfinite(lnp0)
+            if justims0:
+                result.lnp0, result.chis0, result.ims0 = lnp0, chis0, ims0
+                return result
             X = self.getUpdateDirection(tractor, derivs, damp=damping, priors=priors,
                                         scale_columns=False, chiImages=chis0,
                                         shared_params=shared_params)
             if X is None or len(X) == 0:
                 break
+            Xsky = None
+            if sky:
+                Xsky, X = X[:nsky], X[nsky:]
             trial = alphas
             if trial is None:
                 trial = default_alphas()
@@ -314,9 +344,10 @@ class B200Optimizer(object):
                 if damp0 < 1e3:
                     tryAgain = True
             lnpBest, alphaBest, chiBest = lnp0, None, None
+            alpha = None
             for alpha in trial:
                 lnp, chis, ims = self._lnp_for_update(tractor, mod0, imgs, umodels, X, alpha, p0,
-                                                      scales, priors, minFlux)
+                                                      scales, p0sky, Xsky, priors, sky, minFlux)
                 if lnp < lnpBest - 1. or not np.isfinite(lnp):
                     break
                 if lnp > lnpBest:
@@ -326,25 +357,39 @@ class B200Optimizer(object):
                 if minFlux is not None:
                     pa = [max(minFlux, v) for v in pa]
                 tractor.catalog.setParams(pa)
+                if sky:
+                    # as lsqr_optimizer.py:187-189: the sky takes the last
+                    # alpha the line search tried
+                    tractor.images.setParams([p + alpha * d for p, d in zip(p0sky, Xsky)])
                 dlogprob = lnpBest - lnp0
                 lnp0, chis0 = lnpBest, chiBest
             else:
                 dlogprob = 0.
+                if sky:
+                    tractor.images.setParams(p0sky)   # the line search moved it
             if dlogprob < mindlnp and not tryAgain:
                 break
             if quitNow:
                 break
-        if wantims:
+        if wantims or fitstats:
             result.ims0 = ims0
             result.ims1 = imsBest
         if variance:
-            result.IV = self._flux_iv(imgs, umodels, scales, nparams)
+            result.IV = self._flux_iv(imgs, umodels, scales, nparams,
+                                      skyderivs if (sky and skyvariance) else None)
+        if fitstats:
+            if imsBest is None:
+                result.fitstats = None
+            else:
+                result.fitstats = self._get_fitstats(tractor.catalog, imsBest, srcs, imgs,
+                                                     umodsforsource, umodels, scales, nilcounts,
+                                                     extras=fitstat_extras)
         return result
 
     def _unit_models(self, tractor, srcs, imgs, minsb, **kwargs):
-        """(n_images, n_params) unit-flux patches (Optimizer._get_umodels,
-        optimize.py:147-219), rendered in one batch where the source can
-        plan its renders."""
+        """(n_images, n_params) unit-flux patches and, per source, the indices
+        of its patches (Optimizer._get_umodels, optimize.py:147-219),
+        rendered in one batch where the source can plan its renders."""
         plan = RenderPlan()
         pend = []
         for img in imgs:
@@ -362,23 +407,30 @@ class B200Optimizer(object):
                                                                    modelMask=mask, **kwargs)))
             pend.append(row)
         umodels = []
-        for row in pend:
+        umodsforsource = [[] for _ in srcs]
+        for i, row in enumerate(pend):
             umods = []
-            for kind, v in row:
+            for si, (kind, v) in enumerate(row):
                 ums = [v.result()] if kind == 'plan' else list(v)
                 for um in ums:
                     if um is not None and um.patch is not None:
                         assert np.all(np.isfinite(um.patch))
+                if i == 0:
+                    umodsforsource[si].extend(range(len(umods), len(umods) + len(ums)))
                 umods.extend(ums)
             umodels.append(umods)
-        return umodels
+        return umodels, umodsforsource
 
     @staticmethod
-    def _getims(fluxes, imgs, umodels, mod0, scales, minFlux):
-        """Model, inverr and chi images at the given fluxes (optimize.py:472-530)."""
+    def _getims(fluxes, imgs, umodels, mod0, scales, sky, minFlux):
+        """Image, model, inverr and chi images at the given fluxes (the sky
+        rendered from its current parameters when it is fitted)
+        (optimize.py:472-520)."""
         ims = []
         for img, umods, m0, scale in zip(imgs, umodels, mod0, scales):
             mod = m0.copy()
+            if sky:
+                img.getSky().addTo(mod)
             for f, um in zip(fluxes, umods):
                 if um is None or um.patch is None:
                     continue
@@ -389,31 +441,40 @@ class B200Optimizer(object):
                     continue
                 (um * counts).addTo(mod)
             ie = img.getInvError()
-            chi = (img.getImage() - mod) * ie
-            ims.append((img, mod, ie, chi, None))
+            im = img.getImage()
+            chi = (im - mod) * ie
+            ims.append((im, mod, ie, chi, None))
         return ims
 
-    def _lnp_for_update(self, tractor, mod0, imgs, umodels, X, alpha, p0, scales, priors,
-                        minFlux):
+    def _lnp_for_update(self, tractor, mod0, imgs, umodels, X, alpha, p0, scales, p0sky, Xsky,
+                        priors, sky, minFlux):
+        """lsqr_optimizer.py:237-261: the sky is set to its trial value, the
+        prior evaluated at the tractor's current state."""
         pa = p0 if X is None else [p + alpha * d for p, d in zip(p0, X)]
+        if Xsky is not None:
+            tractor.images.setParams([p + alpha * d for p, d in zip(p0sky, Xsky)])
         lnp = 0.
         if priors:
-            saved = tractor.getParams()
-            tractor.setParams(pa)
             lnp += tractor.getLogPrior()
-            tractor.setParams(saved)
             if not np.isfinite(lnp):
                 return lnp, None, None
-        ims = self._getims(pa, imgs, umodels, mod0, scales, minFlux)
+        ims = self._getims(pa, imgs, umodels, mod0, scales, sky, minFlux)
         chis = [chi for _, _, _, chi, _ in ims]
         lnp += -0.5 * sum((chi.astype(np.float64) ** 2).sum() for chi in chis)
         return lnp, chis, ims
 
     @staticmethod
-    def _flux_iv(imgs, umodels, scales, nparams):
-        """Inverse variance of each flux (Optimizer._get_iv, optimize.py:378-423):
-        sum over images of (unit model x scale x inverr)^2."""
-        IV = np.zeros(nparams)
+    def _flux_iv(imgs, umodels, scales, nparams, skyderivs=None):
+        """Inverse variances (Optimizer._get_iv, optimize.py:378-423): for
+        each sky parameter (when given) the sum of (dsky x inverr)^2, then for
+        each flux the sum over images of (unit model x scale x inverr)^2."""
+        nsky = len(skyderivs) if skyderivs else 0
+        IV = np.zeros(nsky + nparams)
+        for di, ((dsky, tim),) in enumerate(skyderivs or []):
+            ie = tim.getInvError()
+            mm = np.zeros(tim.shape)
+            dsky.addTo(mm)
+            IV[di] = np.sum((mm * ie) ** 2)
         for img, umods, scale in zip(imgs, umodels, scales):
             ie = img.getInvError()
             H, W = img.shape
@@ -423,8 +484,98 @@ class B200Optimizer(object):
                 d = um.copy()
                 if not d.clipTo(W, H) or d.patch is None:
                     continue
-                IV[ui] += np.sum((d.patch * scale * ie[d.getSlice(img)]) ** 2)
+                IV[nsky + ui] += np.sum((d.patch * scale * ie[d.getSlice(img)]) ** 2)
         return IV
+
+    @staticmethod
+    def _get_fitstats(catalog, imsBest, srcs, imlist, umodsforsource, umodels, scales, nilcounts,
+                      extras=None):
+        """Optimizer._get_fitstats (optimize.py:233-375): per image the chi^2
+        and pixel count; per source the profile-weighted chi^2, pixel count,
+        masked fraction, fraction of other sources' flux, other sources'
+        flux, pixel count and fraction inside the images (host arithmetic on
+        the images the fit produced; `extras` adds profile-weighted sums of
+        given images)."""
+        if extras is None:
+            extras = []
+
+        class FitStats(object):
+            pass
+        fs = FitStats()
+        fs.imchisq = np.array([(chi ** 2).sum() for _, _, _, chi, _ in imsBest])
+        fs.imnpix = np.array([(ie > 0).sum() for _, _, ie, _, _ in imsBest])
+        n = len(srcs)
+        fs.prochi2 = np.zeros(n)
+        fs.pronpix = np.zeros(n)
+        fs.promasked = np.zeros(n)
+        fracflux_num = np.zeros(n)
+        fracflux_den = np.zeros(n)
+        fs.proflux = np.zeros(n)
+        fs.npix = np.zeros(n, int)
+        fracin_num = np.zeros(n)
+        fracin_den = np.zeros(n)
+        for key, x in extras:
+            setattr(fs, key, np.zeros(n))
+        # others' flux within a profile is measured without the sky
+        skies = []
+        for tim, (img, mod, ie, chi, roi) in zip(imlist, imsBest):
+            tim.getSky().addTo(mod, scale=-1.)
+            skies.append(getattr(tim.getSky(), 'val', 0.))
+        fs.sky = np.array(skies)
+        srcmods = [np.zeros_like(chi) for (img, mod, ie, chi, roi) in imsBest]
+        for si, uis in enumerate(umodsforsource):
+            src = catalog[si]
+            for imi, (umods, scale, tim, (img, mod, ie, chi, roi)) in enumerate(
+                    zip(umodels, scales, imlist, imsBest)):
+                pcal = tim.getPhotoCal()
+                cc = [pcal.brightnessToCounts(b) for b in src.getBrightnesses()]
+                sourcecounts = sum(cc)
+                if sourcecounts == 0:
+                    continue
+                srcmod = srcmods[imi]
+                xlo = xhi = ylo = yhi = None
+                for ui, counts in zip(uis, cc):
+                    if counts == 0:
+                        continue
+                    um = umods[ui]
+                    if um is None:
+                        continue
+                    x0, y0 = um.x0, um.y0
+                    uh, uw = um.shape
+                    xlo = x0 if xlo is None or x0 < xlo else xlo
+                    xhi = x0 + uw if xhi is None or x0 + uw > xhi else xhi
+                    ylo = y0 if ylo is None or y0 < ylo else ylo
+                    yhi = y0 + uh if yhi is None or y0 + uh > yhi else yhi
+                    (um * counts).addTo(srcmod)
+                if xlo is None or xhi is None or ylo is None or yhi is None:
+                    continue
+                slc = slice(ylo, yhi), slice(xlo, xhi)
+                srcmod[slc] /= sourcecounts
+                nz = np.flatnonzero((srcmod[slc] != 0) * (ie[slc] > 0))
+                if len(nz) == 0:
+                    srcmod[slc] = 0.
+                    continue
+                fs.prochi2[si] += np.sum(np.abs(srcmod[slc].flat[nz]) * chi[slc].flat[nz] ** 2)
+                fs.pronpix[si] += np.sum(np.abs(srcmod[slc].flat[nz]))
+                fs.promasked[si] += np.sum(np.abs(srcmod[slc][ie[slc] == 0]))
+                fracflux_num[si] += (np.sum((np.abs(mod[slc] / sourcecounts - srcmod[slc]) *
+                                             np.abs(srcmod[slc])).flat[nz]) /
+                                     np.sum((srcmod[slc] ** 2).flat[nz]))
+                fracflux_den[si] += np.sum(np.abs(srcmod[slc]).flat[nz] / np.abs(sourcecounts))
+                fs.proflux[si] += np.sum((np.abs((mod[slc] - srcmod[slc] * sourcecounts) / scale) *
+                                          np.abs(srcmod[slc])).flat[nz])
+                fs.npix[si] += len(nz)
+                fracin_num[si] += np.sum(np.abs(srcmod[slc]))
+                fracin_den[si] += 1.
+                for key, extraims in extras:
+                    x = getattr(fs, key)
+                    x[si] += np.sum(np.abs(srcmod[slc].flat[nz]) * extraims[imi][slc].flat[nz])
+                srcmod[slc] = 0.
+        fs.profracflux = fracflux_num / np.maximum(1, fracflux_den)
+        fs.fracin = fracin_num / np.maximum(1, fracin_den)
+        for tim, (img, mod, ie, chi, roi) in zip(imlist, imsBest):
+            tim.getSky().addTo(mod)
+        return fs
 
 
 class B200ConstrainedOptimizer(B200Optimizer):
