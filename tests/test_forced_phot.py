@@ -235,3 +235,25 @@ def test_fitstats_port_equals_reference(monkeypatch):
     for k in ('prochi2', 'pronpix', 'promasked', 'profracflux', 'proflux', 'npix', 'fracin',
               'imchisq', 'imnpix', 'sky'):
         assert np.array_equal(np.asarray(getattr(mine, k)), np.asarray(getattr(ref, k))), k
+
+
+def test_nonneg_is_accepted_and_unused(backend):
+    """LsqrOptimizer accepts nonneg and does not use it
+    (lsqr_optimizer.py:11-38): the same fluxes either way."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'forced_phot.npz'))
+    H, W = g['data'].shape[1:]
+    out = []
+    for nonneg in (False, True):
+        tims = [T.Image(data=g['data'][b], inverr=np.full((H, W), 2., np.float32),
+                        psf=T.NCircularGaussianPSF([1.2, 2.6], [0.75, 0.25]),
+                        photocal=T.LinearPhotoCal(float(g['scales'][b]))) for b in range(2)]
+        srcs = [T.PointSource(T.PixPos(px, py), T.Flux(fl))
+                for kind, px, py, fl, re, e1, e2 in g['sources']]
+        tr = T.Tractor(tims, srcs)
+        tr.freezeParam('images')
+        for s in srcs:
+            s.freezeAllBut('brightness')
+        tr.optimize_forced_photometry(nonneg=nonneg, shared_params=False)
+        out.append(np.array(tr.getParams()))
+    assert np.array_equal(out[0], out[1])

@@ -267,10 +267,10 @@ class B200Optimizer(object):
         ims0 / ims1 (image, model, inverr, chi, roi), with justims0 only the
         first evaluation (lnp0, chis0, ims0), with variance=True IV (the
         sky parameters first with skyvariance), with fitstats=True the
-        reference's fit statistics."""
-        if rois is not None or nonneg:
-            raise NotImplementedError('forced photometry with ROIs or non-negativity is not '
-                                      'provided')
+        reference's fit statistics.  nonneg and negfluxval are accepted and,
+        as by LsqrOptimizer (lsqr_optimizer.py:11-38), not used."""
+        if rois is not None:
+            raise NotImplementedError('forced photometry with ROIs is not provided')
         from .basics import LinearPhotoCal
         result = OptResult()
         imgs = list(tractor.getImages())
