@@ -13,6 +13,7 @@ root in the development container:
     python tests/golden/make_golden.py emfit    # emfit.npz
     python tests/golden/make_golden.py psfderiv # psf_derivs.npz
     python tests/golden/make_golden.py forcedsky # forced_sky.npz
+    python tests/golden/make_golden.py varying  # varying_psf.npz
 """
 import os
 import sys
@@ -609,6 +610,46 @@ def forcedsky():
     print('forced_sky fixture written to', OUT)
 
 
+def varying():
+    """VaryingGaussianPSF (psfex.py:8-150) over the degree-2 PsfEx model of
+    psfex.npz (100 x 80 image): (a) GaussianMixtureEllipsePSF on a 4 x 4
+    grid through the reference's own _fitParamGrid (each optimiser fit
+    started from the previous one); (b) GaussianMixturePSF on a 4 x 4 grid,
+    each point fitted by fromStamp's EM from its default start (the
+    reference's grid loop cannot pass one EM fit's parameters to the next)
+    and splined by the reference's fitSavedData.  The mixture parameters at
+    a few positions."""
+    from oracle import refharness
+    refharness.load()
+    from tractor.psf import GaussianMixturePSF, GaussianMixtureEllipsePSF
+    from tractor.psfex import PsfExModel, VaryingGaussianPSF
+    g = np.load(os.path.join(OUT, 'psfex.npz'))
+    deg, x0, y0, xs, ys = g['poly']
+    m = PsfExModel()
+    m.sampling, m.psfbases, m.degree = 1., g['bases'], int(deg)
+    m.x0, m.y0, m.xscale, m.yscale = x0, y0, xs, ys
+    m.radius, m.fwhm = (g['bases'].shape[1] + 1) / 2., 4.0
+
+    class Varying(VaryingGaussianPSF):
+        def instantiateAt(self, x, y):
+            return m.at(x, y)
+
+    pos = np.array([[10.5, 20.25], [60., 45.], [90., 75.], [0., 0.]])
+    ve = Varying(100, 80, nx=4, ny=4, K=2, psfClass=GaussianMixtureEllipsePSF)
+    ve._fitParamGrid()
+    ell = np.array([ve.psfParamsAt(x, y) for x, y in pos])
+    K = 2
+    vm = Varying(100, 80, nx=4, ny=4, K=K)
+    YY, XX = np.linspace(0, 80, 4), np.linspace(0, 100, 4)
+    pp = np.array([[GaussianMixturePSF.fromStamp(m.at(x, y), N=K).getAllParams() for x in XX]
+                   for y in YY])
+    vm.fitSavedData(pp, XX, YY)
+    mog = np.array([vm.psfParamsAt(x, y) for x, y in pos])
+    np.savez_compressed(os.path.join(OUT, 'varying_psf.npz'), pos=pos, ell=ell, mog=mog,
+                        mog_grid=pp)
+    print('varying_psf fixture written to', OUT)
+
+
 if __name__ == '__main__':
     if sys.argv[1:] == ['hybrid']:
         hybrid()
@@ -620,5 +661,7 @@ if __name__ == '__main__':
         psfderiv()
     elif sys.argv[1:] == ['forcedsky']:
         forcedsky()
+    elif sys.argv[1:] == ['varying']:
+        varying()
     else:
         main()

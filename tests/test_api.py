@@ -401,3 +401,48 @@ def test_hybrid_psf_fits_its_gaussian_approximation(backend):
     np.testing.assert_allclose(hyb.gauss.mog.amp, g['hyb_amp'], rtol=1e-9, atol=1e-13)
     np.testing.assert_allclose(hyb.gauss.mog.mean, g['hyb_mean'], rtol=0, atol=1e-9)
     np.testing.assert_allclose(hyb.gauss.mog.var, g['hyb_var'], rtol=1e-9, atol=1e-12)
+
+
+def _varying(T, cls=None, n=4):
+    from tractor_b200.psfex import PsfExModel, VaryingGaussianPSF
+    p = np.load(os.path.join(GOLDEN, 'psfex.npz'))
+    deg, x0, y0, xs, ys = p['poly']
+    m = PsfExModel(bases=p['bases'], degree=int(deg), x0=x0, y0=y0, xscale=xs, yscale=ys,
+                   fwhm=4.0)
+
+    class Varying(VaryingGaussianPSF):
+        def instantiateAt(self, x, y):
+            return m.at(x, y)
+    return Varying(100, 80, nx=n, ny=n, K=2, psfClass=cls)
+
+
+def test_varying_gaussian_psf_matches_reference(backend):
+    """VaryingGaussianPSF (psfex.py:8-150) over a PsfEx model: the mixture
+    parameters at several positions against the reference's -- the EM grid
+    (one batched launch) splined as the reference splines its per-point
+    fits, and the GaussianMixtureEllipsePSF grid fitted one point after
+    another from the previous fit as the reference's _fitParamGrid
+    (varying_psf.npz); point sources rendered with the mixture at their
+    position."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'varying_psf.npz'))
+    vm = _varying(T)
+    got = np.array([vm.psfParamsAt(x, y) for x, y in g['pos']])
+    np.testing.assert_allclose(got, g['mog'], rtol=1e-7, atol=1e-9)
+    ve = _varying(T, T.GaussianMixtureEllipsePSF)
+    got = np.array([ve.psfParamsAt(x, y) for x, y in g['pos']])
+    np.testing.assert_allclose(got, g['ell'], rtol=2e-3, atol=2e-4)
+    # a point source takes the mixture of its position
+    tim = T.Image(data=np.zeros((80, 100), np.float32), inverr=np.ones((80, 100), np.float32),
+                  psf=vm, photocal=T.LinearPhotoCal(1.))
+    src = T.PointSource(T.PixPos(60.3, 45.7), T.Flux(100.))
+    p1 = src.getModelPatch(tim)
+    tim2 = T.Image(data=np.zeros((80, 100), np.float32), inverr=np.ones((80, 100), np.float32),
+                   psf=vm.psfAt(60.3, 45.7), photocal=T.LinearPhotoCal(1.))
+    p2 = src.getModelPatch(tim2)
+    assert (p1.x0, p1.y0) == (p2.x0, p2.y0) and np.array_equal(p1.patch, p2.patch)
+    # and seen from a subimage through getShifted
+    sub = vm.getShifted(20, 10)
+    m1 = sub.getMixtureOfGaussians(px=40.3, py=35.7)
+    m2 = vm.getMixtureOfGaussians(px=60.3, py=45.7)
+    assert np.array_equal(m1.var, m2.var) and np.array_equal(m1.amp, m2.amp)

@@ -11,6 +11,7 @@ reader, `fitsbin`), from rows of merged tables, or built from their arrays.
 import numpy as np
 
 from . import render
+from .params import MultiParams
 from .psf import PixelizedPSF
 
 
@@ -199,3 +200,152 @@ class PixelizedPsfEx(PixelizedPSF):
         spec, cx, cy = render.psf_spectra().compute(self.getImage(px, py), sz)
         key = ('PixelizedPsfEx', id(self), float(px), float(py), self.psfex.x0, self.psfex.y0)
         return key, spec, cx, cy
+
+
+class VaryingGaussianPSF(MultiParams):
+    """A mixture-of-Gaussians PSF varying over the image: the mixture is fit
+    at an nx x ny grid of positions and each of its parameters interpolated
+    by a bicubic spline (tractor/psfex.py:8-150).  Subclasses provide
+    `instantiateAt(x, y)`, the PSF image at a position.
+
+    The grid fits: for the default psfClass (GaussianMixturePSF, fitted by
+    EM) all grid points are fitted in one batched launch, each from
+    fromStamp's default start (the reference starts each fit from the
+    previous one's flat parameter list, which GaussianMixturePSF.fromStamp
+    cannot unpack); for other classes (GaussianMixtureEllipsePSF, or a given
+    `fitfunc`) the fits run one after another, each started from the
+    previous one as the reference does."""
+
+    def __init__(self, W, H, nx=11, ny=11, K=3, psfClass=None):
+        super(VaryingGaussianPSF, self).__init__()
+        from .psf import GaussianMixturePSF
+        self.psfclass = GaussianMixturePSF if psfClass is None else psfClass
+        self.splines = None
+        self.W, self.H = W, H
+        self.K = K
+        self.nx, self.ny = nx, ny
+        self.savesplinedata = False
+
+    def __str__(self):
+        return '%s: %s, %i x %i' % (type(self).__name__, self.psfclass.__name__, self.nx,
+                                    self.ny)
+
+    def getShifted(self, x0, y0):
+        return _ShiftedMogPsf(self, x0, y0)
+
+    def getRadius(self):
+        return getattr(self, 'radius', 25.)
+
+    def fitSavedData(self, pp, XX, YY):
+        import scipy.interpolate
+        self.splines = [scipy.interpolate.RectBivariateSpline(XX, YY, pp[:, :, i].T)
+                        for i in range(len(pp[0][0]))]
+
+    def ensureSplines(self):
+        if self.splines is None:
+            self.fitSavedData(*self.splinedata)
+
+    def ensureFit(self):
+        if self.splines is None:
+            self._fitParamGrid()
+
+    def psfParamsAt(self, x, y):
+        """The mixture parameters at pixel (x, y) (psfex.py:85-101)."""
+        self.ensureFit()
+        return np.array([float(spl(x, y, grid=False)) for spl in self.splines])
+
+    def psfAt(self, x, y):
+        return self.psfclass(*self.psfParamsAt(x, y))
+
+    mogAt = psfAt
+
+    def getMixtureOfGaussians(self, px=None, py=None):
+        return self.psfAt(0. if px is None else px, 0. if py is None else py) \
+            .getMixtureOfGaussians()
+
+    def getPointSourcePatch(self, px, py, **kwargs):
+        return self.psfAt(px, py).getPointSourcePatch(px, py, **kwargs)
+
+    def _plan_point_source(self, plan, px, py, **kwargs):
+        return self.psfAt(px, py)._plan_point_source(plan, px, py, **kwargs)
+
+    def _fitParamGrid(self, fitfunc=None, trim=0, **kwargs):
+        """Fits the mixture at the grid points (psfex.py:118-150)."""
+        from .psf import GaussianMixturePSF
+        YY = np.linspace(0, self.H, self.ny)
+        XX = np.linspace(0, self.W, self.nx)
+        stamps = []
+        for y in YY:
+            for x in XX:
+                im = self.instantiateAt(x, y)
+                if trim > 0:
+                    im = im[trim:-trim, trim:-trim]
+                stamps.append(im)
+        if fitfunc is None and self.psfclass is GaussianMixturePSF:
+            psfs = GaussianMixturePSF.fromStamps(stamps, N=self.K, **kwargs)
+            if any(p is None for p in psfs):
+                raise RuntimeError('VaryingGaussianPSF: an EM fit failed (non-positive '
+                                   'covariance determinant)')
+            flat = [np.array(p.getAllParams()) for p in psfs]
+        else:
+            f = fitfunc if fitfunc is not None else self.psfclass.fromStamp
+            flat, p0, px0 = [], None, None
+            for iy in range(self.ny):
+                p0 = px0
+                for ix in range(self.nx):
+                    psf = f(stamps[iy * self.nx + ix], N=self.K, P0=p0, **kwargs)
+                    p0 = psf.getParams()
+                    if ix == 0:
+                        px0 = p0
+                    flat.append(np.array(psf.getAllParams()))
+        pp = np.array(flat).reshape(self.ny, self.nx, -1)
+        self.fitSavedData(pp, XX, YY)
+        if self.savesplinedata:
+            self.splinedata = (pp, XX, YY)
+
+
+class _ShiftedMogPsf(object):
+    """A position-dependent PSF seen from a subimage starting at (x0, y0)
+    (tractor/shifted.py:63-110): positions are shifted into the parent's
+    frame and patches shifted back."""
+
+    def __init__(self, psf, x0, y0):
+        self.psf, self.x0, self.y0 = psf, x0, y0
+
+    def __str__(self):
+        return ('ShiftedPsf: %i,%i + ' % (self.x0, self.y0)) + str(self.psf)
+
+    def hashkey(self):
+        return ('ShiftedPsf', self.x0, self.y0) + tuple(self.psf.hashkey())
+
+    def getRadius(self):
+        return self.psf.getRadius()
+
+    def getMixtureOfGaussians(self, px=None, py=None):
+        return self.psf.getMixtureOfGaussians(px=(px or 0.) + self.x0, py=(py or 0.) + self.y0)
+
+    def _plan_point_source(self, plan, px, py, **kwargs):
+        # the mixture of the parent's position, rendered at the subimage's
+        return self.psf.psfAt(px + self.x0, py + self.y0)._plan_point_source(plan, px, py,
+                                                                             **kwargs)
+
+    def getPointSourcePatch(self, px, py, **kwargs):
+        return self.psf.psfAt(px + self.x0, py + self.y0).getPointSourcePatch(px, py, **kwargs)
+
+
+class VaryingGaussianPsfEx(VaryingGaussianPSF):
+    """VaryingGaussianPSF of a PsfEx model read from `fn`
+    (tractor/psfex.py:522-553): the grid images are the model's images."""
+
+    def __init__(self, fn, W, H, ext=1, scale=True, nx=11, ny=11, K=3, psfClass=None):
+        assert scale
+        self.psfex = PsfExModel(fn, ext=ext)
+        self.scale = scale
+        super(VaryingGaussianPsfEx, self).__init__(W, H, nx, ny, K, psfClass=psfClass)
+
+    def instantiateAt(self, x, y):
+        return self.psfex.at(x, y)
+
+
+# the reference's original name for VaryingGaussianPsfEx
+PsfEx = VaryingGaussianPsfEx
