@@ -1193,13 +1193,21 @@ def main():
     }
     if not args.no_secondary:
         cpu_s = None if (args.no_cpu_baseline or world > 1 or rank) else min(args.cpu_seconds, 8.0)
-        line['secondary'] = [bench_scene(args, dev, flush, clk, cpu_s),
-                             bench_fit(args, dev, flush, clk, cpu_s),
-                             bench_normal_equations(args, dev, flush, clk,
-                                                    cpu_s and min(cpu_s, 4.0)),
-                             bench_plain_small(args, dev),
-                             bench_emfit(args, dev, flush, clk, cpu_s and min(cpu_s, 4.0)),
-                             bench_segment(args, dev, flush, clk, cpu_s)]
+        runs = [('batched scene', lambda: bench_scene(args, dev, flush, clk, cpu_s)),
+                ('blob fitting', lambda: bench_fit(args, dev, flush, clk, cpu_s)),
+                ('normal equations', lambda: bench_normal_equations(
+                    args, dev, flush, clk, cpu_s and min(cpu_s, 4.0))),
+                ('plain small fit', lambda: bench_plain_small(args, dev)),
+                ('EM PSF fits', lambda: bench_emfit(args, dev, flush, clk,
+                                                    cpu_s and min(cpu_s, 4.0))),
+                ('blob segmentation', lambda: bench_segment(args, dev, flush, clk, cpu_s))]
+        line['secondary'] = []
+        for name, run in runs:
+            # a secondary line that fails is reported in the line, not fatal
+            try:
+                line['secondary'].append(run())
+            except Exception as e:   # noqa: BLE001
+                line['secondary'].append({'workload': name, 'error': repr(e)})
     line['plain_fp64'] = fourier_plain_fp64(srcs, out, dev, budget=3.0)
     if line['plain_fp64']['value']:
         line['speedup_vs_plain_fp64'] = value / line['plain_fp64']['value']
