@@ -446,3 +446,23 @@ def test_varying_gaussian_psf_matches_reference(backend):
     m1 = sub.getMixtureOfGaussians(px=40.3, py=35.7)
     m2 = vm.getMixtureOfGaussians(px=60.3, py=45.7)
     assert np.array_equal(m1.var, m2.var) and np.array_equal(m1.amp, m2.amp)
+
+
+def test_subimage_renders_the_same_pixels(backend):
+    """Image.subimage (image.py:82-92): a source rendered in a subimage
+    equals the same pixels of the full image's render.  NullWCS.shifted
+    ignores the shift, as the reference's (wcs.py:48-49), so the source is
+    placed at its subimage coordinates."""
+    import tractor_b200 as T
+    psf = T.GaussianMixturePSF(np.array([0.8, 0.2]), np.zeros((2, 2)),
+                               np.array([[[1.5, 0.2], [0.2, 1.8]], [[6., 0.], [0., 6.]]]))
+    tim = T.Image(data=np.zeros((50, 60), np.float32), inverr=np.ones((50, 60), np.float32),
+                  psf=psf, sky=T.ConstantSky(2.), photocal=T.LinearPhotoCal(1.), name='full')
+    tim.time = 5.
+    sub = tim.subimage(10, 45, 5, 40)
+    assert sub.shape == (35, 35) and sub.name == 'full' and sub.getTime() == 5.
+    src = T.ExpGalaxy(T.PixPos(30.2, 22.7), T.Flux(500.), T.EllipseE(2., 0.2, -0.1))
+    full = T.Tractor([tim], [src]).getModelImage(0)
+    moved = T.ExpGalaxy(T.PixPos(30.2 - 10, 22.7 - 5), T.Flux(500.), T.EllipseE(2., 0.2, -0.1))
+    part = T.Tractor([sub], [moved]).getModelImage(0)
+    assert np.abs(part - full[5:40, 10:45]).max() <= 1e-5 * np.abs(full).max()

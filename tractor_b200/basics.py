@@ -288,6 +288,20 @@ class Image(MultiParams):
                               wcs=self.wcs.copy(), psf=self.psf.copy(), sky=self.sky.copy(),
                               photocal=self.photocal.copy(), name=self.name, time=self.time)
 
+    def subimage(self, x0, x1, y0, y1):
+        """The image of pixels [x0, x1) x [y0, y1) (image.py:82-92): pixels
+        copied, WCS / PSF / sky shifted to the subimage's origin."""
+        slc = (slice(y0, y1), slice(x0, x1))
+        subtim = Image(data=self.data[slc].copy(), inverr=self.inverr[slc].copy(),
+                       wcs=self.wcs.shifted(x0, y0), psf=self.psf.getShifted(x0, y0),
+                       sky=self.sky.shifted(x0, y0), photocal=self.photocal.copy())
+        subtim.name = self.name
+        subtim.time = self.time
+        return subtim
+
+    def getTime(self):
+        return self.time
+
     def getParamDerivatives(self, tractor, srcs):
         derivs = []
         for s in self._getActiveSubs():
