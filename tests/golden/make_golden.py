@@ -14,6 +14,7 @@ root in the development container:
     python tests/golden/make_golden.py psfderiv # psf_derivs.npz
     python tests/golden/make_golden.py forcedsky # forced_sky.npz
     python tests/golden/make_golden.py varying  # varying_psf.npz
+    python tests/golden/make_golden.py composite # composite.npz
 """
 import os
 import sys
@@ -650,6 +651,34 @@ def varying():
     print('varying_psf fixture written to', OUT)
 
 
+def composite():
+    """CompositeGalaxy (galaxy.py:1032-1160) on a 60 x 60 image with a
+    2-Gaussian PSF: the model patch with and without a mask, and the
+    derivatives with the position thawed and frozen."""
+    from oracle import refharness
+    refharness.load()
+    from tractor import (Image, PixPos, Flux, LinearPhotoCal, NCircularGaussianPSF, EllipseE)
+    from tractor.galaxy import CompositeGalaxy
+    from tractor.patch import ModelMask
+    tim = Image(data=np.zeros((60, 60), np.float32), inverr=np.ones((60, 60), np.float32),
+                psf=NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2]), photocal=LinearPhotoCal(1.))
+    src = CompositeGalaxy(PixPos(30.3, 29.6), Flux(800.), EllipseE(2.5, 0.2, -0.1), Flux(400.),
+                          EllipseE(4.0, -0.1, 0.25))
+    arrays = {}
+    for k, v in patches_to_arrays([src.getModelPatch(tim)]).items():
+        arrays['model.' + k] = v
+    mm = ModelMask(10, 12, 40, 36)
+    for k, v in patches_to_arrays([src.getModelPatch(tim, modelMask=mm)]).items():
+        arrays['masked.' + k] = v
+    for k, v in patches_to_arrays(src.getParamDerivatives(tim)).items():
+        arrays['derivs.' + k] = v
+    src.freezeParam('pos')
+    for k, v in patches_to_arrays(src.getParamDerivatives(tim)).items():
+        arrays['derivs_nopos.' + k] = v
+    np.savez_compressed(os.path.join(OUT, 'composite.npz'), **arrays)
+    print('composite fixture written to', OUT)
+
+
 if __name__ == '__main__':
     if sys.argv[1:] == ['hybrid']:
         hybrid()
@@ -663,5 +692,7 @@ if __name__ == '__main__':
         forcedsky()
     elif sys.argv[1:] == ['varying']:
         varying()
+    elif sys.argv[1:] == ['composite']:
+        composite()
     else:
         main()

@@ -466,3 +466,87 @@ def test_subimage_renders_the_same_pixels(backend):
     moved = T.ExpGalaxy(T.PixPos(30.2 - 10, 22.7 - 5), T.Flux(500.), T.EllipseE(2., 0.2, -0.1))
     part = T.Tractor([sub], [moved]).getModelImage(0)
     assert np.abs(part - full[5:40, 10:45]).max() <= 1e-5 * np.abs(full).max()
+
+
+def test_composite_galaxy_matches_reference(backend):
+    """CompositeGalaxy (galaxy.py:1032-1160): model patches (with and
+    without a mask) and derivatives (the shared position's columns summed;
+    position frozen) against the reference's (composite.npz)."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'composite.npz'))
+    tim = T.Image(data=np.zeros((60, 60), np.float32), inverr=np.ones((60, 60), np.float32),
+                  psf=T.NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2]), photocal=T.LinearPhotoCal(1.))
+    src = T.CompositeGalaxy(T.PixPos(30.3, 29.6), T.Flux(800.), T.EllipseE(2.5, 0.2, -0.1),
+                            T.Flux(400.), T.EllipseE(4.0, -0.1, 0.25))
+    _check_patch(src.getModelPatch(tim), _unpack(g, 'model')[0], PEAK_TOL, 'composite')
+    _check_patch(src.getModelPatch(tim, modelMask=T.ModelMask(10, 12, 40, 36)),
+                 _unpack(g, 'masked')[0], PEAK_TOL, 'composite masked')
+    for key, freeze in (('derivs', False), ('derivs_nopos', True)):
+        if freeze:
+            src.freezeParam('pos')
+        got = src.getParamDerivatives(tim)
+        ref = _unpack(g, key)
+        assert len(got) == len(ref)
+        for i, (p, r) in enumerate(zip(got, ref)):
+            _check_patch(p, r, DERIV_TOL, '%s %d' % (key, i))
+
+
+@pytest.mark.reference
+def test_small_api_helpers_match_reference():
+    """Mags / MagsPhotoCal / FluxesPhotoCal, the NanoMaggies helpers, the
+    GaussianMixturePSF helpers, NCircularGaussianPSF.scale, ConstantSky
+    subtract / scale and Patch.hasNonzeroOverlapWith against the live
+    reference."""
+    from oracle import refharness
+    if not refharness.available():
+        pytest.skip('reference source tree not present')
+    R = refharness.load()
+    import tractor as RT
+    from tractor import brightness as RB
+    from tractor.sky import ConstantSky as RSky
+    import tractor_b200 as T
+    m, rm = T.Mags(r=14.3, g=15.6, order=['r', 'g']), RB.Mags(r=14.3, g=15.6, order=['r', 'g'])
+    for a, b in (((m + 0.1), (rm + 0.1)), ((m * 2.5), (rm * 2.5)), ((m + m), (rm + rm))):
+        assert np.allclose(a.getParams(), b.getParams(), rtol=1e-15)
+    assert m.getStepSizes() == rm.getStepSizes()
+    pc, rpc = T.MagsPhotoCal('g', 24.5), RB.MagsPhotoCal('g', 24.5)
+    assert pc.brightnessToCounts(m) == rpc.brightnessToCounts(rm)
+    assert pc.countsToMag(1234.) == rpc.countsToMag(1234.)
+    assert pc.getParamNames() == rpc.getParamNames()
+    nm, rnm = T.NanoMaggies.fromMag(m), RB.NanoMaggies.fromMag(rm)
+    assert np.array_equal(nm.getParams(), rnm.getParams())
+    assert T.FluxesPhotoCal('g').brightnessToCounts(nm) == \
+        RB.FluxesPhotoCal('g').brightnessToCounts(rnm)
+    for f in ('zeropointToScale', 'scaleToZeropoint'):
+        assert getattr(T.NanoMaggies, f)(23.7) == getattr(RB.NanoMaggies, f)(23.7)
+    fl, iv = np.array([10., -1., 5., 0.3]), np.array([4., 4., 0., 9.])
+    for a, b in zip(T.NanoMaggies.fluxErrorsToMagErrors(fl, iv),
+                    RB.NanoMaggies.fluxErrorsToMagErrors(fl, iv)):
+        assert np.array_equal(a, b, equal_nan=True)
+    amp, mean = np.array([0.7, 0.3]), np.array([[0.1, -0.2], [0., 0.3]])
+    var = np.array([[[1.6, 0.2], [0.2, 1.9]], [[7.5, -0.4], [-0.4, 8.2]]])
+    p, rp = T.GaussianMixturePSF(amp, mean, var), RT.GaussianMixturePSF(amp, mean, var)
+    assert p.computeRadius() == rp.computeRadius()
+    a, b = p.scaleBy(1.7), rp.scaleBy(1.7)
+    assert np.array_equal(a.mog.var, b.mog.var) and np.array_equal(a.mog.mean, b.mog.mean)
+    p.shiftBy(0.5, -1.)
+    rp.shiftBy(0.5, -1.)
+    assert np.array_equal(p.mog.mean, rp.mog.mean)
+    assert all(np.array_equal(x, y) for x, y in zip(p.get_wmuvar(), rp.get_wmuvar()))
+    hdr = dict(('PSF_P%d' % i, v) for i, v in enumerate(rp.getAllParams()))
+    q = T.GaussianMixturePSF.fromFitsHeader(hdr, prefix='PSF_')
+    assert np.array_equal(q.getAllParams(), rp.getAllParams())
+    n, rn = T.NCircularGaussianPSF([1.5, 3.], [0.8, 0.2]), RT.NCircularGaussianPSF([1.5, 3.],
+                                                                                  [0.8, 0.2])
+    assert np.array_equal(n.scale(1.3).getParams(), rn.scale(1.3).getParams())
+    sk, rsk = T.ConstantSky(3.), RSky(3.)
+    for o in (sk, rsk):
+        o.subtract(0.5)
+        o.scale(2.)
+    assert sk.getValue() == rsk.getValue()
+    pa = T.Patch(2, 3, np.ones((4, 5)))
+    for other in (T.Patch(5, 5, np.ones((3, 3))), T.Patch(5, 5, np.zeros((3, 3))),
+                  T.Patch(20, 20, np.ones((2, 2)))):
+        ro = RT.Patch(other.x0, other.y0, other.patch)
+        assert pa.hasNonzeroOverlapWith(other) == RT.Patch(2, 3, np.ones((4, 5))) \
+            .hasNonzeroOverlapWith(ro)

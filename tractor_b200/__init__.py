@@ -12,8 +12,9 @@ __version__ = '0.1.0'
 from .params import (BaseParams, ScalarParam, NamedParams, ParamList, MultiParams,
                      GaussianPriors, GaussianPriorsMixin)
 from .patch import Patch, ModelMask, add_patches, get_overlapping_region
-from .basics import (PixPos, NullWCS, Flux, Mag, Fluxes, NanoMaggies, MultiBandBrightness,
-                     NullPhotoCal, LinearPhotoCal, NullSky, ConstantSky, Image)
+from .basics import (PixPos, NullWCS, Flux, Mag, Mags, Fluxes, NanoMaggies, MultiBandBrightness,
+                     NullPhotoCal, LinearPhotoCal, FluxesPhotoCal, MagsPhotoCal, NullSky,
+                     ConstantSky, Image)
 from .ellipses import GalaxyShape, EllipseE, EllipseESoft
 from .profiles import MixtureOfGaussians, SersicMixture
 from .psf import (HybridPSF, HybridPixelizedPSF, GaussianMixturePSF, GaussianMixtureEllipsePSF,
@@ -21,15 +22,18 @@ from .psf import (HybridPSF, HybridPixelizedPSF, GaussianMixturePSF, GaussianMix
                   PixelizedPSF, NormalizedPixelizedPsf, MogParams)
 from .sources import (BasicSource, SingleProfileSource, PointSource, Galaxy, ProfileGalaxy,
                       HoggGalaxy, GaussianGalaxy, ExpGalaxy, DevGalaxy, SersicGalaxy, SersicIndex,
+                      CompositeGalaxy,
                       FracDev, SoftenedFracDev, FixedCompositeGalaxy)
 from .engine import Tractor, Catalog, Images
-from .optimizer import B200Optimizer, B200ConstrainedOptimizer
+from .optimizer import (B200Optimizer, B200ConstrainedOptimizer, LsqrOptimizer,
+                        ConstrainedOptimizer)
 
 __all__ = [
     'BaseParams', 'ScalarParam', 'NamedParams', 'ParamList', 'MultiParams', 'GaussianPriors',
     'Patch', 'ModelMask', 'add_patches', 'get_overlapping_region',
     'PixPos', 'NullWCS', 'Flux', 'Mag', 'Fluxes', 'NanoMaggies', 'NullPhotoCal', 'LinearPhotoCal',
-    'NullSky', 'ConstantSky', 'Image',
+    'NullSky', 'ConstantSky', 'Image', 'Mags', 'FluxesPhotoCal', 'MagsPhotoCal',
+    'LsqrOptimizer', 'ConstrainedOptimizer',
     'GalaxyShape', 'EllipseE', 'EllipseESoft',
     'MixtureOfGaussians', 'SersicMixture',
     'HybridPSF', 'HybridPixelizedPSF', 'GaussianMixturePSF', 'GaussianMixtureEllipsePSF',
@@ -37,6 +41,6 @@ __all__ = [
     'NormalizedPixelizedPsf',
     'PointSource', 'Galaxy', 'ProfileGalaxy', 'HoggGalaxy', 'GaussianGalaxy', 'ExpGalaxy',
     'DevGalaxy', 'SersicGalaxy', 'SersicIndex', 'FracDev', 'SoftenedFracDev',
-    'FixedCompositeGalaxy',
+    'FixedCompositeGalaxy', 'CompositeGalaxy',
     'Tractor', 'Catalog', 'Images', 'B200Optimizer', 'B200ConstrainedOptimizer',
 ]

@@ -127,6 +127,35 @@ class MultiBandBrightness(ParamList):
         return setattr(self, band, value)
 
 
+class Mags(MultiBandBrightness):
+    """Magnitudes in several bands, for MagsPhotoCal (tractor/brightness.py:72-132)."""
+
+    def __init__(self, **kwargs):
+        super(Mags, self).__init__(**kwargs)
+        self.stepsizes = [-0.01] * self.numberOfParams()
+
+    def getMag(self, bandname):
+        return self.getBand(bandname)
+
+    def setMag(self, bandname, mag):
+        return self.setBand(bandname, mag)
+
+    def __add__(self, other):
+        if np.isscalar(other):
+            return Mags(order=self.order, **dict((b, self.getMag(b) + other) for b in self.order))
+        # the magnitude of the summed fluxes
+        return Mags(order=self.order,
+                    **dict((b, -2.5 * np.log10(10. ** (-self.getMag(b) / 2.5) +
+                                               10. ** (-other.getMag(b) / 2.5)))
+                           for b in self.order))
+
+    def __mul__(self, factor):
+        # the magnitude of the flux scaled by |factor|
+        dmag = -2.5 * np.log10(np.abs(factor))
+        return self.__class__(order=self.order,
+                              **dict((b, self.getMag(b) + dmag) for b in self.order))
+
+
 class Fluxes(MultiBandBrightness):
     """tractor/brightness.py:135-161."""
 
@@ -171,6 +200,99 @@ class NanoMaggies(Fluxes):
     @staticmethod
     def magToNanomaggies(mag):
         return 10. ** ((mag - 22.5) / -2.5)
+
+    @staticmethod
+    def fromMag(mag):
+        """NanoMaggies of a Mags (brightness.py:192-198)."""
+        return NanoMaggies(order=mag.order,
+                           **dict((k, NanoMaggies.magToNanomaggies(mag.getMag(k)))
+                                  for k in mag.order))
+
+    @staticmethod
+    def zeropointToScale(zp):
+        """The factor from nanomaggies to counts of a magnitude zeropoint."""
+        return 10. ** ((zp - 22.5) / 2.5)
+
+    @staticmethod
+    def scaleToZeropoint(zpscale):
+        """The magnitude zeropoint of a nanomaggies-to-counts factor."""
+        return 22.5 + 2.5 * np.log10(zpscale)
+
+    @staticmethod
+    def fluxErrorsToMagErrors(flux, flux_invvar):
+        """(mag, mag error) float32 arrays; NaN where the flux or its inverse
+        variance is not positive (brightness.py:228-243)."""
+        flux = np.atleast_1d(flux)
+        flux_invvar = np.atleast_1d(flux_invvar)
+        dflux = np.zeros(len(flux))
+        okiv = flux_invvar > 0
+        dflux[okiv] = 1. / np.sqrt(flux_invvar[okiv])
+        okflux = flux > 0
+        mag = np.zeros(len(flux))
+        mag[okflux] = NanoMaggies.nanomaggiesToMag(flux[okflux])
+        dmag = np.zeros(len(flux))
+        ok = okiv * okflux
+        dmag[ok] = np.abs((-2.5 / np.log(10.)) * dflux[ok] / flux[ok])
+        mag[np.logical_not(okflux)] = np.nan
+        dmag[np.logical_not(ok)] = np.nan
+        return mag.astype(np.float32), dmag.astype(np.float32)
+
+
+class FluxesPhotoCal(BaseParams):
+    """counts = the flux in the calibration's band (brightness.py:246-259)."""
+
+    def __init__(self, band):
+        self.band = band
+        BaseParams.__init__(self)
+
+    def copy(self):
+        return FluxesPhotoCal(self.band)
+
+    def brightnessToCounts(self, brightness):
+        return brightness.getFlux(self.band)
+
+    def hashkey(self):
+        return ('FluxesPhotoCal', self.band)
+
+    def __str__(self):
+        return 'FluxesPhotoCal(band=%s)' % (self.band)
+
+
+class MagsPhotoCal(ParamList):
+    """Zeropoint calibration of Mags: counts = 10^(0.4 (zp - mag)), 0 beyond
+    mag 50 or for a non-finite mag (brightness.py:262-303)."""
+
+    def __init__(self, band, zeropoint):
+        self.band = band
+        self.maxmag = 50.
+        ParamList.__init__(self, zeropoint)
+
+    def copy(self):
+        return MagsPhotoCal(self.band, self.zp)
+
+    @staticmethod
+    def getNamedParams():
+        return dict(zp=0)
+
+    def getStepSizes(self, *args, **kwargs):
+        return [0.01]
+
+    def brightnessToCounts(self, brightness):
+        mag = brightness.getMag(self.band)
+        if not np.isfinite(mag):
+            return 0.
+        if mag > self.maxmag:
+            return 0.
+        return 10. ** (0.4 * (self.zp - mag))
+
+    def countsToMag(self, counts):
+        return self.zp - 2.5 * np.log10(counts)
+
+    def hashkey(self):
+        return ('MagsPhotoCal', self.band, self.zp)
+
+    def __str__(self):
+        return 'MagsPhotoCal(band=%s, zp=%.3f)' % (self.band, self.zp)
 
 
 class NullPhotoCal(BaseParams):
@@ -243,6 +365,13 @@ class ConstantSky(ScalarParam):
 
     def getConstant(self):
         return self.val
+
+    def subtract(self, con):
+        self.val -= con
+
+    def scale(self, s):
+        """Scales the sky level by s."""
+        self.val *= s
 
     def shifted(self, x0, y0):
         return self.copy()

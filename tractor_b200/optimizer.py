@@ -708,3 +708,9 @@ class B200ConstrainedOptimizer(B200Optimizer):
             if do_break:
                 break
         return results
+
+
+# The reference's optimizer names: the same semantics, the least-squares
+# update solved on the device (lsqr_optimizer.py, constrained_optimizer.py).
+LsqrOptimizer = B200Optimizer
+ConstrainedOptimizer = B200ConstrainedOptimizer

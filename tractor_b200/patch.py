@@ -156,6 +156,22 @@ class Patch(object):
     def hasBboxOverlapWith(self, other):
         return self.overlapsBbox(other.getExtent())
 
+    def hasNonzeroOverlapWith(self, other):
+        """Whether the two patches' product has a positive sum over their
+        overlap (patch.py:171-186)."""
+        if not self.hasBboxOverlapWith(other):
+            return False
+        x0, x1, y0, y1 = self.getExtent()
+        ox0, ox1, oy0, oy1 = other.getExtent()
+        ix, ox = get_overlapping_region(ox0, ox1 - 1, x0, x1 - 1)
+        iy, oy = get_overlapping_region(oy0, oy1 - 1, y0, y1 - 1)
+        ix = slice(ix.start - x0, ix.stop - x0)
+        iy = slice(iy.start - y0, iy.stop - y0)
+        sub = self.patch[iy, ix]
+        osub = other.patch[oy, ox]
+        assert sub.shape == osub.shape
+        return np.sum(sub * osub) > 0.
+
     def getNonZeroMask(self):
         return Patch(self.x0, self.y0, self.patch != 0)
 

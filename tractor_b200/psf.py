@@ -181,6 +181,44 @@ class GaussianMixturePSF(MogParams):
     def getMixtureOfGaussians(self, px=None, py=None):
         return self.mog
 
+    def get_wmuvar(self):
+        return (self.mog.amp, self.mog.mean, self.mog.var)
+
+    @classmethod
+    def fromFitsHeader(clazz, hdr, prefix=''):
+        """The PSF from header cards <prefix>P0, P1, ... holding its
+        parameters (psf.py:407-423)."""
+        params = []
+        for i in range(100):
+            k = prefix + 'P%i' % i
+            if k not in hdr:
+                break
+            params.append(hdr.get(k))
+        if len(params) == 0 or (len(params) % 6 != 0):
+            raise RuntimeError('Failed to create %s from FITS header: expected factor of 6 '
+                               'parameters, got %i' % (str(clazz), len(params)))
+        K = len(params) // 6
+        psf = clazz(np.zeros(K), np.zeros((K, 2)), np.zeros((K, 2, 2)))
+        psf.setParams(params)
+        return psf
+
+    def applyTo(self, image):
+        raise RuntimeError('Not implemented')
+
+    def scaleBy(self, factor):
+        """A new mixture with means x factor and variances x factor^2."""
+        return GaussianMixturePSF(self.mog.amp, self.mog.mean * factor,
+                                  self.mog.var * factor ** 2)
+
+    def shiftBy(self, dx, dy):
+        self.mog.mean[:, 0] += dx
+        self.mog.mean[:, 1] += dy
+
+    def computeRadius(self):
+        """getNSigma() x the largest component's largest standard deviation."""
+        meig = max([max(abs(np.linalg.eigvalsh(v))) for v in self.mog.var])
+        return self.getNSigma() * np.sqrt(meig)
+
     def getRadius(self):
         return self.radius
 
@@ -458,6 +496,10 @@ class NCircularGaussianPSF(MultiParams):
 
     def constantPsfAt(self, x, y):
         return self
+
+    def scale(self, factor):
+        """A new PSF factor times wider (psf.py:860-863)."""
+        return NCircularGaussianPSF(np.array(self.mysigmas) * factor, self.myweights)
 
     @property
     def mysigmas(self):

@@ -766,6 +766,93 @@ class SoftenedFracDev(FracDev):
         return 4. * ef / ((ef + 1) ** 2)
 
 
+class CompositeGalaxy(MultiParams, BasicSource):
+    """Exp and deV components sharing a position, each with its own
+    brightness and shape (tractor/galaxy.py:1032-1160): rendered as an
+    ExpGalaxy plus a DevGalaxy in the same plan."""
+
+    def __init__(self, pos, brightnessExp, shapeExp, brightnessDev, shapeDev):
+        MultiParams.__init__(self, pos, brightnessExp, shapeExp, brightnessDev, shapeDev)
+        self.name = self.getName()
+
+    @staticmethod
+    def getNamedParams():
+        return dict(pos=0, brightnessExp=1, shapeExp=2, brightnessDev=3, shapeDev=4)
+
+    def getName(self):
+        return 'CompositeGalaxy'
+
+    def __str__(self):
+        return (self.name + ' at ' + str(self.pos) + ' with Exp ' + str(self.brightnessExp) +
+                ' ' + str(self.shapeExp) + ' and deV ' + str(self.brightnessDev) + ' ' +
+                str(self.shapeDev))
+
+    def getBrightness(self):
+        return self.brightnessExp + self.brightnessDev
+
+    def getBrightnesses(self):
+        return [self.brightnessExp, self.brightnessDev]
+
+    def _parts(self):
+        e = ExpGalaxy(self.pos, self.brightnessExp, self.shapeExp)
+        d = DevGalaxy(self.pos, self.brightnessDev, self.shapeDev)
+        if hasattr(self, 'halfsize'):
+            e.halfsize = d.halfsize = self.halfsize
+        return e, d
+
+    def _plan_model_patch(self, plan, img, minsb=0., modelMask=None, **kwargs):
+        e, d = self._parts()
+        kw = dict(kwargs)
+        if minsb:
+            kw.update(minsb=minsb / 2.)
+        pe = e._plan_model_patch(plan, img, modelMask=modelMask, **kw)
+        pd = d._plan_model_patch(plan, img, modelMask=modelMask, **kw)
+        return Pending(lambda: add_patches(pe.result(), pd.result()))
+
+    def getModelPatch(self, img, minsb=0., modelMask=None, **kwargs):
+        plan = RenderPlan()
+        return self._plan_model_patch(plan, img, minsb=minsb, modelMask=modelMask,
+                                      **kwargs).result()
+
+    def getUnitFluxModelPatches(self, img, minval=0., modelMask=None, **kwargs):
+        if minval > 0:
+            minval = minval * 0.5   # each component half the error
+        e, d = self._parts()
+        return (e.getUnitFluxModelPatches(img, minval=minval, modelMask=modelMask, **kwargs) +
+                d.getUnitFluxModelPatches(img, minval=minval, modelMask=modelMask, **kwargs))
+
+    def _plan_derivatives(self, plan, img, modelMask=None, **kwargs):
+        """galaxy.py:1108-1160: the components' derivatives, the shared
+        position's columns summed."""
+        e, d = self._parts()
+        for frozen, comp, name in (('pos', e, 'pos'), ('pos', d, 'pos'),
+                                   ('brightnessExp', e, 'brightness'), ('shapeExp', e, 'shape'),
+                                   ('brightnessDev', d, 'brightness'), ('shapeDev', d, 'shape')):
+            if self.isParamFrozen(frozen):
+                comp.freezeParam(name)
+        de = e._plan_derivatives(plan, img, modelMask=modelMask, **kwargs)
+        dd = d._plan_derivatives(plan, img, modelMask=modelMask, **kwargs)
+        if self.isParamFrozen('pos'):
+            return list(de) + list(dd)
+        npos = len(self.pos.getStepSizes())
+
+        def pos_sum(i):
+            def finish():
+                a = de[i].result() if de[i] is not None else None
+                b = dd[i].result() if dd[i] is not None else None
+                dp = add_patches(a, b)
+                if dp is not None:
+                    dp.setName('d(comp)/d(pos%i)' % i)
+                return dp
+            return Pending(finish)
+        return [pos_sum(i) for i in range(npos)] + list(de[npos:]) + list(dd[npos:])
+
+    def getParamDerivatives(self, img, modelMask=None, **kwargs):
+        plan = RenderPlan()
+        return [p.result() if p is not None else None
+                for p in self._plan_derivatives(plan, img, modelMask=modelMask, **kwargs)]
+
+
 class FixedCompositeGalaxy(MultiParams, ProfileGalaxy, SingleProfileSource):
     """deV + exp with a shared position and total brightness and a deV
     fraction (tractor/galaxy.py:798-1029)."""
