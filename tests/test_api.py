@@ -544,6 +544,12 @@ def test_small_api_helpers_match_reference():
         o.subtract(0.5)
         o.scale(2.)
     assert sk.getValue() == rsk.getValue()
+    from tractor import mixture_profiles as RMP
+    from tractor_b200 import profiles as P
+    for a, b in ((P.get_exp_mixture(), RMP.get_exp_mixture()),
+                 (P.get_dev_mixture(), RMP.get_dev_mixture())):
+        assert np.array_equal(a.amp, b.amp) and np.array_equal(a.var, b.var)
+    assert P.get_exp_mixture() is not P.get_exp_mixture()
     pa = T.Patch(2, 3, np.ones((4, 5)))
     for other in (T.Patch(5, 5, np.ones((3, 3))), T.Patch(5, 5, np.zeros((3, 3))),
                   T.Patch(20, 20, np.ones((2, 2)))):

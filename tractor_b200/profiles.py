@@ -98,6 +98,18 @@ def dev_mixture():
     return m
 
 
+def get_exp_mixture():
+    """A new copy of the exp profile's mixture (mixture_profiles.py:41-42)."""
+    m = exp_mixture()
+    return MixtureOfGaussians(m.amp.copy(), m.mean.copy(), m.var.copy())
+
+
+def get_dev_mixture():
+    """A new copy of the deV profile's mixture (mixture_profiles.py:44-45)."""
+    m = dev_mixture()
+    return MixtureOfGaussians(m.amp.copy(), m.mean.copy(), m.var.copy())
+
+
 def gaussian_mixture():
     m = MixtureOfGaussians(np.array([1.]), np.zeros((1, 2)), np.array([[[1., 0.], [0., 1.]]]))
     m.normalize()
