@@ -9,23 +9,33 @@ half-size).  Synthetic, seeded.
 
 One step = render every source's model patch from its parameters already in
 device memory: tb_galaxy_fft_prep (profiles, shapes, item geometry) and
-tb_fourier_render (spectrum, FFTs, Lanczos, crop) -- 2 launches.  The metric
+tb_fourier_render_split (spectrum, FFTs, Lanczos, crop: a column kernel and a
+row kernel through an L2-resident scratch, then the persistent kernel for
+items whose Lanczos window reaches the FFT box edge) -- 4 launches.  The metric
 is Mpix x components per second with Npix = sz^2 per source and the
 source's Gaussian component count (SersicGalaxy mixtures have 5-9), summed
 over sources.  L2 is flushed (a 256 MB write) before every timed step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-The JSON line also carries, under "secondary", the batched-scene workload
-(20,000 point / exp / deV / composite sources on one 4096x4096 image through
-a 3-component MoG PSF; prep + binning + one persistent tile render, the
-tile height autotuned), batched blob fitting (2,000 blobs x 3 bands) and the
-dense normal equations on the tensor cores (512 problems x 63 parameters x
-16,384 rows), each with its own end-to-end number, roofline and CPU baseline,
-the small plain fit through the object API (latency-bound: us per render,
-ms per fit), EM fits of 4,096 PSF stamps (GaussianMixturePSF.fromStamp's
-em_fit_2d_reg, FP64) and blob segmentation of a 4096x4096 detection map
-(--no-secondary skips them).
+The JSON line ends with a summary, under "secondary", of the other
+workloads (the full record of each goes to stderr as its own JSON line):
+C3 the batched scene (20,000 point / exp / deV / composite sources on one
+4096x4096 image through a 3-component MoG PSF; prep + binning + one
+persistent tile render, the tile height autotuned), C5 batched blob fitting
+(2,000 blobs x 3 bands; with N GPUs the blobs are cost-balanced over the
+ranks: strong scaling), C4 the seven analytic derivative columns of the
+Fourier path, K5 the dense normal equations on the tensor cores (512
+problems x 63 parameters x 16,384 rows), C1 the small plain fit through the
+object API (latency-bound: us per render, ms per fit), EM fits of 4,096 PSF
+stamps (GaussianMixturePSF.fromStamp's em_fit_2d_reg, FP64) and SEG blob
+segmentation of a 4096x4096 detection map, each with its own end-to-end
+number, roofline and CPU baseline (--no-secondary skips them, --only picks
+some).
+
+With N GPUs the headline workload is one set of 256 x N sources,
+cost-balanced over the ranks (about 256 each: weak scaling), and the ranks'
+patches are all-gathered once after the timed steps.
 
 --impl reference times the reference's CPU implementation of the same
 workload on the host cores (its own compiled C for the spectrum and the
@@ -67,7 +77,44 @@ def parse():
                          'measurements')
     ap.add_argument('--fit-blobs', type=int, default=2000,
                     help='blobs in the blob-fitting measurement (2000 = the full workload)')
+    ap.add_argument('--only', default='',
+                    help='comma-separated secondary measurements to run (C3, C5, C4, K5, C1, '
+                         'EM, SEG); default all')
     return ap.parse_args()
+
+
+def config_keys():
+    """The workload's config, the same in both arms."""
+    return {'workload': WORKLOAD, 'n_sources': N_SOURCES, 'mask': MASK, 'fft_size': 256,
+            'l2': 'flushed before every timed step (256 MB write)'}
+
+
+def _sig(x, d=4):
+    if isinstance(x, float) and np.isfinite(x) and x != 0.:
+        return float('%.*g' % (d, x))
+    return x
+
+
+def compact(sec):
+    """A secondary measurement's key numbers (value, end to end, roofline
+    fraction, CPU baseline, parity) for the main JSON line."""
+    if 'error' in sec:
+        return {'error': sec['error']}
+    c = {'v': _sig(sec.get('value')), 'u': sec.get('unit'), 'ms': _sig(sec.get('ms_per_step'))}
+    if isinstance(sec.get('e2e'), dict):
+        c['e2e'] = _sig(sec['e2e']['value'])
+    rf = sec.get('roofline')
+    if isinstance(rf, dict):
+        c['frac'] = _sig(rf.get('frac'), 3)
+        c['bound'] = rf.get('bound')
+    cb = sec.get('cpu_baseline')
+    if isinstance(cb, dict):
+        c['cpu'] = _sig(cb.get('value'))
+        c['cpu_kind'] = cb.get('kind')
+        c['cores'] = cb.get('cores')
+    for k, v in (sec.get('summary') or {}).items():
+        c[k] = _sig(v, 3) if isinstance(v, float) else v
+    return c
 
 
 # ---------------------------------------------------------------------------
@@ -446,10 +493,17 @@ def bench_fit(args, dev, flush, clk, cpu_seconds):
     data resident in HBM (warm graph), and end to end with the pixels copied
     in from pinned host memory and the parameters copied out."""
     import torch
-    from tractor_b200 import fit
-    n_blobs = args.fit_blobs
-    w = fit.blob_workload(n_blobs, np.random.default_rng(3000))
-    data, inv = fit.render_blobs(w, w['truth'], seed=3001)
+    from tractor_b200 import fit, shard
+    world, rank, _ = init_dist()
+    n_blobs_job = args.fit_blobs
+    w_all = fit.blob_workload(n_blobs_job, np.random.default_rng(3000))
+    # strong scaling: the one fixed set of blobs, cost-balanced over the ranks
+    costs = shard.blob_costs(w_all['blob_src'], w_all['sides'], w_all['sources'],
+                             w_all['start'])
+    own = np.flatnonzero(shard.balance(costs, world) == rank)
+    w = fit.subset_workload(w_all, own) if world > 1 else w_all
+    n_blobs = len(w['sides'])
+    data, inv = fit.render_blobs(w, w['truth'], seed=3001 + rank)
     f = fit.BlobFitter(w['blob_src'], w['sides'], w['psf'], w['sources'], w['start'], data, inv)
     n_src = int(w['blob_src'][-1])
     for _ in range(max(1, min(args.warmup, 2))):
@@ -467,6 +521,25 @@ def bench_fit(args, dev, flush, clk, cpu_seconds):
         times.append(e0.elapsed_time(e1) / 1e3)
     st = f.states()
     fit_s = float(np.mean(times))
+    n_src_job, n_blobs_job_done, gather_ms = n_src, n_blobs, None
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([fit_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        fit_s = float(t.item())
+        t = torch.tensor([n_src, n_blobs], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        n_src_job, n_blobs_job_done = int(t[0].item()), int(t[1].item())
+        # the fit's one collective: every blob's parameters gathered at the end
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        bs = w_all['blob_src']
+        own_src = np.concatenate([np.arange(bs[b], bs[b + 1]) for b in own]) if len(own) else \
+            np.zeros(0, np.int64)
+        shard.gather_units(f.params.view(n_src, fit.NPAR), own_src, int(bs[-1]))
+        g1.record()
+        g1.synchronize()
+        gather_ms = g0.elapsed_time(g1)
     # the dominant kernel at full activity: one pass over every blob
     f.reset(w['start'])
     f._prep()
@@ -509,8 +582,10 @@ def bench_fit(args, dev, flush, clk, cpu_seconds):
     line = {
         'workload': fit_workload_text(n_blobs),
         'metric': 'fitted sources/s (batched LM blob fitting)',
-        'value': n_src / fit_s, 'unit': 'sources/s', 'ms_per_step': fit_s * 1e3,
-        'steps': steps, 'n_sources': n_src, 'n_blobs': n_blobs,
+        'value': n_src_job / fit_s, 'unit': 'sources/s', 'ms_per_step': fit_s * 1e3,
+        'steps': steps, 'n_sources': n_src_job, 'n_blobs': n_blobs_job_done,
+        'scaling': 'strong (one fixed set of blobs, cost-balanced over the ranks)',
+        'gather_ms': gather_ms,
         'iterations_per_fit': float(np.mean(iters)),
         'status': {'converged': int(np.sum(st['status'] == 1)),
                    'stopped': int(np.sum(st['status'] == 2)),
@@ -537,6 +612,169 @@ def bench_fit(args, dev, flush, clk, cpu_seconds):
                                 'sample': '%d sources in whole blobs fitted by the oracle\'s '
                                           'FP64 fitter (central-difference Jacobian), one '
                                           'process per core' % done}
+    return line
+
+
+# ---------------------------------------------------------------------------
+# secondary workload: analytic derivatives of the Fourier path (C4)
+# ---------------------------------------------------------------------------
+
+DERIV_SEED = 1400
+
+
+def deriv_sources():
+    """The derivative workload: the Fourier-path source mix on masks of 32 to
+    128 px (log-uniform; FFT sizes 64 to 256)."""
+    from tractor_b200 import batch
+    rng = np.random.default_rng(DERIV_SEED)
+    masks = np.round(np.exp(rng.uniform(np.log(32), np.log(128), N_SOURCES))).astype(np.int64)
+    return batch.sersic_sources(N_SOURCES, rng, mask=masks)
+
+
+def _deriv_cpu_worker(args):
+    """The reference's finite-difference derivatives of sources [i0, i1):
+    patch0 plus one render per shape parameter and one for the Sersic index
+    (galaxy.py:137-223, sersic.py:402-445; position and flux columns come from
+    patch0), each through the reference's compiled Fourier-path C with
+    galaxy.py's geometry.  Returns (7 x pix*components, seconds, sources)."""
+    i0, i1, use_ref, budget = args
+    sys.path.insert(0, ROOT)
+    os.environ.setdefault('OMP_NUM_THREADS', '1')
+    from oracle import oracle as O
+    from tractor_b200 import batch
+    srcs = deriv_sources()
+    psf = batch.moffat_psf()
+    kern = O.reference_kernels() if use_ref else None
+    cdinv = O.nullwcs_cdinv()
+    work, done = 0., 0
+    t0 = time.perf_counter()
+    for i in range(i0, i1):
+        s = srcs[i]
+        m = int(s['mw'])
+        th = [float(s['s0']), float(s['s1']), float(s['s2']), float(s['sersic_n'])]
+        for j in range(5):
+            t = list(th)
+            if j > 0:
+                t[j - 1] += 0.01
+            amp, var = O.sersic_profile(t[3])
+            T = cdinv @ O.ellipseE_basis(t[0], t[1], t[2])
+            a2, v2 = O.sheared(amp, var, T)
+            _, (_, _, _, _, sz) = O.galaxy_fft_masked(a2, v2, s['px'], s['py'], psf, 0, 0, m, m,
+                                                      kernels=kern)
+            if j == 0:
+                work += 7. * sz * sz * len(amp)
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    return work, time.perf_counter() - t0, done
+
+
+def bench_derivs(args, dev, flush, clk, cpu_seconds):
+    """All seven analytic derivative columns (x, y, counts, r_e, e1, e2, n)
+    of 256 Sersic galaxies on 32-128 px masks (FFT 64-256): Jacobian through
+    tb_galaxy_fft_jac_prep + tb_fourier_render_deriv (one launch of 7 x 256
+    derivative items), and the fused vector-Jacobian product (TB_FFT_DOT).
+    Metric: Mpix x components / s with every column counted as a render."""
+    import ctypes
+    import torch
+    from tractor_b200 import batch, grad, _lib, render
+    srcs = deriv_sources()
+    n = len(srcs)
+    npix = int((srcs['out_off'] + srcs['mw'].astype(np.int64) * srcs['mh']).max())
+    r = batch.FourierGalaxyRenderer(batch.moffat_psf())
+    jac = grad.FourierJacobian(r)
+    h_src = torch.from_numpy(srcs.view(np.uint8).copy()).pin_memory()
+    d_src = h_src.to(dev)
+    out = torch.empty(7 * npix, dtype=torch.float32, device=dev)
+    upstream = torch.randn(npix, generator=torch.Generator(device=dev).manual_seed(7),
+                           device=dev, dtype=torch.float32)
+    dots = torch.zeros(7 * n, dtype=torch.float64, device=dev)
+    for _ in range(max(3, args.warmup)):
+        jac._run(d_src, n, out, _lib.MOG_STORE, npix)
+        jac._run(d_src, n, upstream, _lib.FFT_DOT, 0, dots=dots)
+    torch.cuda.synchronize()
+    flags = jac._work(n)[4].cpu().numpy()
+    assert np.all(flags == 0), 'jac prep flagged sources: %s' % np.unique(flags)
+    items = jac._work(n)[0].cpu().numpy().view(_lib.FFT_ITEM)
+    pixcomp = float(np.sum(items['sz'].astype(np.float64) ** 2 * items['K']))   # 7 columns
+    ex2 = float(np.sum(items['sz'].astype(np.float64) * (items['sz'] // 2 + 1) * items['K']))
+    steps = max(5, min(args.steps, 20))
+    lib = _lib.load()
+    it_t, camp, cvar, dcoef, flg, misc = jac._work(n)
+
+    def timed(mode, o, dts):
+        tt, kt = [], []
+        for _ in range(steps):
+            flush.zero_()
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record()
+            rc = lib.tb_galaxy_fft_jac_prep(d_src.data_ptr(), n, ctypes.addressof(r.image),
+                                            ctypes.addressof(r.tables.struct), it_t.data_ptr(),
+                                            camp.data_ptr(), cvar.data_ptr(), dcoef.data_ptr(),
+                                            batch.COMP_STRIDE, mode,
+                                            npix if mode == _lib.MOG_STORE else 0,
+                                            flg.data_ptr(), _lib.stream_ptr())
+            _lib.check(rc, 'tb_galaxy_fft_jac_prep')
+            e[1].record()
+            render.fourier_render(it_t.data_ptr(), 7 * n, camp.data_ptr(), cvar.data_ptr(),
+                                  r.spec.data_ptr(), o.data_ptr(), misc.data_ptr() + 16,
+                                  dcoef_ptr=dcoef.data_ptr(),
+                                  dots_ptr=None if dts is None else dts.data_ptr())
+            e[2].record()
+            e[2].synchronize()
+            tt.append(e[0].elapsed_time(e[2]) / 1e3)
+            kt.append(e[1].elapsed_time(e[2]) / 1e3)
+        return float(np.mean(tt)), float(np.mean(kt))
+
+    jac_s, jac_k = timed(_lib.MOG_STORE, out, None)
+    vjp_s, vjp_k = timed(_lib.FFT_DOT, upstream, dots)
+    # end to end: records in from pinned memory, the Jacobian out
+    h_out = torch.empty(7 * npix, dtype=torch.float32).pin_memory()
+    e2e = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d_src.copy_(h_src, non_blocking=True)
+        jac._run(d_src, n, out, _lib.MOG_STORE, npix)
+        h_out.copy_(out, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        e2e.append(e0.elapsed_time(e1) / 1e3)
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak_clk = clk['sm_mhz'] if clk else 1965.0
+    peak = SFU_EX2_PER_CLK_PER_SM * nsm * peak_clk * 1e6 / 1e9
+    line = {
+        'name': 'C4 derivatives',
+        'workload': 'C4: 7 analytic columns of 256 Sersic galaxies, masks 32-128 px, FFT 64-256',
+        'metric': 'Mpix*components/s (7 derivative columns, each a render)',
+        'value': pixcomp / jac_s / 1e6, 'unit': 'Mpix*components/s',
+        'ms_per_step': jac_s * 1e3, 'steps': steps,
+        'vjp_ms_per_step': vjp_s * 1e3, 'vjp_value': pixcomp / vjp_s / 1e6,
+        'e2e': {'value': pixcomp / float(np.mean(e2e)) / 1e6, 'unit': 'Mpix*components/s',
+                'h2d_bytes_per_step': int(h_src.numel()),
+                'd2h_bytes_per_step': int(h_out.numel() * 4)},
+        'gpu_launches_per_step': 2 + 2 * (-(-7 * n // 256)),
+        'roofline': {'bound': 'sfu', 'kernel': 'tb_fourier_render_split (Jacobian items)',
+                     'achieved': ex2 / jac_k / 1e9, 'peak': peak, 'unit': 'Gex2/s',
+                     'frac': ex2 / jac_k / 1e9 / peak, 'kernel_ms': jac_k * 1e3,
+                     'algorithmic': '%.0f ex2 per launch' % ex2,
+                     'traffic': ncu_traffic('fourier_deriv_c4.json')},
+    }
+    if cpu_seconds:
+        ncores = os.cpu_count() or 1
+        from oracle import oracle as O
+        use_ref = O.reference_kernels() is not None
+        per = max(1, n // ncores)
+        tasks = [((c * per) % n, min(n, (c * per) % n + per), use_ref, cpu_seconds)
+                 for c in range(ncores)]
+        with mp.get_context('spawn').Pool(ncores) as pool:
+            res = pool.map(_deriv_cpu_worker, tasks)
+        work = sum(x[0] for x in res)
+        busy = max(x[1] for x in res)
+        line['cpu_baseline'] = {'value': work / busy / 1e6, 'unit': 'Mpix*components/s',
+                                'cores': ncores, 'kind': 'reference' if use_ref else 'port',
+                                'sample': '%d sources, 5 finite-difference renders each' %
+                                          sum(x[2] for x in res)}
     return line
 
 
@@ -1070,8 +1308,13 @@ def main():
     build.build()
     _lib.load()
 
-    rng = np.random.default_rng(1000 + rank)
-    srcs = batch.sersic_sources(N_SOURCES, rng, mask=MASK)
+    # one global workload of 256 sources per GPU, cost-balanced over the
+    # ranks (tractor_b200.shard); each rank renders its share
+    from tractor_b200 import shard
+    all_srcs = batch.sersic_sources(N_SOURCES * world, np.random.default_rng(1000), mask=MASK)
+    own = np.flatnonzero(shard.balance(shard.fourier_costs(all_srcs), world) == rank)
+    srcs = all_srcs[own].copy()
+    srcs['out_off'] = np.arange(len(srcs), dtype=np.int64) * MASK * MASK
     renderer = batch.FourierGalaxyRenderer(batch.moffat_psf())
     n = len(srcs)
     nout = n * MASK * MASK
@@ -1108,6 +1351,10 @@ def main():
     clocks = ClockSampler(gpu_id)
     clocks.start()
     time.sleep(0.3)
+    from tractor_b200 import render as R
+    # column + row kernels per 256 items, and the persistent kernel for the
+    # items outside the split path
+    launches_per_render = 2 * (-(-n // 256)) + 1
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     for k in range(args.steps):
@@ -1123,12 +1370,11 @@ def main():
                                     batch.COMP_STRIDE, flg.data_ptr(), _lib.stream_ptr())
         _lib.check(rc, 'tb_galaxy_fft_prep')
         e1.record(stream)
-        rc = lib.tb_fourier_render(items_t.data_ptr(), n, camp.data_ptr(), cvar.data_ptr(),
-                                   renderer.spec.data_ptr(), out.data_ptr(), misc.data_ptr(),
-                                   misc.data_ptr() + 16, _lib.stream_ptr())
-        _lib.check(rc, 'tb_fourier_render')
+        R.fourier_render(items_t.data_ptr(), n, camp.data_ptr(), cvar.data_ptr(),
+                         renderer.spec.data_ptr(), out.data_ptr(), misc.data_ptr() + 16)
         e2.record(stream)
     torch.cuda.synchronize()
+    gpu_launches = (1 + launches_per_render) * args.steps
     step_ms = [a.elapsed_time(c) for a, b, c in ev]
     render_ms = [b.elapsed_time(c) for a, b, c in ev]
     t_total = sum(step_ms) / 1e3
@@ -1136,7 +1382,6 @@ def main():
         t = torch.tensor([t_total], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_total = float(t.item())
-    gpu_launches = 2 * args.steps
 
     # ---- end to end through the host-buffer API (H2D + render + D2H) ----
     ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -1156,11 +1401,25 @@ def main():
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    from tractor_b200 import render as R
-    R.check_status(renderer.status(n).clone(), 'tb_fourier_render')
+    R.check_status(renderer.status(n).clone(), 'tb_fourier_render_split')
 
-    value = world * pixcomp * args.steps / t_total / 1e6
-    e2e = world * pixcomp * args.steps / e2e_s / 1e6
+    job_pixcomp = pixcomp
+    gather_ms = None
+    if world > 1:
+        t = torch.tensor([pixcomp], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        job_pixcomp = float(t.item())
+        # the job's one collective: every rank's patches gathered (fixed-size
+        # rows, one per source) after the timed steps
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        full = shard.gather_units(out.view(len(srcs), MASK * MASK), own, len(all_srcs))
+        g1.record(stream)
+        torch.cuda.synchronize()
+        gather_ms = g0.elapsed_time(g1)
+        del full
+    value = job_pixcomp * args.steps / t_total / 1e6
+    e2e = job_pixcomp * args.steps / e2e_s / 1e6
     kern_s = float(np.mean(render_ms)) / 1e3
     sm_mhz = clk['sm_mhz'] if clk else None
     nsm = torch.cuda.get_device_properties(dev).multi_processor_count
@@ -1172,42 +1431,49 @@ def main():
         'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': t_total / args.steps * 1e3,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
         'data': 'synthetic (seeded)',
-        'config': {'workload': WORKLOAD, 'n_sources_per_gpu': N_SOURCES, 'mask': MASK,
-                   'fft_size': 256, 'pix_components_per_step': pixcomp,
-                   'l2': 'flushed before every timed step (256 MB write)',
-                   'parallelism': 'independent sources per GPU (weak scaling)'},
+        'config': config_keys(),
+        'pix_components_per_step': job_pixcomp,
+        'parallelism': 'cost-balanced sources per GPU, one all-gather after the timed steps',
         'e2e': {'value': e2e, 'unit': 'Mpix*components/s',
                 'h2d_bytes_per_step': int(src_pinned.numel()),
                 'd2h_bytes_per_step': int(out_pinned.numel() * 4)},
         'gpu_launches': gpu_launches,
-        'roofline': {'bound': 'sfu', 'kernel': 'tb_fourier_render',
+        'roofline': {'bound': 'sfu', 'kernel': 'tb_fourier_render_split (column + row kernels)',
                      'achieved': achieved, 'peak': peak, 'unit': 'Gex2/s',
                      'frac': achieved / peak,
-                     'peak_basis': '%d ex2/clk/SM x %d SMs x median SM clock under load '
-                                   '(%s MHz)' % (SFU_EX2_PER_CLK_PER_SM, nsm, peak_clk),
-                     'algorithmic': 'sum over sources of K * sz * (sz/2+1) spectrum '
-                                    'evaluations per launch = %.0f' % ex2_per_launch,
+                     'peak_basis': '%d ex2/clk/SM x %d SMs x %s MHz (median under load)'
+                                   % (SFU_EX2_PER_CLK_PER_SM, nsm, peak_clk),
+                     'algorithmic': '%.0f ex2 (K sz (sz/2+1) per source)' % ex2_per_launch,
                      'kernel_ms': kern_s * 1e3,
                      'traffic': ncu_traffic()},
         'clocks': clk,
     }
+    if gather_ms is not None:
+        line['gather_ms'] = gather_ms
     if not args.no_secondary:
         cpu_s = None if (args.no_cpu_baseline or world > 1 or rank) else min(args.cpu_seconds, 8.0)
-        runs = [('batched scene', lambda: bench_scene(args, dev, flush, clk, cpu_s)),
-                ('blob fitting', lambda: bench_fit(args, dev, flush, clk, cpu_s)),
-                ('normal equations', lambda: bench_normal_equations(
+        runs = [('C3', lambda: bench_scene(args, dev, flush, clk, cpu_s)),
+                ('C5', lambda: bench_fit(args, dev, flush, clk, cpu_s)),
+                ('C4', lambda: bench_derivs(args, dev, flush, clk, cpu_s and min(cpu_s, 6.0))),
+                ('K5', lambda: bench_normal_equations(
                     args, dev, flush, clk, cpu_s and min(cpu_s, 4.0))),
-                ('plain small fit', lambda: bench_plain_small(args, dev)),
-                ('EM PSF fits', lambda: bench_emfit(args, dev, flush, clk,
-                                                    cpu_s and min(cpu_s, 4.0))),
-                ('blob segmentation', lambda: bench_segment(args, dev, flush, clk, cpu_s))]
-        line['secondary'] = []
+                ('C1', lambda: bench_plain_small(args, dev, cpu_s and min(cpu_s, 6.0))),
+                ('EM', lambda: bench_emfit(args, dev, flush, clk, cpu_s and min(cpu_s, 4.0))),
+                ('SEG', lambda: bench_segment(args, dev, flush, clk, cpu_s))]
+        if args.only:
+            runs = [r for r in runs if r[0] in args.only.split(',')]
+        secondary = {}
         for name, run in runs:
             # a secondary line that fails is reported in the line, not fatal
             try:
-                line['secondary'].append(run())
+                full = run()
             except Exception as e:   # noqa: BLE001
-                line['secondary'].append({'workload': name, 'error': repr(e)})
+                full = {'error': repr(e)[:300]}
+            full['name'] = name
+            if rank == 0:
+                # the full record on stderr; the main line carries a summary
+                print(json.dumps(full), file=sys.stderr, flush=True)
+            secondary[name] = compact(full)
     line['plain_fp64'] = fourier_plain_fp64(srcs, out, dev, budget=3.0)
     if line['plain_fp64']['value']:
         line['speedup_vs_plain_fp64'] = value / line['plain_fp64']['value']
@@ -1217,6 +1483,8 @@ def main():
                                 'kind': 'port',
                                 'sample': '%d of the 256 sources rendered by the oracle, one '
                                           'process per core, %.0f s budget' % (nsrc, args.cpu_seconds)}
+    if not args.no_secondary:
+        line['secondary'] = secondary      # last: the part a short tail of the line shows
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -10,7 +10,9 @@
  * launch) that the caller reads after synchronising.  The library allocates
  * no memory: callers own every buffer, including workspaces, and may call
  * from one stream per host thread.  Its only global state is the scratch
- * array of tb_solve_update_noalloc and that array's cached device addresses.
+ * array of tb_solve_update_noalloc with that array's cached per-device
+ * addresses, and the device counter of tensor-core wait timeouts read by
+ * tb_tensor_core_timeouts.
  *
  * Each entry point names the reference interface (file:line in the Tractor
  * source tree) whose computation it replaces.
@@ -75,7 +77,20 @@ typedef struct {
     int64_t tile0;     /* exclusive prefix of tiles (32x32) over items */
     int64_t deriv_off; /* >= 0: also write d/dmean_x and d/dmean_y (times
                           scale), two w x h planes at out + deriv_off */
+    int32_t diff_c0;   /* >= 0: a difference item (see below); -1 otherwise */
+    int32_t pad;
 } tb_mog_item;
+
+/* Difference items (diff_c0 >= 0): the item evaluates
+ *     scale * sum_k [G'_k(x, y) - G_k(x, y)]
+ * where G_k is component c0+k and G'_k component diff_c0+k, both with the
+ * MEAN of component c0+k: the difference of two renders of the same
+ * rectangle (a finite-difference derivative column, e.g. the Sersic-index
+ * step of SersicGalaxy.getParamDerivatives, tractor/sersic.py:416-444)
+ * computed as G_k (s'_k expm1(e'_k - e_k) + (s'_k - s_k)), so that its
+ * error is relative to the difference, not to the two renders.  The floor
+ * is tested on the base exponent.  Requires floor_mode TB_FLOOR_FIXED and
+ * deriv_off < 0. */
 
 /* TB_FLOOR_MINVAL: each component k gets the floor
  * max(-100, log(minval * 2 pi sqrt(det V_k) / sum(amp))), the per-component
@@ -162,6 +177,13 @@ typedef struct {
 #define TB_FFT_DSPEC 1
 #define TB_FFT_DX 2
 #define TB_FFT_DY 3
+/* DIFF renders the difference of two mixtures with the same geometry:
+ * per component the spectrum a'_k exp(-2 pi^2 f^T C'_k f) - a_k exp(-2 pi^2
+ * f^T C_k f) = exp(-2 pi^2 f^T C_k f) (a'_k expm1(-2 pi^2 f^T (C'_k - C_k) f)
+ * + (a'_k - a_k)), from per-component (a'_k - a_k, C'_k - C_k) in
+ * comp_dcoef -- a finite-difference column (the Sersic-index step of
+ * tractor/sersic.py:416-444) with its error relative to the difference. */
+#define TB_FFT_DIFF 4
 /* Output mode of a Fourier item: instead of writing its pixels, accumulate
  * sum over its pixels of out[pixel] * value into dots[dot_off] (out then
  * holds the upstream gradient, read only): the vector-Jacobian product. */
@@ -183,6 +205,25 @@ int tb_fourier_render_deriv(const tb_fft_item* items, int32_t n_items,
                             const double* comp_dcoef, const float* psf_spec, float* out,
                             double* dots, int32_t* work_counter, tb_status* status,
                             void* stream);
+
+/* The same renders (values, derivative items, TB_FFT_DOT) through the
+ * split spectral path: a column kernel (units of 16 packed columns of one
+ * item: the mixture spectrum times the PSF spectrum and the y taps'
+ * response, inverse FFT along y, the DC and Nyquist columns packed into one
+ * complex transform) writes the kept rows of every column to `workspace`
+ * (L2-resident: at most 256 items per column / row launch pair), and a row
+ * kernel (units of 16 kept rows: times the x taps' response, inverse FFT
+ * along x, two real rows per complex transform) writes the output.  Items
+ * whose Lanczos-3 window reaches the FFT box edge, and TB_FFT_DOT items, go
+ * to tb_fourier_render_deriv's kernel in a third launch.  Results equal
+ * tb_fourier_render's up to FP32 rounding.  workspace: device, 256-byte
+ * aligned, at least tb_fourier_workspace(n_items) bytes. */
+int tb_fourier_workspace(int32_t n_items, int64_t* bytes);
+int tb_fourier_render_split(const tb_fft_item* items, int32_t n_items,
+                            const double* comp_amp, const double* comp_var,
+                            const double* comp_dcoef, const float* psf_spec, float* out,
+                            double* dots, void* workspace, int64_t workspace_bytes,
+                            tb_status* status, void* stream);
 
 /* ------------------------------------------------------------------------
  * Galaxy preparation for the Fourier path
@@ -405,7 +446,8 @@ int tb_tensor_core_timeouts(uint32_t* count);
  * writes X[x_off[b] + i] = update / colscale (zero for empty columns).
  * info[b] = 0 ok, >0 the failing pivot (not positive definite; X is then
  * zero, as LsqrOptimizer returns a zero update on failure,
- * lsqr_optimizer.py:586-604), -1 if P[b] > 320.  work: caller-owned FP64
+ * lsqr_optimizer.py:586-604), -1 if P[b] > 320 or P[b] > max_p (the
+ * problem is skipped and its X left as it was).  work: caller-owned FP64
  * scratch of n_problems * max_p * max_p elements (the Cholesky factors). */
 int tb_solve_update(const double* AtA, const double* Atr,
                     const int64_t* ata_off, const int64_t* atr_off,
@@ -428,7 +470,11 @@ int tb_solve_update(const double* AtA, const double* Atr,
  * whose kernels overlap on the GPU (different streams, or different host
  * threads) race and must be serialised by the caller.  The array keeps the
  * previous call's contents; the solver writes every factor entry it reads,
- * so nothing needs clearing.  Allocates nothing (no cudaMalloc / cudaFree). */
+ * so nothing needs clearing.  Allocates nothing (no cudaMalloc / cudaFree).
+ * info[b] as tb_solve_update (-1 for P[b] > max_p: the factors of one
+ * problem never reach another's slice of the array).  The cached address
+ * (an atomic per device) belongs to the device's primary context: after
+ * cudaDeviceReset the library must be unloaded and loaded again. */
 #define TB_SOLVE_NOALLOC_MAX_DOUBLES 1048576
 int tb_solve_update_noalloc(const double* AtA, const double* Atr,
                             const int64_t* ata_off, const int64_t* atr_off,

@@ -11,16 +11,22 @@
 # that only adds exported entry points.  approx3.c, gauss_masked.c and
 # emfit2.c are #included from where they lie in the reference tree.  Nothing here is used by the product path.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]
+# The tree is the argument, else $TRACTOR_REFERENCE_ROOT, else the build
+# container's read-only copy; when none holds tractor/mix.i nothing is built
+# (the GPU machines have no reference tree and use the files built here).
+# The tree used is recorded in oracle/_ref/REFERENCE_ROOT for the Python
+# harness (oracle/refharness.py) and the tests that read reference files.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${TRACTOR_REFERENCE_ROOT:-/root/reference}}"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/tractor/mix.i" ]; then
     echo "build_ref.sh: reference tree not found at $REF; nothing built" >&2
     exit 0
 fi
 mkdir -p "$OUT"
+printf '%s\n' "$REF" > "$OUT/REFERENCE_ROOT"
 
 # Print the bodies of every %{ ... %} / %inline %{ ... %} block, skipping %init.
 extract() {

@@ -27,9 +27,25 @@ import types
 
 import numpy as np
 
-REFERENCE_ROOT = os.environ.get('TRACTOR_REFERENCE_ROOT', '/root/reference')
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _REFLIB = os.path.join(_HERE, '_ref')
+
+
+def reference_root():
+    """The reference source tree: $TRACTOR_REFERENCE_ROOT, else the tree
+    oracle/build_ref.sh compiled from (recorded in oracle/_ref/REFERENCE_ROOT),
+    else None (no reference on this machine)."""
+    env = os.environ.get('TRACTOR_REFERENCE_ROOT')
+    if env:
+        return env
+    try:
+        with open(os.path.join(_REFLIB, 'REFERENCE_ROOT')) as f:
+            return f.read().strip() or None
+    except OSError:
+        return None
+
+
+REFERENCE_ROOT = reference_root() or ''
 
 _loaded = None
 

@@ -14,62 +14,96 @@ from oracle import oracle as O
 
 
 def mog_items(items, amp, mean, var, masks, out):
-    """tb_mog_render's result, item by item, in FP64."""
+    """tb_mog_render's result, item by item, in FP64 (a difference item as
+    the difference of its two mixtures' values, both with the first one's
+    means)."""
     for it in items:
         x0, y0, w, h, c0, K = (int(it[k]) for k in ('x0', 'y0', 'w', 'h', 'c0', 'K'))
-        a = amp[c0:c0 + K]
         m = mean[c0:c0 + K]
-        V = var[c0:c0 + K]
         yy, xx = np.mgrid[y0:y0 + h, x0:x0 + w].astype(np.float64)
         val = np.zeros((h, w))
         gx = np.zeros((h, w))
         gy = np.zeros((h, w))
-        asum = a.sum()
-        for k in range(K):
-            vxx, vyy = V[k, 0, 0], V[k, 1, 1]
-            vxy = 0.5 * (V[k, 0, 1] + V[k, 1, 0])
-            det = vxx * vyy - vxy * vxy
-            q0, q1, q2 = -0.5 * vyy / det, vxy / det, -0.5 * vxx / det
-            s = a[k] / (2 * np.pi * np.sqrt(det))
-            fl = it['floor']
-            if it['floor_mode'] == 1:
-                fl = -100.
-                if it['floor'] > 0:
-                    fl = max(-100., np.log(it['floor'] * 2 * np.pi * np.sqrt(det) / asum))
-            dx = xx - it['fx'] - m[k, 0]
-            dy = yy - it['fy'] - m[k, 1]
-            e = q0 * dx * dx + q1 * dx * dy + q2 * dy * dy
-            G = np.where(e >= fl, s * np.exp(e), 0.)
-            val += G
-            gx += -G * (2 * q0 * dx + q1 * dy)
-            gy += -G * (2 * q2 * dy + q1 * dx)
-        on = np.ones((h, w), bool)
-        if it['mask_off'] >= 0:
-            on = masks[it['mask_off']:it['mask_off'] + w * h].reshape(h, w).astype(bool)
-        sc = float(np.float32(it['scale']))
-        val = np.where(on, val * sc, 0.).astype(np.float32)
-        ldo = int(it['ldo']) if it['ldo'] > 0 else w
-        base = int(it['out_off'])
-        for r in range(h):
-            dst = out[base + r * ldo: base + r * ldo + w]
-            if it['mode'] == 0:
-                dst[:] = val[r]
-            else:
-                dst[:] += val[r]
-        if it['deriv_off'] >= 0:
-            d = int(it['deriv_off'])
-            out[d:d + w * h] = np.where(on, gx * sc, 0.).astype(np.float32).ravel()
-            out[d + w * h:d + 2 * w * h] = np.where(on, gy * sc, 0.).astype(np.float32).ravel()
+        sets = [(c0, 1.)]
+        if it['diff_c0'] >= 0:
+            sets = [(int(it['diff_c0']), 1.), (c0, -1.)]
+        for cs, sign in sets:
+            a = amp[cs:cs + K]
+            V = var[cs:cs + K]
+            asum = a.sum()
+            v, g1, g2 = _mog_values(it, a, m, V, asum, xx, yy)
+            val += sign * v
+            gx += sign * g1
+            gy += sign * g2
+        _mog_store(it, val, gx, gy, masks, out)
 
 
-def fft_items(items, amp, var, specs, out):
-    """tb_fourier_render's result, item by item."""
+def _mog_values(it, a, m, V, asum, xx, yy):
+    """Values and d/dmean planes of one mixture on the pixel grid (xx, yy)."""
+    val = np.zeros(xx.shape)
+    gx = np.zeros(xx.shape)
+    gy = np.zeros(xx.shape)
+    for k in range(len(a)):
+        vxx, vyy = V[k, 0, 0], V[k, 1, 1]
+        vxy = 0.5 * (V[k, 0, 1] + V[k, 1, 0])
+        det = vxx * vyy - vxy * vxy
+        q0, q1, q2 = -0.5 * vyy / det, vxy / det, -0.5 * vxx / det
+        s = a[k] / (2 * np.pi * np.sqrt(det))
+        fl = it['floor']
+        if it['floor_mode'] == 1:
+            fl = -100.
+            if it['floor'] > 0:
+                fl = max(-100., np.log(it['floor'] * 2 * np.pi * np.sqrt(det) / asum))
+        dx = xx - it['fx'] - m[k, 0]
+        dy = yy - it['fy'] - m[k, 1]
+        e = q0 * dx * dx + q1 * dx * dy + q2 * dy * dy
+        G = np.where(e >= fl, s * np.exp(e), 0.)
+        val += G
+        gx += -G * (2 * q0 * dx + q1 * dy)
+        gy += -G * (2 * q2 * dy + q1 * dx)
+    return val, gx, gy
+
+
+def _mog_store(it, val, gx, gy, masks, out):
+    """Writes one item's planes as the kernel does (mask, scale, mode)."""
+    w, h = int(it['w']), int(it['h'])
+    on = np.ones((h, w), bool)
+    if it['mask_off'] >= 0:
+        on = masks[it['mask_off']:it['mask_off'] + w * h].reshape(h, w).astype(bool)
+    sc = float(np.float32(it['scale']))
+    val = np.where(on, val * sc, 0.).astype(np.float32)
+    ldo = int(it['ldo']) if it['ldo'] > 0 else w
+    base = int(it['out_off'])
+    for r in range(h):
+        dst = out[base + r * ldo: base + r * ldo + w]
+        if it['mode'] == 0:
+            dst[:] = val[r]
+        else:
+            dst[:] += val[r]
+    if it['deriv_off'] >= 0:
+        d = int(it['deriv_off'])
+        out[d:d + w * h] = np.where(on, gx * sc, 0.).astype(np.float32).ravel()
+        out[d + w * h:d + 2 * w * h] = np.where(on, gy * sc, 0.).astype(np.float32).ravel()
+
+
+def fft_items(items, amp, var, specs, out, dcoef=None):
+    """tb_fourier_render's result, item by item (a TB_FFT_DIFF item as the
+    FP64 difference of its two mixtures' spectra)."""
     for it in items:
         c0, K, N = int(it['c0']), int(it['K']), int(it['sz'])
         NH = N // 2 + 1
         so = int(it['spec_off'])
         P = specs[so:so + 2 * N * NH].view(np.complex64).reshape(NH, N).T
-        F = O.fourier_mog(amp[c0:c0 + K], var[c0:c0 + K], np.fft.rfftfreq(N), np.fft.fftfreq(N))
+        fv, fw = np.fft.rfftfreq(N), np.fft.fftfreq(N)
+        F = O.fourier_mog(amp[c0:c0 + K], var[c0:c0 + K], fv, fw)
+        if it['dmode'] == 4:
+            dc = dcoef[int(it['dc0']):int(it['dc0']) + K]
+            V2 = var[c0:c0 + K].copy()
+            V2[:, 0, 0] += dc[:, 1]
+            V2[:, 0, 1] += dc[:, 2]
+            V2[:, 1, 0] += dc[:, 2]
+            V2[:, 1, 1] += dc[:, 3]
+            F = O.fourier_mog(amp[c0:c0 + K] + dc[:, 0], V2, fv, fw) - F
         G = np.fft.irfftn(F * P).astype(np.float32)
         if it['mux'] != 0 or it['muy'] != 0:
             G = O.lanczos_shift(G, it['mux'], it['muy'])
@@ -118,7 +152,8 @@ def install(monkeypatch):
         if self.items:
             items = np.array(self.items, dtype=_lib.FFT_ITEM)
             specs = torch.cat(self.spec_list).numpy()
-            fft_items(items, np.concatenate(self.amp), np.concatenate(self.var), specs, out.numpy())
+            fft_items(items, np.concatenate(self.amp), np.concatenate(self.var), specs, out.numpy(),
+                      np.concatenate(self.dcoef) if self.dcoef else None)
         self.status = torch.zeros(16, dtype=torch.uint8)
         return out
 
@@ -228,4 +263,13 @@ def install(monkeypatch):
     monkeypatch.setattr(render, 'lanczos_shift', lanczos)
     monkeypatch.setattr(render, 'normal_equations', normal_equations)
     monkeypatch.setattr(render, 'solve_update', solve_update)
+
+    def solve_dense(A_colmajor, b, damp=0., stream=None):
+        A = torch.from_numpy(np.ascontiguousarray(A_colmajor, np.float32).ravel())
+        P, R = A_colmajor.shape
+        AtA, Atr, ao, ro = normal_equations(A, torch.from_numpy(np.asarray(b, np.float32)),
+                                            [0], [0], [R], [P], [R])
+        X, info, _ = solve_update(AtA, Atr, ao, ro, [P], damp=damp)
+        return X.numpy(), int(info[0])
+    monkeypatch.setattr(render, 'solve_dense', solve_dense)
     render._spectra.cache.clear()

@@ -15,6 +15,7 @@ root in the development container:
     python tests/golden/make_golden.py forcedsky # forced_sky.npz
     python tests/golden/make_golden.py varying  # varying_psf.npz
     python tests/golden/make_golden.py composite # composite.npz
+    python tests/golden/make_golden.py fittight # fit_plain_tight.npz
 """
 import os
 import sys
@@ -679,8 +680,62 @@ def composite():
     print('composite fixture written to', OUT)
 
 
+def fittight():
+    """The optimum of the small plain fit (scenario 4) in FP64, found on the
+    reference's own FP64 model: scipy.optimize.least_squares on
+    Tractor.getChiImage (tolerances 1e-15) from the scenario's start.  Stored
+    with its log-probability and the Fisher matrix A^T A of the reference's
+    derivative columns there (inverse errors 1; the position columns divided
+    by NullWCS's cd_inverse of 3600 so that the matrix is per pixel), whose
+    inverse gives the parameters' sigmas.  Also the reference's own
+    LsqrOptimizer.optimize_loop(dchisq=1e-10) started at the optimum with the
+    flux and shape moved (0, 0, +20, +0.05, +0.02, -0.02): its end point and
+    step count.  (From the scenario's start the reference's optimizer needs
+    many thousands of steps: NullWCS scales the position derivatives by
+    3600, which shrinks every position step by that factor.)"""
+    from oracle import refharness
+    refharness.load()
+    from scipy.optimize import least_squares
+    from tractor import (Image, PixPos, Flux, LinearPhotoCal, NCircularGaussianPSF, EllipseE,
+                         ExpGalaxy, Tractor)
+    g = np.load(os.path.join(OUT, 'fit_plain.npz'))
+    timc = Image(data=g['data'], invvar=np.ones((64, 64)),
+                 psf=NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2]), photocal=LinearPhotoCal(1.))
+    src = ExpGalaxy(PixPos(32.5, 32.5), Flux(800.), EllipseE.fromRAbPhi(2.4, 0.6, 30.))
+    tr = Tractor([timc], [src])
+    tr.modtype = np.float64
+    tr.freezeParam('images')
+
+    def resid(p):
+        tr.setParams(p)
+        return tr.getChiImage(0).ravel().astype(np.float64)
+    r = least_squares(resid, np.array(tr.getParams()), x_scale=[0.03, 0.03, 10., 0.05, 0.02, 0.02],
+                      xtol=1e-15, ftol=1e-15, gtol=1e-15, diff_step=1e-7)
+    p_opt = r.x
+    tr.setParams(p_opt)
+    lnp = tr.getLogProb()
+    cols = []
+    for k, d in enumerate(src.getParamDerivatives(timc)):
+        full = np.zeros((64, 64))
+        d.addTo(full)
+        cols.append(full.ravel() / (3600. if k < 2 else 1.))
+    A = np.array(cols)
+    fisher = A @ A.T
+    pert = np.array([0., 0., 20., 0.05, 0.02, -0.02])
+    tr.setParams(p_opt + pert)
+    R = tr.optimize_loop(dchisq=1e-10, steps=300)
+    p_ref = np.array(tr.getParams())
+    np.savez_compressed(os.path.join(OUT, 'fit_plain_tight.npz'), p_opt=p_opt, lnp=lnp,
+                        fisher=fisher, pert=pert, p_ref_from_pert=p_ref, ref_steps=R['steps'])
+    sig = np.sqrt(np.diag(np.linalg.inv(fisher)))
+    print('fit_plain_tight fixture written to', OUT, 'reference from the moved start:',
+          R['steps'], 'steps,', np.abs(p_ref - p_opt) / sig, 'sigma')
+
+
 if __name__ == '__main__':
-    if sys.argv[1:] == ['hybrid']:
+    if sys.argv[1:] == ['fittight']:
+        fittight()
+    elif sys.argv[1:] == ['hybrid']:
         hybrid()
     elif sys.argv[1:] == ['psfex']:
         psfex()

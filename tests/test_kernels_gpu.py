@@ -157,6 +157,70 @@ def test_fourier_render_matches_oracle(tb, oracle, sz, mw, mh):
         assert np.abs(got - ref).max() / peak < PEAK_TOL, np.abs(got - ref).max() / peak
 
 
+def test_split_path_matches_persistent_kernel(tb, oracle):
+    """tb_fourier_render_split (column and row kernels through the scratch,
+    the box-edge items by the persistent kernel) against tb_fourier_render
+    (the persistent kernel alone) on the same items: 300 galaxies of every
+    FFT size (more than one column / row launch pair), windows inside and at
+    the edge of the box, store and accumulate modes, and a difference item."""
+    import torch
+    from tractor_b200 import render, _lib
+    rng = np.random.default_rng(31)
+    b = render.FftBatch()
+    spec_keys = {}
+    for i in range(300):
+        sz = [32, 64, 128, 256][i % 4]
+        mw = int(rng.integers(8, sz // 2 + 8))
+        mh = int(rng.integers(8, sz // 2 + 8))
+        psf = _moffat(63 if sz >= 128 else (31 if sz == 64 else 15))
+        if sz not in spec_keys:
+            spec_keys[sz] = render.psf_spectra().get(('split-test', sz), psf, sz)
+        spec, cx, cy = spec_keys[sz]
+        amp, var_s = oracle.exp_profile() if i % 3 else oracle.dev_profile()
+        T = rng.normal(size=(2, 2)) * rng.uniform(0.3, 2.5)
+        amp2, var2 = oracle.sheared(amp, var_s, T)
+        sx, sy = int(rng.integers(-6, 4)), int(rng.integers(-6, 4))
+        mux, muy = rng.uniform(-0.5, 0.5, 2)
+        diff = None
+        if i % 17 == 0:
+            diff = (amp2 * 1.01, var2 * 1.02)
+        b.add(amp2, var2, sz, ('split-test', sz), spec, mw, mh, sx, sy, mux, muy,
+              scale=float(rng.uniform(0.5, 2)), diff=diff)
+    items = np.array(b.items, dtype=_lib.FFT_ITEM)
+    dev = torch.device('cuda')
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    d_items = t(items.view(np.uint8))
+    amp, var = t(np.concatenate(b.amp)), t(np.concatenate(b.var))
+    dcoef = t(np.concatenate(b.dcoef))
+    specs = torch.cat(b.spec_list)
+    lib = _lib.load()
+    out0 = torch.full((b.nout,), 7.0, dtype=torch.float32, device=dev)
+    misc = torch.zeros(8, dtype=torch.int32, device=dev)
+    rc = lib.tb_fourier_render_deriv(d_items.data_ptr(), len(items), amp.data_ptr(),
+                                     var.data_ptr(), dcoef.data_ptr(), specs.data_ptr(),
+                                     out0.data_ptr(), None, misc.data_ptr(), misc.data_ptr() + 16,
+                                     None)
+    assert rc == 0
+    out1 = torch.full((b.nout,), 7.0, dtype=torch.float32, device=dev)
+    render.fourier_render(d_items.data_ptr(), len(items), amp.data_ptr(), var.data_ptr(),
+                          specs.data_ptr(), out1.data_ptr(), misc.data_ptr() + 16,
+                          dcoef_ptr=dcoef.data_ptr())
+    torch.cuda.synchronize()
+    render.check_status(misc[4:8].clone(), 'tb_fourier_render_split')
+    a, c = out0.cpu().numpy(), out1.cpu().numpy()
+    for it in items:
+        o, n = int(it['out_off']), int(it['mw'] * it['mh'])
+        pa, pc = a[o:o + n], c[o:o + n]
+        peak = max(np.abs(pa).max(), 1e-30)
+        assert np.abs(pa - pc).max() <= 1e-6 * peak, (it, np.abs(pa - pc).max() / peak)
+    # a second call over the scratch the first left behind gives the same pixels
+    out2 = torch.zeros_like(out1)
+    render.fourier_render(d_items.data_ptr(), len(items), amp.data_ptr(), var.data_ptr(),
+                          specs.data_ptr(), out2.data_ptr(), misc.data_ptr() + 16,
+                          dcoef_ptr=dcoef.data_ptr())
+    assert torch.equal(out1, out2)
+
+
 def test_normal_equations_and_solve(tb):
     import torch
     from tractor_b200 import render

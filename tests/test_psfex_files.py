@@ -14,7 +14,12 @@ import types
 import numpy as np
 import pytest
 
-REF_TEST = os.path.join(os.environ.get('TRACTOR_REFERENCE_ROOT', '/root/reference'), 'test')
+def _ref_test_dir():
+    from oracle import refharness
+    return os.path.join(refharness.reference_root() or '', 'test')
+
+
+REF_TEST = _ref_test_dir()
 FILES = ['psfex-decam-00392360-S31.fits', 'c4d_140717_065122_ooi_i_ls11-S2-se.psf']
 OVERSAMPLED = 'c4d_140818_002108_ooi_z_v1.ext27.psf'
 

@@ -19,14 +19,14 @@ MOG_ITEM = np.dtype([('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'), ('h', '<i4'),
                      ('fx', '<f8'), ('fy', '<f8'), ('floor', '<f8'),
                      ('scale', '<f4'), ('floor_mode', '<i4'),
                      ('out_off', '<i8'), ('mask_off', '<i8'), ('tile0', '<i8'),
-                     ('deriv_off', '<i8')])
+                     ('deriv_off', '<i8'), ('diff_c0', '<i4'), ('pad', '<i4')])
 FLOOR_FIXED, FLOOR_MINVAL = 0, 1
 FFT_ITEM = np.dtype([('c0', '<i4'), ('K', '<i4'), ('sz', '<i4'), ('mode', '<i4'),
                      ('mw', '<i4'), ('mh', '<i4'), ('sx', '<i4'), ('sy', '<i4'),
                      ('mux', '<f8'), ('muy', '<f8'), ('scale', '<f4'), ('ldo', '<i4'),
                      ('out_off', '<i8'), ('spec_off', '<i8'), ('dmode', '<i4'), ('dc0', '<i4'),
                      ('dot_off', '<i8')])
-FFT_VALUE, FFT_DSPEC, FFT_DX, FFT_DY = 0, 1, 2, 3
+FFT_VALUE, FFT_DSPEC, FFT_DX, FFT_DY, FFT_DIFF = 0, 1, 2, 3, 4
 FFT_DOT = 3
 STATUS = np.dtype([('code', '<i4'), ('item', '<i4'), ('detail', '<i4'), ('count', '<i4')])
 GALAXY_SRC = np.dtype([('px', '<f8'), ('py', '<f8'), ('counts', '<f8'), ('s0', '<f8'),
@@ -119,6 +119,8 @@ SIGNATURES = {
     'tb_galaxy_fft_jac_prep': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _I32, _I32, _I64, _P,
                                       _P]),
     'tb_fourier_render_deriv': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    'tb_fourier_workspace': (_I32, [_I32, _P]),
+    'tb_fourier_render_split': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _P, _I64, _P, _P]),
     'tb_scene_prep': (_I32, [_P, _I32, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P]),
     'tb_scene_workspace': (_I32, [_I64, _I64, _P]),
     'tb_fit_workspace': (_I32, [_I32, _I32, _P]),

@@ -2,9 +2,10 @@
 
 FourierGalaxyRenderer renders thousands of galaxies through the
 pixelized-PSF Fourier path of ProfileGalaxy._realGetUnitFluxModelPatch
-(tractor/galaxy.py:336-519) in two launches: tb_galaxy_fft_prep turns source
-parameters into work items and component tables on the device, and
-tb_fourier_render renders every item in one persistent launch.
+(tractor/galaxy.py:336-519): tb_galaxy_fft_prep turns source parameters into
+work items and component tables on the device, and tb_fourier_render_split
+renders every item (column and row kernels, 256 items per pair, and the
+persistent kernel for the few items they do not cover).
 """
 import ctypes
 
@@ -136,10 +137,9 @@ class FourierGalaxyRenderer(object):
                                     camp.data_ptr(), cvar.data_ptr(), COMP_STRIDE,
                                     flags.data_ptr(), s)
         _lib.check(rc, 'tb_galaxy_fft_prep')
-        rc = lib.tb_fourier_render(items.data_ptr(), n, camp.data_ptr(), cvar.data_ptr(),
-                                   self.spec.data_ptr(), out.data_ptr(), misc.data_ptr(),
-                                   misc.data_ptr() + 16, s)
-        _lib.check(rc, 'tb_fourier_render')
+        render.fourier_render(items.data_ptr(), n, camp.data_ptr(), cvar.data_ptr(),
+                              self.spec.data_ptr(), out.data_ptr(), misc.data_ptr() + 16,
+                              stream=stream)
         return flags
 
     def status(self, n):
@@ -167,10 +167,12 @@ class FourierGalaxyRenderer(object):
 
 
 def sersic_sources(n, rng, mask=128, pos_jitter=0.5, flux=1000.):
-    """Seeded synthetic Sersic galaxies each on its own mask x mask patch:
+    """Seeded synthetic Sersic galaxies each on its own mask x mask patch
+    (`mask` a size, or one size per source; patches packed back to back):
     n ~ U[0.7, 6], r_e log-uniform in [0.5, 8] px, axis ratio U[0.2, 1],
     phi U[0, 180) deg, centre offset U[-0.5, 0.5] px (EllipseE shapes,
     pixel scale 1)."""
+    mask = np.broadcast_to(np.asarray(mask, np.int64), (n,))
     srcs = np.zeros(n, GALAXY_SRC)
     ns = rng.uniform(0.7, 6.0, n)
     re = np.exp(rng.uniform(np.log(0.5), np.log(8.0), n))
@@ -193,7 +195,7 @@ def sersic_sources(n, rng, mask=128, pos_jitter=0.5, flux=1000.):
     srcs['my0'] = 0
     srcs['mw'] = mask
     srcs['mh'] = mask
-    srcs['out_off'] = np.arange(n, dtype=np.int64) * mask * mask
+    srcs['out_off'] = np.concatenate([[0], np.cumsum(mask * mask)[:-1]])
     return srcs
 
 

@@ -138,6 +138,29 @@ __device__ __forceinline__ void dspectrum8(const float4* comp, const float4* dco
     }
 }
 
+// Difference spectrum (TB_FFT_DIFF): acc[m] = sum_k exp2(e_k) (a'_k
+// expm1(de_k) + (a'_k - a_k)), de_k = dca v^2 + dcb v w + dcd w^2 the
+// exponent change in natural-log units; dcomp = (a'_k - a_k, dca, dcb, dcd).
+__device__ __forceinline__ void diffspectrum8(const float4* comp, const float4* dcomp, int K,
+                                              float vf, const float* wf, float* acc) {
+#pragma unroll
+    for (int m = 0; m < 8; m++) acc[m] = 0.f;
+    for (int k = 0; k < K; k++) {
+        const float4 c = comp[k];
+        const float4 d = dcomp[k];
+        const float al = c.y * vf * vf, be = c.z * vf;
+        const float d0 = d.y * vf * vf, d1 = d.z * vf;
+        const float a2 = c.x + d.x;
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const float e = fmaf(wf[m], fmaf(c.w, wf[m], be), al);
+            const float de = fmaf(wf[m], fmaf(d.w, wf[m], d1), d0);
+            const float pre = fmaf(a2, expm1f(de), d.x);
+            acc[m] = fmaf(pre, tb::ex2(e), acc[m]);
+        }
+    }
+}
+
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) { return tb::cmul(a, b); }
 __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
 
@@ -215,6 +238,8 @@ __device__ void render_item_spectral(const tb_fft_item& it, int K, const float* 
             }
             if (kDeriv && it.dmode == TB_FFT_DSPEC)
                 dspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
+            else if (kDeriv && it.dmode == TB_FFT_DIFF)
+                diffspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
             else
                 spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
             float2 x[8];
@@ -312,6 +337,8 @@ __device__ void render_item_spatial(const tb_fft_item& it, int K, const float* _
             }
             if (kDeriv && it.dmode == TB_FFT_DSPEC)
                 dspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
+            else if (kDeriv && it.dmode == TB_FFT_DIFF)
+                diffspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
             else
                 spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
             float2 x[8];
@@ -437,7 +464,9 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
                       const double* __restrict__ amp, const double* __restrict__ var,
                       const double* __restrict__ dcoef, const float* __restrict__ psf_spec,
                       float* __restrict__ out, double* __restrict__ dots, int32_t* counter,
-                      tb_status* st) {
+                      tb_status* st, const int32_t* __restrict__ list = nullptr,
+                      const int32_t* __restrict__ list_count = nullptr) {
+    // `list` (optional): render only items list[0 .. *list_count)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Shared sh;
     unsigned char* p = smem_raw;
@@ -460,14 +489,17 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
     __shared__ int cur_n;
     if (threadIdx.x == 0) cur_n = 0;
 
+    const int64_t n_units = list ? (int64_t)*list_count : (int64_t)n_items;
     for (;;) {
-        const int64_t u = tb::next_unit(counter, &slot);
-        if (u >= n_items) break;
+        const int64_t uu = tb::next_unit(counter, &slot);
+        if (uu >= n_units) break;
+        const int64_t u = list ? (int64_t)list[uu] : uu;
         const tb_fft_item& it = items[u];
         const int N = it.sz, K = it.K;
         const bool okN = N == 32 || N == 64 || N == 128 || N == 256;
-        const bool okD = kDeriv ? (it.dmode >= TB_FFT_VALUE && it.dmode <= TB_FFT_DY &&
-                                   (it.dmode != TB_FFT_DSPEC || dcoef != nullptr) &&
+        const bool okD = kDeriv ? (it.dmode >= TB_FFT_VALUE && it.dmode <= TB_FFT_DIFF &&
+                                   ((it.dmode != TB_FFT_DSPEC && it.dmode != TB_FFT_DIFF) ||
+                                    dcoef != nullptr) &&
                                    (it.mode != TB_FFT_DOT || dots != nullptr))
                                 : (it.dmode == TB_FFT_VALUE && it.mode != TB_FFT_DOT);
         if (!okN || !okD || K < 0 || K > kMaxK || it.mw <= 0 || it.mh <= 0 ||
@@ -488,6 +520,13 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
                 const double m2 = -2.0 * TB_PI * TB_PI * amp[c];
                 sh.dcomp[k] = make_float4((float)dc[0], (float)(m2 * dc[1]),
                                           (float)(m2 * 2.0 * dc[2]), (float)(m2 * dc[3]));
+            }
+            if (kDeriv && it.dmode == TB_FFT_DIFF) {
+                // (a' - a, exponent change -2 pi^2 f^T (C' - C) f in natural-log units)
+                const double* dc = dcoef + 4 * ((int64_t)it.dc0 + k);
+                const double n2 = -2.0 * TB_PI * TB_PI;
+                sh.dcomp[k] = make_float4((float)dc[0], (float)(n2 * dc[1]),
+                                          (float)(n2 * 2.0 * dc[2]), (float)(n2 * dc[3]));
             }
         }
         if (threadIdx.x == 32) {
@@ -536,6 +575,376 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Split spectral path (tb_fourier_render_split): a column kernel and a row
+// kernel joined by an L2-resident scratch, for every item whose Lanczos-3
+// shift is a spectral product (render_item's xin && yin) and whose output is
+// written or added (not TB_FFT_DOT).  Work units are small -- 16 packed
+// columns or 16 kept rows of one item -- so every SM runs several CTAs of
+// 8 warps and the units of 256 galaxies spread evenly over the SMs; the
+// persistent kernel above holds one galaxy per SM and needs the whole
+// sz x (sz/2+1) transpose in its 180 KB of shared memory.
+//
+// Packed columns: c = 0 holds the DC column v = 0 in the real and the
+// Nyquist column v = N/2 in the imaginary part (both transform to real
+// columns, so one complex FFT does both); c = 1 .. N/2-1 are v = c.
+// Scratch: per item, column-major over packed columns, the kept rows
+// [gr0, gr1) of each column transform: S1[c * (gr1 - gr0) + (row - gr0)].
+// Items that are not eligible are appended to a list for the persistent
+// kernel (third launch).
+// ---------------------------------------------------------------------------
+constexpr int kSplitThreads = 256;
+constexpr int kSplitWarps = kSplitThreads / 32;
+constexpr int kColBlock = 16;                 // packed columns per column unit
+constexpr int kRowBlock = 16;                 // kept rows per row unit
+constexpr int kColUnits = 128 / kColBlock;    // per item at N = 256
+constexpr int kRowUnits = 256 / kRowBlock;
+constexpr int64_t kS1PerItem = 256 * 128;     // float2 per item (N x N/2 at N = 256)
+
+struct SplitWs {
+    int32_t col_counter, row_counter, fb_counter, fb_count;
+    int32_t pad[60];
+};
+
+__device__ __forceinline__ bool split_eligible(const tb_fft_item& it) {
+    const int N = it.sz;
+    const int gr0 = max(0, -it.sy), gr1 = min(N, it.mh - it.sy);
+    const int gc0 = max(0, -it.sx), gc1 = min(N, it.mw - it.sx);
+    const bool xin = (it.mux == 0.0 && it.dmode != TB_FFT_DX) || (gc0 >= 3 && gc1 <= N - 3);
+    const bool yin = (it.muy == 0.0 && it.dmode != TB_FFT_DY) || (gr0 >= 3 && gr1 <= N - 3);
+    return xin && yin && it.mode != TB_FFT_DOT;
+}
+
+__device__ __forceinline__ bool item_ok(const tb_fft_item& it, const double* dcoef) {
+    const int N = it.sz;
+    return (N == 32 || N == 64 || N == 128 || N == 256) && it.dmode >= TB_FFT_VALUE &&
+           it.dmode <= TB_FFT_DIFF &&
+           ((it.dmode != TB_FFT_DSPEC && it.dmode != TB_FFT_DIFF) || dcoef != nullptr) &&
+           it.K >= 0 && it.K <= kMaxK && it.mw > 0 && it.mh > 0 && fabs(it.mux) <= 0.5 &&
+           fabs(it.muy) <= 0.5;
+}
+
+// Normalised Lanczos-3 taps (or their derivative) with 7 threads in parallel
+// (the same terms and order as taps3 / taps3_deriv).
+__device__ void taps_parallel(double dx, bool deriv, float* f) {
+    // taps3 / taps3_deriv evaluated by one thread each: small (7 terms); the
+    // other threads wait at the caller's barrier
+    if (threadIdx.x % 32 == 0) {
+        if (deriv) taps3_deriv(dx, f); else taps3(dx, f);
+    }
+}
+
+struct SplitColShared {
+    float2 tw[256];
+    float4 comp[kMaxK];
+    float4 dcomp[kMaxK];
+    float taps[8];
+    float2 hy[256];
+    float2 xbuf[kSplitWarps * kXbufPerWarp];
+    int cur_n;
+    int64_t slot;
+};
+
+__device__ void stage_components(const tb_fft_item& it, const double* __restrict__ amp,
+                                 const double* __restrict__ var, const double* __restrict__ dcoef,
+                                 float4* comp, float4* dcomp) {
+    const double c2 = -2.0 * TB_PI * TB_PI * TB_LOG2E;
+    for (int k = threadIdx.x; k < it.K; k += kSplitThreads) {
+        const int c = it.c0 + k;
+        const double a = var[4 * c], bb = var[4 * c + 1], d = var[4 * c + 3];
+        comp[k] = make_float4((float)amp[c], (float)(c2 * a), (float)(c2 * 2.0 * bb),
+                              (float)(c2 * d));
+        if (it.dmode == TB_FFT_DSPEC) {
+            const double* dc = dcoef + 4 * ((int64_t)it.dc0 + k);
+            const double m2 = -2.0 * TB_PI * TB_PI * amp[c];
+            dcomp[k] = make_float4((float)dc[0], (float)(m2 * dc[1]), (float)(m2 * 2.0 * dc[2]),
+                                   (float)(m2 * dc[3]));
+        } else if (it.dmode == TB_FFT_DIFF) {
+            const double* dc = dcoef + 4 * ((int64_t)it.dc0 + k);
+            const double n2 = -2.0 * TB_PI * TB_PI;
+            dcomp[k] = make_float4((float)dc[0], (float)(n2 * dc[1]), (float)(n2 * 2.0 * dc[2]),
+                                   (float)(n2 * dc[3]));
+        }
+    }
+}
+
+// Spectrum of column v for the 8 rows of one thread, by item mode.
+__device__ __forceinline__ void spectrum_any(const tb_fft_item& it, const float4* comp,
+                                             const float4* dcomp, float vf, const float* wf,
+                                             float* acc) {
+    if (it.dmode == TB_FFT_DSPEC) dspectrum8(comp, dcomp, it.K, vf, wf, acc);
+    else if (it.dmode == TB_FFT_DIFF) diffspectrum8(comp, dcomp, it.K, vf, wf, acc);
+    else spectrum8(comp, it.K, vf, wf, acc);
+}
+
+template <int N>
+__device__ void split_col_unit(const tb_fft_item& it, int cb, const float* __restrict__ spec,
+                               float2* __restrict__ s1, SplitColShared& sh) {
+    constexpr int NH = N / 2;             // packed columns
+    constexpr int T = N / 8;
+    constexpr int GPW = 32 / T;
+    constexpr int XB = tb::fft_xbuf_elems<N>();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = lane % T;
+    float2* xb = sh.xbuf + warp * kXbufPerWarp + (lane / T) * XB;
+    const int gr0 = max(0, -it.sy), gr1 = min(N, it.mh - it.sy);
+    const int nr = gr1 - gr0;
+    const int cend = min(NH, (cb + 1) * kColBlock);
+    float wf[8];
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        const int j = t + m * T;
+        wf[m] = (float)(j < N / 2 ? j : j - N) / (float)N;
+    }
+    for (int c0 = cb * kColBlock + warp * GPW; c0 < cend; c0 += kSplitWarps * GPW) {
+        const bool act = c0 + lane / T < cend;
+        const int c = act ? c0 + lane / T : cend - 1;
+        float2 x[8];
+        if (c == 0) {
+            // DC (v = 0) + i Nyquist (v = N/2)
+            float a0[8], a1[8];
+            spectrum_any(it, sh.comp, sh.dcomp, 0.f, wf, a0);
+            spectrum_any(it, sh.comp, sh.dcomp, 0.5f, wf, a1);
+            const float2* P0 = reinterpret_cast<const float2*>(spec);
+            const float2* P1 = reinterpret_cast<const float2*>(spec) + (int64_t)(N / 2) * N;
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const int j = t + m * T;
+                const float2 p0 = __ldg(P0 + j), p1 = __ldg(P1 + j);
+                const float2 A = cmulf(make_float2(a0[m] * p0.x, a0[m] * p0.y), sh.hy[j]);
+                const float2 B = cmulf(make_float2(a1[m] * p1.x, a1[m] * p1.y), sh.hy[j]);
+                x[m] = make_float2(A.x - B.y, A.y + B.x);
+            }
+        } else {
+            float acc[8];
+            spectrum_any(it, sh.comp, sh.dcomp, (float)c / (float)N, wf, acc);
+            const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)c * N;
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const int j = t + m * T;
+                const float2 p = __ldg(P + j);
+                x[m] = cmulf(make_float2(acc[m] * p.x, acc[m] * p.y), sh.hy[j]);
+            }
+        }
+        float2* col = s1 + (int64_t)c * nr;
+        tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int row, float2 z) {
+            if (act && row >= gr0 && row < gr1) col[row - gr0] = z;
+        });
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(kSplitThreads, 3)
+fourier_split_col_kernel(const tb_fft_item* __restrict__ items, int i0, int n_items,
+                         const double* __restrict__ amp, const double* __restrict__ var,
+                         const double* __restrict__ dcoef, const float* __restrict__ psf_spec,
+                         float* __restrict__ out, SplitWs* ws, int32_t* fb_list,
+                         float2* __restrict__ s1_all, tb_status* st) {
+    __shared__ SplitColShared sh;
+    if (threadIdx.x == 0) sh.cur_n = 0;
+    const int64_t n_units = (int64_t)n_items * kColUnits;
+    for (;;) {
+        const int64_t u = tb::next_unit(&ws->col_counter, &sh.slot);
+        if (u >= n_units) break;
+        const int li = (int)(u / kColUnits), cb = (int)(u % kColUnits);
+        const int ii = i0 + li;
+        const tb_fft_item& it = items[ii];
+        const int N = it.sz;
+        if (cb == 0) {
+            if (!item_ok(it, dcoef)) {
+                if (threadIdx.x == 0) tb::report(st, TB_STATUS_BAD_ITEM, ii, N);
+                continue;
+            }
+            if (!split_eligible(it)) {
+                if (threadIdx.x == 0) fb_list[atomicAdd(&ws->fb_count, 1)] = ii;
+                continue;
+            }
+            // STORE: the mask's pixels outside the transform window are zero
+            const int gr0 = max(0, -it.sy), gr1 = min(N, it.mh - it.sy);
+            const int gc0 = max(0, -it.sx), gc1 = min(N, it.mw - it.sx);
+            if (it.mode == TB_MOG_STORE)
+                zero_outside(out + it.out_off, it.ldo > 0 ? it.ldo : it.mw, it.mw, it.mh, it.sx,
+                             it.sy, gr0, gr1, gc0, gc1, gr0 >= gr1 || gc0 >= gc1);
+        } else if (!item_ok(it, dcoef) || !split_eligible(it)) {
+            continue;
+        }
+        if (cb * kColBlock >= N / 2) continue;
+        {
+            const int gr0 = max(0, -it.sy), gr1 = min(N, it.mh - it.sy);
+            const int gc0 = max(0, -it.sx), gc1 = min(N, it.mw - it.sx);
+            if (gr0 >= gr1 || gc0 >= gc1) continue;
+        }
+        // stage: components, y taps and their frequency response, twiddles
+        stage_components(it, amp, var, dcoef, sh.comp, sh.dcomp);
+        if (threadIdx.x == 0) {
+            if (it.dmode == TB_FFT_DY) taps3_deriv(it.muy, sh.taps);
+            else taps3(it.muy, sh.taps);
+        }
+        if (sh.cur_n != N) {
+            __syncthreads();
+            switch (N) {
+                case 256: tb::build_twiddles<256>(sh.tw); break;
+                case 128: tb::build_twiddles<128>(sh.tw); break;
+                case 64: tb::build_twiddles<64>(sh.tw); break;
+                default: tb::build_twiddles<32>(sh.tw); break;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) sh.cur_n = N;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < N; j += kSplitThreads) {
+            float2 h = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < 7; k++) {
+                const float2 w = sh.tw[(j * (k - 3)) & (N - 1)];
+                h.x = fmaf(sh.taps[k], w.x, h.x);
+                h.y = fmaf(sh.taps[k], w.y, h.y);
+            }
+            sh.hy[j] = h;
+        }
+        __syncthreads();
+        float2* s1 = s1_all + (int64_t)li * kS1PerItem;
+        const float* spec = psf_spec + it.spec_off;
+        switch (N) {
+            case 256: split_col_unit<256>(it, cb, spec, s1, sh); break;
+            case 128: split_col_unit<128>(it, cb, spec, s1, sh); break;
+            case 64: split_col_unit<64>(it, cb, spec, s1, sh); break;
+            default: split_col_unit<32>(it, cb, spec, s1, sh); break;
+        }
+    }
+}
+
+struct SplitRowShared {
+    float2 tw[256];
+    float taps[8];
+    float2 hx[129];
+    float2 xbuf[kSplitWarps * kXbufPerWarp];
+    float2 rows[kRowBlock * 129];     // [r][c], packed columns, padded to 129
+    int cur_n;
+    int64_t slot;
+};
+
+template <int N>
+__device__ void split_row_unit(const tb_fft_item& it, int rb, const float2* __restrict__ s1,
+                               float* __restrict__ out, SplitRowShared& sh) {
+    constexpr int NH = N / 2;
+    constexpr int T = N / 8;
+    constexpr int GPW = 32 / T;
+    constexpr int XB = tb::fft_xbuf_elems<N>();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = lane % T;
+    float2* xb = sh.xbuf + warp * kXbufPerWarp + (lane / T) * XB;
+    const int gr0 = max(0, -it.sy), gr1 = min(N, it.mh - it.sy);
+    const int gc0 = max(0, -it.sx), gc1 = min(N, it.mw - it.sx);
+    const int nr = gr1 - gr0;
+    const int r0 = rb * kRowBlock;
+    const int nrows = min(kRowBlock, nr - r0);
+    // this unit's rows of every packed column, transposed into shared memory
+    for (int e = threadIdx.x; e < NH * kRowBlock; e += kSplitThreads) {
+        const int c = e / kRowBlock, r = e % kRowBlock;
+        if (r < nrows) sh.rows[r * 129 + c] = s1[(int64_t)c * nr + r0 + r];
+    }
+    __syncthreads();
+    const float osc = it.scale / (float)(N * N);
+    float* O = out + it.out_off;
+    const int64_t ldo = it.ldo > 0 ? it.ldo : it.mw;
+    const int npairs = (nrows + 1) / 2;
+    for (int p0 = warp * GPW; p0 < npairs; p0 += kSplitWarps * GPW) {
+        const bool act = p0 + lane / T < npairs;
+        const int p = act ? p0 + lane / T : npairs - 1;
+        const int ia = 2 * p, ib = 2 * p + 1;
+        const bool hasb = ib < nrows;
+        const float2* H1 = sh.rows + ia * 129;
+        const float2* H2 = sh.rows + (hasb ? ib : ia) * 129;
+        float2 x[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const int n = t + m * T;
+            const int q = n <= N / 2 ? n : N - n;
+            float2 g1, g2;
+            if (q == 0) {
+                g1 = make_float2(H1[0].x, 0.f);
+                g2 = make_float2(H2[0].x, 0.f);
+            } else if (q == N / 2) {
+                g1 = make_float2(H1[0].y, 0.f);
+                g2 = make_float2(H2[0].y, 0.f);
+            } else {
+                g1 = H1[q];
+                g2 = H2[q];
+            }
+            const float2 hx = sh.hx[q];
+            const float2 h1 = cmulf(g1, hx);
+            const float2 h2 = hasb ? cmulf(g2, hx) : make_float2(0.f, 0.f);
+            x[m] = n <= N / 2 ? make_float2(h1.x - h2.y, h1.y + h2.x)
+                              : make_float2(h1.x + h2.y, h2.x - h1.y);
+        }
+        float* oa = O + (int64_t)(gr0 + r0 + ia + it.sy) * ldo + it.sx;
+        float* ob = O + (int64_t)(gr0 + r0 + ib + it.sy) * ldo + it.sx;
+        float dummy = 0.f;
+        tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int col, float2 z) {
+            if (act && col >= gc0 && col < gc1) {
+                put<false>(oa + col, z.x * osc, it.mode, dummy);
+                if (hasb) put<false>(ob + col, z.y * osc, it.mode, dummy);
+            }
+        });
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(kSplitThreads, 3)
+fourier_split_row_kernel(const tb_fft_item* __restrict__ items, int i0, int n_items,
+                         const double* __restrict__ dcoef, float* __restrict__ out, SplitWs* ws,
+                         const float2* __restrict__ s1_all) {
+    __shared__ SplitRowShared sh;
+    if (threadIdx.x == 0) sh.cur_n = 0;
+    const int64_t n_units = (int64_t)n_items * kRowUnits;
+    for (;;) {
+        const int64_t u = tb::next_unit(&ws->row_counter, &sh.slot);
+        if (u >= n_units) break;
+        const int li = (int)(u / kRowUnits), rb = (int)(u % kRowUnits);
+        const tb_fft_item& it = items[i0 + li];
+        if (!item_ok(it, dcoef) || !split_eligible(it)) continue;
+        const int N = it.sz;
+        const int gr0 = max(0, -it.sy), gr1 = min(N, it.mh - it.sy);
+        const int gc0 = max(0, -it.sx), gc1 = min(N, it.mw - it.sx);
+        if (gr0 >= gr1 || gc0 >= gc1 || rb * kRowBlock >= gr1 - gr0) continue;
+        if (threadIdx.x == 0) {
+            if (it.dmode == TB_FFT_DX) taps3_deriv(it.mux, sh.taps);
+            else taps3(it.mux, sh.taps);
+        }
+        if (sh.cur_n != N) {
+            __syncthreads();
+            switch (N) {
+                case 256: tb::build_twiddles<256>(sh.tw); break;
+                case 128: tb::build_twiddles<128>(sh.tw); break;
+                case 64: tb::build_twiddles<64>(sh.tw); break;
+                default: tb::build_twiddles<32>(sh.tw); break;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) sh.cur_n = N;
+        }
+        __syncthreads();
+        for (int f = threadIdx.x; f <= N / 2; f += kSplitThreads) {
+            float2 h = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < 7; k++) {
+                const float2 w = sh.tw[(f * (k - 3)) & (N - 1)];
+                h.x = fmaf(sh.taps[k], w.x, h.x);
+                h.y = fmaf(sh.taps[k], w.y, h.y);
+            }
+            sh.hx[f] = h;
+        }
+        __syncthreads();
+        const float2* s1 = s1_all + (int64_t)li * kS1PerItem;
+        switch (N) {
+            case 256: split_row_unit<256>(it, rb, s1, out, sh); break;
+            case 128: split_row_unit<128>(it, rb, s1, out, sh); break;
+            case 64: split_row_unit<64>(it, rb, s1, out, sh); break;
+            default: split_row_unit<32>(it, rb, s1, out, sh); break;
+        }
+    }
+}
+
 }  // namespace
 
 static int launch_fourier(const tb_fft_item* items, int32_t n_items, const double* comp_amp,
@@ -580,6 +989,83 @@ extern "C" int tb_fourier_render_deriv(const tb_fft_item* items, int32_t n_items
                                        tb_status* status, void* stream) {
     return launch_fourier(items, n_items, comp_amp, comp_var, comp_dcoef, psf_spec, out, dots,
                           work_counter, status, stream);
+}
+
+namespace {
+constexpr int kSplitChunk = 256;      // items per column/row launch pair (scratch bound)
+
+int64_t split_list_bytes(int32_t n_items) { return ((int64_t)n_items * 4 + 255) / 256 * 256; }
+
+int split_grid(const void* fn) {
+    static int cached[2] = {0, 0};
+    const int which = fn == (const void*)fourier_split_col_kernel ? 0 : 1;
+    if (cached[which] == 0) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSplitThreads, 0) !=
+                cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        cached[which] = per_sm;
+    }
+    return tb::num_sms() * cached[which];
+}
+}  // namespace
+
+extern "C" int tb_fourier_workspace(int32_t n_items, int64_t* bytes) {
+    if (n_items < 0 || !bytes) return TB_ERR_ARG;
+    const int64_t chunk = n_items < kSplitChunk ? n_items : kSplitChunk;
+    *bytes = (int64_t)sizeof(SplitWs) + split_list_bytes(n_items) +
+             chunk * kS1PerItem * (int64_t)sizeof(float2);
+    return TB_OK;
+}
+
+extern "C" int tb_fourier_render_split(const tb_fft_item* items, int32_t n_items,
+                                       const double* comp_amp, const double* comp_var,
+                                       const double* comp_dcoef, const float* psf_spec,
+                                       float* out, double* dots, void* workspace,
+                                       int64_t workspace_bytes, tb_status* status,
+                                       void* stream) {
+    if (n_items < 0) return TB_ERR_ARG;
+    if (n_items == 0) return TB_OK;
+    if (!items || !comp_amp || !comp_var || !psf_spec || !out || !workspace) return TB_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return TB_ERR_ARG;
+    int64_t need = 0;
+    tb_fourier_workspace(n_items, &need);
+    if (workspace_bytes < need) return TB_ERR_SIZE;
+    cudaStream_t s = (cudaStream_t)stream;
+    SplitWs* ws = static_cast<SplitWs*>(workspace);
+    int32_t* fb_list = reinterpret_cast<int32_t*>(static_cast<char*>(workspace) + sizeof(SplitWs));
+    float2* s1 = reinterpret_cast<float2*>(static_cast<char*>(workspace) + sizeof(SplitWs) +
+                                           split_list_bytes(n_items));
+    if (cudaMemsetAsync(ws, 0, sizeof(SplitWs), s) != cudaSuccess) return TB_ERR_LAUNCH;
+    if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    const int gcol = split_grid((const void*)fourier_split_col_kernel);
+    const int grow = split_grid((const void*)fourier_split_row_kernel);
+    for (int32_t i0 = 0; i0 < n_items; i0 += kSplitChunk) {
+        const int32_t n = n_items - i0 < kSplitChunk ? n_items - i0 : kSplitChunk;
+        if (i0 > 0 && cudaMemsetAsync(ws, 0, 2 * sizeof(int32_t), s) != cudaSuccess)
+            return TB_ERR_LAUNCH;
+        const int64_t cu = (int64_t)n * kColUnits, ru = (int64_t)n * kRowUnits;
+        fourier_split_col_kernel<<<(int)(cu < gcol ? cu : gcol), kSplitThreads, 0, s>>>(
+            items, i0, n, comp_amp, comp_var, comp_dcoef, psf_spec, out, ws, fb_list, s1, status);
+        fourier_split_row_kernel<<<(int)(ru < grow ? ru : grow), kSplitThreads, 0, s>>>(
+            items, i0, n, comp_dcoef, out, ws, s1);
+    }
+    // items outside the split path (Lanczos-3 reaching the box edge, TB_FFT_DOT)
+    const bool deriv = comp_dcoef != nullptr || dots != nullptr;
+    if (cudaFuncSetAttribute(deriv ? fourier_render_kernel<true> : fourier_render_kernel<false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    const int gfb = tb::num_sms() < n_items ? tb::num_sms() : n_items;
+    if (deriv)
+        fourier_render_kernel<true><<<gfb, kThreads, kSmemBytes, s>>>(
+            items, n_items, comp_amp, comp_var, comp_dcoef, psf_spec, out, dots, &ws->fb_counter,
+            status, fb_list, &ws->fb_count);
+    else
+        fourier_render_kernel<false><<<gfb, kThreads, kSmemBytes, s>>>(
+            items, n_items, comp_amp, comp_var, nullptr, psf_spec, out, nullptr, &ws->fb_counter,
+            status, fb_list, &ws->fb_count);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
 // ---------------------------------------------------------------------------

@@ -11,6 +11,8 @@
 // These replace the sparse-matrix assembly and LSQR solve of
 // LsqrOptimizer.getUpdateDirection (tractor/lsqr_optimizer.py:328-644) and
 // the chi-square sum of Tractor.getLogLikelihood (tractor/engine.py:475-479).
+#include <atomic>
+
 #include "tb_common.cuh"
 #include "tc_sm100.cuh"
 
@@ -436,7 +438,10 @@ solve_kernel(const double* __restrict__ AtA, const double* __restrict__ Atr,
     const int P = Pv[b];
     const int tid = threadIdx.x;
     if (P <= 0) return;
-    if (P > kMaxSmemP) {
+    // P[b] is device data: a problem larger than the shared arrays or than
+    // its slice of the workspace (work_stride = max_p^2 doubles) is refused
+    // instead of writing into its neighbours' factors
+    if (P > kMaxSmemP || (int64_t)P * P > work_stride) {
         if (tid == 0) info[b] = -1;
         return;
     }
@@ -964,7 +969,11 @@ static __device__ __align__(256) double g_solve_scratch[TB_SOLVE_NOALLOC_MAX_DOU
 
 namespace {
 constexpr int kMaxDevices = 64;
-double* g_solve_scratch_addr[kMaxDevices] = {nullptr};
+// Per-device address of g_solve_scratch.  Host threads may call at once:
+// relaxed atomics (every thread that looks the address up stores the same
+// value).  The address belongs to the device's primary context; a caller
+// that destroys it (cudaDeviceReset) must reload the library.
+std::atomic<double*> g_solve_scratch_addr[kMaxDevices];
 }  // namespace
 
 extern "C" int tb_solve_update_noalloc(const double* AtA, const double* Atr,
@@ -980,15 +989,14 @@ extern "C" int tb_solve_update_noalloc(const double* AtA, const double* Atr,
     if (!AtA || !Atr || !ata_off || !atr_off || !P || !x_off || !X || !info) return TB_ERR_ARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TB_ERR_LAUNCH;
-    if (g_solve_scratch_addr[dev] == nullptr) {
-        double* addr = nullptr;
-        if (cudaGetSymbolAddress((void**)&addr, g_solve_scratch) != cudaSuccess || !addr)
+    double* scratch = g_solve_scratch_addr[dev].load(std::memory_order_relaxed);
+    if (scratch == nullptr) {
+        if (cudaGetSymbolAddress((void**)&scratch, g_solve_scratch) != cudaSuccess || !scratch)
             return TB_ERR_LAUNCH;
-        g_solve_scratch_addr[dev] = addr;
+        g_solve_scratch_addr[dev].store(scratch, std::memory_order_relaxed);
     }
     solve_kernel<<<n_problems, kSolveThreads, 0, (cudaStream_t)stream>>>(
-        AtA, Atr, ata_off, atr_off, P, x_off, X, info, damp, g_solve_scratch_addr[dev],
-        (int64_t)max_p * max_p);
+        AtA, Atr, ata_off, atr_off, P, x_off, X, info, damp, scratch, (int64_t)max_p * max_p);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 

@@ -21,14 +21,25 @@ struct GaussC {
     float pad;
 };
 
+// Difference items: the perturbed mixture relative to the base one, for
+// G'_k - G_k = exp2(e_k) (s'_k expm1(de_k) + (s'_k - s_k)) with
+// de_k = e'_k - e_k (natural-log units, same mean).
+struct GaussD {
+    float dxx, dxy, dyy;  // de = dxx dx^2 + dxy dx dy + dyy dy^2
+    float sp;             // s'_k = amp'_k / (2 pi sqrt(det V'_k))
+    float ds;             // s'_k - s_k (from FP64)
+    float pad0, pad1, pad2;
+};
+
 constexpr int kThreads = 256;
 constexpr int kRowsPerThread = TB_MOG_TILE / (kThreads / 32);  // 4
 
 // Evaluates the staged components on one tile: thread column `lane`, rows
 // warp + 8 j.  With kDerivs, also the derivatives with respect to the mean
 // (-G (2 I0 dx + I1 dy), tractor/mix.i:44-82), written to two planes.
-template <bool kDerivs>
-__device__ __forceinline__ void eval_tile(const tb_mog_item& it, const GaussC* comps, int total,
+template <bool kDerivs, bool kDiff>
+__device__ __forceinline__ void eval_tile(const tb_mog_item& it, const GaussC* comps,
+                                          const GaussD* dcomps, int total,
                                           int tw, int th, int ox, int oy,
                                           const uint8_t* __restrict__ masks,
                                           float* __restrict__ out) {
@@ -47,8 +58,13 @@ __device__ __forceinline__ void eval_tile(const tb_mog_item& it, const GaussC* c
         for (int j = 0; j < kRowsPerThread; j++) {
             const float dy = (float)(warp + 8 * j) - q.my;
             const float e = fmaf(dy, fmaf(q.qyy, dy, B), A);
-            const float sv = (e >= q.fl) ? q.s : 0.f;
+            float sv = (e >= q.fl) ? q.s : 0.f;
             const float ev = tb::ex2(e);
+            if (kDiff) {
+                const GaussD d = dcomps[c];
+                const float de = fmaf(dy, fmaf(d.dyy, dy, d.dxy * dx), d.dxx * dx * dx);
+                sv = (e >= q.fl) ? fmaf(d.sp, expm1f(de), d.ds) : 0.f;
+            }
             acc[j] = fmaf(sv, ev, acc[j]);
             if (kDerivs) {
                 const float v = sv * ev;
@@ -86,6 +102,7 @@ mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_
                   const double* __restrict__ var, const uint8_t* __restrict__ masks,
                   float* __restrict__ out, int32_t* counter, tb_status* st) {
     __shared__ GaussC comps[TB_MOG_MAX_K];
+    __shared__ GaussD dcomps[TB_MOG_MAX_K];
     __shared__ int64_t slot;
     __shared__ int item_idx;
     __shared__ int warp_count[kThreads / 32];
@@ -115,7 +132,9 @@ mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_
         const int tw = min(TB_MOG_TILE, w - ox);
         const int th = min(TB_MOG_TILE, h - oy);
         const double tx0 = (double)it.x0 + ox, ty0 = (double)it.y0 + oy;
-        if (K < 0 || K > TB_MOG_MAX_K || w <= 0 || h <= 0) {
+        const bool diff = it.diff_c0 >= 0;
+        if (K < 0 || K > TB_MOG_MAX_K || w <= 0 || h <= 0 ||
+            (diff && (it.deriv_off >= 0 || it.floor_mode != TB_FLOOR_FIXED))) {
             if (threadIdx.x == 0) tb::report(st, TB_STATUS_BAD_ITEM, ii, K);
             continue;
         }
@@ -123,6 +142,7 @@ mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_
         // ---- stage + cull components (one thread per component) ----
         bool keep = false;
         GaussC g;
+        GaussD gd;
         if (threadIdx.x < K) {
             const int c = it.c0 + threadIdx.x;
             const double a = amp[c];
@@ -148,14 +168,37 @@ mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_
             g.mx = (float)mx;
             g.my = (float)my;
             g.pad = 0.f;
-            const bool finite = det > 0.0 && isfinite(s) && isfinite(f) && isfinite(mx) &&
-                                isfinite(my) && isfinite(fl);
+            bool finite = det > 0.0 && isfinite(s) && isfinite(f) && isfinite(mx) &&
+                          isfinite(my) && isfinite(fl);
+            double rx2 = 0.0, ry2 = 0.0;
+            bool live = a != 0.0;
+            if (diff) {
+                // perturbed component: same mean, its own amplitude and
+                // covariance; exponent differences in natural-log units
+                const int c2 = it.diff_c0 + threadIdx.x;
+                const double a2 = amp[c2];
+                const double w0 = var[4 * c2], w3 = var[4 * c2 + 3];
+                const double wxy = 0.5 * (var[4 * c2 + 1] + var[4 * c2 + 2]);
+                const double det2 = w0 * w3 - wxy * wxy;
+                const double s2 = a2 / (2.0 * TB_PI * sqrt(det2));
+                gd.dxx = (float)(-0.5 * (w3 / det2 - v3 / det));
+                gd.dxy = (float)(wxy / det2 - vxy / det);
+                gd.dyy = (float)(-0.5 * (w0 / det2 - v0 / det));
+                gd.sp = (float)s2;
+                gd.ds = (float)(s2 - s);
+                gd.pad0 = gd.pad1 = gd.pad2 = 0.f;
+                finite = finite && det2 > 0.0 && isfinite(s2);
+                rx2 = w0;
+                ry2 = w3;
+                live = live || a2 != 0.0;
+            }
             if (!finite) {
                 tb::report(st, TB_STATUS_NONFINITE, ii, threadIdx.x);
-            } else if (a != 0.0) {
-                // Region where the exponent is >= floor: Mahalanobis^2 <= -2 floor.
+            } else if (live) {
+                // Region where the exponent is >= floor: Mahalanobis^2 <= -2 floor
+                // (for a difference item, the larger of the two covariances').
                 const double r2 = -2.0 * fl;
-                const double rx = sqrt(r2 * v0), ry = sqrt(r2 * v3);
+                const double rx = sqrt(r2 * fmax(v0, rx2)), ry = sqrt(r2 * fmax(v3, ry2));
                 keep = (mx + rx >= 0.0) && (mx - rx <= tw - 1) && (my + ry >= 0.0) &&
                        (my - ry <= th - 1);
             }
@@ -170,13 +213,19 @@ mog_render_kernel(const tb_mog_item* __restrict__ items, int n_items, int64_t n_
             base += (i < warp) ? warp_count[i] : 0;
             total += warp_count[i];
         }
-        if (keep) comps[base + __popc(ballot & ((1u << lane) - 1u))] = g;
+        if (keep) {
+            const int slot_k = base + __popc(ballot & ((1u << lane) - 1u));
+            comps[slot_k] = g;
+            if (diff) dcomps[slot_k] = gd;
+        }
         __syncthreads();
 
-        if (it.deriv_off >= 0)
-            eval_tile<true>(it, comps, total, tw, th, ox, oy, masks, out);
+        if (diff)
+            eval_tile<false, true>(it, comps, dcomps, total, tw, th, ox, oy, masks, out);
+        else if (it.deriv_off >= 0)
+            eval_tile<true, false>(it, comps, dcomps, total, tw, th, ox, oy, masks, out);
         else
-            eval_tile<false>(it, comps, total, tw, th, ox, oy, masks, out);
+            eval_tile<false, false>(it, comps, dcomps, total, tw, th, ox, oy, masks, out);
     }
 }
 

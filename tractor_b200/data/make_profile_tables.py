@@ -93,4 +93,6 @@ def main(ref_root):
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    if len(sys.argv) < 2:
+        sys.exit('usage: make_profile_tables.py REFERENCE_ROOT')
+    main(sys.argv[1])

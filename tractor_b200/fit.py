@@ -366,6 +366,25 @@ def blob_workload(n_blobs, rng, side_range=(192, 512), n_bands=3, mean_src=6, ma
                 truth=truth, start=start, noise=noise, n_bands=n_bands)
 
 
+def subset_workload(w, blobs):
+    """The workload dict of blob_workload restricted to `blobs` (indices,
+    kept in their order): a rank's share of a partitioned fit."""
+    blobs = np.asarray(blobs, np.int64)
+    bs = w['blob_src']
+    src = np.concatenate([np.arange(bs[b], bs[b + 1]) for b in blobs]) if len(blobs) else \
+        np.zeros(0, np.int64)
+    nsrc = np.diff(bs)[blobs]
+    out = dict(w)
+    out['blob_src'] = np.concatenate([[0], np.cumsum(nsrc)]).astype(np.int64)
+    out['sides'] = w['sides'][blobs]
+    out['psf'] = [w['psf'][b] for b in blobs]
+    out['sources'] = w['sources'][src]
+    out['truth'] = w['truth'][src]
+    out['start'] = w['start'][src]
+    out['noise'] = w['noise'][blobs]
+    return out
+
+
 def render_blobs(w, params, seed=None):
     """Device images of the blobs' model at `params` through the scene
     renderer (an independent path), plus Gaussian noise of each unit's sigma
@@ -409,6 +428,16 @@ def render_blobs(w, params, seed=None):
     return out, 1. / sig_px
 
 
+def _esoft_params(ell, maxe=0.999999):
+    """(log r_e, ee1, ee2) of the EllipseESoft equal to EllipseE `ell`
+    (EllipseESoft.fromEllipseE, a round ellipse included)."""
+    e = min(ell.e, maxe)
+    if e == 0.:
+        return np.log(ell.re), 0., 0.
+    soft = -np.log(1. - e)
+    return np.log(ell.re), ell.e1 / e * soft, ell.e2 / e * soft
+
+
 def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
     """Fits many independent blobs, each given as a reference-style Tractor,
     in one batched device fit, and writes the fitted parameters back.
@@ -416,10 +445,12 @@ def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
     Each Tractor holds 1 to 3 images of one size with NullWCS, a
     LinearPhotoCal with a band (or no band for a single image) and a
     mixture-of-Gaussians PSF of at most 4 components, and at most 32
-    sources: SersicGalaxy, ExpGalaxy or DevGalaxy with an EllipseESoft
-    shape, or PointSource, at a PixPos, with a brightness holding one value
-    per image band (Flux for a single image, NanoMaggies / Fluxes
-    otherwise).  Model masks set with Tractor.setModelMasks are used (the
+    sources: SersicGalaxy, ExpGalaxy or DevGalaxy with an EllipseESoft or
+    EllipseE shape, or PointSource, at a PixPos, with a brightness holding
+    one value per image band (Flux for a single image, NanoMaggies / Fluxes
+    otherwise).  An EllipseE shape is fitted as the EllipseESoft of the same
+    ellipse (the same models, so the same optimum) and written back as an
+    EllipseE; its three parameters are then fitted or frozen together.  Model masks set with Tractor.setModelMasks are used (the
     same rectangle in every image); without them a source's mask is the
     whole image.  Frozen parameters (freezeParam / freezeAllBut) keep their
     values; every thawed one is fitted.  Returns the per-blob FIT_STATE
@@ -474,9 +505,12 @@ def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
             if isinstance(src, S.PointSource):
                 r['profile'] = _lib.PROFILE_POINT
             elif isinstance(src, (S.SersicGalaxy, S.ExpGalaxy, S.DevGalaxy)):
-                if not isinstance(src.shape, E.EllipseESoft):
-                    raise ValueError('galaxies need an EllipseESoft shape')
-                th[5:8] = src.shape.getAllParams()
+                if isinstance(src.shape, E.EllipseESoft):
+                    th[5:8] = src.shape.getAllParams()
+                elif isinstance(src.shape, E.EllipseE):
+                    th[5:8] = _esoft_params(src.shape)
+                else:
+                    raise ValueError('galaxies need an EllipseESoft or EllipseE shape')
                 if isinstance(src, S.SersicGalaxy):
                     r['profile'] = _lib.PROFILE_SERSIC
                     th[8] = src.sersicindex.val
@@ -498,8 +532,16 @@ def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
             bslots = [('brightness.' + (img.getPhotoCal().band
                                         if img.getPhotoCal().band in bnames else bnames[0]))
                       for img in imgs]
+            shape_names = ['shape.logre', 'shape.ee1', 'shape.ee2']
+            if not isinstance(src, S.PointSource) and not isinstance(src.shape, E.EllipseESoft):
+                # an EllipseE is fitted through its EllipseESoft: all or none
+                ethawed = [n in thawed for n in ('shape.re', 'shape.e1', 'shape.e2')]
+                if any(ethawed) and not all(ethawed):
+                    raise ValueError('an EllipseE shape is fitted whole or frozen whole')
+                if all(ethawed):
+                    thawed = thawed | set(shape_names)
             names = ['pos.x', 'pos.y'] + bslots + [None] * (3 - len(imgs)) + \
-                ['shape.logre', 'shape.ee1', 'shape.ee2', 'sersicindex.SersicIndex']
+                shape_names + ['sersicindex.SersicIndex']
             r['frozen'] = sum(1 << k for k, nm in enumerate(names)
                               if nm is not None and nm not in thawed)
             mask = tr._getModelMaskFor(imgs[0], src)
@@ -544,8 +586,13 @@ def fit_tractors(tractors, tol=1e-3, max_iter=60, check_every=4):
                 else:
                     br.setFlux(pc.band, val)
             if not isinstance(src, S.PointSource):
-                sh = src.shape.getAllParams()
-                src.shape.setAllParams([th[5 + j] if thawed(5 + j) else sh[j] for j in range(3)])
+                if isinstance(src.shape, E.EllipseESoft):
+                    sh = src.shape.getAllParams()
+                    src.shape.setAllParams([th[5 + j] if thawed(5 + j) else sh[j]
+                                            for j in range(3)])
+                elif thawed(5):
+                    src.shape.setAllParams(
+                        E.EllipseESoft(*th[5:8]).toEllipseE().getAllParams())
                 if isinstance(src, S.SersicGalaxy) and thawed(8):
                     src.sersicindex.setAllParams([th[8]])
     return f.states()

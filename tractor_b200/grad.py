@@ -59,12 +59,10 @@ class FourierJacobian(object):
                                         camp.data_ptr(), cvar.data_ptr(), dcoef.data_ptr(),
                                         batch.COMP_STRIDE, mode, col_stride, flags.data_ptr(), s)
         _lib.check(rc, 'tb_galaxy_fft_jac_prep')
-        rc = lib.tb_fourier_render_deriv(items.data_ptr(), 7 * n, camp.data_ptr(),
-                                         cvar.data_ptr(), dcoef.data_ptr(),
-                                         self.r.spec.data_ptr(), out.data_ptr(),
-                                         None if dots is None else dots.data_ptr(),
-                                         misc.data_ptr(), misc.data_ptr() + 16, s)
-        _lib.check(rc, 'tb_fourier_render_deriv')
+        render.fourier_render(items.data_ptr(), 7 * n, camp.data_ptr(), cvar.data_ptr(),
+                              self.r.spec.data_ptr(), out.data_ptr(), misc.data_ptr() + 16,
+                              dcoef_ptr=dcoef.data_ptr(),
+                              dots_ptr=None if dots is None else dots.data_ptr(), stream=stream)
         return flags, misc[4:8]
 
     def jacobian(self, srcs, n, npix, stream=None):

@@ -15,7 +15,6 @@ B200ConstrainedOptimizer adds ConstrainedOptimizer's max-step and bound
 handling (constrained_optimizer.py:12-159).
 """
 import numpy as np
-import torch
 
 from . import render
 from .plan import RenderPlan
@@ -157,15 +156,10 @@ class B200Optimizer(object):
     def _solve(self, A_colmajor, b, damp):
         """argmin ||A x - b||^2 + damp^2 ||x||^2 on the device (columns of A
         are rows of A_colmajor)."""
-        dev = render.device()
-        P, R = A_colmajor.shape
-        A_d = torch.from_numpy(np.ascontiguousarray(A_colmajor).ravel()).to(dev)
-        b_d = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
-        AtA, Atr, ao, ro = render.normal_equations(A_d, b_d, [0], [0], [R], [P], [R])
-        X, info, _ = render.solve_update(AtA, Atr, ao, ro, [P], damp=damp)
-        if int(info.cpu()[0]) != 0:
+        X, info = render.solve_dense(A_colmajor, b, damp=damp)
+        if info != 0:
             return None
-        return X.cpu().numpy()
+        return X
 
     # -- line search ---------------------------------------------------------
     def _batched_logprobs(self, tractor, p0, X, alphas):

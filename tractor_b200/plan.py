@@ -47,18 +47,20 @@ class RenderPlan(object):
 
     # -- adding work -----------------------------------------------------
     def add_mog(self, x0, y0, w, h, amp, mean, var, fx=0., fy=0., floor=render.FLOOR_GRID,
-                mask=None):
+                mask=None, diff=None):
         """Mixture on [x0, x0+w) x [y0, y0+h); returns a handle to its float32
-        (h, w) result."""
+        (h, w) result.  `diff` = (amp2, var2): the result is mixture 2 minus
+        this one (same means), rendered as one difference item."""
         if w <= 0 or h <= 0:
             return ('empty', h, w)
-        off = self.mog.add(x0, y0, w, h, amp, mean, var, fx=fx, fy=fy, floor=floor, mask=mask)
+        off = self.mog.add(x0, y0, w, h, amp, mean, var, fx=fx, fy=fy, floor=floor, mask=mask,
+                           diff=diff)
         return ('mog', off, h, w)
 
-    def add_fft(self, amp, var, sz, spec_key, spec, mw, mh, sx, sy, mux, muy):
+    def add_fft(self, amp, var, sz, spec_key, spec, mw, mh, sx, sy, mux, muy, diff=None):
         if mw <= 0 or mh <= 0:
             return ('empty', mh, mw)
-        off = self.fft.add(amp, var, sz, spec_key, spec, mw, mh, sx, sy, mux, muy)
+        off = self.fft.add(amp, var, sz, spec_key, spec, mw, mh, sx, sy, mux, muy, diff=diff)
         return ('fft', off, mh, mw)
 
     def add_lanczos(self, stamp, dx, dy):

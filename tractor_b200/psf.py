@@ -31,22 +31,25 @@ def _mog_extent(px, py, rr, clipExtent):
     return x0, x1, y0, y1
 
 
-def plan_mog_grid(plan, mix, x0, x1, y0, y1, fx, fy):
+def plan_mog_grid(plan, mix, x0, x1, y0, y1, fx, fy, diff=None):
     """MixtureOfGaussians.evaluate_grid (mixture_profiles.py:248-263) as a
-    pending float64 Patch."""
-    h = plan.add_mog(x0, y0, x1 - x0, y1 - y0, mix.amp, mix.mean, mix.var, fx=fx, fy=fy)
+    pending float64 Patch.  With `diff` (a mixture of the same size and
+    means), the Patch is evaluate_grid(diff) - evaluate_grid(mix), rendered
+    as one difference item."""
+    d = None if diff is None else (diff.amp, diff.var)
+    h = plan.add_mog(x0, y0, x1 - x0, y1 - y0, mix.amp, mix.mean, mix.var, fx=fx, fy=fy, diff=d)
     return Pending(lambda: plan.patch(x0, y0, h, np.float64))
 
 
-def plan_mog_masked(plan, mix, x0, y0, mask, fx, fy):
+def plan_mog_masked(plan, mix, x0, y0, mask, fx, fy, diff=None):
     """MixtureOfGaussians.evaluate_grid_masked (mixture_profiles.py:299-331),
-    values only: float32, zero outside the mask, exponent floor -30."""
+    values only: float32, zero outside the mask, exponent floor -30.  With
+    `diff`, the difference of the two mixtures' values as plan_mog_grid."""
     mh, mw = mask.shape
-    amp = np.asarray(mix.amp, np.float32).astype(np.float64)
-    mean = np.asarray(mix.mean, np.float32).astype(np.float64)
-    var = np.asarray(mix.var, np.float32).astype(np.float64)
-    h = plan.add_mog(x0, y0, mw, mh, amp, mean, var, fx=fx, fy=fy, floor=render.FLOOR_MASKED,
-                     mask=np.asarray(mask, bool))
+    f32 = lambda a: np.asarray(a, np.float32).astype(np.float64)  # noqa: E731
+    d = None if diff is None else (f32(diff.amp), f32(diff.var))
+    h = plan.add_mog(x0, y0, mw, mh, f32(mix.amp), f32(mix.mean), f32(mix.var), fx=fx, fy=fy,
+                     floor=render.FLOOR_MASKED, mask=np.asarray(mask, bool), diff=d)
     return Pending(lambda: plan.patch(x0, y0, h, np.float32))
 
 

@@ -6,6 +6,8 @@ to the device in a single transfer and launches the kernel once.  Device
 outputs stay torch tensors; the Tractor-facing classes copy to numpy only
 where the reference API returns numpy arrays.
 """
+import ctypes
+
 import numpy as np
 import torch
 
@@ -23,6 +25,36 @@ def device():
     return torch.device('cuda', torch.cuda.current_device())
 
 
+class _PinnedPool(object):
+    """Reusable pinned host staging buffers for host-to-device copies.
+    Pinning memory costs far more than a small copy, so buffers are kept;
+    a buffer is handed out again only once the copy that last read it has
+    completed (an event recorded after that copy on its stream)."""
+
+    MAX_BUFFERS = 16
+
+    def __init__(self):
+        self.bufs = []      # [pinned uint8 tensor, event or None]
+
+    def get(self, nbytes):
+        for entry in self.bufs:
+            t, ev = entry
+            if t.numel() >= nbytes and (ev is None or ev.query()):
+                return entry
+        if len(self.bufs) >= self.MAX_BUFFERS:
+            # all busy or too small: wait for the oldest copy and replace it
+            t, ev = self.bufs.pop(0)
+            if ev is not None:
+                ev.synchronize()
+        size = 1 << max(16, int(np.ceil(np.log2(max(nbytes, 1)))))
+        entry = [torch.empty(size, dtype=torch.uint8).pin_memory(), None]
+        self.bufs.append(entry)
+        return entry
+
+
+_pinned = _PinnedPool()
+
+
 class _Packer(object):
     """Accumulates named numpy sections into one 256-byte aligned buffer."""
 
@@ -38,13 +70,23 @@ class _Packer(object):
         return off
 
     def to_device(self, dev):
-        buf = np.zeros(max(self.size, 1), np.uint8)
+        size = max(self.size, 1)
+        if dev.type != 'cuda':
+            buf = np.zeros(size, np.uint8)
+            for off, arr in self.sections:
+                buf[off:off + arr.nbytes] = arr.view(np.uint8).ravel()
+            return torch.from_numpy(buf)
+        entry = _pinned.get(size)
+        host = entry[0][:size]
+        buf = host.numpy()      # padding between sections is never read
         for off, arr in self.sections:
             buf[off:off + arr.nbytes] = arr.view(np.uint8).ravel()
-        host = torch.from_numpy(buf)
-        if dev.type == 'cuda':
-            host = host.pin_memory()
-        return host.to(dev, non_blocking=True)
+        out = torch.empty(size, dtype=torch.uint8, device=dev)
+        out.copy_(host, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        entry[1] = ev
+        return out
 
 
 def check_status(status_tensor, what):
@@ -75,13 +117,16 @@ class MogBatch(object):
         return len(self.items)
 
     def add(self, x0, y0, w, h, amp, mean, var, fx=0., fy=0., floor=FLOOR_GRID, scale=1.,
-            mask=None, out_off=None, ldo=0, mode=MOG_STORE, minval=None, derivs=False):
+            mask=None, out_off=None, ldo=0, mode=MOG_STORE, minval=None, derivs=False,
+            diff=None):
         """Adds one mixture evaluated on [x0, x0+w) x [y0, y0+h).  Returns the
         element offset of its output (a packed w x h patch unless `out_off`
         and `ldo` place it inside a larger buffer).  `minval` selects the
         per-component floors of c_gauss_2d_approx3; `derivs` also writes the
         d/dmean_x and d/dmean_y planes right after the patch (packed outputs
-        only)."""
+        only).  `diff` = (amp2, var2), a second mixture of the same size and
+        means: the item renders (mixture 2) - (this mixture), computed with
+        its error relative to the difference."""
         # copies: a plan renders the state at the time of the call even if
         # the caller's arrays change before it runs (line searches, finite
         # differences of image parameters)
@@ -104,13 +149,27 @@ class MogBatch(object):
         if minval is not None:
             floor_mode = _lib.FLOOR_MINVAL
             floor = float(minval)
+        diff_c0 = -1
+        if diff is not None:
+            if minval is not None or derivs:
+                raise ValueError('difference items take a fixed floor and no derivative planes')
+            diff_c0 = self.ncomp + K
         self.items.append((int(x0), int(y0), int(w), int(h), self.ncomp, K, int(mode), int(ldo),
                            float(fx), float(fy), float(floor), float(scale), floor_mode,
-                           int(out_off), int(mask_off), 0, int(deriv_off)))
+                           int(out_off), int(mask_off), 0, int(deriv_off), diff_c0, 0))
+        mean = np.array(mean, np.float64).reshape(K, 2)
         self.amp.append(amp)
-        self.mean.append(np.array(mean, np.float64).reshape(K, 2))
+        self.mean.append(mean)
         self.var.append(np.array(var, np.float64).reshape(K, 2, 2))
         self.ncomp += K
+        if diff is not None:
+            amp2 = np.array(diff[0], np.float64).ravel()
+            if len(amp2) != K:
+                raise ValueError('a difference item needs two mixtures of one size')
+            self.amp.append(amp2)
+            self.mean.append(mean.copy())
+            self.var.append(np.array(diff[1], np.float64).reshape(K, 2, 2))
+            self.ncomp += K
         return out_off
 
     def run(self, out=None, stream=None, check=True):
@@ -227,12 +286,18 @@ class FftBatch(object):
         self.nspec = 0
         self.ncomp = 0
         self.nout = 0
+        self.dcoef = []
+        self.ndc = 0
 
     def __len__(self):
         return len(self.items)
 
     def add(self, amp, var, sz, spec_key, spec, mw, mh, sx, sy, mux, muy, scale=1.,
-            out_off=None, ldo=0, mode=MOG_STORE):
+            out_off=None, ldo=0, mode=MOG_STORE, diff=None):
+        """Adds one galaxy.  `diff` = (amp2, var2), a second mixture of the
+        same size: the item renders (mixture 2) - (this mixture) through the
+        same geometry (TB_FFT_DIFF), with its error relative to the
+        difference."""
         amp = np.array(amp, np.float64).ravel()   # copies, as MogBatch.add
         K = len(amp)
         if K > 128:
@@ -247,11 +312,23 @@ class FftBatch(object):
             self.spec_off[key] = self.nspec
             self.spec_list.append(spec)
             self.nspec += spec.numel()
+        var = np.array(var, np.float64).reshape(K, 2, 2)
+        dmode, dc0 = _lib.FFT_VALUE, 0
+        if diff is not None:
+            amp2 = np.array(diff[0], np.float64).ravel()
+            if len(amp2) != K:
+                raise ValueError('a difference item needs two mixtures of one size')
+            dv = np.array(diff[1], np.float64).reshape(K, 2, 2) - var
+            dc = np.stack([amp2 - amp, dv[:, 0, 0], 0.5 * (dv[:, 0, 1] + dv[:, 1, 0]),
+                           dv[:, 1, 1]], axis=1)
+            dmode, dc0 = _lib.FFT_DIFF, self.ndc
+            self.dcoef.append(dc)
+            self.ndc += K
         self.items.append((self.ncomp, K, int(sz), int(mode), int(mw), int(mh), int(sx), int(sy),
                            float(mux), float(muy), float(scale), int(ldo), int(out_off),
-                           self.spec_off[key], _lib.FFT_VALUE, 0, 0))
+                           self.spec_off[key], dmode, dc0, 0))
         self.amp.append(amp)
-        self.var.append(np.array(var, np.float64).reshape(K, 2, 2))
+        self.var.append(var)
         self.ncomp += K
         return out_off
 
@@ -268,19 +345,50 @@ class FftBatch(object):
         o_items = pk.add(items)
         o_amp = pk.add(np.concatenate(self.amp))
         o_var = pk.add(np.concatenate(self.var))
+        o_dc = pk.add(np.concatenate(self.dcoef)) if self.dcoef else None
         o_ctr = pk.add(np.zeros(4, np.int32))
         o_st = pk.add(np.zeros(1, _lib.STATUS))
         d = pk.to_device(dev)
         base = d.data_ptr()
-        rc = lib.tb_fourier_render(base + o_items, len(items), base + o_amp, base + o_var,
-                                   specs.data_ptr(), out.data_ptr(), base + o_ctr, base + o_st,
-                                   _lib.stream_ptr(stream))
-        _lib.check(rc, 'tb_fourier_render')
+        fourier_render(base + o_items, len(items), base + o_amp, base + o_var, specs.data_ptr(),
+                       out.data_ptr(), base + o_st,
+                       dcoef_ptr=None if o_dc is None else base + o_dc, stream=stream)
         self._keep = (d, specs)
         self.status = d[o_st:o_st + 16]
         if check:
             check_status(self.status, 'tb_fourier_render')
         return out
+
+
+_fourier_ws = {}
+
+
+def fourier_workspace(n_items, dev=None):
+    """Device scratch of tb_fourier_render_split for n_items items (one
+    buffer per device, grown when needed and reused: launches on one stream
+    use it one after another)."""
+    lib = _lib.load()
+    dev = dev or device()
+    nb = ctypes.c_int64()
+    _lib.check(lib.tb_fourier_workspace(int(n_items), ctypes.byref(nb)), 'tb_fourier_workspace')
+    ws = _fourier_ws.get(dev.index)
+    if ws is None or ws.numel() < nb.value:
+        ws = torch.empty(max(nb.value, 1 << 20), dtype=torch.uint8, device=dev)
+        _fourier_ws[dev.index] = ws
+    return ws
+
+
+def fourier_render(items_ptr, n_items, amp_ptr, var_ptr, spec_ptr, out_ptr, status_ptr,
+                   dcoef_ptr=None, dots_ptr=None, stream=None):
+    """tb_fourier_render_split over device items (the product's Fourier
+    render: column and row kernels through an L2-resident scratch, the
+    items it does not cover by the persistent kernel)."""
+    lib = _lib.load()
+    ws = fourier_workspace(n_items)
+    rc = lib.tb_fourier_render_split(items_ptr, int(n_items), amp_ptr, var_ptr, dcoef_ptr,
+                                     spec_ptr, out_ptr, dots_ptr, ws.data_ptr(), ws.numel(),
+                                     status_ptr, _lib.stream_ptr(stream))
+    _lib.check(rc, 'tb_fourier_render_split')
 
 
 def lanczos_shift(imgs, shifts, stream=None):
@@ -329,6 +437,41 @@ def normal_equations(A, rhs, a_off, r_off, lda, P, R, stream=None):
                                  _lib.stream_ptr(stream))
     _lib.check(rc, 'tb_normal_equations')
     return AtA, Atr, args[5], args[6]
+
+
+def solve_dense(A_colmajor, b, damp=0., stream=None):
+    """argmin ||A x - b||^2 + damp^2 ||x||^2 of one dense problem given on
+    the host (A's columns are the rows of the float32 array A_colmajor, b
+    float32): tb_normal_equations + tb_solve_update with one host-to-device
+    copy of everything and one device-to-host copy of (x, info).  Returns
+    (x float64 numpy array, info)."""
+    lib = _lib.load()
+    dev = device()
+    A_colmajor = np.ascontiguousarray(A_colmajor, np.float32)
+    P, R = A_colmajor.shape
+    pk = _Packer()
+    o_A = pk.add(A_colmajor.ravel())
+    o_b = pk.add(np.ascontiguousarray(b, np.float32))
+    o_i64 = pk.add(np.array([0, 0, 0, 0, 0], np.int64))     # a_off r_off ata_off atr_off x_off
+    o_i32 = pk.add(np.array([R, P, R], np.int32))            # lda P R
+    d = pk.to_device(dev)
+    base = d.data_ptr()
+    ws = torch.empty(P * P + P + P * P + P + 1, dtype=torch.float64, device=dev)
+    wb = ws.data_ptr()
+    AtA, Atr, work, X, info = wb, wb + 8 * P * P, wb + 8 * (P * P + P), \
+        wb + 8 * (2 * P * P + P), wb + 8 * (2 * P * P + 2 * P)
+    s = _lib.stream_ptr(stream)
+    rc = lib.tb_normal_equations(base + o_A, base + o_b, base + o_i64, base + o_i64 + 8,
+                                 base + o_i32, base + o_i32 + 4, base + o_i32 + 8,
+                                 base + o_i64 + 16, base + o_i64 + 24, AtA, Atr, 1, P, s)
+    _lib.check(rc, 'tb_normal_equations')
+    rc = lib.tb_solve_update(AtA, Atr, base + o_i64 + 16, base + o_i64 + 24, base + o_i32 + 4,
+                             base + o_i64 + 32, X, info, float(damp), 1, P, work, s)
+    _lib.check(rc, 'tb_solve_update')
+    host = ws[2 * P * P + P:].cpu().numpy()
+    x = host[:P].copy()
+    info_v = int(host[P:P + 1].view(np.int32)[0])
+    return x, info_v
 
 
 def solve_update(AtA, Atr, ata_off, atr_off, P, damp=0., stream=None):

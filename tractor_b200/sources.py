@@ -442,8 +442,13 @@ class ProfileGalaxy(object):
 
     def _plan_real_unit_patch(self, plan, img, px, py, minval, modelMask=None,
                               inner_real_nsigma=3., outer_real_nsigma=4., force_halfsize=None,
-                              force_sourceOut=False, **kwargs):
-        """ProfileGalaxy._realGetUnitFluxModelPatch (galaxy.py:266-519)."""
+                              force_sourceOut=False, diff_of=None, **kwargs):
+        """ProfileGalaxy._realGetUnitFluxModelPatch (galaxy.py:266-519).
+
+        diff_of: another galaxy with a profile of as many components (and the
+        same geometry): the planned Patch is then its unit-flux patch minus
+        this one's, rendered as difference items (the caller checks that the
+        two renders share their extent; see _difference_render_ok)."""
         if modelMask is not None:
             x0, y0 = modelMask.x0, modelMask.y0
         else:
@@ -461,11 +466,16 @@ class ProfileGalaxy(object):
                 mm = modelMask
             psfmix = psf.getMixtureOfGaussians(px=px, py=py)
             cmix = amix.convolve(psfmix)
+            dmix = None
+            if diff_of is not None:
+                dmix = diff_of._getAffineProfile(img, px, py).convolve(psfmix)
             if mm is None:
+                if dmix is not None:
+                    return plan_mog_grid(plan, cmix, x0, x1, y0, y1, 0., 0., diff=dmix)
                 return mixture_to_patch(plan, cmix, x0, x1, y0, y1, minval)
             if mm.mask is not None:
-                return plan_mog_masked(plan, cmix, mm.x0, mm.y0, mm.mask, 0., 0.)
-            return plan_mog_grid(plan, cmix, mm.x0, mm.x1, mm.y0, mm.y1, 0., 0.)
+                return plan_mog_masked(plan, cmix, mm.x0, mm.y0, mm.mask, 0., 0., diff=dmix)
+            return plan_mog_grid(plan, cmix, mm.x0, mm.x1, mm.y0, mm.y1, 0., 0., diff=dmix)
 
         if hasattr(psf, 'getMixtureOfGaussians') and not hybrid:
             return run_mog(mm=modelMask)
@@ -560,8 +570,12 @@ class ProfileGalaxy(object):
             rx0, ry0, rw, rh = gx0, gy0, max(0, gx1 - gx0), max(0, gy1 - gy0)
             ssx, ssy = ix0 - rx0, iy0 - ry0
         if fftmix is not None and rw > 0 and rh > 0:
+            dmix = None
+            if diff_of is not None:
+                other = diff_of._getShearedProfile(img, px, py)
+                dmix = (other.amp, other.var)
             h = plan.add_fft(fftmix.amp, fftmix.var, sz, spec_key, spec, rw, rh, ssx, ssy,
-                             mux, muy)
+                             mux, muy, diff=dmix)
         else:
             h = ('empty', rh, rw)
         mogp = None
@@ -714,22 +728,55 @@ class SersicGalaxy(HoggGalaxy):
     def _extra_derivative_renders(self, plan, img, px0, py0, modelMask, minval, counts,
                                   **kwargs):
         """sersic.py:416-444: the index step rendered with the caller's
-        modelMask and the default minval."""
+        modelMask and the default minval.  Where the stepped render and
+        patch0 are exact renders of one rectangle with mixtures of as many
+        components, the difference newpatch - patch0 is rendered directly
+        (difference items: its float32 error is relative to the difference,
+        not to the two patches); otherwise newpatch is rendered and
+        patch0 subtracted, as the reference does."""
         if self.isParamFrozen('sersicindex'):
             return []
         step = self._sersic_step()
         old = self.sersicindex.getParams()[0]
+        other = self.copy()
+        other.sersicindex.setParam(0, old + step)
+        if self._difference_render_ok(img, other, px0, py0, modelMask, minval):
+            p = self._plan_unit_patch(plan, img, px=px0, py=py0, modelMask=modelMask,
+                                      diff_of=other, **kwargs)
+            return [(step, p, True)]
         self.sersicindex.setParam(0, old + step)
         p = self._plan_unit_patch(plan, img, px=px0, py=py0, modelMask=modelMask, **kwargs)
         self.sersicindex.setParam(0, old)
-        return [(step, p)]
+        return [(step, p, False)]
+
+    def _difference_render_ok(self, img, other, px, py, modelMask, minval):
+        """True when patch0 (minval) and other's default-minval render are
+        exact renders of the same rectangle by mixtures of equal size: a
+        non-hybrid PSF, no minval cut, equal component counts and, without
+        a mask, equal patch extents."""
+        if minval not in (0., None) or isinstance(img.getPsf(), HybridPSF):
+            return False
+        if len(self.getProfile().amp) != len(other.getProfile().amp):
+            return False
+        if modelMask is None:
+            if self._no_mask_extent(img, px, py, 0.) != other._no_mask_extent(img, px, py, 0.):
+                return False
+            if self._getUnitFluxPatchSize(img, px=px, py=py, minval=0.) != \
+                    other._getUnitFluxPatchSize(img, px=px, py=py, minval=0.):
+                return False
+        return True
 
     def _finish_extra(self, extra, patch0, counts):
         out = []
-        for step, p in extra:
+        for step, p, is_diff in extra:
             newpatch = p.result()
             if newpatch is None:
                 out.append(None)
+                continue
+            if is_diff:
+                d = newpatch * (counts / step)
+                d.setName('d(%s)/d(%s)' % (self.dname, 'SersicIndex'))
+                out.append(d)
                 continue
             d = (newpatch - patch0) * (counts / step)
             d.setName('d(%s)/d(%s)' % (self.dname, 'SersicIndex'))
