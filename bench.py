@@ -895,16 +895,7 @@ def bench_normal_equations(args, dev, flush, clk, cpu_seconds):
     return line
 
 
-def bench_plain_small(args, dev):
-    """The small plain fit through the object API (an ExpGalaxy, r_e 2 px, b/a
-    0.6, phi 30, flux 1000, at the centre of a 64 x 64 FP64 image, two-
-    Gaussian PSF with sigma 1.5 / 3.0 and weights 0.8 / 0.2, noise sigma 1
-    drawn from seed 300; start off by 0.5 px and 20 % in flux and r_e):
-    microseconds per Tractor.getModelImage and milliseconds per
-    optimize_loop(dchisq=1e-3) with B200Optimizer, host timed (each call
-    returns host arrays: copies and launches included).  The case is
-    latency-bound (49k pixel x components per render): no roofline."""
-    import tractor_b200 as T
+def _plain_small_setup(T):
     psf = T.NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2])
     truth = T.ExpGalaxy(T.PixPos(32., 32.), T.Flux(1000.), T.EllipseE.fromRAbPhi(2.0, 0.6, 30.))
     tim = T.Image(data=np.zeros((64, 64)), invvar=np.ones((64, 64)), psf=psf,
@@ -918,30 +909,78 @@ def bench_plain_small(args, dev):
     tr = T.Tractor([tim], [src])
     tr.modtype = np.float64
     tr.freezeParam('images')
-    for _ in range(5):
+    return tr, start
+
+
+def _plain_small_time(T, reps, fits):
+    tr, start = _plain_small_setup(T)
+    for _ in range(3):
         tr.getModelImage(0)
-    reps = 50
     t0 = time.perf_counter()
     for _ in range(reps):
         tr.getModelImage(0)
     render_us = (time.perf_counter() - t0) / reps * 1e6
-    fits, steps = [], 0
-    for _ in range(max(2, min(args.steps, 3)) + 1):
+    times, steps = [], 0
+    for _ in range(fits):
         tr.setParams(start)
         t0 = time.perf_counter()
         R = tr.optimize_loop(dchisq=1e-3)
-        fits.append(time.perf_counter() - t0)
+        times.append(time.perf_counter() - t0)
         steps = R['steps']
-    fit_s = float(np.median(fits[1:]))
-    return {'workload': 'ExpGalaxy on a 64x64 image, 2-Gaussian PSF, LSQ fit of position, flux '
-                        'and shape from an offset start (optimize_loop, dchisq 1e-3)',
+    return render_us, times, steps
+
+
+class _SetAttr(object):
+    """The one method of a monkeypatch that oracle.host_kernels.install uses."""
+
+    @staticmethod
+    def setattr(obj, name, value):
+        setattr(obj, name, value)
+
+
+def _plain_small_cpu_worker(_):
+    """The small plain fit on the host: the same object API with every kernel
+    computed by the oracle (C / numpy), one core."""
+    sys.path.insert(0, ROOT)
+    os.environ.setdefault('OMP_NUM_THREADS', '1')
+    from oracle import host_kernels
+    host_kernels.install(_SetAttr())
+    import tractor_b200 as T
+    render_us, times, steps = _plain_small_time(T, reps=20, fits=2)
+    return render_us, float(np.median(times)), steps
+
+
+def bench_plain_small(args, dev, cpu_seconds=None):
+    """The small plain fit through the object API (an ExpGalaxy, r_e 2 px, b/a
+    0.6, phi 30, flux 1000, at the centre of a 64 x 64 FP64 image, two-
+    Gaussian PSF with sigma 1.5 / 3.0 and weights 0.8 / 0.2, noise sigma 1
+    drawn from seed 300; start off by 0.5 px and 20 % in flux and r_e):
+    microseconds per Tractor.getModelImage and milliseconds per
+    optimize_loop(dchisq=1e-3) with B200Optimizer, host timed (each call
+    returns host arrays: copies and launches included).  The case is
+    latency-bound (49k pixel x components per render): no roofline.  CPU
+    baseline: the same calls with the oracle's kernels on one host core."""
+    import tractor_b200 as T
+    render_us, times, steps = _plain_small_time(T, reps=50,
+                                                fits=max(2, min(args.steps, 3)) + 1)
+    fit_s = float(np.median(times[1:]))
+    line = {'workload': 'C1: ExpGalaxy on 64x64, 2-Gaussian PSF, optimize_loop(dchisq=1e-3)',
             'metric': 'fitted sources/s (plain small fit, object API)',
-            'value': 1.0 / fit_s, 'unit': 'sources/s', 'ms_per_fit': fit_s * 1e3,
-            'steps_per_fit': steps, 'us_per_render': render_us,
+            'value': 1.0 / fit_s, 'unit': 'sources/s', 'ms_per_step': fit_s * 1e3,
+            'ms_per_fit': fit_s * 1e3, 'steps_per_fit': steps, 'us_per_render': render_us,
             'timing': 'host wall clock per call (launches, copies and host logic included)',
-            'roofline': None, 'cpu_baseline': None,
-            'note': 'latency-bound (49k pixel x components per render); the reference CPU '
-                    'fitter is not on the GPU host'}
+            'roofline': None,
+            'summary': {'us_render': render_us, 'steps': steps}}
+    if cpu_seconds:
+        with mp.get_context('spawn').Pool(1) as pool:
+            cr_us, cfit_s, csteps = pool.map(_plain_small_cpu_worker, [0])[0]
+        line['cpu_baseline'] = {'value': 1.0 / cfit_s, 'unit': 'sources/s', 'cores': 1,
+                                'kind': 'port',
+                                'sample': 'the same fit (%d steps) and 20 renders with the '
+                                          'oracle kernels on the host: %.1f ms per fit, %.0f us '
+                                          'per render' % (csteps, cfit_s * 1e3, cr_us)}
+        line['summary']['cpu_us_render'] = cr_us
+    return line
 
 
 # secondary workload: EM fits of PSF stamps (GaussianMixturePSF.fromStamp)

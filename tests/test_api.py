@@ -625,3 +625,37 @@ def test_small_api_helpers_match_reference():
         ro = RT.Patch(other.x0, other.y0, other.patch)
         assert pa.hasNonzeroOverlapWith(other) == RT.Patch(2, 3, np.ones((4, 5))) \
             .hasNonzeroOverlapWith(ro)
+
+
+def test_image_fits_round_trip(tmp_path):
+    """Image.toFits / readFromFits (image.py:186-256) through the numpy FITS
+    writer: the header names each calibration's class and holds its
+    parameters (the default P<i> cards of ducks.py:163-168), the pixels and
+    inverse variance come back exactly, and so do the calibrations."""
+    import tractor_b200 as T
+    from tractor_b200 import fitsbin
+    rng = np.random.default_rng(3)
+    data = rng.normal(size=(20, 30)).astype(np.float32)
+    iv = rng.uniform(0.5, 2, size=(20, 30)).astype(np.float32)
+    psf = T.GaussianMixturePSF(np.array([0.7, 0.3]), np.zeros((2, 2)),
+                               np.array([np.eye(2) * 1.5, np.eye(2) * 4.]))
+    tim = T.Image(data=data, invvar=iv, psf=psf, sky=T.ConstantSky(3.5),
+                  photocal=T.LinearPhotoCal(2.5))
+    fn = str(tmp_path / 'img.fits')
+    with fitsbin.FITS(fn, 'rw', clobber=True) as f:
+        tim.toFits(f)
+    f = fitsbin.FITS(fn)
+    assert len(f) == 3
+    hdr = f[0].read_header()
+    assert hdr['PSF'] == 'tractor_b200.psf.GaussianMixturePSF'
+    assert hdr['WCS'].endswith('NullWCS') and hdr['SKY'].endswith('ConstantSky')
+    assert hdr['PHO_P0'] == 2.5 and hdr['SKY_P0'] == 3.5
+    assert [hdr['PSF_P%d' % i] for i in range(12)] == list(psf.getAllParams())
+    tim2 = T.Image.readFromFits(f)
+    assert tim2.getImage().dtype == np.float32
+    assert np.array_equal(tim2.getImage(), data)
+    assert np.array_equal(tim2.getInvvar(), tim.getInvvar())
+    assert list(tim2.getPsf().getAllParams()) == list(psf.getAllParams())
+    assert tim2.getSky().getValue() == 3.5
+    assert tim2.getPhotoCal().getScale() == 2.5
+    assert isinstance(tim2.getWcs(), T.NullWCS)

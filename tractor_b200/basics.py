@@ -506,3 +506,71 @@ class Image(MultiParams):
 
     def setSky(self, sky):
         self.sky = sky
+
+    # -- FITS (image.py:186-256) ---------------------------------------------
+    def getFitsHeader(self, header=None, prefix=''):
+        """image.py:224-256: the calibration classes' names under PSF, WCS,
+        SKY, PHO and each one's parameters under its prefix (its own
+        toFitsHeader, or ImageCalibration.toFitsHeader's P0, P1, ... cards,
+        ducks.py:162-168).  `header`: a fitsbin.FITSHDR (or any object with
+        add_record)."""
+        from .fitsbin import FITSHDR
+        hdr = FITSHDR() if header is None else header
+        parts = (('PSF', self.getPsf(), 'PSF class'), ('WCS', self.getWcs(), 'WCS class'),
+                 ('SKY', self.getSky(), 'Sky class'), ('PHO', self.getPhotoCal(), 'PhotoCal class'))
+        for key, obj, comment in parts:
+            tt = type(obj)
+            hdr.add_record(dict(name=prefix + key, value='%s.%s' % (tt.__module__, tt.__name__),
+                                comment=comment))
+        for key, obj, _ in parts:
+            calibration_to_fits_header(obj, hdr, prefix + key + '_')
+        return hdr
+
+    def toFits(self, fits, prefix='', primheader=None, imageheader=None, invvarheader=None):
+        """image.py:218-222: the header in an empty primary HDU, then the
+        image and the inverse variance.  `fits`: a fitsbin.FITS (or any object
+        with fitsio.FITS's write(data, header=...))."""
+        hdr = self.getFitsHeader(header=primheader, prefix=prefix)
+        fits.write(None, header=hdr)
+        fits.write(self.getImage(), header=imageheader)
+        fits.write(self.getInvvar(), header=invvarheader)
+
+    @staticmethod
+    def readFromFits(fits, prefix=''):
+        """image.py:186-216: pixels and inverse variance from HDUs 1 and 2,
+        each calibration rebuilt by its class's fromFitsHeader."""
+        hdr = fits[0].read_header()
+        pix = fits[1].read()
+        iv = fits[2].read()
+        assert pix.shape == iv.shape
+
+        def read_object(key):
+            clazz = _class_from_name(hdr[key])
+            return clazz.fromFitsHeader(hdr, prefix=key + '_')
+        return Image(data=pix, invvar=iv, psf=read_object(prefix + 'PSF'),
+                     wcs=read_object(prefix + 'WCS'), sky=read_object(prefix + 'SKY'),
+                     photocal=read_object(prefix + 'PHO'))
+
+
+def calibration_to_fits_header(obj, hdr, prefix=''):
+    """An image calibration's toFitsHeader, or ducks.py:163-168's default:
+    one card P<i> per parameter, the parameter's name as the comment."""
+    own = getattr(obj, 'toFitsHeader', None)
+    if own is not None:
+        own(hdr, prefix)
+        return
+    for i, (name, val) in enumerate(zip(obj.getParamNames(), obj.getAllParams())):
+        hdr.add_record(dict(name=prefix + 'P%i' % i, value=val, comment=name))
+
+
+def _class_from_name(name):
+    """The class a header names: module.Class, or the class of that name
+    exported by tractor_b200 (for headers written by the reference, whose
+    modules are tractor.*)."""
+    import importlib
+    mod, _, cls = str(name).rpartition('.')
+    try:
+        return getattr(importlib.import_module(mod), cls)
+    except (ImportError, AttributeError, ValueError):
+        import tractor_b200
+        return getattr(tractor_b200, cls)

@@ -1,8 +1,9 @@
-"""Minimal FITS binary-table reading and writing (numpy only), enough for
-PsfEx model files: header cards of every HDU, and binary tables whose
-columns are fixed-size numeric arrays (TFORM letters L, B, I, J, K, E, D;
-TDIM honoured).  No compression, no variable-length arrays, no scaling.
-(The reference reads these files with fitsio / astrometry.util.fits.)
+"""Minimal FITS reading and writing (numpy only), enough for PsfEx model
+files and Image.toFits / readFromFits: header cards of every HDU, binary
+tables whose columns are fixed-size numeric arrays (TFORM letters L, B, I,
+J, K, E, D; TDIM honoured), and image HDUs.  No compression, no
+variable-length arrays, no scaling.  (The reference uses fitsio /
+astrometry.util.fits.)
 """
 import numpy as np
 
@@ -171,3 +172,136 @@ def write_table(fn, columns, header=None):
         f.write(_header_bytes(primary))
         f.write(_header_bytes(ext))
         f.write(body + b'\0' * pad)
+
+
+# ---------------------------------------------------------------------------
+# Image HDUs and a small file object with the calls Image.toFits /
+# Image.readFromFits make on a fitsio.FITS (write, [i].read, [i].read_header)
+# ---------------------------------------------------------------------------
+
+_BITPIX = {np.dtype('uint8'): 8, np.dtype('int16'): 16, np.dtype('int32'): 32,
+           np.dtype('int64'): 64, np.dtype('float32'): -32, np.dtype('float64'): -64}
+_DTYPE = {8: 'u1', 16: '>i2', 32: '>i4', 64: '>i8', -32: '>f4', -64: '>f8'}
+
+
+class FITSHDR(object):
+    """An ordered FITS header: records of (name, value, comment)."""
+
+    def __init__(self, records=None):
+        self.records = []
+        for r in records or []:
+            self.add_record(r)
+
+    def add_record(self, rec):
+        name = str(rec['name']).upper()
+        for r in self.records:
+            if r['name'] == name:
+                r['value'] = rec['value']
+                r['comment'] = rec.get('comment', '')
+                return
+        self.records.append(dict(name=name, value=rec['value'], comment=rec.get('comment', '')))
+
+    def __contains__(self, key):
+        return any(r['name'] == str(key).upper() for r in self.records)
+
+    def __getitem__(self, key):
+        for r in self.records:
+            if r['name'] == str(key).upper():
+                return r['value']
+        raise KeyError(key)
+
+    def get(self, key, default=None):
+        return self[key] if key in self else default
+
+    def keys(self):
+        return [r['name'] for r in self.records]
+
+
+def _card_c(key, value, comment=''):
+    card = _card(key, value)
+    if comment:
+        body = card.rstrip()
+        room = 80 - len(body) - 3
+        if room > 0:
+            card = (body + ' / ' + comment[:room]).ljust(80)
+    return card
+
+
+class _HDU(object):
+    def __init__(self, hdr, raw):
+        self.hdr, self.raw = hdr, raw
+
+    def read_header(self):
+        return FITSHDR([dict(name=k, value=v) for k, v in self.hdr.items()])
+
+    def read(self):
+        naxis = int(self.hdr.get('NAXIS', 0))
+        if naxis == 0:
+            return None
+        shape = tuple(int(self.hdr['NAXIS%d' % a]) for a in range(naxis, 0, -1))
+        dt = np.dtype(_DTYPE[int(self.hdr['BITPIX'])])
+        a = np.frombuffer(self.raw[:int(np.prod(shape)) * dt.itemsize], dtype=dt).reshape(shape)
+        return a.astype(dt.newbyteorder('='))
+
+
+class FITS(object):
+    """A FITS file of image HDUs: write(data or None, header=...) appends an
+    HDU (the first is the primary), fits[i].read() / .read_header() read
+    them back.  mode 'rw' with clobber=True starts a new file."""
+
+    def __init__(self, fn, mode='r', clobber=False):
+        self.fn = fn
+        self.hdus = []
+        if mode == 'rw' and clobber:
+            open(fn, 'wb').close()
+        else:
+            try:
+                self.hdus = [_HDU(h, d) for h, d in read_hdus(fn)]
+            except FileNotFoundError:
+                if mode != 'rw':
+                    raise
+                open(fn, 'wb').close()
+
+    def __len__(self):
+        return len(self.hdus)
+
+    def __getitem__(self, i):
+        return self.hdus[i]
+
+    def write(self, data, header=None):
+        primary = len(self.hdus) == 0
+        cards = []
+        if data is None:
+            arr = None
+            cards += [_card('SIMPLE', True) if primary else _card('XTENSION', 'IMAGE'),
+                      _card('BITPIX', 8), _card('NAXIS', 0)]
+        else:
+            arr = np.ascontiguousarray(data)
+            if arr.dtype not in _BITPIX:
+                arr = arr.astype(np.float64)
+            cards += [_card('SIMPLE', True) if primary else _card('XTENSION', 'IMAGE'),
+                      _card('BITPIX', _BITPIX[arr.dtype]), _card('NAXIS', arr.ndim)]
+            cards += [_card('NAXIS%d' % (a + 1), arr.shape[arr.ndim - 1 - a])
+                      for a in range(arr.ndim)]
+        if primary:
+            cards.append(_card('EXTEND', True))
+        else:
+            cards += [_card('PCOUNT', 0), _card('GCOUNT', 1)]
+        for r in (header.records if isinstance(header, FITSHDR) else
+                  [dict(name=k, value=v) for k, v in (header or {}).items()]):
+            cards.append(_card_c(r['name'], r['value'], r.get('comment', '')))
+        body = b'' if arr is None else arr.astype(arr.dtype.newbyteorder('>')).tobytes()
+        pad = (len(body) + BLOCK - 1) // BLOCK * BLOCK - len(body)
+        with open(self.fn, 'ab') as f:
+            f.write(_header_bytes(cards))
+            f.write(body + b'\0' * pad)
+        self.hdus = [_HDU(h, d) for h, d in read_hdus(self.fn)]
+
+    def close(self):
+        pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

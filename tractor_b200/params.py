@@ -37,6 +37,24 @@ class BaseParams(object):
     def hashkey(self):
         return (_class_name(self),) + tuple(self.getAllParams())
 
+    @classmethod
+    def fromFitsHeader(clazz, hdr, prefix=''):
+        """ImageCalibration.fromFitsHeader (ducks.py:170-178): the
+        constructor's arguments from cards <prefix>A0, A1, ...; where a header
+        has none, from the <prefix>P0, P1, ... cards that the default
+        toFitsHeader (ducks.py:163-168) writes, so that images written by
+        Image.toFits read back."""
+        for key in ('A', 'P'):
+            args = []
+            for i in range(100):
+                k = prefix + key + '%i' % i
+                if k not in hdr:
+                    break
+                args.append(hdr.get(k))
+            if args:
+                return clazz(*args)
+        return clazz()
+
     def getParamNames(self):
         return []
 
