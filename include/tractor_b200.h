@@ -121,6 +121,39 @@ int tb_mog_render(const tb_mog_item* items, int32_t n_items, int64_t n_tiles,
                   const double* comp_var, const uint8_t* masks, float* out,
                   int32_t* work_counter, tb_status* status, void* stream);
 
+/* c_gauss_2d_approx3's evaluated region (tractor/approx3.c:126-442) over
+ * values tb_mog_render has already written for a whole box with the
+ * TB_FLOOR_MINVAL floors: starting at (xc, yc) -- or, when that is outside
+ * the box, at the largest value of the edge column / row the caller
+ * evaluated (edge_col_off / edge_row_off, -1 for none; column first, ties to
+ * the first, the default start (dcx, dcy) when no value is above 0) -- square
+ * rings R = 1, 2, ... are visited; a ring pixel counts as evaluated when a
+ * pixel of the previous ring marked it (the reference's next-T/B/L/R arrays:
+ * a passing pixel -- R <= minradius or value >= minval -- marks its
+ * neighbours on the next ring, top and bottom rows own the corners), and the
+ * walk stops at the first ring with nothing evaluated.  Every other pixel of
+ * the box is set to 0 (and of the d/dx, d/dy planes when deriv_off >= 0),
+ * and extent[4 i ..] = (sx0, sx1, sy0, sy1), box-relative with exclusive
+ * upper ends, updated per ring by its rows (y) and columns (x) as
+ * approx3.c does.  w, h <= TB_RING_MAX.  One CTA per item. */
+#define TB_RING_MAX 4096
+typedef struct {
+    int64_t val_off;       /* the box's w x h values in vals */
+    int64_t deriv_off;     /* >= 0: two more w x h planes, zeroed alike */
+    int64_t edge_col_off;  /* >= 0: h values of column edge_x (start search) */
+    int64_t edge_row_off;  /* >= 0: w values of row edge_y */
+    int32_t w, h;
+    int32_t xc, yc;        /* start pixel, box-relative */
+    int32_t edge_x, edge_y;
+    int32_t dcx, dcy;      /* default start, box-relative */
+    int32_t minradius;
+    int32_t start_inside;  /* 1: (xc, yc) is inside the box */
+    double minval;
+} tb_ring_item;
+
+int tb_approx3_region(const tb_ring_item* items, int32_t n_items, float* vals,
+                      int32_t* extent, tb_status* status, void* stream);
+
 /* ------------------------------------------------------------------------
  * Lanczos-3 sub-pixel shift
  * ------------------------------------------------------------------------ */
@@ -675,8 +708,9 @@ const char* tb_version(void);
  * sizeof(tb_status), sizeof(tb_galaxy_src), sizeof(tb_fft_image),
  * sizeof(tb_scene_src), sizeof(tb_scene_image), sizeof(tb_scene_item),
  * sizeof(tb_fit_source), sizeof(tb_fit_blob), sizeof(tb_fit_unit),
- * sizeof(tb_fit_state) into sizes[0..11] (host memory) and returns 12.  No reference counterpart
- * (bindings check their struct layouts with it). */
+ * sizeof(tb_fit_state), sizeof(tb_ring_item) into sizes[0..12] (host memory)
+ * and returns 13.  No reference counterpart (bindings check their struct
+ * layouts with it). */
 int tb_abi_sizes(int32_t* sizes);
 
 #ifdef __cplusplus

@@ -132,6 +132,137 @@ def fft_items(items, amp, var, specs, out, dcoef=None):
                 dst[:] += res[r]
 
 
+def ring_region(vals, cx, cy, minval, minradius):
+    """c_gauss_2d_approx3's ring walk (tractor/approx3.c:126-442) over the
+    box's values: boolean mask of evaluated pixels and (sx0, sx1, sy0, sy1)
+    (exclusive upper bounds), for box-relative start pixel (cx, cy)."""
+    H, W = vals.shape
+    ev = np.zeros((H, W), bool)
+
+    def mark(arr, i, n):
+        if 0 <= i < n:
+            arr[i] = True
+
+    nT, nB = np.zeros(W, bool), np.zeros(W, bool)
+    nL, nR = np.zeros(H, bool), np.zeros(H, bool)
+    if cy > 0:
+        for d in (-1, 0, 1):
+            mark(nB, cx + d, W)
+    if cy < H - 1:
+        for d in (-1, 0, 1):
+            mark(nT, cx + d, W)
+    if cx > 0:
+        mark(nL, cy, H)
+    if cx < W - 1:
+        mark(nR, cy, H)
+    ev[cy, cx] = True
+    sx0 = sx1 = cx
+    sy0 = sy1 = cy
+
+    def spread(marks, n):
+        """Union of i-1, i, i+1 over marked i, clipped to [0, n)."""
+        out = marks.copy()
+        out[1:] |= marks[:-1]
+        out[:-1] |= marks[1:]
+        return out
+
+    R = 1
+    while True:
+        cT, cB, cL, cR = nT, nB, nL, nR
+        nT, nB = np.zeros(W, bool), np.zeros(W, bool)
+        nL, nR = np.zeros(H, bool), np.zeros(H, bool)
+        anyev = False
+        # top (y = cy + R), bottom (y = cy - R)
+        for side in (0, 1):
+            y = cy + R if side == 0 else cy - R
+            if not (0 <= y < H):
+                continue
+            cur = cT if side == 0 else cB
+            idx = np.flatnonzero(cur)
+            if len(idx) == 0:
+                continue
+            anyev = True
+            ev[y, idx] = True
+            if side == 0:
+                sy1 = y
+            else:
+                sy0 = y
+            ok = np.zeros(W, bool)
+            ok[idx] = (R <= minradius) | (vals[y, idx] >= minval)
+            inward = -1 if side == 0 else 1
+            if cx - R > 0 and 0 <= cx - R < W and ok[cx - R]:
+                mark(nL, y, H)
+                mark(nL, y + inward, H)
+            if cx + R < W - 1 and 0 <= cx + R < W and ok[cx + R]:
+                mark(nR, y, H)
+                mark(nR, y + inward, H)
+            if (side == 0 and y < H - 1) or (side == 1 and y > 0):
+                nxt = spread(ok, W)
+                if side == 0:
+                    nT |= nxt
+                else:
+                    nB |= nxt
+        # left (x = cx - R), right (x = cx + R)
+        for side in (0, 1):
+            x = cx - R if side == 0 else cx + R
+            if not (0 <= x < W):
+                continue
+            cur = cL if side == 0 else cR
+            idx = np.flatnonzero(cur)
+            if len(idx) == 0:
+                continue
+            anyev = True
+            ev[idx, x] = True
+            if side == 0:
+                sx0 = x
+            else:
+                sx1 = x
+            ok = np.zeros(H, bool)
+            ok[idx] = (R <= minradius) | (vals[idx, x] >= minval)
+            if (side == 0 and x > 0) or (side == 1 and x < W - 1):
+                nxt = spread(ok, H)
+                if side == 0:
+                    nL |= nxt
+                else:
+                    nR |= nxt
+        if not anyev:
+            break
+        R += 1
+    return ev, (sx0, sx1 + 1, sy0, sy1 + 1)
+
+
+def ring_items(rings, out):
+    """tb_approx3_region's result: each walk's start, region and extent, the
+    other pixels of the box (and of its derivative planes) set to zero."""
+    ext = np.zeros((len(rings), 4), np.int32)
+    for i, r in enumerate(rings):
+        W, H = int(r['w']), int(r['h'])
+        vo = int(r['val_off'])
+        vals = out[vo:vo + W * H].reshape(H, W).astype(np.float64)
+        if r['start_inside']:
+            cx, cy = int(r['xc']), int(r['yc'])
+        else:
+            best, cx, cy = 0., int(r['dcx']), int(r['dcy'])
+            if r['edge_col_off'] >= 0:
+                col = out[int(r['edge_col_off']):int(r['edge_col_off']) + H]
+                for y, v in enumerate(col):
+                    if v > best:
+                        best, cx, cy = v, int(r['edge_x']), y
+            if r['edge_row_off'] >= 0:
+                row = out[int(r['edge_row_off']):int(r['edge_row_off']) + W]
+                for x, v in enumerate(row):
+                    if v > best:
+                        best, cx, cy = v, x, int(r['edge_y'])
+        ev, e = ring_region(vals, cx, cy, float(r['minval']), int(r['minradius']))
+        ext[i] = e
+        offs = [vo] + ([int(r['deriv_off']), int(r['deriv_off']) + W * H]
+                       if r['deriv_off'] >= 0 else [])
+        for o in offs:
+            plane = out[o:o + W * H].reshape(H, W)
+            plane[~ev] = 0.
+    return ext
+
+
 def install(monkeypatch):
     from tractor_b200 import render, _lib
 
@@ -146,6 +277,11 @@ def install(monkeypatch):
             o = out.numpy()
             mog_items(items, np.concatenate(self.amp), np.concatenate(self.mean),
                       np.concatenate(self.var), masks, o)
+        self.extents = None
+        self.ring_status = None
+        if self.rings:
+            self.extents = torch.from_numpy(ring_items(self.rings, out.numpy()).ravel())
+            self.ring_status = torch.zeros(16, dtype=torch.uint8)
         self.status = torch.zeros(16, dtype=torch.uint8)
         return out
 

@@ -221,6 +221,59 @@ def test_split_path_matches_persistent_kernel(tb, oracle):
     assert torch.equal(out1, out2)
 
 
+@pytest.mark.parametrize('derivs', [False, True])
+def test_approx3_region_on_device_matches_oracle(tb, oracle, derivs):
+    """approx3 (tb_mog_render with the minval floors, then tb_approx3_region
+    walking the rings on the device) against the oracle's c_gauss_2d_approx3
+    (pinned to the reference's C): the sliced patch, its extent and, with
+    derivs, the d/dx and d/dy planes, for start pixels inside the box and
+    beyond each of its edges and corners; all walks in one plan."""
+    from tractor_b200 import approx
+    from tractor_b200.plan import RenderPlan
+    from tractor_b200.profiles import MixtureOfGaussians
+    rng = np.random.default_rng(41 + derivs)
+    plan = RenderPlan()
+    cases = []
+    starts = ['in', 'left', 'right', 'below', 'above', 'corner']
+    for i in range(18):
+        K = int(rng.integers(2, 8))
+        amp, mean, var = _rand_mix(rng, K, spread=2.0, vmin=0.5, vmax=9.0)
+        W, H = int(rng.integers(20, 90)), int(rng.integers(20, 90))
+        x0, y0 = int(rng.integers(-30, 30)), int(rng.integers(-30, 30))
+        fx, fy = x0 + W * rng.uniform(0.2, 0.8), y0 + H * rng.uniform(0.2, 0.8)
+        minval = float(10 ** rng.uniform(-5, -2))
+        where = starts[i % len(starts)]
+        xc, yc = int(fx), int(fy)
+        if where == 'left':
+            xc = x0 - 5
+        elif where == 'right':
+            xc = x0 + W + 3
+        elif where == 'below':
+            yc = y0 - 4
+        elif where == 'above':
+            yc = y0 + H
+        elif where == 'corner':
+            xc, yc = x0 - 2, y0 + H + 7
+        mix = MixtureOfGaussians(amp, mean, var)
+        pend = approx.plan_approx3(plan, mix, x0, x0 + W, y0, y0 + H, fx, fy, minval, xc, yc,
+                                   derivs=derivs)
+        cases.append((pend, (x0, W, y0, H, fx, fy, minval, amp, mean, var, xc, yc)))
+    for pend, (x0, W, y0, H, fx, fy, minval, amp, mean, var, xc, yc) in cases:
+        out, dxo, dyo, (sx0, sx1, sy0, sy1) = oracle.mog_approx3(
+            x0, x0 + W, y0, y0 + H, fx, fy, minval, amp, mean, var, xc, yc, derivs=derivs)
+        got = pend.result()
+        planes = got if derivs else (got,)
+        refs = [out, dxo, dyo] if derivs else [out]
+        for p, ref in zip(planes, refs):
+            assert (p.x0, p.y0) == (x0 + sx0, y0 + sy0), ((p.x0, p.y0), (x0 + sx0, y0 + sy0))
+            sub = ref[sy0:sy1, sx0:sx1]
+            assert p.patch.shape == sub.shape
+            peak = max(np.abs(sub).max(), 1e-300)
+            assert np.abs(p.patch - sub).max() <= 1e-5 * peak
+            # the pixels approx3 did not evaluate are exactly zero
+            assert np.array_equal(p.patch == 0, sub == 0)
+
+
 def test_normal_equations_and_solve(tb):
     import torch
     from tractor_b200 import render

@@ -29,6 +29,12 @@ FFT_ITEM = np.dtype([('c0', '<i4'), ('K', '<i4'), ('sz', '<i4'), ('mode', '<i4')
 FFT_VALUE, FFT_DSPEC, FFT_DX, FFT_DY, FFT_DIFF = 0, 1, 2, 3, 4
 FFT_DOT = 3
 STATUS = np.dtype([('code', '<i4'), ('item', '<i4'), ('detail', '<i4'), ('count', '<i4')])
+RING_ITEM = np.dtype([('val_off', '<i8'), ('deriv_off', '<i8'), ('edge_col_off', '<i8'),
+                      ('edge_row_off', '<i8'), ('w', '<i4'), ('h', '<i4'), ('xc', '<i4'),
+                      ('yc', '<i4'), ('edge_x', '<i4'), ('edge_y', '<i4'), ('dcx', '<i4'),
+                      ('dcy', '<i4'), ('minradius', '<i4'), ('start_inside', '<i4'),
+                      ('minval', '<f8')])
+RING_MAX = 4096
 GALAXY_SRC = np.dtype([('px', '<f8'), ('py', '<f8'), ('counts', '<f8'), ('s0', '<f8'),
                        ('s1', '<f8'), ('s2', '<f8'), ('sersic_n', '<f8'), ('out_off', '<i8'),
                        ('profile', '<i4'), ('shape_type', '<i4'), ('mx0', '<i4'), ('my0', '<i4'),
@@ -133,6 +139,7 @@ SIGNATURES = {
                                _I64, _P, _P]),
     'tb_version': (ctypes.c_char_p, []),
     'tb_abi_sizes': (_I32, [_P]),
+    'tb_approx3_region': (_I32, [_P, _I32, _P, _P, _P, _P]),
 }
 
 _lib = None
@@ -158,12 +165,12 @@ def load():
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
-    sizes = np.zeros(12, np.int32)
+    sizes = np.zeros(13, np.int32)
     lib.tb_abi_sizes(sizes.ctypes.data)
     want = (MOG_ITEM.itemsize, FFT_ITEM.itemsize, STATUS.itemsize, GALAXY_SRC.itemsize,
             ctypes.sizeof(FftImage), SCENE_SRC.itemsize, SCENE_IMAGE.itemsize,
             SCENE_ITEM.itemsize, FIT_SOURCE.itemsize, FIT_BLOB.itemsize, FIT_UNIT.itemsize,
-            FIT_STATE.itemsize)
+            FIT_STATE.itemsize, RING_ITEM.itemsize)
     if tuple(int(s) for s in sizes) != want:
         raise ImportError('libtractor_b200.so struct layout %s != binding %s' %
                           (tuple(sizes), want))

@@ -1026,5 +1026,6 @@ extern "C" int tb_abi_sizes(int32_t* sizes) {
     sizes[9] = (int32_t)sizeof(tb_fit_blob);
     sizes[10] = (int32_t)sizeof(tb_fit_unit);
     sizes[11] = (int32_t)sizeof(tb_fit_state);
-    return 12;
+    sizes[12] = (int32_t)sizeof(tb_ring_item);
+    return 13;
 }

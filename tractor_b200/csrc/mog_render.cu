@@ -250,3 +250,181 @@ extern "C" int tb_mog_render(const tb_mog_item* items, int32_t n_items, int64_t 
                                                comp_var, masks, out, work_counter, status);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
+
+// ---------------------------------------------------------------------------
+// approx3's evaluated region (tractor/approx3.c:126-442) over values that
+// tb_mog_render wrote for the whole box: the ring walk of the reference, one
+// CTA per item, with the do / next mark arrays in shared memory.  A pixel of
+// ring R lies on exactly one side (top and bottom rows own the corners; the
+// left and right columns hold the rows strictly between), marks only ever
+// land inside the next ring's sides, and a ring pixel is evaluated iff it is
+// marked; so each unmarked pixel of a visited ring is zeroed in the same
+// pass, and after the walk everything from the first empty ring outward.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kRingThreads = 256;
+
+struct RingShared {
+    uint8_t m[8][TB_RING_MAX];   // doT, doB, doL, doR, nextT, nextB, nextL, nextR
+    int any, anyT, anyB, anyL, anyR;
+    int cx, cy;
+};
+
+__device__ __forceinline__ void ring_set(uint8_t* a, int i, int n) {
+    if (i >= 0 && i < n) a[i] = 1;
+}
+
+__device__ __forceinline__ void ring_zero(float* v, int64_t d, int64_t plane, int64_t o) {
+    v[o] = 0.f;
+    if (d >= 0) {
+        v[d + o] = 0.f;
+        v[d + plane + o] = 0.f;
+    }
+}
+
+__global__ void __launch_bounds__(kRingThreads)
+approx3_ring_kernel(const tb_ring_item* __restrict__ items, int n_items, float* __restrict__ vals,
+                    int32_t* __restrict__ extent, tb_status* st) {
+    __shared__ RingShared sh;
+    const int ii = blockIdx.x;
+    if (ii >= n_items) return;
+    const tb_ring_item it = items[ii];
+    const int W = it.w, H = it.h;
+    if (W <= 0 || H <= 0 || W > TB_RING_MAX || H > TB_RING_MAX) {
+        if (threadIdx.x == 0) tb::report(st, TB_STATUS_BAD_ITEM, ii, W > H ? W : H);
+        return;
+    }
+    float* v = vals + it.val_off;
+    const int64_t d = it.deriv_off;
+    const int64_t plane = (int64_t)W * H;
+    const double minval = it.minval;
+    const int tid = threadIdx.x;
+    uint8_t* dT = sh.m[0];
+    uint8_t* dB = sh.m[1];
+    uint8_t* dL = sh.m[2];
+    uint8_t* dR = sh.m[3];
+    uint8_t* nT = sh.m[4];
+    uint8_t* nB = sh.m[5];
+    uint8_t* nL = sh.m[6];
+    uint8_t* nR = sh.m[7];
+    const int wh = W > H ? W : H;
+    for (int i = tid; i < wh; i += kRingThreads)
+#pragma unroll
+        for (int a = 4; a < 8; a++) sh.m[a][i] = 0;
+    if (tid == 0) {
+        int cx = it.xc, cy = it.yc;
+        if (!it.start_inside) {
+            // the largest value of the edge column, then of the edge row
+            double best = 0.0;
+            cx = it.dcx;
+            cy = it.dcy;
+            if (it.edge_col_off >= 0)
+                for (int y = 0; y < H; y++) {
+                    const double val = vals[it.edge_col_off + y];
+                    if (val > best) { best = val; cx = it.edge_x; cy = y; }
+                }
+            if (it.edge_row_off >= 0)
+                for (int x = 0; x < W; x++) {
+                    const double val = vals[it.edge_row_off + x];
+                    if (val > best) { best = val; cx = x; cy = it.edge_y; }
+                }
+        }
+        sh.cx = cx;
+        sh.cy = cy;
+    }
+    __syncthreads();
+    const int cx = sh.cx, cy = sh.cy;
+    if (tid == 0) {
+        // the eight neighbours of the start pixel
+        if (cy > 0) { ring_set(nB, cx - 1, W); ring_set(nB, cx, W); ring_set(nB, cx + 1, W); }
+        if (cy < H - 1) { ring_set(nT, cx - 1, W); ring_set(nT, cx, W); ring_set(nT, cx + 1, W); }
+        if (cx > 0) ring_set(nL, cy, H);
+        if (cx < W - 1) ring_set(nR, cy, H);
+    }
+    int sx0 = cx, sx1 = cx, sy0 = cy, sy1 = cy;
+    int R = 1;
+    for (;; R++) {
+        __syncthreads();
+        // swap: the next arrays become the do arrays
+        uint8_t* t;
+        t = dT; dT = nT; nT = t;
+        t = dB; dB = nB; nB = t;
+        t = dL; dL = nL; nL = t;
+        t = dR; dR = nR; nR = t;
+        for (int i = tid; i < W; i += kRingThreads) { nT[i] = 0; nB[i] = 0; }
+        for (int i = tid; i < H; i += kRingThreads) { nL[i] = 0; nR[i] = 0; }
+        if (tid == 0) sh.anyT = sh.anyB = sh.anyL = sh.anyR = 0;
+        __syncthreads();
+        const bool pass_all = R <= it.minradius;
+        // top (y = cy + R) and bottom (y = cy - R) rows, x in [cx - R, cx + R]
+        for (int x = tid; x < W; x += kRingThreads) {
+            if (x < cx - R || x > cx + R) continue;
+            for (int side = 0; side < 2; side++) {
+                const int y = side == 0 ? cy + R : cy - R;
+                if (y < 0 || y >= H) continue;
+                const int64_t o = (int64_t)y * W + x;
+                const uint8_t* dm = side == 0 ? dT : dB;
+                if (!dm[x]) { ring_zero(v, d, plane, o); continue; }
+                if (side == 0) sh.anyT = 1; else sh.anyB = 1;
+                if (!pass_all && (double)v[o] < minval) continue;
+                const int inward = side == 0 ? -1 : 1;
+                if (x == cx - R && x > 0) { ring_set(nL, y, H); ring_set(nL, y + inward, H); }
+                if (x == cx + R && x < W - 1) { ring_set(nR, y, H); ring_set(nR, y + inward, H); }
+                if (side == 0 ? y < H - 1 : y > 0) {
+                    uint8_t* nm = side == 0 ? nT : nB;
+                    ring_set(nm, x - 1, W); ring_set(nm, x, W); ring_set(nm, x + 1, W);
+                }
+            }
+        }
+        // left (x = cx - R) and right (x = cx + R) columns, y strictly inside the ring
+        for (int y = tid; y < H; y += kRingThreads) {
+            if (y <= cy - R || y >= cy + R) continue;
+            for (int side = 0; side < 2; side++) {
+                const int x = side == 0 ? cx - R : cx + R;
+                if (x < 0 || x >= W) continue;
+                const int64_t o = (int64_t)y * W + x;
+                const uint8_t* dm = side == 0 ? dL : dR;
+                if (!dm[y]) { ring_zero(v, d, plane, o); continue; }
+                if (side == 0) sh.anyL = 1; else sh.anyR = 1;
+                if (!pass_all && (double)v[o] < minval) continue;
+                if (side == 0 ? x > 0 : x < W - 1) {
+                    uint8_t* nm = side == 0 ? nL : nR;
+                    ring_set(nm, y - 1, H); ring_set(nm, y, H); ring_set(nm, y + 1, H);
+                }
+            }
+        }
+        __syncthreads();
+        if (sh.anyT) sy1 = cy + R;
+        if (sh.anyB) sy0 = cy - R;
+        if (sh.anyL) sx0 = cx - R;
+        if (sh.anyR) sx1 = cx + R;
+        if (!(sh.anyT | sh.anyB | sh.anyL | sh.anyR)) break;
+    }
+    // nothing was evaluated from ring R outward
+    for (int64_t o = tid; o < plane; o += kRingThreads) {
+        const int y = (int)(o / W), x = (int)(o % W);
+        const int dist = max(abs(x - cx), abs(y - cy));
+        if (dist >= R) ring_zero(v, d, plane, o);
+    }
+    if (tid == 0) {
+        extent[4 * ii + 0] = sx0;
+        extent[4 * ii + 1] = sx1 + 1;
+        extent[4 * ii + 2] = sy0;
+        extent[4 * ii + 3] = sy1 + 1;
+    }
+}
+
+}  // namespace
+
+extern "C" int tb_approx3_region(const tb_ring_item* items, int32_t n_items, float* vals,
+                                 int32_t* extent, tb_status* status, void* stream) {
+    if (n_items < 0) return TB_ERR_ARG;
+    if (n_items == 0) return TB_OK;
+    if (!items || !vals || !extent) return TB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    approx3_ring_kernel<<<n_items, kRingThreads, 0, s>>>(items, n_items, vals, extent, status);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}

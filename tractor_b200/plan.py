@@ -42,6 +42,7 @@ class RenderPlan(object):
         self.nlz = 0
         self._ran = False
         self._mog_host = None
+        self._ring_host = None
         self._fft_host = None
         self._lz_host = {}
 
@@ -89,6 +90,9 @@ class RenderPlan(object):
             host = t.cpu().numpy()
             if kind == 'mog':
                 render.check_status(self.mog.status, 'tb_mog_render')
+                if self.mog.extents is not None:
+                    render.check_status(self.mog.ring_status, 'tb_approx3_region')
+                    self._ring_host = self.mog.extents.cpu().numpy().reshape(-1, 4)
                 self._mog_host = host
             else:
                 render.check_status(self.fft.status, 'tb_fourier_render')
@@ -113,6 +117,11 @@ class RenderPlan(object):
             _, key, i = handle
             return self._lz_host[key][i]
         raise KeyError(kind)
+
+    def ring_extent(self, i):
+        """(sx0, sx1, sy0, sy1) of approx3 region walk i (MogBatch.add_ring)."""
+        self.run()
+        return tuple(int(v) for v in self._ring_host[i])
 
     def patch(self, x0, y0, handle, dtype=np.float32):
         return Patch(x0, y0, np.array(self.get(handle), dtype=dtype))

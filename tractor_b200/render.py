@@ -112,9 +112,35 @@ class MogBatch(object):
         self.ncomp = 0
         self.nmask = 0
         self.nout = 0
+        self.rings = []
 
     def __len__(self):
         return len(self.items)
+
+    def add_ring(self, val_off, w, h, minval, minradius, start=None, default_start=(0, 0),
+                 edge_col=None, edge_row=None, deriv_off=-1):
+        """Adds an approx3 region walk (tb_approx3_region) over the w x h
+        values at val_off (an item added with `minval`): start = box-relative
+        (xc, yc) inside the box, or None to start at the largest value of
+        edge_col = (x, offset of its h values) / edge_row = (y, offset of its
+        w values), default_start when none is above 0.  Returns the index of
+        its extent (sx0, sx1, sy0, sy1) in `extents` after run()."""
+        if w > _lib.RING_MAX or h > _lib.RING_MAX:
+            raise ValueError('approx3 boxes up to %d pixels a side' % _lib.RING_MAX)
+        r = np.zeros(1, _lib.RING_ITEM)[0]
+        r['val_off'], r['deriv_off'] = val_off, deriv_off
+        r['edge_col_off'] = edge_col[1] if edge_col else -1
+        r['edge_row_off'] = edge_row[1] if edge_row else -1
+        r['edge_x'] = edge_col[0] if edge_col else 0
+        r['edge_y'] = edge_row[0] if edge_row else 0
+        r['w'], r['h'] = w, h
+        r['start_inside'] = start is not None
+        r['xc'], r['yc'] = start if start is not None else (0, 0)
+        r['dcx'], r['dcy'] = default_start
+        r['minradius'] = minradius
+        r['minval'] = minval
+        self.rings.append(r)
+        return len(self.rings) - 1
 
     def add(self, x0, y0, w, h, amp, mean, var, fx=0., fy=0., floor=FLOOR_GRID, scale=1.,
             mask=None, out_off=None, ldo=0, mode=MOG_STORE, minval=None, derivs=False,
@@ -193,6 +219,8 @@ class MogBatch(object):
         o_mask = pk.add(np.concatenate(self.masks)) if self.masks else None
         o_ctr = pk.add(np.zeros(4, np.int32))
         o_st = pk.add(np.zeros(1, _lib.STATUS))
+        o_ring = pk.add(np.array(self.rings, _lib.RING_ITEM)) if self.rings else None
+        o_rst = pk.add(np.zeros(1, _lib.STATUS))
         d = pk.to_device(dev)
         base = d.data_ptr()
         rc = lib.tb_mog_render(base + o_items, len(items), n_tiles, base + o_amp, base + o_mean,
@@ -200,10 +228,21 @@ class MogBatch(object):
                                out.data_ptr(), base + o_ctr, base + o_st,
                                _lib.stream_ptr(stream))
         _lib.check(rc, 'tb_mog_render')
+        self.extents = None
+        self.ring_status = None
+        if self.rings:
+            self.extents = torch.empty(4 * len(self.rings), dtype=torch.int32, device=dev)
+            rc = lib.tb_approx3_region(base + o_ring, len(self.rings), out.data_ptr(),
+                                       self.extents.data_ptr(), base + o_rst,
+                                       _lib.stream_ptr(stream))
+            _lib.check(rc, 'tb_approx3_region')
+            self.ring_status = d[o_rst:o_rst + 16]
         self._dev = d
         self.status = d[o_st:o_st + 16]
         if check:
             check_status(self.status, 'tb_mog_render')
+            if self.ring_status is not None:
+                check_status(self.ring_status, 'tb_approx3_region')
         return out
 
 
