@@ -240,10 +240,10 @@ int tb_fourier_render_deriv(const tb_fft_item* items, int32_t n_items,
                             void* stream);
 
 /* The same renders (values, derivative items, TB_FFT_DOT) through the
- * split spectral path: a column kernel (units of 16 packed columns of one
+ * split spectral path: a column kernel (units of 16 rfft columns of one
  * item: the mixture spectrum times the PSF spectrum and the y taps'
- * response, inverse FFT along y, the DC and Nyquist columns packed into one
- * complex transform) writes the kept rows of every column to `workspace`
+ * response, inverse FFT along y, the real parts only of the DC and Nyquist
+ * columns) writes the kept rows of every column to `workspace`
  * (L2-resident: at most 256 items per column / row launch pair), and a row
  * kernel (units of 16 kept rows: times the x taps' response, inverse FFT
  * along x, two real rows per complex transform) writes the output.  Items

@@ -579,27 +579,25 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
 // Split spectral path (tb_fourier_render_split): a column kernel and a row
 // kernel joined by an L2-resident scratch, for every item whose Lanczos-3
 // shift is a spectral product (render_item's xin && yin) and whose output is
-// written or added (not TB_FFT_DOT).  Work units are small -- 16 packed
+// written or added (not TB_FFT_DOT).  Work units are small -- 16 rfft
 // columns or 16 kept rows of one item -- so every SM runs several CTAs of
 // 8 warps and the units of 256 galaxies spread evenly over the SMs; the
 // persistent kernel above holds one galaxy per SM and needs the whole
 // sz x (sz/2+1) transpose in its 180 KB of shared memory.
 //
-// Packed columns: c = 0 holds the DC column v = 0 in the real and the
-// Nyquist column v = N/2 in the imaginary part (both transform to real
-// columns, so one complex FFT does both); c = 1 .. N/2-1 are v = c.
-// Scratch: per item, column-major over packed columns, the kept rows
-// [gr0, gr1) of each column transform: S1[c * (gr1 - gr0) + (row - gr0)].
+// Scratch: per item, column-major over the N/2 + 1 rfft columns, the kept
+// rows [gr0, gr1) of each column transform: S1[v * (gr1 - gr0) + (row -
+// gr0)] (the DC and Nyquist columns' real parts only, as irfftn).
 // Items that are not eligible are appended to a list for the persistent
 // kernel (third launch).
 // ---------------------------------------------------------------------------
 constexpr int kSplitThreads = 256;
 constexpr int kSplitWarps = kSplitThreads / 32;
-constexpr int kColBlock = 16;                 // packed columns per column unit
+constexpr int kColBlock = 16;                 // rfft columns per column unit
+constexpr int kColUnits = (128 + 1 + kColBlock - 1) / kColBlock;   // per item at N = 256
 constexpr int kRowBlock = 16;                 // kept rows per row unit
-constexpr int kColUnits = 128 / kColBlock;    // per item at N = 256
 constexpr int kRowUnits = 256 / kRowBlock;
-constexpr int64_t kS1PerItem = 256 * 128;     // float2 per item (N x N/2 at N = 256)
+constexpr int64_t kS1PerItem = 256 * 129;     // float2 per item (N x (N/2+1) at N = 256)
 
 struct SplitWs {
     int32_t col_counter, row_counter, fb_counter, fb_count;
@@ -624,14 +622,38 @@ __device__ __forceinline__ bool item_ok(const tb_fft_item& it, const double* dco
            fabs(it.muy) <= 0.5;
 }
 
-// Normalised Lanczos-3 taps (or their derivative) with 7 threads in parallel
-// (the same terms and order as taps3 / taps3_deriv).
-__device__ void taps_parallel(double dx, bool deriv, float* f) {
-    // taps3 / taps3_deriv evaluated by one thread each: small (7 terms); the
-    // other threads wait at the caller's barrier
-    if (threadIdx.x % 32 == 0) {
-        if (deriv) taps3_deriv(dx, f); else taps3(dx, f);
+// taps3 / taps3_deriv by one warp: lane i < 7 evaluates tap i (the same
+// terms), the sums over the taps by shuffles.  Called by all 32 lanes.
+__device__ void taps_warp(double dx, bool deriv, float* f) {
+    const int i = threadIdx.x & 31;
+    double L = 0.0, D = 0.0;
+    bool on;
+    if (!deriv && dx == 0.0) {
+        if (i < 7) f[i] = i == 3 ? 1.f : 0.f;
+        return;
     }
+    if (deriv) on = i >= (dx >= 0.0 ? 0 : 1) && i < (dx >= 0.0 ? 6 : 7);
+    else on = i >= (dx > 0.0 ? 0 : 1) && i < (dx > 0.0 ? 6 : 7);
+    if (on) {
+        const double p = TB_PI * (i - 3.0 + dx);
+        if (p == 0.0) {
+            L = 1.0;
+        } else {
+            const double sp = sin(p), s3 = sin(p / 3.0);
+            L = 3.0 * sp * s3 / (p * p);
+            if (deriv) {
+                const double cp = cos(p), c3 = cos(p / 3.0);
+                D = TB_PI * 3.0 * (cp * s3 / (p * p) + sp * c3 / (3.0 * p * p) -
+                                   2.0 * sp * s3 / (p * p * p));
+            }
+        }
+    }
+    double S = L, Sd = D;
+    for (int o = 16; o > 0; o >>= 1) {
+        S += __shfl_xor_sync(0xffffffffu, S, o);
+        Sd += __shfl_xor_sync(0xffffffffu, Sd, o);
+    }
+    if (i < 7) f[i] = on ? (float)(deriv ? (D - L / S * Sd) / S : L / S) : 0.f;
 }
 
 struct SplitColShared {
@@ -680,7 +702,7 @@ __device__ __forceinline__ void spectrum_any(const tb_fft_item& it, const float4
 template <int N>
 __device__ void split_col_unit(const tb_fft_item& it, int cb, const float* __restrict__ spec,
                                float2* __restrict__ s1, SplitColShared& sh) {
-    constexpr int NH = N / 2;             // packed columns
+    constexpr int NH = N / 2 + 1;         // rfft columns
     constexpr int T = N / 8;
     constexpr int GPW = 32 / T;
     constexpr int XB = tb::fft_xbuf_elems<N>();
@@ -700,35 +722,22 @@ __device__ void split_col_unit(const tb_fft_item& it, int cb, const float* __res
         const bool act = c0 + lane / T < cend;
         const int c = act ? c0 + lane / T : cend - 1;
         float2 x[8];
-        if (c == 0) {
-            // DC (v = 0) + i Nyquist (v = N/2)
-            float a0[8], a1[8];
-            spectrum_any(it, sh.comp, sh.dcomp, 0.f, wf, a0);
-            spectrum_any(it, sh.comp, sh.dcomp, 0.5f, wf, a1);
-            const float2* P0 = reinterpret_cast<const float2*>(spec);
-            const float2* P1 = reinterpret_cast<const float2*>(spec) + (int64_t)(N / 2) * N;
+        float acc[8];
+        spectrum_any(it, sh.comp, sh.dcomp, (float)c / (float)N, wf, acc);
+        const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)c * N;
 #pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const int j = t + m * T;
-                const float2 p0 = __ldg(P0 + j), p1 = __ldg(P1 + j);
-                const float2 A = cmulf(make_float2(a0[m] * p0.x, a0[m] * p0.y), sh.hy[j]);
-                const float2 B = cmulf(make_float2(a1[m] * p1.x, a1[m] * p1.y), sh.hy[j]);
-                x[m] = make_float2(A.x - B.y, A.y + B.x);
-            }
-        } else {
-            float acc[8];
-            spectrum_any(it, sh.comp, sh.dcomp, (float)c / (float)N, wf, acc);
-            const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)c * N;
-#pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const int j = t + m * T;
-                const float2 p = __ldg(P + j);
-                x[m] = cmulf(make_float2(acc[m] * p.x, acc[m] * p.y), sh.hy[j]);
-            }
+        for (int m = 0; m < 8; m++) {
+            const int j = t + m * T;
+            const float2 p = __ldg(P + j);
+            x[m] = cmulf(make_float2(acc[m] * p.x, acc[m] * p.y), sh.hy[j]);
         }
+        // irfftn keeps only the real parts of the DC and Nyquist columns'
+        // transforms (the Nyquist column of the mixture spectrum is not
+        // Hermitian in w, so the two cannot share one complex transform)
+        const bool realcol = c == 0 || c == N / 2;
         float2* col = s1 + (int64_t)c * nr;
         tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int row, float2 z) {
-            if (act && row >= gr0 && row < gr1) col[row - gr0] = z;
+            if (act && row >= gr0 && row < gr1) col[row - gr0] = realcol ? make_float2(z.x, 0.f) : z;
         });
         __syncwarp();
     }
@@ -768,7 +777,7 @@ fourier_split_col_kernel(const tb_fft_item* __restrict__ items, int i0, int n_it
         } else if (!item_ok(it, dcoef) || !split_eligible(it)) {
             continue;
         }
-        if (cb * kColBlock >= N / 2) continue;
+        if (cb * kColBlock > N / 2) continue;
         {
             const int gr0 = max(0, -it.sy), gr1 = min(N, it.mh - it.sy);
             const int gc0 = max(0, -it.sx), gc1 = min(N, it.mw - it.sx);
@@ -776,10 +785,7 @@ fourier_split_col_kernel(const tb_fft_item* __restrict__ items, int i0, int n_it
         }
         // stage: components, y taps and their frequency response, twiddles
         stage_components(it, amp, var, dcoef, sh.comp, sh.dcomp);
-        if (threadIdx.x == 0) {
-            if (it.dmode == TB_FFT_DY) taps3_deriv(it.muy, sh.taps);
-            else taps3(it.muy, sh.taps);
-        }
+        if (threadIdx.x < 32) taps_warp(it.muy, it.dmode == TB_FFT_DY, sh.taps);
         if (sh.cur_n != N) {
             __syncthreads();
             switch (N) {
@@ -819,7 +825,7 @@ struct SplitRowShared {
     float taps[8];
     float2 hx[129];
     float2 xbuf[kSplitWarps * kXbufPerWarp];
-    float2 rows[kRowBlock * 129];     // [r][c], packed columns, padded to 129
+    float2 rows[kRowBlock * 129];     // [r][v], the N/2 + 1 rfft columns
     int cur_n;
     int64_t slot;
 };
@@ -827,7 +833,7 @@ struct SplitRowShared {
 template <int N>
 __device__ void split_row_unit(const tb_fft_item& it, int rb, const float2* __restrict__ s1,
                                float* __restrict__ out, SplitRowShared& sh) {
-    constexpr int NH = N / 2;
+    constexpr int NH = N / 2 + 1;
     constexpr int T = N / 8;
     constexpr int GPW = 32 / T;
     constexpr int XB = tb::fft_xbuf_elems<N>();
@@ -839,7 +845,7 @@ __device__ void split_row_unit(const tb_fft_item& it, int rb, const float2* __re
     const int nr = gr1 - gr0;
     const int r0 = rb * kRowBlock;
     const int nrows = min(kRowBlock, nr - r0);
-    // this unit's rows of every packed column, transposed into shared memory
+    // this unit's rows of every rfft column, transposed into shared memory
     for (int e = threadIdx.x; e < NH * kRowBlock; e += kSplitThreads) {
         const int c = e / kRowBlock, r = e % kRowBlock;
         if (r < nrows) sh.rows[r * 129 + c] = s1[(int64_t)c * nr + r0 + r];
@@ -861,17 +867,7 @@ __device__ void split_row_unit(const tb_fft_item& it, int rb, const float2* __re
         for (int m = 0; m < 8; m++) {
             const int n = t + m * T;
             const int q = n <= N / 2 ? n : N - n;
-            float2 g1, g2;
-            if (q == 0) {
-                g1 = make_float2(H1[0].x, 0.f);
-                g2 = make_float2(H2[0].x, 0.f);
-            } else if (q == N / 2) {
-                g1 = make_float2(H1[0].y, 0.f);
-                g2 = make_float2(H2[0].y, 0.f);
-            } else {
-                g1 = H1[q];
-                g2 = H2[q];
-            }
+            const float2 g1 = H1[q], g2 = H2[q];
             const float2 hx = sh.hx[q];
             const float2 h1 = cmulf(g1, hx);
             const float2 h2 = hasb ? cmulf(g2, hx) : make_float2(0.f, 0.f);
@@ -908,10 +904,7 @@ fourier_split_row_kernel(const tb_fft_item* __restrict__ items, int i0, int n_it
         const int gr0 = max(0, -it.sy), gr1 = min(N, it.mh - it.sy);
         const int gc0 = max(0, -it.sx), gc1 = min(N, it.mw - it.sx);
         if (gr0 >= gr1 || gc0 >= gc1 || rb * kRowBlock >= gr1 - gr0) continue;
-        if (threadIdx.x == 0) {
-            if (it.dmode == TB_FFT_DX) taps3_deriv(it.mux, sh.taps);
-            else taps3(it.mux, sh.taps);
-        }
+        if (threadIdx.x < 32) taps_warp(it.mux, it.dmode == TB_FFT_DX, sh.taps);
         if (sh.cur_n != N) {
             __syncthreads();
             switch (N) {
