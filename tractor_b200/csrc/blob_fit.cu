@@ -47,6 +47,8 @@ struct SrcTab {
     float dM[3][3];                // d(T T^T) / d(logre, ee1, ee2)
     int32_t K[TB_FIT_MAX_BANDS];   // components in each band (galaxy x PSF)
     int32_t ok;
+    double M64[3];                 // the same in FP64 (refinement pass)
+    double dM64[3][3];
 };
 
 // One PSF-convolved component of a (source, band), written by tb_fit_prep:
@@ -67,6 +69,17 @@ struct FitC {
     float v, dv;              // the galaxy component's variance and d/dn
     float t[4];               // tr(C^-1 dM_j) (j < 3), tr(C^-1 M)
     int32_t pad[7];
+};
+
+// The same component in FP64 for the refinement pass (tb_fit_refine): the
+// model and its derivative columns evaluated in FP64 at the end of a fit.
+struct FitC64 {
+    double mx, my;
+    double i00, i01, i11;     // C^-1
+    double s, sn;             // a / (2 pi sqrt det), d a / d n / (2 pi sqrt det)
+    double v, dv;             // galaxy variance and d/dn
+    double t[4];              // tr(C^-1 dM_j) (j < 3), tr(C^-1 M)
+    double pad[3];
 };
 
 // One component staged for one pixel row y of a tile (origin (ox, oy)) by
@@ -97,7 +110,7 @@ fit_prep_kernel(const tb_fit_source* __restrict__ srcs, int n, const double* __r
                 int n_bands, const tb_fit_unit* __restrict__ units, int n_units,
                 tb_profile_tables Tg, double cd0, double cd1, double cd2, double cd3,
                 SrcTab* __restrict__ tab, FitC* __restrict__ comps,
-                const tb_fit_state* __restrict__ state) {
+                FitC64* __restrict__ comps64, const tb_fit_state* __restrict__ state) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const tb_profile_tables T = tb::stage_tables(Tg, smem_raw);
     const int lane = threadIdx.x & 31;
@@ -229,6 +242,23 @@ fit_prep_kernel(const tb_fit_source* __restrict__ srcs, int n, const double* __r
             const bool good = det > 0.0 && isfinite(norm);
             if (!good) ok = 0;
             comps[((int64_t)i * n_bands + bd) * kCompStride + k] = c;
+            FitC64 c6;
+            c6.mx = c.mx;
+            c6.my = c.my;
+            c6.i00 = i00;
+            c6.i01 = i01;
+            c6.i11 = i11;
+            c6.s = ag * u->psf_amp[pp] * norm;
+            c6.sn = dag * u->psf_amp[pp] * norm;
+            c6.v = vg;
+            c6.dv = dvg;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const double* d = j < 3 ? dM[j] : M;
+                c6.t[j] = i00 * d[0] + 2.0 * i01 * d[1] + i11 * d[2];
+            }
+            c6.pad[0] = c6.pad[1] = c6.pad[2] = 0.0;
+            comps64[((int64_t)i * n_bands + bd) * kCompStride + k] = c6;
         }
     }
     ok = __all_sync(0xffffffffu, ok);
@@ -241,7 +271,11 @@ fit_prep_kernel(const tb_fit_source* __restrict__ srcs, int n, const double* __r
         t.ok = ok;
         for (int q = 0; q < 3; q++) {
             t.M[q] = (float)M[q];
-            for (int j = 0; j < 3; j++) t.dM[j][q] = (float)dM[j][q];
+            t.M64[q] = M[q];
+            for (int j = 0; j < 3; j++) {
+                t.dM[j][q] = (float)dM[j][q];
+                t.dM64[j][q] = dM[j][q];
+            }
         }
         tab[i] = t;
     }
@@ -760,6 +794,230 @@ __device__ double max_step(int off) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// refinement pass (tb_fit_refine): A^T r and chi^2 of finished blobs with the
+// model and its derivative columns evaluated in FP64 (FP64 exp, FP64 sums).
+// At a converged point the gradient is a sum of terms that cancel, and its
+// FP32 evaluation (FP32 model, FP32 partial sums) leaves an error that the
+// flat directions of a blob (the index and radius of a large galaxy)
+// amplify; the polish step (tb_fit_step in polish mode) takes the Newton
+// step with this gradient and the last accepted A^T A.  Same units, slices
+// and layout as tb_fit_pass; A^T A is not touched.
+// ---------------------------------------------------------------------------
+constexpr int kRefThreads = 256;       // one 32 x 8 tile, one pixel per thread
+constexpr double kPolishLambda = 1e-9; // Marquardt damping of a polish step (scaled matrix)
+
+struct RefSrc {
+    int32_t x0, y0, x1, y1;
+    int32_t K;
+    double counts;
+    double M[3];
+    double dM[3][3];
+};
+
+struct RefSmem {
+    RefSrc us[TB_FIT_MAX_SRC];
+    double red[kRefThreads / 32][8];
+    int64_t slot;
+    int skip;
+};
+
+// Block sum of v[0 .. 7) over the CTA's threads, added by thread 0 to
+// out[slot[j]] (slot[j] < 0: dropped).
+__device__ __forceinline__ void ref_block_add(RefSmem& sm, const double* v, double* out,
+                                              const int* slot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 7; j++) {
+        double x = v[j];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sm.red[warp][j] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7 && slot[threadIdx.x] >= 0) {
+        double t = 0.0;
+        for (int w = 0; w < kRefThreads / 32; w++) t += sm.red[w][threadIdx.x];
+        out[slot[threadIdx.x]] += t;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kRefThreads)
+fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict__ order,
+                  int n_units, const tb_fit_blob* __restrict__ blobs,
+                  const tb_fit_source* __restrict__ srcs, const SrcTab* __restrict__ tab,
+                  const FitC64* __restrict__ gcomps, const float* __restrict__ data,
+                  const float* __restrict__ inverr, double* __restrict__ gbuf,
+                  double* __restrict__ chi2_out, const tb_fit_state* __restrict__ state,
+                  int n_bands, const int32_t* __restrict__ tiles, int32_t* counter,
+                  tb_status* st) {
+    __shared__ RefSmem sm;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    for (;;) {
+        const int64_t oi = tb::next_unit(counter, &sm.slot);
+        if (oi >= n_units) break;
+        const int ui = order[oi];
+        if (ui < 0 || ui >= n_units) continue;
+        const tb_fit_unit& u = units[ui];
+        const tb_fit_blob b = blobs[u.blob];
+        const int status = state[u.blob].status;
+        if (status != 1 && status != 2) continue;   // only converged or stopped blobs
+        const int P = b.P;
+        const int nsrc = b.n_src;
+        double* g = gbuf + b.g_off + (int64_t)u.slice * P;
+        for (int e = tid; e < P; e += kRefThreads) g[e] = 0.0;
+        if (warp == 0) {
+            const bool unit_bad = nsrc < 0 || nsrc > TB_FIT_MAX_SRC || P != nsrc * TB_FIT_NPAR ||
+                                  u.band < 0 || u.band >= n_bands || u.slice < 0 ||
+                                  u.slice >= b.n_slices || u.t0 < 0 || u.t1 < u.t0 ||
+                                  u.t1 > b.n_active;
+            bool src_bad = false;
+            if (!unit_bad && lane < nsrc) {
+                const SrcTab& S = tab[b.src0 + lane];
+                const int K = S.K[u.band];
+                src_bad = !S.ok || K < 0 || K > kCompStride;
+                const tb_fit_source fs = srcs[b.src0 + lane];
+                const bool live = fs.w > 0 && fs.h > 0;
+                RefSrc R;
+                R.x0 = live ? fs.x0 : 0;
+                R.y0 = live ? fs.y0 : 0;
+                R.x1 = live ? fs.x0 + fs.w : 0;
+                R.y1 = live ? fs.y0 + fs.h : 0;
+                R.K = K;
+                R.counts = S.flux[u.band];
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    R.M[q] = S.M64[q];
+#pragma unroll
+                    for (int j = 0; j < 3; j++) R.dM[j][q] = S.dM64[j][q];
+                }
+                sm.us[lane] = R;
+            }
+            const bool bad = unit_bad || __any_sync(0xffffffffu, src_bad);
+            if (lane == 0) {
+                sm.skip = bad;
+                if (bad) tb::report(st, TB_STATUS_BAD_ITEM, ui, nsrc);
+            }
+        }
+        __syncthreads();
+        if (sm.skip) {
+            if (tid == 0) chi2_out[b.unit0 + u.slice] = INFINITY;
+            continue;
+        }
+        const FitC64* band_comps = gcomps + ((int64_t)b.src0 * n_bands + u.band) * kCompStride;
+        const int64_t cstride = (int64_t)n_bands * kCompStride;
+        const int n_t = u.t1 - u.t0;
+        const int32_t* tl = tiles + b.tile_off + u.t0;
+        double chi2 = 0.0;
+        for (int t = 0; t < n_t; t++) {
+            const int ox = (tl[t] & 0x3ff) * kTileW, oy = ((tl[t] >> 10) & 0x3ff) * kTileH;
+            const int px = ox + lane, py = oy + warp;
+            const bool in = px < u.W && py < u.H;
+            double d = 0.0, w = 0.0;
+            if (in) {
+                const int64_t pix = u.pix_off + (int64_t)py * u.W + px;
+                d = data[pix];
+                w = inverr[pix];
+            }
+            // the model at this pixel
+            double m = 0.0;
+            for (int sI = 0; sI < nsrc; sI++) {
+                const RefSrc& R = sm.us[sI];
+                if (!(px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1) || !in) continue;
+                const FitC64* cs = band_comps + sI * cstride;
+                double val = 0.0;
+                for (int k = 0; k < R.K; k++) {
+                    const FitC64& c = cs[k];
+                    const double dx = px - c.mx, dy = py - c.my;
+                    const double e = -0.5 * (c.i00 * dx * dx + 2.0 * c.i01 * dx * dy +
+                                             c.i11 * dy * dy);
+                    if (e >= -50.0) val += c.s * exp(e);
+                }
+                m += R.counts * val;
+            }
+            const double r = (d - m) * w;
+            chi2 += r * r;
+            // each source reaching the tile: its seven columns times inverr times r
+            for (int sI = 0; sI < nsrc; sI++) {
+                const RefSrc& R = sm.us[sI];
+                if (R.x1 <= ox || R.x0 >= ox + kTileW || R.y1 <= oy || R.y0 >= oy + kTileH)
+                    continue;   // the same for every thread of the tile
+                double J[7] = {0, 0, 0, 0, 0, 0, 0};
+                if (in && px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1) {
+                    const FitC64* cs = band_comps + sI * cstride;
+                    double S0 = 0, Sx = 0, Sy = 0, Axx = 0, Axy = 0, Ayy = 0;
+                    double At[3] = {0, 0, 0};
+                    double Dxx = 0, Dxy = 0, Dyy = 0, Dt = 0, Sn = 0;
+                    for (int k = 0; k < R.K; k++) {
+                        const FitC64& c = cs[k];
+                        const double dx = px - c.mx, dy = py - c.my;
+                        const double e = -0.5 * (c.i00 * dx * dx + 2.0 * c.i01 * dx * dy +
+                                                 c.i11 * dy * dy);
+                        if (e < -50.0) continue;
+                        const double E = exp(e);
+                        const double val = c.s * E;
+                        const double ux = c.i00 * dx + c.i01 * dy, uy = c.i01 * dx + c.i11 * dy;
+                        S0 += val;
+                        Sx += val * ux;
+                        Sy += val * uy;
+                        const double vv = val * c.v;
+                        Axx += vv * ux * ux;
+                        Axy += vv * ux * uy;
+                        Ayy += vv * uy * uy;
+                        At[0] += vv * c.t[0];
+                        At[1] += vv * c.t[1];
+                        At[2] += vv * c.t[2];
+                        const double vd = val * c.dv;
+                        Dxx += vd * ux * ux;
+                        Dxy += vd * ux * uy;
+                        Dyy += vd * uy * uy;
+                        Dt += vd * c.t[3];
+                        Sn += c.sn * E;
+                    }
+                    const double cn = R.counts;
+                    J[0] = cn * Sx;
+                    J[1] = cn * Sy;
+                    J[2] = S0;
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                        J[3 + j] = cn * 0.5 * (R.dM[j][0] * Axx + 2.0 * R.dM[j][1] * Axy +
+                                               R.dM[j][2] * Ayy - At[j]);
+                    J[6] = cn * (0.5 * (R.M[0] * Dxx + 2.0 * R.M[1] * Dxy + R.M[2] * Dyy - Dt) +
+                                 Sn);
+                    const double wr = w * r;
+#pragma unroll
+                    for (int j = 0; j < 7; j++) J[j] *= wr;
+                }
+                // columns x y flux(band) logre ee1 ee2 n -> the source's slots
+                const tb_fit_source fs = srcs[b.src0 + sI];
+                int slot[7];
+                const int base = sI * TB_FIT_NPAR;
+                slot[0] = base + 0;
+                slot[1] = base + 1;
+                slot[2] = base + 2 + u.band;
+                slot[3] = base + 5;
+                slot[4] = base + 6;
+                slot[5] = base + 7;
+                slot[6] = base + 8;
+                if (fs.profile == TB_PROFILE_POINT) slot[3] = slot[4] = slot[5] = slot[6] = -1;
+                else if (fs.profile != TB_PROFILE_SERSIC) slot[6] = -1;
+                ref_block_add(sm, J, g, slot);
+            }
+        }
+        // the unit's chi^2 (its active tiles; the constant part stays in chi2_const)
+        for (int o = 16; o > 0; o >>= 1) chi2 += __shfl_xor_sync(0xffffffffu, chi2, o);
+        if (lane == 0) sm.red[warp][0] = chi2;
+        __syncthreads();
+        if (tid == 0) {
+            double c2 = 0.0;
+            for (int w2 = 0; w2 < kRefThreads / 32; w2++) c2 += sm.red[w2][0];
+            chi2_out[b.unit0 + u.slice] = c2;
+        }
+        __syncthreads();
+    }
+}
+
 // One CTA per blob.  The factor lives in the blob's global area (L2
 // resident); shared memory and registers stay small so that five blobs
 // share an SM.
@@ -768,7 +1026,7 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
                 const tb_fit_source* __restrict__ srcs, double* __restrict__ params,
                 double* __restrict__ trial, double* __restrict__ hbuf, double* __restrict__ gbuf,
                 const double* __restrict__ chi2_part, tb_fit_state* __restrict__ state,
-                double tol, int max_iter) {
+                double tol, int max_iter, int polish) {
     __shared__ double dsc[TB_FIT_MAX_SRC * TB_FIT_NPAR];
     __shared__ double dinv[TB_FIT_MAX_SRC * TB_FIT_NPAR];
     __shared__ double y[TB_FIT_MAX_SRC * TB_FIT_NPAR];
@@ -785,7 +1043,9 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     tb_fit_state& S = state[bi];
     const int status0 = S.status;
     __syncthreads();   // every thread has read the status before thread 0 updates it
-    if (status0 != 0) return;
+    // an iteration works on running blobs; a polish step on converged or
+    // stopped ones (their last accepted A^T A, the refinement pass's A^T r)
+    if (polish ? (status0 != 1 && status0 != 2) : status0 != 0) return;
     const int P = b.P;
     const int ns = b.n_slices;
     double* Hp = hbuf + b.h_off;                        // slice partials
@@ -796,7 +1056,12 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     double* pa = params + (int64_t)b.src0 * TB_FIT_NPAR;
     double* pt = trial + (int64_t)b.src0 * TB_FIT_NPAR;
 
-    if (tid == 0) {
+    if (polish && tid == 0) {
+        s_accept = 0;
+        s_lambda = kPolishLambda;
+        s_active = 1;
+    }
+    if (!polish && tid == 0) {
         double c2 = 0.0;
         for (int k = 0; k < ns; k++) c2 += chi2_part[b.unit0 + k];
         const bool first = S.accepted == 0;
@@ -830,6 +1095,14 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
                 Ha[(int64_t)r * P + c] = s;
                 Ha[(int64_t)c * P + r] = s;
             }
+        for (int e = tid; e < P; e += kStepThreads) {
+            double s = 0.0;
+            for (int k = 0; k < ns; k++) s += gp[(int64_t)k * P + e];
+            ga[e] = s;
+        }
+    }
+    if (polish) {
+        // the refinement pass's slices of A^T r, in the same fixed order
         for (int e = tid; e < P; e += kStepThreads) {
             double s = 0.0;
             for (int k = 0; k < ns; k++) s += gp[(int64_t)k * P + e];
@@ -888,7 +1161,8 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     }
     if (bad) {
         // not positive definite: treat as a rejected step with more damping
-        if (tid == 0) {
+        // (a polish step is left out)
+        if (tid == 0 && !polish) {
             S.lambda *= 10.0;
             if (!(S.lambda < 1e12)) S.status = 2;
         }
@@ -978,8 +1252,10 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
             double t = 0.0;
             for (int w2 = 0; w2 < kStepThreads / 32; w2++) t += red[w2];
             S.pred = 0.5 * t;
-            s_active = !(0.5 * t < tol && lam <= 1.0);
-            if (!s_active) S.status = 1;
+            if (!polish) {
+                s_active = !(0.5 * t < tol && lam <= 1.0);
+                if (!s_active) S.status = 1;
+            }
         }
         __syncthreads();
         if (!s_active) {
@@ -1017,6 +1293,7 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
             srcs[b.src0 + i / TB_FIT_NPAR].profile == TB_PROFILE_SERSIC)
             v = fmin(fmax(v, TB_FIT_SERSIC_MIN), TB_FIT_SERSIC_MAX);
         pt[i] = v;
+        if (polish) pa[i] = v;   // a polish step is taken without a trial
     }
 }
 
@@ -1040,7 +1317,8 @@ __global__ void fit_reset_kernel(tb_fit_state* state, int n, double lambda0) {
 extern "C" int tb_fit_workspace(int32_t n_src, int32_t n_bands, int64_t* bytes) {
     if (n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS || !bytes) return TB_ERR_ARG;
     const int64_t tab = ((int64_t)n_src * (int64_t)sizeof(SrcTab) + 255) / 256 * 256;
-    *bytes = tab + (int64_t)n_src * n_bands * kCompStride * (int64_t)sizeof(FitC);
+    const int64_t nc = (int64_t)n_src * n_bands * kCompStride;
+    *bytes = tab + nc * (int64_t)sizeof(FitC) + nc * (int64_t)sizeof(FitC64);
     return TB_OK;
 }
 
@@ -1049,6 +1327,10 @@ inline SrcTab* ws_tab(void* ws) { return static_cast<SrcTab*>(ws); }
 inline FitC* ws_comps(void* ws, int32_t n_src) {
     const int64_t tab = ((int64_t)n_src * (int64_t)sizeof(SrcTab) + 255) / 256 * 256;
     return reinterpret_cast<FitC*>(static_cast<char*>(ws) + tab);
+}
+inline FitC64* ws_comps64(void* ws, int32_t n_src, int32_t n_bands) {
+    return reinterpret_cast<FitC64*>(ws_comps(ws, n_src) +
+                                     (int64_t)n_src * n_bands * kCompStride);
 }
 }  // namespace
 
@@ -1078,7 +1360,7 @@ extern "C" int tb_fit_prep(const tb_fit_source* srcs, int32_t n_src, const doubl
                       (cudaStream_t)stream>>>(srcs, n_src, params, n_bands, units, n_units,
                                               *tables, cd_inv[0], cd_inv[1], cd_inv[2], cd_inv[3],
                                               ws_tab(workspace), ws_comps(workspace, n_src),
-                                              state);
+                                              ws_comps64(workspace, n_src, n_bands), state);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
@@ -1125,6 +1407,46 @@ extern "C" int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_
     if (!blobs || !srcs || !params || !trial || !hbuf || !gbuf || !chi2_part || !state)
         return TB_ERR_ARG;
     fit_step_kernel<<<n_blobs, kStepThreads, 0, (cudaStream_t)stream>>>(
-        blobs, n_blobs, n_bands, srcs, params, trial, hbuf, gbuf, chi2_part, state, tol, max_iter);
+        blobs, n_blobs, n_bands, srcs, params, trial, hbuf, gbuf, chi2_part, state, tol, max_iter,
+        0);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+extern "C" int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
+                             const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
+                             const void* workspace, const float* data, const float* inverr,
+                             const int32_t* tiles, double* gbuf, double* chi2_out,
+                             const tb_fit_state* state, int32_t n_bands, int32_t* work_counter,
+                             tb_status* status, void* stream) {
+    if (n_units < 0 || n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS) return TB_ERR_ARG;
+    if (n_units == 0) return TB_OK;
+    if (!units || !order || !blobs || !srcs || !workspace || !data || !inverr || !tiles ||
+        !gbuf || !chi2_out || !state || !work_counter)
+        return TB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync(work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return TB_ERR_LAUNCH;
+    if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fit_refine_kernel, kRefThreads,
+                                                      0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int64_t want = (int64_t)tb::num_sms() * per_sm;
+    const int grid = (int)(n_units < want ? n_units : want);
+    void* ws = const_cast<void*>(workspace);
+    fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
+        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands), data,
+        inverr, gbuf, chi2_out, state, n_bands, tiles, work_counter, status);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+extern "C" int tb_fit_polish(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
+                             const tb_fit_source* srcs, double* params, double* trial,
+                             double* hbuf, double* gbuf, tb_fit_state* state, void* stream) {
+    if (n_blobs < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS) return TB_ERR_ARG;
+    if (n_blobs == 0) return TB_OK;
+    if (!blobs || !srcs || !params || !trial || !hbuf || !gbuf || !state) return TB_ERR_ARG;
+    fit_step_kernel<<<n_blobs, kStepThreads, 0, (cudaStream_t)stream>>>(
+        blobs, n_blobs, n_bands, srcs, params, trial, hbuf, gbuf, nullptr, state, 0.0, 0, 1);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }

@@ -131,6 +131,7 @@ class BlobFitter(object):
         self.chi2_part = torch.zeros(int(n_slices.sum()), dtype=torch.float64,
                                      device=self.dev)
         self.chi2_const = torch.zeros_like(self.chi2_part)
+        self.chi2_refine = torch.zeros_like(self.chi2_part)
         self._const_done = False
         self.state = torch.zeros(self.n_blobs * _lib.FIT_STATE.itemsize, dtype=torch.uint8,
                                  device=self.dev)
@@ -146,13 +147,43 @@ class BlobFitter(object):
         self._graph = None
 
     # -- one iteration -----------------------------------------------------
-    def _prep(self):
+    def _prep(self, all_blobs=False):
         lib = _lib.load()
         _lib.check(lib.tb_fit_prep(self.d_sources.data_ptr(), self.n_src, self.trial.data_ptr(),
                                    self.n_bands, self.d_units.data_ptr(), len(self.units_np),
                                    self.cd_inv.ctypes.data, ctypes.addressof(self.tables.struct),
-                                   self.workspace.data_ptr(), self.state.data_ptr(),
+                                   self.workspace.data_ptr(),
+                                   None if all_blobs else self.state.data_ptr(),
                                    _lib.stream_ptr()), 'tb_fit_prep')
+
+    def refine(self, steps=2):
+        """Polishes every converged or stopped blob: `steps` times, A^T r at
+        the parameters with the model and derivatives in FP64
+        (tb_fit_refine), then one Gauss-Newton step with the last accepted
+        A^T A (tb_fit_polish).  The FP32 passes leave the gradient's
+        cancellation error, which a blob's flat directions (a large
+        galaxy's index and radius) amplify; this brings the parameters to
+        the FP64 optimum.  The states' chi^2 stays that of the last
+        iteration."""
+        lib = _lib.load()
+        s = _lib.stream_ptr()
+        for _ in range(int(steps)):
+            self.trial.copy_(self.params)
+            self._prep(all_blobs=True)
+            _lib.check(lib.tb_fit_refine(self.d_pass_units.data_ptr(), self.d_order.data_ptr(),
+                                         len(self.pass_units_np), self.d_blobs.data_ptr(),
+                                         self.d_sources.data_ptr(), self.n_src,
+                                         self.workspace.data_ptr(), self.data.data_ptr(),
+                                         self.inverr.data_ptr(), self.d_tiles.data_ptr(),
+                                         self.gbuf.data_ptr(), self.chi2_refine.data_ptr(),
+                                         self.state.data_ptr(), self.n_bands,
+                                         self.misc.data_ptr(), self.misc.data_ptr() + 16, s),
+                       'tb_fit_refine')
+            _lib.check(lib.tb_fit_polish(self.d_blobs.data_ptr(), self.n_blobs, self.n_bands,
+                                         self.d_sources.data_ptr(), self.params.data_ptr(),
+                                         self.trial.data_ptr(), self.hbuf.data_ptr(),
+                                         self.gbuf.data_ptr(), self.state.data_ptr(), s),
+                       'tb_fit_polish')
 
     def _pass(self, mode):
         lib = _lib.load()
@@ -198,8 +229,9 @@ class BlobFitter(object):
         return int((st[:, -1] == 0).sum().item())
 
     def fit(self, tol=1e-3, max_iter=50, check_every=4, graph=True, params0=None,
-            lambda0=1e-3):
-        """Runs iterations until every blob stops (or max_iter).  Returns the
+            lambda0=1e-3, refine=2):
+        """Runs iterations until every blob stops (or max_iter), then
+        `refine` FP64-gradient polish steps (see refine()).  Returns the
         number of iterations launched."""
         self.reset(params0, lambda0)
         g = None
@@ -214,6 +246,8 @@ class BlobFitter(object):
             self.iterations += check_every
             if self.running() == 0:
                 break
+        if refine:
+            self.refine(refine)
         return self.iterations
 
     def _capture(self, k, tol, max_iter):
