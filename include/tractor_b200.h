@@ -666,6 +666,26 @@ int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int32_t n_unit
                   const tb_fit_state* state, int32_t n_bands, int32_t* work_counter,
                   tb_status* status, void* stream);
 
+/* The blobs' model and its vector-Jacobian product, in FP64 (the
+ * refinement pass's evaluation): mode TB_FIT_MODEL writes every unit's
+ * model (sum of the sources' PSF-convolved mixtures over their masks) into
+ * `model` at the active tiles' pixels (the caller zeroes the rest); mode
+ * TB_FIT_VJP contracts each source's derivative columns (x, y, flux of the
+ * band, log r_e, ee1, ee2, n: the derivatives Galaxy.getParamDerivatives and
+ * PointSource.getParamDerivatives approximate, tractor/galaxy.py:137-223,
+ * tractor/pointsource.py:130-241) with the upstream gradient `grad` (laid
+ * out as the data), into the gbuf slices (summed over a blob's slices, the
+ * gradient with respect to its parameters).  Run tb_fit_prep with state =
+ * NULL at the parameters first. */
+#define TB_FIT_REFINE 0
+#define TB_FIT_MODEL 1
+#define TB_FIT_VJP 2
+int tb_fit_model_vjp(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
+                     const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
+                     const void* workspace, const float* grad, float* model,
+                     const int32_t* tiles, double* gbuf, int32_t n_bands, int32_t mode,
+                     int32_t* work_counter, tb_status* status, void* stream);
+
 /* One polish step per converged or stopped blob: the step of tb_fit_step with
  * the last accepted A^T A, the A^T r of tb_fit_refine and a Marquardt
  * damping of 1e-9 (the Gauss-Newton step), the same maximum steps, bounds and

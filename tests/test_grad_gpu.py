@@ -185,3 +185,91 @@ def test_columns_match_reference_getParamDerivatives(tb):
         if not e < t:
             bad[k] = e
     assert not bad, (bad, errs)
+
+
+def _blob_oracle_model(oracle, params, profiles, rects, W, H, psf):
+    """FP64 model of one blob (3 bands): Sersic galaxies through the oracle's
+    blob model, point sources as the PSF mixture at their position (the
+    reference's PointSource through GaussianMixturePSF.getPointSourcePatch)."""
+    from tractor_b200 import _lib
+    out = np.zeros((3, H, W))
+    for th, prof, (x0, y0, w, h) in zip(params, profiles, rects):
+        X0, Y0, X1, Y1 = max(x0, 0), max(y0, 0), min(x0 + w, W), min(y0 + h, H)
+        if prof == _lib.PROFILE_SERSIC:
+            out += oracle.blob_model(th[None], [(x0, y0, w, h)], W, H, psf, 3)
+            continue
+        for k in range(3):
+            pamp, pmean, pvar = psf[k]
+            out[k, Y0:Y1, X0:X1] += th[2 + k] * oracle.mog_grid(X0, X1, Y0, Y1, th[0], th[1],
+                                                                pamp, pmean, pvar)
+    return out
+
+
+def test_mog_blob_adjoint_matches_fp64_central_differences(tb, oracle):
+    """The mixture-of-Gaussians PSF path behind torch.autograd
+    (grad.RenderBlobs over tb_fit_model_vjp): the model of two 3-band blobs
+    (Sersic galaxies, a point source) against the oracle's FP64 model (1e-6
+    of the peak), and backward -- the analytic vector-Jacobian product --
+    against FP64 central differences of the oracle's model contracted with
+    the same upstream gradient, every parameter of every source (x, y, the
+    three fluxes, log r_e, ee1, ee2, n; a point source's x, y and fluxes),
+    within 1e-6 of |G| |column|."""
+    import torch
+    from tractor_b200 import fit, grad, _lib
+    rng = np.random.default_rng(61)
+    w = fit.blob_workload(2, rng, side_range=(44, 52), mean_src=2, max_src=2,
+                          flux_range=(500., 3000.))
+    w['blob_src'] = np.array([0, 2, 4])
+    n = 4
+    w['truth'] = np.resize(w['truth'], (n, 9))
+    w['sources'] = np.resize(w['sources'], n)
+    for i in range(n):
+        W = int(w['sides'][i // 2, 0])
+        w['truth'][i, 0:2] = rng.uniform(14, W - 14, 2)
+        w['truth'][i, 8] = [0.8, 2.3, 4.6, 1.5][i]
+        hw = 12
+        cx, cy = (int(round(v)) for v in w['truth'][i, :2])
+        w['sources'][i] = (_lib.PROFILE_SERSIC, cx - hw, cy - hw, 2 * hw + 1, 2 * hw + 1,
+                           i // 2, 0, 0)
+    w['sources'][3]['profile'] = _lib.PROFILE_POINT
+    w['truth'][3, 5:9] = 0.
+    npix = int(fit.pix_offsets(w['sides'], 3)[-1])
+    zeros = torch.zeros(npix, dtype=torch.float32, device='cuda')
+    f = fit.BlobFitter(w['blob_src'], w['sides'], w['psf'], w['sources'], w['truth'], zeros,
+                       torch.ones_like(zeros))
+    bm = grad.BlobModel(f)
+    theta = torch.tensor(w['truth'], dtype=torch.float64, device='cuda', requires_grad=True)
+    model = grad.RenderBlobs.apply(theta, bm)
+    G = torch.randn(npix, generator=torch.Generator(device='cuda').manual_seed(3),
+                    device='cuda', dtype=torch.float32)
+    (model * G).sum().backward()
+    got = theta.grad.cpu().numpy()
+    m = model.detach().cpu().numpy()
+    Gh = G.cpu().numpy().astype(np.float64)
+    po = fit.pix_offsets(w['sides'], 3)
+    for b in range(2):
+        s0, s1 = w['blob_src'][b], w['blob_src'][b + 1]
+        W, H = (int(v) for v in w['sides'][b])
+        rects = [tuple(int(v) for v in (r['x0'], r['y0'], r['w'], r['h']))
+                 for r in w['sources'][s0:s1]]
+        prof = w['sources']['profile'][s0:s1]
+        ref = _blob_oracle_model(oracle, w['truth'][s0:s1], prof, rects, W, H, w['psf'][b])
+        mine = np.stack([m[po[3 * b + k]:po[3 * b + k + 1]].reshape(H, W) for k in range(3)])
+        assert np.abs(mine - ref).max() <= 1e-6 * np.abs(ref).max()
+        Gb = np.stack([Gh[po[3 * b + k]:po[3 * b + k + 1]].reshape(H, W) for k in range(3)])
+        steps = [1e-5, 1e-5, 1., 1., 1., 1e-5, 1e-5, 1e-5, 1e-5]
+        for i in range(s0, s1):
+            slots = range(9) if prof[i - s0] == _lib.PROFILE_SERSIC else range(5)
+            for j in slots:
+                tp, tm = w['truth'][s0:s1].copy(), w['truth'][s0:s1].copy()
+                tp[i - s0, j] += steps[j]
+                tm[i - s0, j] -= steps[j]
+                col = (_blob_oracle_model(oracle, tp, prof, rects, W, H, w['psf'][b]) -
+                       _blob_oracle_model(oracle, tm, prof, rects, W, H, w['psf'][b])) / \
+                    (2 * steps[j])
+                fd = float((Gb * col).sum())
+                scale = np.sqrt((Gb ** 2).sum() * (col ** 2).sum())
+                assert abs(got[i, j] - fd) <= 1e-6 * scale + 1e-6 * abs(fd), \
+                    (i, j, got[i, j], fd, scale)
+        # parameters a source does not have get zero gradient
+    assert np.all(got[3, 5:] == 0)

@@ -54,6 +54,7 @@ SCENE_ITEM = np.dtype([('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'), ('h', '<i4'),
                        ('fx', '<f8'), ('fy', '<f8'), ('scale', '<f4'), ('floor', '<f4')])
 
 FIT_NPAR, FIT_MAX_BANDS, FIT_MAX_SRC, FIT_MAX_PSF = 9, 3, 32, 4
+FIT_REFINE, FIT_MODEL, FIT_VJP = 0, 1, 2
 EM_MAX_K = 8   # TB_EM_MAX_K
 FIT_SOURCE = np.dtype([('profile', '<i4'), ('x0', '<i4'), ('y0', '<i4'), ('w', '<i4'),
                        ('h', '<i4'), ('blob', '<i4'), ('frozen', '<i4'), ('pad', '<i4')])
@@ -138,6 +139,8 @@ SIGNATURES = {
     'tb_fit_refine': (_I32, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _I32, _P,
                              _P, _P]),
     'tb_fit_polish': (_I32, [_P, _I32, _I32, _P, _P, _P, _P, _P, _P, _P]),
+    'tb_fit_model_vjp': (_I32, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P, _I32, _I32, _P,
+                                _P, _P]),
     'tb_scene_render': (_I32, [_P, _I32, _P, _I32, _I64, _I32, _P, _P, _P, _P, _I32, _P, _I64,
                                _I64, _P, _P]),
     'tb_version': (ctypes.c_char_p, []),

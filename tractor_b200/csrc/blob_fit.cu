@@ -850,7 +850,10 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
                   const float* __restrict__ inverr, double* __restrict__ gbuf,
                   double* __restrict__ chi2_out, const tb_fit_state* __restrict__ state,
                   int n_bands, const int32_t* __restrict__ tiles, int32_t* counter,
-                  tb_status* st) {
+                  tb_status* st, int mode, float* __restrict__ model_out) {
+    // mode TB_FIT_REFINE: A^T r of finished blobs, r = (data - model) inverr;
+    // TB_FIT_MODEL: the model into model_out (every blob); TB_FIT_VJP: the
+    // columns contracted with data = an upstream gradient, unweighted
     __shared__ RefSmem sm;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -861,12 +864,15 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
         if (ui < 0 || ui >= n_units) continue;
         const tb_fit_unit& u = units[ui];
         const tb_fit_blob b = blobs[u.blob];
-        const int status = state[u.blob].status;
-        if (status != 1 && status != 2) continue;   // only converged or stopped blobs
+        if (mode == TB_FIT_REFINE) {
+            const int status = state[u.blob].status;
+            if (status != 1 && status != 2) continue;   // only converged or stopped blobs
+        }
         const int P = b.P;
         const int nsrc = b.n_src;
         double* g = gbuf + b.g_off + (int64_t)u.slice * P;
-        for (int e = tid; e < P; e += kRefThreads) g[e] = 0.0;
+        if (mode != TB_FIT_MODEL)
+            for (int e = tid; e < P; e += kRefThreads) g[e] = 0.0;
         if (warp == 0) {
             const bool unit_bad = nsrc < 0 || nsrc > TB_FIT_MAX_SRC || P != nsrc * TB_FIT_NPAR ||
                                   u.band < 0 || u.band >= n_bands || u.slice < 0 ||
@@ -902,7 +908,7 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
         }
         __syncthreads();
         if (sm.skip) {
-            if (tid == 0) chi2_out[b.unit0 + u.slice] = INFINITY;
+            if (tid == 0 && chi2_out) chi2_out[b.unit0 + u.slice] = INFINITY;
             continue;
         }
         const FitC64* band_comps = gcomps + ((int64_t)b.src0 * n_bands + u.band) * kCompStride;
@@ -915,14 +921,14 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
             const int px = ox + lane, py = oy + warp;
             const bool in = px < u.W && py < u.H;
             double d = 0.0, w = 0.0;
+            const int64_t pix = u.pix_off + (int64_t)py * u.W + px;
             if (in) {
-                const int64_t pix = u.pix_off + (int64_t)py * u.W + px;
                 d = data[pix];
-                w = inverr[pix];
+                w = mode == TB_FIT_VJP ? 1.0 : inverr[pix];
             }
             // the model at this pixel
             double m = 0.0;
-            for (int sI = 0; sI < nsrc; sI++) {
+            for (int sI = 0; sI < nsrc && mode != TB_FIT_VJP; sI++) {
                 const RefSrc& R = sm.us[sI];
                 if (!(px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1) || !in) continue;
                 const FitC64* cs = band_comps + sI * cstride;
@@ -936,7 +942,11 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
                 }
                 m += R.counts * val;
             }
-            const double r = (d - m) * w;
+            if (mode == TB_FIT_MODEL) {
+                if (in) model_out[pix] = (float)m;
+                continue;
+            }
+            const double r = mode == TB_FIT_VJP ? d : (d - m) * w;
             chi2 += r * r;
             // each source reaching the tile: its seven columns times inverr times r
             for (int sI = 0; sI < nsrc; sI++) {
@@ -1009,7 +1019,7 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
         for (int o = 16; o > 0; o >>= 1) chi2 += __shfl_xor_sync(0xffffffffu, chi2, o);
         if (lane == 0) sm.red[warp][0] = chi2;
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && chi2_out) {
             double c2 = 0.0;
             for (int w2 = 0; w2 < kRefThreads / 32; w2++) c2 += sm.red[w2][0];
             chi2_out[b.unit0 + u.slice] = c2;
@@ -1436,7 +1446,37 @@ extern "C" int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int
     void* ws = const_cast<void*>(workspace);
     fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
         units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands), data,
-        inverr, gbuf, chi2_out, state, n_bands, tiles, work_counter, status);
+        inverr, gbuf, chi2_out, state, n_bands, tiles, work_counter, status, TB_FIT_REFINE,
+        nullptr);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+extern "C" int tb_fit_model_vjp(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
+                                const tb_fit_blob* blobs, const tb_fit_source* srcs,
+                                int32_t n_src, const void* workspace, const float* grad,
+                                float* model, const int32_t* tiles, double* gbuf,
+                                int32_t n_bands, int32_t mode, int32_t* work_counter,
+                                tb_status* status, void* stream) {
+    if (n_units < 0 || n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS) return TB_ERR_ARG;
+    if (mode != TB_FIT_MODEL && mode != TB_FIT_VJP) return TB_ERR_ARG;
+    if (n_units == 0) return TB_OK;
+    if (!units || !order || !blobs || !srcs || !workspace || !tiles || !work_counter ||
+        (mode == TB_FIT_MODEL && !model) || (mode == TB_FIT_VJP && (!grad || !gbuf)))
+        return TB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync(work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return TB_ERR_LAUNCH;
+    if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fit_refine_kernel, kRefThreads,
+                                                      0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int64_t want = (int64_t)tb::num_sms() * per_sm;
+    const int grid = (int)(n_units < want ? n_units : want);
+    void* ws = const_cast<void*>(workspace);
+    fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
+        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands), grad,
+        nullptr, gbuf, nullptr, nullptr, n_bands, tiles, work_counter, status, mode, model);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 

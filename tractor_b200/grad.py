@@ -1,5 +1,6 @@
-"""Analytic parameter derivatives of the pixelized-PSF (Fourier) path and a
-torch.autograd.Function around it.
+"""Analytic parameter derivatives of the pixelized-PSF (Fourier) path and of
+the mixture-of-Gaussians PSF path (blobs of galaxies and point sources), each
+behind a torch.autograd.Function.
 
 For each galaxy, tb_galaxy_fft_jac_prep makes seven derivative items on the
 geometry of its value item -- position (x, y) through the derivative of the
@@ -118,3 +119,91 @@ class RenderGalaxies(torch.autograd.Function):
             jac = ctx.renderer._jacobian = FourierJacobian(ctx.renderer)
         g, _, _ = jac.vjp(ctx.rec, ctx.n, grad_out.float())
         return g, None, None, None
+
+
+# ---------------------------------------------------------------------------
+# Mixture-of-Gaussians PSF path: blobs of point sources and galaxies
+# ---------------------------------------------------------------------------
+
+class BlobModel(object):
+    """The model images of a BlobFitter's blobs as a function of their
+    parameters (n_src, 9: x, y, flux per band, log r_e, ee1, ee2, Sersic n),
+    and the analytic vector-Jacobian product, both from tb_fit_model_vjp
+    (FP64 evaluation: the sources' PSF-convolved mixtures over their masks,
+    the derivative columns of Galaxy.getParamDerivatives /
+    PointSource.getParamDerivatives, tractor/galaxy.py:137-223,
+    tractor/pointsource.py:130-241, taken analytically).  The images are laid
+    out as the fitter's data (fit.pix_offsets)."""
+
+    def __init__(self, fitter):
+        self.f = fitter
+        f = fitter
+        P = f.blobs_np['P'].astype(np.int64)
+        ns = f.blobs_np['n_slices'].astype(np.int64)
+        maxs = int(ns.max())
+        blob_of = np.repeat(np.arange(f.n_blobs), np.diff(np.concatenate(
+            [[0], np.cumsum(f.blobs_np['n_src'])])))
+        first = np.concatenate([[0], np.cumsum(f.blobs_np['n_src'])[:-1]])
+        idx = np.full((f.n_src * NPAR_FIT, maxs), int(f.gbuf.numel()), np.int64)
+        for q in range(f.n_src * NPAR_FIT):
+            s = q // NPAR_FIT
+            b = blob_of[s]
+            local = (s - first[b]) * NPAR_FIT + q % NPAR_FIT
+            for k in range(int(ns[b])):
+                idx[q, k] = int(f.blobs_np['g_off'][b]) + k * int(P[b]) + local
+        # slot gbuf.numel() reads a zero appended to the slices
+        self._idx = torch.from_numpy(idx).to(f.dev)
+
+    def _prep(self, theta):
+        f = self.f
+        f.trial.copy_(theta.reshape(-1).to(torch.float64))
+        f._prep(all_blobs=True)
+
+    def _launch(self, mode, grad=None, model=None):
+        f = self.f
+        lib = _lib.load()
+        _lib.check(lib.tb_fit_model_vjp(f.d_pass_units.data_ptr(), f.d_order.data_ptr(),
+                                        len(f.pass_units_np), f.d_blobs.data_ptr(),
+                                        f.d_sources.data_ptr(), f.n_src, f.workspace.data_ptr(),
+                                        None if grad is None else grad.data_ptr(),
+                                        None if model is None else model.data_ptr(),
+                                        f.d_tiles.data_ptr(), f.gbuf.data_ptr(), f.n_bands, mode,
+                                        f.misc.data_ptr(), f.misc.data_ptr() + 16,
+                                        _lib.stream_ptr()), 'tb_fit_model_vjp')
+        render.check_status(f.misc[4:8].clone(), 'tb_fit_model_vjp')
+
+    def model(self, theta):
+        """float32 (npix,) device tensor of the blobs' model images."""
+        self._prep(theta)
+        out = torch.zeros(int(self.f.pix_offsets[-1]), dtype=torch.float32, device=self.f.dev)
+        self._launch(_lib.FIT_MODEL, model=out)
+        return out
+
+    def vjp(self, theta, grad):
+        """float64 (n_src, 9): sum over the images of grad * d(model)/d(theta)."""
+        self._prep(theta)
+        g = grad.contiguous().to(torch.float32)
+        self._launch(_lib.FIT_VJP, grad=g)
+        ext = torch.cat([self.f.gbuf, torch.zeros(1, dtype=torch.float64, device=self.f.dev)])
+        return ext[self._idx].sum(dim=1).view(self.f.n_src, NPAR_FIT)
+
+
+NPAR_FIT = _lib.FIT_NPAR
+
+
+class RenderBlobs(torch.autograd.Function):
+    """model = RenderBlobs.apply(theta, blob_model): the blobs' model images
+    (float32, the fitter's data layout) as a differentiable function of theta
+    (n_src, 9) float64; backward is BlobModel.vjp, the analytic
+    vector-Jacobian product (no finite differences, no Jacobian in memory)."""
+
+    @staticmethod
+    def forward(ctx, theta, blob_model):
+        ctx.blob_model = blob_model
+        ctx.save_for_backward(theta)
+        return blob_model.model(theta.detach())
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        theta, = ctx.saved_tensors
+        return ctx.blob_model.vjp(theta.detach(), grad_out), None
