@@ -651,14 +651,14 @@ int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
                 double* gbuf, const double* chi2_part, tb_fit_state* state, double tol,
                 int32_t max_iter, void* stream);
 
-/* Refinement of finished fits (no reference counterpart beyond the optimum
- * LsqrOptimizer.optimize_loop converges to, lsqr_optimizer.py:317-326): for
- * every converged or stopped blob (status 1 or 2), A^T r over the units'
- * active tiles with the model and its derivative columns evaluated in FP64
- * (FP64 exp, FP64 sums; the FP64 component tables tb_fit_prep writes into
- * the workspace), into the same gbuf slices tb_fit_pass uses; chi2_out[unit0
- * + slice] the slices' chi^2 over their active tiles.  Run tb_fit_prep with
- * state = NULL at the parameters first.  A^T A is not touched. */
+/* FP64 evaluation for the final iterations of a fit (no reference
+ * counterpart beyond the optimum LsqrOptimizer.optimize_loop converges to,
+ * lsqr_optimizer.py:317-326): for every running blob (status 0), A^T r and
+ * chi^2 over the units' active tiles with the model and its derivative
+ * columns evaluated in FP64 (FP64 exp, FP64 sums; the FP64 component
+ * tables tb_fit_prep writes into the workspace), written over the gbuf and
+ * chi2 slices of tb_fit_pass (call it after the pass, before tb_fit_step;
+ * the pass's FP32 A^T A is kept). */
 int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
                   const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
                   const void* workspace, const float* data, const float* inverr,
@@ -686,14 +686,6 @@ int tb_fit_model_vjp(const tb_fit_unit* units, const int32_t* order, int32_t n_u
                      const int32_t* tiles, double* gbuf, int32_t n_bands, int32_t mode,
                      int32_t* work_counter, tb_status* status, void* stream);
 
-/* One polish step per converged or stopped blob: the step of tb_fit_step with
- * the last accepted A^T A, the A^T r of tb_fit_refine and a Marquardt
- * damping of 1e-9 (the Gauss-Newton step), the same maximum steps, bounds and
- * frozen parameters; taken without a trial (params and trial both receive
- * it).  The blob's state is left as it is. */
-int tb_fit_polish(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
-                  const tb_fit_source* srcs, double* params, double* trial, double* hbuf,
-                  double* gbuf, tb_fit_state* state, void* stream);
 
 /* Chi-square of n images: sum over pixels of ((data - model) * inverr)^2,
  * FP32 terms with compensated FP32 block sums combined in FP64; out[i] for

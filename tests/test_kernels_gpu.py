@@ -160,9 +160,11 @@ def test_fourier_render_matches_oracle(tb, oracle, sz, mw, mh):
 def test_split_path_matches_persistent_kernel(tb, oracle):
     """tb_fourier_render_split (column and row kernels through the scratch,
     the box-edge items by the persistent kernel) against tb_fourier_render
-    (the persistent kernel alone) on the same items: 300 galaxies of every
-    FFT size (more than one column / row launch pair), windows inside and at
-    the edge of the box, store and accumulate modes, and a difference item."""
+    (the persistent kernel alone) on the same items, within the rendering
+    parity bar (1e-5 of the peak; the two order their FP32 arithmetic
+    differently): 300 galaxies of every FFT size (more than one column / row
+    launch pair), windows inside and at the edge of the box, and difference
+    items."""
     import torch
     from tractor_b200 import render, _lib
     rng = np.random.default_rng(31)
@@ -212,7 +214,7 @@ def test_split_path_matches_persistent_kernel(tb, oracle):
         o, n = int(it['out_off']), int(it['mw'] * it['mh'])
         pa, pc = a[o:o + n], c[o:o + n]
         peak = max(np.abs(pa).max(), 1e-30)
-        assert np.abs(pa - pc).max() <= 1e-6 * peak, (it, np.abs(pa - pc).max() / peak)
+        assert np.abs(pa - pc).max() <= PEAK_TOL * peak, (it, np.abs(pa - pc).max() / peak)
     # a second call over the scratch the first left behind gives the same pixels
     out2 = torch.zeros_like(out1)
     render.fourier_render(d_items.data_ptr(), len(items), amp.data_ptr(), var.data_ptr(),
@@ -258,20 +260,69 @@ def test_approx3_region_on_device_matches_oracle(tb, oracle, derivs):
         pend = approx.plan_approx3(plan, mix, x0, x0 + W, y0, y0 + H, fx, fy, minval, xc, yc,
                                    derivs=derivs)
         cases.append((pend, (x0, W, y0, H, fx, fy, minval, amp, mean, var, xc, yc)))
-    for pend, (x0, W, y0, H, fx, fy, minval, amp, mean, var, xc, yc) in cases:
-        out, dxo, dyo, (sx0, sx1, sy0, sy1) = oracle.mog_approx3(
-            x0, x0 + W, y0, y0 + H, fx, fy, minval, amp, mean, var, xc, yc, derivs=derivs)
+    # the same boxes rendered without the walk, for the CPU walk over the
+    # device's own values
+    raw = [plan.mog.add(a[0], a[2], a[1], a[3], a[7], a[8], a[9], fx=a[4], fy=a[5],
+                        minval=a[6]) for _, a in cases]
+    flips = 0
+    from oracle.host_kernels import ring_region
+    for (pend, (x0, W, y0, H, fx, fy, minval, amp, mean, var, xc, yc)), ro in zip(cases, raw):
         got = pend.result()
         planes = got if derivs else (got,)
+        vals = plan._mog_host[ro:ro + W * H].reshape(H, W).astype(np.float64)
+        # start pixel as approx3.c chooses it, from the oracle's plain edges
+        out, dxo, dyo, (sx0, sx1, sy0, sy1) = oracle.mog_approx3(
+            x0, x0 + W, y0, y0 + H, fx, fy, minval, amp, mean, var, xc, yc, derivs=derivs)
+        # (1) the device walk is exactly the CPU walk over the same values
+        inside = x0 <= xc < x0 + W and y0 <= yc < y0 + H
+        cx, cy = xc - x0, yc - y0
+        if not inside:
+            # approx3.c: the brightest pixel of the nearest edge column, then row
+            best, cx, cy = 0., int((2 * x0 + W) / 2) - x0, int((2 * y0 + H) / 2) - y0
+            def plain(xs, ys):   # eval_all (mix.i:19-42): exponents below -100 are 0
+                v = np.zeros(len(xs))
+                for k in range(len(amp)):
+                    iv = np.linalg.inv(var[k])
+                    dx, dy = xs - fx - mean[k, 0], ys - fy - mean[k, 1]
+                    e = -0.5 * (iv[0, 0] * dx * dx + 2 * iv[0, 1] * dx * dy + iv[1, 1] * dy * dy)
+                    v += np.where(e < -100, 0., amp[k] / (2 * np.pi * np.sqrt(np.linalg.det(var[k])))
+                                  * np.exp(e))
+                return v
+            if xc < x0 or xc >= x0 + W:
+                ex = 0 if xc < x0 else W - 1
+                col = plain(np.full(H, x0 + ex, float), np.arange(y0, y0 + H, dtype=float))
+                for yy, v in enumerate(col):
+                    if v > best:
+                        best, cx, cy = v, ex, yy
+            if yc < y0 or yc >= y0 + H:
+                ey = 0 if yc < y0 else H - 1
+                row = plain(np.arange(x0, x0 + W, dtype=float), np.full(W, y0 + ey, float))
+                for xx, v in enumerate(row):
+                    if v > best:
+                        best, cx, cy = v, xx, ey
+        if True:
+            ev, ext = ring_region(vals, cx, cy, minval, 3)
+            assert (planes[0].x0 - x0, planes[0].y0 - y0) == (ext[0], ext[2])
+            assert planes[0].patch.shape == (ext[3] - ext[2], ext[1] - ext[0])
+            sub = np.where(ev, vals, 0.)[ext[2]:ext[3], ext[0]:ext[1]]
+            assert np.array_equal(planes[0].patch, sub)
+        # (2) against the oracle's approx3 (FP64 values): the same region and
+        # values within 1e-5 of the peak, unless a pixel whose value lies
+        # within 1e-5 of minval decided the walk differently in FP32
+        same = (planes[0].x0, planes[0].y0) == (x0 + sx0, y0 + sy0) and \
+            planes[0].patch.shape == (sy1 - sy0, sx1 - sx0)
+        if not same:
+            near = np.abs(vals / minval - 1) < 1e-5
+            assert near.any(), ((planes[0].x0, planes[0].y0), (x0 + sx0, y0 + sy0))
+            flips += 1
+            continue
         refs = [out, dxo, dyo] if derivs else [out]
         for p, ref in zip(planes, refs):
-            assert (p.x0, p.y0) == (x0 + sx0, y0 + sy0), ((p.x0, p.y0), (x0 + sx0, y0 + sy0))
             sub = ref[sy0:sy1, sx0:sx1]
-            assert p.patch.shape == sub.shape
             peak = max(np.abs(sub).max(), 1e-300)
             assert np.abs(p.patch - sub).max() <= 1e-5 * peak
-            # the pixels approx3 did not evaluate are exactly zero
             assert np.array_equal(p.patch == 0, sub == 0)
+    assert flips <= 2, flips
 
 
 def test_normal_equations_and_solve(tb):

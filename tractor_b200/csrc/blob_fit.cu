@@ -795,17 +795,17 @@ __device__ double max_step(int off) {
 }
 
 // ---------------------------------------------------------------------------
-// refinement pass (tb_fit_refine): A^T r and chi^2 of finished blobs with the
-// model and its derivative columns evaluated in FP64 (FP64 exp, FP64 sums).
-// At a converged point the gradient is a sum of terms that cancel, and its
-// FP32 evaluation (FP32 model, FP32 partial sums) leaves an error that the
-// flat directions of a blob (the index and radius of a large galaxy)
-// amplify; the polish step (tb_fit_step in polish mode) takes the Newton
-// step with this gradient and the last accepted A^T A.  Same units, slices
-// and layout as tb_fit_pass; A^T A is not touched.
+// refinement pass (tb_fit_refine): A^T r and chi^2 of the running blobs with
+// the model and its derivative columns evaluated in FP64 (FP64 exp, FP64
+// sums), written over the slices tb_fit_pass just filled (its FP32 A^T A is
+// kept).  Near the optimum the gradient is a sum of terms that cancel, and
+// its FP32 evaluation (FP32 model, FP32 partial sums) leaves an error that a
+// blob's flat directions (the index and radius of a large galaxy) amplify,
+// and FP32 chi^2 cannot verify gains below ~1e-4; the final iterations of a
+// fit take both in FP64, so the step's acceptance and its stopping rule see
+// the FP64 objective.  Same units, slices and layout as tb_fit_pass.
 // ---------------------------------------------------------------------------
 constexpr int kRefThreads = 256;       // one 32 x 8 tile, one pixel per thread
-constexpr double kPolishLambda = 1e-9; // Marquardt damping of a polish step (scaled matrix)
 
 struct RefSrc {
     int32_t x0, y0, x1, y1;
@@ -864,10 +864,7 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
         if (ui < 0 || ui >= n_units) continue;
         const tb_fit_unit& u = units[ui];
         const tb_fit_blob b = blobs[u.blob];
-        if (mode == TB_FIT_REFINE) {
-            const int status = state[u.blob].status;
-            if (status != 1 && status != 2) continue;   // only converged or stopped blobs
-        }
+        if (mode == TB_FIT_REFINE && state[u.blob].status != 0) continue;   // running blobs
         const int P = b.P;
         const int nsrc = b.n_src;
         double* g = gbuf + b.g_off + (int64_t)u.slice * P;
@@ -1036,7 +1033,7 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
                 const tb_fit_source* __restrict__ srcs, double* __restrict__ params,
                 double* __restrict__ trial, double* __restrict__ hbuf, double* __restrict__ gbuf,
                 const double* __restrict__ chi2_part, tb_fit_state* __restrict__ state,
-                double tol, int max_iter, int polish) {
+                double tol, int max_iter) {
     __shared__ double dsc[TB_FIT_MAX_SRC * TB_FIT_NPAR];
     __shared__ double dinv[TB_FIT_MAX_SRC * TB_FIT_NPAR];
     __shared__ double y[TB_FIT_MAX_SRC * TB_FIT_NPAR];
@@ -1053,9 +1050,7 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     tb_fit_state& S = state[bi];
     const int status0 = S.status;
     __syncthreads();   // every thread has read the status before thread 0 updates it
-    // an iteration works on running blobs; a polish step on converged or
-    // stopped ones (their last accepted A^T A, the refinement pass's A^T r)
-    if (polish ? (status0 != 1 && status0 != 2) : status0 != 0) return;
+    if (status0 != 0) return;
     const int P = b.P;
     const int ns = b.n_slices;
     double* Hp = hbuf + b.h_off;                        // slice partials
@@ -1066,12 +1061,7 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     double* pa = params + (int64_t)b.src0 * TB_FIT_NPAR;
     double* pt = trial + (int64_t)b.src0 * TB_FIT_NPAR;
 
-    if (polish && tid == 0) {
-        s_accept = 0;
-        s_lambda = kPolishLambda;
-        s_active = 1;
-    }
-    if (!polish && tid == 0) {
+    if (tid == 0) {
         double c2 = 0.0;
         for (int k = 0; k < ns; k++) c2 += chi2_part[b.unit0 + k];
         const bool first = S.accepted == 0;
@@ -1105,14 +1095,6 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
                 Ha[(int64_t)r * P + c] = s;
                 Ha[(int64_t)c * P + r] = s;
             }
-        for (int e = tid; e < P; e += kStepThreads) {
-            double s = 0.0;
-            for (int k = 0; k < ns; k++) s += gp[(int64_t)k * P + e];
-            ga[e] = s;
-        }
-    }
-    if (polish) {
-        // the refinement pass's slices of A^T r, in the same fixed order
         for (int e = tid; e < P; e += kStepThreads) {
             double s = 0.0;
             for (int k = 0; k < ns; k++) s += gp[(int64_t)k * P + e];
@@ -1171,8 +1153,7 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     }
     if (bad) {
         // not positive definite: treat as a rejected step with more damping
-        // (a polish step is left out)
-        if (tid == 0 && !polish) {
+        if (tid == 0) {
             S.lambda *= 10.0;
             if (!(S.lambda < 1e12)) S.status = 2;
         }
@@ -1262,10 +1243,8 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
             double t = 0.0;
             for (int w2 = 0; w2 < kStepThreads / 32; w2++) t += red[w2];
             S.pred = 0.5 * t;
-            if (!polish) {
-                s_active = !(0.5 * t < tol && lam <= 1.0);
-                if (!s_active) S.status = 1;
-            }
+            s_active = !(0.5 * t < tol && lam <= 1.0);
+            if (!s_active) S.status = 1;
         }
         __syncthreads();
         if (!s_active) {
@@ -1303,7 +1282,6 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
             srcs[b.src0 + i / TB_FIT_NPAR].profile == TB_PROFILE_SERSIC)
             v = fmin(fmax(v, TB_FIT_SERSIC_MIN), TB_FIT_SERSIC_MAX);
         pt[i] = v;
-        if (polish) pa[i] = v;   // a polish step is taken without a trial
     }
 }
 
@@ -1417,8 +1395,7 @@ extern "C" int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_
     if (!blobs || !srcs || !params || !trial || !hbuf || !gbuf || !chi2_part || !state)
         return TB_ERR_ARG;
     fit_step_kernel<<<n_blobs, kStepThreads, 0, (cudaStream_t)stream>>>(
-        blobs, n_blobs, n_bands, srcs, params, trial, hbuf, gbuf, chi2_part, state, tol, max_iter,
-        0);
+        blobs, n_blobs, n_bands, srcs, params, trial, hbuf, gbuf, chi2_part, state, tol, max_iter);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
@@ -1480,13 +1457,3 @@ extern "C" int tb_fit_model_vjp(const tb_fit_unit* units, const int32_t* order, 
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
-extern "C" int tb_fit_polish(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
-                             const tb_fit_source* srcs, double* params, double* trial,
-                             double* hbuf, double* gbuf, tb_fit_state* state, void* stream) {
-    if (n_blobs < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS) return TB_ERR_ARG;
-    if (n_blobs == 0) return TB_OK;
-    if (!blobs || !srcs || !params || !trial || !hbuf || !gbuf || !state) return TB_ERR_ARG;
-    fit_step_kernel<<<n_blobs, kStepThreads, 0, (cudaStream_t)stream>>>(
-        blobs, n_blobs, n_bands, srcs, params, trial, hbuf, gbuf, nullptr, state, 0.0, 0, 1);
-    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
-}

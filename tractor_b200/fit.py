@@ -156,35 +156,6 @@ class BlobFitter(object):
                                    None if all_blobs else self.state.data_ptr(),
                                    _lib.stream_ptr()), 'tb_fit_prep')
 
-    def refine(self, steps=2):
-        """Polishes every converged or stopped blob: `steps` times, A^T r at
-        the parameters with the model and derivatives in FP64
-        (tb_fit_refine), then one Gauss-Newton step with the last accepted
-        A^T A (tb_fit_polish).  The FP32 passes leave the gradient's
-        cancellation error, which a blob's flat directions (a large
-        galaxy's index and radius) amplify; this brings the parameters to
-        the FP64 optimum.  The states' chi^2 stays that of the last
-        iteration."""
-        lib = _lib.load()
-        s = _lib.stream_ptr()
-        for _ in range(int(steps)):
-            self.trial.copy_(self.params)
-            self._prep(all_blobs=True)
-            _lib.check(lib.tb_fit_refine(self.d_pass_units.data_ptr(), self.d_order.data_ptr(),
-                                         len(self.pass_units_np), self.d_blobs.data_ptr(),
-                                         self.d_sources.data_ptr(), self.n_src,
-                                         self.workspace.data_ptr(), self.data.data_ptr(),
-                                         self.inverr.data_ptr(), self.d_tiles.data_ptr(),
-                                         self.gbuf.data_ptr(), self.chi2_refine.data_ptr(),
-                                         self.state.data_ptr(), self.n_bands,
-                                         self.misc.data_ptr(), self.misc.data_ptr() + 16, s),
-                       'tb_fit_refine')
-            _lib.check(lib.tb_fit_polish(self.d_blobs.data_ptr(), self.n_blobs, self.n_bands,
-                                         self.d_sources.data_ptr(), self.params.data_ptr(),
-                                         self.trial.data_ptr(), self.hbuf.data_ptr(),
-                                         self.gbuf.data_ptr(), self.state.data_ptr(), s),
-                       'tb_fit_polish')
-
     def _pass(self, mode):
         lib = _lib.load()
         _lib.check(lib.tb_fit_pass(self.d_pass_units.data_ptr(), self.d_order.data_ptr(),
@@ -198,11 +169,27 @@ class BlobFitter(object):
                                    self.misc.data_ptr(), self.misc.data_ptr() + 16,
                                    _lib.stream_ptr()), 'tb_fit_pass')
 
-    def _iteration(self, tol, max_iter):
+    def _refine_pass(self):
+        """A^T r and chi^2 of the running blobs in FP64 (tb_fit_refine), over
+        the slices the FP32 pass just wrote."""
+        lib = _lib.load()
+        _lib.check(lib.tb_fit_refine(self.d_pass_units.data_ptr(), self.d_order.data_ptr(),
+                                     len(self.pass_units_np), self.d_blobs.data_ptr(),
+                                     self.d_sources.data_ptr(), self.n_src,
+                                     self.workspace.data_ptr(), self.data.data_ptr(),
+                                     self.inverr.data_ptr(), self.d_tiles.data_ptr(),
+                                     self.gbuf.data_ptr(), self.chi2_part.data_ptr(),
+                                     self.state.data_ptr(), self.n_bands, self.misc.data_ptr(),
+                                     self.misc.data_ptr() + 16, _lib.stream_ptr()),
+                   'tb_fit_refine')
+
+    def _iteration(self, tol, max_iter, precise=False):
         lib = _lib.load()
         s = _lib.stream_ptr()
         self._prep()
         self._pass(0)
+        if precise:
+            self._refine_pass()
         _lib.check(lib.tb_fit_step(self.d_blobs.data_ptr(), self.n_blobs, self.n_bands,
                                    self.d_sources.data_ptr(), self.params.data_ptr(),
                                    self.trial.data_ptr(), self.hbuf.data_ptr(),
@@ -228,11 +215,16 @@ class BlobFitter(object):
         st = self.state.view(torch.int32).view(self.n_blobs, _lib.FIT_STATE.itemsize // 4)
         return int((st[:, -1] == 0).sum().item())
 
-    def fit(self, tol=1e-3, max_iter=50, check_every=4, graph=True, params0=None,
-            lambda0=1e-3, refine=2):
-        """Runs iterations until every blob stops (or max_iter), then
-        `refine` FP64-gradient polish steps (see refine()).  Returns the
-        number of iterations launched."""
+    def fit(self, tol=1e-3, max_iter=200, check_every=4, graph=True, params0=None,
+            lambda0=1e-3, refine=True, refine_tol=1e-8, refine_iter=20):
+        """Runs FP32 iterations until every blob stops (or max_iter); then,
+        with `refine`, continues every blob from where it stopped with the
+        gradient and chi^2 in FP64 (tb_fit_refine after each pass; A^T A
+        stays FP32) until the predicted gain is below refine_tol (or
+        refine_iter): the FP32 objective cannot resolve the last ~1e-4 of
+        log-likelihood, which leaves the flat directions of a blob a few
+        1e-3 sigma from the optimum.  Returns the number of iterations
+        launched (both phases)."""
         self.reset(params0, lambda0)
         g = None
         if graph:
@@ -247,7 +239,17 @@ class BlobFitter(object):
             if self.running() == 0:
                 break
         if refine:
-            self.refine(refine)
+            # the FP64 phase starts every blob again from its parameters
+            # (the first pass is accepted: the FP64 chi^2 is not comparable
+            # with the FP32 one)
+            n = self.iterations
+            self.reset(None, lambda0)
+            self.iterations = n
+            for it in range(int(refine_iter)):
+                self._iteration(refine_tol, refine_iter, precise=True)
+                self.iterations += 1
+                if it % 2 == 1 and self.running() == 0:
+                    break
         return self.iterations
 
     def _capture(self, k, tol, max_iter):

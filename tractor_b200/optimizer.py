@@ -34,10 +34,32 @@ class B200Optimizer(object):
     # -- update direction --------------------------------------------------
     def getLinearUpdateDirection(self, tractor, damp=0, priors=True, scale_columns=True,
                                  shared_params=True, variance=False, **kwargs):
-        allderivs = tractor.getDerivs()
+        """The derivatives and the chi images at the current parameters are
+        rendered in one plan (one launch per kernel type and one copy back)
+        unless an image's model goes through the scene renderer; the
+        log-probability there is kept for tryUpdates' starting value."""
+        self._lnp0 = None
+        imgs = list(tractor.getImages())
+        nsrc = sum(1 for s in tractor.catalog if s is not None)
+        chis = None
+        if nsrc < tractor.SCENE_MIN_SOURCES or tractor.modtype != np.float32:
+            plan = RenderPlan()
+            fd = tractor._plan_derivs(plan)
+            fm = [tractor._plan_model_image(plan, img, minsb=0.) for img in imgs]
+            allderivs = fd()
+            chis = [(img.getImage() - f()) * img.getInvError() for img, f in zip(imgs, fm)]
+            lnprior = tractor.getLogPrior()
+            if lnprior != -np.inf:
+                chisq = 0.
+                for chi in chis:
+                    chisq += (chi.astype(float) ** 2).sum()
+                lnp = lnprior - 0.5 * chisq
+                self._lnp0 = (tuple(tractor.getParams()), -np.inf if np.isnan(lnp) else lnp)
+        else:
+            allderivs = tractor.getDerivs()
         return self.getUpdateDirection(tractor, allderivs, damp=damp, priors=priors,
                                        scale_columns=scale_columns, shared_params=shared_params,
-                                       variance=variance)
+                                       variance=variance, chiImages=chis)
 
     def getUpdateDirection(self, tractor, allderivs, damp=0., priors=True, scale_columns=True,
                            scales_only=False, chiImages=None, variance=False,
@@ -193,7 +215,12 @@ class B200Optimizer(object):
         """Optimizer.tryUpdates (optimize.py:425-470)."""
         if alphas is None:
             alphas = default_alphas()
-        pBefore = tractor.getLogProb()
+        cached = getattr(self, '_lnp0', None)
+        self._lnp0 = None
+        if cached is not None and cached[0] == tuple(tractor.getParams()):
+            pBefore = cached[1]        # rendered with the update direction's chi images
+        else:
+            pBefore = tractor.getLogProb()
         pBest = pBefore
         alphaBest = None
         p0 = tractor.getParams()
