@@ -658,13 +658,14 @@ int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
  * columns evaluated in FP64 (FP64 exp, FP64 sums; the FP64 component
  * tables tb_fit_prep writes into the workspace), written over the gbuf and
  * chi2 slices of tb_fit_pass (call it after the pass, before tb_fit_step;
- * the pass's FP32 A^T A is kept). */
+ * the pass's FP32 A^T A is kept); chi2_const (may be NULL) is added to each
+ * slice's chi^2 as the pass does. */
 int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
                   const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
                   const void* workspace, const float* data, const float* inverr,
                   const int32_t* tiles, double* gbuf, double* chi2_out,
-                  const tb_fit_state* state, int32_t n_bands, int32_t* work_counter,
-                  tb_status* status, void* stream);
+                  const double* chi2_const, const tb_fit_state* state, int32_t n_bands,
+                  int32_t* work_counter, tb_status* status, void* stream);
 
 /* The blobs' model and its vector-Jacobian product, in FP64 (the
  * refinement pass's evaluation): mode TB_FIT_MODEL writes every unit's

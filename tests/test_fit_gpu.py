@@ -57,7 +57,7 @@ def test_normal_equations_match_oracle(tb, oracle):
     columns reproduce the FP64 central-difference A^T A, A^T r, chi^2."""
     w, datas, inverrs = _small_blobs(oracle, 1)
     f = _fitter(w, datas, inverrs)
-    f.fit(max_iter=1, check_every=1, graph=False)
+    f.fit(max_iter=1, check_every=1, graph=False, refine=False)
     st = f.states()
     for b in range(len(datas)):
         s0, s1, W, H, rects = _blob_args(w, b)
@@ -126,7 +126,7 @@ def test_many_blobs_fit_at_least_as_well_as_truth(tb):
     assert np.all(st['status'] != 0)
     assert np.mean(st['status'] == 1) > 0.95, np.bincount(st['status'])
     fitted = st['chi2'].copy()
-    f.fit(max_iter=1, check_every=1, graph=False, params0=w['truth'])
+    f.fit(max_iter=1, check_every=1, graph=False, params0=w['truth'], refine=False)
     truth = f.states()['chi2']
     npix = np.diff(fit.pix_offsets(w['sides'], 3)).reshape(-1, 3).sum(axis=1)
     assert np.all(np.abs(truth / npix - 1) < 0.05)          # noise model sanity
@@ -291,12 +291,15 @@ def test_c5_blobs_reach_the_fp64_optimum(tb, oracle):
     f = fit.BlobFitter(w['blob_src'], w['sides'], w['psf'], w['sources'], w['start'], data, inv)
     f.fit(tol=1e-3, max_iter=200)
     st = f.states()
-    assert np.all(st['status'] != 0) and np.all(st['status'] != 3), np.bincount(st['status'])
+    # every blob stops; a few may end the FP64 phase at its iteration limit
+    # (predicted gain not yet below 1e-8) and are held to the same bound
+    assert np.all(st['status'] != 0) and np.sum(st['status'] == 3) <= 3, \
+        np.bincount(st['status'])
     got = f.result()
     po = fit.pix_offsets(w['sides'], 3)
     hd, hi = data.cpu().numpy(), inv.cpu().numpy()
     worst = []
-    for b in np.flatnonzero(st['status'] == 1):
+    for b in np.flatnonzero(st['status'] != 2):
         s0, s1 = w['blob_src'][b], w['blob_src'][b + 1]
         W, H = (int(v) for v in w['sides'][b])
         d3 = np.stack([hd[po[3 * b + k]:po[3 * b + k + 1]].reshape(H, W) for k in range(3)])

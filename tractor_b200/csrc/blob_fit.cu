@@ -850,7 +850,8 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
                   const float* __restrict__ inverr, double* __restrict__ gbuf,
                   double* __restrict__ chi2_out, const tb_fit_state* __restrict__ state,
                   int n_bands, const int32_t* __restrict__ tiles, int32_t* counter,
-                  tb_status* st, int mode, float* __restrict__ model_out) {
+                  tb_status* st, int mode, float* __restrict__ model_out,
+                  const double* __restrict__ chi2_const) {
     // mode TB_FIT_REFINE: A^T r of finished blobs, r = (data - model) inverr;
     // TB_FIT_MODEL: the model into model_out (every blob); TB_FIT_VJP: the
     // columns contracted with data = an upstream gradient, unweighted
@@ -919,7 +920,9 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
             const bool in = px < u.W && py < u.H;
             double d = 0.0, w = 0.0;
             const int64_t pix = u.pix_off + (int64_t)py * u.W + px;
-            if (in) {
+            // MODEL reads neither data nor inverr (both may be NULL); VJP
+            // reads the upstream gradient in `data` and no weights
+            if (in && mode != TB_FIT_MODEL) {
                 d = data[pix];
                 w = mode == TB_FIT_VJP ? 1.0 : inverr[pix];
             }
@@ -1017,7 +1020,9 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
         if (lane == 0) sm.red[warp][0] = chi2;
         __syncthreads();
         if (tid == 0 && chi2_out) {
-            double c2 = 0.0;
+            // the slice's chi^2 with its constant part (the tiles no mask
+            // reaches), as tb_fit_pass writes it
+            double c2 = chi2_const ? chi2_const[b.unit0 + u.slice] : 0.0;
             for (int w2 = 0; w2 < kRefThreads / 32; w2++) c2 += sm.red[w2][0];
             chi2_out[b.unit0 + u.slice] = c2;
         }
@@ -1403,8 +1408,9 @@ extern "C" int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int
                              const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
                              const void* workspace, const float* data, const float* inverr,
                              const int32_t* tiles, double* gbuf, double* chi2_out,
-                             const tb_fit_state* state, int32_t n_bands, int32_t* work_counter,
-                             tb_status* status, void* stream) {
+                             const double* chi2_const, const tb_fit_state* state,
+                             int32_t n_bands, int32_t* work_counter, tb_status* status,
+                             void* stream) {
     if (n_units < 0 || n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS) return TB_ERR_ARG;
     if (n_units == 0) return TB_OK;
     if (!units || !order || !blobs || !srcs || !workspace || !data || !inverr || !tiles ||
@@ -1424,7 +1430,7 @@ extern "C" int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int
     fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
         units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands), data,
         inverr, gbuf, chi2_out, state, n_bands, tiles, work_counter, status, TB_FIT_REFINE,
-        nullptr);
+        nullptr, chi2_const);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
@@ -1453,7 +1459,8 @@ extern "C" int tb_fit_model_vjp(const tb_fit_unit* units, const int32_t* order, 
     void* ws = const_cast<void*>(workspace);
     fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
         units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands), grad,
-        nullptr, gbuf, nullptr, nullptr, n_bands, tiles, work_counter, status, mode, model);
+        nullptr, gbuf, nullptr, nullptr, n_bands, tiles, work_counter, status, mode, model,
+        nullptr);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 

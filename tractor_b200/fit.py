@@ -131,7 +131,6 @@ class BlobFitter(object):
         self.chi2_part = torch.zeros(int(n_slices.sum()), dtype=torch.float64,
                                      device=self.dev)
         self.chi2_const = torch.zeros_like(self.chi2_part)
-        self.chi2_refine = torch.zeros_like(self.chi2_part)
         self._const_done = False
         self.state = torch.zeros(self.n_blobs * _lib.FIT_STATE.itemsize, dtype=torch.uint8,
                                  device=self.dev)
@@ -179,7 +178,8 @@ class BlobFitter(object):
                                      self.workspace.data_ptr(), self.data.data_ptr(),
                                      self.inverr.data_ptr(), self.d_tiles.data_ptr(),
                                      self.gbuf.data_ptr(), self.chi2_part.data_ptr(),
-                                     self.state.data_ptr(), self.n_bands, self.misc.data_ptr(),
+                                     self.chi2_const.data_ptr(), self.state.data_ptr(),
+                                     self.n_bands, self.misc.data_ptr(),
                                      self.misc.data_ptr() + 16, _lib.stream_ptr()),
                    'tb_fit_refine')
 
@@ -216,7 +216,7 @@ class BlobFitter(object):
         return int((st[:, -1] == 0).sum().item())
 
     def fit(self, tol=1e-3, max_iter=200, check_every=4, graph=True, params0=None,
-            lambda0=1e-3, refine=True, refine_tol=1e-8, refine_iter=20):
+            lambda0=1e-3, refine=True, refine_tol=1e-8, refine_iter=40):
         """Runs FP32 iterations until every blob stops (or max_iter); then,
         with `refine`, continues every blob from where it stopped with the
         gradient and chi^2 in FP64 (tb_fit_refine after each pass; A^T A
