@@ -654,12 +654,12 @@ int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
 /* FP64 evaluation for the final iterations of a fit (no reference
  * counterpart beyond the optimum LsqrOptimizer.optimize_loop converges to,
  * lsqr_optimizer.py:317-326): for every running blob (status 0), A^T r and
- * chi^2 over the units' active tiles with the model and its derivative
- * columns evaluated in FP64 (FP64 exp, FP64 sums; the FP64 component
- * tables tb_fit_prep writes into the workspace), written over the gbuf and
- * chi2 slices of tb_fit_pass (call it after the pass, before tb_fit_step;
- * the pass's FP32 A^T A is kept); chi2_const (may be NULL) is added to each
- * slice's chi^2 as the pass does. */
+ * chi^2 over the units' active tiles with the model, the residuals and the
+ * sums in FP64 (FP64 exp from the FP64 component tables tb_fit_prep writes
+ * into the workspace; the derivative columns in FP32), written into the
+ * gbuf and chi2 slices that tb_fit_pass fills (call it in place of the
+ * pass, before tb_fit_step; A^T A stays the last pass's); chi2_const (may
+ * be NULL) is added to each slice's chi^2 as the pass does. */
 int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
                   const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
                   const void* workspace, const float* data, const float* inverr,

@@ -317,7 +317,8 @@ def test_c5_blobs_reach_the_fp64_optimum(tb, oracle):
         sig = np.full(o.size, np.inf)
         sig[free] = np.sqrt(np.diag(np.linalg.inv(Hf[np.ix_(free, free)])))
         err = np.abs(got[s0:s1].ravel() - o) / sig
-        worst.append((float(err.max()), int(b)))
+        worst.append((float(err.max()), int(b), int(st['status'][b]), int(st['iters'][b]),
+                      float(st['pred'][b]), int(err.argmax() % 9)))
     worst.sort(reverse=True)
     assert len(worst) >= 110, len(worst)
     assert worst[0][0] < 1e-3, worst[:5]

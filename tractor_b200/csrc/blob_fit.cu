@@ -796,9 +796,8 @@ __device__ double max_step(int off) {
 
 // ---------------------------------------------------------------------------
 // refinement pass (tb_fit_refine): A^T r and chi^2 of the running blobs with
-// the model and its derivative columns evaluated in FP64 (FP64 exp, FP64
-// sums), written over the slices tb_fit_pass just filled (its FP32 A^T A is
-// kept).  Near the optimum the gradient is a sum of terms that cancel, and
+// the model, the residuals and the sums in FP64 (FP64 exp; the derivative
+// columns in FP32), written over the gradient and chi^2 slices.  Near the optimum the gradient is a sum of terms that cancel, and
 // its FP32 evaluation (FP32 model, FP32 partial sums) leaves an error that a
 // blob's flat directions (the index and radius of a large galaxy) amplify,
 // and FP32 chi^2 cannot verify gains below ~1e-4; the final iterations of a
@@ -846,7 +845,8 @@ __global__ void __launch_bounds__(kRefThreads)
 fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict__ order,
                   int n_units, const tb_fit_blob* __restrict__ blobs,
                   const tb_fit_source* __restrict__ srcs, const SrcTab* __restrict__ tab,
-                  const FitC64* __restrict__ gcomps, const float* __restrict__ data,
+                  const FitC64* __restrict__ gcomps, const FitC* __restrict__ gcomps32,
+                  const float* __restrict__ data,
                   const float* __restrict__ inverr, double* __restrict__ gbuf,
                   double* __restrict__ chi2_out, const tb_fit_state* __restrict__ state,
                   int n_bands, const int32_t* __restrict__ tiles, int32_t* counter,
@@ -910,6 +910,7 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
             continue;
         }
         const FitC64* band_comps = gcomps + ((int64_t)b.src0 * n_bands + u.band) * kCompStride;
+        const FitC* band_comps32 = gcomps32 + ((int64_t)b.src0 * n_bands + u.band) * kCompStride;
         const int64_t cstride = (int64_t)n_bands * kCompStride;
         const int n_t = u.t1 - u.t0;
         const int32_t* tl = tiles + b.tile_off + u.t0;
@@ -955,35 +956,37 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
                     continue;   // the same for every thread of the tile
                 double J[7] = {0, 0, 0, 0, 0, 0, 0};
                 if (in && px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1) {
-                    const FitC64* cs = band_comps + sI * cstride;
-                    double S0 = 0, Sx = 0, Sy = 0, Axx = 0, Axy = 0, Ayy = 0;
-                    double At[3] = {0, 0, 0};
-                    double Dxx = 0, Dxy = 0, Dyy = 0, Dt = 0, Sn = 0;
+                    // the derivative columns in FP32 (their errors, multiplied by
+                    // residuals that are noise at the optimum, average out); the
+                    // model and the residual above are FP64
+                    const FitC* cs = band_comps32 + sI * cstride;
+                    float S0 = 0, Sx = 0, Sy = 0, Axx = 0, Axy = 0, Ayy = 0;
+                    float At[3] = {0, 0, 0};
+                    float Dxx = 0, Dxy = 0, Dyy = 0, Dt = 0, Sn = 0;
                     for (int k = 0; k < R.K; k++) {
-                        const FitC64& c = cs[k];
-                        const double dx = px - c.mx, dy = py - c.my;
-                        const double e = -0.5 * (c.i00 * dx * dx + 2.0 * c.i01 * dx * dy +
-                                                 c.i11 * dy * dy);
-                        if (e < -50.0) continue;
-                        const double E = exp(e);
-                        const double val = c.s * E;
-                        const double ux = c.i00 * dx + c.i01 * dy, uy = c.i01 * dx + c.i11 * dy;
+                        const FitC& c = cs[k];
+                        const float dx = (float)(px - c.mx), dy = (float)(py - c.my);
+                        const float e = fmaf(dy, fmaf(c.qyy, dy, c.qxy * dx), c.qxx * dx * dx);
+                        if (e < c.fl) continue;
+                        const float E = tb::ex2(e);
+                        const float val = c.s * E;
+                        const float ux = fmaf(c.ixx, dx, c.ixy * dy), uy = fmaf(c.ixy, dx, c.iyy * dy);
                         S0 += val;
-                        Sx += val * ux;
-                        Sy += val * uy;
-                        const double vv = val * c.v;
-                        Axx += vv * ux * ux;
-                        Axy += vv * ux * uy;
-                        Ayy += vv * uy * uy;
-                        At[0] += vv * c.t[0];
-                        At[1] += vv * c.t[1];
-                        At[2] += vv * c.t[2];
-                        const double vd = val * c.dv;
-                        Dxx += vd * ux * ux;
-                        Dxy += vd * ux * uy;
-                        Dyy += vd * uy * uy;
-                        Dt += vd * c.t[3];
-                        Sn += c.sn * E;
+                        Sx = fmaf(val, ux, Sx);
+                        Sy = fmaf(val, uy, Sy);
+                        const float vv = val * c.v;
+                        Axx = fmaf(vv * ux, ux, Axx);
+                        Axy = fmaf(vv * ux, uy, Axy);
+                        Ayy = fmaf(vv * uy, uy, Ayy);
+                        At[0] = fmaf(vv, c.t[0], At[0]);
+                        At[1] = fmaf(vv, c.t[1], At[1]);
+                        At[2] = fmaf(vv, c.t[2], At[2]);
+                        const float vd = val * c.dv;
+                        Dxx = fmaf(vd * ux, ux, Dxx);
+                        Dxy = fmaf(vd * ux, uy, Dxy);
+                        Dyy = fmaf(vd * uy, uy, Dyy);
+                        Dt = fmaf(vd, c.t[3], Dt);
+                        Sn = fmaf(c.sn, E, Sn);
                     }
                     const double cn = R.counts;
                     J[0] = cn * Sx;
@@ -1428,9 +1431,9 @@ extern "C" int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int
     const int grid = (int)(n_units < want ? n_units : want);
     void* ws = const_cast<void*>(workspace);
     fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
-        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands), data,
-        inverr, gbuf, chi2_out, state, n_bands, tiles, work_counter, status, TB_FIT_REFINE,
-        nullptr, chi2_const);
+        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands),
+        ws_comps(ws, n_src), data, inverr, gbuf, chi2_out, state, n_bands, tiles, work_counter,
+        status, TB_FIT_REFINE, nullptr, chi2_const);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
@@ -1458,9 +1461,9 @@ extern "C" int tb_fit_model_vjp(const tb_fit_unit* units, const int32_t* order, 
     const int grid = (int)(n_units < want ? n_units : want);
     void* ws = const_cast<void*>(workspace);
     fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
-        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands), grad,
-        nullptr, gbuf, nullptr, nullptr, n_bands, tiles, work_counter, status, mode, model,
-        nullptr);
+        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands),
+        ws_comps(ws, n_src), grad, nullptr, gbuf, nullptr, nullptr, n_bands, tiles, work_counter,
+        status, mode, model, nullptr);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 

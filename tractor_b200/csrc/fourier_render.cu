@@ -603,6 +603,14 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
 // Items that are not eligible are appended to a list for the persistent
 // kernel (third launch).
 // ---------------------------------------------------------------------------
+// CTAs per SM the column and row kernels are compiled for (their register
+// budget: 3 -> 80, 4 -> 64 registers per thread)
+#ifndef TB_SPLIT_COL_MINB
+#define TB_SPLIT_COL_MINB 3
+#endif
+#ifndef TB_SPLIT_ROW_MINB
+#define TB_SPLIT_ROW_MINB 4
+#endif
 constexpr int kSplitThreads = 256;
 constexpr int kSplitWarps = kSplitThreads / 32;
 constexpr int kColBlock = 16;                 // rfft columns per column unit
@@ -796,7 +804,7 @@ __device__ void split_col_unit(const tb_fft_item& it, int cb, const float* __res
     }
 }
 
-__global__ void __launch_bounds__(kSplitThreads, 3)
+__global__ void __launch_bounds__(kSplitThreads, TB_SPLIT_COL_MINB)
 fourier_split_col_kernel(const tb_fft_item* __restrict__ items, int i0, int n_items,
                          const double* __restrict__ amp, const double* __restrict__ var,
                          const double* __restrict__ dcoef, const float* __restrict__ psf_spec,
@@ -932,7 +940,7 @@ __device__ void split_row_unit(const tb_fft_item& it, int rb, const float2* __re
     }
 }
 
-__global__ void __launch_bounds__(kSplitThreads, 3)
+__global__ void __launch_bounds__(kSplitThreads, TB_SPLIT_ROW_MINB)
 fourier_split_row_kernel(const tb_fft_item* __restrict__ items, int i0, int n_items,
                          const double* __restrict__ dcoef, float* __restrict__ out, SplitWs* ws,
                          const float2* __restrict__ s1_all, const float2* __restrict__ hresp) {

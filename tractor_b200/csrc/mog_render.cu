@@ -275,11 +275,13 @@ __device__ __forceinline__ void ring_set(uint8_t* a, int i, int n) {
     if (i >= 0 && i < n) a[i] = 1;
 }
 
-__device__ __forceinline__ void ring_zero(float* v, int64_t d, int64_t plane, int64_t o) {
+// Zeroes pixel o of the value plane and, when present, of the two
+// derivative planes (dv: their start, both planes w x h).
+__device__ __forceinline__ void ring_zero(float* v, float* dv, int64_t plane, int64_t o) {
     v[o] = 0.f;
-    if (d >= 0) {
-        v[d + o] = 0.f;
-        v[d + plane + o] = 0.f;
+    if (dv) {
+        dv[o] = 0.f;
+        dv[plane + o] = 0.f;
     }
 }
 
@@ -296,7 +298,7 @@ approx3_ring_kernel(const tb_ring_item* __restrict__ items, int n_items, float* 
         return;
     }
     float* v = vals + it.val_off;
-    const int64_t d = it.deriv_off;
+    float* d = it.deriv_off >= 0 ? vals + it.deriv_off : nullptr;
     const int64_t plane = (int64_t)W * H;
     const double minval = it.minval;
     const int tid = threadIdx.x;

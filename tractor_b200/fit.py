@@ -187,9 +187,12 @@ class BlobFitter(object):
         lib = _lib.load()
         s = _lib.stream_ptr()
         self._prep()
-        self._pass(0)
         if precise:
+            # A^T r and chi^2 in FP64; A^T A stays the FP32 one of the last
+            # pass of the FP32 phase (it changes little over the last steps)
             self._refine_pass()
+        else:
+            self._pass(0)
         _lib.check(lib.tb_fit_step(self.d_blobs.data_ptr(), self.n_blobs, self.n_bands,
                                    self.d_sources.data_ptr(), self.params.data_ptr(),
                                    self.trial.data_ptr(), self.hbuf.data_ptr(),
@@ -216,13 +219,13 @@ class BlobFitter(object):
         return int((st[:, -1] == 0).sum().item())
 
     def fit(self, tol=1e-3, max_iter=200, check_every=4, graph=True, params0=None,
-            lambda0=1e-3, refine=True, refine_tol=1e-8, refine_iter=40):
+            lambda0=1e-3, refine=True, refine_tol=1e-10, refine_iter=40):
         """Runs FP32 iterations until every blob stops (or max_iter); then,
         with `refine`, continues every blob from where it stopped with the
-        gradient and chi^2 in FP64 (tb_fit_refine after each pass; A^T A
-        stays FP32) until the predicted gain is below refine_tol (or
-        refine_iter): the FP32 objective cannot resolve the last ~1e-4 of
-        log-likelihood, which leaves the flat directions of a blob a few
+        gradient and chi^2 in FP64 (tb_fit_refine in place of the pass; A^T A
+        is the last FP32 one) until the predicted gain is below refine_tol
+        (or refine_iter): the FP32 objective cannot resolve the last ~1e-4
+        of log-likelihood, which leaves the flat directions of a blob a few
         1e-3 sigma from the optimum.  Returns the number of iterations
         launched (both phases)."""
         self.reset(params0, lambda0)
