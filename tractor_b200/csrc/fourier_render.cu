@@ -100,15 +100,6 @@ __device__ void taps3_deriv(double dx, float* f) {
     for (int i = 0; i < 7; i++) f[i] = (i >= lo && i < hi) ? (float)((D[i] - L[i] / S * Sd) / S) : 0.f;
 }
 
-// A component whose exponent stays below -60 (log2 units: a factor 2^-60 of
-// its amplitude) on the whole column v is left out of the column: its
-// contribution is far below FP32 resolution.  The largest exponent along
-// the column is at w = -cb v / (2 cd): v^2 (ca - cb^2 / (4 cd)).
-__device__ __forceinline__ bool column_culled(const float4& c, float vf) {
-    const float emax = c.w < 0.f ? vf * vf * (c.y - c.z * c.z / (4.f * c.w)) : c.y * vf * vf;
-    return emax < -60.f;
-}
-
 // Mixture spectrum at (v, w) for the 8 rows of one thread: acc[m] =
 // sum_k amp_k exp2(ca v^2 + cb v w_m + cd w_m^2).
 __device__ __forceinline__ void spectrum8(const float4* comp, int K, float vf, const float* wf,
@@ -117,7 +108,6 @@ __device__ __forceinline__ void spectrum8(const float4* comp, int K, float vf, c
     for (int m = 0; m < 8; m++) acc[m] = 0.f;
     for (int k = 0; k < K; k++) {
         const float4 c = comp[k];
-        if (column_culled(c, vf)) continue;
         const float al = c.y * vf * vf, be = c.z * vf;
 #pragma unroll
         for (int m = 0; m < 8; m++) {
@@ -136,7 +126,6 @@ __device__ __forceinline__ void dspectrum8(const float4* comp, const float4* dco
     for (int m = 0; m < 8; m++) acc[m] = 0.f;
     for (int k = 0; k < K; k++) {
         const float4 c = comp[k];
-        if (column_culled(c, vf)) continue;
         const float4 d = dcomp[k];
         const float al = c.y * vf * vf, be = c.z * vf;
         const float d0 = fmaf(d.y * vf, vf, d.x), d1 = d.z * vf;
@@ -158,7 +147,6 @@ __device__ __forceinline__ void diffspectrum8(const float4* comp, const float4* 
     for (int m = 0; m < 8; m++) acc[m] = 0.f;
     for (int k = 0; k < K; k++) {
         const float4 c = comp[k];
-        if (column_culled(c, vf)) continue;
         const float4 d = dcomp[k];
         const float al = c.y * vf * vf, be = c.z * vf;
         const float d0 = d.y * vf * vf, d1 = d.z * vf;
