@@ -245,8 +245,10 @@ class BlobFitter(object):
             # the FP64 phase starts every blob again from its parameters
             # (the first pass is accepted: the FP64 chi^2 is not comparable
             # with the FP32 one)
+            # near the optimum: Gauss-Newton steps (a Marquardt damping of
+            # 1e-9; a damped start would crawl along the flat directions)
             n = self.iterations
-            self.reset(None, lambda0)
+            self.reset(None, 1e-9)
             self.iterations = n
             for it in range(int(refine_iter)):
                 self._iteration(refine_tol, refine_iter, precise=True)
