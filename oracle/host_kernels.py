@@ -270,7 +270,9 @@ def install(monkeypatch):
 
     def mog_run(self, out=None, stream=None, check=True):
         if out is None:
-            out = torch.zeros(max(self.nout, 1), dtype=torch.float32)
+            # packed outputs carry the (zero) status word at their end, as the
+            # device batches do
+            out = torch.zeros(max(self.nout, 1) + 4, dtype=torch.float32)
         if self.items:
             items = np.array(self.items, dtype=_lib.MOG_ITEM)
             masks = np.concatenate(self.masks) if self.masks else None
@@ -287,7 +289,9 @@ def install(monkeypatch):
 
     def fft_run(self, out=None, stream=None, check=True):
         if out is None:
-            out = torch.zeros(max(self.nout, 1), dtype=torch.float32)
+            # packed outputs carry the (zero) status word at their end, as the
+            # device batches do
+            out = torch.zeros(max(self.nout, 1) + 4, dtype=torch.float32)
         if self.items:
             items = np.array(self.items, dtype=_lib.FFT_ITEM)
             specs = torch.cat(self.spec_list).numpy()

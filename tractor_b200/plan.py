@@ -87,15 +87,16 @@ class RenderPlan(object):
             shifts = np.array([[dx, dy] for _, dx, dy in lst])
             lz[key] = render.lanczos_shift(imgs, shifts)
         for kind, t in outs:
-            host = t.cpu().numpy()
+            host = t.cpu().numpy()     # the status word rides at the end
+            st = torch.from_numpy(host[-4:].view(np.uint8).copy())
             if kind == 'mog':
-                render.check_status(self.mog.status, 'tb_mog_render')
+                render.check_status(st, 'tb_mog_render')
                 if self.mog.extents is not None:
                     render.check_status(self.mog.ring_status, 'tb_approx3_region')
                     self._ring_host = self.mog.extents.cpu().numpy().reshape(-1, 4)
                 self._mog_host = host
             else:
-                render.check_status(self.fft.status, 'tb_fourier_render')
+                render.check_status(st, 'tb_fourier_render')
                 self._fft_host = host
         for key, t in lz.items():
             self._lz_host[key] = t.cpu().numpy()

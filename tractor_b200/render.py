@@ -200,11 +200,15 @@ class MogBatch(object):
 
     def run(self, out=None, stream=None, check=True):
         """Launches one tb_mog_render over all items.  `out` (float32 device
-        tensor) defaults to a new packed buffer of all patches."""
+        tensor) defaults to a new packed buffer of all patches followed by
+        the launch's 16-byte status word (its last 4 elements)."""
         lib = _lib.load()
         dev = device()
+        self.status_in_out = out is None
         if out is None:
-            out = torch.empty(max(self.nout, 1), dtype=torch.float32, device=dev)
+            # the launch's status word rides at the end of the packed output,
+            # so one copy brings both back
+            out = torch.empty(max(self.nout, 1) + 4, dtype=torch.float32, device=dev)
         if not self.items:
             return out
         items = np.array(self.items, dtype=_lib.MOG_ITEM)
@@ -223,9 +227,10 @@ class MogBatch(object):
         o_rst = pk.add(np.zeros(1, _lib.STATUS))
         d = pk.to_device(dev)
         base = d.data_ptr()
+        st_ptr = out.data_ptr() + 4 * (out.numel() - 4) if self.status_in_out else base + o_st
         rc = lib.tb_mog_render(base + o_items, len(items), n_tiles, base + o_amp, base + o_mean,
                                base + o_var, None if o_mask is None else base + o_mask,
-                               out.data_ptr(), base + o_ctr, base + o_st,
+                               out.data_ptr(), base + o_ctr, st_ptr,
                                _lib.stream_ptr(stream))
         _lib.check(rc, 'tb_mog_render')
         self.extents = None
@@ -238,7 +243,7 @@ class MogBatch(object):
             _lib.check(rc, 'tb_approx3_region')
             self.ring_status = d[o_rst:o_rst + 16]
         self._dev = d
-        self.status = d[o_st:o_st + 16]
+        self.status = (out[-4:].view(torch.uint8) if self.status_in_out else d[o_st:o_st + 16])
         if check:
             check_status(self.status, 'tb_mog_render')
             if self.ring_status is not None:
@@ -374,8 +379,9 @@ class FftBatch(object):
     def run(self, out=None, stream=None, check=True):
         lib = _lib.load()
         dev = device()
+        self.status_in_out = out is None
         if out is None:
-            out = torch.empty(max(self.nout, 1), dtype=torch.float32, device=dev)
+            out = torch.empty(max(self.nout, 1) + 4, dtype=torch.float32, device=dev)
         if not self.items:
             return out
         items = np.array(self.items, dtype=_lib.FFT_ITEM)
@@ -389,11 +395,12 @@ class FftBatch(object):
         o_st = pk.add(np.zeros(1, _lib.STATUS))
         d = pk.to_device(dev)
         base = d.data_ptr()
+        st_ptr = out.data_ptr() + 4 * (out.numel() - 4) if self.status_in_out else base + o_st
         fourier_render(base + o_items, len(items), base + o_amp, base + o_var, specs.data_ptr(),
-                       out.data_ptr(), base + o_st,
+                       out.data_ptr(), st_ptr,
                        dcoef_ptr=None if o_dc is None else base + o_dc, stream=stream)
         self._keep = (d, specs)
-        self.status = d[o_st:o_st + 16]
+        self.status = (out[-4:].view(torch.uint8) if self.status_in_out else d[o_st:o_st + 16])
         if check:
             check_status(self.status, 'tb_fourier_render')
         return out
