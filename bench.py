@@ -1381,6 +1381,10 @@ def main():
     def step():
         renderer.render_device(d_src, n, out)
 
+    # the faster Fourier method on this workload (persistent or split)
+    tune = renderer.autotune(d_src, n, out)
+    from tractor_b200 import render as R
+    method = R.fourier_method[dev.index]
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
@@ -1403,10 +1407,9 @@ def main():
     clocks = ClockSampler(gpu_id)
     clocks.start()
     time.sleep(0.3)
-    from tractor_b200 import render as R
-    # column + row kernels per 256 items, and the persistent kernel for the
-    # items outside the split path
-    launches_per_render = 2 * (-(-n // 256)) + 1
+    # split: setup + column + row kernels per 256 items and the persistent
+    # kernel for the items outside the split path; persistent: one launch
+    launches_per_render = 3 * (-(-n // 256)) + 1 if method == 'split' else 1
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     for k in range(args.steps):
@@ -1423,7 +1426,8 @@ def main():
         _lib.check(rc, 'tb_galaxy_fft_prep')
         e1.record(stream)
         R.fourier_render(items_t.data_ptr(), n, camp.data_ptr(), cvar.data_ptr(),
-                         renderer.spec.data_ptr(), out.data_ptr(), misc.data_ptr() + 16)
+                         renderer.spec.data_ptr(), out.data_ptr(), misc.data_ptr() + 16,
+                         method=method)
         e2.record(stream)
     torch.cuda.synchronize()
     gpu_launches = (1 + launches_per_render) * args.steps
@@ -1490,7 +1494,10 @@ def main():
                 'h2d_bytes_per_step': int(src_pinned.numel()),
                 'd2h_bytes_per_step': int(out_pinned.numel() * 4)},
         'gpu_launches': gpu_launches,
-        'roofline': {'bound': 'sfu', 'kernel': 'tb_fourier_render_split (column + row kernels)',
+        'fourier_method': {'chosen': method, 'ms': {k: _sig(v) for k, v in tune.items()}},
+        'roofline': {'bound': 'sfu', 'kernel': 'tb_fourier_render_split (setup + column + row '
+                                               'kernels)' if method == 'split' else
+                     'tb_fourier_render (persistent)',
                      'achieved': achieved, 'peak': peak, 'unit': 'Gex2/s',
                      'frac': achieved / peak,
                      'peak_basis': '%d ex2/clk/SM x %d SMs x %s MHz (median under load)'

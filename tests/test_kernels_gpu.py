@@ -206,7 +206,7 @@ def test_split_path_matches_persistent_kernel(tb, oracle):
     out1 = torch.full((b.nout,), 7.0, dtype=torch.float32, device=dev)
     render.fourier_render(d_items.data_ptr(), len(items), amp.data_ptr(), var.data_ptr(),
                           specs.data_ptr(), out1.data_ptr(), misc.data_ptr() + 16,
-                          dcoef_ptr=dcoef.data_ptr())
+                          dcoef_ptr=dcoef.data_ptr(), method='split')
     torch.cuda.synchronize()
     render.check_status(misc[4:8].clone(), 'tb_fourier_render_split')
     a, c = out0.cpu().numpy(), out1.cpu().numpy()
@@ -223,7 +223,7 @@ def test_split_path_matches_persistent_kernel(tb, oracle):
     out2 = torch.zeros_like(out1)
     render.fourier_render(d_items.data_ptr(), len(items), amp.data_ptr(), var.data_ptr(),
                           specs.data_ptr(), out2.data_ptr(), misc.data_ptr() + 16,
-                          dcoef_ptr=dcoef.data_ptr())
+                          dcoef_ptr=dcoef.data_ptr(), method='split')
     assert torch.equal(out1, out2)
 
 

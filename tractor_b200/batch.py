@@ -124,7 +124,7 @@ class FourierGalaxyRenderer(object):
             self._scratch[n] = (items, camp, cvar, flags, misc)
         return self._scratch[n]
 
-    def render_device(self, srcs, n, out, stream=None):
+    def render_device(self, srcs, n, out, stream=None, method=None):
         """Renders n sources whose GALAXY_SRC records are in device tensor
         `srcs` (uint8 view) into float32 device tensor `out`.  Two kernel
         launches; nothing is copied to or from the host.  Returns the flags
@@ -139,8 +139,13 @@ class FourierGalaxyRenderer(object):
         _lib.check(rc, 'tb_galaxy_fft_prep')
         render.fourier_render(items.data_ptr(), n, camp.data_ptr(), cvar.data_ptr(),
                               self.spec.data_ptr(), out.data_ptr(), misc.data_ptr() + 16,
-                              stream=stream)
+                              stream=stream, method=method)
         return flags
+
+    def autotune(self, srcs, n, out):
+        """Times both Fourier methods on these device records and makes the
+        faster the device's default (render.autotune_fourier)."""
+        return render.autotune_fourier(lambda m: self.render_device(srcs, n, out, method=m))
 
     def status(self, n):
         return self._work(n)[4][4:8]

@@ -424,17 +424,70 @@ def fourier_workspace(n_items, dev=None):
     return ws
 
 
+FOURIER_METHODS = ('persistent', 'split')
+fourier_method = {'default': 'persistent'}   # per device index, set by autotune_fourier
+
+
 def fourier_render(items_ptr, n_items, amp_ptr, var_ptr, spec_ptr, out_ptr, status_ptr,
-                   dcoef_ptr=None, dots_ptr=None, stream=None):
-    """tb_fourier_render_split over device items (the product's Fourier
-    render: column and row kernels through an L2-resident scratch, the
-    items it does not cover by the persistent kernel)."""
+                   dcoef_ptr=None, dots_ptr=None, stream=None, method=None):
+    """Renders device Fourier items: 'persistent' -- tb_fourier_render(_deriv),
+    one CTA per galaxy holding its whole transpose in shared memory -- or
+    'split' -- tb_fourier_render_split, column and row kernels through an
+    L2-resident scratch.  The default is the device's autotuned choice
+    (autotune_fourier), else 'persistent'."""
     lib = _lib.load()
-    ws = fourier_workspace(n_items)
-    rc = lib.tb_fourier_render_split(items_ptr, int(n_items), amp_ptr, var_ptr, dcoef_ptr,
-                                     spec_ptr, out_ptr, dots_ptr, ws.data_ptr(), ws.numel(),
-                                     status_ptr, _lib.stream_ptr(stream))
-    _lib.check(rc, 'tb_fourier_render_split')
+    if method is None:
+        dev = device()
+        method = fourier_method.get(dev.index, fourier_method['default'])
+    s = _lib.stream_ptr(stream)
+    if method == 'split':
+        ws = fourier_workspace(n_items)
+        rc = lib.tb_fourier_render_split(items_ptr, int(n_items), amp_ptr, var_ptr, dcoef_ptr,
+                                         spec_ptr, out_ptr, dots_ptr, ws.data_ptr(), ws.numel(),
+                                         status_ptr, s)
+        _lib.check(rc, 'tb_fourier_render_split')
+        return
+    ctr = _counter(device())
+    if dcoef_ptr is None and dots_ptr is None:
+        rc = lib.tb_fourier_render(items_ptr, int(n_items), amp_ptr, var_ptr, spec_ptr, out_ptr,
+                                   ctr.data_ptr(), status_ptr, s)
+    else:
+        rc = lib.tb_fourier_render_deriv(items_ptr, int(n_items), amp_ptr, var_ptr, dcoef_ptr,
+                                         spec_ptr, out_ptr, dots_ptr, ctr.data_ptr(), status_ptr,
+                                         s)
+    _lib.check(rc, 'tb_fourier_render')
+
+
+_counters = {}
+
+
+def _counter(dev):
+    """A device int32 work counter for the persistent kernels (zeroed by each
+    launch on its stream before use)."""
+    c = _counters.get(dev.index)
+    if c is None:
+        c = _counters[dev.index] = torch.zeros(4, dtype=torch.int32, device=dev)
+    return c
+
+
+def autotune_fourier(run, reps=3):
+    """Times run(method) for each Fourier method (device events, after a
+    warm-up) and makes the fastest this device's default.  Returns
+    {method: ms}."""
+    dev = device()
+    times = {}
+    for m in FOURIER_METHODS:
+        run(m)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            run(m)
+        e1.record()
+        e1.synchronize()
+        times[m] = e0.elapsed_time(e1) / reps
+    fourier_method[dev.index] = min(times, key=times.get)
+    return times
 
 
 def lanczos_shift(imgs, shifts, stream=None):
