@@ -653,17 +653,19 @@ int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
 
 /* FP64 evaluation for the final iterations of a fit (no reference
  * counterpart beyond the optimum LsqrOptimizer.optimize_loop converges to,
- * lsqr_optimizer.py:317-326): for every running blob (status 0), A^T r and
- * chi^2 over the units' active tiles with the model, the residuals and the
- * sums in FP64 (FP64 exp from the FP64 component tables tb_fit_prep writes
- * into the workspace; the derivative columns in FP32), written into the
- * gbuf and chi2 slices that tb_fit_pass fills (call it in place of the
- * pass, before tb_fit_step; A^T A stays the last pass's); chi2_const (may
- * be NULL) is added to each slice's chi^2 as the pass does. */
+ * lsqr_optimizer.py:317-326): for every running blob (status 0), A^T A,
+ * A^T r and chi^2 over the units' active tiles with the model, the
+ * derivative columns, the residuals and the sums in FP64 (FP64 exp from the
+ * FP64 component tables tb_fit_prep writes into the workspace), written into
+ * the hbuf, gbuf and chi2 slices that tb_fit_pass fills (call it in place
+ * of the pass, before tb_fit_step); chi2_const (may be NULL) is added to
+ * each slice's chi^2 as the pass does.  hbuf = NULL: A^T A is left as it
+ * is and the columns of A^T r are evaluated in FP32 (the model, the
+ * residuals and the sums stay FP64), about half the cost. */
 int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
                   const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
                   const void* workspace, const float* data, const float* inverr,
-                  const int32_t* tiles, double* gbuf, double* chi2_out,
+                  const int32_t* tiles, double* hbuf, double* gbuf, double* chi2_out,
                   const double* chi2_const, const tb_fit_state* state, int32_t n_bands,
                   int32_t* work_counter, tb_status* status, void* stream);
 

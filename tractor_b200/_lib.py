@@ -136,8 +136,8 @@ SIGNATURES = {
     'tb_fit_pass': (_I32, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32,
                            _I32, _P, _P, _P]),
     'tb_fit_step': (_I32, [_P, _I32, _I32, _P, _P, _P, _P, _P, _P, _P, _D, _I32, _P]),
-    'tb_fit_refine': (_I32, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _I32,
-                             _P, _P, _P]),
+    'tb_fit_refine': (_I32, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                             _I32, _P, _P, _P]),
     'tb_fit_model_vjp': (_I32, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P, _I32, _I32, _P,
                                 _P, _P]),
     'tb_scene_render': (_I32, [_P, _I32, _P, _I32, _I64, _I32, _P, _P, _P, _P, _I32, _P, _I64,

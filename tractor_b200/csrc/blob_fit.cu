@@ -795,20 +795,22 @@ __device__ double max_step(int off) {
 }
 
 // ---------------------------------------------------------------------------
-// refinement pass (tb_fit_refine): A^T r and chi^2 of the running blobs with
-// the model, the residuals and the sums in FP64 (FP64 exp; the derivative
-// columns in FP32), written over the gradient and chi^2 slices.  Near the optimum the gradient is a sum of terms that cancel, and
-// its FP32 evaluation (FP32 model, FP32 partial sums) leaves an error that a
-// blob's flat directions (the index and radius of a large galaxy) amplify,
-// and FP32 chi^2 cannot verify gains below ~1e-4; the final iterations of a
-// fit take both in FP64, so the step's acceptance and its stopping rule see
-// the FP64 objective.  Same units, slices and layout as tb_fit_pass.
+// refinement pass (tb_fit_refine): the normal equations of the running blobs
+// in FP64 -- the model, the seven derivative columns of every source, the
+// residuals, A^T A, A^T r and chi^2 -- written over the slices tb_fit_pass
+// fills.  Near the optimum the gradient is a sum of terms that cancel, FP32
+// chi^2 cannot verify gains below ~1e-4, and an FP32 A^T A (FP32 columns:
+// the index column is a difference of nearly equal sums) is too inexact for
+// the steps of an ill-conditioned blob to converge; the final iterations of
+// a fit take all of them in FP64.  Same units, slices and layout as
+// tb_fit_pass.
 // ---------------------------------------------------------------------------
 constexpr int kRefThreads = 256;       // one 32 x 8 tile, one pixel per thread
+constexpr int kRefChunks = 8;          // 16-value chunks staged before a flush
 
 struct RefSrc {
     int32_t x0, y0, x1, y1;
-    int32_t K;
+    int32_t K, profile;
     double counts;
     double M[3];
     double dM[3][3];
@@ -816,48 +818,276 @@ struct RefSrc {
 
 struct RefSmem {
     RefSrc us[TB_FIT_MAX_SRC];
-    double red[kRefThreads / 32][8];
+    double red[kRefThreads / 32][kRefChunks * 16];
+    int dst[kRefChunks * 16];   // >= 0: H index; <= -2: g index -dst - 2; -1: none
     int64_t slot;
     int skip;
 };
 
-// Block sum of v[0 .. 7) over the CTA's threads, added by thread 0 to
-// out[slot[j]] (slot[j] < 0: dropped).
-__device__ __forceinline__ void ref_block_add(RefSmem& sm, const double* v, double* out,
-                                              const int* slot) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// Sum over the warp of v[0 .. 16): afterwards lanes 2k and 2k + 1 hold the
+// sum of v[k] (a reduce-scatter: 16 shuffles instead of 16 x 5).
+__device__ __forceinline__ double warp_reduce_scatter16(double (&v)[16], int lane) {
+    {
+        const bool hi = lane & 16;
 #pragma unroll
-    for (int j = 0; j < 7; j++) {
-        double x = v[j];
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) sm.red[warp][j] = x;
+        for (int i = 0; i < 8; i++) {
+            const double send = hi ? v[i] : v[i + 8];
+            const double keep = hi ? v[i + 8] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
     }
-    __syncthreads();
-    if (threadIdx.x < 7 && slot[threadIdx.x] >= 0) {
-        double t = 0.0;
-        for (int w = 0; w < kRefThreads / 32; w++) t += sm.red[w][threadIdx.x];
-        out[slot[threadIdx.x]] += t;
+    {
+        const bool hi = lane & 8;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const double send = hi ? v[i] : v[i + 4];
+            const double keep = hi ? v[i + 4] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        }
     }
-    __syncthreads();
+    {
+        const bool hi = lane & 4;
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const double send = hi ? v[i] : v[i + 2];
+            const double keep = hi ? v[i + 2] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+        }
+    }
+    {
+        const bool hi = lane & 2;
+        const double send = hi ? v[0] : v[1];
+        const double keep = hi ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
 }
 
-__global__ void __launch_bounds__(kRefThreads)
+// The staged chunks summed over the warps and added to their destinations
+// (each destination at most once per flush: a flush never spans two tiles).
+__device__ void ref_flush(RefSmem& sm, int& nc, double* H, double* g) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < nc * 16; j += kRefThreads) {
+        const int d = sm.dst[j];
+        if (d == -1) continue;
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kRefThreads / 32; w++) s += sm.red[w][j];
+        if (d >= 0) H[d] += s;
+        else g[-d - 2] += s;
+    }
+    __syncthreads();
+    nc = 0;
+}
+
+// Stages NV values (value(q), q a compile-time index after unrolling) in
+// chunks of 16, their destinations dest(q) (run time, warp 0).
+template <int NV, class Val, class Dst>
+__device__ __forceinline__ void ref_emit(RefSmem& sm, int& nc, double* H, double* g, Val value,
+                                         Dst dest) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c0 = 0; c0 < NV; c0 += 16) {
+        double v[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) v[k] = c0 + k < NV ? value(c0 + k) : 0.0;
+        const double s = warp_reduce_scatter16(v, lane);
+        const int k = lane >> 1;
+        if (!(lane & 1)) {
+            sm.red[warp][nc * 16 + k] = s;
+            if (warp == 0) sm.dst[nc * 16 + k] = c0 + k < NV ? dest(c0 + k) : -1;
+        }
+        if (++nc == kRefChunks) ref_flush(sm, nc, H, g);
+    }
+}
+
+// (i, j), i <= j < 7, of the q-th element of a 7 x 7 upper triangle
+// (row-major; rows start at 0, 7, 13, 18, 22, 25, 27).  Branch-free, so that
+// a compile-time q folds to constants.
+__host__ __device__ constexpr int tri_row(int q) {
+    return (q >= 7) + (q >= 13) + (q >= 18) + (q >= 22) + (q >= 25) + (q >= 27);
+}
+__host__ __device__ constexpr int tri_col(int q) {
+    return q - (tri_row(q) * 7 - tri_row(q) * (tri_row(q) - 1) / 2) + tri_row(q);
+}
+
+// Parameter slot of column i (x y flux(band) logre ee1 ee2 n) of source sI;
+// -1 where the profile has no such parameter.
+__device__ __forceinline__ int ref_slot(int sI, int profile, int band, int i) {
+    if (i >= 3 && profile == TB_PROFILE_POINT) return -1;
+    if (i == 6 && profile != TB_PROFILE_SERSIC) return -1;
+    const int base = sI * TB_FIT_NPAR;
+    return i < 2 ? base + i : i == 2 ? base + 2 + band : base + 2 + i;
+}
+
+// Source R's model at (px, py) (counts x its unit-flux mixture), FP64.
+__device__ __forceinline__ double ref_model(const RefSrc& R, const FitC64* cs, int px, int py) {
+    if (!(px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1)) return 0.0;
+    double val = 0.0;
+    for (int k = 0; k < R.K; k++) {
+        const FitC64& c = cs[k];
+        const double dx = px - c.mx, dy = py - c.my;
+        const double ux = c.i00 * dx + c.i01 * dy, uy = c.i01 * dx + c.i11 * dy;
+        const double e = -0.5 * (dx * ux + dy * uy);
+        if (e >= -50.0) val += c.s * exp(e);
+    }
+    return R.counts * val;
+}
+
+// Source R's seven derivative columns at (px, py) (zero outside its
+// rectangle) and its model there, FP64: per component the moments of
+// C^-1 u (u = pixel - mean) that d/d(mean, C, amplitude) produce, combined
+// once per source with dM (shape) and M (index).
+__device__ __forceinline__ double ref_cols(const RefSrc& R, const FitC64* cs, int px, int py,
+                                           double (&J)[7]) {
+#pragma unroll
+    for (int j = 0; j < 7; j++) J[j] = 0.0;
+    if (!(px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1)) return 0.0;
+    double S0 = 0, Sx = 0, Sy = 0, Axx = 0, Axy = 0, Ayy = 0, At0 = 0, At1 = 0, At2 = 0;
+    double Dxx = 0, Dxy = 0, Dyy = 0, Dt = 0, Sn = 0;
+    for (int k = 0; k < R.K; k++) {
+        const FitC64& c = cs[k];
+        const double dx = px - c.mx, dy = py - c.my;
+        const double ux = c.i00 * dx + c.i01 * dy, uy = c.i01 * dx + c.i11 * dy;
+        const double e = -0.5 * (dx * ux + dy * uy);
+        if (e < -50.0) continue;
+        const double E = exp(e);
+        const double val = c.s * E;
+        S0 += val;
+        Sx = fma(val, ux, Sx);
+        Sy = fma(val, uy, Sy);
+        const double vv = val * c.v;
+        Axx = fma(vv * ux, ux, Axx);
+        Axy = fma(vv * ux, uy, Axy);
+        Ayy = fma(vv * uy, uy, Ayy);
+        At0 = fma(vv, c.t[0], At0);
+        At1 = fma(vv, c.t[1], At1);
+        At2 = fma(vv, c.t[2], At2);
+        const double vd = val * c.dv;
+        Dxx = fma(vd * ux, ux, Dxx);
+        Dxy = fma(vd * ux, uy, Dxy);
+        Dyy = fma(vd * uy, uy, Dyy);
+        Dt = fma(vd, c.t[3], Dt);
+        Sn = fma(c.sn, E, Sn);
+    }
+    const double cn = R.counts;
+    const double At[3] = {At0, At1, At2};
+    J[0] = cn * Sx;
+    J[1] = cn * Sy;
+    J[2] = S0;
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+        J[3 + j] = cn * 0.5 * (R.dM[j][0] * Axx + 2.0 * R.dM[j][1] * Axy + R.dM[j][2] * Ayy - At[j]);
+    J[6] = cn * (0.5 * (R.M[0] * Dxx + 2.0 * R.M[1] * Dxy + R.M[2] * Dyy - Dt) + Sn);
+    return cn * S0;
+}
+
+// Source R's seven derivative columns at (px, py) from the FP32 component
+// tables (FP32 exp and moments; for A^T r, whose column errors multiply
+// residuals that are noise at the optimum and average out).
+__device__ __forceinline__ void ref_cols32(const RefSrc& R, const FitC* cs, int px, int py,
+                                           double (&J)[7]) {
+#pragma unroll
+    for (int j = 0; j < 7; j++) J[j] = 0.0;
+    if (!(px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1)) return;
+    float S0 = 0, Sx = 0, Sy = 0, Axx = 0, Axy = 0, Ayy = 0;
+    float At[3] = {0, 0, 0};
+    float Dxx = 0, Dxy = 0, Dyy = 0, Dt = 0, Sn = 0;
+    for (int k = 0; k < R.K; k++) {
+        const FitC& c = cs[k];
+        const float dx = (float)(px - c.mx), dy = (float)(py - c.my);
+        const float e = fmaf(dy, fmaf(c.qyy, dy, c.qxy * dx), c.qxx * dx * dx);
+        if (e < c.fl) continue;
+        const float E = tb::ex2(e);
+        const float val = c.s * E;
+        const float ux = fmaf(c.ixx, dx, c.ixy * dy), uy = fmaf(c.ixy, dx, c.iyy * dy);
+        S0 += val;
+        Sx = fmaf(val, ux, Sx);
+        Sy = fmaf(val, uy, Sy);
+        const float vv = val * c.v;
+        Axx = fmaf(vv * ux, ux, Axx);
+        Axy = fmaf(vv * ux, uy, Axy);
+        Ayy = fmaf(vv * uy, uy, Ayy);
+        At[0] = fmaf(vv, c.t[0], At[0]);
+        At[1] = fmaf(vv, c.t[1], At[1]);
+        At[2] = fmaf(vv, c.t[2], At[2]);
+        const float vd = val * c.dv;
+        Dxx = fmaf(vd * ux, ux, Dxx);
+        Dxy = fmaf(vd * ux, uy, Dxy);
+        Dyy = fmaf(vd * uy, uy, Dyy);
+        Dt = fmaf(vd, c.t[3], Dt);
+        Sn = fmaf(c.sn, E, Sn);
+    }
+    const double cn = R.counts;
+    J[0] = cn * Sx;
+    J[1] = cn * Sy;
+    J[2] = S0;
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+        J[3 + j] = cn * 0.5 * (R.dM[j][0] * Axx + 2.0 * R.dM[j][1] * Axy + R.dM[j][2] * Ayy - At[j]);
+    J[6] = cn * (0.5 * (R.M[0] * Dxx + 2.0 * R.M[1] * Dxy + R.M[2] * Dyy - Dt) + Sn);
+}
+
+// A source's own block: REFINE, its 28 A^T A products (upper triangle) and
+// 7 A^T r values; VJP, the 7 contracted columns.
+__device__ __forceinline__ void ref_emit_own(RefSmem& sm, int& nc, double* H, double* g,
+                                             const double (&Jw)[7], double rr, int sI,
+                                             const RefSrc& R, int band, int P, bool refine) {
+    if (refine) {
+        ref_emit<35>(sm, nc, H, g,
+            [&](int q) { return q < 28 ? Jw[tri_row(q)] * Jw[tri_col(q)] : Jw[q - 28] * rr; },
+            [&](int q) {
+                if (q >= 28) {
+                    const int s = ref_slot(sI, R.profile, band, q - 28);
+                    return s < 0 ? -1 : -s - 2;
+                }
+                const int a = ref_slot(sI, R.profile, band, tri_row(q));
+                const int c = ref_slot(sI, R.profile, band, tri_col(q));
+                return a < 0 || c < 0 ? -1 : a * P + c;
+            });
+    } else {
+        ref_emit<7>(sm, nc, H, g, [&](int q) { return Jw[q] * rr; },
+            [&](int q) {
+                const int s = ref_slot(sI, R.profile, band, q);
+                return s < 0 ? -1 : -s - 2;
+            });
+    }
+}
+
+// The A^T A block of two sources sA < sB (49 products).
+__device__ __forceinline__ void ref_emit_pair(RefSmem& sm, int& nc, double* H, double* g,
+                                              const double (&Ja)[7], const double (&Jb)[7],
+                                              int sA, int sB, int band, int P) {
+    const int pa = sm.us[sA].profile, pb = sm.us[sB].profile;
+    ref_emit<49>(sm, nc, H, g, [&](int q) { return Ja[q / 7] * Jb[q % 7]; },
+        [&](int q) {
+            const int a = ref_slot(sA, pa, band, q / 7);
+            const int c = ref_slot(sB, pb, band, q % 7);
+            return a < 0 || c < 0 ? -1 : a * P + c;
+        });
+}
+
+__global__ void __launch_bounds__(kRefThreads, 2)
 fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict__ order,
                   int n_units, const tb_fit_blob* __restrict__ blobs,
                   const tb_fit_source* __restrict__ srcs, const SrcTab* __restrict__ tab,
                   const FitC64* __restrict__ gcomps, const FitC* __restrict__ gcomps32,
                   const float* __restrict__ data,
-                  const float* __restrict__ inverr, double* __restrict__ gbuf,
-                  double* __restrict__ chi2_out, const tb_fit_state* __restrict__ state,
-                  int n_bands, const int32_t* __restrict__ tiles, int32_t* counter,
-                  tb_status* st, int mode, float* __restrict__ model_out,
-                  const double* __restrict__ chi2_const) {
-    // mode TB_FIT_REFINE: A^T r of finished blobs, r = (data - model) inverr;
-    // TB_FIT_MODEL: the model into model_out (every blob); TB_FIT_VJP: the
-    // columns contracted with data = an upstream gradient, unweighted
+                  const float* __restrict__ inverr, double* __restrict__ hbuf,
+                  double* __restrict__ gbuf, double* __restrict__ chi2_out,
+                  const tb_fit_state* __restrict__ state, int n_bands,
+                  const int32_t* __restrict__ tiles, int32_t* counter, tb_status* st, int mode,
+                  float* __restrict__ model_out, const double* __restrict__ chi2_const) {
+    // mode TB_FIT_REFINE: A^T A (hbuf != NULL), A^T r and chi^2 of the
+    // running blobs, r = (data - model) inverr; without hbuf the columns of
+    // A^T r come from the FP32 tables (the model stays FP64); TB_FIT_MODEL:
+    // the model into model_out (every blob); TB_FIT_VJP: the columns
+    // contracted with data = an upstream gradient, unweighted
     __shared__ RefSmem sm;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
+    const bool refine = mode == TB_FIT_REFINE && hbuf != nullptr;
+    const bool grad_only = mode == TB_FIT_REFINE && hbuf == nullptr;
     for (;;) {
         const int64_t oi = tb::next_unit(counter, &sm.slot);
         if (oi >= n_units) break;
@@ -868,9 +1098,12 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
         if (mode == TB_FIT_REFINE && state[u.blob].status != 0) continue;   // running blobs
         const int P = b.P;
         const int nsrc = b.n_src;
-        double* g = gbuf + b.g_off + (int64_t)u.slice * P;
+        double* g = gbuf ? gbuf + b.g_off + (int64_t)u.slice * P : nullptr;
+        double* H = refine ? hbuf + b.h_off + (int64_t)u.slice * P * P : nullptr;
         if (mode != TB_FIT_MODEL)
             for (int e = tid; e < P; e += kRefThreads) g[e] = 0.0;
+        if (refine)
+            for (int e = tid; e < P * P; e += kRefThreads) H[e] = 0.0;
         if (warp == 0) {
             const bool unit_bad = nsrc < 0 || nsrc > TB_FIT_MAX_SRC || P != nsrc * TB_FIT_NPAR ||
                                   u.band < 0 || u.band >= n_bands || u.slice < 0 ||
@@ -889,6 +1122,7 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
                 R.x1 = live ? fs.x0 + fs.w : 0;
                 R.y1 = live ? fs.y0 + fs.h : 0;
                 R.K = K;
+                R.profile = fs.profile;
                 R.counts = S.flux[u.band];
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
@@ -915,10 +1149,19 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
         const int n_t = u.t1 - u.t0;
         const int32_t* tl = tiles + b.tile_off + u.t0;
         double chi2 = 0.0;
+        int nc = 0;
         for (int t = 0; t < n_t; t++) {
             const int ox = (tl[t] & 0x3ff) * kTileW, oy = ((tl[t] >> 10) & 0x3ff) * kTileH;
             const int px = ox + lane, py = oy + warp;
             const bool in = px < u.W && py < u.H;
+            // the sources whose rectangles meet the tile (the same for every thread)
+            unsigned reach = 0u;
+            if (lane < nsrc) {
+                const RefSrc& R = sm.us[lane];
+                reach = R.x1 > ox && R.x0 < ox + kTileW && R.y1 > oy && R.y0 < oy + kTileH;
+            }
+            reach = __ballot_sync(0xffffffffu, reach);
+            const int nreach = __popc(reach);
             double d = 0.0, w = 0.0;
             const int64_t pix = u.pix_off + (int64_t)py * u.W + px;
             // MODEL reads neither data nor inverr (both may be NULL); VJP
@@ -927,97 +1170,85 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
                 d = data[pix];
                 w = mode == TB_FIT_VJP ? 1.0 : inverr[pix];
             }
-            // the model at this pixel
-            double m = 0.0;
-            for (int sI = 0; sI < nsrc && mode != TB_FIT_VJP; sI++) {
-                const RefSrc& R = sm.us[sI];
-                if (!(px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1) || !in) continue;
-                const FitC64* cs = band_comps + sI * cstride;
-                double val = 0.0;
-                for (int k = 0; k < R.K; k++) {
-                    const FitC64& c = cs[k];
-                    const double dx = px - c.mx, dy = py - c.my;
-                    const double e = -0.5 * (c.i00 * dx * dx + 2.0 * c.i01 * dx * dy +
-                                             c.i11 * dy * dy);
-                    if (e >= -50.0) val += c.s * exp(e);
-                }
-                m += R.counts * val;
-            }
             if (mode == TB_FIT_MODEL) {
+                double m = 0.0;
+                for (unsigned rm = reach; rm && in; rm &= rm - 1) {
+                    const int sI = __ffs(rm) - 1;
+                    m += ref_model(sm.us[sI], band_comps + sI * cstride, px, py);
+                }
                 if (in) model_out[pix] = (float)m;
                 continue;
             }
-            const double r = mode == TB_FIT_VJP ? d : (d - m) * w;
-            chi2 += r * r;
-            // each source reaching the tile: its seven columns times inverr times r
-            for (int sI = 0; sI < nsrc; sI++) {
-                const RefSrc& R = sm.us[sI];
-                if (R.x1 <= ox || R.x0 >= ox + kTileW || R.y1 <= oy || R.y0 >= oy + kTileH)
-                    continue;   // the same for every thread of the tile
-                double J[7] = {0, 0, 0, 0, 0, 0, 0};
-                if (in && px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1) {
-                    // the derivative columns in FP32 (their errors, multiplied by
-                    // residuals that are noise at the optimum, average out); the
-                    // model and the residual above are FP64
-                    const FitC* cs = band_comps32 + sI * cstride;
-                    float S0 = 0, Sx = 0, Sy = 0, Axx = 0, Axy = 0, Ayy = 0;
-                    float At[3] = {0, 0, 0};
-                    float Dxx = 0, Dxy = 0, Dyy = 0, Dt = 0, Sn = 0;
-                    for (int k = 0; k < R.K; k++) {
-                        const FitC& c = cs[k];
-                        const float dx = (float)(px - c.mx), dy = (float)(py - c.my);
-                        const float e = fmaf(dy, fmaf(c.qyy, dy, c.qxy * dx), c.qxx * dx * dx);
-                        if (e < c.fl) continue;
-                        const float E = tb::ex2(e);
-                        const float val = c.s * E;
-                        const float ux = fmaf(c.ixx, dx, c.ixy * dy), uy = fmaf(c.ixy, dx, c.iyy * dy);
-                        S0 += val;
-                        Sx = fmaf(val, ux, Sx);
-                        Sy = fmaf(val, uy, Sy);
-                        const float vv = val * c.v;
-                        Axx = fmaf(vv * ux, ux, Axx);
-                        Axy = fmaf(vv * ux, uy, Axy);
-                        Ayy = fmaf(vv * uy, uy, Ayy);
-                        At[0] = fmaf(vv, c.t[0], At[0]);
-                        At[1] = fmaf(vv, c.t[1], At[1]);
-                        At[2] = fmaf(vv, c.t[2], At[2]);
-                        const float vd = val * c.dv;
-                        Dxx = fmaf(vd * ux, ux, Dxx);
-                        Dxy = fmaf(vd * ux, uy, Dxy);
-                        Dyy = fmaf(vd * uy, uy, Dyy);
-                        Dt = fmaf(vd, c.t[3], Dt);
-                        Sn = fmaf(c.sn, E, Sn);
-                    }
-                    const double cn = R.counts;
-                    J[0] = cn * Sx;
-                    J[1] = cn * Sy;
-                    J[2] = S0;
-#pragma unroll
-                    for (int j = 0; j < 3; j++)
-                        J[3 + j] = cn * 0.5 * (R.dM[j][0] * Axx + 2.0 * R.dM[j][1] * Axy +
-                                               R.dM[j][2] * Ayy - At[j]);
-                    J[6] = cn * (0.5 * (R.M[0] * Dxx + 2.0 * R.M[1] * Dxy + R.M[2] * Dyy - Dt) +
-                                 Sn);
-                    const double wr = w * r;
-#pragma unroll
-                    for (int j = 0; j < 7; j++) J[j] *= wr;
+            if (grad_only) {
+                // the FP64 model, then each source's FP32 columns times w r
+                double m = 0.0;
+                for (unsigned rm = reach; rm; rm &= rm - 1) {
+                    const int sI = __ffs(rm) - 1;
+                    m += ref_model(sm.us[sI], band_comps + sI * cstride, px, py);
                 }
-                // columns x y flux(band) logre ee1 ee2 n -> the source's slots
-                const tb_fit_source fs = srcs[b.src0 + sI];
-                int slot[7];
-                const int base = sI * TB_FIT_NPAR;
-                slot[0] = base + 0;
-                slot[1] = base + 1;
-                slot[2] = base + 2 + u.band;
-                slot[3] = base + 5;
-                slot[4] = base + 6;
-                slot[5] = base + 7;
-                slot[6] = base + 8;
-                if (fs.profile == TB_PROFILE_POINT) slot[3] = slot[4] = slot[5] = slot[6] = -1;
-                else if (fs.profile != TB_PROFILE_SERSIC) slot[6] = -1;
-                ref_block_add(sm, J, g, slot);
+                const double r = (d - m) * w;
+                chi2 += r * r;
+                for (unsigned ra = reach; ra; ra &= ra - 1) {
+                    const int sA = __ffs(ra) - 1;
+                    double Ja[7];
+                    ref_cols32(sm.us[sA], band_comps32 + sA * cstride, px, py, Ja);
+#pragma unroll
+                    for (int j = 0; j < 7; j++) Ja[j] *= w;
+                    ref_emit_own(sm, nc, H, g, Ja, r, sA, sm.us[sA], u.band, P, false);
+                }
+            } else if (nreach <= 2) {
+                // one or two sources: their columns and the model in one evaluation
+                const int s0 = nreach > 0 ? __ffs(reach) - 1 : -1;
+                const int s1 = nreach > 1 ? __ffs(reach & (reach - 1)) - 1 : -1;
+                double J0[7], J1[7];
+                double m = 0.0;
+                if (s0 >= 0) m += ref_cols(sm.us[s0], band_comps + s0 * cstride, px, py, J0);
+                if (s1 >= 0) m += ref_cols(sm.us[s1], band_comps + s1 * cstride, px, py, J1);
+                const double r = refine ? (d - m) * w : d;
+                if (refine) chi2 += r * r;
+                if (s0 >= 0) {
+#pragma unroll
+                    for (int j = 0; j < 7; j++) J0[j] *= w;
+                    ref_emit_own(sm, nc, H, g, J0, r, s0, sm.us[s0], u.band, P, refine);
+                }
+                if (s1 >= 0) {
+#pragma unroll
+                    for (int j = 0; j < 7; j++) J1[j] *= w;
+                    ref_emit_own(sm, nc, H, g, J1, r, s1, sm.us[s1], u.band, P, refine);
+                    if (refine) ref_emit_pair(sm, nc, H, g, J0, J1, s0, s1, u.band, P);
+                }
+            } else {
+                // three or more: the model first, then each source's columns
+                // (a pair's block re-evaluates the later source)
+                double m = 0.0;
+                if (refine)
+                    for (unsigned rm = reach; rm; rm &= rm - 1) {
+                        const int sI = __ffs(rm) - 1;
+                        m += ref_model(sm.us[sI], band_comps + sI * cstride, px, py);
+                    }
+                const double r = refine ? (d - m) * w : d;
+                if (refine) chi2 += r * r;
+                for (unsigned ra = reach; ra; ra &= ra - 1) {
+                    const int sA = __ffs(ra) - 1;
+                    double Ja[7];
+                    ref_cols(sm.us[sA], band_comps + sA * cstride, px, py, Ja);
+#pragma unroll
+                    for (int j = 0; j < 7; j++) Ja[j] *= w;
+                    ref_emit_own(sm, nc, H, g, Ja, r, sA, sm.us[sA], u.band, P, refine);
+                    if (!refine) continue;
+                    for (unsigned rb = ra & (ra - 1); rb; rb &= rb - 1) {
+                        const int sB = __ffs(rb) - 1;
+                        double Jb[7];
+                        ref_cols(sm.us[sB], band_comps + sB * cstride, px, py, Jb);
+#pragma unroll
+                        for (int j = 0; j < 7; j++) Jb[j] *= w;
+                        ref_emit_pair(sm, nc, H, g, Ja, Jb, sA, sB, u.band, P);
+                    }
+                }
             }
+            if (nc > 0) ref_flush(sm, nc, H, g);
         }
+        if (mode == TB_FIT_MODEL) continue;
         // the unit's chi^2 (its active tiles; the constant part stays in chi2_const)
         for (int o = 16; o > 0; o >>= 1) chi2 += __shfl_xor_sync(0xffffffffu, chi2, o);
         if (lane == 0) sm.red[warp][0] = chi2;
@@ -1410,10 +1641,10 @@ extern "C" int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_
 extern "C" int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
                              const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
                              const void* workspace, const float* data, const float* inverr,
-                             const int32_t* tiles, double* gbuf, double* chi2_out,
-                             const double* chi2_const, const tb_fit_state* state,
-                             int32_t n_bands, int32_t* work_counter, tb_status* status,
-                             void* stream) {
+                             const int32_t* tiles, double* hbuf, double* gbuf,
+                             double* chi2_out, const double* chi2_const,
+                             const tb_fit_state* state, int32_t n_bands, int32_t* work_counter,
+                             tb_status* status, void* stream) {
     if (n_units < 0 || n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS) return TB_ERR_ARG;
     if (n_units == 0) return TB_OK;
     if (!units || !order || !blobs || !srcs || !workspace || !data || !inverr || !tiles ||
@@ -1432,8 +1663,8 @@ extern "C" int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int
     void* ws = const_cast<void*>(workspace);
     fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
         units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands),
-        ws_comps(ws, n_src), data, inverr, gbuf, chi2_out, state, n_bands, tiles, work_counter,
-        status, TB_FIT_REFINE, nullptr, chi2_const);
+        ws_comps(ws, n_src), data, inverr, hbuf, gbuf, chi2_out, state, n_bands, tiles,
+        work_counter, status, TB_FIT_REFINE, nullptr, chi2_const);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
@@ -1462,8 +1693,8 @@ extern "C" int tb_fit_model_vjp(const tb_fit_unit* units, const int32_t* order, 
     void* ws = const_cast<void*>(workspace);
     fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
         units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands),
-        ws_comps(ws, n_src), grad, nullptr, gbuf, nullptr, nullptr, n_bands, tiles, work_counter,
-        status, mode, model, nullptr);
+        ws_comps(ws, n_src), grad, nullptr, nullptr, gbuf, nullptr, nullptr, n_bands, tiles,
+        work_counter, status, mode, model, nullptr);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 

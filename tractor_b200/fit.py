@@ -168,29 +168,29 @@ class BlobFitter(object):
                                    self.misc.data_ptr(), self.misc.data_ptr() + 16,
                                    _lib.stream_ptr()), 'tb_fit_pass')
 
-    def _refine_pass(self):
-        """A^T r and chi^2 of the running blobs in FP64 (tb_fit_refine), over
-        the slices the FP32 pass just wrote."""
+    def _refine_pass(self, hessian=True):
+        """A^T A, A^T r and chi^2 of the running blobs in FP64
+        (tb_fit_refine), into the slices the FP32 pass writes; without
+        `hessian`, A^T r and chi^2 only (A^T A stays the last one)."""
         lib = _lib.load()
         _lib.check(lib.tb_fit_refine(self.d_pass_units.data_ptr(), self.d_order.data_ptr(),
                                      len(self.pass_units_np), self.d_blobs.data_ptr(),
                                      self.d_sources.data_ptr(), self.n_src,
                                      self.workspace.data_ptr(), self.data.data_ptr(),
                                      self.inverr.data_ptr(), self.d_tiles.data_ptr(),
+                                     self.hbuf.data_ptr() if hessian else None,
                                      self.gbuf.data_ptr(), self.chi2_part.data_ptr(),
                                      self.chi2_const.data_ptr(), self.state.data_ptr(),
                                      self.n_bands, self.misc.data_ptr(),
                                      self.misc.data_ptr() + 16, _lib.stream_ptr()),
                    'tb_fit_refine')
 
-    def _iteration(self, tol, max_iter, precise=False):
+    def _iteration(self, tol, max_iter, precise=False, hessian=True):
         lib = _lib.load()
         s = _lib.stream_ptr()
         self._prep()
         if precise:
-            # A^T r and chi^2 in FP64; A^T A stays the FP32 one of the last
-            # pass of the FP32 phase (it changes little over the last steps)
-            self._refine_pass()
+            self._refine_pass(hessian)
         else:
             self._pass(0)
         _lib.check(lib.tb_fit_step(self.d_blobs.data_ptr(), self.n_blobs, self.n_bands,
@@ -219,15 +219,19 @@ class BlobFitter(object):
         return int((st[:, -1] == 0).sum().item())
 
     def fit(self, tol=1e-3, max_iter=200, check_every=4, graph=True, params0=None,
-            lambda0=1e-3, refine=True, refine_tol=1e-10, refine_iter=40):
+            lambda0=1e-3, refine=True, refine_tol=1e-9, refine_iter=25, handoff=0.005,
+            refresh=4):
         """Runs FP32 iterations until every blob stops (or max_iter); then,
         with `refine`, continues every blob from where it stopped with the
-        gradient and chi^2 in FP64 (tb_fit_refine in place of the pass; A^T A
-        is the last FP32 one) until the predicted gain is below refine_tol
-        (or refine_iter): the FP32 objective cannot resolve the last ~1e-4
-        of log-likelihood, which leaves the flat directions of a blob a few
-        1e-3 sigma from the optimum.  Returns the number of iterations
-        launched (both phases)."""
+        normal equations in FP64 (tb_fit_refine in place of the pass) until
+        the predicted gain is below refine_tol (or refine_iter): the FP32
+        objective cannot resolve the last ~1e-4 of log-likelihood, which
+        leaves the flat directions of a blob a few 1e-3 sigma from the
+        optimum, and an FP32 A^T A is too inexact for an ill-conditioned
+        blob's steps to converge.  With `refine`, the FP32 phase also ends
+        once at most a fraction `handoff` of the blobs still runs: those
+        continue in the FP64 phase from where they are.  Returns the number
+        of iterations launched (both phases)."""
         self.reset(params0, lambda0)
         g = None
         if graph:
@@ -239,7 +243,8 @@ class BlobFitter(object):
                 for _ in range(check_every):
                     self._iteration(tol, max_iter)
             self.iterations += check_every
-            if self.running() == 0:
+            r = self.running()
+            if r == 0 or (refine and r <= handoff * self.n_blobs):
                 break
         if refine:
             # the FP64 phase starts every blob again from its parameters
@@ -251,7 +256,9 @@ class BlobFitter(object):
             self.reset(None, 1e-9)
             self.iterations = n
             for it in range(int(refine_iter)):
-                self._iteration(refine_tol, refine_iter, precise=True)
+                # A^T A in FP64 at the start and every `refresh` iterations
+                self._iteration(refine_tol, refine_iter, precise=True,
+                                hessian=it % int(refresh) == 0)
                 self.iterations += 1
                 if it % 2 == 1 and self.running() == 0:
                     break

@@ -270,3 +270,53 @@ class BlobFitFP64(object):
                 if lam > 1e12:
                     break
         return theta, it
+
+
+def sersic_edges():
+    """Sersic indices where the mixture tables change: the inner edges of
+    the index ranges (each range is a separate fit, with its own component
+    count) and n = 1, above which the core component is added.  The model
+    is not smooth across them."""
+    R = profiles.tables()['sersic']['ranges']
+    return np.array(sorted({r['lo'] for r in R[1:]} | {1.0}))
+
+
+def optimum_distance(w, data, inv, fitted, status, blobs, device, tol=1e-10, max_iter=40,
+                     edge=1e-3):
+    """Distance of batched-fit results from the FP64 optimum, per blob of
+    `blobs` (a blob workload of tractor_b200.fit): the FP64 fitter continued
+    from the batched result to a predicted gain of `tol`, then
+    max_i |fitted_i - opt_i| / sigma_i with sigma from its FP64 Fisher
+    matrix (a Sersic index held at a bound, and directions the Fisher
+    matrix leaves unconstrained, count as sigma = inf).  Returns one record
+    per blob: (sigma, blob, status, on_edge), on_edge when a Sersic index
+    (batched or FP64) lies within `edge` of sersic_edges()."""
+    from . import fit as _fit
+    po = _fit.pix_offsets(w['sides'], 3)
+    hd, hi = data.cpu().numpy(), inv.cpu().numpy()
+    edges = sersic_edges()
+    out = []
+    for b in blobs:
+        s0, s1 = int(w['blob_src'][b]), int(w['blob_src'][b + 1])
+        W, H = (int(v) for v in w['sides'][b])
+        d3 = np.stack([hd[po[3 * b + k]:po[3 * b + k + 1]].reshape(H, W) for k in range(3)])
+        i3 = np.stack([hi[po[3 * b + k]:po[3 * b + k + 1]].reshape(H, W) for k in range(3)])
+        rects = [tuple(int(v) for v in (r['x0'], r['y0'], r['w'], r['h']))
+                 for r in w['sources'][s0:s1]]
+        pf = BlobFitFP64(d3, i3, w['psf'][b], rects, device)
+        opt, _ = pf.fit(fitted[s0:s1], tol=tol, max_iter=max_iter)
+        Hf = pf.fisher(opt)
+        o = opt.ravel()
+        n_idx = np.arange(8, o.size, 9)
+        held = np.zeros(o.size, bool)
+        held[n_idx] = (o[n_idx] >= _fit.SERSIC_MAX) | (o[n_idx] <= _fit.SERSIC_MIN)
+        free = ~held & (np.diag(Hf) > 0)
+        sig = np.full(o.size, np.inf)
+        with np.errstate(invalid='ignore'):
+            sig[free] = np.sqrt(np.diag(np.linalg.inv(Hf[np.ix_(free, free)])))
+        sig[~(np.isfinite(sig) & (sig > 0))] = np.inf
+        err = float(np.max(np.abs(np.asarray(fitted[s0:s1]).ravel() - o) / sig))
+        nn = np.concatenate([np.asarray(fitted[s0:s1])[:, 8], opt[:, 8]])
+        on_edge = bool(np.min(np.abs(nn[:, None] - edges[None])) < edge)
+        out.append((err, int(b), int(status[b]), on_edge))
+    return out
