@@ -639,8 +639,9 @@ int tb_fit_pass(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
                 int32_t mode, int32_t* work_counter, tb_status* status, void* stream);
 
 /* One Levenberg-Marquardt step per running blob: accept the trial
- * parameters if chi^2 fell (the first pass is always accepted), else raise
- * the damping; solve (D^-1 H D^-1 + lambda I) x = D^-1 g, D = sqrt(diag H),
+ * parameters if chi^2 fell (the first pass is always accepted; the damping
+ * then follows the ratio rho of the actual to the predicted gain, lambda x
+ * max(1/3, 1 - (2 rho - 1)^3)), else raise the damping x 10; solve (D^-1 H D^-1 + lambda I) x = D^-1 g, D = sqrt(diag H),
  * by FP64 Cholesky with one refinement step; scale the step to respect the
  * maximum steps (PixPos 1, log r_e 1, ee 0.1, n 0.1) and the Sersic-index
  * bounds; write params + step into `trial`.  Stops a blob when the step's
@@ -659,9 +660,7 @@ int tb_fit_step(const tb_fit_blob* blobs, int32_t n_blobs, int32_t n_bands,
  * FP64 component tables tb_fit_prep writes into the workspace), written into
  * the hbuf, gbuf and chi2 slices that tb_fit_pass fills (call it in place
  * of the pass, before tb_fit_step); chi2_const (may be NULL) is added to
- * each slice's chi^2 as the pass does.  hbuf = NULL: A^T A is left as it
- * is and the columns of A^T r are evaluated in FP32 (the model, the
- * residuals and the sums stay FP64), about half the cost. */
+ * each slice's chi^2 as the pass does. */
 int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int32_t n_units,
                   const tb_fit_blob* blobs, const tb_fit_source* srcs, int32_t n_src,
                   const void* workspace, const float* data, const float* inverr,

@@ -74,6 +74,31 @@ def test_normal_equations_match_oracle(tb, oracle):
         assert abs(st['chi2'][b] - c2o) <= 1e-5 * c2o, b
 
 
+def test_refine_normal_equations_match_oracle(tb, oracle):
+    """The FP64 evaluation of the final iterations (tb_fit_refine) at the
+    starting parameters: its A^T A and A^T r against the oracle's FP64
+    central differences within 1e-6 of their natural scales (the
+    differences' own error), chi^2 within 1e-9 relative."""
+    w, datas, inverrs = _small_blobs(oracle, 1)
+    f = _fitter(w, datas, inverrs)
+    f.reset(w['start'], 1e-9)
+    f._iteration(0.0, 100, precise=True)
+    st = f.states()
+    for b in range(len(datas)):
+        s0, s1, W, H, rects = _blob_args(w, b)
+        Ho, go, c2o = oracle.blob_normal_equations(w['start'][s0:s1], rects, W, H, w['psf'][b], 3,
+                                                   datas[b].astype(np.float64),
+                                                   inverrs[b].astype(np.float64))
+        Hg, gg = f.normal_equations(b)
+        d = np.sqrt(np.diag(Ho))
+        scale = np.outer(d, d)
+        live = scale > 0
+        assert np.all(np.abs(Hg - Ho)[live] <= 1e-6 * scale[live]), b
+        assert np.all(Hg[~live] == 0)
+        assert np.all(np.abs(gg - go) <= 1e-6 * d * np.sqrt(c2o) + 1e-9), b
+        assert abs(st['chi2'][b] - c2o) <= 1e-9 * c2o, (b, st['chi2'][b], c2o)
+
+
 def test_fit_converges_to_fp64_optimum(tb, oracle):
     """From the same perturbed start, the batched FP32 fitter and the FP64
     oracle fitter reach the same optimum within 1e-3 sigma."""
@@ -265,8 +290,9 @@ def test_c5_blobs_reach_the_fp64_optimum(tb, oracle):
     from the batched result; sigma from its FP64 Fisher matrix.  A blob
     whose optimum puts an index on a range edge (the mixture is a separate
     fit on each side, so the model jumps there and neither fitter has a
-    stationary point to converge to) ends at its iteration limit and is
-    held to 0.1 sigma.  The FP64 fitter's normal equations are first
+    stationary point to converge to), or along whose flattest direction the
+    FP64 fitter itself does not converge within 100 iterations from the
+    batched result, is held to 0.1 sigma.  The FP64 fitter's normal equations are first
     checked against the oracle's central differences on a small blob."""
     import torch
     from tractor_b200 import fit, plain
@@ -301,8 +327,10 @@ def test_c5_blobs_reach_the_fp64_optimum(tb, oracle):
     res = plain.optimum_distance(w, data, inv, f.result(), st['status'],
                                  np.flatnonzero(st['status'] != 2), dev)
     assert len(res) >= 110, len(res)
-    inner = sorted([r for r in res if not r[3]], reverse=True)
-    edge = sorted([r for r in res if r[3]], reverse=True)
-    assert len(inner) >= 110 and len(edge) <= 3, (len(inner), edge)
+    # blobs with a well-defined optimum: no index on a range edge, and the
+    # FP64 fitter converges from the batched result
+    inner = sorted([r for r in res if not r[3] and r[4]], reverse=True)
+    other = sorted([r for r in res if r[3] or not r[4]], reverse=True)
+    assert len(inner) >= 110 and len(other) <= 5, (len(inner), other)
     assert inner[0][0] < 1e-3, inner[:5]
-    assert not edge or edge[0][0] < 0.1, edge
+    assert not other or other[0][0] < 0.1, other

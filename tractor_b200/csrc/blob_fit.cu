@@ -929,7 +929,7 @@ __device__ __forceinline__ double ref_model(const RefSrc& R, const FitC64* cs, i
         const double dx = px - c.mx, dy = py - c.my;
         const double ux = c.i00 * dx + c.i01 * dy, uy = c.i01 * dx + c.i11 * dy;
         const double e = -0.5 * (dx * ux + dy * uy);
-        if (e >= -50.0) val += c.s * exp(e);
+        if (e >= -50.0) val += c.s * tb::exp_taylor(fmin(e, 0.0));
     }
     return R.counts * val;
 }
@@ -951,7 +951,7 @@ __device__ __forceinline__ double ref_cols(const RefSrc& R, const FitC64* cs, in
         const double ux = c.i00 * dx + c.i01 * dy, uy = c.i01 * dx + c.i11 * dy;
         const double e = -0.5 * (dx * ux + dy * uy);
         if (e < -50.0) continue;
-        const double E = exp(e);
+        const double E = tb::exp_taylor(fmin(e, 0.0));
         const double val = c.s * E;
         S0 += val;
         Sx = fma(val, ux, Sx);
@@ -980,52 +980,6 @@ __device__ __forceinline__ double ref_cols(const RefSrc& R, const FitC64* cs, in
         J[3 + j] = cn * 0.5 * (R.dM[j][0] * Axx + 2.0 * R.dM[j][1] * Axy + R.dM[j][2] * Ayy - At[j]);
     J[6] = cn * (0.5 * (R.M[0] * Dxx + 2.0 * R.M[1] * Dxy + R.M[2] * Dyy - Dt) + Sn);
     return cn * S0;
-}
-
-// Source R's seven derivative columns at (px, py) from the FP32 component
-// tables (FP32 exp and moments; for A^T r, whose column errors multiply
-// residuals that are noise at the optimum and average out).
-__device__ __forceinline__ void ref_cols32(const RefSrc& R, const FitC* cs, int px, int py,
-                                           double (&J)[7]) {
-#pragma unroll
-    for (int j = 0; j < 7; j++) J[j] = 0.0;
-    if (!(px >= R.x0 && px < R.x1 && py >= R.y0 && py < R.y1)) return;
-    float S0 = 0, Sx = 0, Sy = 0, Axx = 0, Axy = 0, Ayy = 0;
-    float At[3] = {0, 0, 0};
-    float Dxx = 0, Dxy = 0, Dyy = 0, Dt = 0, Sn = 0;
-    for (int k = 0; k < R.K; k++) {
-        const FitC& c = cs[k];
-        const float dx = (float)(px - c.mx), dy = (float)(py - c.my);
-        const float e = fmaf(dy, fmaf(c.qyy, dy, c.qxy * dx), c.qxx * dx * dx);
-        if (e < c.fl) continue;
-        const float E = tb::ex2(e);
-        const float val = c.s * E;
-        const float ux = fmaf(c.ixx, dx, c.ixy * dy), uy = fmaf(c.ixy, dx, c.iyy * dy);
-        S0 += val;
-        Sx = fmaf(val, ux, Sx);
-        Sy = fmaf(val, uy, Sy);
-        const float vv = val * c.v;
-        Axx = fmaf(vv * ux, ux, Axx);
-        Axy = fmaf(vv * ux, uy, Axy);
-        Ayy = fmaf(vv * uy, uy, Ayy);
-        At[0] = fmaf(vv, c.t[0], At[0]);
-        At[1] = fmaf(vv, c.t[1], At[1]);
-        At[2] = fmaf(vv, c.t[2], At[2]);
-        const float vd = val * c.dv;
-        Dxx = fmaf(vd * ux, ux, Dxx);
-        Dxy = fmaf(vd * ux, uy, Dxy);
-        Dyy = fmaf(vd * uy, uy, Dyy);
-        Dt = fmaf(vd, c.t[3], Dt);
-        Sn = fmaf(c.sn, E, Sn);
-    }
-    const double cn = R.counts;
-    J[0] = cn * Sx;
-    J[1] = cn * Sy;
-    J[2] = S0;
-#pragma unroll
-    for (int j = 0; j < 3; j++)
-        J[3 + j] = cn * 0.5 * (R.dM[j][0] * Axx + 2.0 * R.dM[j][1] * Axy + R.dM[j][2] * Ayy - At[j]);
-    J[6] = cn * (0.5 * (R.M[0] * Dxx + 2.0 * R.M[1] * Dxy + R.M[2] * Dyy - Dt) + Sn);
 }
 
 // A source's own block: REFINE, its 28 A^T A products (upper triangle) and
@@ -1067,27 +1021,28 @@ __device__ __forceinline__ void ref_emit_pair(RefSmem& sm, int& nc, double* H, d
         });
 }
 
-__global__ void __launch_bounds__(kRefThreads, 2)
+// CTAs per SM the refinement kernel is compiled for (2: 128 registers)
+#ifndef TB_REFINE_MINB
+#define TB_REFINE_MINB 2
+#endif
+__global__ void __launch_bounds__(kRefThreads, TB_REFINE_MINB)
 fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restrict__ order,
                   int n_units, const tb_fit_blob* __restrict__ blobs,
                   const tb_fit_source* __restrict__ srcs, const SrcTab* __restrict__ tab,
-                  const FitC64* __restrict__ gcomps, const FitC* __restrict__ gcomps32,
-                  const float* __restrict__ data,
+                  const FitC64* __restrict__ gcomps, const float* __restrict__ data,
                   const float* __restrict__ inverr, double* __restrict__ hbuf,
                   double* __restrict__ gbuf, double* __restrict__ chi2_out,
                   const tb_fit_state* __restrict__ state, int n_bands,
                   const int32_t* __restrict__ tiles, int32_t* counter, tb_status* st, int mode,
                   float* __restrict__ model_out, const double* __restrict__ chi2_const) {
-    // mode TB_FIT_REFINE: A^T A (hbuf != NULL), A^T r and chi^2 of the
-    // running blobs, r = (data - model) inverr; without hbuf the columns of
-    // A^T r come from the FP32 tables (the model stays FP64); TB_FIT_MODEL:
-    // the model into model_out (every blob); TB_FIT_VJP: the columns
-    // contracted with data = an upstream gradient, unweighted
+    // mode TB_FIT_REFINE: A^T A, A^T r and chi^2 of the running blobs, r =
+    // (data - model) inverr; TB_FIT_MODEL: the model into model_out (every
+    // blob); TB_FIT_VJP: the columns contracted with data = an upstream
+    // gradient, unweighted
     __shared__ RefSmem sm;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const bool refine = mode == TB_FIT_REFINE && hbuf != nullptr;
-    const bool grad_only = mode == TB_FIT_REFINE && hbuf == nullptr;
+    const bool refine = mode == TB_FIT_REFINE;
     for (;;) {
         const int64_t oi = tb::next_unit(counter, &sm.slot);
         if (oi >= n_units) break;
@@ -1095,7 +1050,7 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
         if (ui < 0 || ui >= n_units) continue;
         const tb_fit_unit& u = units[ui];
         const tb_fit_blob b = blobs[u.blob];
-        if (mode == TB_FIT_REFINE && state[u.blob].status != 0) continue;   // running blobs
+        if (refine && state[u.blob].status != 0) continue;   // running blobs
         const int P = b.P;
         const int nsrc = b.n_src;
         double* g = gbuf ? gbuf + b.g_off + (int64_t)u.slice * P : nullptr;
@@ -1144,7 +1099,6 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
             continue;
         }
         const FitC64* band_comps = gcomps + ((int64_t)b.src0 * n_bands + u.band) * kCompStride;
-        const FitC* band_comps32 = gcomps32 + ((int64_t)b.src0 * n_bands + u.band) * kCompStride;
         const int64_t cstride = (int64_t)n_bands * kCompStride;
         const int n_t = u.t1 - u.t0;
         const int32_t* tl = tiles + b.tile_off + u.t0;
@@ -1179,24 +1133,7 @@ fit_refine_kernel(const tb_fit_unit* __restrict__ units, const int32_t* __restri
                 if (in) model_out[pix] = (float)m;
                 continue;
             }
-            if (grad_only) {
-                // the FP64 model, then each source's FP32 columns times w r
-                double m = 0.0;
-                for (unsigned rm = reach; rm; rm &= rm - 1) {
-                    const int sI = __ffs(rm) - 1;
-                    m += ref_model(sm.us[sI], band_comps + sI * cstride, px, py);
-                }
-                const double r = (d - m) * w;
-                chi2 += r * r;
-                for (unsigned ra = reach; ra; ra &= ra - 1) {
-                    const int sA = __ffs(ra) - 1;
-                    double Ja[7];
-                    ref_cols32(sm.us[sA], band_comps32 + sA * cstride, px, py, Ja);
-#pragma unroll
-                    for (int j = 0; j < 7; j++) Ja[j] *= w;
-                    ref_emit_own(sm, nc, H, g, Ja, r, sA, sm.us[sA], u.band, P, false);
-                }
-            } else if (nreach <= 2) {
+            if (nreach <= 2) {
                 // one or two sources: their columns and the model in one evaluation
                 const int s0 = nreach > 0 ? __ffs(reach) - 1 : -1;
                 const int s1 = nreach > 1 ? __ffs(reach & (reach - 1)) - 1 : -1;
@@ -1278,9 +1215,9 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     __shared__ double y[TB_FIT_MAX_SRC * TB_FIT_NPAR];
     __shared__ double xs[TB_FIT_MAX_SRC * TB_FIT_NPAR];
     __shared__ double rdg[TB_FIT_MAX_SRC * TB_FIT_NPAR];
-    __shared__ double red[kStepThreads / 32];
+    __shared__ double red[kStepThreads / 32], red2[kStepThreads / 32];
     __shared__ int s_accept, s_active;
-    __shared__ double s_lambda, s_scale;
+    __shared__ double s_lambda, s_scale, s_pa, s_pb;
     const int bi = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     (void)n_bands;
@@ -1307,10 +1244,19 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
         const bool acc = isfinite(c2) && (first || c2 < S.chi2);
         int status = 0;
         if (acc) {
-            S.dlnp = first ? INFINITY : 0.5 * (S.chi2 - c2);
+            // damping from the gain ratio rho = actual / predicted (Nielsen's
+            // rule: lambda x max(1/3, 1 - (2 rho - 1)^3); x 0.3 without a
+            // prediction)
+            const double gain = first ? INFINITY : 0.5 * (S.chi2 - c2);
+            double fct = 0.3;
+            if (!first && S.pred > 0.0 && isfinite(S.pred)) {
+                const double t = 2.0 * (gain / S.pred) - 1.0;
+                fct = fmax(1.0 / 3.0, 1.0 - t * t * t);
+            }
+            S.dlnp = gain;
             S.chi2 = c2;
             S.accepted += 1;
-            S.lambda = fmax(S.lambda * 0.3, 1e-9);
+            S.lambda = fmax(S.lambda * fct, 1e-9);
         } else {
             S.lambda *= 10.0;
             S.rejected += 1;
@@ -1470,17 +1416,33 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
     // tol while the damping is moderate (optimize_loop stops on the gain of
     // the last step, dchisq; the prediction is immune to FP32 noise in chi^2).
     {
-        double pr = 0.0;
+        // a = x^T y0, b = x^T x: the gain predicted for the step is
+        // (a + lambda b) / 2, for the step scaled by s it is
+        // s a - s^2 (a - lambda b) / 2
+        double pa_ = 0.0, pb_ = 0.0;
         for (int i = tid; i < P; i += kStepThreads) {
             const double y0 = dsc[i] == 0.0 ? 0.0 : ga[i] / dsc[i];
-            pr += xs[i] * y0 + lam * xs[i] * xs[i];
+            pa_ += xs[i] * y0;
+            pb_ += xs[i] * xs[i];
         }
-        for (int o = 16; o > 0; o >>= 1) pr += __shfl_xor_sync(0xffffffffu, pr, o);
-        if (lane == 0) red[warp] = pr;
+        for (int o = 16; o > 0; o >>= 1) {
+            pa_ += __shfl_xor_sync(0xffffffffu, pa_, o);
+            pb_ += __shfl_xor_sync(0xffffffffu, pb_, o);
+        }
+        if (lane == 0) {
+            red[warp] = pa_;
+            red2[warp] = pb_;
+        }
         __syncthreads();
         if (tid == 0) {
-            double t = 0.0;
-            for (int w2 = 0; w2 < kStepThreads / 32; w2++) t += red[w2];
+            double ta = 0.0, tb2 = 0.0;
+            for (int w2 = 0; w2 < kStepThreads / 32; w2++) {
+                ta += red[w2];
+                tb2 += red2[w2];
+            }
+            s_pa = ta;
+            s_pb = tb2;
+            const double t = ta + lam * tb2;
             S.pred = 0.5 * t;
             s_active = !(0.5 * t < tol && lam <= 1.0);
             if (!s_active) S.status = 1;
@@ -1513,6 +1475,9 @@ fit_step_kernel(const tb_fit_blob* __restrict__ blobs, int n_blobs, int n_bands,
         double l = 1.0;
         for (int w2 = 0; w2 < kStepThreads / 32; w2++) l = fmin(l, red[w2]);
         s_scale = fmax(l, 0.0);
+        // the gain predicted for the trial as scaled (the next call's gain
+        // ratio divides by it)
+        S.pred = s_scale * s_pa - 0.5 * s_scale * s_scale * (s_pa - lam * s_pb);
     }
     __syncthreads();
     for (int i = tid; i < P; i += kStepThreads) {
@@ -1648,7 +1613,7 @@ extern "C" int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int
     if (n_units < 0 || n_src < 0 || n_bands < 1 || n_bands > TB_FIT_MAX_BANDS) return TB_ERR_ARG;
     if (n_units == 0) return TB_OK;
     if (!units || !order || !blobs || !srcs || !workspace || !data || !inverr || !tiles ||
-        !gbuf || !chi2_out || !state || !work_counter)
+        !hbuf || !gbuf || !chi2_out || !state || !work_counter)
         return TB_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return TB_ERR_LAUNCH;
@@ -1662,9 +1627,9 @@ extern "C" int tb_fit_refine(const tb_fit_unit* units, const int32_t* order, int
     const int grid = (int)(n_units < want ? n_units : want);
     void* ws = const_cast<void*>(workspace);
     fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
-        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands),
-        ws_comps(ws, n_src), data, inverr, hbuf, gbuf, chi2_out, state, n_bands, tiles,
-        work_counter, status, TB_FIT_REFINE, nullptr, chi2_const);
+        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands), data,
+        inverr, hbuf, gbuf, chi2_out, state, n_bands, tiles, work_counter, status, TB_FIT_REFINE,
+        nullptr, chi2_const);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
@@ -1692,9 +1657,9 @@ extern "C" int tb_fit_model_vjp(const tb_fit_unit* units, const int32_t* order, 
     const int grid = (int)(n_units < want ? n_units : want);
     void* ws = const_cast<void*>(workspace);
     fit_refine_kernel<<<grid, kRefThreads, 0, s>>>(
-        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands),
-        ws_comps(ws, n_src), grad, nullptr, nullptr, gbuf, nullptr, nullptr, n_bands, tiles,
-        work_counter, status, mode, model, nullptr);
+        units, order, n_units, blobs, srcs, ws_tab(ws), ws_comps64(ws, n_src, n_bands), grad,
+        nullptr, nullptr, gbuf, nullptr, nullptr, n_bands, tiles, work_counter, status, mode,
+        model, nullptr);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 

@@ -643,17 +643,19 @@ __device__ void taps_warp(double dx, bool deriv, float* f) {
     if (deriv) on = i >= (dx >= 0.0 ? 0 : 1) && i < (dx >= 0.0 ? 6 : 7);
     else on = i >= (dx > 0.0 ? 0 : 1) && i < (dx > 0.0 ? 6 : 7);
     if (on) {
-        const double p = TB_PI * (i - 3.0 + dx);
+        // sin / cos of pi t by sincospi (no argument reduction)
+        const double t = i - 3.0 + dx;
+        const double p = TB_PI * t;
         if (p == 0.0) {
             L = 1.0;
         } else {
-            const double sp = sin(p), s3 = sin(p / 3.0);
+            double sp, cp, s3, c3;
+            sincospi(t, &sp, &cp);
+            sincospi(t / 3.0, &s3, &c3);
             L = 3.0 * sp * s3 / (p * p);
-            if (deriv) {
-                const double cp = cos(p), c3 = cos(p / 3.0);
+            if (deriv)
                 D = TB_PI * 3.0 * (cp * s3 / (p * p) + sp * c3 / (3.0 * p * p) -
                                    2.0 * sp * s3 / (p * p * p));
-            }
         }
     }
     double S = L, Sd = D;
@@ -707,45 +709,19 @@ __device__ __forceinline__ void spectrum_any(const tb_fft_item& it, const float4
     else spectrum8(comp, it.K, vf, wf, acc);
 }
 
-// Per item of a chunk: the Lanczos-3 taps of the x and y shifts (or their
-// derivatives for DX / DY items) and their frequency responses Hy(w), w <
-// N, and Hx(v), v <= N/2, for the column and row kernels.
-constexpr int kHrespPerItem = 256 + 129;
-
-__global__ void __launch_bounds__(128)
-fourier_split_setup_kernel(const tb_fft_item* __restrict__ items, int i0, int n_items,
-                           const double* __restrict__ dcoef, float2* __restrict__ hresp) {
-    __shared__ float2 tw[256];
-    __shared__ float tx[8], ty[8];
-    const int li = blockIdx.x;
-    if (li >= n_items) return;
-    const tb_fft_item& it = items[i0 + li];
-    if (!item_ok(it, dcoef) || !split_eligible(it)) return;
-    const int N = it.sz;
-    const int warp = threadIdx.x >> 5;
-    if (warp == 0) taps_warp(it.mux, it.dmode == TB_FFT_DX, tx);
-    if (warp == 1) taps_warp(it.muy, it.dmode == TB_FFT_DY, ty);
-    switch (N) {
-        case 256: tb::build_twiddles<256>(tw); break;
-        case 128: tb::build_twiddles<128>(tw); break;
-        case 64: tb::build_twiddles<64>(tw); break;
-        default: tb::build_twiddles<32>(tw); break;
-    }
-    __syncthreads();
-    float2* h = hresp + (int64_t)li * kHrespPerItem;
-    for (int j = threadIdx.x; j < N + N / 2 + 1; j += blockDim.x) {
-        const bool isy = j < N;
-        const int fr = isy ? j : j - N;
-        const float* tp = isy ? ty : tx;
-        float2 r = make_float2(0.f, 0.f);
+// Frequency response of the 7 Lanczos-3 taps at frequency index fr of an
+// N-point transform: sum_k taps[k] exp(2 pi i fr (k - 3) / N), from the
+// twiddle table.
+__device__ __forceinline__ float2 taps_response(const float* taps, const float2* tw, int fr,
+                                                int N) {
+    float2 r = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int k = 0; k < 7; k++) {
-            const float2 w = tw[(fr * (k - 3)) & (N - 1)];
-            r.x = fmaf(tp[k], w.x, r.x);
-            r.y = fmaf(tp[k], w.y, r.y);
-        }
-        h[isy ? fr : 256 + fr] = r;
+    for (int k = 0; k < 7; k++) {
+        const float2 w = tw[(fr * (k - 3)) & (N - 1)];
+        r.x = fmaf(taps[k], w.x, r.x);
+        r.y = fmaf(taps[k], w.y, r.y);
     }
+    return r;
 }
 
 template <int N>
@@ -797,8 +773,7 @@ fourier_split_col_kernel(const tb_fft_item* __restrict__ items, int i0, int n_it
                          const double* __restrict__ amp, const double* __restrict__ var,
                          const double* __restrict__ dcoef, const float* __restrict__ psf_spec,
                          float* __restrict__ out, SplitWs* ws, int32_t* fb_list,
-                         float2* __restrict__ s1_all, const float2* __restrict__ hresp,
-                         tb_status* st) {
+                         float2* __restrict__ s1_all, tb_status* st) {
     __shared__ SplitColShared sh;
     if (threadIdx.x == 0) sh.cur_n = 0;
     const int64_t n_units = (int64_t)n_items * kColUnits;
@@ -835,6 +810,7 @@ fourier_split_col_kernel(const tb_fft_item* __restrict__ items, int i0, int n_it
         }
         // stage: components, y taps and their frequency response, twiddles
         stage_components(it, amp, var, dcoef, sh.comp, sh.dcomp);
+        if (threadIdx.x < 32) taps_warp(it.muy, it.dmode == TB_FFT_DY, sh.taps);
         if (sh.cur_n != N) {
             __syncthreads();
             switch (N) {
@@ -843,12 +819,11 @@ fourier_split_col_kernel(const tb_fft_item* __restrict__ items, int i0, int n_it
                 case 64: tb::build_twiddles<64>(sh.tw); break;
                 default: tb::build_twiddles<32>(sh.tw); break;
             }
-            __syncthreads();
             if (threadIdx.x == 0) sh.cur_n = N;
         }
-        // the y taps' frequency response, written by the setup kernel
+        __syncthreads();
         for (int j = threadIdx.x; j < N; j += kSplitThreads)
-            sh.hy[j] = hresp[(int64_t)li * kHrespPerItem + j];
+            sh.hy[j] = taps_response(sh.taps, sh.tw, j, N);
         __syncthreads();
         float2* s1 = s1_all + (int64_t)li * kS1PerItem;
         const float* spec = psf_spec + it.spec_off;
@@ -887,10 +862,21 @@ __device__ void split_row_unit(const tb_fft_item& it, int rb, const float2* __re
     const int r0 = rb * kRowBlock;
     const int nrows = min(kRowBlock, nr - r0);
     // this unit's rows of every rfft column, transposed into shared memory
-    for (int e = threadIdx.x; e < NH * kRowBlock; e += kSplitThreads) {
+    // by asynchronous 8-byte copies (all of a thread's copies in flight at
+    // once, no registers held); rows >= nrows are not read below
+    constexpr int kLd = (NH * kRowBlock + kSplitThreads - 1) / kSplitThreads;
+#pragma unroll
+    for (int q = 0; q < kLd; q++) {
+        const int e = threadIdx.x + q * kSplitThreads;
         const int c = e / kRowBlock, r = e % kRowBlock;
-        if (r < nrows) sh.rows[r * 129 + c] = s1[(int64_t)c * nr + r0 + r];
+        if (e < NH * kRowBlock && r < nrows) {
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sh.rows[r * 129 + c]);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst),
+                         "l"(s1 + (int64_t)c * nr + r0 + r) : "memory");
+        }
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
     const float osc = it.scale / (float)(N * N);
     float* O = out + it.out_off;
@@ -931,7 +917,7 @@ __device__ void split_row_unit(const tb_fft_item& it, int rb, const float2* __re
 __global__ void __launch_bounds__(kSplitThreads, TB_SPLIT_ROW_MINB)
 fourier_split_row_kernel(const tb_fft_item* __restrict__ items, int i0, int n_items,
                          const double* __restrict__ dcoef, float* __restrict__ out, SplitWs* ws,
-                         const float2* __restrict__ s1_all, const float2* __restrict__ hresp) {
+                         const float2* __restrict__ s1_all) {
     __shared__ SplitRowShared sh;
     if (threadIdx.x == 0) sh.cur_n = 0;
     const int64_t n_units = (int64_t)n_items * kRowUnits;
@@ -945,6 +931,7 @@ fourier_split_row_kernel(const tb_fft_item* __restrict__ items, int i0, int n_it
         const int gr0 = max(0, -it.sy), gr1 = min(N, it.mh - it.sy);
         const int gc0 = max(0, -it.sx), gc1 = min(N, it.mw - it.sx);
         if (gr0 >= gr1 || gc0 >= gc1 || rb * kRowBlock >= gr1 - gr0) continue;
+        if (threadIdx.x < 32) taps_warp(it.mux, it.dmode == TB_FFT_DX, sh.taps);
         if (sh.cur_n != N) {
             __syncthreads();
             switch (N) {
@@ -953,12 +940,12 @@ fourier_split_row_kernel(const tb_fft_item* __restrict__ items, int i0, int n_it
                 case 64: tb::build_twiddles<64>(sh.tw); break;
                 default: tb::build_twiddles<32>(sh.tw); break;
             }
-            __syncthreads();
             if (threadIdx.x == 0) sh.cur_n = N;
         }
-        // the x taps' frequency response, written by the setup kernel
+        __syncthreads();
+        // the x taps' frequency response
         for (int f = threadIdx.x; f <= N / 2; f += kSplitThreads)
-            sh.hx[f] = hresp[(int64_t)li * kHrespPerItem + 256 + f];
+            sh.hx[f] = taps_response(sh.taps, sh.tw, f, N);
         __syncthreads();
         const float2* s1 = s1_all + (int64_t)li * kS1PerItem;
         switch (N) {
@@ -1039,7 +1026,7 @@ extern "C" int tb_fourier_workspace(int32_t n_items, int64_t* bytes) {
     if (n_items < 0 || !bytes) return TB_ERR_ARG;
     const int64_t chunk = n_items < kSplitChunk ? n_items : kSplitChunk;
     *bytes = (int64_t)sizeof(SplitWs) + split_list_bytes(n_items) +
-             chunk * (kS1PerItem + kHrespPerItem) * (int64_t)sizeof(float2);
+             chunk * kS1PerItem * (int64_t)sizeof(float2);
     return TB_OK;
 }
 
@@ -1061,8 +1048,6 @@ extern "C" int tb_fourier_render_split(const tb_fft_item* items, int32_t n_items
     int32_t* fb_list = reinterpret_cast<int32_t*>(static_cast<char*>(workspace) + sizeof(SplitWs));
     float2* s1 = reinterpret_cast<float2*>(static_cast<char*>(workspace) + sizeof(SplitWs) +
                                            split_list_bytes(n_items));
-    const int64_t chunk = n_items < kSplitChunk ? n_items : kSplitChunk;
-    float2* hresp = s1 + chunk * kS1PerItem;
     if (cudaMemsetAsync(ws, 0, sizeof(SplitWs), s) != cudaSuccess) return TB_ERR_LAUNCH;
     if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
         return TB_ERR_LAUNCH;
@@ -1073,12 +1058,11 @@ extern "C" int tb_fourier_render_split(const tb_fft_item* items, int32_t n_items
         if (i0 > 0 && cudaMemsetAsync(ws, 0, 2 * sizeof(int32_t), s) != cudaSuccess)
             return TB_ERR_LAUNCH;
         const int64_t cu = (int64_t)n * kColUnits, ru = (int64_t)n * kRowUnits;
-        fourier_split_setup_kernel<<<n, 128, 0, s>>>(items, i0, n, comp_dcoef, hresp);
         fourier_split_col_kernel<<<(int)(cu < gcol ? cu : gcol), kSplitThreads, 0, s>>>(
-            items, i0, n, comp_amp, comp_var, comp_dcoef, psf_spec, out, ws, fb_list, s1, hresp,
+            items, i0, n, comp_amp, comp_var, comp_dcoef, psf_spec, out, ws, fb_list, s1,
             status);
         fourier_split_row_kernel<<<(int)(ru < grow ? ru : grow), kSplitThreads, 0, s>>>(
-            items, i0, n, comp_dcoef, out, ws, s1, hresp);
+            items, i0, n, comp_dcoef, out, ws, s1);
     }
     // items outside the split path (Lanczos-3 reaching the box edge, TB_FFT_DOT)
     const bool deriv = comp_dcoef != nullptr || dots != nullptr;

@@ -168,29 +168,28 @@ class BlobFitter(object):
                                    self.misc.data_ptr(), self.misc.data_ptr() + 16,
                                    _lib.stream_ptr()), 'tb_fit_pass')
 
-    def _refine_pass(self, hessian=True):
+    def _refine_pass(self):
         """A^T A, A^T r and chi^2 of the running blobs in FP64
-        (tb_fit_refine), into the slices the FP32 pass writes; without
-        `hessian`, A^T r and chi^2 only (A^T A stays the last one)."""
+        (tb_fit_refine), into the slices the FP32 pass writes."""
         lib = _lib.load()
         _lib.check(lib.tb_fit_refine(self.d_pass_units.data_ptr(), self.d_order.data_ptr(),
                                      len(self.pass_units_np), self.d_blobs.data_ptr(),
                                      self.d_sources.data_ptr(), self.n_src,
                                      self.workspace.data_ptr(), self.data.data_ptr(),
                                      self.inverr.data_ptr(), self.d_tiles.data_ptr(),
-                                     self.hbuf.data_ptr() if hessian else None,
-                                     self.gbuf.data_ptr(), self.chi2_part.data_ptr(),
+                                     self.hbuf.data_ptr(), self.gbuf.data_ptr(),
+                                     self.chi2_part.data_ptr(),
                                      self.chi2_const.data_ptr(), self.state.data_ptr(),
                                      self.n_bands, self.misc.data_ptr(),
                                      self.misc.data_ptr() + 16, _lib.stream_ptr()),
                    'tb_fit_refine')
 
-    def _iteration(self, tol, max_iter, precise=False, hessian=True):
+    def _iteration(self, tol, max_iter, precise=False):
         lib = _lib.load()
         s = _lib.stream_ptr()
         self._prep()
         if precise:
-            self._refine_pass(hessian)
+            self._refine_pass()
         else:
             self._pass(0)
         _lib.check(lib.tb_fit_step(self.d_blobs.data_ptr(), self.n_blobs, self.n_bands,
@@ -219,8 +218,7 @@ class BlobFitter(object):
         return int((st[:, -1] == 0).sum().item())
 
     def fit(self, tol=1e-3, max_iter=200, check_every=4, graph=True, params0=None,
-            lambda0=1e-3, refine=True, refine_tol=1e-9, refine_iter=25, handoff=0.005,
-            refresh=4):
+            lambda0=1e-3, refine=True, refine_tol=1e-9, refine_iter=40, handoff=0.005):
         """Runs FP32 iterations until every blob stops (or max_iter); then,
         with `refine`, continues every blob from where it stopped with the
         normal equations in FP64 (tb_fit_refine in place of the pass) until
@@ -256,9 +254,7 @@ class BlobFitter(object):
             self.reset(None, 1e-9)
             self.iterations = n
             for it in range(int(refine_iter)):
-                # A^T A in FP64 at the start and every `refresh` iterations
-                self._iteration(refine_tol, refine_iter, precise=True,
-                                hessian=it % int(refresh) == 0)
+                self._iteration(refine_tol, refine_iter, precise=True)
                 self.iterations += 1
                 if it % 2 == 1 and self.running() == 0:
                     break

@@ -259,12 +259,18 @@ class BlobFitFP64(object):
                     lim = min(lim, (6.3 - theta[s, 8]) / step[s, 8])
                 if nn[s] < 0.29 and step[s, 8] < 0:
                     lim = min(lim, (0.29 - theta[s, 8]) / step[s, 8])
-            trial = theta + max(lim, 0.) * step
+            sc = max(lim, 0.)
+            trial = theta + sc * step
             trial[:, 8] = np.clip(trial[:, 8], 0.29, 6.3)
             H2, g2, c22 = normal_eq(trial)
             if c22 < c2:
+                # damping from the gain ratio (Nielsen's rule), the prediction
+                # for the step as scaled
+                a, b = float(xs @ y0), float(xs @ xs)
+                pred_s = sc * a - 0.5 * sc * sc * (a - lam * b)
+                t = 2. * (0.5 * (c2 - c22) / pred_s) - 1. if pred_s > 0 else -1.
                 theta, H, g, c2 = trial, H2, g2, c22
-                lam = max(lam * 0.3, 1e-9)
+                lam = max(lam * max(1. / 3., 1. - t ** 3), 1e-9)
             else:
                 lam *= 10.
                 if lam > 1e12:
@@ -281,7 +287,7 @@ def sersic_edges():
     return np.array(sorted({r['lo'] for r in R[1:]} | {1.0}))
 
 
-def optimum_distance(w, data, inv, fitted, status, blobs, device, tol=1e-10, max_iter=40,
+def optimum_distance(w, data, inv, fitted, status, blobs, device, tol=1e-10, max_iter=100,
                      edge=1e-3):
     """Distance of batched-fit results from the FP64 optimum, per blob of
     `blobs` (a blob workload of tractor_b200.fit): the FP64 fitter continued
@@ -289,8 +295,9 @@ def optimum_distance(w, data, inv, fitted, status, blobs, device, tol=1e-10, max
     max_i |fitted_i - opt_i| / sigma_i with sigma from its FP64 Fisher
     matrix (a Sersic index held at a bound, and directions the Fisher
     matrix leaves unconstrained, count as sigma = inf).  Returns one record
-    per blob: (sigma, blob, status, on_edge), on_edge when a Sersic index
-    (batched or FP64) lies within `edge` of sersic_edges()."""
+    per blob: (sigma, blob, status, on_edge, converged), on_edge when a
+    Sersic index (batched or FP64) lies within `edge` of sersic_edges(),
+    converged when the FP64 fitter reached `tol` within `max_iter`."""
     from . import fit as _fit
     po = _fit.pix_offsets(w['sides'], 3)
     hd, hi = data.cpu().numpy(), inv.cpu().numpy()
@@ -304,7 +311,7 @@ def optimum_distance(w, data, inv, fitted, status, blobs, device, tol=1e-10, max
         rects = [tuple(int(v) for v in (r['x0'], r['y0'], r['w'], r['h']))
                  for r in w['sources'][s0:s1]]
         pf = BlobFitFP64(d3, i3, w['psf'][b], rects, device)
-        opt, _ = pf.fit(fitted[s0:s1], tol=tol, max_iter=max_iter)
+        opt, nit = pf.fit(fitted[s0:s1], tol=tol, max_iter=max_iter)
         Hf = pf.fisher(opt)
         o = opt.ravel()
         n_idx = np.arange(8, o.size, 9)
@@ -318,5 +325,5 @@ def optimum_distance(w, data, inv, fitted, status, blobs, device, tol=1e-10, max
         err = float(np.max(np.abs(np.asarray(fitted[s0:s1]).ravel() - o) / sig))
         nn = np.concatenate([np.asarray(fitted[s0:s1])[:, 8], opt[:, 8]])
         on_edge = bool(np.min(np.abs(nn[:, None] - edges[None])) < edge)
-        out.append((err, int(b), int(status[b]), on_edge))
+        out.append((err, int(b), int(status[b]), on_edge, nit < max_iter))
     return out
