@@ -198,9 +198,11 @@ def ptr(t):
 
 
 def stream_ptr(stream=None):
+    """cudaStream_t of `stream`, or of the current device's current stream
+    (read without building a torch Stream object: this runs on every launch)."""
     import torch
     if stream is None:
-        stream = torch.cuda.current_stream()
+        return torch._C._cuda_getCurrentRawStream(torch._C._cuda_getDevice())
     return stream.cuda_stream
 
 

@@ -138,7 +138,12 @@ constexpr int kChunkRows = 128;     // rows per FP32 accumulation chunk
 constexpr uint64_t kWaitNs = 1000000000ull;   // 1 s: far above any real MMA batch
 __host__ __device__ constexpr int elems(int qm) { return 32 * qm; }        // per raw stage
 __host__ __device__ constexpr int qpt(int qm) { return elems(qm) / 4 / kThreads; }   // quads
-__host__ __device__ constexpr int raw_stages(int qm) { return qm == 128 ? 4 : 2; }
+// raw stages in flight (QM = 128: the copies of 3 stages ahead of the one
+// being converted)
+#ifndef TB_NE_RAW128
+#define TB_NE_RAW128 4
+#endif
+__host__ __device__ constexpr int raw_stages(int qm) { return qm == 128 ? TB_NE_RAW128 : 2; }
 __host__ __device__ constexpr int kc_of(int qm, int q8) {
     int kc = 128;
     while (kc > 32 && kc * q8 > elems(qm)) kc >>= 1;
@@ -604,7 +609,10 @@ constexpr int kConv = 256;                 // converter threads
 constexpr int kThreads = kConv + 32;       // + the MMA warp
 constexpr int kKc = 32;                    // pixel rows per stage
 constexpr int kChunkSt = 4;                // stages per 128-row accumulation chunk
-constexpr int kRaw = 3;                    // raw stages in flight
+#ifndef TB_NE64_RAW
+#define TB_NE64_RAW 3
+#endif
+constexpr int kRaw = TB_NE64_RAW;          // raw stages in flight
 constexpr int kKq = kKc / 4;               // quads per operand row and stage
 constexpr int kRowStep = kConv / kKq;      // operand rows between a thread's quads
 constexpr int kQpt = 64 / kRowStep;        // quads per thread and stage (64 x 32 / 4 / 256)

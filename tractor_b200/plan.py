@@ -86,17 +86,24 @@ class RenderPlan(object):
             imgs = torch.from_numpy(np.stack([s for s, _, _ in lst])).to(render.device())
             shifts = np.array([[dx, dy] for _, dx, dy in lst])
             lz[key] = render.lanczos_shift(imgs, shifts)
+        stream = None
         for kind, t in outs:
-            host = t.cpu().numpy()     # the status word rides at the end
-            st = torch.from_numpy(host[-4:].view(np.uint8).copy())
+            # the status word rides at the end
+            if t.device.type == 'cuda':
+                if stream is None:
+                    stream = torch.cuda.current_stream()
+                host = render.to_host(t, np.float32, stream)
+            else:
+                host = t.numpy().copy()
+            st = host[-4:]
             if kind == 'mog':
-                render.check_status(st, 'tb_mog_render')
+                render.check_status_host(st, 'tb_mog_render')
                 if self.mog.extents is not None:
                     render.check_status(self.mog.ring_status, 'tb_approx3_region')
                     self._ring_host = self.mog.extents.cpu().numpy().reshape(-1, 4)
                 self._mog_host = host
             else:
-                render.check_status(st, 'tb_fourier_render')
+                render.check_status_host(st, 'tb_fourier_render')
                 self._fft_host = host
         for key, t in lz.items():
             self._lz_host[key] = t.cpu().numpy()

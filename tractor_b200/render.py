@@ -8,6 +8,8 @@ where the reference API returns numpy arrays.
 """
 import ctypes
 
+import threading
+
 import numpy as np
 import torch
 
@@ -87,6 +89,46 @@ class _Packer(object):
         ev.record()
         entry[1] = ev
         return out
+
+
+class _PinnedOut(threading.local):
+    """Pinned host staging for device-to-host copies of finished renders
+    (one reused buffer per thread): the copy lands in pinned memory
+    (pageable destinations take a slower, staged path), the stream is
+    synchronised and the bytes are copied out into a new array."""
+
+    buf = None
+
+    def to_host(self, t, dtype, stream):
+        n = t.numel() * t.element_size()
+        if self.buf is None or self.buf.numel() < n:
+            size = 1 << max(16, int(np.ceil(np.log2(max(n, 1)))))
+            self.buf = torch.empty(size, dtype=torch.uint8).pin_memory()
+        host = self.buf[:n]
+        host.copy_(t.reshape(-1).view(torch.uint8), non_blocking=True)
+        stream.synchronize()
+        return host.numpy().view(dtype).copy()
+
+
+_pinned_out = _PinnedOut()
+
+
+def to_host(t, dtype, stream=None):
+    """numpy copy of device tensor `t` (contiguous) as `dtype`, after the
+    stream (default: the current one) has finished writing it."""
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return _pinned_out.to_host(t, dtype, stream)
+
+
+def check_status_host(raw, what):
+    """check_status of a status word already on the host (16 bytes)."""
+    st = np.ascontiguousarray(raw).view(np.uint8).view(_lib.STATUS)[0]
+    if st['code'] != 0:
+        kind = {1: 'non-finite value', 2: 'invalid item', 3: 'not positive definite'}
+        raise RuntimeError('%s: %s at item %d (detail %d, %d reports)' %
+                           (what, kind.get(int(st['code']), 'error'), st['item'], st['detail'],
+                            st['count']))
 
 
 def check_status(status_tensor, what):
