@@ -28,7 +28,7 @@
 // ModelMask (tractor/galaxy.py:336-519) for a non-hybrid PixelizedPSF.
 // Windows taller than the row buffer are processed in row chunks (the column
 // pass is repeated per chunk).
-#include "fft_warp.cuh"
+#include "fft16.cuh"
 
 namespace {
 
@@ -36,6 +36,10 @@ constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxK = 128;
 constexpr int kXbufPerWarp = 272;                  // float2, any N in [32, 256]
+// the persistent kernel's exchange buffers: two half-warp radix-16
+// transforms per warp at N = 256, one radix-8/8/4 transform below
+constexpr int kXbufPersist = 2 * tb::kR16Xbuf;
+static_assert(kXbufPersist >= kXbufPerWarp, "exchange buffer covers every N");
 constexpr int kRmax256 = 134;                      // kept rows at sz = 256
 
 __host__ __device__ constexpr int s1_bytes(int N, int rmax) { return rmax * (N / 2 + 1) * 8; }
@@ -46,7 +50,7 @@ constexpr int kSmemBytes = 256 * 8               /* twiddles */
                            + 2 * kMaxK * 16       /* components, derivative prefactors */
                            + 16 * 4               /* taps */
                            + (129 + 256) * 8      /* Hx, Hy */
-                           + kWarps * kXbufPerWarp * 8 + kS1Bytes;
+                           + kWarps * kXbufPersist * 8 + kS1Bytes + 2 * 256 * 4;
 
 struct Shared {
     float2* tw;
@@ -57,60 +61,61 @@ struct Shared {
     float2* hy;     // frequency response of the y taps, row index j = 0..N-1
     float2* xbuf;
     float2* s1;
+    float* gsp;     // N = 256: mixture spectrum of the DC and Nyquist columns, all rows
 };
 
-__device__ void taps3(double dx, float* f) {
-    double t[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (dx == 0.0) {
-        t[3] = 1.0;
-    } else {
-        const int lo = dx > 0.0 ? 0 : 1, hi = dx > 0.0 ? 6 : 7;
-        double s = 0.0;
-        for (int i = lo; i < hi; i++) {
-            const double p = TB_PI * (i - 3.0 + dx);
-            t[i] = 3.0 * sin(p) * sin(p / 3.0) / (p * p);
-            s += t[i];
-        }
-        for (int i = lo; i < hi; i++) t[i] /= s;
+// The 7 Lanczos-3 taps of a sub-pixel shift dx (lanczos_shift_3f's kernel
+// L(p) = 3 sin(p) sin(p/3) / p^2, p = pi (i - 3 + dx), normalised to unit
+// sum; dx = 0 is the identity) or, with `deriv`, their derivative d/d dx by
+// the quotient rule (at dx = 0 the limit from dx > 0: support 0..5).  One
+// warp: lane i < 7 evaluates tap i, the sums over the taps by shuffles.
+// Called by all 32 lanes.
+__device__ void taps_warp(double dx, bool deriv, float* f) {
+    const int i = threadIdx.x & 31;
+    double L = 0.0, D = 0.0;
+    bool on;
+    if (!deriv && dx == 0.0) {
+        if (i < 7) f[i] = i == 3 ? 1.f : 0.f;
+        return;
     }
-    for (int i = 0; i < 7; i++) f[i] = (float)t[i];
-}
-
-// d taps / d dx of the normalised Lanczos-3 taps above (quotient rule on
-// L(p) = 3 sin(p) sin(p/3) / p^2, p = pi (i - 3 + dx)); at dx = 0 the limit
-// from dx > 0 (the taps' support 0..5; the |i - 3| = 3 terms vanish).
-__device__ void taps3_deriv(double dx, float* f) {
-    double L[7] = {0, 0, 0, 0, 0, 0, 0}, D[7] = {0, 0, 0, 0, 0, 0, 0};
-    const int lo = dx >= 0.0 ? 0 : 1, hi = dx >= 0.0 ? 6 : 7;
-    double S = 0.0, Sd = 0.0;
-    for (int i = lo; i < hi; i++) {
-        const double p = TB_PI * (i - 3.0 + dx);
+    if (deriv) on = i >= (dx >= 0.0 ? 0 : 1) && i < (dx >= 0.0 ? 6 : 7);
+    else on = i >= (dx > 0.0 ? 0 : 1) && i < (dx > 0.0 ? 6 : 7);
+    if (on) {
+        // sin / cos of pi t by sincospi (no argument reduction)
+        const double t = i - 3.0 + dx;
+        const double p = TB_PI * t;
         if (p == 0.0) {
-            L[i] = 1.0;
-            D[i] = 0.0;
+            L = 1.0;
         } else {
-            const double sp = sin(p), s3 = sin(p / 3.0), cp = cos(p), c3 = cos(p / 3.0);
-            L[i] = 3.0 * sp * s3 / (p * p);
-            D[i] = TB_PI * 3.0 * (cp * s3 / (p * p) + sp * c3 / (3.0 * p * p) -
-                                  2.0 * sp * s3 / (p * p * p));
+            double sp, cp, s3, c3;
+            sincospi(t, &sp, &cp);
+            sincospi(t / 3.0, &s3, &c3);
+            L = 3.0 * sp * s3 / (p * p);
+            if (deriv)
+                D = TB_PI * 3.0 * (cp * s3 / (p * p) + sp * c3 / (3.0 * p * p) -
+                                   2.0 * sp * s3 / (p * p * p));
         }
-        S += L[i];
-        Sd += D[i];
     }
-    for (int i = 0; i < 7; i++) f[i] = (i >= lo && i < hi) ? (float)((D[i] - L[i] / S * Sd) / S) : 0.f;
+    double S = L, Sd = D;
+    for (int o = 16; o > 0; o >>= 1) {
+        S += __shfl_xor_sync(0xffffffffu, S, o);
+        Sd += __shfl_xor_sync(0xffffffffu, Sd, o);
+    }
+    if (i < 7) f[i] = on ? (float)(deriv ? (D - L / S * Sd) / S : L / S) : 0.f;
 }
 
-// Mixture spectrum at (v, w) for the 8 rows of one thread: acc[m] =
+// Mixture spectrum at (v, w) for the R rows of one thread: acc[m] =
 // sum_k amp_k exp2(ca v^2 + cb v w_m + cd w_m^2).
-__device__ __forceinline__ void spectrum8(const float4* comp, int K, float vf, const float* wf,
+template <int R>
+__device__ __forceinline__ void spectrum_rows(const float4* comp, int K, float vf, const float* wf,
                                           float* acc) {
 #pragma unroll
-    for (int m = 0; m < 8; m++) acc[m] = 0.f;
+    for (int m = 0; m < R; m++) acc[m] = 0.f;
     for (int k = 0; k < K; k++) {
         const float4 c = comp[k];
         const float al = c.y * vf * vf, be = c.z * vf;
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
+        for (int m = 0; m < R; m++) {
             const float e = fmaf(wf[m], fmaf(c.w, wf[m], be), al);
             acc[m] = fmaf(c.x, tb::ex2(e), acc[m]);
         }
@@ -120,17 +125,18 @@ __device__ __forceinline__ void spectrum8(const float4* comp, int K, float vf, c
 // Derivative spectrum: acc[m] = sum_k (da_k + ba_k v^2 + bb_k v w_m + bc_k w_m^2)
 // * amp-less exp2(...) -- d/dtheta [a exp(-2 pi^2 f^T C f)] for a parameter
 // theta that moves a and C.
-__device__ __forceinline__ void dspectrum8(const float4* comp, const float4* dcomp, int K,
+template <int R>
+__device__ __forceinline__ void dspectrum_rows(const float4* comp, const float4* dcomp, int K,
                                            float vf, const float* wf, float* acc) {
 #pragma unroll
-    for (int m = 0; m < 8; m++) acc[m] = 0.f;
+    for (int m = 0; m < R; m++) acc[m] = 0.f;
     for (int k = 0; k < K; k++) {
         const float4 c = comp[k];
         const float4 d = dcomp[k];
         const float al = c.y * vf * vf, be = c.z * vf;
         const float d0 = fmaf(d.y * vf, vf, d.x), d1 = d.z * vf;
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
+        for (int m = 0; m < R; m++) {
             const float e = fmaf(wf[m], fmaf(c.w, wf[m], be), al);
             const float pre = fmaf(wf[m], fmaf(d.w, wf[m], d1), d0);
             acc[m] = fmaf(pre, tb::ex2(e), acc[m]);
@@ -141,10 +147,11 @@ __device__ __forceinline__ void dspectrum8(const float4* comp, const float4* dco
 // Difference spectrum (TB_FFT_DIFF): acc[m] = sum_k exp2(e_k) (a'_k
 // expm1(de_k) + (a'_k - a_k)), de_k = dca v^2 + dcb v w + dcd w^2 the
 // exponent change in natural-log units; dcomp = (a'_k - a_k, dca, dcb, dcd).
-__device__ __forceinline__ void diffspectrum8(const float4* comp, const float4* dcomp, int K,
+template <int R>
+__device__ __forceinline__ void diffspectrum_rows(const float4* comp, const float4* dcomp, int K,
                                               float vf, const float* wf, float* acc) {
 #pragma unroll
-    for (int m = 0; m < 8; m++) acc[m] = 0.f;
+    for (int m = 0; m < R; m++) acc[m] = 0.f;
     for (int k = 0; k < K; k++) {
         const float4 c = comp[k];
         const float4 d = dcomp[k];
@@ -152,7 +159,7 @@ __device__ __forceinline__ void diffspectrum8(const float4* comp, const float4* 
         const float d0 = d.y * vf * vf, d1 = d.z * vf;
         const float a2 = c.x + d.x;
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
+        for (int m = 0; m < R; m++) {
             const float e = fmaf(wf[m], fmaf(c.w, wf[m], be), al);
             const float de = fmaf(wf[m], fmaf(d.w, wf[m], d1), d0);
             const float pre = fmaf(a2, expm1f(de), d.x);
@@ -162,12 +169,13 @@ __device__ __forceinline__ void diffspectrum8(const float4* comp, const float4* 
 }
 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) { return tb::cmul(a, b); }
-__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
 
 // Zero-fills (STORE mode) the output pixels outside the window
 // [gr0, gr1) x [gc0, gc1) of G coordinates.
 __device__ void zero_outside(float* O, int64_t ldo, int mw, int mh, int sx, int sy, int gr0,
                              int gr1, int gc0, int gc1, bool empty) {
+    // nothing to do when the window covers the whole mask
+    if (!empty && gr0 + sy <= 0 && gr1 + sy >= mh && gc0 + sx <= 0 && gc1 + sx >= mw) return;
     for (int i = threadIdx.x; i < mh * mw; i += kThreads) {
         const int r = i / mw - sy, c = i % mw - sx;
         if (empty || r < gr0 || r >= gr1 || c < gc0 || c >= gc1)
@@ -186,6 +194,170 @@ __device__ __forceinline__ void put(float* o, float v, int mode, float& dot) {
     else *o = v;
 }
 
+// ---------------------------------------------------------------------------
+// N = 256: radix-16 transforms (tb::fft256_r16), one per half warp, so each
+// warp runs two side by side.  Thread t of a half holds rows (column pass)
+// or columns (row pass) t + 16 m, m = 0..15.
+// ---------------------------------------------------------------------------
+template <bool kDeriv, int R>
+__device__ __forceinline__ void col_spectrum(const tb_fft_item& it, int K, const Shared& sh,
+                                             float vf, const float* wf, float* acc) {
+    if (kDeriv && it.dmode == TB_FFT_DSPEC) dspectrum_rows<R>(sh.comp, sh.dcomp, K, vf, wf, acc);
+    else if (kDeriv && it.dmode == TB_FFT_DIFF)
+        diffspectrum_rows<R>(sh.comp, sh.dcomp, K, vf, wf, acc);
+    else spectrum_rows<R>(sh.comp, K, vf, wf, acc);
+}
+
+// Column pass: the 127 interior rfft columns and one transform carrying both
+// the DC and the Nyquist column, 128 transforms over the 32 half warps (four
+// per warp).  irfftn keeps the real parts of the DC and Nyquist columns'
+// transforms along w, which are the transforms of their Hermitian parts
+// Xh(w) = (X(w) + conj X(-w)) / 2 (row -w = row (N - j) mod N); those are
+// real, so Z = Xh_0 + i Xh_N gives both in one complex transform (real part
+// -> DC, imaginary part -> Nyquist).  The mixture spectrum of those two
+// columns is evaluated first by the whole block (one row per thread), so
+// every half warp evaluates at most one column.  With kHy every column is
+// multiplied by the y taps' frequency response.  Rows [rlo, rhi) of every
+// column go to S1 (row-major, N/2 + 1 columns).  Called by the whole block.
+template <bool kDeriv, bool kHy>
+__device__ void colpass256(const tb_fft_item& it, int K, const float* __restrict__ spec,
+                           const Shared& sh, int rlo, int rhi) {
+    constexpr int N = 256, NH = 129;
+    static_assert(kThreads == 2 * N, "one thread per row of the DC and Nyquist columns");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int half = lane >> 4, t = lane & 15;
+    float2* xb = sh.xbuf + warp * kXbufPersist + half * tb::kR16Xbuf;
+    const float2* P = reinterpret_cast<const float2*>(spec);
+    {
+        const int j = threadIdx.x & (N - 1);
+        const float w1 = (float)(j < N / 2 ? j : j - N) / (float)N;
+        float g;
+        col_spectrum<kDeriv, 1>(it, K, sh, threadIdx.x < N ? 0.f : 0.5f, &w1, &g);
+        sh.gsp[threadIdx.x] = g;
+    }
+    __syncthreads();
+    float wf[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int j = t + 16 * m;
+        wf[m] = (float)(j < N / 2 ? j : j - N) / (float)N;
+    }
+    for (int s0 = 2 * warp; s0 < 128; s0 += 2 * kWarps) {
+        const int slot = s0 + half;          // 0: DC + Nyquist, else the column v = slot
+        float2 x[16];
+        if (slot != 0) {
+            // the PSF spectrum's loads go out before the mixture spectrum is evaluated
+            const float2* Pc = P + (int64_t)slot * N;
+#pragma unroll
+            for (int m = 0; m < 16; m++) x[m] = __ldg(Pc + t + 16 * m);
+            float acc[16];
+            col_spectrum<kDeriv, 16>(it, K, sh, (float)slot / (float)N, wf, acc);
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+                const float2 z = make_float2(acc[m] * x[m].x, acc[m] * x[m].y);
+                x[m] = kHy ? cmulf(z, sh.hy[t + 16 * m]) : z;
+            }
+        } else {
+            const float2* Pn = P + (int64_t)(N / 2) * N;
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+                const int j = t + 16 * m, jn = (N - j) & (N - 1);
+                float2 a = __ldg(P + j), b = __ldg(P + jn);
+                float2 an = __ldg(Pn + j), bn = __ldg(Pn + jn);
+                if (kHy) {
+                    const float2 hj = sh.hy[j], hn = sh.hy[jn];
+                    a = cmulf(a, hj);
+                    b = cmulf(b, hn);
+                    an = cmulf(an, hj);
+                    bn = cmulf(bn, hn);
+                }
+                const float g0 = sh.gsp[j], g0n = sh.gsp[jn];
+                const float gN = sh.gsp[N + j], gNn = sh.gsp[N + jn];
+                // Xh_0 = (G0(w) a + G0(-w) conj b) / 2, Xh_N likewise; Z = Xh_0 + i Xh_N
+                const float2 h0 = make_float2(0.5f * (g0 * a.x + g0n * b.x),
+                                              0.5f * (g0 * a.y - g0n * b.y));
+                const float2 hN = make_float2(0.5f * (gN * an.x + gNn * bn.x),
+                                              0.5f * (gN * an.y - gNn * bn.y));
+                x[m] = make_float2(h0.x - hN.y, h0.y + hN.x);
+            }
+        }
+        tb::fft256_r16<+1>(x, t, xb, sh.tw, [&](int row, float2 z) {
+            if (row >= rlo && row < rhi) {
+                float2* r = sh.s1 + (row - rlo) * NH;
+                if (slot != 0) {
+                    r[slot] = z;
+                } else {
+                    r[0] = make_float2(z.x, 0.f);
+                    r[N / 2] = make_float2(z.y, 0.f);
+                }
+            }
+        });
+        __syncwarp();
+    }
+}
+
+// Row pass: pairs of S1 rows (times Hx with kHx), packed as H1 + i H2 with
+// their Hermitian extension, two pairs per warp; one inverse transform gives
+// both real rows.  kToS1: the rows' columns [c0, c1) go back into the rows'
+// own S1 storage (as floats, for the spatial Lanczos pass); otherwise the
+// columns [gc0, gc1) go to the output (oa / ob rows) through put().
+template <bool kDeriv, bool kHx, bool kToS1>
+__device__ void rowpass256(const tb_fft_item& it, const Shared& sh, int nrows, float* O,
+                           int64_t ldo, int row0, int sx, int c0, int c1, float osc, float& dot) {
+    constexpr int N = 256, NH = 129;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int half = lane >> 4, t = lane & 15;
+    float2* xb = sh.xbuf + warp * kXbufPersist + half * tb::kR16Xbuf;
+    const int npairs = (nrows + 1) / 2;
+    for (int p0 = 2 * warp; p0 < npairs; p0 += 2 * kWarps) {
+        const bool act = p0 + half < npairs;
+        const int p = act ? p0 + half : npairs - 1;
+        const int ia = 2 * p, ib = 2 * p + 1;
+        const bool hasb = ib < nrows;
+        const float2* H1 = sh.s1 + ia * NH;
+        const float2* H2 = sh.s1 + (hasb ? ib : ia) * NH;
+        float2 x[16];
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            const int n = t + 16 * m;
+            const int q = n <= N / 2 ? n : N - n;
+            float2 h1 = H1[q];
+            float2 h2 = hasb ? H2[q] : make_float2(0.f, 0.f);
+            if (kHx) {
+                const float2 hx = sh.hx[q];
+                h1 = cmulf(h1, hx);
+                h2 = cmulf(h2, hx);
+            }
+            if (q == 0 || q == N / 2) {
+                h1.y = 0.f;
+                h2.y = 0.f;
+            }
+            x[m] = n <= N / 2 ? make_float2(h1.x - h2.y, h1.y + h2.x)
+                              : make_float2(h1.x + h2.y, h2.x - h1.y);
+        }
+        if (kToS1) {
+            float* rowA = reinterpret_cast<float*>(sh.s1 + ia * NH);
+            float* rowB = reinterpret_cast<float*>(sh.s1 + ib * NH);
+            tb::fft256_r16<+1>(x, t, xb, sh.tw, [&](int col, float2 z) {
+                if (act && col >= c0 && col < c1) {
+                    rowA[col - c0] = z.x;
+                    if (hasb) rowB[col - c0] = z.y;
+                }
+            });
+        } else {
+            float* oa = O + (int64_t)(row0 + ia) * ldo + sx;
+            float* ob = O + (int64_t)(row0 + ib) * ldo + sx;
+            tb::fft256_r16<+1>(x, t, xb, sh.tw, [&](int col, float2 z) {
+                if (act && col >= c0 && col < c1) {
+                    put<kDeriv>(oa + col, z.x * osc, it.mode, dot);
+                    if (hasb) put<kDeriv>(ob + col, z.y * osc, it.mode, dot);
+                }
+            });
+        }
+        __syncwarp();
+    }
+}
+
 template <int N, bool kDeriv>
 __device__ void render_item_spectral(const tb_fft_item& it, int K, const float* __restrict__ spec,
                                      float* __restrict__ out, const Shared& sh, int rcap,
@@ -197,7 +369,7 @@ __device__ void render_item_spectral(const tb_fft_item& it, int K, const float* 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int t = lane % T;
     const int ngroups = kWarps * GPW;
-    float2* xb = sh.xbuf + warp * kXbufPerWarp + (lane / T) * XB;
+    float2* xb = sh.xbuf + warp * kXbufPersist + (lane / T) * XB;
 
     const int mw = it.mw, mh = it.mh, sx = it.sx, sy = it.sy;
     const float osc = it.scale / (float)(N * N);
@@ -222,77 +394,88 @@ __device__ void render_item_spectral(const tb_fft_item& it, int K, const float* 
     }
     __syncthreads();
 
-    for (int a = gr0; a < gr1; a += rcap) {
-        const int rlo = a, rhi = min(gr1, a + rcap);
-        const int nrows = rhi - rlo;
-
-        // ---- 1. column pass: N/2 + 1 column FFTs, times Hy ----
-        for (int v0 = warp * GPW; v0 < NH; v0 += ngroups) {
-            const bool act = v0 + lane / T < NH;
-            const int v = act ? v0 + lane / T : NH - 1;
-            float wf[8], acc[8];
-#pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const int j = t + m * T;
-                wf[m] = (float)(j < N / 2 ? j : j - N) / (float)N;
-            }
-            if (kDeriv && it.dmode == TB_FFT_DSPEC)
-                dspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
-            else if (kDeriv && it.dmode == TB_FFT_DIFF)
-                diffspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
-            else
-                spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
-            float2 x[8];
-            const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)v * N;
-#pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const int j = t + m * T;
-                const float2 p = __ldg(P + j);
-                x[m] = cmulf(make_float2(acc[m] * p.x, acc[m] * p.y), sh.hy[j]);
-            }
-            // irfftn drops the imaginary parts of the DC and Nyquist columns
-            // after the transform along y.
-            const bool realcol = v == 0 || v == N / 2;
-            float2* S1 = sh.s1;
-            tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int row, float2 z) {
-                if (act && row >= rlo && row < rhi)
-                    S1[(row - rlo) * NH + v] = realcol ? make_float2(z.x, 0.f) : z;
-            });
-            __syncwarp();
+    if constexpr (N == 256) {
+        for (int a = gr0; a < gr1; a += rcap) {
+            const int rlo = a, rhi = min(gr1, a + rcap);
+            colpass256<kDeriv, true>(it, K, spec, sh, rlo, rhi);
+            __syncthreads();
+            rowpass256<kDeriv, true, false>(it, sh, rhi - rlo, O, ldo, rlo + sy, sx, gc0, gc1, osc,
+                                            dot);
+            __syncthreads();
         }
-        __syncthreads();
+    } else {
+        for (int a = gr0; a < gr1; a += rcap) {
+            const int rlo = a, rhi = min(gr1, a + rcap);
+            const int nrows = rhi - rlo;
 
-        // ---- 2. row pass: two real rows per complex FFT, straight to the output ----
-        const int npairs = (nrows + 1) / 2;
-        for (int p0 = warp * GPW; p0 < npairs; p0 += ngroups) {
-            const bool act = p0 + lane / T < npairs;
-            const int p = act ? p0 + lane / T : npairs - 1;
-            const int ia = 2 * p, ib = 2 * p + 1;
-            const bool hasb = ib < nrows;
-            const float2* H1 = sh.s1 + ia * NH;
-            const float2* H2 = sh.s1 + (hasb ? ib : ia) * NH;
-            float2 x[8];
+            // ---- 1. column pass: N/2 + 1 column FFTs, times Hy ----
+            for (int v0 = warp * GPW; v0 < NH; v0 += ngroups) {
+                const bool act = v0 + lane / T < NH;
+                const int v = act ? v0 + lane / T : NH - 1;
+                float wf[8], acc[8];
 #pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const int n = t + m * T;
-                const int q = n <= N / 2 ? n : N - n;
-                const float2 hx = sh.hx[q];
-                const float2 h1 = cmulf(H1[q], hx);
-                const float2 h2 = hasb ? cmulf(H2[q], hx) : make_float2(0.f, 0.f);
-                x[m] = n <= N / 2 ? make_float2(h1.x - h2.y, h1.y + h2.x)
-                                  : make_float2(h1.x + h2.y, h2.x - h1.y);
-            }
-            float* oa = O + (int64_t)(rlo + ia + sy) * ldo + sx;
-            float* ob = O + (int64_t)(rlo + ib + sy) * ldo + sx;
-            tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int col, float2 z) {
-                if (act && col >= gc0 && col < gc1) {
-                    put<kDeriv>(oa + col, z.x * osc, it.mode, dot);
-                    if (hasb) put<kDeriv>(ob + col, z.y * osc, it.mode, dot);
+                for (int m = 0; m < 8; m++) {
+                    const int j = t + m * T;
+                    wf[m] = (float)(j < N / 2 ? j : j - N) / (float)N;
                 }
-            });
-            __syncwarp();
+                if (kDeriv && it.dmode == TB_FFT_DSPEC)
+                    dspectrum_rows<8>(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
+                else if (kDeriv && it.dmode == TB_FFT_DIFF)
+                    diffspectrum_rows<8>(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
+                else
+                    spectrum_rows<8>(sh.comp, K, (float)v / (float)N, wf, acc);
+                float2 x[8];
+                const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)v * N;
+#pragma unroll
+                for (int m = 0; m < 8; m++) {
+                    const int j = t + m * T;
+                    const float2 p = __ldg(P + j);
+                    x[m] = cmulf(make_float2(acc[m] * p.x, acc[m] * p.y), sh.hy[j]);
+                }
+                // irfftn drops the imaginary parts of the DC and Nyquist columns
+                // after the transform along y.
+                const bool realcol = v == 0 || v == N / 2;
+                float2* S1 = sh.s1;
+                tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int row, float2 z) {
+                    if (act && row >= rlo && row < rhi)
+                        S1[(row - rlo) * NH + v] = realcol ? make_float2(z.x, 0.f) : z;
+                });
+                __syncwarp();
+            }
+            __syncthreads();
+
+            // ---- 2. row pass: two real rows per complex FFT, straight to the output ----
+            const int npairs = (nrows + 1) / 2;
+            for (int p0 = warp * GPW; p0 < npairs; p0 += ngroups) {
+                const bool act = p0 + lane / T < npairs;
+                const int p = act ? p0 + lane / T : npairs - 1;
+                const int ia = 2 * p, ib = 2 * p + 1;
+                const bool hasb = ib < nrows;
+                const float2* H1 = sh.s1 + ia * NH;
+                const float2* H2 = sh.s1 + (hasb ? ib : ia) * NH;
+                float2 x[8];
+#pragma unroll
+                for (int m = 0; m < 8; m++) {
+                    const int n = t + m * T;
+                    const int q = n <= N / 2 ? n : N - n;
+                    const float2 hx = sh.hx[q];
+                    const float2 h1 = cmulf(H1[q], hx);
+                    const float2 h2 = hasb ? cmulf(H2[q], hx) : make_float2(0.f, 0.f);
+                    x[m] = n <= N / 2 ? make_float2(h1.x - h2.y, h1.y + h2.x)
+                                      : make_float2(h1.x + h2.y, h2.x - h1.y);
+                }
+                float* oa = O + (int64_t)(rlo + ia + sy) * ldo + sx;
+                float* ob = O + (int64_t)(rlo + ib + sy) * ldo + sx;
+                tb::fft_run<N, +1>(x, t, xb, sh.tw, [&](int col, float2 z) {
+                    if (act && col >= gc0 && col < gc1) {
+                        put<kDeriv>(oa + col, z.x * osc, it.mode, dot);
+                        if (hasb) put<kDeriv>(ob + col, z.y * osc, it.mode, dot);
+                    }
+                });
+                __syncwarp();
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
@@ -307,7 +490,7 @@ __device__ void render_item_spatial(const tb_fft_item& it, int K, const float* _
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int t = lane % T;
     const int ngroups = kWarps * GPW;
-    float2* xb = sh.xbuf + warp * kXbufPerWarp + (lane / T) * XB;
+    float2* xb = sh.xbuf + warp * kXbufPersist + (lane / T) * XB;
 
     const int mw = it.mw, mh = it.mh, sx = it.sx, sy = it.sy;
     const float osc = it.scale / (float)(N * N);
@@ -326,6 +509,9 @@ __device__ void render_item_spatial(const tb_fft_item& it, int K, const float* _
         const int nrows = rhi - rlo;
 
         // ---- 1. column pass (all N/2 + 1 columns) ----
+        if constexpr (N == 256) {
+            colpass256<kDeriv, false>(it, K, spec, sh, rlo, rhi);
+        } else
         for (int v0 = warp * GPW; v0 < NH; v0 += ngroups) {
             const bool act = v0 + lane / T < NH;
             const int v = act ? v0 + lane / T : NH - 1;
@@ -336,11 +522,11 @@ __device__ void render_item_spatial(const tb_fft_item& it, int K, const float* _
                 wf[m] = (float)(j < N / 2 ? j : j - N) / (float)N;
             }
             if (kDeriv && it.dmode == TB_FFT_DSPEC)
-                dspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
+                dspectrum_rows<8>(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
             else if (kDeriv && it.dmode == TB_FFT_DIFF)
-                diffspectrum8(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
+                diffspectrum_rows<8>(sh.comp, sh.dcomp, K, (float)v / (float)N, wf, acc);
             else
-                spectrum8(sh.comp, K, (float)v / (float)N, wf, acc);
+                spectrum_rows<8>(sh.comp, K, (float)v / (float)N, wf, acc);
             float2 x[8];
             const float2* P = reinterpret_cast<const float2*>(spec) + (int64_t)v * N;
 #pragma unroll
@@ -358,6 +544,9 @@ __device__ void render_item_spatial(const tb_fft_item& it, int K, const float* _
 
         // ---- 2. row pass (two real rows per complex FFT) ----
         const int npairs = (nrows + 1) / 2;
+        if constexpr (N == 256) {
+            rowpass256<kDeriv, false, true>(it, sh, nrows, nullptr, 0, 0, 0, c0, c1, 0.f, dot);
+        } else
         for (int p0 = warp * GPW; p0 < npairs; p0 += ngroups) {
             const bool act = p0 + lane / T < npairs;
             const int p = act ? p0 + lane / T : npairs - 1;
@@ -483,8 +672,10 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
     sh.hy = reinterpret_cast<float2*>(p);
     p += 256 * 8;
     sh.xbuf = reinterpret_cast<float2*>(p);
-    p += kWarps * kXbufPerWarp * 8;
+    p += kWarps * kXbufPersist * 8;
     sh.s1 = reinterpret_cast<float2*>(p);
+    p += kS1Bytes;
+    sh.gsp = reinterpret_cast<float*>(p);
     __shared__ int64_t slot;
     __shared__ int cur_n;
     if (threadIdx.x == 0) cur_n = 0;
@@ -529,14 +720,10 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
                                           (float)(n2 * 2.0 * dc[2]), (float)(n2 * dc[3]));
             }
         }
-        if (threadIdx.x == 32) {
-            if (kDeriv && it.dmode == TB_FFT_DX) taps3_deriv(it.mux, sh.taps);
-            else taps3(it.mux, sh.taps);
-        }
-        if (threadIdx.x == 64) {
-            if (kDeriv && it.dmode == TB_FFT_DY) taps3_deriv(it.muy, sh.taps + 7);
-            else taps3(it.muy, sh.taps + 7);
-        }
+        if (threadIdx.x >= 32 && threadIdx.x < 64)
+            taps_warp(it.mux, kDeriv && it.dmode == TB_FFT_DX, sh.taps);
+        if (threadIdx.x >= 64 && threadIdx.x < 96)
+            taps_warp(it.muy, kDeriv && it.dmode == TB_FFT_DY, sh.taps + 7);
         __syncthreads();
         if (cur_n != N) {
             __syncthreads();
@@ -630,42 +817,6 @@ __device__ __forceinline__ bool item_ok(const tb_fft_item& it, const double* dco
            fabs(it.muy) <= 0.5;
 }
 
-// taps3 / taps3_deriv by one warp: lane i < 7 evaluates tap i (the same
-// terms), the sums over the taps by shuffles.  Called by all 32 lanes.
-__device__ void taps_warp(double dx, bool deriv, float* f) {
-    const int i = threadIdx.x & 31;
-    double L = 0.0, D = 0.0;
-    bool on;
-    if (!deriv && dx == 0.0) {
-        if (i < 7) f[i] = i == 3 ? 1.f : 0.f;
-        return;
-    }
-    if (deriv) on = i >= (dx >= 0.0 ? 0 : 1) && i < (dx >= 0.0 ? 6 : 7);
-    else on = i >= (dx > 0.0 ? 0 : 1) && i < (dx > 0.0 ? 6 : 7);
-    if (on) {
-        // sin / cos of pi t by sincospi (no argument reduction)
-        const double t = i - 3.0 + dx;
-        const double p = TB_PI * t;
-        if (p == 0.0) {
-            L = 1.0;
-        } else {
-            double sp, cp, s3, c3;
-            sincospi(t, &sp, &cp);
-            sincospi(t / 3.0, &s3, &c3);
-            L = 3.0 * sp * s3 / (p * p);
-            if (deriv)
-                D = TB_PI * 3.0 * (cp * s3 / (p * p) + sp * c3 / (3.0 * p * p) -
-                                   2.0 * sp * s3 / (p * p * p));
-        }
-    }
-    double S = L, Sd = D;
-    for (int o = 16; o > 0; o >>= 1) {
-        S += __shfl_xor_sync(0xffffffffu, S, o);
-        Sd += __shfl_xor_sync(0xffffffffu, Sd, o);
-    }
-    if (i < 7) f[i] = on ? (float)(deriv ? (D - L / S * Sd) / S : L / S) : 0.f;
-}
-
 struct SplitColShared {
     float2 tw[256];
     float4 comp[kMaxK];
@@ -704,9 +855,9 @@ __device__ void stage_components(const tb_fft_item& it, const double* __restrict
 __device__ __forceinline__ void spectrum_any(const tb_fft_item& it, const float4* comp,
                                              const float4* dcomp, float vf, const float* wf,
                                              float* acc) {
-    if (it.dmode == TB_FFT_DSPEC) dspectrum8(comp, dcomp, it.K, vf, wf, acc);
-    else if (it.dmode == TB_FFT_DIFF) diffspectrum8(comp, dcomp, it.K, vf, wf, acc);
-    else spectrum8(comp, it.K, vf, wf, acc);
+    if (it.dmode == TB_FFT_DSPEC) dspectrum_rows<8>(comp, dcomp, it.K, vf, wf, acc);
+    else if (it.dmode == TB_FFT_DIFF) diffspectrum_rows<8>(comp, dcomp, it.K, vf, wf, acc);
+    else spectrum_rows<8>(comp, it.K, vf, wf, acc);
 }
 
 // Frequency response of the 7 Lanczos-3 taps at frequency index fr of an
