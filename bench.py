@@ -77,6 +77,9 @@ def parse():
                          'measurements')
     ap.add_argument('--fit-blobs', type=int, default=2000,
                     help='blobs in the blob-fitting measurement (2000 = the full workload)')
+    ap.add_argument('--fourier-method', default='auto', choices=['auto', 'persistent', 'split'],
+                    help='Fourier render method of the headline (auto: the faster on this '
+                         'workload, timed first)')
     ap.add_argument('--only', default='',
                     help='comma-separated secondary measurements to run (C3, C5, C4, K5, C1, '
                          'EM, SEG); default all')
@@ -1384,9 +1387,14 @@ def main():
     def step():
         renderer.render_device(d_src, n, out)
 
-    # the faster Fourier method on this workload (persistent or split)
-    tune = renderer.autotune(d_src, n, out)
+    # the faster Fourier method on this workload (persistent or split), unless
+    # one is asked for
     from tractor_b200 import render as R
+    if args.fourier_method == 'auto':
+        tune = renderer.autotune(d_src, n, out)
+    else:
+        tune = {}
+        R.fourier_method[dev.index] = args.fourier_method
     method = R.fourier_method[dev.index]
     for _ in range(max(3, args.warmup)):
         step()

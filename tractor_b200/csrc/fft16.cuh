@@ -60,10 +60,12 @@ template <int S> __device__ __forceinline__ void dft16(float2* a) {
 // Runs one 256-point transform on the 16 threads of a half warp (t = lane
 // within the half).  `v[m]` = x[t + 16 m] on entry.  `store(idx, value)`
 // receives the outputs X[t + 16 q], q = 0..15 (16 calls per thread).  `xb` is
-// the half warp's exchange buffer (kR16Xbuf float2), `tw` the table of
-// exp(2 pi i e / 256).  Both halves of the warp must call this together.
+// the half warp's exchange buffer (kR16Xbuf float2), `tw16` the pass-2
+// twiddles laid out by thread: tw16[16 m + t] = exp(2 pi i m t / 256)
+// (build_r16_twiddles), so a half warp's loads of one m are conflict-free.
+// Both halves of the warp must call this together.
 template <int S, class Store>
-__device__ __forceinline__ void fft256_r16(float2* v, int t, float2* xb, const float2* tw,
+__device__ __forceinline__ void fft256_r16(float2* v, int t, float2* xb, const float2* tw16,
                                            Store store) {
     dft16<S>(v);
 #pragma unroll
@@ -73,10 +75,23 @@ __device__ __forceinline__ void fft256_r16(float2* v, int t, float2* xb, const f
     for (int m = 0; m < 16; m++) v[m] = xb[r16pad(t + 16 * m)];
     __syncwarp();
 #pragma unroll
-    for (int m = 1; m < 16; m++) v[m] = cmul(v[m], twid<256, S>(tw, m * t));
+    for (int m = 1; m < 16; m++) {
+        const float2 w = tw16[16 * m + t];
+        v[m] = cmul(v[m], S > 0 ? w : make_float2(w.x, -w.y));
+    }
     dft16<S>(v);
 #pragma unroll
     for (int q = 0; q < 16; q++) store(t + 16 * q, v[q]);
+}
+
+// tw16[16 m + t] = exp(2 pi i m t / 256), m, t = 0..15, built once per CTA in
+// FP64.
+__device__ inline void build_r16_twiddles(float2* tw16) {
+    for (int e = threadIdx.x; e < 256; e += blockDim.x) {
+        double s, c;
+        sincospi(2.0 * (double)((e >> 4) * (e & 15)) / 256.0, &s, &c);
+        tw16[e] = make_float2((float)c, (float)s);
+    }
 }
 
 }  // namespace tb

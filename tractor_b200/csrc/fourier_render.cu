@@ -50,7 +50,8 @@ constexpr int kSmemBytes = 256 * 8               /* twiddles */
                            + 2 * kMaxK * 16       /* components, derivative prefactors */
                            + 16 * 4               /* taps */
                            + (129 + 256) * 8      /* Hx, Hy */
-                           + kWarps * kXbufPersist * 8 + kS1Bytes + 2 * 256 * 4;
+                           + kWarps * kXbufPersist * 8 + kS1Bytes + 2 * 256 * 4
+                           + 256 * 8 /* radix-16 twiddles */;
 
 struct Shared {
     float2* tw;
@@ -62,6 +63,7 @@ struct Shared {
     float2* xbuf;
     float2* s1;
     float* gsp;     // N = 256: mixture spectrum of the DC and Nyquist columns, all rows
+    float2* tw16;   // N = 256: the radix-16 pass-2 twiddles by thread (build_r16_twiddles)
 };
 
 // The 7 Lanczos-3 taps of a sub-pixel shift dx (lanczos_shift_3f's kernel
@@ -281,7 +283,7 @@ __device__ void colpass256(const tb_fft_item& it, int K, const float* __restrict
                 x[m] = make_float2(h0.x - hN.y, h0.y + hN.x);
             }
         }
-        tb::fft256_r16<+1>(x, t, xb, sh.tw, [&](int row, float2 z) {
+        tb::fft256_r16<+1>(x, t, xb, sh.tw16, [&](int row, float2 z) {
             if (row >= rlo && row < rhi) {
                 float2* r = sh.s1 + (row - rlo) * NH;
                 if (slot != 0) {
@@ -338,7 +340,7 @@ __device__ void rowpass256(const tb_fft_item& it, const Shared& sh, int nrows, f
         if (kToS1) {
             float* rowA = reinterpret_cast<float*>(sh.s1 + ia * NH);
             float* rowB = reinterpret_cast<float*>(sh.s1 + ib * NH);
-            tb::fft256_r16<+1>(x, t, xb, sh.tw, [&](int col, float2 z) {
+            tb::fft256_r16<+1>(x, t, xb, sh.tw16, [&](int col, float2 z) {
                 if (act && col >= c0 && col < c1) {
                     rowA[col - c0] = z.x;
                     if (hasb) rowB[col - c0] = z.y;
@@ -347,7 +349,7 @@ __device__ void rowpass256(const tb_fft_item& it, const Shared& sh, int nrows, f
         } else {
             float* oa = O + (int64_t)(row0 + ia) * ldo + sx;
             float* ob = O + (int64_t)(row0 + ib) * ldo + sx;
-            tb::fft256_r16<+1>(x, t, xb, sh.tw, [&](int col, float2 z) {
+            tb::fft256_r16<+1>(x, t, xb, sh.tw16, [&](int col, float2 z) {
                 if (act && col >= c0 && col < c1) {
                     put<kDeriv>(oa + col, z.x * osc, it.mode, dot);
                     if (hasb) put<kDeriv>(ob + col, z.y * osc, it.mode, dot);
@@ -676,6 +678,8 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
     sh.s1 = reinterpret_cast<float2*>(p);
     p += kS1Bytes;
     sh.gsp = reinterpret_cast<float*>(p);
+    p += 2 * 256 * 4;
+    sh.tw16 = reinterpret_cast<float2*>(p);
     __shared__ int64_t slot;
     __shared__ int cur_n;
     if (threadIdx.x == 0) cur_n = 0;
@@ -728,7 +732,10 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
         if (cur_n != N) {
             __syncthreads();
             switch (N) {
-                case 256: tb::build_twiddles<256>(sh.tw); break;
+                case 256:
+                    tb::build_twiddles<256>(sh.tw);
+                    tb::build_r16_twiddles(sh.tw16);
+                    break;
                 case 128: tb::build_twiddles<128>(sh.tw); break;
                 case 64: tb::build_twiddles<64>(sh.tw); break;
                 default: tb::build_twiddles<32>(sh.tw); break;

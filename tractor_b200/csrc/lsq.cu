@@ -634,10 +634,6 @@ static_assert(kSmem + 1024 > 232448 / 3 && 2 * (kSmem + 1024) <= 232448, "two CT
 __device__ __forceinline__ void conv_barrier() {
     asm volatile("bar.sync 1, 256;" ::: "memory");
 }
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tb::tc::smem_u32(bar))
-                 : "memory");
-}
 
 __global__ void __launch_bounds__(tc64::kThreads, 2)
 normal_eq_tc64_kernel(const float* __restrict__ A, const float* __restrict__ rhs,
@@ -816,7 +812,7 @@ normal_eq_tc64_kernel(const float* __restrict__ A, const float* __restrict__ rhs
             // before every S warp has read it (the next drain needs the next
             // chunk, whose stages need every converter's arrival)
             fence_before_sync();
-            mbar_arrive(&accfree[drains & 1]);
+            tb::tc::mbar_arrive(&accfree[drains & 1]);
             drains++;
             return ok;
         };
@@ -843,7 +839,7 @@ normal_eq_tc64_kernel(const float* __restrict__ A, const float* __restrict__ rhs
                 *reinterpret_cast<float4*>(buf + soff[m] + 1024) = l;   // row 64 + c
             }
             fence_async_smem();
-            mbar_arrive(&full[bi]);
+            tb::tc::mbar_arrive(&full[bi]);
             // the previous chunk's accumulators, while this chunk is multiplied
             if (s % kChunkSt == 0 && s > 0 && !drain(s - 1, fail)) fail = true;
         }
