@@ -80,6 +80,11 @@ def parse():
     ap.add_argument('--fourier-method', default='auto', choices=['auto', 'persistent', 'split'],
                     help='Fourier render method of the headline (auto: the faster on this '
                          'workload, timed first)')
+    ap.add_argument('--ne-problems', type=int, default=0,
+                    help='problems in the normal-equation measurement (0: the full workload)')
+    ap.add_argument('--secondary-only', action='store_true',
+                    help='run only the secondary measurements (with --only: one kernel, for '
+                         'profiling); the line then carries no headline figures')
     ap.add_argument('--only', default='',
                     help='comma-separated secondary measurements to run (C3, C5, C4, K5, C1, '
                          'EM, SEG); default all')
@@ -811,7 +816,7 @@ def bench_normal_equations(args, dev, flush, clk, cpu_seconds):
     import torch
     from tractor_b200 import _lib
     lib = _lib.load()
-    n, P, R = NE_PROBLEMS, NE_P, NE_R
+    n, P, R = (args.ne_problems or NE_PROBLEMS), NE_P, NE_R
     g = torch.Generator(device=dev).manual_seed(4000)
     A = torch.randn(n * P * R, device=dev, generator=g)
     r = torch.randn(n * R, device=dev, generator=g)
@@ -1348,6 +1353,34 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_secondaries(args, dev, flush, clk, cpu_s, rank):
+    """Runs the secondary measurements (all, or those --only names); each
+    full record goes to stderr, the returned dict holds their summaries."""
+    runs = [('C3', lambda: bench_scene(args, dev, flush, clk, cpu_s)),
+            ('C5', lambda: bench_fit(args, dev, flush, clk, cpu_s)),
+            ('C4', lambda: bench_derivs(args, dev, flush, clk, cpu_s and min(cpu_s, 6.0))),
+            ('K5', lambda: bench_normal_equations(
+                args, dev, flush, clk, cpu_s and min(cpu_s, 4.0))),
+            ('C1', lambda: bench_plain_small(args, dev, cpu_s and min(cpu_s, 6.0))),
+            ('EM', lambda: bench_emfit(args, dev, flush, clk, cpu_s and min(cpu_s, 4.0))),
+            ('SEG', lambda: bench_segment(args, dev, flush, clk, cpu_s))]
+    if args.only:
+        runs = [r for r in runs if r[0] in args.only.split(',')]
+    secondary = {}
+    for name, run in runs:
+        # a secondary line that fails is reported in the line, not fatal
+        try:
+            full = run()
+        except Exception as e:   # noqa: BLE001
+            full = {'error': repr(e)[:300]}
+        full['name'] = name
+        if rank == 0:
+            # the full record on stderr; the main line carries a summary
+            print(json.dumps(full), file=sys.stderr, flush=True)
+        secondary[name] = compact(full)
+    return secondary
+
+
 def main():
     args = parse()
     world, rank, local = init_dist()
@@ -1365,6 +1398,19 @@ def main():
     from tractor_b200 import batch, _lib, build
     build.build()
     _lib.load()
+
+    if args.secondary_only:
+        dev = torch.device('cuda', local)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+        cpu_s = None if (args.no_cpu_baseline or world > 1 or rank) else min(args.cpu_seconds, 8.0)
+        secondary = run_secondaries(args, dev, flush, None, cpu_s, rank)
+        if rank == 0:
+            print(json.dumps({'metric': METRIC, 'secondary_only': True, 'secondary': secondary}),
+                  flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     # one global workload of 256 sources per GPU, cost-balanced over the
     # ranks (tractor_b200.shard); each rank renders its share
@@ -1539,28 +1585,7 @@ def main():
         line['gather_ms'] = gather_ms
     if not args.no_secondary:
         cpu_s = None if (args.no_cpu_baseline or world > 1 or rank) else min(args.cpu_seconds, 8.0)
-        runs = [('C3', lambda: bench_scene(args, dev, flush, clk, cpu_s)),
-                ('C5', lambda: bench_fit(args, dev, flush, clk, cpu_s)),
-                ('C4', lambda: bench_derivs(args, dev, flush, clk, cpu_s and min(cpu_s, 6.0))),
-                ('K5', lambda: bench_normal_equations(
-                    args, dev, flush, clk, cpu_s and min(cpu_s, 4.0))),
-                ('C1', lambda: bench_plain_small(args, dev, cpu_s and min(cpu_s, 6.0))),
-                ('EM', lambda: bench_emfit(args, dev, flush, clk, cpu_s and min(cpu_s, 4.0))),
-                ('SEG', lambda: bench_segment(args, dev, flush, clk, cpu_s))]
-        if args.only:
-            runs = [r for r in runs if r[0] in args.only.split(',')]
-        secondary = {}
-        for name, run in runs:
-            # a secondary line that fails is reported in the line, not fatal
-            try:
-                full = run()
-            except Exception as e:   # noqa: BLE001
-                full = {'error': repr(e)[:300]}
-            full['name'] = name
-            if rank == 0:
-                # the full record on stderr; the main line carries a summary
-                print(json.dumps(full), file=sys.stderr, flush=True)
-            secondary[name] = compact(full)
+        secondary = run_secondaries(args, dev, flush, clk, cpu_s, rank)
     line['plain_fp64'] = fourier_plain_fp64(srcs, out, dev, budget=3.0)
     if line['plain_fp64']['value']:
         line['speedup_vs_plain_fp64'] = value / line['plain_fp64']['value']

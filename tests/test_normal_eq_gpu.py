@@ -81,6 +81,16 @@ def test_stacked_kernel_mixed_sizes(tb):
     print('worst scaled error (stacked):', w, w2)
 
 
+def test_stacked_kernel_whole_quads(tb):
+    """P <= 63 with 16-byte-aligned columns and R a multiple of 4 (whole
+    16-byte copies in every stage): a last stage of 4 .. 28 rows, a single
+    short stage, exact stage and chunk multiples, more stages than the raw
+    ring holds, the benchmark's 16,384 rows."""
+    w = _run_and_check([63, 63, 1, 31, 32, 47, 7, 63],
+                       [16384, 1004, 4, 36, 4096, 2052, 128, 96], seed=11, align=True)
+    print('worst scaled error (stacked, whole quads):', w)
+
+
 def test_one_m_tile_mixed_sizes(tb):
     """Q = P + 1 <= 128: sizes on and off the 8 / 16 / 32 boundaries, rows not
     a multiple of the 32-row stage, several 1024-row chunks, R = 0."""
