@@ -257,3 +257,71 @@ def test_nonneg_is_accepted_and_unused(backend):
         tr.optimize_forced_photometry(nonneg=nonneg, shared_params=False)
         out.append(np.array(tr.getParams()))
     assert np.array_equal(out[0], out[1])
+
+
+def _roi_tractor(T, g, sky):
+    H, W = g['data'].shape[1:]
+    psfs = [T.NCircularGaussianPSF([1.2, 2.6], [0.75, 0.25]),
+            T.GaussianMixturePSF(np.array([0.6, 0.3, 0.1]), np.zeros((3, 2)),
+                                 np.array([np.eye(2) * s ** 2 for s in (1.5, 3.0, 6.0)]))]
+    tims = [T.Image(data=g['data'][b], inverr=np.full((H, W), 2., np.float32), psf=psfs[b],
+                    photocal=T.LinearPhotoCal([1.0, 2.5][b]), sky=T.ConstantSky(0.))
+            for b in range(2)]
+    srcs = []
+    for kind, px, py, fl, re, e1, e2 in g['sources']:
+        pos, br = T.PixPos(px, py), T.Flux(fl)
+        if int(kind) == 0:
+            s = T.PointSource(pos, br)
+        elif int(kind) == 1:
+            s = T.ExpGalaxy(pos, br, T.EllipseE(re, e1, e2))
+        else:
+            s = T.DevGalaxy(pos, br, T.EllipseE(re, e1, e2))
+        s.freezeAllBut('brightness')
+        srcs.append(s)
+    for tim in tims:
+        if sky:
+            tim.freezeAllBut('sky')
+        else:
+            tim.freezeAllParams()
+    return tims, srcs
+
+
+@pytest.mark.parametrize('sky', [False, True])
+def test_rois_equal_the_fit_with_zero_weight_outside(backend, sky):
+    """forced_photometry(rois=...) (optimize.py:45-83: unit-flux models of the
+    full images shifted into each ROI, the fit on the ROI subimages, so
+    sources whose centres lie outside an ROI still contribute their wings)
+    equals the same fit on the full images with the inverse error set to
+    zero outside each ROI: first evaluation, fluxes, variances and fitted
+    skies (copied back to the full images).  The images and their model
+    masks are put back afterwards."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'forced_sky.npz'))
+    H, W = g['data'].shape[1:]
+    rois = [(slice(6, H - 9), slice(4, W - 5)), (slice(0, H - 3), slice(7, W))]
+    start = np.array(g['start']) if sky else np.array(g['start'])[2:]
+    tims, srcs = _roi_tractor(T, g, sky)
+    tr = T.Tractor(tims, srcs)
+    tr.setParams(start)
+    R0 = tr.optimize_forced_photometry(sky=sky, justims0=True, shared_params=False, rois=rois)
+    R = tr.optimize_forced_photometry(sky=sky, variance=True, shared_params=False, rois=rois)
+    got = np.array(tr.getParams())
+    assert list(tr.getImages()) == tims
+    assert tr.modelMasks is None
+    # the same fit on the full images, weighted by the ROIs only
+    tims2, srcs2 = _roi_tractor(T, g, sky)
+    for t, r in zip(tims2, rois):
+        ie = np.zeros_like(t.getInvError())
+        ie[r] = t.getInvError()[r]
+        t.inverr = ie
+    tr2 = T.Tractor(tims2, srcs2)
+    tr2.setParams(start)
+    S0 = tr2.optimize_forced_photometry(sky=sky, justims0=True, shared_params=False)
+    S = tr2.optimize_forced_photometry(sky=sky, variance=True, shared_params=False)
+    want = np.array(tr2.getParams())
+    assert np.isclose(R0.lnp0, S0.lnp0, rtol=1e-9), (R0.lnp0, S0.lnp0)
+    for a, b, r in zip(R0.chis0, S0.chis0, rois):
+        assert a.shape == b[r].shape
+        assert np.abs(a - b[r]).max() < 1e-4
+    np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(R.IV, S.IV, rtol=1e-6)

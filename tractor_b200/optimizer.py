@@ -24,6 +24,15 @@ class OptResult(object):
     """Results of a forced-photometry fit (optimize.py: OptResult)."""
 
 
+def _copy_thaw_state(src, dst):
+    """Gives `dst` (a parameter object of the same structure, e.g. a
+    subimage) the thawed / frozen state of `src`, recursively."""
+    if hasattr(src, 'liquid') and hasattr(dst, 'liquid') and len(src.liquid) == len(dst.liquid):
+        dst.liquid[:] = list(src.liquid)
+    for a, b in zip(getattr(src, 'subs', None) or [], getattr(dst, 'subs', None) or []):
+        _copy_thaw_state(a, b)
+
+
 def default_alphas():
     """1/1024 .. 1 in factors of 2, then sqrt(2), 2 (optimize.py:426-428)."""
     return np.append(2. ** np.arange(-10, 1), [np.sqrt(2.), 2.])
@@ -289,9 +298,20 @@ class B200Optimizer(object):
         first evaluation (lnp0, chis0, ims0), with variance=True IV (the
         sky parameters first with skyvariance), with fitstats=True the
         reference's fit statistics.  nonneg and negfluxval are accepted and,
-        as by LsqrOptimizer (lsqr_optimizer.py:11-38), not used."""
-        if rois is not None:
-            raise NotImplementedError('forced photometry with ROIs is not provided')
+        as by LsqrOptimizer (lsqr_optimizer.py:11-38), not used.
+
+        rois: one (slice(y0, y1), slice(x0, x1)) per image.  As in
+        optimize.py:45-83 and 147-219, the unit-flux models are rendered on
+        the full images (with their model masks) and shifted into each ROI,
+        and the fit runs on img.subimage(x0, x1, y0, y1): the frozen
+        sources' model, chi, update, line search, variances and fit
+        statistics all cover the ROI pixels only; a fitted sky is copied back
+        to the full images' skies (a one-parameter sky does not depend on the
+        origin).  The reference's own ROI path takes chi from the inverse
+        error instead of the image (optimize.py:503-506: `im = ie[roi]` after
+        `ie = ie[roi]`), which fails on a shape mismatch for any ROI not at
+        the origin; here chi is (image - model) x inverr of the ROI, which is
+        what the reference computes without ROIs on the same subimages."""
         from .basics import LinearPhotoCal
         result = OptResult()
         imgs = list(tractor.getImages())
@@ -307,6 +327,81 @@ class B200Optimizer(object):
         umodels, umodsforsource = self._unit_models(tractor, srcs, imgs, minsb, **kwargs)
         for um in umodels:
             assert len(um) == nparams
+        if rois is not None:
+            return self._forced_photometry_rois(
+                tractor, rois, umodels, umodsforsource, srcs, nparams, scales, result,
+                dict(alphas=alphas, damp=damp, priors=priors, minsb=minsb, mindlnp=mindlnp,
+                     sky=sky, minFlux=minFlux, fitstats=fitstats, fitstat_extras=fitstat_extras,
+                     justims0=justims0, variance=variance, skyvariance=skyvariance,
+                     shared_params=shared_params, nilcounts=nilcounts, wantims=wantims))
+        return self._forced_core(tractor, imgs, umodels, umodsforsource, srcs, nparams, scales,
+                                 result, alphas=alphas, damp=damp, priors=priors, minsb=minsb,
+                                 mindlnp=mindlnp, sky=sky, minFlux=minFlux, fitstats=fitstats,
+                                 fitstat_extras=fitstat_extras, justims0=justims0,
+                                 variance=variance, skyvariance=skyvariance,
+                                 shared_params=shared_params, nilcounts=nilcounts,
+                                 wantims=wantims)
+
+    def _forced_photometry_rois(self, tractor, rois, umodels, umodsforsource, srcs, nparams,
+                                scales, result, kw):
+        """forced_photometry over ROIs: the full images' unit-flux models
+        shifted into ROI coordinates (optimize.py:166-184), the fit run with
+        the tractor's images replaced by the ROI subimages (their model masks
+        shifted alike), the images and masks put back afterwards."""
+        from .engine import Images
+        from .patch import ModelMask
+        imgs = list(tractor.getImages())
+        assert len(rois) == len(imgs)
+        origins, subimgs, shifted = [], [], []
+        for img, roi, umods in zip(imgs, rois, umodels):
+            y0, y1 = roi[0].start, roi[0].stop
+            x0, x1 = roi[1].start, roi[1].stop
+            origins.append((x0, y0))
+            sub = img.subimage(x0, x1, y0, y1)
+            _copy_thaw_state(img, sub)     # the fit's parameters are the full images' thawed ones
+            subimgs.append(sub)
+            row = []
+            for um in umods:
+                if um is not None and um.patch is not None:
+                    um = um.copy()
+                    um.x0 -= x0
+                    um.y0 -= y0
+                row.append(um)
+            shifted.append(row)
+        realims, realmasks = tractor.images, tractor.modelMasks
+        masks = None
+        if realmasks is not None:
+            masks = []
+            for (x0, y0), mm in zip(origins, realmasks):
+                d = {}
+                for src, m in mm.items():
+                    if m is None:
+                        d[src] = None
+                    elif m.mask is not None:
+                        d[src] = ModelMask(m.x0 - x0, m.y0 - y0, m.mask)
+                    else:
+                        d[src] = ModelMask(m.x0 - x0, m.y0 - y0, m.w, m.h)
+                masks.append(d)
+        tractor.images = Images(*subimgs)
+        tractor.modelMasks = masks
+        try:
+            result = self._forced_core(tractor, subimgs, shifted, umodsforsource, srcs, nparams,
+                                       scales, result, **kw)
+        finally:
+            if kw.get('sky'):
+                for img, sub in zip(imgs, subimgs):
+                    img.getSky().setParams(sub.getSky().getParams())
+            tractor.images = realims
+            tractor.modelMasks = realmasks
+        return result
+
+    def _forced_core(self, tractor, imgs, umodels, umodsforsource, srcs, nparams, scales,
+                     result, alphas=None, damp=0, priors=False, minsb=0., mindlnp=1.,
+                     sky=False, minFlux=None, fitstats=False, fitstat_extras=None,
+                     justims0=False, variance=False, skyvariance=False, shared_params=True,
+                     nilcounts=-1e30, wantims=True):
+        """The forced-photometry fit proper (optimize.py:85-145,
+        lsqr_optimizer.py:11-235) on `imgs` with their unit-flux models."""
         fsrcs = list(tractor.catalog.getFrozenSources())
         # with the sky fitted, each trial renders it from its parameters
         mod0 = [tractor.getModelImage(img, fsrcs, minsb=minsb, sky=not sky) for img in imgs]
