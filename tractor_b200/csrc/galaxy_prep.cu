@@ -76,8 +76,10 @@ galaxy_fft_prep_kernel(const tb_galaxy_src* __restrict__ srcs, int n, tb_fft_ima
                        tb_profile_tables Tg, tb_fft_item* __restrict__ items,
                        double* __restrict__ camp, double* __restrict__ cvar, int stride,
                        int32_t* __restrict__ flags) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const tb_profile_tables T = tb::stage_tables(Tg, smem_raw);
+    // The tables are read where they lie (L1-cached): each warp touches only
+    // its range's few knots and coefficients, and copying all of them into
+    // shared memory first cost each block more latency than it saved.
+    const tb_profile_tables T = Tg;
     const int lane = threadIdx.x & 31;
     const int i = blockIdx.x * (kPrepThreads / 32) + (threadIdx.x >> 5);
     if (i >= n) return;   // whole warps leave together
@@ -279,14 +281,8 @@ extern "C" int tb_galaxy_fft_prep(const tb_galaxy_src* srcs, int32_t n, const tb
     if (n == 0) return TB_OK;
     if (!srcs || !image || !tables || !items || !comp_amp || !comp_var || !flags) return TB_ERR_ARG;
     if (comp_stride < kMaxComp) return TB_ERR_SIZE;
-    const int smem = tb::tables_smem_bytes(*tables);
-    if (smem > TB_PROFILE_SMEM_MAX) return TB_ERR_SIZE;
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(galaxy_fft_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             smem) != cudaSuccess)
-        return TB_ERR_LAUNCH;
     const int per_block = kPrepThreads / 32;
-    galaxy_fft_prep_kernel<<<(n + per_block - 1) / per_block, kPrepThreads, smem,
+    galaxy_fft_prep_kernel<<<(n + per_block - 1) / per_block, kPrepThreads, 0,
                              (cudaStream_t)stream>>>(
         srcs, n, *image, *tables, items, comp_amp, comp_var, comp_stride, flags);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
