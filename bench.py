@@ -8,10 +8,12 @@ size is 256 (the reference's next power of two of twice the patch
 half-size).  Synthetic, seeded.
 
 One step = render every source's model patch from its parameters already in
-device memory: tb_galaxy_fft_prep (profiles, shapes, item geometry) and
-tb_fourier_render_split (spectrum, FFTs, Lanczos, crop: a column kernel and a
-row kernel through an L2-resident scratch, then the persistent kernel for
-items whose Lanczos window reaches the FFT box edge) -- 4 launches.  The metric
+device memory, by the fastest of three methods timed first on the workload:
+tb_galaxy_fft_render (each source's profile, shape and geometry prepared by
+one warp into shared memory, then spectrum, FFTs, Lanczos and crop by its
+block: one persistent launch), or tb_galaxy_fft_prep followed by the
+persistent tb_fourier_render or by tb_fourier_render_split (column and row
+kernels through an L2-resident scratch).  The metric
 is Mpix x components per second with Npix = sz^2 per source and the
 source's Gaussian component count (SersicGalaxy mixtures have 5-9), summed
 over sources.  L2 is flushed (a 256 MB write) before every timed step.
@@ -77,8 +79,9 @@ def parse():
                          'measurements')
     ap.add_argument('--fit-blobs', type=int, default=2000,
                     help='blobs in the blob-fitting measurement (2000 = the full workload)')
-    ap.add_argument('--fourier-method', default='auto', choices=['auto', 'persistent', 'split'],
-                    help='Fourier render method of the headline (auto: the faster on this '
+    ap.add_argument('--fourier-method', default='auto',
+                    choices=['auto', 'fused', 'persistent', 'split'],
+                    help='Fourier render method of the headline (auto: the fastest on this '
                          'workload, timed first)')
     ap.add_argument('--ne-problems', type=int, default=0,
                     help='problems in the normal-equation measurement (0: the full workload)')
@@ -1433,15 +1436,15 @@ def main():
     def step():
         renderer.render_device(d_src, n, out)
 
-    # the faster Fourier method on this workload (persistent or split), unless
-    # one is asked for
+    # the fastest Fourier method on this workload (fused prep + render, or
+    # prep then the persistent or split render), unless one is asked for
     from tractor_b200 import render as R
     if args.fourier_method == 'auto':
         tune = renderer.autotune(d_src, n, out)
     else:
         tune = {}
-        R.fourier_method[dev.index] = args.fourier_method
-    method = R.fourier_method[dev.index]
+        renderer.method = args.fourier_method
+    method = renderer.method
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
@@ -1466,6 +1469,7 @@ def main():
     time.sleep(0.3)
     # split: setup + column + row kernels per 256 items and the persistent
     # kernel for the items outside the split path; persistent: one launch
+    # after the prep; fused: one launch in all
     launches_per_render = 3 * (-(-n // 256)) + 1 if method == 'split' else 1
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -1475,19 +1479,30 @@ def main():
         e0.record(stream)
         lib = _lib.load()
         items_t, camp, cvar, flg, misc = renderer._work(n)
-        rc = lib.tb_galaxy_fft_prep(d_src.data_ptr(), n,
-                                    __import__('ctypes').addressof(renderer.image),
-                                    __import__('ctypes').addressof(renderer.tables.struct),
-                                    items_t.data_ptr(), camp.data_ptr(), cvar.data_ptr(),
-                                    batch.COMP_STRIDE, flg.data_ptr(), _lib.stream_ptr())
-        _lib.check(rc, 'tb_galaxy_fft_prep')
-        e1.record(stream)
-        R.fourier_render(items_t.data_ptr(), n, camp.data_ptr(), cvar.data_ptr(),
-                         renderer.spec.data_ptr(), out.data_ptr(), misc.data_ptr() + 16,
-                         method=method)
+        if method == 'fused':
+            # preparation and render in one launch: the kernel is the step
+            e1.record(stream)
+            rc = lib.tb_galaxy_fft_render(d_src.data_ptr(), n,
+                                          __import__('ctypes').addressof(renderer.image),
+                                          __import__('ctypes').addressof(renderer.tables.struct),
+                                          renderer.spec.data_ptr(), out.data_ptr(),
+                                          items_t.data_ptr(), flg.data_ptr(), misc.data_ptr(),
+                                          misc.data_ptr() + 16, _lib.stream_ptr())
+            _lib.check(rc, 'tb_galaxy_fft_render')
+        else:
+            rc = lib.tb_galaxy_fft_prep(d_src.data_ptr(), n,
+                                        __import__('ctypes').addressof(renderer.image),
+                                        __import__('ctypes').addressof(renderer.tables.struct),
+                                        items_t.data_ptr(), camp.data_ptr(), cvar.data_ptr(),
+                                        batch.COMP_STRIDE, flg.data_ptr(), _lib.stream_ptr())
+            _lib.check(rc, 'tb_galaxy_fft_prep')
+            e1.record(stream)
+            R.fourier_render(items_t.data_ptr(), n, camp.data_ptr(), cvar.data_ptr(),
+                             renderer.spec.data_ptr(), out.data_ptr(), misc.data_ptr() + 16,
+                             method=method)
         e2.record(stream)
     torch.cuda.synchronize()
-    gpu_launches = (1 + launches_per_render) * args.steps
+    gpu_launches = ((0 if method == 'fused' else 1) + launches_per_render) * args.steps
     step_ms = [a.elapsed_time(c) for a, b, c in ev]
     render_ms = [b.elapsed_time(c) for a, b, c in ev]
     t_total = sum(step_ms) / 1e3
@@ -1530,7 +1545,8 @@ def main():
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    R.check_status(renderer.status(n).clone(), 'tb_fourier_render_split')
+    R.check_status(renderer.status(n).clone(), 'tb_galaxy_fft_render' if method == 'fused'
+                   else 'tb_fourier_render')
 
     job_pixcomp = pixcomp
     gather_ms = None
@@ -1569,9 +1585,11 @@ def main():
                 'overlap': 'D2H of step k on a copy stream during step k+1'},
         'gpu_launches': gpu_launches,
         'fourier_method': {'chosen': method, 'ms': {k: _sig(v) for k, v in tune.items()}},
-        'roofline': {'bound': 'sfu', 'kernel': 'tb_fourier_render_split (setup + column + row '
-                                               'kernels)' if method == 'split' else
-                     'tb_fourier_render (persistent)',
+        'roofline': {'bound': 'sfu', 'kernel': {
+                         'split': 'tb_fourier_render_split (setup + column + row kernels)',
+                         'persistent': 'tb_fourier_render (persistent)',
+                         'fused': 'tb_galaxy_fft_render (preparation + persistent render, '
+                                  'one launch)'}[method],
                      'achieved': achieved, 'peak': peak, 'unit': 'Gex2/s',
                      'frac': achieved / peak,
                      'peak_basis': '%d ex2/clk/SM x %d SMs x %s MHz (median under load)'

@@ -307,7 +307,9 @@ typedef struct {
     int32_t n_ranges;
     int32_t core_spline;          /* spline index of the core fraction */
     const double* range_lohi;     /* 2 per Sersic-index range */
-    const int32_t* range_info;    /* 4 per range: K, first amp spline, first log-var spline, 0 */
+    const int32_t* range_info;    /* 4 per range: K, first amp spline, first log-var spline,
+                                     1 if all its splines share the first one's knots
+                                     (at most 32) and degree, else 0 */
     const int32_t* spline_info;   /* 4 per spline: knot offset, knot count, coef offset, degree */
     const double* knots;
     const double* coefs;
@@ -319,7 +321,7 @@ typedef struct {
     int32_t n_splines, n_knots, n_coefs, pad;
 } tb_profile_tables;
 
-#define TB_PROFILE_SMEM_MAX 49152  /* bytes of tables the prep kernel stages */
+#define TB_PROFILE_SMEM_MAX 49152  /* bytes of tables the prep kernels that stage them hold */
 
 /* flags[i]: 0 = item written; 1 = no patch (zero counts, or the source lies
  * outside its mask farther than its radius: getModelPatch returns None);
@@ -331,6 +333,22 @@ int tb_galaxy_fft_prep(const tb_galaxy_src* srcs, int32_t n, const tb_fft_image*
                        const tb_profile_tables* tables, tb_fft_item* items,
                        double* comp_amp, double* comp_var, int32_t comp_stride,
                        int32_t* flags, void* stream);
+
+/* tb_galaxy_fft_prep and tb_fourier_render in one persistent launch: each
+ * source is prepared (as tb_galaxy_fft_prep) by one warp straight into
+ * shared memory and rendered (as tb_fourier_render) by its block, so no
+ * component tables go through global memory; the patches are bit-for-bit
+ * those of the two-launch path.  The per-source work of
+ * ProfileGalaxy._realGetUnitFluxModelPatch's FFT branch times its counts
+ * (tractor/galaxy.py:336-519) for a non-hybrid PixelizedPSF, as the two
+ * entry points it joins.  psf_spec: the spectra image->spec_off points into
+ * (tb_psf_spectrum).  flags as tb_galaxy_fft_prep; items (may be NULL):
+ * receives each source's item (c0 = 0: its components stay on chip).
+ * work_counter: one int32 of device scratch. */
+int tb_galaxy_fft_render(const tb_galaxy_src* srcs, int32_t n, const tb_fft_image* image,
+                         const tb_profile_tables* tables, const float* psf_spec, float* out,
+                         tb_fft_item* items, int32_t* flags, int32_t* work_counter,
+                         tb_status* status, void* stream);
 
 /* Jacobian items of n galaxies: items[7 i + j] for the parameters j = x, y,
  * counts, s0, s1, s2 (shape, per shape_type), Sersic n of source i, on the

@@ -55,7 +55,8 @@ def test_prep_and_render_match_oracle(tb, oracle):
     srcs = _srcs_random(rng, 48)
     psf = batch.moffat_psf()
     r = batch.FourierGalaxyRenderer(psf)
-    out, flags = r.render(srcs)
+    # the two-launch path leaves the component tables in device memory
+    out, flags = r.render(srcs, method='persistent')
     assert np.all(flags == 0)
     out = out.numpy()
     items = r._work(len(srcs))[0].cpu().numpy().view(_lib.FFT_ITEM)
@@ -121,3 +122,48 @@ def test_full_workload_properties(tb, oracle):
         a2, v2 = _oracle_source(oracle, s)
         ref, _ = oracle.galaxy_fft_masked(a2, v2, s['px'], s['py'], psf, 0, 0, 128, 128)
         assert np.abs(out[i] / s['counts'] - ref).max() / ref.max() < PEAK_TOL
+
+
+def test_fused_equals_two_launch_path(tb):
+    """tb_galaxy_fft_render (preparation and render in one launch) gives the
+    two-launch path's patches bit for bit (the same FP64 products become the
+    same FP32 coefficients) and its flags and items: the benchmark's 256
+    sources, random profiles and shape types, masks of other sizes (FFT 64 /
+    128 / 256), zero counts and a source far outside its mask (no patch),
+    one outside its mask within its radius and one whose FFT size would
+    exceed 256 (unsupported: zero patches and flag 2)."""
+    import numpy as np
+    from tractor_b200 import batch, _lib
+    rng = np.random.default_rng(29)
+    a = batch.sersic_sources(256, rng, mask=128)
+    b = _srcs_random(rng, 64)
+    srcs = np.concatenate([a, b])
+    n = len(srcs)
+    sizes = rng.choice([24, 48, 96, 128], n)
+    sizes[:256] = 128
+    srcs['mw'] = sizes
+    srcs['mh'] = np.where(rng.random(n) < 0.8, sizes, np.maximum(sizes // 2, 8))
+    srcs['px'] = srcs['mw'] / 2.0 + rng.uniform(-3, 3, n)
+    srcs['py'] = srcs['mh'] / 2.0 + rng.uniform(-3, 3, n)
+    srcs['counts'][300] = 0.                                  # no patch
+    srcs['px'][301], srcs['py'][301] = -500., -500.           # far outside: no patch
+    srcs['px'][302] = -2.                                     # just outside: unsupported
+    srcs['mw'][303] = srcs['mh'][303] = 300                   # FFT 512: unsupported
+    srcs['px'][303], srcs['py'][303] = 150., 150.
+    srcs['out_off'] = np.concatenate([[0], np.cumsum(srcs['mw'].astype(np.int64) *
+                                                     srcs['mh'])[:-1]])
+    r = batch.FourierGalaxyRenderer(batch.moffat_psf())
+    got, f1 = r.render(srcs, method='fused')
+    got = got.numpy().copy()
+    it1 = r._work(n)[0].cpu().numpy().view(_lib.FFT_ITEM).copy()
+    want, f2 = r.render(srcs, method='persistent')
+    want = want.numpy().copy()
+    it2 = r._work(n)[0].cpu().numpy().view(_lib.FFT_ITEM).copy()
+    assert np.array_equal(f1, f2)
+    assert f1[300] == 1 and f1[301] == 1 and f1[302] == 2 and f1[303] == 2
+    assert np.sum(f1 == 0) == n - 4
+    for k in it1.dtype.names:
+        if k != 'c0':
+            assert np.array_equal(it1[k], it2[k]), k
+    assert np.all(np.isfinite(got))
+    assert np.array_equal(got, want)

@@ -42,7 +42,13 @@ class DeviceProfileTables(object):
             v0 = len(sinfo)
             for sp in r['logvar_splines']:
                 add_spline(sp)
-            rinfo.append([r['K'], a0, v0, 0])
+            # 1: every spline of the range has the same knots and degree (at
+            # most 32 knots), so a warp finds one knot span for all of them
+            sps = r['amp_splines'] + r['logvar_splines']
+            shared = int(len(sps[0]['t']) <= 32 and
+                         all(np.array_equal(sp['t'], sps[0]['t']) and sp['k'] == sps[0]['k']
+                             for sp in sps))
+            rinfo.append([r['K'], a0, v0, shared])
         core = add_spline(S['core_spline'])
         exp_m, dev_m = profiles.exp_mixture(), profiles.dev_mixture()
         arrays = dict(
@@ -124,14 +130,28 @@ class FourierGalaxyRenderer(object):
             self._scratch[n] = (items, camp, cvar, flags, misc)
         return self._scratch[n]
 
+    METHODS = ('fused', 'persistent', 'split')
+
     def render_device(self, srcs, n, out, stream=None, method=None):
         """Renders n sources whose GALAXY_SRC records are in device tensor
-        `srcs` (uint8 view) into float32 device tensor `out`.  Two kernel
-        launches; nothing is copied to or from the host.  Returns the flags
-        tensor (see tb_galaxy_fft_prep)."""
+        `srcs` (uint8 view) into float32 device tensor `out`; nothing is
+        copied to or from the host.  method: 'fused' (tb_galaxy_fft_render:
+        preparation and render in one persistent launch), 'persistent' or
+        'split' (tb_galaxy_fft_prep, then tb_fourier_render /
+        tb_fourier_render_split); None: the method autotune chose, else
+        'fused'.  Returns the flags tensor (see tb_galaxy_fft_prep)."""
         lib = _lib.load()
         items, camp, cvar, flags, misc = self._work(n)
         s = _lib.stream_ptr(stream)
+        method = method or getattr(self, 'method', None) or 'fused'
+        if method == 'fused':
+            rc = lib.tb_galaxy_fft_render(srcs.data_ptr(), n, ctypes.addressof(self.image),
+                                          ctypes.addressof(self.tables.struct),
+                                          self.spec.data_ptr(), out.data_ptr(), items.data_ptr(),
+                                          flags.data_ptr(), misc.data_ptr(), misc.data_ptr() + 16,
+                                          s)
+            _lib.check(rc, 'tb_galaxy_fft_render')
+            return flags
         rc = lib.tb_galaxy_fft_prep(srcs.data_ptr(), n, ctypes.addressof(self.image),
                                     ctypes.addressof(self.tables.struct), items.data_ptr(),
                                     camp.data_ptr(), cvar.data_ptr(), COMP_STRIDE,
@@ -143,17 +163,33 @@ class FourierGalaxyRenderer(object):
         return flags
 
     def autotune(self, srcs, n, out):
-        """Times both Fourier methods on these device records and makes the
-        faster the device's default (render.autotune_fourier)."""
-        return render.autotune_fourier(lambda m: self.render_device(srcs, n, out, method=m))
+        """Times the three methods on these device records (CUDA events,
+        after a warm-up each) and keeps the fastest as this renderer's
+        method; returns {method: ms}."""
+        times = {}
+        for m in self.METHODS:
+            self.render_device(srcs, n, out, method=m)
+            ts = []
+            for _ in range(5):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                self.render_device(srcs, n, out, method=m)
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            times[m] = float(np.median(ts))
+        self.method = min(times, key=times.get)
+        return times
 
     def status(self, n):
         return self._work(n)[4][4:8]
 
-    def render(self, srcs_host, out_host=None, stream=None):
+    def render(self, srcs_host, out_host=None, stream=None, method=None):
         """End-to-end call with host buffers: copies the GALAXY_SRC records
-        to the device, renders, and copies the patches back into `out_host`
-        (pinned float32, allocated if None).  Returns (out_host, flags)."""
+        to the device, renders (render_device's `method`), and copies the
+        patches back into `out_host` (pinned float32, allocated if None).
+        Returns (out_host, flags)."""
         srcs_host = np.ascontiguousarray(srcs_host, dtype=GALAXY_SRC)
         n = len(srcs_host)
         nout = int((srcs_host['out_off'] + srcs_host['mw'].astype(np.int64) * srcs_host['mh']).max())
@@ -163,7 +199,7 @@ class FourierGalaxyRenderer(object):
         src_pinned = torch.from_numpy(srcs_host.view(np.uint8)).pin_memory()
         d_src = src_pinned.to(dev, non_blocking=True)
         out = torch.empty(nout, dtype=torch.float32, device=dev)
-        flags = self.render_device(d_src, n, out, stream)
+        flags = self.render_device(d_src, n, out, stream, method=method)
         out_host.copy_(out, non_blocking=True)
         flags_host = flags.to('cpu', non_blocking=True)
         torch.cuda.current_stream().synchronize()

@@ -29,6 +29,7 @@
 // Windows taller than the row buffer are processed in row chunks (the column
 // pass is repeated per chunk).
 #include "fft16.cuh"
+#include "galaxy_geom.cuh"
 
 namespace {
 
@@ -649,16 +650,8 @@ __device__ void render_item(const tb_fft_item& it, int K, const float* __restric
     else render_item_spatial<N, kDeriv>(it, K, spec, out, sh, N == 256 ? kRmax256 : N + 6, dot);
 }
 
-template <bool kDeriv>
-__global__ void __launch_bounds__(kThreads, 1)
-fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
-                      const double* __restrict__ amp, const double* __restrict__ var,
-                      const double* __restrict__ dcoef, const float* __restrict__ psf_spec,
-                      float* __restrict__ out, double* __restrict__ dots, int32_t* counter,
-                      tb_status* st, const int32_t* __restrict__ list = nullptr,
-                      const int32_t* __restrict__ list_count = nullptr) {
-    // `list` (optional): render only items list[0 .. *list_count)
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// Shared-memory carve-up of the persistent kernels.
+__device__ __forceinline__ Shared carve_shared(unsigned char* smem_raw) {
     Shared sh;
     unsigned char* p = smem_raw;
     sh.tw = reinterpret_cast<float2*>(p);
@@ -680,6 +673,72 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
     sh.gsp = reinterpret_cast<float*>(p);
     p += 2 * 256 * 4;
     sh.tw16 = reinterpret_cast<float2*>(p);
+    return sh;
+}
+
+// The rest of one item once its components (and derivative coefficients)
+// are in shared memory: taps, twiddles for its FFT size, the render, and
+// for TB_FFT_DOT the item's dot product.  Called by the whole block.
+template <bool kDeriv>
+__device__ void render_staged_item(const tb_fft_item& it, int K,
+                                   const float* __restrict__ psf_spec, float* __restrict__ out,
+                                   double* __restrict__ dots, Shared& sh, int& cur_n) {
+    const int N = it.sz;
+    if (threadIdx.x >= 32 && threadIdx.x < 64)
+        taps_warp(it.mux, kDeriv && it.dmode == TB_FFT_DX, sh.taps);
+    if (threadIdx.x >= 64 && threadIdx.x < 96)
+        taps_warp(it.muy, kDeriv && it.dmode == TB_FFT_DY, sh.taps + 7);
+    __syncthreads();
+    if (cur_n != N) {
+        __syncthreads();
+        switch (N) {
+            case 256:
+                tb::build_twiddles<256>(sh.tw);
+                tb::build_r16_twiddles(sh.tw16);
+                break;
+            case 128: tb::build_twiddles<128>(sh.tw); break;
+            case 64: tb::build_twiddles<64>(sh.tw); break;
+            default: tb::build_twiddles<32>(sh.tw); break;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) cur_n = N;
+    }
+    __syncthreads();
+    const float* spec = psf_spec + it.spec_off;
+    float dot = 0.f;
+    switch (N) {
+        case 256: render_item<256, kDeriv>(it, K, spec, out, sh, dot); break;
+        case 128: render_item<128, kDeriv>(it, K, spec, out, sh, dot); break;
+        case 64: render_item<64, kDeriv>(it, K, spec, out, sh, dot); break;
+        default: render_item<32, kDeriv>(it, K, spec, out, sh, dot); break;
+    }
+    if (kDeriv && it.mode == TB_FFT_DOT) {
+        // fixed-order block reduction of the item's dot product
+        __shared__ double red[kWarps];
+        double dd = (double)dot;
+        for (int o = 16; o > 0; o >>= 1) dd += __shfl_xor_sync(0xffffffffu, dd, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dd;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s2 = 0.0;
+            for (int w = 0; w < kWarps; w++) s2 += red[w];
+            dots[it.dot_off] = s2;
+        }
+        __syncthreads();
+    }
+}
+
+template <bool kDeriv>
+__global__ void __launch_bounds__(kThreads, 1)
+fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
+                      const double* __restrict__ amp, const double* __restrict__ var,
+                      const double* __restrict__ dcoef, const float* __restrict__ psf_spec,
+                      float* __restrict__ out, double* __restrict__ dots, int32_t* counter,
+                      tb_status* st, const int32_t* __restrict__ list = nullptr,
+                      const int32_t* __restrict__ list_count = nullptr) {
+    // `list` (optional): render only items list[0 .. *list_count)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Shared sh = carve_shared(smem_raw);
     __shared__ int64_t slot;
     __shared__ int cur_n;
     if (threadIdx.x == 0) cur_n = 0;
@@ -724,48 +783,53 @@ fourier_render_kernel(const tb_fft_item* __restrict__ items, int n_items,
                                           (float)(n2 * 2.0 * dc[2]), (float)(n2 * dc[3]));
             }
         }
-        if (threadIdx.x >= 32 && threadIdx.x < 64)
-            taps_warp(it.mux, kDeriv && it.dmode == TB_FFT_DX, sh.taps);
-        if (threadIdx.x >= 64 && threadIdx.x < 96)
-            taps_warp(it.muy, kDeriv && it.dmode == TB_FFT_DY, sh.taps + 7);
-        __syncthreads();
-        if (cur_n != N) {
-            __syncthreads();
-            switch (N) {
-                case 256:
-                    tb::build_twiddles<256>(sh.tw);
-                    tb::build_r16_twiddles(sh.tw16);
-                    break;
-                case 128: tb::build_twiddles<128>(sh.tw); break;
-                case 64: tb::build_twiddles<64>(sh.tw); break;
-                default: tb::build_twiddles<32>(sh.tw); break;
+        render_staged_item<kDeriv>(it, K, psf_spec, out, dots, sh, cur_n);
+    }
+}
+
+// Fused preparation and render (tb_galaxy_fft_render): the persistent
+// kernel taking galaxy source records instead of prepared items.  For each
+// source warp 0 does the prep kernel's work (tb::prep_galaxy_warp: profile,
+// shape, geometry) straight into shared memory -- the FP32 exponent
+// coefficients from the same FP64 products the two-launch path writes and
+// reads back, so both paths render the same item bit for bit -- then the
+// block renders it.  One launch per batch instead of two, and no component
+// tables in global memory.
+__global__ void __launch_bounds__(kThreads, 1)
+galaxy_fft_render_kernel(const tb_galaxy_src* __restrict__ srcs, int n, tb_fft_image img,
+                         tb_profile_tables T, const float* __restrict__ psf_spec,
+                         float* __restrict__ out, tb_fft_item* __restrict__ items,
+                         int32_t* __restrict__ flags, int32_t* counter) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Shared sh = carve_shared(smem_raw);
+    __shared__ int64_t slot;
+    __shared__ int cur_n;
+    __shared__ tb_fft_item item;
+    if (threadIdx.x == 0) cur_n = 0;
+    for (;;) {
+        const int64_t u = tb::next_unit(counter, &slot);
+        if (u >= n) break;
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            const tb_galaxy_src s = srcs[u];
+            double a, v, M[3];
+            int rank, flag;
+            tb_fft_item it;
+            const int K = tb::prep_galaxy_warp(s, img, T, lane, a, v, rank, M, flag, it);
+            if (flag == 0 && lane < K) {
+                const double c2 = -2.0 * TB_PI * TB_PI * TB_LOG2E;
+                sh.comp[rank] = make_float4((float)a, (float)(c2 * (v * M[0])),
+                                            (float)(c2 * 2.0 * (v * M[1])),
+                                            (float)(c2 * (v * M[2])));
             }
-            __syncthreads();
-            if (threadIdx.x == 0) cur_n = N;
+            if (lane == 0) {
+                item = it;
+                if (items) items[u] = it;
+                flags[u] = flag;
+            }
         }
         __syncthreads();
-        const float* spec = psf_spec + it.spec_off;
-        float dot = 0.f;
-        switch (N) {
-            case 256: render_item<256, kDeriv>(it, K, spec, out, sh, dot); break;
-            case 128: render_item<128, kDeriv>(it, K, spec, out, sh, dot); break;
-            case 64: render_item<64, kDeriv>(it, K, spec, out, sh, dot); break;
-            default: render_item<32, kDeriv>(it, K, spec, out, sh, dot); break;
-        }
-        if (kDeriv && it.mode == TB_FFT_DOT) {
-            // fixed-order block reduction of the item's dot product
-            __shared__ double red[kWarps];
-            double dd = (double)dot;
-            for (int o = 16; o > 0; o >>= 1) dd += __shfl_xor_sync(0xffffffffu, dd, o);
-            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dd;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double s2 = 0.0;
-                for (int w = 0; w < kWarps; w++) s2 += red[w];
-                dots[it.dot_off] = s2;
-            }
-            __syncthreads();
-        }
+        render_staged_item<false>(item, item.K, psf_spec, out, nullptr, sh, cur_n);
     }
 }
 
@@ -1159,6 +1223,28 @@ extern "C" int tb_fourier_render_deriv(const tb_fft_item* items, int32_t n_items
                                        tb_status* status, void* stream) {
     return launch_fourier(items, n_items, comp_amp, comp_var, comp_dcoef, psf_spec, out, dots,
                           work_counter, status, stream);
+}
+
+extern "C" int tb_galaxy_fft_render(const tb_galaxy_src* srcs, int32_t n,
+                                    const tb_fft_image* image, const tb_profile_tables* tables,
+                                    const float* psf_spec, float* out, tb_fft_item* items,
+                                    int32_t* flags, int32_t* work_counter, tb_status* status,
+                                    void* stream) {
+    if (n < 0) return TB_ERR_ARG;
+    if (n == 0) return TB_OK;
+    if (!srcs || !image || !tables || !psf_spec || !out || !flags || !work_counter)
+        return TB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaFuncSetAttribute(galaxy_fft_render_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSmemBytes) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    if (cudaMemsetAsync(work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return TB_ERR_LAUNCH;
+    if (status && cudaMemsetAsync(status, 0, sizeof(tb_status), s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    const int grid = n < tb::num_sms() ? n : tb::num_sms();
+    galaxy_fft_render_kernel<<<grid, kThreads, kSmemBytes, s>>>(srcs, n, *image, *tables, psf_spec,
+                                                                out, items, flags, work_counter);
+    return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
 }
 
 namespace {

@@ -15,22 +15,16 @@
 
 namespace tb {
 
-// B-spline value of spline s at x (FITPACK knots / coefficients, degree
-// 1..3), by de Boor's recursion with the knot span clamped to the table.
-__device__ inline double bspline(const tb_profile_tables& T, int s, double x) {
-    const int to = T.spline_info[4 * s], nt = T.spline_info[4 * s + 1];
-    const int co = T.spline_info[4 * s + 2], k = T.spline_info[4 * s + 3];
-    const double* t = T.knots + to;
-    const double* c = T.coefs + co;
-    const int n = nt - k - 1;
-    // knot span l: t[l] <= x < t[l+1], clamped to [k, n-1]
-    int l = k;
-    while (l + 1 < n && t[l + 1] <= x) l++;
-    // d_j <- (1 - a) d_{j-1} + a d_j, a = (x - t_i) / (t_{i+k+1-r} - t_i),
-    // i = j + l - k, for r = 1..k and j = k..r.
+// De Boor's recursion for a B-spline of degree k (1..3) with coefficients c
+// at x, given its knot span l and the knots around it: tk[j] = t[l - k + 1
+// + j], j = 0 .. 2k - 1.
+//   d_j <- (1 - a) d_{j-1} + a d_j, a = (x - t_i) / (t_{i+k+1-r} - t_i),
+//   i = j + l - k, for r = 1..k and j = k..r.
+__device__ inline double deboor(const double* c, const double* tk, int k, int l, double x) {
+    auto t = [&](int i) { return tk[i - (l - k + 1)]; };
     auto blend = [&](double lo, double hi, int i, int r) {
-        const double den = t[i + k + 1 - r] - t[i];
-        const double a = den == 0.0 ? 0.0 : (x - t[i]) / den;
+        const double den = t(i + k + 1 - r) - t(i);
+        const double a = den == 0.0 ? 0.0 : (x - t(i)) / den;
         return (1.0 - a) * lo + a * hi;
     };
     if (k == 3) {
@@ -52,6 +46,55 @@ __device__ inline double bspline(const tb_profile_tables& T, int s, double x) {
     }
     if (k == 1) return blend(c[l - 1], c[l], l, 1);
     return c[l];
+}
+
+// B-spline value of spline s at x (FITPACK knots / coefficients, degree
+// 1..3), by de Boor's recursion with the knot span clamped to the table.
+__device__ inline double bspline(const tb_profile_tables& T, int s, double x) {
+    const int to = T.spline_info[4 * s], nt = T.spline_info[4 * s + 1];
+    const int co = T.spline_info[4 * s + 2], k = T.spline_info[4 * s + 3];
+    const double* t = T.knots + to;
+    const int n = nt - k - 1;
+    // knot span l: t[l] <= x < t[l+1], clamped to [k, n-1] -- the largest
+    // j in (k, n-1] with t[j] <= x, else k (knots are non-decreasing), by
+    // bisection: a few dependent loads instead of one per knot
+    int l = k, hi = n - 1;
+    while (l < hi) {
+        const int mid = (l + hi + 1) >> 1;
+        if (t[mid] <= x) l = mid;
+        else hi = mid - 1;
+    }
+    double tk[6];
+    for (int j = 0; j < 2 * k; j++) tk[j] = t[l - k + 1 + j];
+    return deboor(T.coefs + co, tk, k, l, x);
+}
+
+// The knot span of x in a knot vector of nt <= 32 knots and degree k,
+// found by the whole warp at once: lane j holds t[j]; the span is the
+// largest j in (k, nt - k - 2] with t[j] <= x, else k (as bspline's
+// search), and every lane receives the 2k knots around it in tk.  All 32
+// lanes must call this together.
+__device__ inline int warp_knot_span(const double* t, int nt, int k, double x, double* tk) {
+    const int j = (int)(threadIdx.x & 31);
+    const double tj = j < nt ? t[j] : 0.0;
+    const int n = nt - k - 1;
+    const unsigned m = __ballot_sync(0xffffffffu, j >= k + 1 && j <= n - 1 && tj <= x);
+    const int l = m ? 31 - __clz((int)m) : k;
+    for (int q = 0; q < 2 * k; q++) tk[q] = __shfl_sync(0xffffffffu, tj, l - k + 1 + q);
+    return l;
+}
+
+// bspline() of one spline evaluated by the whole warp (all lanes get the
+// value): the knot span by warp_knot_span when the spline has at most 32
+// knots.  All 32 lanes must call this together.
+__device__ inline double warp_bspline(const tb_profile_tables& T, int s, double x) {
+    const int nt = T.spline_info[4 * s + 1];
+    if (nt > 32) return bspline(T, s, x);
+    const int to = T.spline_info[4 * s], co = T.spline_info[4 * s + 2];
+    const int k = T.spline_info[4 * s + 3];
+    double tk[6];
+    const int l = warp_knot_span(T.knots + to, nt, k, x, tk);
+    return deboor(T.coefs + co, tk, k, l, x);
 }
 
 // Radius of a profile in units of r_e beyond which the reference treats a
@@ -141,21 +184,38 @@ __device__ inline int warp_profile(const tb_profile_tables& T, int profile, doub
     if (nn <= lowest) { r = 0; nn = lowest; }
     else if (nn >= highest) { r = T.n_ranges - 1; nn = highest; }
     else {
-        for (int q = 0; q < T.n_ranges; q++)
-            if (T.range_lohi[2 * q] <= nn && nn < T.range_lohi[2 * q + 1]) { r = q; break; }
+        // the first range holding nn: lane q tests range q (one round of loads)
+        for (int q0 = 0; q0 < T.n_ranges && r < 0; q0 += 32) {
+            const int q = q0 + (int)(threadIdx.x & 31);
+            const bool in = q < T.n_ranges && T.range_lohi[2 * q] <= nn &&
+                            nn < T.range_lohi[2 * q + 1];
+            const unsigned m = __ballot_sync(0xffffffffu, in);
+            if (m) r = q0 + __ffs(m) - 1;
+        }
     }
     if (r < 0) return -1;
     const int Kr = T.range_info[4 * r], sa = T.range_info[4 * r + 1];
     const int sv = T.range_info[4 * r + 2];
     if (Kr + 1 > max_k) return -1;
-    if (lane < Kr) {
+    if (T.range_info[4 * r + 3] == 1) {
+        // every spline of the range has spline sa's knots (<= 32 of them):
+        // one knot span for the warp, then each lane's coefficients
+        const int to = T.spline_info[4 * sa], nt = T.spline_info[4 * sa + 1];
+        const int kd = T.spline_info[4 * sa + 3];
+        double tk[6];
+        const int l = warp_knot_span(T.knots + to, nt, kd, nn, tk);
+        if (lane < Kr) {
+            a = deboor(T.coefs + T.spline_info[4 * (sa + lane) + 2], tk, kd, l, nn);
+            v = exp(deboor(T.coefs + T.spline_info[4 * (sv + lane) + 2], tk, kd, l, nn));
+        }
+    } else if (lane < Kr) {
         a = bspline(T, sa + lane, nn);
         v = exp(bspline(T, sv + lane, nn));
     }
     a /= lane_sum(a, Kr);
     int K = Kr;
     if (nn > 1.0) {
-        const double core = bspline(T, T.core_spline, nn);
+        const double core = warp_bspline(T, T.core_spline, nn);
         a *= (1.0 - core) / lane_sum(a, Kr);
         if (lane == Kr) { a = core; v = 0.0; }
         K = Kr + 1;
