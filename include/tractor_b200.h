@@ -334,6 +334,22 @@ int tb_galaxy_fft_prep(const tb_galaxy_src* srcs, int32_t n, const tb_fft_image*
                        double* comp_amp, double* comp_var, int32_t comp_stride,
                        int32_t* flags, void* stream);
 
+/* Mixture spectrum times PSF spectrum on the full sz x (sz/2 + 1) rfft grid,
+ * for Fourier-path galaxies whose FFT size exceeds 256 (tb_fourier_render's
+ * limit): out[w][v] (row-major, interleaved complex64: the input of an
+ * inverse 2-D real FFT) = psf_spec[v][w] (column-major, as
+ * tb_psf_spectrum writes it) x sum_k amp_k exp(-2 pi^2 f^T var_k f),
+ * f = (v, fftfreq(w)) / sz; with comp_dcoef (K rows of a'_k - a_k, dC00,
+ * dC01, dC11; may be NULL) the difference of the two mixtures as
+ * TB_FFT_DIFF items render it.  K <= 128.  Replaces
+ * MixtureOfGaussians.getFourierTransform(v, w, zero_mean=True) times P in
+ * ProfileGalaxy._realGetUnitFluxModelPatch (tractor/galaxy.py:457-470,
+ * tractor/mp_fourier.i:405-430); the caller runs the inverse transform, the
+ * Lanczos-3 shift (tb_lanczos3_shift) and the crop. */
+int tb_fourier_spectrum_grid(const double* comp_amp, const double* comp_var,
+                             const double* comp_dcoef, int32_t K, const float* psf_spec,
+                             int32_t sz, float* out, void* stream);
+
 /* tb_galaxy_fft_prep and tb_fourier_render in one persistent launch: each
  * source is prepared (as tb_galaxy_fft_prep) by one warp straight into
  * shared memory and rendered (as tb_fourier_render) by its block, so no

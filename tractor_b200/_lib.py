@@ -124,6 +124,7 @@ SIGNATURES = {
     'tb_chi2': (_I32, [_P, _P, _P, _P, _P, _I32, _P, _P]),
     'tb_galaxy_fft_prep': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _I32, _P, _P]),
     'tb_galaxy_fft_render': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    'tb_fourier_spectrum_grid': (_I32, [_P, _P, _P, _I32, _P, _I32, _P, _P]),
     'tb_galaxy_fft_jac_prep': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _I32, _I32, _I64, _P,
                                       _P]),
     'tb_fourier_render_deriv': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),

@@ -11,7 +11,7 @@ LIB = os.path.join(HERE, 'libtractor_b200.so')
 INCLUDE = os.path.join(ROOT, 'include')
 
 SOURCES = ['mog_render.cu', 'lanczos.cu', 'fourier_render.cu', 'galaxy_prep.cu', 'lsq.cu',
-           'scene_render.cu', 'blob_fit.cu', 'emfit.cu', 'blobs.cu']
+           'scene_render.cu', 'blob_fit.cu', 'emfit.cu', 'blobs.cu', 'fourier_large.cu']
 NVCC_FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-lineinfo', '-O3',
               '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr']
 

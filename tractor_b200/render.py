@@ -338,9 +338,19 @@ class PsfSpectra(object):
 
     def compute(self, img, sz, normalize=False):
         """(device spectrum tensor, cx, cy) of `img` at FFT size sz, not cached
-        (position-dependent PSFs)."""
+        (position-dependent PSFs).  Sizes above 256 (beyond tb_psf_spectrum)
+        are transformed in FP64 by cuFFT and rounded to complex64, as the
+        reference's np.fft.rfft2 + astype(complex64), into the same
+        column-major layout."""
         lib = _lib.load()
         dev = device()
+        if sz > 256:
+            pad, cx, cy = self.pad(img, sz)
+            P = torch.fft.rfft2(torch.from_numpy(pad.astype(np.float64)).to(dev))
+            if normalize:
+                P = P / torch.abs(P[0, 0])
+            P = P.to(torch.complex64).transpose(0, 1).contiguous()   # [v][w]
+            return (torch.view_as_real(P).reshape(-1), cx, cy)
         pad, cx, cy = self.pad(img, sz)
         dpad = torch.from_numpy(pad).to(dev)
         spec = torch.empty(sz * (sz // 2 + 1) * 2, dtype=torch.float32, device=dev)
@@ -374,9 +384,10 @@ class FftBatch(object):
         self.nout = 0
         self.dcoef = []
         self.ndc = 0
+        self.large = []          # items above FFT size 256 (run_large)
 
     def __len__(self):
-        return len(self.items)
+        return len(self.items) + len(self.large)
 
     def add(self, amp, var, sz, spec_key, spec, mw, mh, sx, sy, mux, muy, scale=1.,
             out_off=None, ldo=0, mode=MOG_STORE, diff=None):
@@ -388,11 +399,27 @@ class FftBatch(object):
         K = len(amp)
         if K > 128:
             raise ValueError('at most 128 components per galaxy (got %d)' % K)
-        if sz not in (32, 64, 128, 256):
-            raise ValueError('FFT size %d not supported (32..256)' % sz)
+        if sz < 32 or sz > LARGE_FFT_MAX or (sz & (sz - 1)) != 0:
+            raise ValueError('FFT size %d not supported (powers of two, 32..%d)'
+                             % (sz, LARGE_FFT_MAX))
         if out_off is None:
             out_off = self.nout
             self.nout += mw * mh
+        if sz > 256:
+            # beyond the fused renderer: run_large's spectrum grid + cuFFT
+            dc = None
+            var2 = np.array(var, np.float64).reshape(K, 2, 2)
+            if diff is not None:
+                amp2 = np.array(diff[0], np.float64).ravel()
+                if len(amp2) != K:
+                    raise ValueError('a difference item needs two mixtures of one size')
+                dv = np.array(diff[1], np.float64).reshape(K, 2, 2) - var2
+                dc = np.stack([amp2 - amp, dv[:, 0, 0], 0.5 * (dv[:, 0, 1] + dv[:, 1, 0]),
+                               dv[:, 1, 1]], axis=1)
+            self.large.append((amp, var2, dc, int(sz), spec, int(mw), int(mh), int(sx), int(sy),
+                               float(mux), float(muy), float(scale), int(out_off), int(ldo),
+                               int(mode)))
+            return out_off
         key = (sz, spec_key)
         if key not in self.spec_off:
             self.spec_off[key] = self.nspec
@@ -424,7 +451,12 @@ class FftBatch(object):
         self.status_in_out = out is None
         if out is None:
             out = torch.empty(max(self.nout, 1) + 4, dtype=torch.float32, device=dev)
+        if self.large:
+            self.run_large(out, stream)
         if not self.items:
+            if self.status_in_out:
+                out[-4:].zero_()
+            self.status = out[-4:].view(torch.uint8) if self.status_in_out else None
             return out
         items = np.array(self.items, dtype=_lib.FFT_ITEM)
         specs = torch.cat(self.spec_list) if len(self.spec_list) > 1 else self.spec_list[0]
@@ -447,6 +479,54 @@ class FftBatch(object):
             check_status(self.status, 'tb_fourier_render')
         return out
 
+
+    def run_large(self, out, stream=None):
+        """Items whose FFT size exceeds 256 (ProfileGalaxy's FFT branch,
+        tractor/galaxy.py:457-519, for galaxies with a half-size above 128):
+        the mixture spectrum times the PSF spectrum on the full rfft grid
+        (tb_fourier_spectrum_grid), the inverse 2-D real transform as irfftn
+        does it (a complex inverse FFT along w, the DC and Nyquist columns'
+        imaginary parts dropped, a real inverse FFT along v; cuFFT), the
+        Lanczos-3 shift of the whole sz x sz image with zero edges
+        (tb_lanczos3_shift, the reference's lanczos_shift_image), then the
+        integer shift and crop into the item's rectangle of `out`."""
+        lib = _lib.load()
+        dev = out.device
+        s = _lib.stream_ptr(stream)
+        for (amp, var, dc, N, spec, mw, mh, sx, sy, mux, muy, scale, off, ldo,
+             mode) in self.large:
+            K = len(amp)
+            NH = N // 2 + 1
+            a_d = torch.as_tensor(amp, device=dev)
+            v_d = torch.as_tensor(var.reshape(K, 4), device=dev)
+            dc_d = None if dc is None else torch.as_tensor(dc, device=dev)
+            S = torch.empty(N * NH * 2, dtype=torch.float32, device=dev)
+            rc = lib.tb_fourier_spectrum_grid(a_d.data_ptr() if K else None,
+                                              v_d.data_ptr() if K else None,
+                                              None if dc_d is None else dc_d.data_ptr(), K,
+                                              spec.data_ptr(), N, S.data_ptr(), s)
+            _lib.check(rc, 'tb_fourier_spectrum_grid')
+            G1 = torch.fft.ifft(torch.view_as_complex(S.view(N, NH, 2)), dim=0)
+            G1[:, 0].imag.zero_()
+            G1[:, N // 2].imag.zero_()
+            G = torch.fft.irfft(G1, n=N, dim=1).to(torch.float32)
+            if mux != 0. or muy != 0.:
+                G = lanczos_shift(G[None], [(mux, muy)], stream=stream)[0]
+            ld = ldo if ldo > 0 else mw
+            view = out[off:off + (mh - 1) * ld + mw].as_strided((mh, mw), (ld, 1))
+            gr0, gr1 = max(0, -sy), min(N, mh - sy)
+            gc0, gc1 = max(0, -sx), min(N, mw - sx)
+            if mode == _lib.MOG_STORE:
+                view.zero_()
+            if gr0 < gr1 and gc0 < gc1:
+                blk = G[gr0:gr1, gc0:gc1] * scale
+                if mode == _lib.MOG_STORE:
+                    view[gr0 + sy:gr1 + sy, gc0 + sx:gc1 + sx] = blk
+                else:
+                    view[gr0 + sy:gr1 + sy, gc0 + sx:gc1 + sx] += blk
+
+
+LARGE_FFT_MAX = 8192     # the reference warns above a half-size of 4096 (galaxy.py:376)
 
 _fourier_ws = {}
 

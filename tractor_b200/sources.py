@@ -10,7 +10,7 @@ Tractor-level calls batch all sources into one launch per kernel.
 """
 import numpy as np
 
-from . import profiles
+from . import profiles, render
 from .params import MultiParams, ScalarParam
 from .patch import Patch, ModelMask, add_patches, get_overlapping_region
 from .plan import RenderPlan, Pending, NONE, done
@@ -514,8 +514,9 @@ class ProfileGalaxy(object):
         else:
             halfsize = self._getUnitFluxPatchSize(img, px=px, py=py, minval=minval)
         sz = psf.getFourierTransformSize(halfsize)
-        if sz > 256:
-            raise NotImplementedError('Fourier-path patch size %d above the supported 256' % sz)
+        if sz > render.LARGE_FFT_MAX:
+            raise NotImplementedError('Fourier-path patch size %d above the supported %d'
+                                      % (sz, render.LARGE_FFT_MAX))
         spec_key, spec, cx, cy = psf.fourier_spectrum(px, py, sz)
         pH = pW = sz
         dx = px - cx
