@@ -750,6 +750,19 @@ int tb_em_fit_2d(const double* img, int32_t n, int32_t ny, int32_t nx, const int
                  double* amp, double* mean, double* var, int32_t K, double alpha,
                  int32_t steps, int32_t* status, void* stream);
 
+/* The EM fit with a flat sky term, em_fit_2d_reg2 (tractor/emfit2.c), that
+ * GaussianMixturePSF.fromStamp(v2=True) runs (tractor/psf.py:579-588), in
+ * the layout of tb_em_fit_2d.  Pixels at or below zero count toward the sky
+ * only; a component's responsibility is cut where its squared Mahalanobis
+ * distance reaches -2 log(approx sqrt((2 pi)^2 det C)) (approx > 0);
+ * second moments are taken about the previous iteration's mean, as the
+ * reference accumulates them.  skyamp[s] (optional) receives the fit's
+ * final sky level per pixel (the reference's skyamp output). */
+int tb_em_fit_2d_sky(const double* img, int32_t n, int32_t ny, int32_t nx, const int32_t* xy0,
+                     double* amp, double* mean, double* var, int32_t K, double alpha,
+                     int32_t steps, double approx, double* skyamp, int32_t* status,
+                     void* stream);
+
 /* Blob segmentation for callers that cut images into blobs before
  * Tractor.setModelMasks / the batched fitter (the callers of
  * tractor/engine.py:341-361).  tb_label_components labels the connected

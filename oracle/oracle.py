@@ -812,6 +812,73 @@ def sersic_fft_model_f64(theta, psf_img, mask_x0, mask_y0, mw, mh, shape='E'):
 # EM fit of a Gaussian mixture to an image (tractor/emfit.i)
 # ---------------------------------------------------------------------------
 
+def em_fit_2d_reg2(img, x0, y0, amp, mean, var, alpha, steps, approx):
+    """em_fit_2d_reg2 (tractor/emfit2.c:1-298): EM with a flat sky term,
+    vectorised over pixels.  Each step: per component the symmetrised
+    covariance's determinant (a non-positive one returns -1), its inverse,
+    amp / sqrt((2 pi)^2 det) and the cut maxD = -2 log(approx sqrt((2 pi)^2
+    det)) (emfit2.c:144-166); per pixel: a pixel <= 0 adds |img| to the sky
+    and takes no part; z_k = 0 where dsq >= maxD_k; a pixel whose z sum to 0
+    adds img to the sky; otherwise the sky's level psky joins the sum and
+    img psky / sum goes to the sky, and w_k = img z_k / sum (emfit2.c:
+    184-236); then mean = sum w x / sum w, covariance = (alpha I + sum w
+    (x - old mean)(x - old mean)^T) / (sum w + alpha), amplitude = sum w,
+    and psky = sky sum / npix (emfit2.c:239-248).  psky starts at 0.01 x
+    the image mean.  amp / mean / var are updated in place; returns
+    (0 or -1, psky)."""
+    img = np.asarray(img, np.float64)
+    NY, NX = img.shape
+    K = len(amp)
+    iy, ix = np.mgrid[:NY, :NX]
+    x = (x0 + ix).ravel().astype(np.float64)
+    y = (y0 + iy).ravel().astype(np.float64)
+    I = img.ravel()
+    tpd = (2. * np.pi) ** 2
+    psky = 0.
+    pos = I > 0
+    for step in range(steps):
+        if step == 0:
+            psky = 0.01 * I.sum() / (NX * NY)
+        V = var.reshape(K, 4)
+        v12 = (V[:, 1] + V[:, 2]) / 2.
+        det = V[:, 0] * V[:, 3] - v12 * v12
+        if np.any(det <= 0.):
+            return -1, psky
+        iv0, iv1, iv3 = V[:, 3] / det, -2. * v12 / det, V[:, 0] / det
+        scale = amp / np.sqrt(tpd * det)
+        maxD = np.log(approx * np.sqrt(tpd * det)) / -0.5
+        dx = x[None, :] - mean[:, 0:1]
+        dy = y[None, :] - mean[:, 1:2]
+        dsq = iv0[:, None] * dx * dx + iv1[:, None] * dx * dy + iv3[:, None] * dy * dy
+        Z = np.where(dsq >= maxD[:, None], 0.,
+                     scale[:, None] * np.exp(-0.5 * np.where(dsq >= maxD[:, None], 0., dsq)))
+        zsum = np.zeros_like(I)
+        for k in range(K):
+            zsum = zsum + Z[k]
+        used = pos & (zsum != 0)
+        sky = np.abs(I[~pos]).sum() + I[pos & (zsum == 0)].sum()
+        zs = zsum[used] + psky
+        sky += (I[used] * (psky / zs)).sum()
+        W = np.zeros((K, len(I)))
+        W[:, used] = I[used][None, :] * Z[:, used] / zs[None, :]
+        wsum = W.sum(axis=1)
+        sx = (W * x[None, :]).sum(axis=1)
+        sy = (W * y[None, :]).sum(axis=1)
+        vxx = alpha + (W * dx * dx).sum(axis=1)
+        vxy = (W * dx * dy).sum(axis=1)
+        vyy = alpha + (W * dy * dy).sum(axis=1)
+        mean[:, 0] = sx / wsum
+        mean[:, 1] = sy / wsum
+        den = wsum + alpha
+        var[:, 0, 0] = vxx / den
+        var[:, 0, 1] = vxy / den
+        var[:, 1, 0] = vxy / den
+        var[:, 1, 1] = vyy / den
+        amp[:] = wsum
+        psky = sky / (NX * NY)
+    return 0, psky
+
+
 def em_fit_2d_reg(img, x0, y0, amp, mean, var, alpha, steps):
     """em_fit_2d_reg (tractor/emfit.i:274-557), vectorised over pixels: each
     step computes C^-1 and amp / sqrt((2 pi)^2 det) (a non-positive

@@ -174,7 +174,18 @@ def _emfit_module():
         return lib.ref_em_fit_2d_reg(img, int(x0), int(y0), amp, mean, var, float(alpha),
                                      int(steps))
 
+    lib.ref_em_fit_2d_reg2.argtypes = [P, I, I, P, P, P, D, I, D, ctypes.POINTER(D)]
+    lib.ref_em_fit_2d_reg2.restype = I
+
+    def em_fit_2d_reg2(img, x0, y0, amp, mean, var, alpha, steps, approx):
+        # SWIG's double* OUTPUT: returns [status, skyamp]
+        sky = D(0.)
+        r = lib.ref_em_fit_2d_reg2(img, int(x0), int(y0), amp, mean, var, float(alpha),
+                                   int(steps), float(approx), ctypes.byref(sky))
+        return [r, sky.value]
+
     m.em_fit_2d_reg = em_fit_2d_reg
+    m.em_fit_2d_reg2 = em_fit_2d_reg2
     m._lib = lib
     return m
 

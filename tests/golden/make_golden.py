@@ -11,6 +11,7 @@ root in the development container:
     python tests/golden/make_golden.py hybrid   # hybrid_psf.npz
     python tests/golden/make_golden.py psfex    # psfex.npz
     python tests/golden/make_golden.py emfit    # emfit.npz
+    python tests/golden/make_golden.py emfitsky # emfit_sky.npz
     python tests/golden/make_golden.py psfderiv # psf_derivs.npz
     python tests/golden/make_golden.py forcedsky # forced_sky.npz
     python tests/golden/make_golden.py varying  # varying_psf.npz
@@ -472,6 +473,50 @@ def emfit():
     print('emfit fixture written to', OUT)
 
 
+def emfitsky():
+    """GaussianMixturePSF.fromStamp(v2=True) (psf.py:579-588) -- the EM fit
+    with a flat sky term, em_fit_2d_reg2 (emfit2.c), on the stamp as given --
+    on seeded stamps with a background and noise (pixels at or below zero
+    go to the sky), 1 to 3 components, with and without the alpha prior,
+    two approx cuts, default and explicit origins."""
+    from oracle import refharness
+    refharness.load()
+    from tractor.psf import GaussianMixturePSF
+    rng = np.random.default_rng(778)
+
+    def stamp(h, w, sig, bg, noise):
+        y, x = np.mgrid[:h, :w]
+        x = x - w // 2 + rng.uniform(-0.4, 0.4)
+        y = y - h // 2 + rng.uniform(-0.4, 0.4)
+        img = np.zeros((h, w))
+        for a, s in sig:
+            img += a * np.exp(-0.5 * (x ** 2 + y ** 2) / s ** 2) / (2 * np.pi * s ** 2)
+        return img + bg + rng.normal(0., noise, img.shape)
+
+    cases = [
+        # stamp, N, alpha, steps, approx, xy0
+        (stamp(25, 25, [(100., 1.5), (40., 3.5)], 0.05, 0.02), 2, 0., 300, 1e-30, None),
+        (stamp(31, 27, [(80., 1.2), (30., 2.5), (10., 6.)], 0.02, 0.01), 3, 0., 500, 1e-30,
+         None),
+        (stamp(21, 21, [(50., 2.0)], 0.1, 0.05), 1, 0.5, 200, 1e-30, (-10, -10)),
+        (stamp(25, 25, [(100., 1.5), (40., 3.5)], 0.0, 0.03), 2, 0.1, 400, 1e-12, None),
+    ]
+    arrays = {}
+    for i, (st, N, alpha, steps, approx, xy0) in enumerate(cases):
+        psf, sky = GaussianMixturePSF.fromStamp(st, N=N, xy0=xy0, alpha=alpha, emsteps=steps,
+                                                v2=True, approx=approx)
+        arrays['stamp%d' % i] = st
+        arrays['cfg%d' % i] = np.array([N, alpha, steps, approx, xy0 is not None,
+                                        0 if xy0 is None else xy0[0],
+                                        0 if xy0 is None else xy0[1]])
+        arrays['amp%d' % i] = psf.mog.amp
+        arrays['mean%d' % i] = psf.mog.mean
+        arrays['var%d' % i] = psf.mog.var
+        arrays['sky%d' % i] = np.array(sky)
+    np.savez_compressed(os.path.join(OUT, 'emfit_sky.npz'), n=len(cases), **arrays)
+    print('emfit_sky fixture written to', OUT)
+
+
 def psf_scene(tractor_mod, ellipse):
     """A 40 x 36 image with two point sources and an exp galaxy under a
     2-component MoG PSF (GaussianMixturePSF, or GaussianMixtureEllipsePSF
@@ -741,6 +786,8 @@ if __name__ == '__main__':
         psfex()
     elif sys.argv[1:] == ['emfit']:
         emfit()
+    elif sys.argv[1:] == ['emfitsky']:
+        emfitsky()
     elif sys.argv[1:] == ['psfderiv']:
         psfderiv()
     elif sys.argv[1:] == ['forcedsky']:

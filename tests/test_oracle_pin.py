@@ -223,3 +223,24 @@ def test_em_oracle_matches_live_reference(oracle):
         np.testing.assert_allclose(a2, amp, rtol=1e-11, atol=1e-14)
         np.testing.assert_allclose(m2, mean, rtol=0, atol=1e-10)
         np.testing.assert_allclose(v2, var, rtol=1e-11, atol=1e-13)
+
+
+def test_em_sky_oracle_matches_golden(oracle):
+    """The oracle's em_fit_2d_reg2 (EM with a flat sky term, emfit2.c)
+    against GaussianMixturePSF.fromStamp(v2=True) run by the reference
+    (emfit_sky.npz): the mixtures and the sky level."""
+    from tractor_b200.emfit import em_init_params
+    g = _golden('emfit_sky.npz')
+    for i in range(int(g['n'])):
+        N, alpha, steps, approx, hasxy, x0, y0 = g['cfg%d' % i]
+        st = g['stamp%d' % i]
+        h, w_ = st.shape
+        xm, ym = (int(x0), int(y0)) if hasxy else (-(w_ // 2), -(h // 2))
+        w, mu, var = em_init_params(int(N), None, None, None)
+        r, sky = oracle.em_fit_2d_reg2(st, xm, ym, w, mu, var, float(alpha), int(steps),
+                                       float(approx))
+        assert r == 0
+        np.testing.assert_allclose(w, g['amp%d' % i], rtol=1e-11)
+        np.testing.assert_allclose(mu, g['mean%d' % i], rtol=0, atol=1e-11)
+        np.testing.assert_allclose(var, g['var%d' % i], rtol=1e-11)
+        assert abs(sky - float(g['sky%d' % i])) <= 1e-11 * abs(float(g['sky%d' % i]))

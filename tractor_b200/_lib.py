@@ -116,6 +116,8 @@ SIGNATURES = {
     'tb_normal_equations': (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _I32, _P]),
     'tb_tensor_core_timeouts': (_I32, [_P]),
     'tb_em_fit_2d': (_I32, [_P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _D, _I32, _P, _P]),
+    'tb_em_fit_2d_sky': (_I32, [_P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _D, _I32, _D,
+                                 _P, _P, _P]),
     'tb_label_workspace_bytes': (ctypes.c_int64, [_I32, _I32]),
     'tb_label_components': (_I32, [_P, _I32, _I32, _I32, _P, _P, _P, _P, _P]),
     'tb_component_boxes': (_I32, [_P, _I32, _I32, _I32, _P, _P]),

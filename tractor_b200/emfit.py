@@ -88,6 +88,59 @@ def em_fit_2d_reg(img, x0, y0, amp, mean, var, alpha, steps):
     return -1 if st[0] else 0
 
 
+def em_fit_2d_reg2_batch(imgs, amp, mean, var, alpha=0., steps=1000, approx=1e-30, xy0=None):
+    """The EM fits with a flat sky term (em_fit_2d_reg2, tractor/emfit2.c) of
+    n images in one tb_em_fit_2d_sky launch, in em_fit_2d_batch's layout.
+    Returns (amp, mean, var, skyamp, status)."""
+    imgs = np.ascontiguousarray(imgs, np.float64)
+    if imgs.ndim != 3:
+        raise ValueError('imgs must be (n, ny, nx)')
+    n, ny, nx = imgs.shape
+    amp = np.array(amp, np.float64).reshape(n, -1)
+    K = amp.shape[1]
+    if not 1 <= K <= _lib.EM_MAX_K:
+        raise ValueError('1 <= K <= %d components' % _lib.EM_MAX_K)
+    mean = np.array(mean, np.float64).reshape(n, K, 2)
+    var = np.array(var, np.float64).reshape(n, K, 2, 2)
+    if n == 0:
+        return amp, mean, var, np.zeros(0), np.zeros(0, np.int32)
+    dev = render.device()
+    d_img = torch.from_numpy(imgs).to(dev)
+    d_amp = torch.from_numpy(amp.copy()).to(dev)
+    d_mean = torch.from_numpy(mean.copy()).to(dev)
+    d_var = torch.from_numpy(var.copy()).to(dev)
+    d_sky = torch.zeros(n, dtype=torch.float64, device=dev)
+    d_st = torch.zeros(n, dtype=torch.int32, device=dev)
+    d_xy = None
+    if xy0 is not None:
+        d_xy = torch.from_numpy(np.array(np.broadcast_to(np.asarray(xy0, np.int32), (n, 2)))
+                                ).to(dev)
+    lib = _lib.load()
+    _lib.check(lib.tb_em_fit_2d_sky(d_img.data_ptr(), n, ny, nx,
+                                    d_xy.data_ptr() if d_xy is not None else None,
+                                    d_amp.data_ptr(), d_mean.data_ptr(), d_var.data_ptr(), K,
+                                    float(alpha), int(steps), float(approx), d_sky.data_ptr(),
+                                    d_st.data_ptr(), _lib.stream_ptr()),
+               'tb_em_fit_2d_sky')
+    return (d_amp.cpu().numpy(), d_mean.cpu().numpy(), d_var.cpu().numpy(),
+            d_sky.cpu().numpy(), d_st.cpu().numpy())
+
+
+def em_fit_2d_reg2(img, x0, y0, amp, mean, var, alpha, steps, approx):
+    """em_fit_2d_reg2 (tractor/emfit2.c): fits the mixture (amp, mean, var),
+    updated in place, and a flat sky to img, pixel (ix, iy) at (x0 + ix,
+    y0 + iy); returns [status, skyamp] as the reference's wrapper does
+    (status 0, or -1 when a covariance determinant became non-positive)."""
+    img = np.asarray(img)
+    a, m, v, sky, st = em_fit_2d_reg2_batch(img[None], np.asarray(amp)[None],
+                                            np.asarray(mean)[None], np.asarray(var)[None],
+                                            alpha, steps, approx, xy0=(x0, y0))
+    amp[...] = a[0]
+    mean[...] = m[0]
+    var[...] = v[0]
+    return [-1 if st[0] else 0, float(sky[0])]
+
+
 def em_fit_2d(img, x0, y0, amp, mean, var):
     """em_fit_2d (tractor/emfit.i:570-576): no prior, 1000 iterations."""
     return em_fit_2d_reg(img, x0, y0, amp, mean, var, 0.0, 1000)

@@ -282,8 +282,9 @@ class GaussianMixturePSF(MogParams):
     def fromStamp(stamp, N=3, P0=None, xy0=None, alpha=0., emsteps=1000, v2=False,
                   approx=1e-30, v3=False):
         """GaussianMixturePSF.fromStamp (tractor/psf.py:536-597): an N-component
-        mixture fit to a PSF stamp by EM on the GPU (em_fit_2d_reg), or with
-        v3 by the Tractor optimiser with the PSF's parameters thawed."""
+        mixture fit to a PSF stamp by EM on the GPU (em_fit_2d_reg), with v2
+        by EM with a flat sky term (em_fit_2d_reg2; returns (psf, skyamp)), or
+        with v3 by the Tractor optimiser with the PSF's parameters thawed."""
         from .emfit import em_init_params, em_fit_2d_reg
         if P0 is not None:
             w, mu, var = P0
@@ -312,8 +313,14 @@ class GaussianMixturePSF(MogParams):
                     break
             return tpsf
         if v2:
-            raise NotImplementedError('fromStamp(v2=True) (em_fit_2d_reg2, a mixture plus a '
-                                      'sky term) is not provided')
+            # the EM fit with a flat sky term on the stamp as given: returns
+            # (psf, sky level per pixel), as the reference does
+            from .emfit import em_fit_2d_reg2
+            w = np.array(w, np.float64)
+            mu = np.array(mu, np.float64)
+            var = np.array(var, np.float64)
+            ok, skyamp = em_fit_2d_reg2(stamp, xm, ym, w, mu, var, alpha, emsteps, approx)
+            return GaussianMixturePSF(w, mu, var), skyamp
         stamp = GaussianMixturePSF._stamp_for_em(stamp)
         w = np.array(w, np.float64)
         mu = np.array(mu, np.float64)
