@@ -1344,8 +1344,7 @@ def run_reference(args, world, rank):
         'n_gpus': 0, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': wall / max(1, args.steps) * 1e3, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64/f32 (reference CPU path)',
-        'data': 'synthetic', 'config': {'workload': WORKLOAD, 'n_sources': N_SOURCES,
-                                        'mask': MASK, 'fft_size': 256},
+        'data': 'synthetic', 'config': config_keys(),   # the same keys as the GPU arm
         'cpu_baseline': {'value': value, 'unit': 'Mpix*components/s', 'cores': ncores,
                          'kind': kind,
                          'sample': '%d source renders over %d steps (%.0f s budget per step), '
