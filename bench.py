@@ -612,6 +612,8 @@ def bench_fit(args, dev, flush, clk, cpu_seconds):
                     'edge': plain['edge_blobs'], 'edge_sigma': plain['edge_max_sigma'],
                     'flat': plain['flat_blobs'], 'flat_sigma': plain['flat_max_sigma'],
                     'limit': int(np.sum(st['status'] == 3)),
+                    'limit_sigma': plain['limit_max_sigma'],
+                    'limit_inner_sigma': plain['limit_inner_max_sigma'],
                     'stopped': int(np.sum(st['status'] == 2))},
         'roofline': {'bound': 'fp32', 'kernel': 'tb_fit_pass (all blobs running)',
                      'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
@@ -1269,10 +1271,14 @@ def fit_plain_fp64(w, data, inv, batched, status, dev, budget):
     # by convergence or at the iteration limit is eligible)
     ok = np.flatnonzero(status != 2)
     pick = ok[np.linspace(0, len(ok) - 1, min(120, len(ok))).astype(int)] if len(ok) else ok
+    # and every blob that stopped at the iteration limit, reported apart
+    limit_blobs = np.flatnonzero(status == 3)
+    pick = np.union1d(pick, limit_blobs)
     res = plain.optimum_distance(w, data, inv, batched, status, pick, dev)
     inner = [r[0] for r in res if not r[3] and r[4]]
     edge = [r[0] for r in res if r[3]]
     flat = [r[0] for r in res if not r[3] and not r[4]]
+    limit = [r for r in res if r[2] == 3]
     return {'value': done / secs, 'unit': 'sources/s', 'blobs': blobs, 'sources': int(done),
             'seconds': secs, 'parity_blobs': len(res),
             'batched_vs_fp64_optimum_max_sigma': float(np.max(inner)) if inner else None,
@@ -1281,13 +1287,18 @@ def fit_plain_fp64(w, data, inv, batched, status, dev, budget):
             'edge_max_sigma': float(np.max(edge)) if edge else None,
             'flat_blobs': len(flat),
             'flat_max_sigma': float(np.max(flat)) if flat else None,
+            'limit_blobs': len(limit),
+            'limit_max_sigma': float(np.max([r[0] for r in limit])) if limit else None,
+            'limit_inner_max_sigma': (float(np.max([r[0] for r in limit if not r[3] and r[4]]))
+                                      if any(not r[3] and r[4] for r in limit) else None),
             'how': 'tractor_b200.plain.BlobFitFP64 (FP64 torch ops + cuSOLVER, one blob at a '
                    'time, same GPU) from the start for the rate; continued from the batched '
                    'result to predicted dlnp 1e-10 for the FP64 optimum; sigma from its FP64 '
                    'Fisher matrix; edge blobs have a Sersic index within 1e-3 of a profile '
                    'range edge, where the mixture tables change and the model jumps; flat '
                    'blobs are those the FP64 fitter itself does not converge on within 100 '
-                   'iterations'}
+                   'iterations; the parity set is 120 blobs spread over the workload plus '
+                   'every blob that stopped at the iteration limit (limit_*: those alone)'}
 
 
 def fit_ncomp(n):
