@@ -1267,13 +1267,11 @@ def fit_plain_fp64(w, data, inv, batched, status, dev, budget):
     e1.record()
     e1.synchronize()
     secs = e0.elapsed_time(e1) / 1e3
-    # parity: 120 blobs spread over the workload (every blob that stopped
-    # by convergence or at the iteration limit is eligible)
-    ok = np.flatnonzero(status != 2)
-    pick = ok[np.linspace(0, len(ok) - 1, min(120, len(ok))).astype(int)] if len(ok) else ok
-    # and every blob that stopped at the iteration limit, reported apart
-    limit_blobs = np.flatnonzero(status == 3)
-    pick = np.union1d(pick, limit_blobs)
+    # parity: 120 blobs spread over the workload, and every blob that
+    # stopped by rejections (status 2) or at the iteration limit (status 3)
+    n_b = len(status)
+    pick = np.linspace(0, n_b - 1, min(120, n_b)).astype(int)
+    pick = np.union1d(pick, np.flatnonzero(status >= 2))
     res = plain.optimum_distance(w, data, inv, batched, status, pick, dev)
     inner = [r[0] for r in res if not r[3] and r[4]]
     edge = [r[0] for r in res if r[3]]
@@ -1298,7 +1296,8 @@ def fit_plain_fp64(w, data, inv, batched, status, dev, budget):
                    'range edge, where the mixture tables change and the model jumps; flat '
                    'blobs are those the FP64 fitter itself does not converge on within 100 '
                    'iterations; the parity set is 120 blobs spread over the workload plus '
-                   'every blob that stopped at the iteration limit (limit_*: those alone)'}
+                   'every blob that stopped by rejections near its optimum or at the iteration '
+                   'limit (limit_*: those at the limit alone)'}
 
 
 def fit_ncomp(n):

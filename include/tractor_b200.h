@@ -121,6 +121,31 @@ int tb_mog_render(const tb_mog_item* items, int32_t n_items, int64_t n_tiles,
                   const double* comp_var, const uint8_t* masks, float* out,
                   int32_t* work_counter, tb_status* status, void* stream);
 
+/* tb_mog_render over HOST buffers, the way c_gauss_2d_grid /
+ * c_gauss_2d_masked (tractor/mix.i:452-524, tractor/gauss_masked.c:1-159)
+ * take and fill numpy arrays: items[n_items], comp_amp[n_comp],
+ * comp_mean[2 n_comp], comp_var[4 n_comp], masks[mask_bytes] (may be NULL
+ * when mask_bytes = 0) are read from host memory, the n_out output elements
+ * are written to host `out` and the launch's status word to host `status`.
+ * Staging goes through two caller-owned buffers of
+ * tb_mog_render_host_bytes() bytes each: `pinned` (page-locked host memory,
+ * e.g. cudaHostAlloc) and `workspace` (device memory); the call packs the
+ * inputs into `pinned`, copies them to `workspace` in one copy, renders,
+ * copies the output and status back in one copy and synchronises `stream`
+ * before returning, so both buffers may be reused at once.  Every item must
+ * lie inside the given sizes (components, mask, output; tile0 the exclusive
+ * prefix of its tiles, n_tiles their total), else TB_ERR_ARG before any
+ * copy; ws_bytes smaller than needed gives TB_ERR_SIZE.  Outputs that no
+ * item writes, and the targets of TB_MOG_ACCUM / TB_MOG_ATOMIC items, start
+ * at zero. */
+int tb_mog_render_host_bytes(int32_t n_items, int64_t n_comp, int64_t mask_bytes,
+                             int64_t n_out, int64_t* bytes);
+int tb_mog_render_host(const tb_mog_item* items, int32_t n_items, int64_t n_tiles,
+                       const double* comp_amp, const double* comp_mean,
+                       const double* comp_var, int64_t n_comp, const uint8_t* masks,
+                       int64_t mask_bytes, float* out, int64_t n_out, tb_status* status,
+                       void* pinned, void* workspace, int64_t ws_bytes, void* stream);
+
 /* c_gauss_2d_approx3's evaluated region (tractor/approx3.c:126-442) over
  * values tb_mog_render has already written for a whole box with the
  * TB_FLOOR_MINVAL floors: starting at (xc, yc) -- or, when that is outside

@@ -87,6 +87,72 @@ def test_mog_atomic_image_matches_sum(tb, oracle):
     assert np.abs(got - ref).max() / ref.max() < PEAK_TOL
 
 
+def test_mog_host_entry_equals_device_path(tb):
+    """tb_mog_render_host (host buffers in and out, staging inside) writes
+    exactly what tb_mog_render writes into device memory: grid, masked,
+    derivative-plane and difference items in one batch, and ATOMIC items
+    into a shared image; items outside the given sizes and a short
+    workspace are rejected before any copy."""
+    import ctypes
+    import torch
+    from tractor_b200 import _lib, render
+    rng = np.random.default_rng(11)
+    b = render.MogBatch()
+    for (w, h, K) in [(33, 33, 12), (64, 64, 6), (1, 1, 2), (100, 70, 27)]:
+        amp, mean, var = _rand_mix(rng, K, spread=w / 6)
+        b.add(int(rng.integers(-20, 20)), int(rng.integers(-20, 20)), w, h, amp, mean, var,
+              fx=w / 2, fy=h / 2)
+    amp, mean, var = _rand_mix(rng, 9, spread=5)
+    b.add(-3, 4, 50, 40, amp, mean, var, fx=20.5, fy=22.25, floor=render.FLOOR_MASKED,
+          mask=rng.uniform(size=(40, 50)) > 0.3)
+    b.add(0, 0, 31, 29, amp, mean, var, fx=15., fy=14., derivs=True)
+    amp2, _, var2 = _rand_mix(rng, 9, spread=5)
+    b.add(2, 1, 40, 36, amp, mean, var, fx=20., fy=18., diff=(amp2, var2))
+    dev = b.run().cpu().numpy()[:b.nout]
+    host = b.run_host()
+    assert host.dtype == np.float32 and host.shape == (b.nout,)
+    assert np.array_equal(host, dev)
+    # ATOMIC items into one image (outputs start at zero)
+    H, W = 60, 70
+    a = render.MogBatch()
+    for i in range(8):
+        amp, mean, var = _rand_mix(rng, 4, spread=1)
+        x0, y0 = int(rng.integers(0, W - 20)), int(rng.integers(0, H - 20))
+        a.add(x0, y0, 20, 20, amp, mean, var, fx=x0 + 10., fy=y0 + 10., scale=100.,
+              out_off=y0 * W + x0, ldo=W, mode=render.MOG_ATOMIC)
+    a.nout = H * W
+    img = torch.zeros(H * W, dtype=torch.float32, device='cuda')
+    a.run(out=img)
+    got = a.run_host()
+    assert np.abs(got - img.cpu().numpy()).max() <= 1e-5 * np.abs(got).max()
+    # rejections: an output beyond n_out, a workspace one byte short
+    lib = _lib.load()
+    items = np.array(b.items[:1], dtype=_lib.MOG_ITEM)
+    w0, h0 = int(items['w'][0]), int(items['h'][0])
+    tiles = ((w0 + 31) // 32) * ((h0 + 31) // 32)
+    K = int(items['K'][0])
+    ca, cm, cv = b.amp[0], b.mean[0], b.var[0]
+    nbytes = ctypes.c_int64()
+    assert lib.tb_mog_render_host_bytes(1, K, 0, w0 * h0, ctypes.byref(nbytes)) == _lib.TB_OK
+    pinned = torch.empty(nbytes.value, dtype=torch.uint8).pin_memory()
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device='cuda')
+    st = np.zeros(1, _lib.STATUS)
+
+    def call(n_out, ws_bytes):
+        out = np.full(max(n_out, 1), -7., np.float32)
+        rc = lib.tb_mog_render_host(items.ctypes.data, 1, tiles, ca.ctypes.data, cm.ctypes.data,
+                                    cv.ctypes.data, K, None, 0, out.ctypes.data, n_out,
+                                    st.ctypes.data, pinned.data_ptr(), ws.data_ptr(), ws_bytes,
+                                    _lib.stream_ptr())
+        return rc, out
+    rc, out = call(w0 * h0, nbytes.value)
+    assert rc == _lib.TB_OK and np.array_equal(out, dev[:w0 * h0])
+    rc, out = call(w0 * h0 - 1, nbytes.value)
+    assert rc == _lib.TB_ERR_ARG and np.all(out == -7.)
+    rc, out = call(w0 * h0, nbytes.value - 1)
+    assert rc == _lib.TB_ERR_SIZE and np.all(out == -7.)
+
+
 def test_lanczos_bit_exact(tb, oracle):
     import torch
     from tractor_b200 import render

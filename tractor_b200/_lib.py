@@ -100,6 +100,7 @@ MOG_STORE, MOG_ACCUM, MOG_ATOMIC = 0, 1, 2
 MOG_TILE = 32
 
 TB_OK = 0
+TB_ERR_ARG, TB_ERR_LAUNCH, TB_ERR_SIZE = -1, -2, -3
 _ERRORS = {-1: 'invalid argument', -2: 'CUDA launch error', -3: 'unsupported size'}
 
 _P = ctypes.c_void_p
@@ -110,6 +111,9 @@ _D = ctypes.c_double
 # name -> (restype, argtypes)
 SIGNATURES = {
     'tb_mog_render': (_I32, [_P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P, _P]),
+    'tb_mog_render_host_bytes': (_I32, [_I32, _I64, _I64, _I64, _P]),
+    'tb_mog_render_host': (_I32, [_P, _I32, _I64, _P, _P, _P, _I64, _P, _I64, _P, _I64, _P, _P,
+                                  _P, _I64, _P]),
     'tb_lanczos3_shift': (_I32, [_P, _P, _P, _I32, _I32, _I32, _P]),
     'tb_fourier_render': (_I32, [_P, _I32, _P, _P, _P, _P, _P, _P, _P]),
     'tb_psf_spectrum': (_I32, [_P, _P, _I32, _I32, _I32, _P]),

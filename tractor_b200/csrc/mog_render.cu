@@ -9,6 +9,8 @@
 // one column and four rows of the tile and evaluates every surviving
 // component with one SFU ex2 per pixel.  Component order (and so summation
 // order) is the item's order, as in c_gauss_2d_grid (tractor/mix.i:452-524).
+#include <cstring>
+
 #include "tb_common.cuh"
 
 namespace {
@@ -249,6 +251,126 @@ extern "C" int tb_mog_render(const tb_mog_item* items, int32_t n_items, int64_t 
     mog_render_kernel<<<grid, kThreads, 0, s>>>(items, n_items, n_tiles, comp_amp, comp_mean,
                                                comp_var, masks, out, work_counter, status);
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ERR_LAUNCH;
+}
+
+// ---------------------------------------------------------------------------
+// tb_mog_render over host buffers: the items, components and masks are
+// packed into the caller's page-locked staging buffer, copied to the caller's
+// device workspace in one copy, rendered, and the packed output and status
+// word brought back in one copy; the stream is synchronised before return.
+// One call per render instead of a staging copy, an output allocation, a
+// launch and a read-back issued one by one from the host language.
+// ---------------------------------------------------------------------------
+namespace {
+
+inline int64_t up256(int64_t x) { return (x + 255) & ~(int64_t)255; }
+
+struct MogHostLayout {
+    int64_t items, amp, mean, var, mask, in_end, counter, out, status, total;
+};
+
+MogHostLayout mog_host_layout(int64_t n_items, int64_t n_comp, int64_t mask_bytes,
+                              int64_t n_out) {
+    MogHostLayout L;
+    int64_t o = 0;
+    L.items = o;   o = up256(o + n_items * (int64_t)sizeof(tb_mog_item));
+    L.amp = o;     o = up256(o + n_comp * 8);
+    L.mean = o;    o = up256(o + n_comp * 16);
+    L.var = o;     o = up256(o + n_comp * 32);
+    L.mask = o;    o = up256(o + mask_bytes);
+    L.in_end = o;
+    L.counter = o; o = up256(o + 4);
+    L.out = o;     o = o + n_out * 4;
+    L.status = (o + 15) & ~(int64_t)15;
+    L.total = L.status + (int64_t)sizeof(tb_status);
+    return L;
+}
+
+// Every item's components, mask and output inside the sizes given, so that
+// the device never reads or writes outside the workspace.
+bool mog_items_fit(const tb_mog_item* items, int32_t n_items, int64_t n_tiles, int64_t n_comp,
+                   int64_t mask_bytes, int64_t n_out, bool* any_accum) {
+    int64_t tiles = 0;
+    *any_accum = false;
+    for (int32_t i = 0; i < n_items; i++) {
+        const tb_mog_item& it = items[i];
+        if (it.w < 0 || it.h < 0 || it.K < 0 || it.c0 < 0 || it.ldo < 0) return false;
+        if ((int64_t)it.c0 + it.K > n_comp) return false;
+        if (it.diff_c0 >= 0 && (int64_t)it.diff_c0 + it.K > n_comp) return false;
+        if (it.tile0 != tiles) return false;
+        tiles += (int64_t)((it.w + TB_MOG_TILE - 1) / TB_MOG_TILE) *
+                 ((it.h + TB_MOG_TILE - 1) / TB_MOG_TILE);
+        if (it.w == 0 || it.h == 0) continue;
+        const int64_t ldo = it.ldo ? it.ldo : it.w;
+        if (ldo < it.w || it.out_off < 0) return false;
+        if (it.out_off + (int64_t)(it.h - 1) * ldo + it.w > n_out) return false;
+        if (it.deriv_off >= 0 && it.deriv_off + 2 * (int64_t)it.w * it.h > n_out) return false;
+        if (it.mask_off >= 0 && it.mask_off + (int64_t)it.w * it.h > mask_bytes) return false;
+        if (it.mode != TB_MOG_STORE) *any_accum = true;
+    }
+    return tiles == n_tiles;
+}
+
+}  // namespace
+
+extern "C" int tb_mog_render_host_bytes(int32_t n_items, int64_t n_comp, int64_t mask_bytes,
+                                        int64_t n_out, int64_t* bytes) {
+    if (n_items < 0 || n_comp < 0 || mask_bytes < 0 || n_out < 0 || !bytes) return TB_ERR_ARG;
+    *bytes = mog_host_layout(n_items, n_comp, mask_bytes, n_out).total;
+    return TB_OK;
+}
+
+extern "C" int tb_mog_render_host(const tb_mog_item* items, int32_t n_items, int64_t n_tiles,
+                                  const double* comp_amp, const double* comp_mean,
+                                  const double* comp_var, int64_t n_comp, const uint8_t* masks,
+                                  int64_t mask_bytes, float* out, int64_t n_out,
+                                  tb_status* status, void* pinned, void* workspace,
+                                  int64_t ws_bytes, void* stream) {
+    if (n_items < 0 || n_tiles < 0 || n_comp < 0 || mask_bytes < 0 || n_out < 0 || !status)
+        return TB_ERR_ARG;
+    if ((n_items > 0 && !items) || (n_comp > 0 && (!comp_amp || !comp_mean || !comp_var)) ||
+        (mask_bytes > 0 && !masks) || (n_out > 0 && !out) || !pinned || !workspace)
+        return TB_ERR_ARG;
+    const MogHostLayout L = mog_host_layout(n_items, n_comp, mask_bytes, n_out);
+    if (ws_bytes < L.total) return TB_ERR_SIZE;
+    bool any_accum = false;
+    if (!mog_items_fit(items, n_items, n_tiles, n_comp, mask_bytes, n_out, &any_accum))
+        return TB_ERR_ARG;
+    char* P = static_cast<char*>(pinned);
+    char* D = static_cast<char*>(workspace);
+    std::memcpy(P + L.items, items, (size_t)n_items * sizeof(tb_mog_item));
+    std::memcpy(P + L.amp, comp_amp, (size_t)n_comp * 8);
+    std::memcpy(P + L.mean, comp_mean, (size_t)n_comp * 16);
+    std::memcpy(P + L.var, comp_var, (size_t)n_comp * 32);
+    if (mask_bytes > 0) std::memcpy(P + L.mask, masks, (size_t)mask_bytes);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(D, P, (size_t)L.in_end, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    // ACCUM / ATOMIC targets start at zero, as does an output no tile writes
+    const bool launches = n_items > 0 && n_tiles > 0;
+    if ((any_accum || !launches) && n_out > 0 &&
+        cudaMemsetAsync(D + L.out, 0, (size_t)n_out * 4, s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    // (tb_mog_render zeroes the status word itself when it launches)
+    if (!launches && cudaMemsetAsync(D + L.status, 0, sizeof(tb_status), s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    const int rc = tb_mog_render(reinterpret_cast<const tb_mog_item*>(D + L.items), n_items,
+                                 n_tiles, reinterpret_cast<const double*>(D + L.amp),
+                                 reinterpret_cast<const double*>(D + L.mean),
+                                 reinterpret_cast<const double*>(D + L.var),
+                                 mask_bytes > 0 ? reinterpret_cast<const uint8_t*>(D + L.mask)
+                                                : nullptr,
+                                 reinterpret_cast<float*>(D + L.out),
+                                 reinterpret_cast<int32_t*>(D + L.counter),
+                                 reinterpret_cast<tb_status*>(D + L.status), stream);
+    if (rc != TB_OK) return rc;
+    if (cudaMemcpyAsync(P + L.out, D + L.out, (size_t)(L.total - L.out), cudaMemcpyDeviceToHost,
+                        s) != cudaSuccess)
+        return TB_ERR_LAUNCH;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return TB_ERR_LAUNCH;
+    if (n_out > 0) std::memcpy(out, P + L.out, (size_t)n_out * 4);
+    std::memcpy(status, P + L.status, sizeof(tb_status));
+    return TB_OK;
 }
 
 // ---------------------------------------------------------------------------

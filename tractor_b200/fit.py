@@ -218,7 +218,7 @@ class BlobFitter(object):
         return int((st[:, -1] == 0).sum().item())
 
     def fit(self, tol=1e-3, max_iter=200, check_every=4, graph=True, params0=None,
-            lambda0=1e-3, refine=True, refine_tol=1e-9, refine_iter=40, handoff=0.005):
+            lambda0=1e-3, refine=True, refine_tol=1e-9, refine_iter=100, handoff=0.005):
         """Runs FP32 iterations until every blob stops (or max_iter); then,
         with `refine`, continues every blob from where it stopped with the
         normal equations in FP64 (tb_fit_refine in place of the pass) until
@@ -228,8 +228,12 @@ class BlobFitter(object):
         optimum, and an FP32 A^T A is too inexact for an ill-conditioned
         blob's steps to converge.  With `refine`, the FP32 phase also ends
         once at most a fraction `handoff` of the blobs still runs: those
-        continue in the FP64 phase from where they are.  Returns the number
-        of iterations launched (both phases)."""
+        continue in the FP64 phase from where they are.  The slowest blobs
+        of a 2,000-blob fit of 192-512 px blobs need about 60 FP64
+        iterations (Gauss-Newton steps rejected and re-damped along an
+        ill-conditioned direction); 40 left some of them several sigma from
+        the optimum.  Returns the number of iterations launched (both
+        phases)."""
         self.reset(params0, lambda0)
         g = None
         if graph:

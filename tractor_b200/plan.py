@@ -78,7 +78,11 @@ class RenderPlan(object):
         self._ran = True
         outs = []
         if len(self.mog):
-            outs.append(('mog', self.mog.run(check=False)))
+            if self.mog.rings or render.device().type != 'cuda':
+                outs.append(('mog', self.mog.run(check=False)))
+            else:
+                # staging, launch and read-back in one library call
+                self._mog_host = self.mog.run_host()
         if len(self.fft):
             outs.append(('fft', self.fft.run(check=False)))
         lz = {}

@@ -293,6 +293,63 @@ class MogBatch(object):
         return out
 
 
+    def run_host(self, stream=None):
+        """Renders all items with tb_mog_render_host and returns the packed
+        float32 output (nout elements) as a host array: inputs staged, the
+        launch made, the output and status word read back and the stream
+        synchronised in one library call.  Plans without approx3 region
+        walks take this path."""
+        lib = _lib.load()
+        if self.rings:
+            raise ValueError('approx3 region walks need the device output (run)')
+        out = np.empty(max(self.nout, 1), np.float32)
+        if not self.items:
+            out[:] = 0.
+            return out[:self.nout]
+        items = np.array(self.items, dtype=_lib.MOG_ITEM)
+        tiles = ((items['w'] + 31) // 32).astype(np.int64) * ((items['h'] + 31) // 32)
+        items['tile0'] = np.concatenate([[0], np.cumsum(tiles)[:-1]])
+        amp = np.concatenate(self.amp)
+        mean = np.concatenate(self.mean)
+        var = np.concatenate(self.var)
+        masks = np.concatenate(self.masks) if self.masks else None
+        nmask = 0 if masks is None else masks.size
+        nbytes = ctypes.c_int64()
+        _lib.check(lib.tb_mog_render_host_bytes(len(items), amp.size, nmask, self.nout,
+                                                ctypes.byref(nbytes)),
+                   'tb_mog_render_host_bytes')
+        pinned, ws = _host_staging.get(nbytes.value, device())
+        st = np.zeros(1, _lib.STATUS)
+        rc = lib.tb_mog_render_host(items.ctypes.data, len(items), int(tiles.sum()),
+                                    amp.ctypes.data, mean.ctypes.data, var.ctypes.data,
+                                    amp.size, None if masks is None else masks.ctypes.data,
+                                    nmask, out.ctypes.data, self.nout, st.ctypes.data,
+                                    pinned.data_ptr(), ws.data_ptr(), ws.numel(),
+                                    _lib.stream_ptr(stream))
+        _lib.check(rc, 'tb_mog_render_host')
+        check_status_host(st, 'tb_mog_render')
+        return out[:self.nout]
+
+
+class _HostStaging(threading.local):
+    """One page-locked host buffer and one device workspace per thread for
+    tb_mog_render_host (grown to the next power of two; the call
+    synchronises its stream, so both are free again when it returns)."""
+
+    pinned = None
+    ws = None
+
+    def get(self, nbytes, dev):
+        if self.ws is None or self.ws.numel() < nbytes or self.ws.device != dev:
+            size = 1 << max(16, int(np.ceil(np.log2(max(nbytes, 1)))))
+            self.pinned = torch.empty(size, dtype=torch.uint8).pin_memory()
+            self.ws = torch.empty(size, dtype=torch.uint8, device=dev)
+        return self.pinned, self.ws
+
+
+_host_staging = _HostStaging()
+
+
 class PsfSpectra(object):
     """Device spectra of pixelized PSFs, one per (PSF image, size), computed
     by tb_psf_spectrum (PixelizedPSF.getFourierTransform, tractor/psf.py:249-280)."""
