@@ -133,9 +133,9 @@ class B200Optimizer(object):
                     continue
                 anyval = True
                 h, w = vals.shape
-                r0 = row0[img] + (d.y0 - y0) * rw + (d.x0 - x0)
-                idx = r0 + np.arange(h)[:, None] * rw + np.arange(w)[None, :]
-                A[col, idx.ravel()] += vals.ravel().astype(np.float32)
+                # the image's ROI rows of column col as a (rows, rw) view
+                roi = A[col, row0[img]:row0[img] + (y1 - y0) * rw].reshape(y1 - y0, rw)
+                roi[d.y0 - y0:d.y0 - y0 + h, d.x0 - x0:d.x0 - x0 + w] += vals.astype(np.float32)
         if prior is not None:
             rA, cA, vA, pb, nr = prior
             for ri, ci, vi in zip(rA, cA, vA):
@@ -165,11 +165,12 @@ class B200Optimizer(object):
         # merges shared parameters afterwards)
         cs = np.where(colscales > 0, colscales, 1.)
         As = A / cs[:, None].astype(np.float32) if scale_columns else A
-        if shared_params:
+        if shared_params and not np.array_equal(paramindexmap, np.arange(Ncols)):
             ncols = int(paramindexmap.max()) + 1
             Am = np.zeros((ncols, nrows), np.float32)
             np.add.at(Am, paramindexmap, As)
         else:
+            # no parameter shared: the merge would copy every column once
             Am = As
         X = self._solve(Am, b, damp)
         if X is None:
