@@ -35,3 +35,48 @@ def test_invalid_arguments_are_rejected_without_a_device():
                                    None, 1, 400, None) == -3
     assert lib.tb_em_fit_2d(None, 1, 9, 9, None, None, None, None, 3, 0., 10, None, None) == -1
     assert lib.tb_em_fit_2d(None, 1, 9, 9, None, None, None, None, 9, 0., 10, None, None) == -1
+
+
+def test_mog_render_host_checks_items_before_any_copy():
+    """tb_mog_render_host sizes its staging and refuses items that reach
+    outside the given component, mask or output sizes, a wrong tile count
+    and a short workspace, all on the host before any CUDA call."""
+    import numpy as np
+    from tractor_b200 import _lib
+    lib = _lib.load()
+    K, w, h = 3, 40, 20
+    item = np.zeros(1, _lib.MOG_ITEM)
+    item[0] = (0, 0, w, h, 0, K, _lib.MOG_STORE, 0, 10., 5., -50., 1., _lib.FLOOR_FIXED,
+               0, -1, 0, -1, -1, 0)
+    tiles = ((w + 31) // 32) * ((h + 31) // 32)
+    amp, mean, var = np.ones(K), np.zeros((K, 2)), np.tile(np.eye(2), (K, 1, 1))
+    nbytes = ctypes.c_int64()
+    assert lib.tb_mog_render_host_bytes(1, K, 0, w * h, ctypes.byref(nbytes)) == _lib.TB_OK
+    assert nbytes.value >= item.nbytes + K * 56 + w * h * 4 + 16
+    assert lib.tb_mog_render_host_bytes(-1, K, 0, w * h, ctypes.byref(nbytes)) == _lib.TB_ERR_ARG
+    lib.tb_mog_render_host_bytes(1, K, 0, w * h, ctypes.byref(nbytes))
+    # host stand-ins for the staging buffers: every call below returns first
+    pinned = np.zeros(nbytes.value, np.uint8)
+    ws = np.zeros(nbytes.value, np.uint8)
+    out = np.full(w * h, -7., np.float32)
+    st = np.zeros(1, _lib.STATUS)
+
+    def call(it, n_tiles=tiles, n_comp=K, n_out=w * h, ws_bytes=nbytes.value):
+        return lib.tb_mog_render_host(it.ctypes.data, 1, n_tiles, amp.ctypes.data,
+                                      mean.ctypes.data, var.ctypes.data, n_comp, None, 0,
+                                      out.ctypes.data, n_out, st.ctypes.data,
+                                      pinned.ctypes.data, ws.ctypes.data, ws_bytes, None)
+    assert call(item, n_out=w * h - 1) == _lib.TB_ERR_ARG          # output too small
+    assert call(item, n_comp=K - 1) == _lib.TB_ERR_ARG             # components beyond n_comp
+    assert call(item, n_tiles=tiles + 1) == _lib.TB_ERR_ARG        # tile count disagrees
+    bad = item.copy()
+    bad['mask_off'] = 0                                            # a mask with mask_bytes = 0
+    assert call(bad) == _lib.TB_ERR_ARG
+    bad = item.copy()
+    bad['deriv_off'] = w * h                                       # derivative planes past n_out
+    assert call(bad) == _lib.TB_ERR_ARG
+    bad = item.copy()
+    bad['ldo'] = w - 1                                             # row stride below the width
+    assert call(bad) == _lib.TB_ERR_ARG
+    assert call(item, ws_bytes=nbytes.value - 1) == _lib.TB_ERR_SIZE
+    assert np.all(out == -7.)
