@@ -133,11 +133,14 @@ def test_columns_match_reference_getParamDerivatives(tb):
     flux column is the same render (1e-5).  The position columns are a
     one-pixel central difference of the patch times the NullWCS cdInverse of
     3600 (galaxy.py:163-178): the same difference of our value render
-    reproduces them (1e-4), and the analytic columns differ from them by the
-    difference's truncation error (< 15 % of the peak for these profiles).
-    Shape and index columns are forward differences of step 0.01: the same
-    differences of our value renders reproduce them (2e-3), and the analytic
-    columns are within their truncation error (< 10 %)."""
+    reproduces them (1e-5; measured 6e-7), and the analytic columns differ
+    from them by the difference's truncation error (< 15 % of the peak for
+    these profiles).  Shape and index columns are forward differences of
+    step 0.01: the same differences of our value renders reproduce them
+    (shape 2e-4, measured 9e-5; Sersic index 5e-4, measured 3.5e-4: both
+    sides difference two float32 renders, so their rounding is amplified
+    100-fold), and the analytic columns are within their truncation error
+    (< 10 %)."""
     import torch
     from tractor_b200 import batch, grad, _lib
     g = np.load(os.path.join(GOLDEN, 'fft_sersic.npz'))
@@ -181,7 +184,10 @@ def test_columns_match_reference_getParamDerivatives(tb):
     tol = {0: 0.15, 1: 0.15, 2: 1e-5, 3: 0.1, 4: 0.1, 5: 0.1, 6: 0.1}
     bad = {}
     for k, e in errs.items():
-        t = {'grid': 1e-4, 'fwd': 2e-3}[k[2]] if len(k) == 3 else tol[k[1]]
+        if len(k) == 3:
+            t = 1e-5 if k[2] == 'grid' else (5e-4 if k[1] == 6 else 2e-4)
+        else:
+            t = tol[k[1]]
         if not e < t:
             bad[k] = e
     assert not bad, (bad, errs)
