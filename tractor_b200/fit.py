@@ -39,10 +39,13 @@ class BlobFitter(object):
     sources:    FIT_SOURCE records (profile, mask rectangle in blob pixels);
     params0:    (n_src, 9) starting parameters;
     data, inverr: float32 device tensors, unit (blob, band) images packed in
-                blob-major, band-minor order (see `pix_offsets`)."""
+                blob-major, band-minor order (see `pix_offsets`);
+    unit_tiles: active 32 x 8 tiles per pass unit at most (a (blob, band)
+                image with more is split into that many units, each with its
+                own partial normal-equation slice)."""
 
     def __init__(self, blob_src, sides, psf, sources, params0, data, inverr, n_bands=3,
-                 cd_inv=None):
+                 cd_inv=None, unit_tiles=UNIT_TILES):
         lib = _lib.load()
         self.dev = render.device()
         self.n_bands = int(n_bands)
@@ -67,7 +70,10 @@ class BlobFitter(object):
         # a band's active tiles go to ceil(n_active / UNIT_TILES) pass units,
         # each with its own partial blocks (slices), so that no unit holds
         # one CTA for long while few blobs are still running
-        parts = np.maximum(1, -(-n_active // UNIT_TILES)).astype(np.int64)
+        unit_tiles = int(unit_tiles)
+        if unit_tiles < 1:
+            raise ValueError('unit_tiles must be positive')
+        parts = np.maximum(1, -(-n_active // unit_tiles)).astype(np.int64)
         n_slices = self.n_bands * parts
         blobs['n_slices'] = n_slices
         blobs['unit0'] = np.concatenate([[0], np.cumsum(n_slices)[:-1]])
