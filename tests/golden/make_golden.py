@@ -725,6 +725,51 @@ def composite():
     print('composite fixture written to', OUT)
 
 
+def edges():
+    """Empty and degenerate inputs through the object API (engine.py,
+    galaxy.py, pointsource.py) on a 50 x 40 image with a constant sky: a
+    catalog with no sources; galaxies and point sources entirely off the
+    image or of zero flux; a ModelMask off the image.  The model images, the
+    log-likelihoods, every patch (None where the reference returns None) and
+    getDerivs' entries per parameter (image parameters thawed)."""
+    from oracle import refharness
+    refharness.load()
+    from tractor import (Image, Tractor, PixPos, Flux, LinearPhotoCal, NCircularGaussianPSF,
+                         EllipseE, ConstantSky, PointSource, ExpGalaxy)
+    from tractor.patch import ModelMask
+    data = np.random.default_rng(44).normal(2.5, 1., (40, 50))
+
+    def image():
+        return Image(data=data.copy(), invvar=np.ones((40, 50)),
+                     psf=NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2]),
+                     photocal=LinearPhotoCal(1.), sky=ConstantSky(2.5))
+    arrays = {'data': data}
+    tr0 = Tractor([image()], [])
+    arrays['empty_model'] = tr0.getModelImage(0)
+    arrays['empty_lnl'] = tr0.getLogLikelihood()
+    tim = image()
+    srcs = [ExpGalaxy(PixPos(-200., 20.), Flux(100.), EllipseE(2., 0.1, 0.)),
+            PointSource(PixPos(300., 20.), Flux(100.)),
+            ExpGalaxy(PixPos(20., 20.), Flux(0.), EllipseE(2., 0.1, 0.)),
+            PointSource(PixPos(20., 20.), Flux(0.))]
+    patches = [s.getModelPatch(tim) for s in srcs]
+    mm = ModelMask(500, 500, 10, 10)
+    patches += [s.getModelPatch(tim, modelMask=mm)
+                for s in (ExpGalaxy(PixPos(20., 20.), Flux(100.), EllipseE(2., 0.1, 0.)),
+                          PointSource(PixPos(20., 20.), Flux(100.)))]
+    for k, v in patches_to_arrays(patches).items():
+        arrays['patches.' + k] = v
+    tr = Tractor([tim], srcs)
+    arrays['model'] = tr.getModelImage(0)
+    arrays['lnl'] = tr.getLogLikelihood()
+    d = tr.getDerivs()
+    arrays['deriv_count'] = np.array([len(x) for x in d])
+    for k, v in patches_to_arrays([p for x in d for (p, _) in x]).items():
+        arrays['derivs.' + k] = v
+    np.savez_compressed(os.path.join(OUT, 'edges.npz'), **arrays)
+    print('edge-case fixture written to', OUT)
+
+
 def fittight():
     """The optimum of the small plain fit (scenario 4) in FP64, found on the
     reference's own FP64 model: scipy.optimize.least_squares on
@@ -796,5 +841,7 @@ if __name__ == '__main__':
         varying()
     elif sys.argv[1:] == ['composite']:
         composite()
+    elif sys.argv[1:] == ['edges']:
+        edges()
     else:
         main()

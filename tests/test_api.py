@@ -659,3 +659,53 @@ def test_image_fits_round_trip(tmp_path):
     assert tim2.getSky().getValue() == 3.5
     assert tim2.getPhotoCal().getScale() == 2.5
     assert isinstance(tim2.getWcs(), T.NullWCS)
+
+
+def test_empty_and_degenerate_inputs_match_reference(backend):
+    """Empty and degenerate inputs against the reference's own results
+    (tests/golden/edges.npz): an empty catalog renders the sky alone; sources
+    entirely off the image, or of zero flux, have no patch and leave the
+    model at the sky; a ModelMask off the image gives a patch of zeros on
+    the mask; getDerivs gives no entries for the off-image sources' and the
+    zero-flux sources' non-flux parameters, the unit-flux patch for a
+    zero-flux source's flux, and the image parameters' columns."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'edges.npz'))
+
+    def image():
+        return T.Image(data=g['data'].copy(), invvar=np.ones((40, 50)),
+                       psf=T.NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2]),
+                       photocal=T.LinearPhotoCal(1.), sky=T.ConstantSky(2.5))
+    tr0 = T.Tractor([image()], [])
+    m0 = tr0.getModelImage(0)
+    assert m0.shape == g['empty_model'].shape and np.array_equal(m0, g['empty_model'])
+    assert abs(tr0.getLogLikelihood() - g['empty_lnl']) <= 1e-12 * abs(g['empty_lnl'])
+    tim = image()
+    srcs = [T.ExpGalaxy(T.PixPos(-200., 20.), T.Flux(100.), T.EllipseE(2., 0.1, 0.)),
+            T.PointSource(T.PixPos(300., 20.), T.Flux(100.)),
+            T.ExpGalaxy(T.PixPos(20., 20.), T.Flux(0.), T.EllipseE(2., 0.1, 0.)),
+            T.PointSource(T.PixPos(20., 20.), T.Flux(0.))]
+    patches = [s.getModelPatch(tim) for s in srcs]
+    mm = T.ModelMask(500, 500, 10, 10)
+    patches += [s.getModelPatch(tim, modelMask=mm)
+                for s in (T.ExpGalaxy(T.PixPos(20., 20.), T.Flux(100.), T.EllipseE(2., 0.1, 0.)),
+                          T.PointSource(T.PixPos(20., 20.), T.Flux(100.)))]
+    for i, (p, ref) in enumerate(zip(patches, _unpack(g, 'patches'))):
+        if ref is None:
+            assert p is None or p.patch is None, i
+        else:
+            assert (p.x0, p.y0) == ref[:2] and np.array_equal(p.patch, ref[2]), i
+    tr = T.Tractor([tim], srcs)
+    m = tr.getModelImage(0)
+    assert np.array_equal(m, g['model'])
+    assert abs(tr.getLogLikelihood() - g['lnl']) <= 1e-12 * abs(g['lnl'])
+    d = tr.getDerivs()
+    assert [len(x) for x in d] == g['deriv_count'].tolist()
+    flat = [p for x in d for (p, _) in x]
+    for i, (p, ref) in enumerate(zip(flat, _unpack(g, 'derivs'))):
+        if ref is None:
+            assert p is None or p.patch is None, i
+            continue
+        assert (p.x0, p.y0) == ref[:2] and p.patch.shape == ref[2].shape, i
+        scale = max(np.abs(ref[2]).max(), 1e-30)
+        assert np.abs(p.patch - ref[2]).max() <= 1e-5 * scale, i

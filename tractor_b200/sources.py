@@ -290,8 +290,10 @@ class Galaxy(MultiParams, SingleProfileSource):
         shape_plans = None
         mm_fixed = modelMask
         if mm_fixed is None and self._extent_known(img, px0, py0, minval):
-            x0, x1, y0, y1 = self._no_mask_extent(img, px0, py0, minval)
-            mm_fixed = ModelMask.fromExtent(x0, x1, y0, y1)
+            ext = self._no_mask_extent(img, px0, py0, minval)
+            # (no extent: the source misses the image and patch0 is None)
+            if ext is not None:
+                mm_fixed = ModelMask.fromExtent(*ext)
         if mm_fixed is not None:
             shape_plans = self._plan_shape_steps(plan, img, px0, py0, minval, mm_fixed, counts,
                                                  **kwargs)
