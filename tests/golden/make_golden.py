@@ -766,6 +766,11 @@ def edges():
     arrays['deriv_count'] = np.array([len(x) for x in d])
     for k, v in patches_to_arrays([p for x in d for (p, _) in x]).items():
         arrays['derivs.' + k] = v
+    # a galaxy much smaller than a pixel: its shape columns are small
+    # differences of two FP64 renders
+    tiny = ExpGalaxy(PixPos(20.3, 19.6), Flux(100.), EllipseE(0.02, 0.2, -0.1))
+    for k, v in patches_to_arrays(tiny.getParamDerivatives(image())).items():
+        arrays['tiny.' + k] = v
     np.savez_compressed(os.path.join(OUT, 'edges.npz'), **arrays)
     print('edge-case fixture written to', OUT)
 

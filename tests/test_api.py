@@ -709,3 +709,51 @@ def test_empty_and_degenerate_inputs_match_reference(backend):
         assert (p.x0, p.y0) == ref[:2] and p.patch.shape == ref[2].shape, i
         scale = max(np.abs(ref[2]).max(), 1e-30)
         assert np.abs(p.patch - ref[2]).max() <= 1e-5 * scale, i
+
+
+def test_small_galaxy_shape_columns(backend):
+    """A galaxy much smaller than a pixel (ExpGalaxy, r_e 0.02 px, MoG PSF):
+    its shape columns are small differences of two renders, and against the
+    reference's own FP64 columns (tests/golden/edges.npz) they hold to 1e-4
+    of their peak, as every column does: the stepped and the unstepped
+    mixtures are rendered as one difference item, so the float32 error is
+    relative to the difference."""
+    import tractor_b200 as T
+    g = np.load(os.path.join(GOLDEN, 'edges.npz'))
+    tim = T.Image(data=g['data'].copy(), invvar=np.ones((40, 50)),
+                  psf=T.NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2]),
+                  photocal=T.LinearPhotoCal(1.), sky=T.ConstantSky(2.5))
+    src = T.ExpGalaxy(T.PixPos(20.3, 19.6), T.Flux(100.), T.EllipseE(0.02, 0.2, -0.1))
+    got = src.getParamDerivatives(tim)
+    ref = _unpack(g, 'tiny')
+    assert len(got) == len(ref) == 6
+    for i, (p, r) in enumerate(zip(got, ref)):
+        _check_patch(p, r, DERIV_TOL, 'column %d' % i)
+
+
+@pytest.mark.gpu
+def test_small_galaxy_fourier_shape_columns_are_exact(tb, oracle):
+    """The same on the pixelized-PSF (Fourier) path: a SersicGalaxy with r_e
+    0.02 px on a 64 x 64 ModelMask; its shape columns against the FP64
+    forward difference (step 0.01, galaxy.py:196-222) of the oracle's FP64
+    Fourier model, to 1e-4 of their peak.  (The reference's own columns
+    cast both renders to float32 before subtracting them, galaxy.py:470,
+    which for such a galaxy leaves them mostly rounding.)"""
+    import tractor_b200 as T
+    from tractor_b200 import batch
+    psf_img = batch.moffat_psf()
+    th = [32.3, 31.6, 1000., 0.02, 0.2, -0.1, 2.5]
+    src = T.SersicGalaxy(T.PixPos(th[0], th[1]), T.Flux(th[2]), T.EllipseE(*th[3:6]),
+                         T.SersicIndex(th[6]))
+    tim = T.Image(data=np.zeros((64, 64), np.float32), inverr=np.ones((64, 64), np.float32),
+                  psf=T.PixelizedPSF(psf_img), photocal=T.LinearPhotoCal(1.))
+    d = src.getParamDerivatives(tim, modelMask=T.ModelMask(0, 0, 64, 64))
+    base = oracle.sersic_fft_model_f64(th, psf_img, 0, 0, 64, 64)
+    for j in (3, 4, 5):
+        t2 = list(th)
+        t2[j] += 0.01
+        exact = (oracle.sersic_fft_model_f64(t2, psf_img, 0, 0, 64, 64) - base) / 0.01
+        p = d[j]
+        assert (p.x0, p.y0) == (0, 0) and p.patch.shape == exact.shape, j
+        err = np.abs(p.patch - exact).max() / np.abs(exact).max()
+        assert err < 1e-4, (j, err)

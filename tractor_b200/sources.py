@@ -235,6 +235,22 @@ class PointSource(MultiParams, SingleProfileSource):
 # Galaxies
 # ---------------------------------------------------------------------------
 
+class _SteppedProfiles(object):
+    """A galaxy's affine and sheared profiles at (px, py), taken when this
+    is made (with a parameter stepped): the `diff_of` of a difference
+    render, which reads only these two."""
+
+    def __init__(self, gal, img, px, py):
+        self.affine = gal._getAffineProfile(img, px, py)
+        self.sheared = gal._getShearedProfile(img, px, py)
+
+    def _getAffineProfile(self, img, px, py):
+        return self.affine
+
+    def _getShearedProfile(self, img, px, py):
+        return self.sheared
+
+
 class Galaxy(MultiParams, SingleProfileSource):
     """Position, brightness, shape (tractor/galaxy.py:92-223)."""
 
@@ -352,12 +368,15 @@ class Galaxy(MultiParams, SingleProfileSource):
                 if counts == 0:
                     derivs.extend([None] * len(self.shape.getParams()))
                 else:
-                    for i, (gstep, pend) in enumerate(sp):
+                    for i, (gstep, pend, is_diff) in enumerate(sp):
                         patchx = pend.result()
                         if patchx is None:
                             derivs.append(None)
                             continue
-                        d = (patchx - patch0) * (counts / gstep)
+                        if is_diff:
+                            d = patchx * (counts / gstep)
+                        else:
+                            d = (patchx - patch0) * (counts / gstep)
                         d.setName('d(%s)/d(%s)' % (self.dname, gnames[i]))
                         derivs.append(d)
             derivs.extend(self._finish_extra(ex, patch0, counts) if ex is not None else [])
@@ -370,18 +389,36 @@ class Galaxy(MultiParams, SingleProfileSource):
         return []
 
     def _plan_shape_steps(self, plan, img, px0, py0, minval, mm, counts, **kwargs):
-        """The forward-difference shape renders (galaxy.py:196-222)."""
+        """The forward-difference shape renders (galaxy.py:196-222), on
+        patch0's rectangle `mm`.  Returns (step, pending, is_difference) per
+        shape parameter.  Without a minval cut or a hybrid PSF the stepped
+        and the unstepped mixtures render the same rectangle with as many
+        components and the same means, so the difference patchx - patch0 is
+        rendered directly as difference items (as the Sersic-index column):
+        its float32 error is then relative to the difference, not to the two
+        patches, which matters where a shape step barely changes the model
+        (a galaxy much smaller than a pixel).  Otherwise patchx is rendered
+        and patch0 subtracted, as the reference does."""
         if self.isParamFrozen('shape') or counts == 0:
             return []
         gsteps = self.shape.getStepSizes()
         oldvals = self.shape.getParams()
+        diff_ok = (mm is not None and minval in (0., None)
+                   and not isinstance(img.getPsf(), HybridPSF))
         out = []
         for i, gstep in enumerate(gsteps):
             old = self.shape.setParam(i, oldvals[i] + gstep)
-            p = self._plan_unit_patch(plan, img, px=px0, py=py0, minval=minval, modelMask=mm,
-                                      force_sourceOut=True, **kwargs)
-            self.shape.setParam(i, old)
-            out.append((gstep, p))
+            if diff_ok:
+                stepped = _SteppedProfiles(self, img, px0, py0)
+                self.shape.setParam(i, old)
+                p = self._plan_unit_patch(plan, img, px=px0, py=py0, minval=minval,
+                                          modelMask=mm, force_sourceOut=True, diff_of=stepped,
+                                          **kwargs)
+            else:
+                p = self._plan_unit_patch(plan, img, px=px0, py=py0, minval=minval,
+                                          modelMask=mm, force_sourceOut=True, **kwargs)
+                self.shape.setParam(i, old)
+            out.append((gstep, p, diff_ok))
         return out
 
     def _extent_known(self, img, px, py, minval):
