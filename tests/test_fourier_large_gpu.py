@@ -5,8 +5,8 @@ getModelPatch / getParamDerivatives through the large-size path
 against the oracle's restatement of the reference's FFT branch.
 
 Tolerances as for the other sizes: model pixels within 1e-5 of the patch
-peak, the Sersic-index column within 1e-4 of its peak against the exact FP64
-forward difference."""
+peak, the shape and Sersic-index columns within 1e-4 of their peak against
+the exact FP64 forward differences."""
 import numpy as np
 import pytest
 
@@ -59,14 +59,16 @@ def test_large_fft_galaxy_matches_oracle(tb, oracle, case):
     assert sz == want_sz
     _check(p, mx0, my0, 1000. * ref, PEAK_TOL, '%s %d' % (kind, sz))
     if kind == 'sersic' and sz == 512:
-        # the Sersic-index column (a difference item of the large-size path)
+        # the shape and Sersic-index columns (difference items of the
+        # large-size path) against FP64 forward differences of step 0.01
         d = gal.getParamDerivatives(tim, modelMask=mm)
         th = [px, py, 1000., re, e1, e2, n]
-        th2 = list(th)
-        th2[6] = n + 0.01
-        exact = (oracle.sersic_fft_model_f64(th2, psf_img, mx0, my0, mw, mh) -
-                 oracle.sersic_fft_model_f64(th, psf_img, mx0, my0, mw, mh)) / 0.01
-        _check(d[-1], mx0, my0, exact, DERIV_TOL, 'sersic-index column %d' % sz)
+        base = oracle.sersic_fft_model_f64(th, psf_img, mx0, my0, mw, mh)
+        for j in (3, 4, 5, 6):
+            th2 = list(th)
+            th2[j] += 0.01
+            exact = (oracle.sersic_fft_model_f64(th2, psf_img, mx0, my0, mw, mh) - base) / 0.01
+            _check(d[j], mx0, my0, exact, DERIV_TOL, 'column %d at size %d' % (j, sz))
 
 
 def test_large_psf_spectrum_matches_numpy(tb):
