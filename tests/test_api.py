@@ -757,3 +757,23 @@ def test_small_galaxy_fourier_shape_columns_are_exact(tb, oracle):
         assert (p.x0, p.y0) == (0, 0) and p.patch.shape == exact.shape, j
         err = np.abs(p.patch - exact).max() / np.abs(exact).max()
         assert err < 1e-4, (j, err)
+
+
+def test_fourier_source_outside_its_mask(backend):
+    """A SersicGalaxy on a PixelizedPSF image whose ModelMask does not
+    contain its centre, farther than its radius (galaxy.py:354-370): the
+    reference returns no patch and no derivative columns; the shape steps
+    (rendered with force_sourceOut, which on a non-hybrid PSF raises) are
+    not taken then."""
+    import tractor_b200 as T
+    from tractor_b200 import batch
+    tim = T.Image(data=np.zeros((40, 50), np.float32), inverr=np.ones((40, 50), np.float32),
+                  psf=T.PixelizedPSF(batch.moffat_psf(25)), photocal=T.LinearPhotoCal(1.))
+    gal = T.SersicGalaxy(T.PixPos(10.3, 12.2), T.Flux(100.), T.EllipseE(2., 0.1, 0.),
+                         T.SersicIndex(3.))
+    mm = T.ModelMask(30, 25, 15, 12)
+    p = gal.getModelPatch(tim, modelMask=mm)
+    assert p is None or p.patch is None
+    d = gal.getParamDerivatives(tim, modelMask=mm)
+    assert len(d) == gal.numberOfParams()
+    assert all(x is None or x.patch is None for x in d)

@@ -305,7 +305,12 @@ class Galaxy(MultiParams, SingleProfileSource):
         # common case (a mask, or an exact grid) is known in advance.
         shape_plans = None
         mm_fixed = modelMask
-        if mm_fixed is None and self._extent_known(img, px0, py0, minval):
+        if modelMask is not None and (px0 < modelMask.x0 or px0 > modelMask.x1 - 1 or
+                                      py0 < modelMask.y0 or py0 > modelMask.y1 - 1):
+            # the source lies outside its mask: patch0 may be None (the
+            # reference then takes no shape step), so the steps wait for it
+            mm_fixed = None
+        elif mm_fixed is None and self._extent_known(img, px0, py0, minval):
             ext = self._no_mask_extent(img, px0, py0, minval)
             # (no extent: the source misses the image and patch0 is None)
             if ext is not None:
@@ -335,9 +340,9 @@ class Galaxy(MultiParams, SingleProfileSource):
             if mm is None:
                 x0, x1, y0, y1 = patch0.getExtent()
                 mm = ModelMask.fromExtent(x0, x1, y0, y1)
-                if sp is None:
-                    sub = RenderPlan()
-                    sp = self._plan_shape_steps(sub, img, px0, py0, minval, mm, counts, **kwargs)
+            if sp is None:
+                sub = RenderPlan()
+                sp = self._plan_shape_steps(sub, img, px0, py0, minval, mm, counts, **kwargs)
             if self.isParamThawed('pos') and self.pos.numberOfParams() > 0:
                 if counts == 0:
                     derivs.extend([None] * len(pos0.getParams()))
