@@ -235,6 +235,13 @@ class PointSource(MultiParams, SingleProfileSource):
 # Galaxies
 # ---------------------------------------------------------------------------
 
+class _NoDifference(Exception):
+    """Raised while planning a difference render that one difference item
+    cannot stand for (a hybrid PSF splitting the two mixtures' components
+    differently between its Fourier and pixel-space parts), before anything
+    is added to the plan; the caller renders and subtracts instead."""
+
+
 class _SteppedProfiles(object):
     """A galaxy's affine and sheared profiles at (px, py), taken when this
     is made (with a parameter stepped): the `diff_of` of a difference
@@ -317,6 +324,7 @@ class Galaxy(MultiParams, SingleProfileSource):
                 mm_fixed = ModelMask.fromExtent(*ext)
         if mm_fixed is not None:
             shape_plans = self._plan_shape_steps(plan, img, px0, py0, minval, mm_fixed, counts,
+                                                 patch0_mask=modelMask,
                                                  **kwargs)
         # Extra columns (Sersic index) render with the caller's modelMask.
         extra = self._extra_derivative_renders(plan, img, px0, py0, modelMask, minval, counts,
@@ -342,7 +350,8 @@ class Galaxy(MultiParams, SingleProfileSource):
                 mm = ModelMask.fromExtent(x0, x1, y0, y1)
             if sp is None:
                 sub = RenderPlan()
-                sp = self._plan_shape_steps(sub, img, px0, py0, minval, mm, counts, **kwargs)
+                sp = self._plan_shape_steps(sub, img, px0, py0, minval, mm, counts,
+                                            patch0_mask=modelMask, **kwargs)
             if self.isParamThawed('pos') and self.pos.numberOfParams() > 0:
                 if counts == 0:
                     derivs.extend([None] * len(pos0.getParams()))
@@ -393,7 +402,8 @@ class Galaxy(MultiParams, SingleProfileSource):
     def _finish_extra(self, extra, patch0, counts):
         return []
 
-    def _plan_shape_steps(self, plan, img, px0, py0, minval, mm, counts, **kwargs):
+    def _plan_shape_steps(self, plan, img, px0, py0, minval, mm, counts, patch0_mask=None,
+                          **kwargs):
         """The forward-difference shape renders (galaxy.py:196-222), on
         patch0's rectangle `mm`.  Returns (step, pending, is_difference) per
         shape parameter.  Without a minval cut or a hybrid PSF the stepped
@@ -408,22 +418,34 @@ class Galaxy(MultiParams, SingleProfileSource):
             return []
         gsteps = self.shape.getStepSizes()
         oldvals = self.shape.getParams()
-        diff_ok = (mm is not None and minval in (0., None)
-                   and not isinstance(img.getPsf(), HybridPSF))
+        # One difference item stands for patchx - patch0 only when both are
+        # rendered the same way: on the Fourier path a source outside `mm`
+        # is rendered in pixel space (hybrid PSF, galaxy.py:354-372), so
+        # unless patch0 had that same mask its render took the other path.
+        psf = img.getPsf()
+        pure_mog = hasattr(psf, 'getMixtureOfGaussians') and not isinstance(psf, HybridPSF)
+        outside = mm is not None and (px0 < mm.x0 or px0 > mm.x1 - 1 or
+                                      py0 < mm.y0 or py0 > mm.y1 - 1)
+        diff_ok = (mm is not None and minval in (0., None) and
+                   (pure_mog or not outside or mm is patch0_mask))
         out = []
         for i, gstep in enumerate(gsteps):
             old = self.shape.setParam(i, oldvals[i] + gstep)
             if diff_ok:
                 stepped = _SteppedProfiles(self, img, px0, py0)
                 self.shape.setParam(i, old)
-                p = self._plan_unit_patch(plan, img, px=px0, py=py0, minval=minval,
-                                          modelMask=mm, force_sourceOut=True, diff_of=stepped,
-                                          **kwargs)
-            else:
-                p = self._plan_unit_patch(plan, img, px=px0, py=py0, minval=minval,
-                                          modelMask=mm, force_sourceOut=True, **kwargs)
-                self.shape.setParam(i, old)
-            out.append((gstep, p, diff_ok))
+                try:
+                    p = self._plan_unit_patch(plan, img, px=px0, py=py0, minval=minval,
+                                              modelMask=mm, force_sourceOut=True,
+                                              diff_of=stepped, **kwargs)
+                    out.append((gstep, p, True))
+                    continue
+                except _NoDifference:
+                    self.shape.setParam(i, oldvals[i] + gstep)
+            p = self._plan_unit_patch(plan, img, px=px0, py=py0, minval=minval,
+                                      modelMask=mm, force_sourceOut=True, **kwargs)
+            self.shape.setParam(i, old)
+            out.append((gstep, p, False))
         return out
 
     def _extent_known(self, img, px, py, minval):
@@ -503,7 +525,7 @@ class ProfileGalaxy(object):
         psf = img.getPsf()
         hybrid = isinstance(psf, HybridPSF)
 
-        def run_mog(amix=None, mm=None):
+        def run_mog(amix=None, mm=None, damix=None):
             if amix is None:
                 amix = self._getAffineProfile(img, px, py)
             if mm is None:
@@ -512,7 +534,9 @@ class ProfileGalaxy(object):
             cmix = amix.convolve(psfmix)
             dmix = None
             if diff_of is not None:
-                dmix = diff_of._getAffineProfile(img, px, py).convolve(psfmix)
+                if damix is None:
+                    damix = diff_of._getAffineProfile(img, px, py)
+                dmix = damix.convolve(psfmix)
             if mm is None:
                 if dmix is not None:
                     return plan_mog_grid(plan, cmix, x0, x1, y0, y1, 0., 0., diff=dmix)
@@ -582,18 +606,41 @@ class ProfileGalaxy(object):
         amix = self._getShearedProfile(img, px, py)
         fftmix = amix
         mogmix = None
+        dfft = None     # a difference item's second mixture: (amp, var) of the FFT part
+        dmog = None     # and the pixel-space part's (an affine MixtureOfGaussians)
+        if diff_of is not None:
+            other = diff_of._getShearedProfile(img, px, py)
+            dfft = (other.amp, other.var)
         if hybrid and inner_real_nsigma is not None and outer_real_nsigma is not None:
-            vv = amix.var[:, 0, 0] + amix.var[:, 1, 1]
             nsigma1, nsigma2 = inner_real_nsigma, outer_real_nsigma
-            IM = ((pW / 2) ** 2 < (nsigma2 ** 2 * vv))
-            IF = ((pW / 2) ** 2 > (nsigma1 ** 2 * vv))
-            ramp = np.any(IM * IF)
+
+            def split(mix):
+                # components for pixel space (IM) and for the FFT (IF), and
+                # their weights across the ramp between the two
+                vv = mix.var[:, 0, 0] + mix.var[:, 1, 1]
+                IM = ((pW / 2) ** 2 < (nsigma2 ** 2 * vv))
+                IF = ((pW / 2) ** 2 > (nsigma1 ** 2 * vv))
+                mw_, fw_ = np.ones(int(IM.sum())), np.ones(int(IF.sum()))
+                if np.any(IM * IF):
+                    ns = (pW / 2) / np.maximum(1e-6, np.sqrt(vv))
+                    mw_ = np.minimum(1., (nsigma2 - ns[IM]) / (nsigma2 - nsigma1))
+                    fw_ = np.minimum(1., (ns[IF] - nsigma1) / (nsigma2 - nsigma1))
+                return IM, IF, np.any(IM * IF), mw_, fw_
+            IM, IF, ramp, mogweights, fftweights = split(amix)
+            if diff_of is not None:
+                if len(other.amp) != len(amix.amp):
+                    raise _NoDifference()
+                IM2, IF2, ramp2, mw2, fw2 = split(other)
+                if not (np.array_equal(IM, IM2) and np.array_equal(IF, IF2)):
+                    raise _NoDifference()
+                dfft = (other.amp[IF] * fw2 if ramp2 else other.amp[IF], other.var[IF])
+                if np.any(IM):
+                    dmog = MixtureOfGaussians(other.amp[IM] * mw2 if ramp2 else other.amp[IM],
+                                              amix.mean[IM, :] + np.array([px, py]),
+                                              other.var[IM], quick=True)
             if np.any(IM):
                 amps = amix.amp[IM]
                 if ramp:
-                    ns = (pW / 2) / np.maximum(1e-6, np.sqrt(vv))
-                    mogweights = np.minimum(1., (nsigma2 - ns[IM]) / (nsigma2 - nsigma1))
-                    fftweights = np.minimum(1., (ns[IF] - nsigma1) / (nsigma2 - nsigma1))
                     amps = amps * mogweights
                 mogmix = MixtureOfGaussians(amps, amix.mean[IM, :] + np.array([px, py]),
                                             amix.var[IM, :, :], quick=True)
@@ -615,18 +662,14 @@ class ProfileGalaxy(object):
             rx0, ry0, rw, rh = gx0, gy0, max(0, gx1 - gx0), max(0, gy1 - gy0)
             ssx, ssy = ix0 - rx0, iy0 - ry0
         if fftmix is not None and rw > 0 and rh > 0:
-            dmix = None
-            if diff_of is not None:
-                other = diff_of._getShearedProfile(img, px, py)
-                dmix = (other.amp, other.var)
             h = plan.add_fft(fftmix.amp, fftmix.var, sz, spec_key, spec, rw, rh, ssx, ssy,
-                             mux, muy, diff=dmix)
+                             mux, muy, diff=dfft)
         else:
             h = ('empty', rh, rw)
         mogp = None
         if mogmix is not None:
             mogp = run_mog(amix=mogmix, mm=modelMask if modelMask is not None else
-                           ModelMask(rx0, ry0, rw, rh))
+                           ModelMask(rx0, ry0, rw, rh), damix=dmog)
 
         def finish():
             G = np.array(plan.get(h), np.float32)
@@ -786,9 +829,12 @@ class SersicGalaxy(HoggGalaxy):
         other = self.copy()
         other.sersicindex.setParam(0, old + step)
         if self._difference_render_ok(img, other, px0, py0, modelMask, minval):
-            p = self._plan_unit_patch(plan, img, px=px0, py=py0, modelMask=modelMask,
-                                      diff_of=other, **kwargs)
-            return [(step, p, True)]
+            try:
+                p = self._plan_unit_patch(plan, img, px=px0, py=py0, modelMask=modelMask,
+                                          diff_of=other, **kwargs)
+                return [(step, p, True)]
+            except _NoDifference:
+                pass
         self.sersicindex.setParam(0, old + step)
         p = self._plan_unit_patch(plan, img, px=px0, py=py0, modelMask=modelMask, **kwargs)
         self.sersicindex.setParam(0, old)
@@ -796,10 +842,11 @@ class SersicGalaxy(HoggGalaxy):
 
     def _difference_render_ok(self, img, other, px, py, modelMask, minval):
         """True when patch0 (minval) and other's default-minval render are
-        exact renders of the same rectangle by mixtures of equal size: a
-        non-hybrid PSF, no minval cut, equal component counts and, without
-        a mask, equal patch extents."""
-        if minval not in (0., None) or isinstance(img.getPsf(), HybridPSF):
+        exact renders of the same rectangle by mixtures of equal size: no
+        minval cut, equal component counts and, without a mask, equal patch
+        extents (a hybrid PSF that splits the two mixtures differently is
+        found while planning: _NoDifference)."""
+        if minval not in (0., None):
             return False
         if len(self.getProfile().amp) != len(other.getProfile().amp):
             return False
