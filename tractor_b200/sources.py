@@ -243,19 +243,29 @@ class _NoDifference(Exception):
 
 
 class _SteppedProfiles(object):
-    """A galaxy's affine and sheared profiles at (px, py), taken when this
-    is made (with a parameter stepped): the `diff_of` of a difference
-    render, which reads only these two."""
+    """The `diff_of` of a difference render: a galaxy's affine and sheared
+    profiles with shape parameter i set to `value`, each computed when the
+    render path first asks for it (the shape is stepped for that call and
+    restored)."""
 
-    def __init__(self, gal, img, px, py):
-        self.affine = gal._getAffineProfile(img, px, py)
-        self.sheared = gal._getShearedProfile(img, px, py)
+    def __init__(self, gal, i, value):
+        self.gal, self.i, self.value = gal, i, value
+        self.cache = {}
+
+    def _profile(self, method, img, px, py):
+        if method not in self.cache:
+            old = self.gal.shape.setParam(self.i, self.value)
+            try:
+                self.cache[method] = getattr(self.gal, method)(img, px, py)
+            finally:
+                self.gal.shape.setParam(self.i, old)
+        return self.cache[method]
 
     def _getAffineProfile(self, img, px, py):
-        return self.affine
+        return self._profile('_getAffineProfile', img, px, py)
 
     def _getShearedProfile(self, img, px, py):
-        return self.sheared
+        return self._profile('_getShearedProfile', img, px, py)
 
 
 class Galaxy(MultiParams, SingleProfileSource):
@@ -430,10 +440,8 @@ class Galaxy(MultiParams, SingleProfileSource):
                    (pure_mog or not outside or mm is patch0_mask))
         out = []
         for i, gstep in enumerate(gsteps):
-            old = self.shape.setParam(i, oldvals[i] + gstep)
             if diff_ok:
-                stepped = _SteppedProfiles(self, img, px0, py0)
-                self.shape.setParam(i, old)
+                stepped = _SteppedProfiles(self, i, oldvals[i] + gstep)
                 try:
                     p = self._plan_unit_patch(plan, img, px=px0, py=py0, minval=minval,
                                               modelMask=mm, force_sourceOut=True,
@@ -441,7 +449,8 @@ class Galaxy(MultiParams, SingleProfileSource):
                     out.append((gstep, p, True))
                     continue
                 except _NoDifference:
-                    self.shape.setParam(i, oldvals[i] + gstep)
+                    pass
+            old = self.shape.setParam(i, oldvals[i] + gstep)
             p = self._plan_unit_patch(plan, img, px=px0, py=py0, minval=minval,
                                       modelMask=mm, force_sourceOut=True, **kwargs)
             self.shape.setParam(i, old)
