@@ -144,3 +144,51 @@ def test_corner_case_matches_reference(case, ref_ns, host_only):
         masked_f32 = mask == 'bool' and j >= 3
         tol = 1e-3 if (fourier_step or index_edge) else (1e-4 if masked_f32 else 1e-5)
         _same(od[j], rd[j], tol, 'column %d' % j)
+
+
+def _fit_scene(M, opt_cls):
+    rng = np.random.default_rng(9)
+    T = M.T
+
+    def srcs():
+        return [T.PointSource(T.PixPos(12.3, 14.1), T.Flux(200.)),
+                T.PointSource(T.PixPos(-100., 14.1), T.Flux(200.)),
+                T.ExpGalaxy(T.PixPos(30.2, 25.7), T.Flux(0.), T.EllipseE(2., 0.1, 0.)),
+                T.ExpGalaxy(T.PixPos(35.2, 15.7), T.Flux(300.), T.EllipseE(2., 0.1, 0.))]
+    tim = T.Image(data=rng.normal(0., 1., (40, 50)), invvar=np.ones((40, 50)),
+                  psf=T.NCircularGaussianPSF([1.5, 3.0], [0.8, 0.2]),
+                  photocal=T.LinearPhotoCal(1.), sky=T.ConstantSky(0.))
+    tr = T.Tractor([tim], srcs(), optimizer=opt_cls())
+    tr.freezeParam('images')
+    truth = tr.getModelImage(0)
+    tim.data = truth + np.random.default_rng(3).normal(0, 1., truth.shape)
+    return tr
+
+
+def test_forced_photometry_and_fit_with_corner_sources(ref_ns, host_only):
+    """A catalog with a source off the image and one of zero flux beside
+    two ordinary ones: forced photometry (fluxes, fit statistics) and an
+    optimize_loop (parameters, steps) end where the reference's do."""
+    from tractor.lsqr_optimizer import LsqrOptimizer as RefLsqr
+    import tractor_b200 as T
+    rtr, otr = _fit_scene(ref_ns, RefLsqr), _fit_scene(_ours(), T.LsqrOptimizer)
+    for tr in (rtr, otr):
+        tr.freezeParamsRecursive('*')
+        tr.thawPathsTo('brightness')
+    rr = rtr.optimize_forced_photometry(fitstats=True)
+    orr = otr.optimize_forced_photometry(fitstats=True)
+    rp, op = np.array(rtr.getParams()), np.array(otr.getParams())
+    assert np.all(np.abs(op - rp) <= 1e-4 * np.maximum(np.abs(rp), 1.)), (op, rp)
+    for k in ('prochi2', 'pronpix', 'profracflux', 'proflux', 'npix'):
+        a = np.asarray(getattr(rr.fitstats, k), np.float64)
+        b = np.asarray(getattr(orr.fitstats, k), np.float64)
+        scale = np.nanmax(np.abs(a)) if np.any(np.isfinite(a)) else 0.
+        assert np.allclose(a, b, rtol=1e-4, atol=1e-4 * scale, equal_nan=True), (k, a, b)
+    rtr, otr = _fit_scene(ref_ns, RefLsqr), _fit_scene(_ours(), T.LsqrOptimizer)
+    for tr in (rtr, otr):
+        tr.setParams(np.array(tr.getParams()) * 1.01)
+    rs = rtr.optimize_loop(dchisq=1e-3, steps=30)
+    os_ = otr.optimize_loop(dchisq=1e-3, steps=30)
+    rp, op = np.array(rtr.getParams()), np.array(otr.getParams())
+    assert rs['steps'] == os_['steps']
+    assert np.all(np.abs(op - rp) <= 1e-4 * np.maximum(np.abs(rp), 1.)), (op, rp)
