@@ -14,7 +14,12 @@ PSFs, which the reference takes as differences of two float32 renders
 up to 1e-3 there, and a Sersic index stepped across a profile-range edge
 (the mixture changes size; both sides subtract two renders); with a boolean
 mask the reference evaluates in float32 (gauss_masked.c), so its shape
-columns are differences of float32 patches: 1e-4."""
+columns are differences of float32 patches: 1e-4; with a minval (approx3)
+the reference stays in FP64 while the renders here are float32 patches
+and their derivative planes: the derivative bar, 1e-4, and 1e-3 for the
+Sersic-index column, which the reference takes as a full-grid render
+(sersic.py:431-432 passes no minval) minus the approx3-cut patch0, so that
+both sides subtract two renders and the float32 ones here cancel."""
 import types
 
 import numpy as np
@@ -82,9 +87,10 @@ def _mask(M, m):
     return M.ModelMask(*m)
 
 
-def _run(M, psf, src, mask):
+def _run(M, psf, src, mask, minval=0.):
     tim = M.T.Image(data=np.zeros((40, 50)), invvar=np.ones((40, 50)), psf=_psf(M, psf),
                     photocal=M.T.LinearPhotoCal(1.))
+    tim.modelMinval = minval
     s = _source(M, src)
     mm = _mask(M, mask)
     patch = s.getModelPatch(tim, modelMask=mm)
@@ -112,6 +118,13 @@ CASES = [
     ('mog', ('pt', 11.3, 9.6, 100., None), (0, 0, 15, 14)),
     ('mog', ('exp', -200., 20., 100., (2., 0.1, 0.)), None),
     ('mog', ('ser', 30.3, 19.6, 0., (2., 0.1, 0.), 2.), None),
+    # approx3 (the image's modelMinval): ring-grown regions at the image
+    # edge, off it, for a faint source and through a ModelMask
+    ('mog', ('exp', 0.3, 38.6, 100., (3., 0.2, -0.1)), None, 0.01),
+    ('mog', ('exp', -30.3, 18.6, 100., (3., 0.2, -0.1)), None, 0.01),
+    ('mog', ('exp', 20.3, 19.6, 0.05, (2., 0.2, -0.1)), None, 0.01),
+    ('mog', ('ser', 20.3, 19.6, 100., (2., 0.2, -0.1), 2.2), (10, 8, 25, 22), 0.01),
+    ('mog', ('pt', 49.3, 0.6, 100., None), None, 0.01),
 ]
 
 
@@ -128,11 +141,13 @@ def _same(p, r, tol, what):
 
 
 @pytest.mark.parametrize('case', CASES, ids=[
-    '%s-%s-%s-%s' % (c[0], c[1][0], i, 'mask' if c[2] else 'nomask') for i, c in enumerate(CASES)])
+    '%s-%s-%s-%s%s' % (c[0], c[1][0], i, 'mask' if c[2] else 'nomask',
+                        '-minval' if len(c) > 3 else '') for i, c in enumerate(CASES)])
 def test_corner_case_matches_reference(case, ref_ns, host_only):
-    psf, src, mask = case
-    rp, rd, n = _run(ref_ns, psf, src, mask)
-    op, od, on = _run(_ours(), psf, src, mask)
+    psf, src, mask = case[:3]
+    minval = case[3] if len(case) > 3 else 0.
+    rp, rd, n = _run(ref_ns, psf, src, mask, minval)
+    op, od, on = _run(_ours(), psf, src, mask, minval)
     assert n == on
     _same(op, rp, 1e-6, 'patch')
     # the reference appends one more None to a SersicGalaxy's columns when it
@@ -140,9 +155,9 @@ def test_corner_case_matches_reference(case, ref_ns, host_only):
     assert len(od) == on and len(rd) in (n, n + 1), (len(od), len(rd))
     for j in range(n):
         fourier_step = psf != 'mog' and src[0] != 'pt' and j >= 3
-        index_edge = src[0] == 'ser' and j == 6 and src[5] in (0.995,)
-        masked_f32 = mask == 'bool' and j >= 3
-        tol = 1e-3 if (fourier_step or index_edge) else (1e-4 if masked_f32 else 1e-5)
+        index_edge = src[0] == 'ser' and j == 6 and (src[5] in (0.995,) or minval > 0)
+        f32_columns = (mask == 'bool' and j >= 3) or minval > 0
+        tol = 1e-3 if (fourier_step or index_edge) else (1e-4 if f32_columns else 1e-5)
         _same(od[j], rd[j], tol, 'column %d' % j)
 
 
